@@ -1,0 +1,302 @@
+/*
+ * maul3d_b200 — B200-native step path for the Maul3D rigid-body engine.
+ *
+ * This header is the drop-in C ABI.  Every function in section 2 keeps the
+ * name, signature, argument meaning and error behaviour of the reference
+ * engine's public API (the file:line of the declaration it replaces is
+ * given beside each one), so a host program written against the
+ * reference's include/maul3d/*.h for the features covered here links
+ * against libmaul3d_b200.so unchanged.  Section 3 adds the batched and
+ * device-management entries the reference has no counterpart for.
+ *
+ * Value types and definition structs are laid out byte-for-byte like the
+ * reference's (include/maul3d/math.h:26-66, base.h:69-106, world.h:43-80,
+ * body.h:21-39, shape.h:25-107, joint.h:85-132); the layouts are checked
+ * against the reference build by the parity tests.
+ *
+ * Plain pointers and sizes only; no torch or CUDA types cross this ABI.
+ */
+#ifndef MAUL3D_B200_H
+#define MAUL3D_B200_H
+
+#include <stdbool.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define M3GPU_API __attribute__((visibility("default"))) extern
+#else
+#define M3GPU_API extern
+#endif
+
+/* ---------------------------------------------------------------------
+ * 1. Value types (include/maul3d/math.h:26-66, base.h:69-106)
+ * ------------------------------------------------------------------- */
+typedef float m3real;
+#define M3_PI 3.14159265358979323846f
+#define M3_HASH_INIT 0xCBF29CE484222325ull
+
+typedef struct m3Vec3 { m3real x, y, z; } m3Vec3;
+typedef struct m3Pos3 { double x, y, z; } m3Pos3;
+typedef struct m3Quat { m3real x, y, z, w; } m3Quat;
+typedef struct m3Transform { m3Pos3 p; m3Quat q; } m3Transform;
+typedef struct m3Mat3 { m3Vec3 cx, cy, cz; } m3Mat3;
+
+typedef struct m3WorldId { int32_t index1; uint16_t generation; } m3WorldId;
+typedef struct m3BodyId { int32_t index1; uint16_t world0; uint16_t generation; } m3BodyId;
+typedef struct m3ShapeId { int32_t index1; uint16_t world0; uint16_t generation; } m3ShapeId;
+typedef struct m3JointId { int32_t index1; uint16_t world0; uint16_t generation; } m3JointId;
+
+typedef enum m3BodyType { m3_staticBody = 0, m3_kinematicBody = 1, m3_dynamicBody = 2 } m3BodyType;
+
+typedef enum m3ShapeType {
+    m3_sphereShape = 0,
+    m3_planeShape = 1,
+    m3_hullShape = 2,
+    m3_capsuleShape = 3,
+    m3_meshShape = 4,
+    m3_voxelShape = 5,
+    m3_heightFieldShape = 6
+} m3ShapeType;
+
+typedef enum m3JointType {
+    m3_sphericalJoint = 0,
+    m3_revoluteJoint = 1,
+    m3_prismaticJoint = 2,
+    m3_fixedJoint = 3,
+    m3_distanceJoint = 4,
+    m3_genericJoint = 5,
+    m3_wheelJoint = 6,
+    m3_filterJoint = 7,
+    m3_parallelJoint = 8,
+    m3_motorJoint = 9,
+    m3_gearJoint = 10,
+    m3_pulleyJoint = 11
+} m3JointType;
+
+/* Task hooks (world.h:15-26).  Accepted for ABI compatibility; the device
+ * path ignores them (parallelism comes from the GPU, not host threads). */
+typedef void m3TaskFn(int32_t startIndex, int32_t endIndex, void* taskContext);
+typedef void* m3EnqueueTaskFn(m3TaskFn* task, int32_t itemCount, int32_t minRange,
+                              void* taskContext, void* userContext);
+typedef void m3FinishTaskFn(void* userTask, void* userContext);
+
+/* world.h:43-80 */
+typedef struct m3WorldDef {
+    m3Vec3 gravity;
+    int32_t bodyCapacity;
+    int32_t shapeCapacity;
+    int32_t meshCapacity;
+    int32_t jointCapacity;
+    int32_t voxelCapacity;
+    int32_t characterCapacity;
+    int32_t vehicleCapacity;
+    int32_t softBodyCapacity;
+    int32_t workerCount;
+    m3EnqueueTaskFn* enqueueTask;
+    m3FinishTaskFn* finishTask;
+    void* userTaskContext;
+    float contactHertz;
+    float contactDampingRatio;
+    float contactPushMaxSpeed;
+    float restitutionThreshold;
+    float maximumLinearSpeed;
+    int32_t enableSleeping;
+    int32_t enableContinuous;
+    float hitEventThreshold;
+    int32_t internalValue;
+} m3WorldDef;
+
+/* body.h:21-39 */
+typedef struct m3BodyDef {
+    int32_t type;
+    m3Pos3 position;
+    m3Quat rotation;
+    m3Vec3 linearVelocity;
+    m3Vec3 angularVelocity;
+    float gravityScale;
+    float linearDamping;
+    float angularDamping;
+    uint64_t userData;
+    bool isBullet;
+    int32_t internalValue;
+} m3BodyDef;
+
+/* shape.h:25-38, 102-107 */
+typedef struct m3Sphere { m3Vec3 center; m3real radius; } m3Sphere;
+typedef struct m3Plane { m3Vec3 normal; m3real offset; } m3Plane;
+typedef struct m3Capsule { m3Vec3 point1; m3Vec3 point2; m3real radius; } m3Capsule;
+
+/* shape.h:40-74 */
+typedef struct m3ShapeDef {
+    float density;
+    float friction;
+    float restitution;
+    uint64_t categoryBits;
+    uint64_t maskBits;
+    int32_t groupIndex;
+    float rollingResistance;
+    uint64_t userData;
+    bool isSensor;
+    bool enableHitEvents;
+    bool enablePreSolveEvents;
+    m3Vec3 localPosition;
+    m3Quat localRotation;
+    int32_t internalValue;
+} m3ShapeDef;
+
+/* joint.h:85-132 */
+typedef struct m3JointDef {
+    int32_t type;
+    m3BodyId bodyA;
+    m3BodyId bodyB;
+    m3Vec3 localAnchorA;
+    m3Vec3 localAnchorB;
+    m3Vec3 localAxisA;
+    m3Vec3 localAxisB;
+    bool enableLimit;
+    m3real lowerLimit;
+    m3real upperLimit;
+    bool enableMotor;
+    m3real motorSpeed;
+    m3real maxMotorEffort;
+    bool enableCone;
+    m3real coneAngle;
+    bool collideConnected;
+    uint8_t genericLinear[3];
+    uint8_t genericAngular[3];
+    uint8_t genericMotorAxis;
+    uint8_t genericReserved;
+    m3real genericLinearLower[3];
+    m3real genericLinearUpper[3];
+    m3real genericAngularLower[3];
+    m3real genericAngularUpper[3];
+    m3real ratio;
+    m3Pos3 groundAnchorA;
+    m3Pos3 groundAnchorB;
+    int32_t internalValue;
+} m3JointDef;
+
+/* ---------------------------------------------------------------------
+ * 2. Drop-in entry points (reference names and semantics)
+ * ------------------------------------------------------------------- */
+
+/* core.c:40 (base.h:38): major*10000 + minor*100 + patch of the engine
+ * release whose step this library reproduces (1.22.0). */
+M3GPU_API int m3GetVersion(void);
+
+/* core.c:46 (base.h:110): FNV-1a 64 over `count` bytes. */
+M3GPU_API uint64_t m3Hash64(uint64_t h, const void* bytes, int32_t count);
+
+/* world.c:64 (world.h:88): pinned defaults; gravity (0,-10,0), 1024
+ * bodies, 2048 shapes, 64 joints, tuning knobs at the reference values. */
+M3GPU_API m3WorldDef m3DefaultWorldDef(void);
+/* world.c:90 (world.h:92): null id on an invalid def or a full table. */
+M3GPU_API m3WorldId m3CreateWorld(const m3WorldDef* def);
+/* world.h:93 */
+M3GPU_API void m3DestroyWorld(m3WorldId worldId);
+/* world.h:94 */
+M3GPU_API bool m3World_IsValid(m3WorldId worldId);
+
+/* solver.c:4322 (world.h:195): one step of `dt` seconds in `substeps`
+ * substeps, computed on the GPU.  Refuses (no-op) a stale id, dt <= 0 or
+ * substeps outside [1, 256], like the reference.  A device-side refusal
+ * (a capacity or feature the device path does not cover) leaves the
+ * world unstepped and is reported by m3gpu_last_error(). */
+M3GPU_API void m3World_Step(m3WorldId worldId, float dt, int32_t substeps);
+
+/* snapshot.c:932 (world.h:510): FNV-1a over the curated world state,
+ * bit-identical to the reference's hash for the same world. 0 for a
+ * stale id. */
+M3GPU_API uint64_t m3World_Hash(m3WorldId worldId);
+
+/* body.c:35 (body.h:43) / body.h:49 / body.h:56-59 */
+M3GPU_API m3BodyDef m3DefaultBodyDef(void);
+M3GPU_API m3BodyId m3CreateBody(m3WorldId worldId, const m3BodyDef* def);
+M3GPU_API bool m3Body_IsValid(m3BodyId bodyId);
+M3GPU_API m3Pos3 m3Body_GetPosition(m3BodyId bodyId);
+M3GPU_API m3Quat m3Body_GetRotation(m3BodyId bodyId);
+M3GPU_API m3Vec3 m3Body_GetLinearVelocity(m3BodyId bodyId);
+M3GPU_API m3Vec3 m3Body_GetAngularVelocity(m3BodyId bodyId);
+/* body.h: awake query (dynamic bodies sleep; others report true) */
+M3GPU_API bool m3Body_IsAwake(m3BodyId bodyId);
+
+/* shape.c:31 (shape.h:78) and the creators shape.c:763/782/802/1334 */
+M3GPU_API m3ShapeDef m3DefaultShapeDef(void);
+M3GPU_API m3ShapeId m3CreateSphereShape(m3BodyId bodyId, const m3ShapeDef* def,
+                                        const m3Sphere* sphere);
+M3GPU_API m3ShapeId m3CreatePlaneShape(m3BodyId bodyId, const m3ShapeDef* def,
+                                       const m3Plane* plane);
+M3GPU_API m3ShapeId m3CreateCapsuleShape(m3BodyId bodyId, const m3ShapeDef* def,
+                                         const m3Capsule* capsule);
+M3GPU_API m3ShapeId m3CreateBoxShape(m3BodyId bodyId, const m3ShapeDef* def,
+                                     m3Vec3 halfExtents);
+M3GPU_API bool m3Shape_IsValid(m3ShapeId shapeId);
+
+/* joint.c:15 (joint.h:134) and joint.h:136: spherical, revolute and
+ * fixed joints are stepped on the device. */
+M3GPU_API m3JointDef m3DefaultJointDef(void);
+M3GPU_API m3JointId m3CreateJoint(const m3JointDef* def);
+M3GPU_API bool m3Joint_IsValid(m3JointId jointId);
+
+/* ---------------------------------------------------------------------
+ * 3. Device extensions (no reference counterpart)
+ * ------------------------------------------------------------------- */
+
+/* Error codes reported by m3gpu_last_error(). */
+#define M3GPU_OK 0
+#define M3GPU_ERR_INVALID 1      /* bad argument or stale id */
+#define M3GPU_ERR_CUDA 2         /* a CUDA call failed (message available) */
+#define M3GPU_ERR_CAPACITY 3     /* pair table full: the world stalled */
+#define M3GPU_ERR_UNSUPPORTED 4  /* a feature the device path does not cover */
+#define M3GPU_ERR_NO_DEVICE 5    /* no CUDA device visible */
+
+/* Last error raised on the calling thread's most recent m3gpu or drop-in
+ * call, and a one-line message for it (never NULL). */
+M3GPU_API int32_t m3gpu_last_error(void);
+M3GPU_API const char* m3gpu_last_error_message(void);
+
+/* Step `count` independent worlds `steps` times each in ONE batched
+ * launch sequence (one CTA per world; a CUDA graph captures the step).
+ * Equivalent, world by world and bit for bit, to calling m3World_Step on
+ * each world in turn.  Returns M3GPU_OK or an error code; on error no
+ * world is partially stepped past the failing step. */
+M3GPU_API int32_t m3gpu_step_worlds(const m3WorldId* worlds, int32_t count, float dt,
+                                    int32_t substeps, int32_t steps);
+
+/* World hashes of `count` worlds computed on the device (one thread per
+ * world), written to out[i].  Same values as m3World_Hash. */
+M3GPU_API int32_t m3gpu_hash_worlds(const m3WorldId* worlds, int32_t count, uint64_t* out);
+
+/* Wait for all device work of the library to finish. */
+M3GPU_API int32_t m3gpu_synchronize(void);
+
+/* Kernel launches the library issued since process start (the evidence
+ * a device step really ran), and elapsed device time in milliseconds of
+ * the last m3gpu_step_worlds call measured with CUDA events. */
+M3GPU_API int64_t m3gpu_launch_count(void);
+M3GPU_API float m3gpu_last_step_ms(void);
+
+/* White-box readback for parity tests.  Each copies [0, maxIndex) (or
+ * [0, pairCount)) records in the reference's byte layout and returns the
+ * record count, or -1 when `cap` is too small or the id is stale. */
+M3GPU_API int32_t m3gpu_body_max(m3WorldId world);
+M3GPU_API int32_t m3gpu_pair_count(m3WorldId world);
+M3GPU_API int32_t m3gpu_copy_bodies(m3WorldId world, void* transforms, void* lin, void* ang,
+                                    uint8_t* awake, float* sleepTimes, int32_t cap);
+M3GPU_API int32_t m3gpu_copy_mass(m3WorldId world, float* invMass, void* invInertia,
+                                  void* inertia, void* localCenters, float* minExt,
+                                  float* maxExt, int32_t cap);
+M3GPU_API int32_t m3gpu_copy_pairs(m3WorldId world, uint64_t* keys, void* manifolds,
+                                   int32_t cap);
+M3GPU_API int32_t m3gpu_copy_joints(m3WorldId world, void* impulse, void* perp, void* limit,
+                                    void* angular, int32_t cap);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MAUL3D_B200_H */

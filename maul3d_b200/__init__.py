@@ -1,0 +1,164 @@
+"""maul3d_b200: the Maul3D step path on NVIDIA B200 (sm_100a).
+
+Python host mirror of the reference engine's public API for the step
+path (include/maul3d/world.h: m3World_Step, m3World_Hash), bound to the
+in-tree shared library libmaul3d_b200.so over its C ABI.  There is no
+Python or CPU fallback: if the library is missing, importing this
+package raises, and stepping without a CUDA device raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+from . import abi
+from .abi import MANIFOLD, TRANSFORM, VEC3, MAT3, WorldState, m3WorldId
+
+_LIB_PATH = Path(__file__).resolve().parent / "libmaul3d_b200.so"
+
+M3GPU_OK = 0
+M3GPU_ERR_INVALID = 1
+M3GPU_ERR_CUDA = 2
+M3GPU_ERR_CAPACITY = 3
+M3GPU_ERR_UNSUPPORTED = 4
+M3GPU_ERR_NO_DEVICE = 5
+
+
+class M3GpuError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"maul3d_b200 error {code}: {message}")
+        self.code = code
+
+
+def _load() -> C.CDLL:
+    if not _LIB_PATH.exists():
+        raise ImportError(
+            f"{_LIB_PATH} is missing: build it with `python -m maul3d_b200.build` "
+            "(the CUDA path has no CPU fallback)")
+    lib = C.CDLL(str(_LIB_PATH))
+    abi.bind_common(lib)
+    lib.m3gpu_last_error.restype = C.c_int32
+    lib.m3gpu_last_error_message.restype = C.c_char_p
+    lib.m3gpu_step_worlds.argtypes = [C.POINTER(m3WorldId), C.c_int32, C.c_float, C.c_int32, C.c_int32]
+    lib.m3gpu_step_worlds.restype = C.c_int32
+    lib.m3gpu_hash_worlds.argtypes = [C.POINTER(m3WorldId), C.c_int32, C.POINTER(C.c_uint64)]
+    lib.m3gpu_hash_worlds.restype = C.c_int32
+    lib.m3gpu_synchronize.restype = C.c_int32
+    lib.m3gpu_launch_count.restype = C.c_int64
+    lib.m3gpu_last_step_ms.restype = C.c_float
+    lib.m3gpu_body_max.argtypes = [m3WorldId]
+    lib.m3gpu_body_max.restype = C.c_int32
+    lib.m3gpu_pair_count.argtypes = [m3WorldId]
+    lib.m3gpu_pair_count.restype = C.c_int32
+    for name, n in (("m3gpu_copy_bodies", 5), ("m3gpu_copy_pairs", 2), ("m3gpu_copy_joints", 4)):
+        fn = getattr(lib, name)
+        fn.argtypes = [m3WorldId] + [C.c_void_p] * n + [C.c_int32]
+        fn.restype = C.c_int32
+    lib.m3gpu_copy_mass.argtypes = [m3WorldId] + [C.c_void_p] * 6 + [C.c_int32]
+    lib.m3gpu_copy_mass.restype = C.c_int32
+    return lib
+
+
+lib = _load()
+
+
+def last_error() -> tuple[int, str]:
+    return int(lib.m3gpu_last_error()), lib.m3gpu_last_error_message().decode()
+
+
+def _check(rc: int) -> None:
+    if rc != M3GPU_OK:
+        code, msg = last_error()
+        raise M3GpuError(rc, msg)
+
+
+def _ids(worlds) -> "C.Array":
+    arr = (m3WorldId * len(worlds))()
+    for i, w in enumerate(worlds):
+        arr[i] = w.id
+    return arr
+
+
+class World:
+    """One world living in this library (host image + HBM slab)."""
+
+    def __init__(self, wid: m3WorldId):
+        if wid.index1 == 0:
+            code, msg = last_error()
+            raise M3GpuError(code or M3GPU_ERR_INVALID, msg)
+        self.id = wid
+
+    @classmethod
+    def scene(cls, scene: int, seed: int = 0, param: int = 0) -> "World":
+        """Build one of the seeded synthetic scenes (csrc/scenes.c)."""
+        return cls(lib.m3s_build(scene, seed, param))
+
+    def step(self, dt: float = 1.0 / 60.0, substeps: int = 4, steps: int = 1) -> None:
+        _check(lib.m3gpu_step_worlds(_ids([self]), 1, dt, substeps, steps))
+
+    def hash(self) -> int:
+        h = int(lib.m3World_Hash(self.id))
+        code, msg = last_error()
+        if code != M3GPU_OK:
+            raise M3GpuError(code, msg)
+        return h
+
+    def destroy(self) -> None:
+        lib.m3DestroyWorld(self.id)
+
+    def body_count(self) -> int:
+        return int(lib.m3gpu_body_max(self.id))
+
+    def state(self) -> WorldState:
+        n = self.body_count()
+        xf = np.zeros(n, TRANSFORM)
+        lin = np.zeros(n, VEC3)
+        ang = np.zeros(n, VEC3)
+        awake = np.zeros(n, np.uint8)
+        sleep = np.zeros(n, np.float32)
+        got = lib.m3gpu_copy_bodies(self.id, xf.ctypes.data, lin.ctypes.data, ang.ctypes.data,
+                                    awake.ctypes.data, sleep.ctypes.data, n)
+        if got < 0:
+            raise M3GpuError(M3GPU_ERR_INVALID, "body readback failed")
+        p = int(lib.m3gpu_pair_count(self.id))
+        keys = np.zeros(max(p, 0), np.uint64)
+        man = np.zeros(max(p, 0), MANIFOLD)
+        if p > 0:
+            lib.m3gpu_copy_pairs(self.id, keys.ctypes.data, man.ctypes.data, p)
+        return WorldState(xf, lin, ang, awake, sleep, keys, man)
+
+    def mass(self) -> dict:
+        n = self.body_count()
+        out = {"invMass": np.zeros(n, np.float32), "invInertia": np.zeros(n, MAT3),
+               "inertia": np.zeros(n, MAT3), "localCenter": np.zeros(n, VEC3),
+               "minExtent": np.zeros(n, np.float32), "maxExtent": np.zeros(n, np.float32)}
+        lib.m3gpu_copy_mass(self.id, *[out[k].ctypes.data for k in
+                                       ("invMass", "invInertia", "inertia", "localCenter",
+                                        "minExtent", "maxExtent")], n)
+        return out
+
+
+def step_worlds(worlds, dt: float = 1.0 / 60.0, substeps: int = 4, steps: int = 1) -> None:
+    """Step many worlds in one batched launch sequence (one block per world)."""
+    _check(lib.m3gpu_step_worlds(_ids(worlds), len(worlds), dt, substeps, steps))
+
+
+def hash_worlds(worlds) -> np.ndarray:
+    """World hashes computed on the device, one thread per world."""
+    out = (C.c_uint64 * len(worlds))()
+    _check(lib.m3gpu_hash_worlds(_ids(worlds), len(worlds), out))
+    return np.array(list(out), dtype=np.uint64)
+
+
+def synchronize() -> None:
+    _check(lib.m3gpu_synchronize())
+
+
+def launch_count() -> int:
+    return int(lib.m3gpu_launch_count())
+
+
+def last_step_ms() -> float:
+    return float(lib.m3gpu_last_step_ms())

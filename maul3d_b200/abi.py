@@ -1,0 +1,103 @@
+"""ctypes mirror of the C ABI in include/maul3d_b200.h.
+
+The value types and the drop-in entry points have the reference engine's
+names and layouts, so the same declarations bind both this library and a
+reference build; `bind_common` declares them on any handle.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+
+class m3Vec3(C.Structure):
+    _fields_ = [("x", C.c_float), ("y", C.c_float), ("z", C.c_float)]
+
+
+class m3Pos3(C.Structure):
+    _fields_ = [("x", C.c_double), ("y", C.c_double), ("z", C.c_double)]
+
+
+class m3Quat(C.Structure):
+    _fields_ = [("x", C.c_float), ("y", C.c_float), ("z", C.c_float), ("w", C.c_float)]
+
+
+class m3WorldId(C.Structure):
+    _fields_ = [("index1", C.c_int32), ("generation", C.c_uint16)]
+
+
+class m3BodyId(C.Structure):
+    _fields_ = [("index1", C.c_int32), ("world0", C.c_uint16), ("generation", C.c_uint16)]
+
+
+# Record dtypes in the reference's byte layouts (world_internal.h).
+TRANSFORM = np.dtype([("p", "<f8", 3), ("q", "<f4", 4)])  # 40 bytes
+VEC3 = np.dtype(("<f4", 3))
+MAT3 = np.dtype(("<f4", 9))
+MANIFOLD_POINT = np.dtype([("anchorA", "<f4", 3), ("anchorB", "<f4", 3), ("separation", "<f4"),
+                           ("normalImpulse", "<f4"), ("id", "<u2"), ("flags", "<u2")])
+MANIFOLD = np.dtype([("normal", "<f4", 3), ("pointCount", "<i4"), ("frictionImpulse", "<f4", 3),
+                     ("twistImpulse", "<f4"), ("rollingImpulse", "<f4", 3),
+                     ("points", MANIFOLD_POINT, 4)])
+assert TRANSFORM.itemsize == 40 and MANIFOLD.itemsize == 188
+
+SCENE_SPHERE_PYRAMID = 0
+SCENE_BOX_PYRAMID = 1
+SCENE_UNEVEN = 2
+SCENE_FREEFALL = 3
+
+
+def _ptr(a: np.ndarray) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data)
+
+
+def bind_common(lib: C.CDLL) -> C.CDLL:
+    """Declare the reference-named entry points shared by both engines."""
+    lib.m3World_Step.argtypes = [m3WorldId, C.c_float, C.c_int32]
+    lib.m3World_Step.restype = None
+    lib.m3World_Hash.argtypes = [m3WorldId]
+    lib.m3World_Hash.restype = C.c_uint64
+    lib.m3DestroyWorld.argtypes = [m3WorldId]
+    lib.m3DestroyWorld.restype = None
+    lib.m3World_IsValid.argtypes = [m3WorldId]
+    lib.m3World_IsValid.restype = C.c_bool
+    lib.m3s_build.argtypes = [C.c_int32, C.c_uint64, C.c_int32]
+    lib.m3s_build.restype = m3WorldId
+    lib.m3s_uneven_size.argtypes = [C.c_uint64, C.c_int32, C.c_int32, C.c_int32]
+    lib.m3s_uneven_size.restype = C.c_int32
+    lib.m3Hash64.argtypes = [C.c_uint64, C.c_void_p, C.c_int32]
+    lib.m3Hash64.restype = C.c_uint64
+    lib.m3GetVersion.argtypes = []
+    lib.m3GetVersion.restype = C.c_int
+    return lib
+
+
+class WorldState:
+    """Readback of one world's per-step state in the reference layouts."""
+
+    def __init__(self, transforms, lin, ang, awake, sleep, keys, manifolds):
+        self.transforms = transforms
+        self.lin = lin
+        self.ang = ang
+        self.awake = awake
+        self.sleep = sleep
+        self.keys = keys
+        self.manifolds = manifolds
+
+    def first_difference(self, other: "WorldState") -> str | None:
+        """Describe the first field where two states differ, or None."""
+        checks = [("pair keys", self.keys, other.keys), ("transforms", self.transforms, other.transforms),
+                  ("linear velocity", self.lin, other.lin), ("angular velocity", self.ang, other.ang),
+                  ("awake", self.awake, other.awake), ("sleep time", self.sleep, other.sleep),
+                  ("manifolds", self.manifolds, other.manifolds)]
+        for name, a, b in checks:
+            if a.shape != b.shape:
+                return f"{name}: shape {a.shape} vs {b.shape}"
+            ab = a.view(np.uint8).reshape(len(a), -1) if len(a) else a.view(np.uint8)
+            bb = b.view(np.uint8).reshape(len(b), -1) if len(b) else b.view(np.uint8)
+            if not np.array_equal(ab, bb):
+                rows = np.nonzero((ab != bb).any(axis=1))[0]
+                i = int(rows[0])
+                return f"{name}: first differing record {i} of {len(a)} ({len(rows)} differ): {a[i]} vs {b[i]}"
+        return None

@@ -1,0 +1,228 @@
+// The exported C ABI glue: error state, the drop-in step and hash
+// entries (solver.c:4322-4355, snapshot.c:932), the batched device
+// entries and the white-box readbacks the parity tests use.
+
+#include "m3_world.h"
+#include "m3_hash.h"
+
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <vector>
+
+static thread_local int32_t t_error = M3GPU_OK;
+static thread_local char t_message[512] = "ok";
+
+int32_t m3gpuSetError(int32_t code, const char* fmt, ...)
+{
+    t_error = code;
+    va_list args;
+    va_start(args, fmt);
+    vsnprintf(t_message, sizeof(t_message), fmt, args);
+    va_end(args);
+    return code;
+}
+
+void m3gpuClearError(void)
+{
+    t_error = M3GPU_OK;
+    strcpy(t_message, "ok");
+}
+
+extern "C" int32_t m3gpu_last_error(void)
+{
+    return t_error;
+}
+
+extern "C" const char* m3gpu_last_error_message(void)
+{
+    return t_message;
+}
+
+extern "C" int m3GetVersion(void)
+{
+    return 1 * 10000 + 22 * 100 + 0;
+}
+
+extern "C" uint64_t m3Hash64(uint64_t h, const void* bytes, int32_t count)
+{
+    return m3Fnv(h, bytes, count);
+}
+
+extern "C" void m3World_Step(m3WorldId worldId, float dt, int32_t substeps)
+{
+    m3gpuClearError();
+    m3HostWorld* w = m3gpuWorldFromId(worldId);
+    if (w == nullptr || !(dt > 0.0f) || substeps < 1 || substeps > M3_MAX_SUBSTEPS)
+    {
+        m3gpuSetError(M3GPU_ERR_INVALID, "m3World_Step: stale world or invalid dt/substeps");
+        return;
+    }
+    m3gpuStepBatch(&w, 1, dt, substeps, 1);
+}
+
+extern "C" uint64_t m3World_Hash(m3WorldId worldId)
+{
+    m3gpuClearError();
+    m3HostWorld* w = m3gpuWorldFromId(worldId);
+    if (w == nullptr)
+    {
+        return 0;
+    }
+    if (w->deviceAhead)
+    {
+        uint64_t h = 0;
+        if (m3gpuHashBatch(&w, 1, &h) == M3GPU_OK)
+        {
+            return h;
+        }
+        return 0;
+    }
+    m3WorldView view = w->hv;
+    view.hulls = w->hulls.empty() ? nullptr : w->hulls.data();
+    return m3WorldHashView(&view);
+}
+
+static int32_t Resolve(const m3WorldId* ids, int32_t count, std::vector<m3HostWorld*>& out)
+{
+    if (ids == nullptr || count <= 0)
+    {
+        return m3gpuSetError(M3GPU_ERR_INVALID, "empty world list");
+    }
+    out.resize((size_t)count);
+    for (int32_t i = 0; i < count; ++i)
+    {
+        out[(size_t)i] = m3gpuWorldFromId(ids[i]);
+        if (out[(size_t)i] == nullptr)
+        {
+            return m3gpuSetError(M3GPU_ERR_INVALID, "stale world id at position %d", i);
+        }
+    }
+    return M3GPU_OK;
+}
+
+extern "C" int32_t m3gpu_step_worlds(const m3WorldId* worlds, int32_t count, float dt,
+                                     int32_t substeps, int32_t steps)
+{
+    m3gpuClearError();
+    if (!(dt > 0.0f) || substeps < 1 || substeps > M3_MAX_SUBSTEPS || steps < 0)
+    {
+        return m3gpuSetError(M3GPU_ERR_INVALID, "invalid dt, substeps or steps");
+    }
+    std::vector<m3HostWorld*> ws;
+    int32_t rc = Resolve(worlds, count, ws);
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
+    if (steps == 0)
+    {
+        return M3GPU_OK;
+    }
+    return m3gpuStepBatch(ws.data(), count, dt, substeps, steps);
+}
+
+extern "C" int32_t m3gpu_hash_worlds(const m3WorldId* worlds, int32_t count, uint64_t* out)
+{
+    m3gpuClearError();
+    std::vector<m3HostWorld*> ws;
+    int32_t rc = Resolve(worlds, count, ws);
+    if (rc != M3GPU_OK || out == nullptr)
+    {
+        return rc != M3GPU_OK ? rc : m3gpuSetError(M3GPU_ERR_INVALID, "null output");
+    }
+    return m3gpuHashBatch(ws.data(), count, out);
+}
+
+// ----------------------------------------------------------------------
+// White-box readbacks
+// ----------------------------------------------------------------------
+static m3HostWorld* Synced(m3WorldId id)
+{
+    m3HostWorld* w = m3gpuWorldFromId(id);
+    if (w == nullptr || m3gpuSyncHost(w) != M3GPU_OK)
+    {
+        return nullptr;
+    }
+    return w;
+}
+
+extern "C" int32_t m3gpu_body_max(m3WorldId world)
+{
+    m3HostWorld* w = m3gpuWorldFromId(world);
+    return w ? w->hv.sc->bodyMax : -1;
+}
+
+extern "C" int32_t m3gpu_pair_count(m3WorldId world)
+{
+    m3HostWorld* w = Synced(world);
+    return w ? w->hv.sc->pairCount : -1;
+}
+
+extern "C" int32_t m3gpu_copy_bodies(m3WorldId world, void* transforms, void* lin, void* ang,
+                                     uint8_t* awake, float* sleepTimes, int32_t cap)
+{
+    m3HostWorld* w = Synced(world);
+    if (w == nullptr || cap < w->hv.sc->bodyMax)
+    {
+        return -1;
+    }
+    int32_t n = w->hv.sc->bodyMax;
+    memcpy(transforms, w->hv.xf, (size_t)n * sizeof(m3Transform));
+    memcpy(lin, w->hv.v, (size_t)n * sizeof(m3Vec3));
+    memcpy(ang, w->hv.w, (size_t)n * sizeof(m3Vec3));
+    memcpy(awake, w->hv.awake, (size_t)n);
+    memcpy(sleepTimes, w->hv.sleepTime, (size_t)n * sizeof(float));
+    return n;
+}
+
+extern "C" int32_t m3gpu_copy_mass(m3WorldId world, float* invMass, void* invInertia,
+                                   void* inertia, void* localCenters, float* minExt,
+                                   float* maxExt, int32_t cap)
+{
+    m3HostWorld* w = Synced(world);
+    if (w == nullptr || cap < w->hv.sc->bodyMax)
+    {
+        return -1;
+    }
+    int32_t n = w->hv.sc->bodyMax;
+    memcpy(invMass, w->hv.invMass, (size_t)n * sizeof(float));
+    memcpy(invInertia, w->hv.invI, (size_t)n * sizeof(m3Mat3));
+    memcpy(inertia, w->hv.inertia, (size_t)n * sizeof(m3Mat3));
+    memcpy(localCenters, w->hv.lc, (size_t)n * sizeof(m3Vec3));
+    memcpy(minExt, w->hv.minExt, (size_t)n * sizeof(float));
+    memcpy(maxExt, w->hv.maxExt, (size_t)n * sizeof(float));
+    return n;
+}
+
+extern "C" int32_t m3gpu_copy_pairs(m3WorldId world, uint64_t* keys, void* manifolds, int32_t cap)
+{
+    m3HostWorld* w = Synced(world);
+    if (w == nullptr || cap < w->hv.sc->pairCount)
+    {
+        return -1;
+    }
+    int32_t n = w->hv.sc->pairCount;
+    const uint64_t* k = w->hv.sc->pairBuf == 0 ? w->hv.keys0 : w->hv.keys1;
+    const m3Manifold* m = w->hv.sc->pairBuf == 0 ? w->hv.man0 : w->hv.man1;
+    memcpy(keys, k, (size_t)n * sizeof(uint64_t));
+    memcpy(manifolds, m, (size_t)n * sizeof(m3Manifold));
+    return n;
+}
+
+extern "C" int32_t m3gpu_copy_joints(m3WorldId world, void* impulse, void* perp, void* limit,
+                                     void* angular, int32_t cap)
+{
+    m3HostWorld* w = Synced(world);
+    if (w == nullptr || cap < w->hv.sc->jointMax)
+    {
+        return -1;
+    }
+    int32_t n = w->hv.sc->jointMax;
+    memcpy(impulse, w->hv.jimpulse, (size_t)n * sizeof(m3Vec3));
+    memcpy(perp, w->hv.jperp, (size_t)n * sizeof(m3Vec3));
+    memcpy(limit, w->hv.jlimitImp, (size_t)n * sizeof(m3Vec3));
+    memcpy(angular, w->hv.jangular, (size_t)n * sizeof(m3Vec3));
+    return n;
+}

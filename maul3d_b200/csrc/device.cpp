@@ -1,0 +1,202 @@
+// Device residency of worlds: one HBM slab per world (persistent image
+// followed by the step's scratch), one device hull pool per world, and
+// the host<->device copies that keep the host image and the slab in
+// agreement.  A world is uploaded whole before its first device step
+// after any host-side change; the host image is refreshed lazily, only
+// the sections a step can change (bodies, joints, the current pair
+// lists, the scalars).
+
+#include "m3_world.h"
+
+#include <cuda_runtime.h>
+
+#include <string.h>
+
+static int s_deviceState = 0; // 0 unknown, 1 ready, -1 absent
+
+int32_t m3gpuEnsureDevice(void)
+{
+    if (s_deviceState == 1)
+    {
+        return M3GPU_OK;
+    }
+    if (s_deviceState == -1)
+    {
+        return m3gpuSetError(M3GPU_ERR_NO_DEVICE, "no CUDA device is visible");
+    }
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count <= 0)
+    {
+        s_deviceState = -1;
+        cudaGetLastError();
+        return m3gpuSetError(M3GPU_ERR_NO_DEVICE, "no CUDA device is visible (%s)",
+                             cudaGetErrorString(e));
+    }
+    s_deviceState = 1;
+    return M3GPU_OK;
+}
+
+static int32_t CudaCheck(cudaError_t e, const char* what)
+{
+    if (e != cudaSuccess)
+    {
+        return m3gpuSetError(M3GPU_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    }
+    return M3GPU_OK;
+}
+
+// Offsets of a field inside the host image.
+static int64_t Offset(const m3HostWorld* w, const void* hostPtr)
+{
+    return (int64_t)((const uint8_t*)hostPtr - w->image.data());
+}
+
+static void BuildDeviceView(m3HostWorld* w)
+{
+    m3LayoutPersistent(&w->dv, w->dslab, w->bodyCap, w->shapeCap, w->jointCap, w->pairCap);
+    w->dv.hulls = w->dhulls;
+    w->dv.scratch = w->dslab + w->persistentBytes;
+    w->dv.scratchBytes = w->scratchBytes;
+}
+
+int32_t m3gpuUpload(m3HostWorld* w)
+{
+    int32_t rc = m3gpuEnsureDevice();
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
+    if (w->dslab == nullptr)
+    {
+        w->scratchBytes = m3gpuScratchBytes(w->bodyCap, w->shapeCap, w->jointCap, w->pairCap);
+        w->dslabBytes = w->persistentBytes + w->scratchBytes;
+        rc = CudaCheck(cudaMalloc((void**)&w->dslab, (size_t)w->dslabBytes), "cudaMalloc(slab)");
+        if (rc != M3GPU_OK)
+        {
+            w->dslab = nullptr;
+            return rc;
+        }
+    }
+    int32_t hullCount = (int32_t)w->hulls.size();
+    if (hullCount > w->dhullCap)
+    {
+        if (w->dhulls != nullptr)
+        {
+            cudaFree(w->dhulls);
+            w->dhulls = nullptr;
+        }
+        int32_t cap = hullCount < 4 ? 4 : hullCount;
+        rc = CudaCheck(cudaMalloc((void**)&w->dhulls, (size_t)cap * sizeof(m3HullData)),
+                       "cudaMalloc(hulls)");
+        if (rc != M3GPU_OK)
+        {
+            w->dhullCap = 0;
+            return rc;
+        }
+        w->dhullCap = cap;
+    }
+    if (w->dhulls == nullptr)
+    {
+        rc = CudaCheck(cudaMalloc((void**)&w->dhulls, 4 * sizeof(m3HullData)), "cudaMalloc(hulls)");
+        if (rc != M3GPU_OK)
+        {
+            return rc;
+        }
+        w->dhullCap = 4;
+    }
+    BuildDeviceView(w);
+    rc = CudaCheck(cudaMemcpy(w->dslab, w->image.data(), (size_t)w->persistentBytes,
+                              cudaMemcpyHostToDevice),
+                   "upload world image");
+    if (rc == M3GPU_OK && hullCount > 0)
+    {
+        rc = CudaCheck(cudaMemcpy(w->dhulls, w->hulls.data(),
+                                  (size_t)hullCount * sizeof(m3HullData), cudaMemcpyHostToDevice),
+                       "upload hulls");
+    }
+    if (rc == M3GPU_OK)
+    {
+        w->hostDirty = false;
+    }
+    return rc;
+}
+
+int32_t m3gpuDownload(m3HostWorld* w)
+{
+    if (w->dslab == nullptr)
+    {
+        return M3GPU_OK;
+    }
+    // Scalars first: they say which pair buffer is current and how long.
+    int32_t rc = CudaCheck(cudaMemcpy(w->hv.sc, w->dv.sc, sizeof(m3WorldScalars),
+                                      cudaMemcpyDeviceToHost),
+                           "download scalars");
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
+    // Body section: [xf, shapeBody).
+    int64_t b0 = Offset(w, w->hv.xf);
+    int64_t b1 = Offset(w, w->hv.shapeBody);
+    rc = CudaCheck(cudaMemcpy(w->image.data() + b0, w->dslab + b0, (size_t)(b1 - b0),
+                              cudaMemcpyDeviceToHost),
+                   "download bodies");
+    // Joint section: [jtype, keys0).
+    int64_t j0 = Offset(w, w->hv.jtype);
+    int64_t j1 = Offset(w, w->hv.keys0);
+    if (rc == M3GPU_OK)
+    {
+        rc = CudaCheck(cudaMemcpy(w->image.data() + j0, w->dslab + j0, (size_t)(j1 - j0),
+                                  cudaMemcpyDeviceToHost),
+                       "download joints");
+    }
+    // The current pair lists up to pairCount.
+    int32_t n = w->hv.sc->pairCount;
+    if (rc == M3GPU_OK && n > 0)
+    {
+        uint64_t* hk = w->hv.sc->pairBuf == 0 ? w->hv.keys0 : w->hv.keys1;
+        uint64_t* dk = w->hv.sc->pairBuf == 0 ? w->dv.keys0 : w->dv.keys1;
+        m3Manifold* hm = w->hv.sc->pairBuf == 0 ? w->hv.man0 : w->hv.man1;
+        m3Manifold* dm = w->hv.sc->pairBuf == 0 ? w->dv.man0 : w->dv.man1;
+        rc = CudaCheck(cudaMemcpy(hk, dk, (size_t)n * sizeof(uint64_t), cudaMemcpyDeviceToHost),
+                       "download pair keys");
+        if (rc == M3GPU_OK)
+        {
+            rc = CudaCheck(
+                cudaMemcpy(hm, dm, (size_t)n * sizeof(m3Manifold), cudaMemcpyDeviceToHost),
+                "download manifolds");
+        }
+    }
+    if (rc == M3GPU_OK)
+    {
+        w->deviceAhead = false;
+    }
+    return rc;
+}
+
+int32_t m3gpuSyncHost(m3HostWorld* w)
+{
+    if (!w->deviceAhead)
+    {
+        return M3GPU_OK;
+    }
+    return m3gpuDownload(w);
+}
+
+void m3gpuRelease(m3HostWorld* w)
+{
+    if (w->dslab != nullptr)
+    {
+        cudaFree(w->dslab);
+        w->dslab = nullptr;
+    }
+    if (w->dhulls != nullptr)
+    {
+        cudaFree(w->dhulls);
+        w->dhulls = nullptr;
+    }
+    w->dhullCap = 0;
+    w->hostDirty = true;
+    w->deviceAhead = false;
+}

@@ -1,0 +1,221 @@
+// One world's memory image: a single slab holding every persistent SoA
+// array the step reads or writes, followed (on the device only) by the
+// step's scratch arrays.  The host keeps a byte-identical copy of the
+// persistent part, so moving a world between host and HBM is one copy
+// each way and a batch of thousands of worlds is thousands of slabs
+// addressed through one descriptor table.
+//
+// Field lists are X-macros so the offsets, the host view and the
+// device view are generated from a single declaration.  Every array is
+// sized by the world's capacity (bodies, shapes, joints, pairs) like
+// the reference's persistent arrays (src/world.c:160-440), and aligned
+// to 256 bytes so warp accesses start on a sector boundary.
+#ifndef M3_LAYOUT_H
+#define M3_LAYOUT_H
+
+#include "maul3d_b200.h"
+#include "m3_core.h"
+
+// World-global scalars (the m3World header fields the step touches).
+typedef struct m3WorldScalars
+{
+    m3Vec3 gravity;
+    float contactHertz;
+    float contactDampingRatio;
+    float contactPushMaxSpeed;
+    float restitutionThreshold;
+    float maximumLinearSpeed;
+    float maximumAngularSpeed;
+    float hitEventThreshold;
+    uint8_t sleepEnabled;
+    uint8_t continuousEnabled;
+    uint8_t pad0[2];
+    m3Vec3 windDir;
+    float windSpeed;
+    float windGustHertz;
+    float windGustScale;
+    float windPhase;
+    float lastInvH;
+    uint64_t stepCount;
+    int32_t bodyCap;
+    int32_t shapeCap;
+    int32_t jointCap;
+    int32_t pairCap;
+    int32_t bodyMax;
+    int32_t shapeMax;
+    int32_t jointMax;
+    int32_t hullMax;
+    int32_t pairCount;
+    int32_t pairBuf;    // which of the two pair buffers is current
+    int32_t status;     // M3GPU_* code of the last device step (0 = ok)
+    int32_t statusDetail;
+    int32_t lastColorCount;
+    int32_t lastIslandCount;
+    int32_t constraintCount;
+    int32_t moverCount;
+    int32_t jointConstraintCount;
+    int32_t pad1;
+} m3WorldScalars;
+
+// Per-body persistent arrays (capacity = bodyCap).
+#define M3_BODY_FIELDS(X)                                                                          \
+    X(m3Transform, xf)                                                                             \
+    X(m3Vec3, v)                                                                                   \
+    X(m3Vec3, w)                                                                                   \
+    X(float, invMass)                                                                              \
+    X(m3Mat3, invI)                                                                                \
+    X(m3Mat3, inertia)                                                                             \
+    X(m3Vec3, lc)                                                                                  \
+    X(float, gravityScale)                                                                         \
+    X(float, linDamp)                                                                              \
+    X(float, angDamp)                                                                              \
+    X(uint8_t, btype)                                                                              \
+    X(uint8_t, awake)                                                                              \
+    X(float, sleepTime)                                                                            \
+    X(uint8_t, bullet)                                                                             \
+    X(float, minExt)                                                                               \
+    X(float, maxExt)                                                                               \
+    X(m3Vec3, force)                                                                               \
+    X(m3Vec3, torque)                                                                              \
+    X(uint8_t, enabled)                                                                            \
+    X(uint8_t, locks)                                                                              \
+    X(float, sleepThreshold)                                                                       \
+    X(uint8_t, canSleep)                                                                           \
+    X(uint8_t, hasTarget)                                                                          \
+    X(m3Transform, target)                                                                         \
+    X(int32_t, shapeHead)                                                                          \
+    X(int32_t, jointHead)                                                                          \
+    X(uint8_t, bodyAlive)                                                                          \
+    X(uint16_t, bodyGen)                                                                           \
+    X(uint64_t, userData)
+
+// Per-shape persistent arrays (capacity = shapeCap).
+#define M3_SHAPE_FIELDS(X)                                                                         \
+    X(int32_t, shapeBody)                                                                          \
+    X(uint8_t, shapeType)                                                                          \
+    X(m3ShapeGeom, geom)                                                                           \
+    X(float, density)                                                                              \
+    X(float, friction)                                                                             \
+    X(float, restitution)                                                                          \
+    X(float, rolling)                                                                              \
+    X(uint8_t, sensor)                                                                             \
+    X(uint8_t, hitEvents)                                                                          \
+    X(uint8_t, preSolve)                                                                           \
+    X(m3Vec3, surfVel)                                                                             \
+    X(m3Vec3, localPos)                                                                            \
+    X(m3Quat, localRot)                                                                            \
+    X(uint8_t, hasOffset)                                                                          \
+    X(uint64_t, category)                                                                          \
+    X(uint64_t, mask)                                                                              \
+    X(int32_t, group)                                                                              \
+    X(int32_t, shapeNext)                                                                          \
+    X(int32_t, hullIndex)                                                                          \
+    X(uint8_t, shapeAlive)                                                                         \
+    X(uint16_t, shapeGen)                                                                          \
+    X(uint64_t, shapeUserData)
+
+// Per-joint persistent arrays (capacity = jointCap).
+#define M3_JOINT_FIELDS(X)                                                                         \
+    X(uint8_t, jtype)                                                                              \
+    X(int32_t, jbodyA)                                                                             \
+    X(int32_t, jbodyB)                                                                             \
+    X(m3Vec3, jlocalA)                                                                             \
+    X(m3Vec3, jlocalB)                                                                             \
+    X(uint8_t, jcollide)                                                                           \
+    X(m3Vec3, jimpulse)                                                                            \
+    X(m3Vec3, jperp)                                                                               \
+    X(m3Vec3, jlimitImp)                                                                           \
+    X(m3Vec3, jangular)                                                                            \
+    X(m3Quat, jframeA)                                                                             \
+    X(m3Quat, jframeB)                                                                             \
+    X(uint8_t, jflags)                                                                             \
+    X(m3Vec3, jmotor)                                                                              \
+    X(m3Vec3, jbreak)                                                                              \
+    X(m3Vec3, jspring)                                                                             \
+    X(float, jtargetScalar)                                                                        \
+    X(m3Quat, jtargetQ)                                                                            \
+    X(m3Vec3, jspringImp)                                                                          \
+    X(m3Vec3, jlimits)                                                                             \
+    X(int32_t, jnextA)                                                                             \
+    X(int32_t, jnextB)                                                                             \
+    X(uint8_t, jointAlive)                                                                         \
+    X(uint16_t, jointGen)
+
+// Candidate pairs and manifolds, double-buffered: the step reads the
+// previous step's lists for the warm-start carry while it writes the
+// new ones (capacity = pairCap each).
+#define M3_PAIR_FIELDS(X)                                                                          \
+    X(uint64_t, keys0)                                                                             \
+    X(uint64_t, keys1)                                                                             \
+    X(m3Manifold, man0)                                                                            \
+    X(m3Manifold, man1)
+
+// Pointers into one slab (host or device address space).
+typedef struct m3WorldView
+{
+    m3WorldScalars* sc;
+#define M3_X_PTR(T, name) T* name;
+    M3_BODY_FIELDS(M3_X_PTR)
+    M3_SHAPE_FIELDS(M3_X_PTR)
+    M3_JOINT_FIELDS(M3_X_PTR)
+    M3_PAIR_FIELDS(M3_X_PTR)
+#undef M3_X_PTR
+    // Interned hull slabs (count-derived pool, outside the slab).
+    m3HullData* hulls;
+    // Device-only scratch (null in host views), laid out by the step
+    // module which owns its record types.
+    uint8_t* scratch;
+    int64_t scratchBytes;
+} m3WorldView;
+
+#define M3_SLAB_ALIGN 256
+
+M3_HD int64_t m3AlignUp(int64_t x, int64_t a)
+{
+    return (x + a - 1) / a * a;
+}
+
+// Assign offsets for the persistent part; returns its byte size.
+// `base` may be null to only measure.
+static inline int64_t m3LayoutPersistent(m3WorldView* view, uint8_t* base, int32_t bodyCap,
+                                         int32_t shapeCap, int32_t jointCap, int32_t pairCap)
+{
+    int64_t off = 0;
+    if (view)
+    {
+        view->sc = (m3WorldScalars*)(base ? base + off : 0);
+    }
+    off = m3AlignUp(off + (int64_t)sizeof(m3WorldScalars), M3_SLAB_ALIGN);
+#define M3_X_OFF(T, name, n)                                                                       \
+    if (view)                                                                                      \
+    {                                                                                              \
+        view->name = (T*)(base ? base + off : 0);                                                  \
+    }                                                                                              \
+    off = m3AlignUp(off + (int64_t)sizeof(T) * (int64_t)(n), M3_SLAB_ALIGN);
+#define M3_X_BODY(T, name) M3_X_OFF(T, name, bodyCap)
+#define M3_X_SHAPE(T, name) M3_X_OFF(T, name, shapeCap)
+#define M3_X_JOINT(T, name) M3_X_OFF(T, name, jointCap)
+#define M3_X_PAIR(T, name) M3_X_OFF(T, name, pairCap)
+    M3_BODY_FIELDS(M3_X_BODY)
+    M3_SHAPE_FIELDS(M3_X_SHAPE)
+    M3_JOINT_FIELDS(M3_X_JOINT)
+    M3_PAIR_FIELDS(M3_X_PAIR)
+#undef M3_X_BODY
+#undef M3_X_SHAPE
+#undef M3_X_JOINT
+#undef M3_X_PAIR
+#undef M3_X_OFF
+    return off;
+}
+
+// Bytes of device scratch one world needs (implemented by the step
+// module, which owns the scratch record layouts).
+#ifdef __cplusplus
+extern "C" {
+#endif
+int64_t m3gpuScratchBytes(int32_t bodyCap, int32_t shapeCap, int32_t jointCap, int32_t pairCap);
+#ifdef __cplusplus
+}
+#endif
+
+#endif // M3_LAYOUT_H

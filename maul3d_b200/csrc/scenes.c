@@ -1,0 +1,274 @@
+// Seeded synthetic scenes: the workload generator for tests and the
+// benchmark.  Written against the reference-named public API only, so
+// the very same source builds a world in this library and, compiled
+// against the reference's headers (oracle/Makefile), in the reference
+// engine.  Both worlds then hold identical bytes from identical seeds.
+//
+// Randomness is SplitMix64 (Steele, Lea, Flood 2014), the generator
+// the reference bench uses for its scenes (bench/bench_main.c:44-57),
+// mapped to [lo, hi) through the top 53 bits.
+//
+// Scenes:
+//   M3S_SPHERE_PYRAMID  the reference bench "pyramid" layout
+//                       (bench/bench_main.c:68-96); its hash after 300
+//                       steps of dt 1/60, 4 substeps is pinned in
+//                       bench/pins.txt:1 (975f319f2f44cc5d).
+//   M3S_BOX_PYRAMID     a 2D wall pyramid of unit boxes on a plane,
+//                       `param` rows (20 rows = 210 boxes).
+//   M3S_UNEVEN          one world of the batched workload: `param`
+//                       dynamic bodies of 8-high box stacks, loose
+//                       spheres and three revolute chains of 8 capsules
+//                       hung from static anchors, laid out from `seed`.
+//   M3S_FREEFALL        `param` spheres and boxes in free fall, no
+//                       contacts for the first steps (integration only).
+
+#include <m3_scene_api.h> // resolved by -I: product or oracle shim
+
+#include <math.h>
+#include <stdint.h>
+
+enum
+{
+    M3S_SPHERE_PYRAMID = 0,
+    M3S_BOX_PYRAMID = 1,
+    M3S_UNEVEN = 2,
+    M3S_FREEFALL = 3,
+};
+
+static uint64_t SceneSplitMix(uint64_t* state)
+{
+    *state += 0x9E3779B97F4A7C15ull;
+    uint64_t z = *state;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+static double SceneRand(uint64_t* state, double lo, double hi)
+{
+    double unit = (double)(SceneSplitMix(state) >> 11) * (1.0 / 9007199254740992.0);
+    return lo + (hi - lo) * unit;
+}
+
+static m3BodyId SceneGround(m3WorldId world, float friction)
+{
+    m3BodyDef gd = m3DefaultBodyDef();
+    m3BodyId ground = m3CreateBody(world, &gd);
+    m3ShapeDef sd = m3DefaultShapeDef();
+    sd.friction = friction;
+    m3Plane floor = {{0.0f, 1.0f, 0.0f}, 0.0f};
+    m3CreatePlaneShape(ground, &sd, &floor);
+    return ground;
+}
+
+static m3WorldId SphereLayers(void)
+{
+    m3WorldDef def = m3DefaultWorldDef();
+    def.bodyCapacity = 256;
+    def.shapeCapacity = 256;
+    m3WorldId world = m3CreateWorld(&def);
+    SceneGround(world, 0.6f);
+    m3BodyDef bd = m3DefaultBodyDef();
+    bd.type = m3_dynamicBody;
+    m3ShapeDef sd = m3DefaultShapeDef();
+    sd.friction = 0.6f;
+    for (int32_t layer = 0; layer < 6; ++layer)
+    {
+        int32_t n = 6 - layer;
+        for (int32_t i = 0; i < n; ++i)
+        {
+            for (int32_t j = 0; j < n; ++j)
+            {
+                bd.position = (m3Pos3){(double)i - 0.5 * (double)n + 0.05 * (double)layer,
+                                       0.5 + 1.02 * (double)layer, (double)j - 0.5 * (double)n};
+                m3BodyId body = m3CreateBody(world, &bd);
+                m3Sphere ball = {{0.0f, 0.0f, 0.0f}, 0.5f};
+                m3CreateSphereShape(body, &sd, &ball);
+            }
+        }
+    }
+    return world;
+}
+
+static m3WorldId BoxWall(int32_t rows)
+{
+    m3WorldDef def = m3DefaultWorldDef();
+    m3WorldId world = m3CreateWorld(&def);
+    SceneGround(world, 0.6f);
+    m3BodyDef bd = m3DefaultBodyDef();
+    bd.type = m3_dynamicBody;
+    m3ShapeDef sd = m3DefaultShapeDef();
+    sd.friction = 0.6f;
+    sd.density = 1.0f;
+    for (int32_t r = 0; r < rows; ++r)
+    {
+        int32_t n = rows - r;
+        for (int32_t i = 0; i < n; ++i)
+        {
+            bd.position =
+                (m3Pos3){(double)i - 0.5 * (double)n + 0.5, 0.5 + (double)r, 0.0};
+            m3BodyId body = m3CreateBody(world, &bd);
+            m3CreateBoxShape(body, &sd, (m3Vec3){0.5f, 0.5f, 0.5f});
+        }
+    }
+    return world;
+}
+
+static m3WorldId UnevenWorld(uint64_t seed, int32_t bodies)
+{
+    if (bodies < 32)
+    {
+        bodies = 32;
+    }
+    const int32_t chainCount = 3;
+    const int32_t chainLinks = 8;
+    int32_t rest = bodies - chainCount * chainLinks;
+    int32_t stacks = (rest * 2 / 3) / 8;
+    int32_t spheres = rest - 8 * stacks;
+
+    m3WorldDef def = m3DefaultWorldDef();
+    def.bodyCapacity = bodies + 8;
+    def.shapeCapacity = bodies + 8;
+    def.jointCapacity = chainCount * chainLinks + 8;
+    m3WorldId world = m3CreateWorld(&def);
+    SceneGround(world, 0.6f);
+
+    uint64_t rng = seed;
+    m3ShapeDef sd = m3DefaultShapeDef();
+    sd.friction = 0.6f;
+    m3BodyDef bd = m3DefaultBodyDef();
+    bd.type = m3_dynamicBody;
+
+    // Box stacks on a square grid of 2.5 m cells, one half extent per
+    // stack drawn from U[0.25, 0.75], boxes resting face to face.
+    int32_t side = 1;
+    while (side * side < stacks + spheres / 4 + 4)
+    {
+        side += 1;
+    }
+    for (int32_t s = 0; s < stacks; ++s)
+    {
+        double cx = 2.5 * (double)(s % side) - 1.25 * (double)side;
+        double cz = 2.5 * (double)(s / side) - 1.25 * (double)side;
+        float h = (float)SceneRand(&rng, 0.25, 0.75);
+        for (int32_t k = 0; k < 8; ++k)
+        {
+            bd.position = (m3Pos3){cx, (double)h * (double)(2 * k + 1), cz};
+            bd.linearVelocity = (m3Vec3){0.0f, 0.0f, 0.0f};
+            m3BodyId body = m3CreateBody(world, &bd);
+            m3CreateBoxShape(body, &sd, (m3Vec3){h, h, h});
+        }
+    }
+
+    // Loose spheres thrown low across the field: radius U[0.2, 0.5],
+    // a short drop and a horizontal velocity toward the stacks.
+    for (int32_t b = 0; b < spheres; ++b)
+    {
+        float r = (float)SceneRand(&rng, 0.2, 0.5);
+        double x = -1.25 * (double)side + 1.2 * (double)(b / 16);
+        double z = -1.25 * (double)side - 3.0 - 1.2 * (double)(b % 16);
+        bd.position = (m3Pos3){x, (double)r + SceneRand(&rng, 0.0, 0.3), z};
+        bd.linearVelocity = (m3Vec3){(float)SceneRand(&rng, -1.0, 1.0), 0.0f,
+                                     (float)SceneRand(&rng, 1.0, 3.0)};
+        m3BodyId body = m3CreateBody(world, &bd);
+        m3Sphere ball = {{0.0f, 0.0f, 0.0f}, r};
+        m3CreateSphereShape(body, &sd, &ball);
+    }
+    bd.linearVelocity = (m3Vec3){0.0f, 0.0f, 0.0f};
+
+    // Three revolute chains: a shapeless static anchor, 8 capsule
+    // links (radius 0.1, half-height 0.4) laid out horizontally from
+    // it along +x, hinged about z, released to swing down.
+    for (int32_t c = 0; c < chainCount; ++c)
+    {
+        double ax = 1.25 * (double)side + 1.0;
+        double ay = 9.5;
+        double az = -1.25 * (double)side + 2.5 * (double)c;
+        m3BodyDef anchorDef = m3DefaultBodyDef();
+        anchorDef.position = (m3Pos3){ax, ay, az};
+        m3BodyId prev = m3CreateBody(world, &anchorDef);
+        for (int32_t k = 0; k < chainLinks; ++k)
+        {
+            bd.position = (m3Pos3){ax + 0.5 + 1.0 * (double)k, ay, az};
+            m3BodyId link = m3CreateBody(world, &bd);
+            m3Capsule cap = {{-0.4f, 0.0f, 0.0f}, {0.4f, 0.0f, 0.0f}, 0.1f};
+            m3CreateCapsuleShape(link, &sd, &cap);
+            m3JointDef jd = m3DefaultJointDef();
+            jd.type = m3_revoluteJoint;
+            jd.bodyA = prev;
+            jd.bodyB = link;
+            jd.localAnchorA = k == 0 ? (m3Vec3){0.0f, 0.0f, 0.0f} : (m3Vec3){0.5f, 0.0f, 0.0f};
+            jd.localAnchorB = (m3Vec3){-0.5f, 0.0f, 0.0f};
+            jd.localAxisA = (m3Vec3){0.0f, 0.0f, 1.0f};
+            jd.localAxisB = (m3Vec3){0.0f, 0.0f, 1.0f};
+            m3CreateJoint(&jd);
+            prev = link;
+        }
+    }
+    return world;
+}
+
+static m3WorldId FreeFall(int32_t count)
+{
+    m3WorldDef def = m3DefaultWorldDef();
+    def.bodyCapacity = count + 4;
+    def.shapeCapacity = count + 4;
+    m3WorldId world = m3CreateWorld(&def);
+    m3BodyDef bd = m3DefaultBodyDef();
+    bd.type = m3_dynamicBody;
+    m3ShapeDef sd = m3DefaultShapeDef();
+    uint64_t rng = 0xF4EEull;
+    for (int32_t k = 0; k < count; ++k)
+    {
+        bd.position = (m3Pos3){3.0 * (double)k, 50.0 + SceneRand(&rng, 0.0, 5.0), 0.0};
+        bd.linearVelocity = (m3Vec3){(float)SceneRand(&rng, -1.0, 1.0), 0.0f,
+                                     (float)SceneRand(&rng, -1.0, 1.0)};
+        bd.angularVelocity = (m3Vec3){(float)SceneRand(&rng, -2.0, 2.0),
+                                      (float)SceneRand(&rng, -2.0, 2.0),
+                                      (float)SceneRand(&rng, -2.0, 2.0)};
+        m3BodyId body = m3CreateBody(world, &bd);
+        if (k % 2 == 0)
+        {
+            m3Sphere ball = {{0.0f, 0.0f, 0.0f}, 0.4f};
+            m3CreateSphereShape(body, &sd, &ball);
+        }
+        else
+        {
+            m3CreateBoxShape(body, &sd, (m3Vec3){0.3f, 0.45f, 0.6f});
+        }
+    }
+    return world;
+}
+
+// Build one seeded scene; returns the null world id for an unknown
+// scene number.
+M3S_API m3WorldId m3s_build(int32_t scene, uint64_t seed, int32_t param)
+{
+    switch (scene)
+    {
+    case M3S_SPHERE_PYRAMID:
+        return SphereLayers();
+    case M3S_BOX_PYRAMID:
+        return BoxWall(param > 0 ? param : 20);
+    case M3S_UNEVEN:
+        return UnevenWorld(seed, param);
+    case M3S_FREEFALL:
+        return FreeFall(param > 0 ? param : 8);
+    default:
+    {
+        m3WorldId none = {0, 0};
+        return none;
+    }
+    }
+}
+
+// Body count the uneven-world generator produces for world `index` of
+// a batch seeded by `seed`: log-uniform in [lo, hi].
+M3S_API int32_t m3s_uneven_size(uint64_t seed, int32_t index, int32_t lo, int32_t hi)
+{
+    uint64_t s = seed ^ (0xA0761D6478BD642Full * (uint64_t)(index + 1));
+    double u = SceneRand(&s, 0.0, 1.0);
+    double n = exp(log((double)lo) + u * (log((double)hi) - log((double)lo)));
+    int32_t b = (int32_t)n;
+    return b < lo ? lo : (b > hi ? hi : b);
+}

@@ -1,0 +1,1427 @@
+// The device step: m3StepInternal (src/solver.c:3662-4320) for a batch
+// of independent worlds, one thread block per world.
+//
+// Two kernels per step, each a grid of one block per world:
+//   m3CollideKernel  fresh bounds, the canonical pair list, and the
+//                    narrowphase with the warm-start carry;
+//   m3SolveKernel    islands and wake, contact preparation, graph
+//                    colouring, the substep loop (integrate, warm start,
+//                    colour-by-colour solve, integrate positions, relax),
+//                    restitution and store, the continuous pass against
+//                    planes, the sleep pass and the step counter.
+// Block barriers separate every dependent phase, so inside a world the
+// order of every write is the reference's; across worlds nothing is
+// shared.  Worlds are ordered largest first so the long worlds start
+// first (greedy longest-processing-time packing onto the SMs).
+//
+// Refusals: a world that needs something this path does not implement
+// (a pair family, rolling resistance on a static contact, a bullet, a
+// breakable joint, ...) or whose pair list would exceed its capacity is
+// left unstepped with its status word set; the host reports it.
+
+#include "m3_world.h"
+#include "m3_hash.h"
+#include "m3_narrow.cuh"
+#include "m3_solver.cuh"
+#include "m3_joints.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#define M3_BLOCK 256
+
+// ---------------------------------------------------------------------
+// Scratch layout (device only)
+// ---------------------------------------------------------------------
+struct m3Aabb
+{
+    double lo[3];
+    double hi[3];
+};
+
+struct m3Scratch
+{
+    m3Aabb* aabb;          // per shape
+    int32_t* shapeCount;   // per shape, then exclusive offsets
+    m3Pos3* com0;          // per body
+    m3Quat* rot0;          // per body
+    int32_t* parent;       // per body (island union-find)
+    int32_t* forced;       // per body
+    int32_t* forcedRoot;   // per body
+    int32_t* ready;        // per body
+    m3Vec3* deltaPos;      // per body
+    m3Quat* deltaRot;      // per body
+    int32_t* movers;       // per body
+    int32_t* moverFlag;    // per body
+    uint32_t* bodyMask;    // per body
+    m3ContactDev* cons;    // per pair
+    int32_t* pairFlag;     // per pair (compaction)
+    uint8_t* colors;       // per pair
+    int32_t* lists;        // per pair
+    int32_t* starts;       // M3_GRAPH_COLORS + 2
+    m3JointDev* joints;    // per joint
+};
+
+static __host__ __device__ inline int64_t ScratchCarve(m3Scratch* s, uint8_t* base, int32_t bodyCap,
+                                                     int32_t shapeCap, int32_t jointCap,
+                                                     int32_t pairCap)
+{
+    int64_t off = 0;
+#define M3_CARVE(field, T, n)                                                                      \
+    if (s)                                                                                         \
+    {                                                                                              \
+        s->field = (T*)(base + off);                                                               \
+    }                                                                                              \
+    off = m3AlignUp(off + (int64_t)sizeof(T) * (int64_t)(n), M3_SLAB_ALIGN);
+    M3_CARVE(aabb, m3Aabb, shapeCap)
+    M3_CARVE(shapeCount, int32_t, shapeCap + 1)
+    M3_CARVE(com0, m3Pos3, bodyCap)
+    M3_CARVE(rot0, m3Quat, bodyCap)
+    M3_CARVE(parent, int32_t, bodyCap)
+    M3_CARVE(forced, int32_t, bodyCap)
+    M3_CARVE(forcedRoot, int32_t, bodyCap)
+    M3_CARVE(ready, int32_t, bodyCap)
+    M3_CARVE(deltaPos, m3Vec3, bodyCap)
+    M3_CARVE(deltaRot, m3Quat, bodyCap)
+    M3_CARVE(movers, int32_t, bodyCap)
+    M3_CARVE(moverFlag, int32_t, bodyCap + 1)
+    M3_CARVE(bodyMask, uint32_t, bodyCap)
+    M3_CARVE(cons, m3ContactDev, pairCap)
+    M3_CARVE(pairFlag, int32_t, pairCap + 1)
+    M3_CARVE(colors, uint8_t, pairCap)
+    M3_CARVE(lists, int32_t, pairCap)
+    M3_CARVE(starts, int32_t, M3_GRAPH_COLORS + 2)
+    M3_CARVE(joints, m3JointDev, jointCap)
+#undef M3_CARVE
+    return off;
+}
+
+extern "C" int64_t m3gpuScratchBytes(int32_t bodyCap, int32_t shapeCap, int32_t jointCap,
+                                     int32_t pairCap)
+{
+    return ScratchCarve(nullptr, nullptr, bodyCap, shapeCap, jointCap, pairCap);
+}
+
+// ---------------------------------------------------------------------
+// Block utilities
+// ---------------------------------------------------------------------
+
+// Exclusive prefix sum of a[0, n) in place; returns the total.  Each
+// thread scans a contiguous chunk, chunk totals are scanned in shared
+// memory.  Must be called by every thread of the block.
+__device__ int32_t BlockExclusiveScan(int32_t* a, int32_t n)
+{
+    __shared__ int32_t partial[M3_BLOCK];
+    __shared__ int32_t total;
+    const int32_t t = threadIdx.x;
+    const int32_t chunk = (n + M3_BLOCK - 1) / M3_BLOCK;
+    const int32_t lo = t * chunk < n ? t * chunk : n;
+    const int32_t hi = lo + chunk < n ? lo + chunk : n;
+    int32_t sum = 0;
+    for (int32_t i = lo; i < hi; ++i)
+    {
+        sum += a[i];
+    }
+    partial[t] = sum;
+    __syncthreads();
+    if (t == 0)
+    {
+        int32_t run = 0;
+        for (int32_t k = 0; k < M3_BLOCK; ++k)
+        {
+            int32_t x = partial[k];
+            partial[k] = run;
+            run += x;
+        }
+        total = run;
+    }
+    __syncthreads();
+    int32_t run = partial[t];
+    for (int32_t i = lo; i < hi; ++i)
+    {
+        int32_t x = a[i];
+        a[i] = run;
+        run += x;
+    }
+    __syncthreads();
+    return total;
+}
+
+// ---------------------------------------------------------------------
+// Broadphase (broad_phase.c:22-215, :641-681)
+// ---------------------------------------------------------------------
+
+// Fresh bounds of one shape, tight plus the margin (broad_phase.c:22-135).
+__device__ m3Aabb ShapeBounds(const m3WorldView& w, int32_t shape)
+{
+    m3Transform xf = m3ShapeXf(w, shape);
+    m3Aabb box;
+    uint8_t type = w.shapeType[shape];
+    if (type == M3_SHAPE_HULL)
+    {
+        const m3HullData* hull = &w.hulls[w.hullIndex[shape]];
+        for (int32_t k = 0; k < 3; ++k)
+        {
+            box.lo[k] = 1.0e30;
+            box.hi[k] = -1.0e30;
+        }
+        const int32_t nv = hull->vertexCount;
+        for (int32_t v = 0; v < nv; ++v)
+        {
+            m3Vec3 r = m3RotateVec3(xf.q, hull->vertices[v]);
+            double p[3] = {xf.p.x + (double)r.x, xf.p.y + (double)r.y, xf.p.z + (double)r.z};
+            for (int32_t k = 0; k < 3; ++k)
+            {
+                box.lo[k] = p[k] < box.lo[k] ? p[k] : box.lo[k];
+                box.hi[k] = p[k] > box.hi[k] ? p[k] : box.hi[k];
+            }
+        }
+        for (int32_t k = 0; k < 3; ++k)
+        {
+            box.lo[k] -= (double)M3_AABB_MARGIN;
+            box.hi[k] += (double)M3_AABB_MARGIN;
+        }
+        return box;
+    }
+    if (type == M3_SHAPE_CAPSULE)
+    {
+        m3Vec3 r1 = m3RotateVec3(xf.q, w.geom[shape].v);
+        m3Vec3 r2 = m3RotateVec3(xf.q, w.geom[shape].v2);
+        double c1[3] = {xf.p.x + (double)r1.x, xf.p.y + (double)r1.y, xf.p.z + (double)r1.z};
+        double c2[3] = {xf.p.x + (double)r2.x, xf.p.y + (double)r2.y, xf.p.z + (double)r2.z};
+        double fat = (double)(w.geom[shape].s + M3_AABB_MARGIN);
+        for (int32_t k = 0; k < 3; ++k)
+        {
+            box.lo[k] = (c1[k] < c2[k] ? c1[k] : c2[k]) - fat;
+            box.hi[k] = (c1[k] > c2[k] ? c1[k] : c2[k]) + fat;
+        }
+        return box;
+    }
+    m3Vec3 r = m3RotateVec3(xf.q, w.geom[shape].v);
+    double cx = xf.p.x + (double)r.x;
+    double cy = xf.p.y + (double)r.y;
+    double cz = xf.p.z + (double)r.z;
+    double fat = (double)(w.geom[shape].s + M3_AABB_MARGIN);
+    box.lo[0] = cx - fat;
+    box.lo[1] = cy - fat;
+    box.lo[2] = cz - fat;
+    box.hi[0] = cx + fat;
+    box.hi[1] = cy + fat;
+    box.hi[2] = cz + fat;
+    return box;
+}
+
+__device__ __forceinline__ bool Overlap(const m3Aabb& a, const m3Aabb& b)
+{
+    return a.lo[0] <= b.hi[0] && b.lo[0] <= a.hi[0] && a.lo[1] <= b.hi[1] && b.lo[1] <= a.hi[1] &&
+           a.lo[2] <= b.hi[2] && b.lo[2] <= a.hi[2];
+}
+
+// The shared pair filter (broad_phase.c:182-230).
+__device__ bool PairAllowed(const m3WorldView& w, int32_t i, int32_t j)
+{
+    int32_t bodyI = w.shapeBody[i];
+    int32_t bodyJ = w.shapeBody[j];
+    if (bodyI == bodyJ)
+    {
+        return false;
+    }
+    if (w.enabled[bodyI] == 0 || w.enabled[bodyJ] == 0)
+    {
+        return false;
+    }
+    if (w.btype[bodyI] == M3_BODY_STATIC && w.btype[bodyJ] == M3_BODY_STATIC)
+    {
+        return false;
+    }
+    if (w.sensor[i] != 0 && w.sensor[j] != 0)
+    {
+        return false;
+    }
+    int32_t gi = w.group[i];
+    if (gi != 0 && gi == w.group[j])
+    {
+        if (gi < 0)
+        {
+            return false;
+        }
+    }
+    else if (!((w.category[i] & w.mask[j]) != 0 && (w.category[j] & w.mask[i]) != 0))
+    {
+        return false;
+    }
+    for (int32_t jt = w.jointHead[bodyI]; jt != -1;
+         jt = w.jbodyA[jt] == bodyI ? w.jnextA[jt] : w.jnextB[jt])
+    {
+        int32_t other = w.jbodyA[jt] == bodyI ? w.jbodyB[jt] : w.jbodyA[jt];
+        if (other == bodyJ && w.jcollide[jt] == 0)
+        {
+            return false;
+        }
+    }
+    return true;
+}
+
+// The candidate rule of the reference's brute-force referee
+// (broad_phase.c:641-681): every allowed plane/non-plane pair, and every
+// allowed non-plane pair whose fresh bounds overlap.  The tree path
+// (broad_phase.c:430-639) is held equal to it by the reference's own
+// referee test; this evaluates the rule directly, row i emitting its
+// partners j > i in ascending order, so the list comes out sorted.
+__device__ __forceinline__ bool PairCandidate(const m3WorldView& w, const m3Scratch& s, int32_t i,
+                                              int32_t j)
+{
+    if (w.shapeAlive[j] == 0)
+    {
+        return false;
+    }
+    uint8_t ti = w.shapeType[i];
+    uint8_t tj = w.shapeType[j];
+    if (ti == M3_SHAPE_PLANE || tj == M3_SHAPE_PLANE)
+    {
+        if (ti == tj)
+        {
+            return false;
+        }
+    }
+    else if (!Overlap(s.aabb[i], s.aabb[j]))
+    {
+        return false;
+    }
+    return PairAllowed(w, i, j);
+}
+
+// ---------------------------------------------------------------------
+// Kernel 1: bounds, pairs, narrowphase
+// ---------------------------------------------------------------------
+__global__ void __launch_bounds__(M3_BLOCK) m3CollideKernel(const m3WorldView* views,
+                                                            const int32_t* order, int32_t count)
+{
+    const int32_t wi = order[blockIdx.x];
+    const m3WorldView& w = views[wi];
+    m3WorldScalars* sc = w.sc;
+    m3Scratch s;
+    ScratchCarve(&s, w.scratch, sc->bodyCap, sc->shapeCap, sc->jointCap, sc->pairCap);
+    const int32_t tid = threadIdx.x;
+    __shared__ int32_t s_status;
+    if (tid == 0)
+    {
+        s_status = sc->status;
+    }
+    __syncthreads();
+    if (s_status != 0)
+    {
+        return;
+    }
+    const int32_t shapeMax = sc->shapeMax;
+
+    // Fresh bounds once per shape (the reference's per-step cache).
+    for (int32_t i = tid; i < shapeMax; i += M3_BLOCK)
+    {
+        if (w.shapeAlive[i] != 0 && w.shapeType[i] != M3_SHAPE_PLANE)
+        {
+            s.aabb[i] = ShapeBounds(w, i);
+        }
+    }
+    __syncthreads();
+
+    // Count each row's partners.
+    for (int32_t i = tid; i < shapeMax; i += M3_BLOCK)
+    {
+        int32_t n = 0;
+        if (w.shapeAlive[i] != 0)
+        {
+            for (int32_t j = i + 1; j < shapeMax; ++j)
+            {
+                n += PairCandidate(w, s, i, j) ? 1 : 0;
+            }
+        }
+        s.shapeCount[i] = n;
+    }
+    __syncthreads();
+    int32_t total = BlockExclusiveScan(s.shapeCount, shapeMax);
+    if (total > sc->pairCap)
+    {
+        // The reference's m3UpdatePairs refuses with m3_errorCapacity
+        // and the step stalls (broad_phase.c:257-260, solver.c:3722).
+        if (tid == 0)
+        {
+            sc->status = M3GPU_ERR_CAPACITY;
+            sc->statusDetail = total;
+        }
+        return;
+    }
+    const int32_t cur = sc->pairBuf;
+    const uint64_t* oldKeys = cur == 0 ? w.keys0 : w.keys1;
+    const m3Manifold* oldMan = cur == 0 ? w.man0 : w.man1;
+    const int32_t oldCount = sc->pairCount;
+    uint64_t* newKeys = cur == 0 ? w.keys1 : w.keys0;
+    m3Manifold* newMan = cur == 0 ? w.man1 : w.man0;
+
+    // Emit keys in canonical ascending order.
+    for (int32_t i = tid; i < shapeMax; i += M3_BLOCK)
+    {
+        if (w.shapeAlive[i] == 0)
+        {
+            continue;
+        }
+        int32_t o = s.shapeCount[i];
+        for (int32_t j = i + 1; j < shapeMax; ++j)
+        {
+            if (PairCandidate(w, s, i, j))
+            {
+                newKeys[o++] = ((uint64_t)(uint32_t)i << 32) | (uint64_t)(uint32_t)j;
+            }
+        }
+    }
+    __syncthreads();
+
+    // Narrowphase and warm-start carry, one pair per thread.
+    for (int32_t k = tid; k < total; k += M3_BLOCK)
+    {
+        uint64_t key = newKeys[k];
+        m3Manifold fresh;
+        int32_t st = m3CollidePair(w, key, &fresh);
+        if (st != M3_NARROW_OK)
+        {
+            s_status = M3GPU_ERR_UNSUPPORTED;
+            sc->statusDetail = 1000 + (int32_t)w.shapeType[(int32_t)(key >> 32)] * 10 +
+                               (int32_t)w.shapeType[(int32_t)(key & 0xFFFFFFFFu)];
+        }
+        m3WarmCarry(&fresh, key, oldKeys, oldMan, oldCount);
+        newMan[k] = fresh;
+    }
+    __syncthreads();
+    if (tid == 0)
+    {
+        if (s_status != 0)
+        {
+            sc->status = s_status;
+        }
+        else
+        {
+            sc->pairBuf = 1 - cur;
+            sc->pairCount = total;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------
+// Islands (solver.c:3437-3578): a lock-free union-find whose links
+// always point a root at a smaller root, so each component's final
+// root is its smallest body index, the reference's "lower root wins".
+// ---------------------------------------------------------------------
+__device__ __forceinline__ int32_t IslandFind(int32_t* parent, int32_t i)
+{
+    while (true)
+    {
+        int32_t p = parent[i];
+        if (p == i)
+        {
+            return i;
+        }
+        int32_t gp = parent[p];
+        if (gp != p)
+        {
+            parent[i] = gp; // halving: gp is an ancestor of i
+        }
+        i = p;
+    }
+}
+
+__device__ void IslandUnion(int32_t* parent, int32_t a, int32_t b)
+{
+    while (true)
+    {
+        a = IslandFind(parent, a);
+        b = IslandFind(parent, b);
+        if (a == b)
+        {
+            return;
+        }
+        if (a > b)
+        {
+            int32_t t = a;
+            a = b;
+            b = t;
+        }
+        int32_t old = atomicCAS(&parent[b], b, a);
+        if (old == b)
+        {
+            return;
+        }
+        b = old;
+    }
+}
+
+__device__ __forceinline__ void MarkKinematicContact(const m3WorldView& w, const m3Scratch& s,
+                                                     int32_t bodyA, int32_t bodyB)
+{
+    int dynA = w.btype[bodyA] == M3_BODY_DYNAMIC;
+    int dynB = w.btype[bodyB] == M3_BODY_DYNAMIC;
+    if (dynA && dynB)
+    {
+        IslandUnion(s.parent, bodyA, bodyB);
+    }
+    else if (dynA || dynB)
+    {
+        int32_t kin = dynA ? bodyB : bodyA;
+        int32_t dyn = dynA ? bodyA : bodyB;
+        if (w.btype[kin] == M3_BODY_KINEMATIC)
+        {
+            m3Vec3 v = w.v[kin];
+            m3Vec3 om = w.w[kin];
+            if (m3Dot3(v, v) > 0.0f || m3Dot3(om, om) > 0.0f)
+            {
+                s.forced[dyn] = 1;
+            }
+        }
+    }
+}
+
+// Continuous collision against planes for one fast non-bullet body
+// (solver.c:3286-3347, the plane arm of SolveContinuousPhase :3349-3425).
+__device__ m3Transform SweepTransform(const m3Vec3& lc, const m3Vec3& c1, const m3Vec3& c2,
+                                      const m3Quat& q1, m3Quat q2, m3real time)
+{
+    m3Transform xf;
+    if (q1.x * q2.x + q1.y * q2.y + q1.z * q2.z + q1.w * q2.w < 0.0f)
+    {
+        q2 = q4(-q2.x, -q2.y, -q2.z, -q2.w);
+    }
+    m3Quat q = q4(q1.x + time * (q2.x - q1.x), q1.y + time * (q2.y - q1.y),
+                  q1.z + time * (q2.z - q1.z), q1.w + time * (q2.w - q1.w));
+    xf.q = m3NormalizeQuat(q);
+    m3Vec3 c = m3Add3(c1, m3MulSV3(time, m3Sub3(c2, c1)));
+    m3Vec3 r = m3RotateVec3(xf.q, lc);
+    xf.p.x = (double)(c.x - r.x);
+    xf.p.y = (double)(c.y - r.y);
+    xf.p.z = (double)(c.z - r.z);
+    return xf;
+}
+
+// Support points of the fast shape's distance proxy (manifold.c:463-499).
+__device__ __forceinline__ int32_t ProxyPoints(const m3WorldView& w, int32_t shape,
+                                               const m3Vec3** pts, m3Vec3 scratch[2],
+                                               m3real* radius)
+{
+    uint8_t type = w.shapeType[shape];
+    if (type == M3_SHAPE_HULL)
+    {
+        const m3HullData* hull = &w.hulls[w.hullIndex[shape]];
+        *pts = hull->vertices;
+        *radius = 0.0f;
+        return hull->vertexCount;
+    }
+    if (type == M3_SHAPE_CAPSULE)
+    {
+        scratch[0] = w.geom[shape].v;
+        scratch[1] = w.geom[shape].v2;
+        *pts = scratch;
+        *radius = w.geom[shape].s;
+        return 2;
+    }
+    scratch[0] = w.geom[shape].v;
+    *pts = scratch;
+    *radius = w.geom[shape].s;
+    return 1;
+}
+
+__device__ void ContinuousVersusPlane(const m3WorldView& w, int32_t body, int32_t fastShape,
+                                      int32_t planeShape, const m3Pos3& base, const m3Vec3& lc,
+                                      const m3Vec3& c1, const m3Vec3& c2, const m3Quat& q1,
+                                      const m3Quat& q2, m3real* fraction)
+{
+    m3Vec3 n = w.geom[planeShape].v;
+    m3real offset = w.geom[planeShape].s -
+                    (m3real)((double)n.x * base.x + (double)n.y * base.y + (double)n.z * base.z);
+    m3Vec3 scratch[2];
+    const m3Vec3* pts;
+    m3real radius;
+    int32_t count = ProxyPoints(w, fastShape, &pts, scratch, &radius);
+    const m3real linearSlop = M3_LINEAR_SLOP;
+    m3real target = m3MaxF(linearSlop, radius - linearSlop);
+    m3real tolerance = 0.25f * linearSlop;
+    m3Vec3 travel = m3Sub3(c2, c1);
+    m3Quat dq = m3MulQuat(q2, q4(-q1.x, -q1.y, -q1.z, q1.w));
+    m3real arc = 2.0f * sqrtf(dq.x * dq.x + dq.y * dq.y + dq.z * dq.z) * w.maxExt[body];
+    m3real rate = sqrtf(m3Dot3(travel, travel)) + arc;
+    if (!(rate > 0.0f))
+    {
+        return;
+    }
+    m3real t = 0.0f;
+    for (int32_t iter = 0; iter < 25; ++iter)
+    {
+        m3Transform xf = SweepTransform(lc, c1, c2, q1, q2, t);
+        m3real minD = 3.4e38f;
+        for (int32_t k = 0; k < count; ++k)
+        {
+            m3Vec3 r = m3RotateVec3(xf.q, pts[k]);
+            m3real d = n.x * ((m3real)xf.p.x + r.x) + n.y * ((m3real)xf.p.y + r.y) +
+                       n.z * ((m3real)xf.p.z + r.z);
+            minD = m3MinF(minD, d);
+        }
+        m3real sep = minD - offset;
+        if (sep <= 0.0f)
+        {
+            return;
+        }
+        if (sep <= target + tolerance)
+        {
+            if (t > 0.0f && t < *fraction)
+            {
+                *fraction = t;
+            }
+            return;
+        }
+        t += (sep - target) / rate;
+        if (t >= *fraction)
+        {
+            return;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------
+// Kernel 2: islands, prepare, colour, substeps, store, continuous, sleep
+// ---------------------------------------------------------------------
+__global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* views,
+                                                          const int32_t* order, int32_t count,
+                                                          float dt, int32_t substeps)
+{
+    const int32_t wi = order[blockIdx.x];
+    const m3WorldView& w = views[wi];
+    m3WorldScalars* sc = w.sc;
+    m3Scratch s;
+    ScratchCarve(&s, w.scratch, sc->bodyCap, sc->shapeCap, sc->jointCap, sc->pairCap);
+    const int32_t tid = threadIdx.x;
+    __shared__ int32_t s_status;
+    __shared__ int32_t s_anyRestitution;
+    __shared__ int32_t s_starts[M3_GRAPH_COLORS + 2];
+    if (tid == 0)
+    {
+        s_status = sc->status;
+        s_anyRestitution = 0;
+    }
+    __syncthreads();
+    if (s_status != 0)
+    {
+        return;
+    }
+    const int32_t bodyMax = sc->bodyMax;
+    const int32_t shapeMax = sc->shapeMax;
+    const int32_t jointMax = sc->jointMax;
+    const int32_t pairCount = sc->pairCount;
+    const uint64_t* keys = sc->pairBuf == 0 ? w.keys0 : w.keys1;
+    m3Manifold* man = sc->pairBuf == 0 ? w.man0 : w.man1;
+
+    // Begin-of-step centres and rotations (solver.c:3866-3877); island
+    // arrays reset.
+    for (int32_t i = tid; i < bodyMax; i += M3_BLOCK)
+    {
+        s.parent[i] = i;
+        s.forced[i] = 0;
+        s.forcedRoot[i] = 0;
+        if (w.bodyAlive[i] == 0)
+        {
+            continue;
+        }
+        const m3Transform xf = w.xf[i];
+        m3Vec3 rlc = m3RotateVec3(xf.q, w.lc[i]);
+        m3Pos3 c;
+        c.x = xf.p.x + (double)rlc.x;
+        c.y = xf.p.y + (double)rlc.y;
+        c.z = xf.p.z + (double)rlc.z;
+        s.com0[i] = c;
+        s.rot0[i] = xf.q;
+    }
+    __syncthreads();
+
+    // Island wake pass (solver.c:3468-3578).
+    for (int32_t k = tid; k < pairCount; k += M3_BLOCK)
+    {
+        if (man[k].pointCount == 0)
+        {
+            continue;
+        }
+        uint64_t key = keys[k];
+        int32_t shapeA = (int32_t)(key >> 32);
+        int32_t shapeB = (int32_t)(key & 0xFFFFFFFFu);
+        if (w.sensor[shapeA] != 0 || w.sensor[shapeB] != 0)
+        {
+            continue;
+        }
+        MarkKinematicContact(w, s, w.shapeBody[shapeA], w.shapeBody[shapeB]);
+    }
+    for (int32_t j = tid; j < jointMax; j += M3_BLOCK)
+    {
+        if (w.jointAlive[j] != 0)
+        {
+            MarkKinematicContact(w, s, w.jbodyA[j], w.jbodyB[j]);
+        }
+    }
+    __syncthreads();
+    for (int32_t i = tid; i < bodyMax; i += M3_BLOCK)
+    {
+        if (w.bodyAlive[i] == 0 || w.btype[i] != M3_BODY_DYNAMIC)
+        {
+            continue;
+        }
+        if (w.awake[i] != 0 || s.forced[i] != 0)
+        {
+            s.forcedRoot[IslandFind(s.parent, i)] = 1;
+        }
+    }
+    __syncthreads();
+    for (int32_t i = tid; i < bodyMax; i += M3_BLOCK)
+    {
+        if (w.bodyAlive[i] == 0 || w.btype[i] != M3_BODY_DYNAMIC)
+        {
+            continue;
+        }
+        if (w.awake[i] == 0 && s.forcedRoot[IslandFind(s.parent, i)] != 0)
+        {
+            w.awake[i] = 1;
+            w.sleepTime[i] = 0.0f;
+        }
+    }
+    for (int32_t i = tid; i < bodyMax; i += M3_BLOCK)
+    {
+        s.deltaPos[i] = v3(0.0f, 0.0f, 0.0f);
+        s.deltaRot[i] = m3IdentityQuat();
+    }
+    __syncthreads();
+
+    // Contact selection and preparation (solver.c:156-405).
+    const m3real h = dt / (m3real)substeps;
+    const m3real invH = h > 0.0f ? 1.0f / h : 0.0f;
+    const m3SoftDev soft = m3MakeSoft(sc->contactHertz, sc->contactDampingRatio, h);
+    const m3SoftDev staticSoft = m3MakeSoft(2.0f * sc->contactHertz, sc->contactDampingRatio, h);
+    for (int32_t k = tid; k < pairCount; k += M3_BLOCK)
+    {
+        int32_t flag = 0;
+        if (man[k].pointCount != 0)
+        {
+            uint64_t key = keys[k];
+            int32_t shapeA = (int32_t)(key >> 32);
+            int32_t shapeB = (int32_t)(key & 0xFFFFFFFFu);
+            int32_t bodyA = w.shapeBody[shapeA];
+            int32_t bodyB = w.shapeBody[shapeB];
+            int awakeDynA = w.btype[bodyA] == M3_BODY_DYNAMIC && w.awake[bodyA] != 0;
+            int awakeDynB = w.btype[bodyB] == M3_BODY_DYNAMIC && w.awake[bodyB] != 0;
+            if ((awakeDynA || awakeDynB) && w.sensor[shapeA] == 0 && w.sensor[shapeB] == 0)
+            {
+                flag = 1;
+            }
+        }
+        s.pairFlag[k] = flag;
+    }
+    __syncthreads();
+    const int32_t constraintCount = BlockExclusiveScan(s.pairFlag, pairCount);
+    for (int32_t k = tid; k < pairCount; k += M3_BLOCK)
+    {
+        int32_t next = k + 1 < pairCount ? s.pairFlag[k + 1] : constraintCount;
+        if (next == s.pairFlag[k])
+        {
+            continue; // not selected
+        }
+        m3ContactDev* c = &s.cons[s.pairFlag[k]];
+        m3PrepareContact(w, c, k, keys, man, soft, staticSoft);
+        if (c->restitution != 0.0f)
+        {
+            s_anyRestitution = 1;
+        }
+        if (c->rollingResistance > 0.0f && (!c->dynA || !c->dynB))
+        {
+            s_status = M3GPU_ERR_UNSUPPORTED;
+            sc->statusDetail = 2001;
+        }
+    }
+    // Joints prepare in slot order (solver.c:699-1042).
+    if (tid == 0)
+    {
+        sc->jointConstraintCount = m3PrepareJoints(w, s.joints, h, &s_status, &sc->statusDetail);
+    }
+    __syncthreads();
+    if (s_status != 0)
+    {
+        if (tid == 0)
+        {
+            sc->status = s_status;
+        }
+        return;
+    }
+
+    // Greedy 16-colour first-free-bit colouring in constraint order, the
+    // overflow bucket last (solver.c:2750-2810).
+    if (tid == 0)
+    {
+        for (int32_t i = 0; i < bodyMax; ++i)
+        {
+            s.bodyMask[i] = 0u;
+        }
+        int32_t counts[M3_GRAPH_COLORS + 1];
+        for (int32_t c = 0; c <= M3_GRAPH_COLORS; ++c)
+        {
+            counts[c] = 0;
+        }
+        for (int32_t i = 0; i < constraintCount; ++i)
+        {
+            const m3ContactDev* c = &s.cons[i];
+            int dynA = c->dynA && w.awake[c->bodyA];
+            int dynB = c->dynB && w.awake[c->bodyB];
+            uint32_t mask = (dynA ? s.bodyMask[c->bodyA] : 0u) | (dynB ? s.bodyMask[c->bodyB] : 0u);
+            int32_t color = M3_GRAPH_COLORS;
+            for (int32_t bit = 0; bit < M3_GRAPH_COLORS; ++bit)
+            {
+                if ((mask & (1u << bit)) == 0u)
+                {
+                    color = bit;
+                    break;
+                }
+            }
+            s.colors[i] = (uint8_t)color;
+            if (color < M3_GRAPH_COLORS)
+            {
+                if (dynA)
+                {
+                    s.bodyMask[c->bodyA] |= 1u << color;
+                }
+                if (dynB)
+                {
+                    s.bodyMask[c->bodyB] |= 1u << color;
+                }
+            }
+            counts[color] += 1;
+        }
+        int32_t cursor = 0;
+        int32_t used = 0;
+        for (int32_t c = 0; c <= M3_GRAPH_COLORS; ++c)
+        {
+            s_starts[c] = cursor;
+            cursor += counts[c];
+            used += counts[c] > 0 ? 1 : 0;
+        }
+        s_starts[M3_GRAPH_COLORS + 1] = cursor;
+        int32_t fill[M3_GRAPH_COLORS + 1];
+        for (int32_t c = 0; c <= M3_GRAPH_COLORS; ++c)
+        {
+            fill[c] = s_starts[c];
+        }
+        for (int32_t i = 0; i < constraintCount; ++i)
+        {
+            s.lists[fill[s.colors[i]]++] = i;
+        }
+        sc->lastColorCount = used;
+        sc->constraintCount = constraintCount;
+    }
+
+    // Movers: alive, enabled, kinematic or awake dynamic, ascending
+    // (solver.c:3945-3983), with the kinematic servo.
+    for (int32_t i = tid; i < bodyMax; i += M3_BLOCK)
+    {
+        int32_t flag = 0;
+        if (w.bodyAlive[i] != 0 && w.enabled[i] != 0)
+        {
+            uint8_t type = w.btype[i];
+            if (type == M3_BODY_KINEMATIC || (type == M3_BODY_DYNAMIC && w.awake[i] != 0))
+            {
+                flag = 1;
+            }
+            if (type == M3_BODY_KINEMATIC && w.hasTarget[i] != 0)
+            {
+                m3real servoInvDt = 1.0f / dt;
+                const m3Transform now = w.xf[i];
+                const m3Transform want = w.target[i];
+                w.v[i] = v3((m3real)(want.p.x - now.p.x) * servoInvDt,
+                            (m3real)(want.p.y - now.p.y) * servoInvDt,
+                            (m3real)(want.p.z - now.p.z) * servoInvDt);
+                m3Quat dq = m3MulQuat(want.q, q4(-now.q.x, -now.q.y, -now.q.z, now.q.w));
+                if (dq.w < 0.0f)
+                {
+                    dq = q4(-dq.x, -dq.y, -dq.z, -dq.w);
+                }
+                w.w[i] = m3MulSV3(2.0f * servoInvDt, v3(dq.x, dq.y, dq.z));
+                w.hasTarget[i] = 0;
+            }
+        }
+        s.moverFlag[i] = flag;
+    }
+    __syncthreads();
+    const int32_t moverCount = BlockExclusiveScan(s.moverFlag, bodyMax);
+    for (int32_t i = tid; i < bodyMax; i += M3_BLOCK)
+    {
+        int32_t next = i + 1 < bodyMax ? s.moverFlag[i + 1] : moverCount;
+        if (next != s.moverFlag[i])
+        {
+            s.movers[s.moverFlag[i]] = i;
+        }
+    }
+    __syncthreads();
+    const int32_t jointCount = sc->jointConstraintCount;
+    const m3real pushMax = sc->contactPushMaxSpeed;
+
+    // The substep loop (solver.c:4085-4203).
+    for (int32_t sub = 0; sub < substeps; ++sub)
+    {
+        for (int32_t m = tid; m < moverCount; m += M3_BLOCK)
+        {
+            int32_t i = s.movers[m];
+            if (w.btype[i] == M3_BODY_DYNAMIC)
+            {
+                m3IntegrateVelocity(w, i, h);
+            }
+        }
+        __syncthreads();
+        if (tid == 0 && jointCount > 0)
+        {
+            m3WarmStartJoints(w, s.joints, jointCount, s.deltaRot);
+        }
+        __syncthreads();
+        // Warm start, colour by colour; the overflow bucket serially.
+        for (int32_t color = 0; color < M3_GRAPH_COLORS; ++color)
+        {
+            int32_t a = s_starts[color];
+            int32_t b = s_starts[color + 1];
+            if (a == b)
+            {
+                continue;
+            }
+            for (int32_t k = a + tid; k < b; k += M3_BLOCK)
+            {
+                m3WarmStartContact(w, &s.cons[s.lists[k]]);
+            }
+            __syncthreads();
+        }
+        if (tid == 0)
+        {
+            for (int32_t k = s_starts[M3_GRAPH_COLORS]; k < s_starts[M3_GRAPH_COLORS + 1]; ++k)
+            {
+                m3WarmStartContact(w, &s.cons[s.lists[k]]);
+            }
+            if (jointCount > 0)
+            {
+                m3SolveJoints(w, s.joints, jointCount, s.deltaPos, s.deltaRot, h, invH, true);
+            }
+        }
+        __syncthreads();
+        for (int32_t color = 0; color < M3_GRAPH_COLORS; ++color)
+        {
+            int32_t a = s_starts[color];
+            int32_t b = s_starts[color + 1];
+            if (a == b)
+            {
+                continue;
+            }
+            for (int32_t k = a + tid; k < b; k += M3_BLOCK)
+            {
+                m3SolveContact(w, &s.cons[s.lists[k]], s.deltaPos, s.deltaRot, invH, pushMax, true);
+            }
+            __syncthreads();
+        }
+        if (tid == 0)
+        {
+            for (int32_t k = s_starts[M3_GRAPH_COLORS]; k < s_starts[M3_GRAPH_COLORS + 1]; ++k)
+            {
+                m3SolveContact(w, &s.cons[s.lists[k]], s.deltaPos, s.deltaRot, invH, pushMax, true);
+            }
+        }
+        __syncthreads();
+        for (int32_t m = tid; m < moverCount; m += M3_BLOCK)
+        {
+            m3IntegratePosition(w, s.movers[m], h, s.deltaPos, s.deltaRot);
+        }
+        __syncthreads();
+        if (tid == 0 && jointCount > 0)
+        {
+            m3SolveJoints(w, s.joints, jointCount, s.deltaPos, s.deltaRot, h, invH, false);
+        }
+        __syncthreads();
+        for (int32_t color = 0; color < M3_GRAPH_COLORS; ++color)
+        {
+            int32_t a = s_starts[color];
+            int32_t b = s_starts[color + 1];
+            if (a == b)
+            {
+                continue;
+            }
+            for (int32_t k = a + tid; k < b; k += M3_BLOCK)
+            {
+                m3SolveContact(w, &s.cons[s.lists[k]], s.deltaPos, s.deltaRot, invH, pushMax,
+                               false);
+            }
+            __syncthreads();
+        }
+        if (tid == 0)
+        {
+            for (int32_t k = s_starts[M3_GRAPH_COLORS]; k < s_starts[M3_GRAPH_COLORS + 1]; ++k)
+            {
+                m3SolveContact(w, &s.cons[s.lists[k]], s.deltaPos, s.deltaRot, invH, pushMax,
+                               false);
+            }
+        }
+        __syncthreads();
+    }
+
+    // Forces live one step (solver.c:4207-4211).
+    for (int32_t m = tid; m < moverCount; m += M3_BLOCK)
+    {
+        int32_t i = s.movers[m];
+        w.force[i] = v3(0.0f, 0.0f, 0.0f);
+        w.torque[i] = v3(0.0f, 0.0f, 0.0f);
+    }
+    // Restitution is serial in constraint order (solver.c:2879-2906).
+    if (tid == 0 && s_anyRestitution)
+    {
+        const m3real threshold = sc->restitutionThreshold;
+        for (int32_t i = 0; i < constraintCount; ++i)
+        {
+            m3RestituteContact(w, &s.cons[i], threshold);
+        }
+    }
+    __syncthreads();
+    for (int32_t i = tid; i < constraintCount; i += M3_BLOCK)
+    {
+        m3StoreContact(&s.cons[i], man);
+    }
+    if (tid == 0)
+    {
+        m3StoreJointImpulses(w, s.joints, jointCount);
+        sc->lastInvH = invH;
+        // Wind phase (solver.c:4220-4229).
+        if (sc->windGustHertz > 0.0f)
+        {
+            sc->windPhase += 2.0f * M3_PI * sc->windGustHertz * dt;
+            if (sc->windPhase > 2.0f * M3_PI)
+            {
+                sc->windPhase -=
+                    2.0f * M3_PI * (m3real)(int32_t)(sc->windPhase / (2.0f * M3_PI));
+            }
+        }
+    }
+    __syncthreads();
+
+    // Continuous phase (solver.c:3349-3425).  A non-bullet fast body
+    // sweeps only against static targets, and a pull-back moves only the
+    // fast body itself, so bodies are independent and run in parallel.
+    // Planes are swept here; a static non-plane target in range, or a
+    // bullet, is refused.
+    if (sc->continuousEnabled != 0)
+    {
+        for (int32_t i = tid; i < bodyMax; i += M3_BLOCK)
+        {
+            if (w.bodyAlive[i] == 0 || w.btype[i] != M3_BODY_DYNAMIC)
+            {
+                continue;
+            }
+            const m3Transform xfEnd = w.xf[i];
+            m3Vec3 rlc = m3RotateVec3(xfEnd.q, w.lc[i]);
+            double cx = xfEnd.p.x + (double)rlc.x;
+            double cy = xfEnd.p.y + (double)rlc.y;
+            double cz = xfEnd.p.z + (double)rlc.z;
+            const m3Pos3 c0 = s.com0[i];
+            m3Vec3 dc = v3((m3real)(cx - c0.x), (m3real)(cy - c0.y), (m3real)(cz - c0.z));
+            m3Quat q0 = s.rot0[i];
+            m3Quat dq = m3MulQuat(xfEnd.q, q4(-q0.x, -q0.y, -q0.z, q0.w));
+            m3real arc = 2.0f * sqrtf(dq.x * dq.x + dq.y * dq.y + dq.z * dq.z) * w.maxExt[i];
+            m3real maxMotion = sqrtf(m3Dot3(dc, dc)) + arc;
+            if (!(maxMotion > 0.5f * w.minExt[i]))
+            {
+                continue;
+            }
+            if (w.bullet[i] != 0)
+            {
+                s_status = M3GPU_ERR_UNSUPPORTED;
+                sc->statusDetail = 3001;
+                continue;
+            }
+            // Relative sweep about the begin centre (MakeRelativeSweep).
+            const m3Pos3 base = c0;
+            const m3Vec3 lc = w.lc[i];
+            const m3Vec3 sc1 = v3((m3real)(c0.x - base.x), (m3real)(c0.y - base.y),
+                                  (m3real)(c0.z - base.z));
+            const m3Vec3 sc2 = v3((m3real)(xfEnd.p.x + (double)rlc.x - base.x),
+                                  (m3real)(xfEnd.p.y + (double)rlc.y - base.y),
+                                  (m3real)(xfEnd.p.z + (double)rlc.z - base.z));
+            m3real fraction = 1.0f;
+            double pad = (double)(w.maxExt[i] + M3_AABB_MARGIN);
+            double lo[3] = {(c0.x < cx ? c0.x : cx) - pad, (c0.y < cy ? c0.y : cy) - pad,
+                            (c0.z < cz ? c0.z : cz) - pad};
+            double hi[3] = {(c0.x > cx ? c0.x : cx) + pad, (c0.y > cy ? c0.y : cy) + pad,
+                            (c0.z > cz ? c0.z : cz) + pad};
+            for (int32_t sh = w.shapeHead[i]; sh != -1; sh = w.shapeNext[sh])
+            {
+                if (w.sensor[sh] != 0)
+                {
+                    continue;
+                }
+                // Static non-plane shapes whose fresh bounds touch the
+                // swept box would need the general time of impact.
+                for (int32_t o = 0; o < shapeMax; ++o)
+                {
+                    if (w.shapeAlive[o] == 0 || w.shapeType[o] == M3_SHAPE_PLANE)
+                    {
+                        continue;
+                    }
+                    int32_t ob = w.shapeBody[o];
+                    if (ob == i || w.btype[ob] != M3_BODY_STATIC || w.enabled[ob] == 0)
+                    {
+                        continue;
+                    }
+                    const m3Aabb& ab = s.aabb[o];
+                    if (ab.hi[0] + (double)M3_AABB_MARGIN >= lo[0] &&
+                        ab.lo[0] - (double)M3_AABB_MARGIN <= hi[0] &&
+                        ab.hi[1] + (double)M3_AABB_MARGIN >= lo[1] &&
+                        ab.lo[1] - (double)M3_AABB_MARGIN <= hi[1] &&
+                        ab.hi[2] + (double)M3_AABB_MARGIN >= lo[2] &&
+                        ab.lo[2] - (double)M3_AABB_MARGIN <= hi[2])
+                    {
+                        s_status = M3GPU_ERR_UNSUPPORTED;
+                        sc->statusDetail = 3002;
+                    }
+                }
+                for (int32_t p = 0; p < shapeMax; ++p)
+                {
+                    if (w.shapeAlive[p] != 0 && w.shapeType[p] == M3_SHAPE_PLANE)
+                    {
+                        ContinuousVersusPlane(w, i, sh, p, base, lc, sc1, sc2, q0, xfEnd.q,
+                                              &fraction);
+                    }
+                }
+            }
+            if (fraction < 1.0f)
+            {
+                m3Transform xf = SweepTransform(lc, sc1, sc2, q0, xfEnd.q, fraction);
+                m3Transform out;
+                out.q = xf.q;
+                out.p.x = base.x + xf.p.x;
+                out.p.y = base.y + xf.p.y;
+                out.p.z = base.z + xf.p.z;
+                w.xf[i] = out;
+            }
+        }
+        __syncthreads();
+        if (s_status != 0)
+        {
+            if (tid == 0)
+            {
+                sc->status = s_status;
+            }
+            return;
+        }
+    }
+
+    // Sleep pass (solver.c:3582-3660).
+    if (sc->sleepEnabled != 0)
+    {
+        const m3real invDt = dt > 0.0f ? 1.0f / dt : 0.0f;
+        for (int32_t i = tid; i < bodyMax; i += M3_BLOCK)
+        {
+            s.ready[i] = 1;
+            if (w.bodyAlive[i] == 0 || w.btype[i] != M3_BODY_DYNAMIC || w.awake[i] == 0)
+            {
+                continue;
+            }
+            m3Vec3 v = w.v[i];
+            m3Vec3 om = w.w[i];
+            m3real velocity = sqrtf(m3Dot3(v, v)) + sqrtf(m3Dot3(om, om)) * w.maxExt[i];
+            const m3Transform xf = w.xf[i];
+            m3Vec3 rlc = m3RotateVec3(xf.q, w.lc[i]);
+            const m3Pos3 c0 = s.com0[i];
+            m3Vec3 dc = v3((m3real)(xf.p.x + (double)rlc.x - c0.x),
+                           (m3real)(xf.p.y + (double)rlc.y - c0.y),
+                           (m3real)(xf.p.z + (double)rlc.z - c0.z));
+            m3Quat q0 = s.rot0[i];
+            m3Quat dq = m3MulQuat(xf.q, q4(-q0.x, -q0.y, -q0.z, q0.w));
+            m3real motion = sqrtf(m3Dot3(dc, dc)) +
+                            2.0f * sqrtf(dq.x * dq.x + dq.y * dq.y + dq.z * dq.z) * w.maxExt[i];
+            m3real sleepVelocity = m3MaxF(velocity, 0.5f * invDt * motion);
+            if (w.canSleep[i] == 0)
+            {
+                sleepVelocity = 3.4e38f;
+            }
+            if (sleepVelocity < w.sleepThreshold[i])
+            {
+                w.sleepTime[i] += dt;
+            }
+            else
+            {
+                w.sleepTime[i] = 0.0f;
+            }
+        }
+        __syncthreads();
+        for (int32_t i = tid; i < bodyMax; i += M3_BLOCK)
+        {
+            if (w.bodyAlive[i] == 0 || w.btype[i] != M3_BODY_DYNAMIC || w.awake[i] == 0)
+            {
+                continue;
+            }
+            if (w.sleepTime[i] < M3_TIME_TO_SLEEP)
+            {
+                s.ready[IslandFind(s.parent, i)] = 0;
+            }
+        }
+        __syncthreads();
+        for (int32_t i = tid; i < bodyMax; i += M3_BLOCK)
+        {
+            if (w.bodyAlive[i] == 0 || w.btype[i] != M3_BODY_DYNAMIC || w.awake[i] == 0)
+            {
+                continue;
+            }
+            if (s.ready[IslandFind(s.parent, i)] != 0)
+            {
+                w.awake[i] = 0;
+                w.v[i] = v3(0.0f, 0.0f, 0.0f);
+                w.w[i] = v3(0.0f, 0.0f, 0.0f);
+            }
+        }
+        __syncthreads();
+    }
+    if (tid == 0)
+    {
+        sc->moverCount = moverCount;
+        sc->stepCount += 1;
+    }
+}
+
+// ---------------------------------------------------------------------
+// Hash kernel: one thread per world over its HBM slab.
+// ---------------------------------------------------------------------
+__global__ void m3HashKernel(const m3WorldView* views, int32_t count, uint64_t* out)
+{
+    int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count)
+    {
+        out[i] = m3WorldHashView(&views[i]);
+    }
+}
+
+// ---------------------------------------------------------------------
+// Host launch
+// ---------------------------------------------------------------------
+static int64_t s_launches = 0;
+static float s_lastStepMs = 0.0f;
+
+extern "C" int64_t m3gpu_launch_count(void)
+{
+    return s_launches;
+}
+
+extern "C" float m3gpu_last_step_ms(void)
+{
+    return s_lastStepMs;
+}
+
+extern "C" int32_t m3gpu_synchronize(void)
+{
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess)
+    {
+        return m3gpuSetError(M3GPU_ERR_CUDA, "synchronize: %s", cudaGetErrorString(e));
+    }
+    return M3GPU_OK;
+}
+
+// Device copies of the world views and the largest-first launch order,
+// cached across calls while the batch stays the same.
+struct m3BatchCache
+{
+    std::vector<m3HostWorld*> worlds;
+    std::vector<void*> slabs;
+    m3WorldView* dviews = nullptr;
+    int32_t* dorder = nullptr;
+    uint64_t* dhash = nullptr;
+    int32_t cap = 0;
+};
+static m3BatchCache s_batch;
+
+static int32_t Check(cudaError_t e, const char* what)
+{
+    if (e != cudaSuccess)
+    {
+        return m3gpuSetError(M3GPU_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    }
+    return M3GPU_OK;
+}
+
+static int32_t PrepareBatch(m3HostWorld** worlds, int32_t count)
+{
+    for (int32_t i = 0; i < count; ++i)
+    {
+        m3HostWorld* w = worlds[i];
+        if (w->hostDirty || w->dslab == nullptr)
+        {
+            w->hv.sc->status = 0;
+            int32_t rc = m3gpuUpload(w);
+            if (rc != M3GPU_OK)
+            {
+                return rc;
+            }
+        }
+    }
+    bool same = (int32_t)s_batch.worlds.size() == count;
+    for (int32_t i = 0; same && i < count; ++i)
+    {
+        same = s_batch.worlds[(size_t)i] == worlds[i] &&
+               s_batch.slabs[(size_t)i] == (void*)worlds[i]->dslab &&
+               true;
+    }
+    if (same && s_batch.dviews != nullptr)
+    {
+        // Hull pools may have been reallocated by an upload.
+        bool hullsSame = true;
+        for (int32_t i = 0; i < count && hullsSame; ++i)
+        {
+            hullsSame = worlds[i]->dv.hulls == worlds[i]->dhulls;
+        }
+        if (hullsSame)
+        {
+            return M3GPU_OK;
+        }
+    }
+    if (count > s_batch.cap)
+    {
+        cudaFree(s_batch.dviews);
+        cudaFree(s_batch.dorder);
+        cudaFree(s_batch.dhash);
+        s_batch.dviews = nullptr;
+        s_batch.dorder = nullptr;
+        s_batch.dhash = nullptr;
+        int32_t rc = Check(cudaMalloc((void**)&s_batch.dviews, sizeof(m3WorldView) * (size_t)count),
+                           "cudaMalloc(views)");
+        if (rc == M3GPU_OK)
+        {
+            rc = Check(cudaMalloc((void**)&s_batch.dorder, sizeof(int32_t) * (size_t)count),
+                       "cudaMalloc(order)");
+        }
+        if (rc == M3GPU_OK)
+        {
+            rc = Check(cudaMalloc((void**)&s_batch.dhash, sizeof(uint64_t) * (size_t)count),
+                       "cudaMalloc(hash)");
+        }
+        if (rc != M3GPU_OK)
+        {
+            s_batch.cap = 0;
+            return rc;
+        }
+        s_batch.cap = count;
+    }
+    std::vector<m3WorldView> views((size_t)count);
+    std::vector<int32_t> order((size_t)count);
+    for (int32_t i = 0; i < count; ++i)
+    {
+        worlds[i]->dv.hulls = worlds[i]->dhulls;
+        views[(size_t)i] = worlds[i]->dv;
+        order[(size_t)i] = i;
+    }
+    // Largest first: the per-world work grows with bodies and pairs.
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+        return worlds[a]->hv.sc->shapeMax > worlds[b]->hv.sc->shapeMax;
+    });
+    int32_t rc = Check(cudaMemcpy(s_batch.dviews, views.data(), sizeof(m3WorldView) * (size_t)count,
+                                  cudaMemcpyHostToDevice),
+                       "upload views");
+    if (rc == M3GPU_OK)
+    {
+        rc = Check(cudaMemcpy(s_batch.dorder, order.data(), sizeof(int32_t) * (size_t)count,
+                              cudaMemcpyHostToDevice),
+                   "upload order");
+    }
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
+    s_batch.worlds.assign(worlds, worlds + count);
+    s_batch.slabs.resize((size_t)count);
+    for (int32_t i = 0; i < count; ++i)
+    {
+        s_batch.slabs[(size_t)i] = worlds[i]->dslab;
+    }
+    return M3GPU_OK;
+}
+
+int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t substeps,
+                       int32_t steps)
+{
+    int32_t rc = m3gpuEnsureDevice();
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
+    rc = PrepareBatch(worlds, count);
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0);
+    for (int32_t step = 0; step < steps; ++step)
+    {
+        m3CollideKernel<<<count, M3_BLOCK>>>(s_batch.dviews, s_batch.dorder, count);
+        m3SolveKernel<<<count, M3_BLOCK>>>(s_batch.dviews, s_batch.dorder, count, dt, substeps);
+        s_launches += 2;
+    }
+    cudaEventRecord(e1);
+    rc = Check(cudaGetLastError(), "step launch");
+    if (rc == M3GPU_OK)
+    {
+        rc = Check(cudaEventSynchronize(e1), "step");
+    }
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    s_lastStepMs = ms;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    for (int32_t i = 0; i < count; ++i)
+    {
+        worlds[i]->deviceAhead = true;
+    }
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
+    // Surface device-side refusals.
+    for (int32_t i = 0; i < count; ++i)
+    {
+        int32_t status = 0;
+        int32_t detail = 0;
+        cudaMemcpy(&status, &worlds[i]->dv.sc->status, sizeof(int32_t), cudaMemcpyDeviceToHost);
+        if (status != 0)
+        {
+            cudaMemcpy(&detail, &worlds[i]->dv.sc->statusDetail, sizeof(int32_t),
+                       cudaMemcpyDeviceToHost);
+            return m3gpuSetError(status, "world %d stalled on the device (status %d, detail %d)",
+                                 worlds[i]->slot, status, detail);
+        }
+    }
+    return M3GPU_OK;
+}
+
+int32_t m3gpuHashBatch(m3HostWorld** worlds, int32_t count, uint64_t* out)
+{
+    int32_t rc = m3gpuEnsureDevice();
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
+    rc = PrepareBatch(worlds, count);
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
+    m3HashKernel<<<(count + 127) / 128, 128>>>(s_batch.dviews, count, s_batch.dhash);
+    s_launches += 1;
+    rc = Check(cudaGetLastError(), "hash launch");
+    if (rc == M3GPU_OK)
+    {
+        rc = Check(cudaMemcpy(out, s_batch.dhash, sizeof(uint64_t) * (size_t)count,
+                              cudaMemcpyDeviceToHost),
+                   "hash readback");
+    }
+    return rc;
+}

@@ -1,0 +1,1130 @@
+// World creation and the host-side mirror of the reference's creation
+// API: worlds, bodies, shapes (sphere, plane, capsule, box hull) and
+// joints (spherical, revolute, fixed), with the same validation, the
+// same slot allocation, the same hull interning and the same mass
+// properties, so a world built here hashes bit-identically to one built
+// by the reference from the same calls.  All of this is create-time
+// host work; the per-step path is in step.cu.
+//
+// Reference counterparts: src/world.c:64-460 (world def and create),
+// src/body.c:35-103 (body def and create), src/shape.c:31-300 and
+// :411-620, :717-830, :1334 (shape defs, mass, create), src/hull.c
+// (box hull and half edges, interning), src/joint.c:15-330 (joint def,
+// frames, create).
+
+#include "m3_world.h"
+#include "m3_hash.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+// ---------------------------------------------------------------------
+// Cookies: a def must come from its m3Default*Def factory
+// (world_internal.h:88-93, joint.c:13).  The struct sizes equal the
+// reference's, so the cookie values do too.
+// ---------------------------------------------------------------------
+#define M3_COOKIE 0x4D33u
+#define M3_WORLD_COOKIE ((int32_t)(M3_COOKIE ^ ((int32_t)sizeof(m3WorldDef) << 8)))
+#define M3_BODY_COOKIE ((int32_t)(M3_COOKIE ^ ((int32_t)sizeof(m3BodyDef) << 8) ^ 1))
+#define M3_SHAPE_COOKIE ((int32_t)(M3_COOKIE ^ ((int32_t)sizeof(m3ShapeDef) << 8) ^ 2))
+#define M3_JOINT_COOKIE ((int32_t)(M3_COOKIE ^ ((int32_t)sizeof(m3JointDef) << 8) ^ 3))
+
+static_assert(sizeof(m3WorldDef) == 112, "m3WorldDef must match the reference layout");
+static_assert(sizeof(m3BodyDef) == 104, "m3BodyDef must match the reference layout");
+static_assert(sizeof(m3ShapeDef) == 88, "m3ShapeDef must match the reference layout");
+static_assert(sizeof(m3JointDef) == 224, "m3JointDef must match the reference layout");
+
+// Worlds this library can hold at once (ids carry the slot in 16 bits).
+#define M3GPU_MAX_WORLDS 65535
+
+static std::vector<m3HostWorld*> s_worlds;
+static std::vector<uint16_t> s_worldGenerations;
+
+static bool FiniteF(float x)
+{
+    return isfinite(x) != 0;
+}
+static bool FiniteV3(m3Vec3 v)
+{
+    return FiniteF(v.x) && FiniteF(v.y) && FiniteF(v.z);
+}
+static bool FiniteQuat(m3Quat q)
+{
+    return FiniteF(q.x) && FiniteF(q.y) && FiniteF(q.z) && FiniteF(q.w);
+}
+static bool FinitePos3(m3Pos3 p)
+{
+    return isfinite(p.x) && isfinite(p.y) && isfinite(p.z);
+}
+
+m3HostWorld* m3gpuWorldFromIndex0(uint16_t index0)
+{
+    return index0 < s_worlds.size() ? s_worlds[index0] : nullptr;
+}
+
+m3HostWorld* m3gpuWorldFromId(m3WorldId id)
+{
+    int32_t slot = id.index1 - 1;
+    if (slot < 0 || slot >= (int32_t)s_worlds.size() || s_worlds[slot] == nullptr ||
+        s_worlds[slot]->generation != id.generation)
+    {
+        return nullptr;
+    }
+    return s_worlds[slot];
+}
+
+// ---------------------------------------------------------------------
+// Worlds
+// ---------------------------------------------------------------------
+extern "C" m3WorldDef m3DefaultWorldDef(void)
+{
+    m3WorldDef def;
+    memset(&def, 0, sizeof(def));
+    def.gravity = v3(0.0f, -10.0f, 0.0f);
+    def.bodyCapacity = 1024;
+    def.shapeCapacity = 2048;
+    def.meshCapacity = 4;
+    def.jointCapacity = 64;
+    def.voxelCapacity = 4;
+    def.characterCapacity = 4;
+    def.vehicleCapacity = 2;
+    def.softBodyCapacity = 2;
+    def.workerCount = 1;
+    def.contactHertz = M3_CONTACT_HERTZ_DEFAULT;
+    def.contactDampingRatio = M3_CONTACT_DAMPING_RATIO_DEFAULT;
+    def.contactPushMaxSpeed = M3_CONTACT_PUSH_MAX_SPEED_DEFAULT;
+    def.restitutionThreshold = M3_RESTITUTION_THRESHOLD_DEFAULT;
+    def.maximumLinearSpeed = M3_MAX_LINEAR_SPEED_DEFAULT;
+    def.enableSleeping = 1;
+    def.enableContinuous = 1;
+    def.hitEventThreshold = M3_HIT_EVENT_THRESHOLD_DEFAULT;
+    def.internalValue = M3_WORLD_COOKIE;
+    return def;
+}
+
+extern "C" m3WorldId m3CreateWorld(const m3WorldDef* def)
+{
+    m3WorldId nullId = {0, 0};
+    m3gpuClearError();
+    if (def == nullptr || def->internalValue != M3_WORLD_COOKIE || def->bodyCapacity <= 0 ||
+        def->shapeCapacity <= 0 || def->meshCapacity <= 0 || def->jointCapacity <= 0 ||
+        def->voxelCapacity <= 0 || def->characterCapacity <= 0 || def->vehicleCapacity <= 0 ||
+        def->softBodyCapacity <= 0 || def->workerCount <= 0 ||
+        (def->enqueueTask == nullptr) != (def->finishTask == nullptr) ||
+        !FiniteV3(def->gravity) || !FiniteF(def->contactHertz) || def->contactHertz <= 0.0f ||
+        !FiniteF(def->contactDampingRatio) || def->contactDampingRatio <= 0.0f ||
+        !FiniteF(def->contactPushMaxSpeed) || def->contactPushMaxSpeed <= 0.0f ||
+        !FiniteF(def->restitutionThreshold) || def->restitutionThreshold < 0.0f ||
+        !FiniteF(def->maximumLinearSpeed) || def->maximumLinearSpeed <= 0.0f ||
+        !FiniteF(def->hitEventThreshold) || def->hitEventThreshold < 0.0f)
+    {
+        m3gpuSetError(M3GPU_ERR_INVALID, "m3CreateWorld: invalid world def");
+        return nullId;
+    }
+    int32_t slot = -1;
+    for (int32_t i = 0; i < (int32_t)s_worlds.size(); ++i)
+    {
+        if (s_worlds[i] == nullptr)
+        {
+            slot = i;
+            break;
+        }
+    }
+    if (slot < 0)
+    {
+        if ((int32_t)s_worlds.size() >= M3GPU_MAX_WORLDS)
+        {
+            m3gpuSetError(M3GPU_ERR_CAPACITY, "m3CreateWorld: world table full");
+            return nullId;
+        }
+        slot = (int32_t)s_worlds.size();
+        s_worlds.push_back(nullptr);
+        s_worldGenerations.push_back(0);
+    }
+
+    m3HostWorld* w = new m3HostWorld();
+    w->slot = slot;
+    w->generation = s_worldGenerations[slot];
+    w->bodyCap = def->bodyCapacity;
+    w->shapeCap = def->shapeCapacity;
+    w->jointCap = def->jointCapacity;
+    w->pairCap = 8 * def->shapeCapacity; // world.c:429
+    w->persistentBytes =
+        m3LayoutPersistent(nullptr, nullptr, w->bodyCap, w->shapeCap, w->jointCap, w->pairCap);
+    w->image.assign((size_t)w->persistentBytes, 0);
+    m3LayoutPersistent(&w->hv, w->image.data(), w->bodyCap, w->shapeCap, w->jointCap, w->pairCap);
+    w->hv.hulls = nullptr;
+    w->hv.scratch = nullptr;
+    w->hv.scratchBytes = 0;
+
+    m3WorldScalars* sc = w->hv.sc;
+    sc->gravity = def->gravity;
+    sc->contactHertz = def->contactHertz;
+    sc->contactDampingRatio = def->contactDampingRatio;
+    sc->contactPushMaxSpeed = def->contactPushMaxSpeed;
+    sc->restitutionThreshold = def->restitutionThreshold;
+    sc->maximumLinearSpeed = def->maximumLinearSpeed;
+    sc->maximumAngularSpeed = M3_MAX_ANGULAR_SPEED_DEFAULT;
+    sc->sleepEnabled = def->enableSleeping != 0 ? 1 : 0;
+    sc->continuousEnabled = def->enableContinuous != 0 ? 1 : 0;
+    sc->hitEventThreshold = def->hitEventThreshold;
+    sc->bodyCap = w->bodyCap;
+    sc->shapeCap = w->shapeCap;
+    sc->jointCap = w->jointCap;
+    sc->pairCap = w->pairCap;
+
+    // Array initial values of the reference's create (world.c:160-440):
+    // empty list heads and unset slots read -1; joint targets identity.
+    for (int32_t i = 0; i < w->bodyCap; ++i)
+    {
+        w->hv.shapeHead[i] = -1;
+        w->hv.jointHead[i] = -1;
+    }
+    for (int32_t i = 0; i < w->shapeCap; ++i)
+    {
+        w->hv.shapeNext[i] = -1;
+        w->hv.hullIndex[i] = -1;
+        w->hv.shapeBody[i] = -1;
+    }
+    for (int32_t i = 0; i < w->jointCap; ++i)
+    {
+        w->hv.jbodyA[i] = -1;
+        w->hv.jbodyB[i] = -1;
+        w->hv.jnextA[i] = -1;
+        w->hv.jnextB[i] = -1;
+        w->hv.jtargetQ[i] = m3IdentityQuat();
+        w->hv.jframeA[i] = m3IdentityQuat();
+        w->hv.jframeB[i] = m3IdentityQuat();
+    }
+    s_worlds[slot] = w;
+    m3WorldId id = {slot + 1, w->generation};
+    return id;
+}
+
+extern "C" void m3DestroyWorld(m3WorldId worldId)
+{
+    m3HostWorld* w = m3gpuWorldFromId(worldId);
+    if (w == nullptr)
+    {
+        return;
+    }
+    m3gpuRelease(w);
+    s_worlds[w->slot] = nullptr;
+    s_worldGenerations[w->slot] = (uint16_t)(s_worldGenerations[w->slot] + 1);
+    delete w;
+}
+
+extern "C" bool m3World_IsValid(m3WorldId worldId)
+{
+    return m3gpuWorldFromId(worldId) != nullptr;
+}
+
+// ---------------------------------------------------------------------
+// Bodies (body.c:35-103)
+// ---------------------------------------------------------------------
+extern "C" m3BodyDef m3DefaultBodyDef(void)
+{
+    m3BodyDef def;
+    memset(&def, 0, sizeof(def));
+    def.type = m3_staticBody;
+    def.rotation = m3IdentityQuat();
+    def.gravityScale = 1.0f;
+    def.internalValue = M3_BODY_COOKIE;
+    return def;
+}
+
+static int32_t BodySlot(const m3HostWorld* w, m3BodyId id)
+{
+    int32_t index = id.index1 - 1;
+    if (w == nullptr || id.world0 != (uint16_t)w->slot || index < 0 ||
+        index >= w->hv.sc->bodyMax || w->hv.bodyAlive[index] == 0 ||
+        w->hv.bodyGen[index] != id.generation)
+    {
+        return -1;
+    }
+    return index;
+}
+
+static m3HostWorld* ResolveBody(m3BodyId id, int32_t* index)
+{
+    m3HostWorld* w = m3gpuWorldFromIndex0(id.world0);
+    *index = w != nullptr ? BodySlot(w, id) : -1;
+    return *index >= 0 ? w : nullptr;
+}
+
+extern "C" m3BodyId m3CreateBody(m3WorldId worldId, const m3BodyDef* def)
+{
+    m3BodyId nullId = {0, 0, 0};
+    m3gpuClearError();
+    m3HostWorld* w = m3gpuWorldFromId(worldId);
+    if (w == nullptr || def == nullptr || def->internalValue != M3_BODY_COOKIE)
+    {
+        m3gpuSetError(M3GPU_ERR_INVALID, "m3CreateBody: stale world or invalid def");
+        return nullId;
+    }
+    m3real qq = def->rotation.x * def->rotation.x + def->rotation.y * def->rotation.y +
+                def->rotation.z * def->rotation.z + def->rotation.w * def->rotation.w;
+    if ((def->type != m3_staticBody && def->type != m3_kinematicBody &&
+         def->type != m3_dynamicBody) ||
+        !FinitePos3(def->position) || !FiniteQuat(def->rotation) ||
+        !FiniteV3(def->linearVelocity) || !FiniteV3(def->angularVelocity) ||
+        !FiniteF(def->gravityScale) || !FiniteF(def->linearDamping) ||
+        !FiniteF(def->angularDamping) || def->linearDamping < 0.0f ||
+        def->angularDamping < 0.0f || !(qq > 0.98f) || !(qq < 1.02f))
+    {
+        m3gpuSetError(M3GPU_ERR_INVALID, "m3CreateBody: invalid body def");
+        return nullId;
+    }
+    if (m3gpuSyncHost(w) != M3GPU_OK)
+    {
+        return nullId;
+    }
+    m3WorldView& v = w->hv;
+    if (v.sc->bodyMax >= w->bodyCap)
+    {
+        m3gpuSetError(M3GPU_ERR_CAPACITY, "m3CreateBody: body pool exhausted");
+        return nullId;
+    }
+    int32_t i = v.sc->bodyMax;
+    v.sc->bodyMax += 1;
+    v.bodyAlive[i] = 1;
+    v.xf[i].p = def->position;
+    v.xf[i].q = m3NormalizeQuat(def->rotation);
+    v.v[i] = def->linearVelocity;
+    v.w[i] = def->angularVelocity;
+    v.invMass[i] = def->type == m3_dynamicBody ? 1.0f : 0.0f;
+    v.invI[i] = m3ZeroMat3();
+    v.inertia[i] = m3ZeroMat3();
+    v.awake[i] = 1;
+    v.sleepTime[i] = 0.0f;
+    v.minExt[i] = 1.0e30f;
+    v.maxExt[i] = 0.0f;
+    v.lc[i] = v3(0.0f, 0.0f, 0.0f);
+    v.gravityScale[i] = def->gravityScale;
+    v.linDamp[i] = def->linearDamping;
+    v.angDamp[i] = def->angularDamping;
+    v.btype[i] = (uint8_t)def->type;
+    v.bullet[i] = def->isBullet ? 1 : 0;
+    v.userData[i] = def->userData;
+    v.enabled[i] = 1;
+    v.locks[i] = 0;
+    v.sleepThreshold[i] = M3_SLEEP_VELOCITY_DEFAULT;
+    v.canSleep[i] = 1;
+    v.hasTarget[i] = 0;
+    v.target[i].p.x = 0.0;
+    v.target[i].p.y = 0.0;
+    v.target[i].p.z = 0.0;
+    v.target[i].q = m3IdentityQuat();
+    v.shapeHead[i] = -1;
+    v.jointHead[i] = -1;
+    w->hostDirty = true;
+    m3BodyId id = {i + 1, (uint16_t)w->slot, v.bodyGen[i]};
+    return id;
+}
+
+extern "C" bool m3Body_IsValid(m3BodyId bodyId)
+{
+    int32_t index;
+    return ResolveBody(bodyId, &index) != nullptr;
+}
+
+template <typename T, typename F> static T ReadBody(m3BodyId id, T zero, F get)
+{
+    int32_t index;
+    m3HostWorld* w = ResolveBody(id, &index);
+    if (w == nullptr || m3gpuSyncHost(w) != M3GPU_OK)
+    {
+        return zero;
+    }
+    return get(w->hv, index);
+}
+
+extern "C" m3Pos3 m3Body_GetPosition(m3BodyId bodyId)
+{
+    m3Pos3 zero = {0.0, 0.0, 0.0};
+    return ReadBody(bodyId, zero, [](const m3WorldView& v, int32_t i) { return v.xf[i].p; });
+}
+
+extern "C" m3Quat m3Body_GetRotation(m3BodyId bodyId)
+{
+    return ReadBody(bodyId, m3IdentityQuat(),
+                    [](const m3WorldView& v, int32_t i) { return v.xf[i].q; });
+}
+
+extern "C" m3Vec3 m3Body_GetLinearVelocity(m3BodyId bodyId)
+{
+    return ReadBody(bodyId, v3(0.0f, 0.0f, 0.0f),
+                    [](const m3WorldView& v, int32_t i) { return v.v[i]; });
+}
+
+extern "C" m3Vec3 m3Body_GetAngularVelocity(m3BodyId bodyId)
+{
+    return ReadBody(bodyId, v3(0.0f, 0.0f, 0.0f),
+                    [](const m3WorldView& v, int32_t i) { return v.w[i]; });
+}
+
+extern "C" bool m3Body_IsAwake(m3BodyId bodyId)
+{
+    return ReadBody(bodyId, false, [](const m3WorldView& v, int32_t i) {
+        return v.btype[i] != M3_BODY_DYNAMIC || v.awake[i] != 0;
+    });
+}
+
+// ---------------------------------------------------------------------
+// Mass properties (shape.c:48-300)
+// ---------------------------------------------------------------------
+
+// Adjugate inverse of a symmetric 3x3; singular or non-positive gives
+// zero (shape.c:48-71).
+static m3Mat3 InvertSymmetric(m3Mat3 m)
+{
+    m3real a = m.cx.x;
+    m3real b = m.cy.x;
+    m3real c = m.cz.x;
+    m3real d = m.cy.y;
+    m3real e = m.cz.y;
+    m3real f = m.cz.z;
+    m3real co00 = d * f - e * e;
+    m3real co01 = c * e - b * f;
+    m3real co02 = b * e - c * d;
+    m3real det = a * co00 + b * co01 + c * co02;
+    if (!(det > 0.0f))
+    {
+        return m3ZeroMat3();
+    }
+    m3real inv = 1.0f / det;
+    m3Mat3 r;
+    r.cx = v3(co00 * inv, co01 * inv, co02 * inv);
+    r.cy = v3(co01 * inv, (a * f - c * c) * inv, (b * c - a * e) * inv);
+    r.cz = v3(co02 * inv, (b * c - a * e) * inv, (a * d - b * b) * inv);
+    return r;
+}
+
+// Shape frame to body frame: c' = p + R c, I' = R I R^T (shape.c:79-112).
+static void ComposeMassProps(const m3WorldView& v, int32_t s, m3Vec3* com, m3Mat3* inertia)
+{
+    if (v.hasOffset[s] == 0)
+    {
+        return;
+    }
+    m3Quat q = v.localRot[s];
+    *com = m3Add3(v.localPos[s], m3RotateVec3(q, *com));
+    m3Mat3 r;
+    r.cx = m3RotateVec3(q, v3(1.0f, 0.0f, 0.0f));
+    r.cy = m3RotateVec3(q, v3(0.0f, 1.0f, 0.0f));
+    r.cz = m3RotateVec3(q, v3(0.0f, 0.0f, 1.0f));
+    const m3Mat3 in = *inertia;
+    m3Mat3 t;
+    t.cx = v3(in.cx.x * r.cx.x + in.cy.x * r.cx.y + in.cz.x * r.cx.z,
+              in.cx.y * r.cx.x + in.cy.y * r.cx.y + in.cz.y * r.cx.z,
+              in.cx.z * r.cx.x + in.cy.z * r.cx.y + in.cz.z * r.cx.z);
+    t.cy = v3(in.cx.x * r.cy.x + in.cy.x * r.cy.y + in.cz.x * r.cy.z,
+              in.cx.y * r.cy.x + in.cy.y * r.cy.y + in.cz.y * r.cy.z,
+              in.cx.z * r.cy.x + in.cy.z * r.cy.y + in.cz.z * r.cy.z);
+    t.cz = v3(in.cx.x * r.cz.x + in.cy.x * r.cz.y + in.cz.x * r.cz.z,
+              in.cx.y * r.cz.x + in.cy.y * r.cz.y + in.cz.y * r.cz.z,
+              in.cx.z * r.cz.x + in.cy.z * r.cz.y + in.cz.z * r.cz.z);
+    inertia->cx = v3(r.cx.x * t.cx.x + r.cy.x * t.cx.y + r.cz.x * t.cx.z,
+                     r.cx.y * t.cx.x + r.cy.y * t.cx.y + r.cz.y * t.cx.z,
+                     r.cx.z * t.cx.x + r.cy.z * t.cx.y + r.cz.z * t.cx.z);
+    inertia->cy = v3(r.cx.x * t.cy.x + r.cy.x * t.cy.y + r.cz.x * t.cy.z,
+                     r.cx.y * t.cy.x + r.cy.y * t.cy.y + r.cz.y * t.cy.z,
+                     r.cx.z * t.cy.x + r.cy.z * t.cy.y + r.cz.z * t.cy.z);
+    inertia->cz = v3(r.cx.x * t.cz.x + r.cy.x * t.cz.y + r.cz.x * t.cz.z,
+                     r.cx.y * t.cz.x + r.cy.y * t.cz.y + r.cz.y * t.cz.z,
+                     r.cx.z * t.cz.x + r.cy.z * t.cz.y + r.cz.z * t.cz.z);
+}
+
+// Density-scaled mass, centroid and centroid inertia of one shape;
+// planes carry none (shape.c:114-180).
+static int ShapeMassProps(const m3HostWorld* w, int32_t s, float* massOut, m3Vec3* comOut,
+                          m3Mat3* inertiaOut)
+{
+    const m3WorldView& v = w->hv;
+    uint8_t type = v.shapeType[s];
+    if (type == M3_SHAPE_SPHERE)
+    {
+        float r = v.geom[s].s;
+        float m = v.density[s] * (4.0f / 3.0f) * M3_PI * r * r * r;
+        float ic = 0.4f * m * r * r;
+        *massOut = m;
+        *comOut = v.geom[s].v;
+        *inertiaOut = m3ZeroMat3();
+        inertiaOut->cx.x = ic;
+        inertiaOut->cy.y = ic;
+        inertiaOut->cz.z = ic;
+        return 1;
+    }
+    if (type == M3_SHAPE_CAPSULE)
+    {
+        // Cylinder plus two hemispheres about the segment midpoint:
+        // I = Iperp Id + (Iaxial - Iperp) u u^T.
+        m3Vec3 p1 = v.geom[s].v;
+        m3Vec3 p2 = v.geom[s].v2;
+        float r = v.geom[s].s;
+        m3Vec3 axis = m3Sub3(p2, p1);
+        float length = sqrtf(m3Dot3(axis, axis));
+        m3Vec3 u = length > 0.0f ? m3MulSV3(1.0f / length, axis) : v3(1.0f, 0.0f, 0.0f);
+        float density = v.density[s];
+        float mCyl = density * M3_PI * r * r * length;
+        float mSph = density * (4.0f / 3.0f) * M3_PI * r * r * r;
+        float axial = 0.5f * mCyl * r * r + 0.4f * mSph * r * r;
+        float perp = mCyl * (length * length / 12.0f + 0.25f * r * r) +
+                     mSph * (0.4f * r * r + 0.25f * length * length + 0.375f * length * r);
+        *massOut = mCyl + mSph;
+        *comOut = m3MulSV3(0.5f, m3Add3(p1, p2));
+        m3Mat3 ic2 = m3ZeroMat3();
+        float d = axial - perp;
+        ic2.cx = v3(perp + d * u.x * u.x, d * u.x * u.y, d * u.x * u.z);
+        ic2.cy = v3(d * u.x * u.y, perp + d * u.y * u.y, d * u.y * u.z);
+        ic2.cz = v3(d * u.x * u.z, d * u.y * u.z, perp + d * u.z * u.z);
+        *inertiaOut = ic2;
+        return 1;
+    }
+    if (type == M3_SHAPE_HULL)
+    {
+        const m3HullData* hull = &w->hulls[v.hullIndex[s]];
+        float density = v.density[s];
+        *massOut = density * hull->unitMass;
+        *comOut = hull->unitCom;
+        m3Mat3 ic = hull->unitInertiaCom;
+        ic.cx = m3MulSV3(density, ic.cx);
+        ic.cy = m3MulSV3(density, ic.cy);
+        ic.cz = m3MulSV3(density, ic.cz);
+        *inertiaOut = ic;
+        return 1;
+    }
+    return 0;
+}
+
+// Two passes: mass and centre, then the parallel-axis inertia; then the
+// continuous-collision extents (shape.c:182-300).
+static void RecomputeMass(m3HostWorld* w, int32_t b)
+{
+    m3WorldView& v = w->hv;
+    if (v.btype[b] != M3_BODY_DYNAMIC)
+    {
+        v.invMass[b] = 0.0f;
+        v.invI[b] = m3ZeroMat3();
+        v.inertia[b] = m3ZeroMat3();
+        v.lc[b] = v3(0.0f, 0.0f, 0.0f);
+        v.minExt[b] = 1.0e30f;
+        v.maxExt[b] = 0.0f;
+        return;
+    }
+    float mass = 0.0f;
+    m3Vec3 center = v3(0.0f, 0.0f, 0.0f);
+    for (int32_t s = v.shapeHead[b]; s != -1; s = v.shapeNext[s])
+    {
+        float m;
+        m3Vec3 c;
+        m3Mat3 ic;
+        if (!ShapeMassProps(w, s, &m, &c, &ic))
+        {
+            continue;
+        }
+        ComposeMassProps(v, s, &c, &ic);
+        mass += m;
+        center = m3Add3(center, m3MulSV3(m, c));
+    }
+    if (!(mass > 0.0f))
+    {
+        v.invMass[b] = 1.0f;
+        v.invI[b] = m3ZeroMat3();
+        v.inertia[b] = m3ZeroMat3();
+        v.lc[b] = v3(0.0f, 0.0f, 0.0f);
+        v.minExt[b] = 1.0e30f;
+        v.maxExt[b] = 0.0f;
+        return;
+    }
+    center = m3MulSV3(1.0f / mass, center);
+    m3Mat3 inertia = m3ZeroMat3();
+    for (int32_t s = v.shapeHead[b]; s != -1; s = v.shapeNext[s])
+    {
+        float m;
+        m3Vec3 c;
+        m3Mat3 ic;
+        if (!ShapeMassProps(w, s, &m, &c, &ic))
+        {
+            continue;
+        }
+        ComposeMassProps(v, s, &c, &ic);
+        m3Vec3 d = m3Sub3(c, center);
+        float d2 = m3Dot3(d, d);
+        inertia.cx.x += ic.cx.x + m * (d2 - d.x * d.x);
+        inertia.cy.y += ic.cy.y + m * (d2 - d.y * d.y);
+        inertia.cz.z += ic.cz.z + m * (d2 - d.z * d.z);
+        inertia.cy.x += ic.cy.x - m * d.x * d.y;
+        inertia.cx.y += ic.cx.y - m * d.x * d.y;
+        inertia.cz.x += ic.cz.x - m * d.x * d.z;
+        inertia.cx.z += ic.cx.z - m * d.x * d.z;
+        inertia.cz.y += ic.cz.y - m * d.y * d.z;
+        inertia.cy.z += ic.cy.z - m * d.y * d.z;
+    }
+    v.invMass[b] = 1.0f / mass;
+    v.inertia[b] = inertia;
+    v.invI[b] = InvertSymmetric(inertia);
+
+    float minExtent = 1.0e30f;
+    float maxExtent = 0.0f;
+    for (int32_t s2 = v.shapeHead[b]; s2 != -1; s2 = v.shapeNext[s2])
+    {
+        uint8_t type = v.shapeType[s2];
+        if (type == M3_SHAPE_SPHERE)
+        {
+            float r = v.geom[s2].s;
+            m3Vec3 d = m3Sub3(v.geom[s2].v, center);
+            minExtent = m3MinF(minExtent, r);
+            maxExtent = m3MaxF(maxExtent, sqrtf(m3Dot3(d, d)) + r);
+        }
+        else if (type == M3_SHAPE_CAPSULE)
+        {
+            float r = v.geom[s2].s;
+            m3Vec3 d1 = m3Sub3(v.geom[s2].v, center);
+            m3Vec3 d2 = m3Sub3(v.geom[s2].v2, center);
+            minExtent = m3MinF(minExtent, r);
+            maxExtent = m3MaxF(maxExtent, sqrtf(m3MaxF(m3Dot3(d1, d1), m3Dot3(d2, d2))) + r);
+        }
+        else if (type == M3_SHAPE_HULL)
+        {
+            const m3HullData* hull = &w->hulls[v.hullIndex[s2]];
+            for (int32_t f = 0; f < hull->faceCount; ++f)
+            {
+                float dist = hull->faceOffsets[f] - m3Dot3(hull->faceNormals[f], center);
+                minExtent = m3MinF(minExtent, dist);
+            }
+            for (int32_t k = 0; k < hull->vertexCount; ++k)
+            {
+                m3Vec3 d = m3Sub3(hull->vertices[k], center);
+                maxExtent = m3MaxF(maxExtent, sqrtf(m3Dot3(d, d)));
+            }
+        }
+    }
+    v.minExt[b] = minExtent;
+    v.maxExt[b] = maxExtent;
+    v.lc[b] = center;
+}
+
+// ---------------------------------------------------------------------
+// Hulls (hull.c)
+// ---------------------------------------------------------------------
+
+// Half-edge adjacency from the face loops, twins at 2k and 2k+1, and
+// the vertex centroid (hull.c:71-130).
+static void BuildHalfEdges(m3HullData* hull)
+{
+    int32_t count = 0;
+    int32_t dirKey[M3_HULL_MAX_HALF_EDGES];
+    int32_t dirSlot[M3_HULL_MAX_HALF_EDGES];
+    int32_t dirCount = 0;
+    int32_t faceEdgeSlot[M3_HULL_MAX_FACE_INDICES];
+    for (int32_t f = 0; f < hull->faceCount; ++f)
+    {
+        int32_t n = hull->faceVertCounts[f];
+        int32_t start = hull->faceVertStart[f];
+        for (int32_t k = 0; k < n; ++k)
+        {
+            int32_t a = hull->faceIndices[start + k];
+            int32_t b = hull->faceIndices[start + (k + 1) % n];
+            int32_t reverse = b * 256 + a;
+            int32_t slot = -1;
+            for (int32_t d = 0; d < dirCount; ++d)
+            {
+                if (dirKey[d] == reverse)
+                {
+                    slot = dirSlot[d] ^ 1;
+                    break;
+                }
+            }
+            if (slot < 0)
+            {
+                slot = count;
+                count += 2;
+                dirKey[dirCount] = a * 256 + b;
+                dirSlot[dirCount] = slot;
+                dirCount += 1;
+            }
+            hull->edges[slot].origin = (uint8_t)a;
+            hull->edges[slot].twin = (uint16_t)(slot ^ 1);
+            hull->edges[slot].face = (uint8_t)f;
+            faceEdgeSlot[start + k] = slot;
+        }
+    }
+    for (int32_t f = 0; f < hull->faceCount; ++f)
+    {
+        int32_t n = hull->faceVertCounts[f];
+        int32_t start = hull->faceVertStart[f];
+        for (int32_t k = 0; k < n; ++k)
+        {
+            hull->edges[faceEdgeSlot[start + k]].next = (uint16_t)faceEdgeSlot[start + (k + 1) % n];
+        }
+    }
+    hull->edgeCount = count;
+    m3Vec3 c = v3(0.0f, 0.0f, 0.0f);
+    for (int32_t k = 0; k < hull->vertexCount; ++k)
+    {
+        c = m3Add3(c, hull->vertices[k]);
+    }
+    hull->center = m3MulSV3(1.0f / (m3real)hull->vertexCount, c);
+}
+
+// Closed-form box: canonical vertex order, six outward CCW faces, unit
+// density mass (hull.c:14-64).
+static void BuildBoxHull(m3HullData* out, m3Vec3 he)
+{
+    memset(out, 0, sizeof(*out));
+    m3real hx = he.x;
+    m3real hy = he.y;
+    m3real hz = he.z;
+    const m3Vec3 verts[8] = {
+        v3(-hx, -hy, -hz), v3(hx, -hy, -hz), v3(hx, hy, -hz), v3(-hx, hy, -hz),
+        v3(-hx, -hy, hz),  v3(hx, -hy, hz),  v3(hx, hy, hz),  v3(-hx, hy, hz),
+    };
+    const m3Vec3 normals[6] = {
+        v3(1.0f, 0.0f, 0.0f),  v3(-1.0f, 0.0f, 0.0f), v3(0.0f, 1.0f, 0.0f),
+        v3(0.0f, -1.0f, 0.0f), v3(0.0f, 0.0f, 1.0f),  v3(0.0f, 0.0f, -1.0f),
+    };
+    const m3real offsets[6] = {hx, hx, hy, hy, hz, hz};
+    static const uint8_t loops[6][4] = {
+        {1, 2, 6, 5}, {0, 4, 7, 3}, {2, 3, 7, 6}, {0, 1, 5, 4}, {4, 5, 6, 7}, {0, 3, 2, 1},
+    };
+    out->vertexCount = 8;
+    out->faceCount = 6;
+    out->indexCount = 24;
+    memcpy(out->vertices, verts, sizeof(verts));
+    memcpy(out->faceNormals, normals, sizeof(normals));
+    memcpy(out->faceOffsets, offsets, sizeof(offsets));
+    for (int32_t f = 0; f < 6; ++f)
+    {
+        out->faceVertCounts[f] = 4;
+        out->faceVertStart[f] = (uint16_t)(4 * f);
+        for (int32_t k = 0; k < 4; ++k)
+        {
+            out->faceIndices[4 * f + k] = loops[f][k];
+        }
+    }
+    float m = 8.0f * hx * hy * hz;
+    out->unitMass = m;
+    out->unitCom = v3(0.0f, 0.0f, 0.0f);
+    out->unitInertiaCom = m3ZeroMat3();
+    out->unitInertiaCom.cx.x = (m / 3.0f) * (hy * hy + hz * hz);
+    out->unitInertiaCom.cy.y = (m / 3.0f) * (hx * hx + hz * hz);
+    out->unitInertiaCom.cz.z = (m / 3.0f) * (hx * hx + hy * hy);
+    BuildHalfEdges(out);
+}
+
+// Content-deduplicated interning in ascending slot order (hull.c:132-152).
+static int32_t InternHull(m3HostWorld* w, const m3HullData* data)
+{
+    m3WorldScalars* sc = w->hv.sc;
+    for (int32_t i = 0; i < sc->hullMax; ++i)
+    {
+        if (w->hullRefs[i] > 0 && memcmp(&w->hulls[i], data, sizeof(m3HullData)) == 0)
+        {
+            w->hullRefs[i] += 1;
+            return i;
+        }
+    }
+    if (sc->hullMax >= w->shapeCap)
+    {
+        return -1;
+    }
+    int32_t index = sc->hullMax;
+    sc->hullMax += 1;
+    w->hulls.push_back(*data);
+    w->hullRefs.push_back(1);
+    return index;
+}
+
+// ---------------------------------------------------------------------
+// Shapes (shape.c:411-620, :717-830, :1334)
+// ---------------------------------------------------------------------
+extern "C" m3ShapeDef m3DefaultShapeDef(void)
+{
+    m3ShapeDef def;
+    memset(&def, 0, sizeof(def));
+    def.density = 1.0f;
+    def.friction = 0.6f;
+    def.restitution = 0.0f;
+    def.categoryBits = 1ull;
+    def.maskBits = ~0ull;
+    def.groupIndex = 0;
+    def.localRotation = q4(0.0f, 0.0f, 0.0f, 1.0f);
+    def.internalValue = M3_SHAPE_COOKIE;
+    return def;
+}
+
+static m3ShapeId CreateShapeCommon(m3BodyId bodyId, const m3ShapeDef* def, uint8_t type,
+                                   const m3ShapeGeom* geom)
+{
+    m3ShapeId nullId = {0, 0, 0};
+    int32_t b;
+    m3HostWorld* w = ResolveBody(bodyId, &b);
+    if (w == nullptr || def == nullptr || def->internalValue != M3_SHAPE_COOKIE)
+    {
+        m3gpuSetError(M3GPU_ERR_INVALID, "create shape: stale body or invalid def");
+        return nullId;
+    }
+    float rotLen2 = def->localRotation.x * def->localRotation.x +
+                    def->localRotation.y * def->localRotation.y +
+                    def->localRotation.z * def->localRotation.z +
+                    def->localRotation.w * def->localRotation.w;
+    if (!FiniteV3(def->localPosition) || !FiniteQuat(def->localRotation) || rotLen2 < 0.99f ||
+        rotLen2 > 1.01f || !FiniteF(def->density) || !(def->density > 0.0f) ||
+        !FiniteF(def->friction) || def->friction < 0.0f || !FiniteF(def->restitution) ||
+        def->restitution < 0.0f || !FiniteF(def->rollingResistance) ||
+        def->rollingResistance < 0.0f)
+    {
+        m3gpuSetError(M3GPU_ERR_INVALID, "create shape: invalid material or offset");
+        return nullId;
+    }
+    if (m3gpuSyncHost(w) != M3GPU_OK)
+    {
+        return nullId;
+    }
+    m3WorldView& v = w->hv;
+    if (v.sc->shapeMax >= w->shapeCap)
+    {
+        m3gpuSetError(M3GPU_ERR_CAPACITY, "create shape: shape pool exhausted");
+        return nullId;
+    }
+    int32_t hullIndex = -1;
+    if (type == M3_SHAPE_HULL)
+    {
+        m3HullData data;
+        BuildBoxHull(&data, geom->v);
+        hullIndex = InternHull(w, &data);
+        if (hullIndex < 0)
+        {
+            m3gpuSetError(M3GPU_ERR_CAPACITY, "create shape: hull pool exhausted");
+            return nullId;
+        }
+    }
+    int32_t s = v.sc->shapeMax;
+    v.sc->shapeMax += 1;
+    v.shapeAlive[s] = 1;
+    v.shapeBody[s] = b;
+    v.shapeType[s] = type;
+    v.geom[s] = *geom;
+    v.density[s] = def->density;
+    v.friction[s] = def->friction;
+    v.restitution[s] = def->restitution;
+    v.rolling[s] = def->rollingResistance;
+    v.category[s] = def->categoryBits;
+    v.mask[s] = def->maskBits;
+    v.group[s] = def->groupIndex;
+    v.shapeUserData[s] = def->userData;
+    v.sensor[s] = def->isSensor ? 1 : 0;
+    v.hitEvents[s] = def->enableHitEvents ? 1 : 0;
+    v.preSolve[s] = def->enablePreSolveEvents ? 1 : 0;
+    v.surfVel[s] = v3(0.0f, 0.0f, 0.0f);
+    v.localPos[s] = def->localPosition;
+    v.localRot[s] = def->localRotation;
+    v.hasOffset[s] = (def->localPosition.x != 0.0f || def->localPosition.y != 0.0f ||
+                      def->localPosition.z != 0.0f || def->localRotation.x != 0.0f ||
+                      def->localRotation.y != 0.0f || def->localRotation.z != 0.0f ||
+                      def->localRotation.w != 1.0f)
+                         ? 1
+                         : 0;
+    v.shapeNext[s] = v.shapeHead[b];
+    v.shapeHead[b] = s;
+    v.hullIndex[s] = hullIndex;
+    RecomputeMass(w, b);
+    w->hostDirty = true;
+    m3ShapeId id = {s + 1, (uint16_t)w->slot, v.shapeGen[s]};
+    return id;
+}
+
+extern "C" m3ShapeId m3CreateSphereShape(m3BodyId bodyId, const m3ShapeDef* def,
+                                         const m3Sphere* sphere)
+{
+    m3ShapeId nullId = {0, 0, 0};
+    m3gpuClearError();
+    if (sphere == nullptr || !(sphere->radius > 0.0f) || !FiniteF(sphere->radius) ||
+        !FiniteV3(sphere->center))
+    {
+        m3gpuSetError(M3GPU_ERR_INVALID, "m3CreateSphereShape: invalid sphere");
+        return nullId;
+    }
+    m3ShapeGeom geom;
+    geom.v = sphere->center;
+    geom.s = sphere->radius;
+    geom.v2 = v3(0.0f, 0.0f, 0.0f);
+    geom.s2 = 0.0f;
+    return CreateShapeCommon(bodyId, def, M3_SHAPE_SPHERE, &geom);
+}
+
+extern "C" m3ShapeId m3CreatePlaneShape(m3BodyId bodyId, const m3ShapeDef* def,
+                                        const m3Plane* plane)
+{
+    m3ShapeId nullId = {0, 0, 0};
+    m3gpuClearError();
+    if (plane == nullptr || !FiniteV3(plane->normal) || !FiniteF(plane->offset) ||
+        !(m3Dot3(plane->normal, plane->normal) > 1.0e-12f))
+    {
+        m3gpuSetError(M3GPU_ERR_INVALID, "m3CreatePlaneShape: invalid plane");
+        return nullId;
+    }
+    int32_t b;
+    m3HostWorld* w = ResolveBody(bodyId, &b);
+    if (w == nullptr || m3gpuSyncHost(w) != M3GPU_OK || w->hv.btype[b] != M3_BODY_STATIC)
+    {
+        m3gpuSetError(M3GPU_ERR_INVALID, "m3CreatePlaneShape: planes need a static body");
+        return nullId;
+    }
+    m3ShapeGeom geom;
+    geom.v = m3Normalize3(plane->normal);
+    geom.s = plane->offset;
+    geom.v2 = v3(0.0f, 0.0f, 0.0f);
+    geom.s2 = 0.0f;
+    return CreateShapeCommon(bodyId, def, M3_SHAPE_PLANE, &geom);
+}
+
+extern "C" m3ShapeId m3CreateCapsuleShape(m3BodyId bodyId, const m3ShapeDef* def,
+                                          const m3Capsule* capsule)
+{
+    m3ShapeId nullId = {0, 0, 0};
+    m3gpuClearError();
+    if (capsule == nullptr || !(capsule->radius > 0.0f) || !FiniteF(capsule->radius) ||
+        !FiniteV3(capsule->point1) || !FiniteV3(capsule->point2))
+    {
+        m3gpuSetError(M3GPU_ERR_INVALID, "m3CreateCapsuleShape: invalid capsule");
+        return nullId;
+    }
+    m3Vec3 axis = m3Sub3(capsule->point2, capsule->point1);
+    if (!(m3Dot3(axis, axis) > 0.0f))
+    {
+        m3gpuSetError(M3GPU_ERR_INVALID, "m3CreateCapsuleShape: zero-length capsule");
+        return nullId;
+    }
+    m3ShapeGeom geom;
+    geom.v = capsule->point1;
+    geom.s = capsule->radius;
+    geom.v2 = capsule->point2;
+    geom.s2 = 0.0f;
+    return CreateShapeCommon(bodyId, def, M3_SHAPE_CAPSULE, &geom);
+}
+
+extern "C" m3ShapeId m3CreateBoxShape(m3BodyId bodyId, const m3ShapeDef* def, m3Vec3 halfExtents)
+{
+    m3ShapeId nullId = {0, 0, 0};
+    m3gpuClearError();
+    if (!(halfExtents.x > 0.0f) || !(halfExtents.y > 0.0f) || !(halfExtents.z > 0.0f) ||
+        !FiniteV3(halfExtents))
+    {
+        m3gpuSetError(M3GPU_ERR_INVALID, "m3CreateBoxShape: invalid half extents");
+        return nullId;
+    }
+    m3ShapeGeom geom;
+    geom.v = halfExtents;
+    geom.s = 0.0f;
+    geom.v2 = v3(0.0f, 0.0f, 0.0f);
+    geom.s2 = 0.0f;
+    return CreateShapeCommon(bodyId, def, M3_SHAPE_HULL, &geom);
+}
+
+extern "C" bool m3Shape_IsValid(m3ShapeId shapeId)
+{
+    m3HostWorld* w = m3gpuWorldFromIndex0(shapeId.world0);
+    int32_t index = shapeId.index1 - 1;
+    return w != nullptr && index >= 0 && index < w->hv.sc->shapeMax &&
+           w->hv.shapeAlive[index] != 0 && w->hv.shapeGen[index] == shapeId.generation;
+}
+
+// ---------------------------------------------------------------------
+// Joints (joint.c:15-330, :387-520)
+// ---------------------------------------------------------------------
+extern "C" m3JointDef m3DefaultJointDef(void)
+{
+    m3JointDef def;
+    memset(&def, 0, sizeof(def));
+    def.type = m3_sphericalJoint;
+    def.localAxisA = v3(0.0f, 0.0f, 1.0f);
+    def.localAxisB = v3(0.0f, 0.0f, 1.0f);
+    def.genericMotorAxis = 255;
+    def.ratio = 1.0f;
+    def.internalValue = M3_JOINT_COOKIE;
+    return def;
+}
+
+// Quaternion of a right-handed column basis, Shepperd's largest-diagonal
+// branch (joint.c:30-70).
+static m3Quat QuatFromBasis(m3Vec3 t1, m3Vec3 t2, m3Vec3 axis)
+{
+    m3real m00 = t1.x, m01 = t2.x, m02 = axis.x;
+    m3real m10 = t1.y, m11 = t2.y, m12 = axis.y;
+    m3real m20 = t1.z, m21 = t2.z, m22 = axis.z;
+    m3Quat q;
+    m3real trace = m00 + m11 + m22;
+    if (trace > 0.0f)
+    {
+        m3real s = sqrtf(trace + 1.0f) * 2.0f;
+        q.w = 0.25f * s;
+        q.x = (m21 - m12) / s;
+        q.y = (m02 - m20) / s;
+        q.z = (m10 - m01) / s;
+    }
+    else if (m00 > m11 && m00 > m22)
+    {
+        m3real s = sqrtf(1.0f + m00 - m11 - m22) * 2.0f;
+        q.w = (m21 - m12) / s;
+        q.x = 0.25f * s;
+        q.y = (m01 + m10) / s;
+        q.z = (m02 + m20) / s;
+    }
+    else if (m11 > m22)
+    {
+        m3real s = sqrtf(1.0f + m11 - m00 - m22) * 2.0f;
+        q.w = (m02 - m20) / s;
+        q.x = (m01 + m10) / s;
+        q.y = 0.25f * s;
+        q.z = (m12 + m21) / s;
+    }
+    else
+    {
+        m3real s = sqrtf(1.0f + m22 - m00 - m11) * 2.0f;
+        q.w = (m10 - m01) / s;
+        q.x = (m02 + m20) / s;
+        q.y = (m12 + m21) / s;
+        q.z = 0.25f * s;
+    }
+    return m3NormalizeQuat(q);
+}
+
+static m3Quat QuatFromAxisZ(m3Vec3 axis)
+{
+    m3Vec3 t1;
+    m3Vec3 t2;
+    m3MakeTangentBasis(axis, &t1, &t2);
+    return QuatFromBasis(t1, t2, axis);
+}
+
+extern "C" m3JointId m3CreateJoint(const m3JointDef* def)
+{
+    m3JointId nullId = {0, 0, 0};
+    m3gpuClearError();
+    if (def == nullptr || def->internalValue != M3_JOINT_COOKIE)
+    {
+        m3gpuSetError(M3GPU_ERR_INVALID, "m3CreateJoint: invalid def");
+        return nullId;
+    }
+    if (def->type != m3_sphericalJoint && def->type != m3_revoluteJoint &&
+        def->type != m3_fixedJoint)
+    {
+        m3gpuSetError(M3GPU_ERR_UNSUPPORTED,
+                      "m3CreateJoint: joint type %d is not on the device path", def->type);
+        return nullId;
+    }
+    if (def->type == m3_revoluteJoint && (!(m3Dot3(def->localAxisA, def->localAxisA) > 0.0f) ||
+                                          !(m3Dot3(def->localAxisB, def->localAxisB) > 0.0f)))
+    {
+        m3gpuSetError(M3GPU_ERR_INVALID, "m3CreateJoint: a hinge needs real axes");
+        return nullId;
+    }
+    if (!FiniteV3(def->localAnchorA) || !FiniteV3(def->localAnchorB) ||
+        !FiniteV3(def->localAxisA) || !FiniteV3(def->localAxisB) || !FiniteF(def->lowerLimit) ||
+        !FiniteF(def->upperLimit) || !FiniteF(def->motorSpeed) ||
+        !FiniteF(def->maxMotorEffort) || !FiniteF(def->coneAngle) ||
+        def->maxMotorEffort < 0.0f || (def->enableLimit && def->lowerLimit > def->upperLimit) ||
+        (def->enableCone && def->coneAngle < 0.0f))
+    {
+        m3gpuSetError(M3GPU_ERR_INVALID, "m3CreateJoint: non-finite or unordered fields");
+        return nullId;
+    }
+    if (def->type == m3_sphericalJoint && (def->enableCone || def->enableLimit))
+    {
+        m3gpuSetError(M3GPU_ERR_UNSUPPORTED,
+                      "m3CreateJoint: spherical cone and twist limits are not on the device path");
+        return nullId;
+    }
+    m3HostWorld* w = m3gpuWorldFromIndex0(def->bodyA.world0);
+    if (w == nullptr || def->bodyB.world0 != def->bodyA.world0)
+    {
+        m3gpuSetError(M3GPU_ERR_INVALID, "m3CreateJoint: bodies must share a world");
+        return nullId;
+    }
+    int32_t a = BodySlot(w, def->bodyA);
+    int32_t b = BodySlot(w, def->bodyB);
+    if (a < 0 || b < 0 || a == b)
+    {
+        m3gpuSetError(M3GPU_ERR_INVALID, "m3CreateJoint: stale or identical bodies");
+        return nullId;
+    }
+    if (m3gpuSyncHost(w) != M3GPU_OK)
+    {
+        return nullId;
+    }
+    m3WorldView& v = w->hv;
+    if (v.btype[a] != M3_BODY_DYNAMIC && v.btype[b] != M3_BODY_DYNAMIC)
+    {
+        m3gpuSetError(M3GPU_ERR_INVALID, "m3CreateJoint: a joint between immovables");
+        return nullId;
+    }
+    if (v.sc->jointMax >= w->jointCap)
+    {
+        m3gpuSetError(M3GPU_ERR_CAPACITY, "m3CreateJoint: joint pool exhausted");
+        return nullId;
+    }
+    int32_t j = v.sc->jointMax;
+    v.sc->jointMax += 1;
+    v.jointAlive[j] = 1;
+    v.jtype[j] = (uint8_t)def->type;
+    v.jbodyA[j] = a;
+    v.jbodyB[j] = b;
+    v.jlocalA[j] = def->localAnchorA;
+    v.jlocalB[j] = def->localAnchorB;
+    v.jcollide[j] = def->collideConnected ? 1 : 0;
+    v.jimpulse[j] = v3(0.0f, 0.0f, 0.0f);
+    v.jperp[j] = v3(0.0f, 0.0f, 0.0f);
+    v.jlimitImp[j] = v3(0.0f, 0.0f, 0.0f);
+    v.jangular[j] = v3(0.0f, 0.0f, 0.0f);
+    if (def->type == m3_fixedJoint)
+    {
+        const m3Transform& xa = v.xf[a];
+        const m3Transform& xb = v.xf[b];
+        v.jframeA[j] = m3IdentityQuat();
+        v.jframeB[j] = m3NormalizeQuat(m3MulQuat(m3Conj(xb.q), xa.q));
+    }
+    else
+    {
+        v.jframeA[j] = QuatFromAxisZ(m3Normalize3(def->localAxisA));
+        v.jframeB[j] = QuatFromAxisZ(m3Normalize3(def->localAxisB));
+    }
+    v.jflags[j] = (uint8_t)((def->enableLimit ? 1 : 0) | (def->enableMotor ? 2 : 0) |
+                            (def->enableCone ? 4 : 0));
+    v.jmotor[j] = v3(def->motorSpeed, def->maxMotorEffort, 0.0f);
+    v.jbreak[j] = v3(0.0f, 0.0f, 0.0f);
+    v.jspring[j] = v3(0.0f, 0.0f, 0.0f);
+    v.jtargetScalar[j] = 0.0f;
+    v.jtargetQ[j] = m3IdentityQuat();
+    v.jspringImp[j] = v3(0.0f, 0.0f, 0.0f);
+    v.jlimits[j] = v3(def->lowerLimit, def->upperLimit, def->coneAngle);
+    v.jnextA[j] = v.jointHead[a];
+    v.jointHead[a] = j;
+    v.jnextB[j] = v.jointHead[b];
+    v.jointHead[b] = j;
+    if (v.btype[a] == M3_BODY_DYNAMIC)
+    {
+        v.awake[a] = 1;
+        v.sleepTime[a] = 0.0f;
+    }
+    if (v.btype[b] == M3_BODY_DYNAMIC)
+    {
+        v.awake[b] = 1;
+        v.sleepTime[b] = 0.0f;
+    }
+    w->hostDirty = true;
+    m3JointId id = {j + 1, (uint16_t)w->slot, v.jointGen[j]};
+    return id;
+}
+
+extern "C" bool m3Joint_IsValid(m3JointId jointId)
+{
+    m3HostWorld* w = m3gpuWorldFromIndex0(jointId.world0);
+    int32_t index = jointId.index1 - 1;
+    return w != nullptr && index >= 0 && index < w->hv.sc->jointMax &&
+           w->hv.jointAlive[index] != 0 && w->hv.jointGen[index] == jointId.generation;
+}
