@@ -101,3 +101,77 @@ class WorldState:
                 i = int(rows[0])
                 return f"{name}: first differing record {i} of {len(a)} ({len(rows)} differ): {a[i]} vs {b[i]}"
         return None
+
+
+class m3ShapeId(C.Structure):
+    _fields_ = [("index1", C.c_int32), ("world0", C.c_uint16), ("generation", C.c_uint16)]
+
+
+class m3JointId(C.Structure):
+    _fields_ = [("index1", C.c_int32), ("world0", C.c_uint16), ("generation", C.c_uint16)]
+
+
+class m3WorldDef(C.Structure):
+    _fields_ = [("gravity", m3Vec3), ("bodyCapacity", C.c_int32), ("shapeCapacity", C.c_int32),
+                ("meshCapacity", C.c_int32), ("jointCapacity", C.c_int32),
+                ("voxelCapacity", C.c_int32), ("characterCapacity", C.c_int32),
+                ("vehicleCapacity", C.c_int32), ("softBodyCapacity", C.c_int32),
+                ("workerCount", C.c_int32), ("enqueueTask", C.c_void_p),
+                ("finishTask", C.c_void_p), ("userTaskContext", C.c_void_p),
+                ("contactHertz", C.c_float), ("contactDampingRatio", C.c_float),
+                ("contactPushMaxSpeed", C.c_float), ("restitutionThreshold", C.c_float),
+                ("maximumLinearSpeed", C.c_float), ("enableSleeping", C.c_int32),
+                ("enableContinuous", C.c_int32), ("hitEventThreshold", C.c_float),
+                ("internalValue", C.c_int32)]
+
+
+class m3BodyDef(C.Structure):
+    _fields_ = [("type", C.c_int32), ("position", m3Pos3), ("rotation", m3Quat),
+                ("linearVelocity", m3Vec3), ("angularVelocity", m3Vec3),
+                ("gravityScale", C.c_float), ("linearDamping", C.c_float),
+                ("angularDamping", C.c_float), ("userData", C.c_uint64), ("isBullet", C.c_bool),
+                ("internalValue", C.c_int32)]
+
+
+class m3ShapeDef(C.Structure):
+    _fields_ = [("density", C.c_float), ("friction", C.c_float), ("restitution", C.c_float),
+                ("categoryBits", C.c_uint64), ("maskBits", C.c_uint64), ("groupIndex", C.c_int32),
+                ("rollingResistance", C.c_float), ("userData", C.c_uint64),
+                ("isSensor", C.c_bool), ("enableHitEvents", C.c_bool),
+                ("enablePreSolveEvents", C.c_bool), ("localPosition", m3Vec3),
+                ("localRotation", m3Quat), ("internalValue", C.c_int32)]
+
+
+class m3Sphere(C.Structure):
+    _fields_ = [("center", m3Vec3), ("radius", C.c_float)]
+
+
+class m3Plane(C.Structure):
+    _fields_ = [("normal", m3Vec3), ("offset", C.c_float)]
+
+
+class m3Capsule(C.Structure):
+    _fields_ = [("point1", m3Vec3), ("point2", m3Vec3), ("radius", C.c_float)]
+
+
+assert C.sizeof(m3WorldDef) == 112 and C.sizeof(m3BodyDef) == 104 and C.sizeof(m3ShapeDef) == 88
+
+
+def bind_create(lib: C.CDLL) -> C.CDLL:
+    """Declare the reference-named creation API on a handle."""
+    lib.m3DefaultWorldDef.restype = m3WorldDef
+    lib.m3CreateWorld.argtypes = [C.POINTER(m3WorldDef)]
+    lib.m3CreateWorld.restype = m3WorldId
+    lib.m3DefaultBodyDef.restype = m3BodyDef
+    lib.m3CreateBody.argtypes = [m3WorldId, C.POINTER(m3BodyDef)]
+    lib.m3CreateBody.restype = m3BodyId
+    lib.m3DefaultShapeDef.restype = m3ShapeDef
+    lib.m3CreateSphereShape.argtypes = [m3BodyId, C.POINTER(m3ShapeDef), C.POINTER(m3Sphere)]
+    lib.m3CreateSphereShape.restype = m3ShapeId
+    lib.m3CreatePlaneShape.argtypes = [m3BodyId, C.POINTER(m3ShapeDef), C.POINTER(m3Plane)]
+    lib.m3CreatePlaneShape.restype = m3ShapeId
+    lib.m3CreateCapsuleShape.argtypes = [m3BodyId, C.POINTER(m3ShapeDef), C.POINTER(m3Capsule)]
+    lib.m3CreateCapsuleShape.restype = m3ShapeId
+    lib.m3CreateBoxShape.argtypes = [m3BodyId, C.POINTER(m3ShapeDef), m3Vec3]
+    lib.m3CreateBoxShape.restype = m3ShapeId
+    return lib

@@ -436,6 +436,38 @@ __device__ m3Manifold m3CollideHullsDev(const m3HullData* hullA, const m3HullDat
     return manifold;
 }
 
+#include "m3_distance.cuh"
+
+// GJK proxy of a shape in its own frame (manifold.c:463-499).
+__device__ __forceinline__ m3ProxyDev m3MakeProxyDev(const m3WorldView& w, int32_t shape,
+                                                     m3Vec3 scratch[2])
+{
+    m3ProxyDev proxy;
+    uint8_t type = w.shapeType[shape];
+    if (type == M3_SHAPE_HULL)
+    {
+        const m3HullData* hull = &w.hulls[w.hullIndex[shape]];
+        proxy.points = hull->vertices;
+        proxy.count = hull->vertexCount;
+        proxy.radius = 0.0f;
+        return proxy;
+    }
+    if (type == M3_SHAPE_CAPSULE)
+    {
+        scratch[0] = w.geom[shape].v;
+        scratch[1] = w.geom[shape].v2;
+        proxy.points = scratch;
+        proxy.count = 2;
+        proxy.radius = w.geom[shape].s;
+        return proxy;
+    }
+    scratch[0] = w.geom[shape].v;
+    proxy.points = scratch;
+    proxy.count = 1;
+    proxy.radius = w.geom[shape].s;
+    return proxy;
+}
+
 // ---------------------------------------------------------------------
 // The pair dispatcher (manifold.c:2357-2911) for the shape families on
 // the device path.  Returns M3_NARROW_UNSUPPORTED for a pair family it
@@ -642,12 +674,159 @@ __device__ int32_t m3CollidePair(const m3WorldView& w, uint64_t key, m3Manifold*
             }
         }
     }
+    else if (hullPair && capsulePair)
+    {
+        // Capsule versus hull: the segment SAT in the hull frame
+        // (manifold.c:2617-2663).
+        int32_t hullShape = typeA == M3_SHAPE_HULL ? shapeA : shapeB;
+        int32_t capShape = hullShape == shapeA ? shapeB : shapeA;
+        int32_t hullBody = w.shapeBody[hullShape];
+        int32_t capBody = w.shapeBody[capShape];
+        m3Transform xfH = m3ShapeXf(w, hullShape);
+        m3Transform xfC = m3ShapeXf(w, capShape);
+        m3Quat qRel = m3MulQuat(m3Conj(xfH.q), xfC.q);
+        m3Vec3 dp = v3((m3real)(xfC.p.x - xfH.p.x), (m3real)(xfC.p.y - xfH.p.y),
+                       (m3real)(xfC.p.z - xfH.p.z));
+        m3Vec3 pRel = m3InvRotateVec3(xfH.q, dp);
+        m3Vec3 s1 = m3Add3(m3RotateVec3(qRel, w.geom[capShape].v), pRel);
+        m3Vec3 s2 = m3Add3(m3RotateVec3(qRel, w.geom[capShape].v2), pRel);
+        const m3HullData* hull = &w.hulls[w.hullIndex[hullShape]];
+        m3Manifold local = m3CollideSegmentHullDev(hull, s1, s2, w.geom[capShape].s);
+        if (local.pointCount > 0)
+        {
+            m3Vec3 nWorld = m3RotateVec3(xfH.q, local.normal);
+            fresh.normal = hullShape == shapeA ? nWorld : m3Neg3(nWorld);
+            fresh.pointCount = local.pointCount;
+            for (int32_t k = 0; k < local.pointCount; ++k)
+            {
+                m3Vec3 rH = m3RotateVec3(xfH.q, local.points[k].anchorA);
+                m3Vec3 rC = m3RotateVec3(xfH.q, local.points[k].anchorB);
+                m3Vec3 aHull = m3FromCom(w, hullBody, xfH.p.x + (double)rH.x,
+                                         xfH.p.y + (double)rH.y, xfH.p.z + (double)rH.z);
+                m3Vec3 aCap = m3FromCom(w, capBody, xfH.p.x + (double)rC.x,
+                                        xfH.p.y + (double)rC.y, xfH.p.z + (double)rC.z);
+                fresh.points[k].anchorA = hullShape == shapeA ? aHull : aCap;
+                fresh.points[k].anchorB = hullShape == shapeA ? aCap : aHull;
+                fresh.points[k].separation = local.points[k].separation;
+                fresh.points[k].id = local.points[k].id;
+            }
+        }
+    }
     else if (hullPair || capsulePair)
     {
-        // Capsule-hull segment SAT and the GJK families arrive in the
-        // distance module.
-        *out = fresh;
-        return M3_NARROW_UNSUPPORTED;
+        // Hull-sphere, capsule-sphere, capsule-capsule: GJK on the
+        // cores in A's frame, radii applied analytically, one point,
+        // feature id 0; exact answers for a deep core overlap
+        // (manifold.c:2664-2807).
+        int32_t bodyA = w.shapeBody[shapeA];
+        int32_t bodyB = w.shapeBody[shapeB];
+        m3Transform xfA = m3ShapeXf(w, shapeA);
+        m3Transform xfB = m3ShapeXf(w, shapeB);
+        m3Quat qIn = m3MulQuat(m3Conj(xfA.q), xfB.q);
+        m3Vec3 dp = v3((m3real)(xfB.p.x - xfA.p.x), (m3real)(xfB.p.y - xfA.p.y),
+                       (m3real)(xfB.p.z - xfA.p.z));
+        m3Vec3 pIn = m3InvRotateVec3(xfA.q, dp);
+        m3Vec3 pointsA[2];
+        m3Vec3 pointsB[2];
+        m3ProxyDev proxyA = m3MakeProxyDev(w, shapeA, pointsA);
+        m3ProxyDev proxyB = m3MakeProxyDev(w, shapeB, pointsB);
+        m3DistanceOutDev dout = m3ShapeDistanceDev(proxyA, proxyB, qIn, pIn);
+        m3real rA = proxyA.radius;
+        m3real rB = proxyB.radius;
+        m3real sep = dout.distance - rA - rB;
+        if (sep <= M3_SPECULATIVE_DISTANCE)
+        {
+            m3Vec3 nLocal;
+            m3Vec3 pALocal;
+            m3Vec3 pBLocal;
+            if (dout.distance > 0.0f)
+            {
+                nLocal = dout.normal;
+                pALocal = m3Add3(dout.pointA, m3MulSV3(rA, nLocal));
+                pBLocal = m3Sub3(dout.pointB, m3MulSV3(rB, nLocal));
+            }
+            else if (hullPair)
+            {
+                int hullIsA = typeA == M3_SHAPE_HULL;
+                const m3HullData* hull = &w.hulls[w.hullIndex[hullIsA ? shapeA : shapeB]];
+                const m3ProxyDev& round = hullIsA ? proxyB : proxyA;
+                m3Vec3 core = hullIsA ? m3Add3(m3RotateVec3(qIn, round.points[0]), pIn)
+                                      : m3InvRotateVec3(qIn, m3Sub3(round.points[0], pIn));
+                m3Vec3 nHull;
+                m3real coreSep;
+                m3Vec3 onHull;
+                m3DeepPointInHull(hull, core, &nHull, &coreSep, &onHull);
+                m3real rRound = round.radius;
+                sep = coreSep - rRound;
+                if (hullIsA)
+                {
+                    nLocal = nHull;
+                    pALocal = onHull;
+                    pBLocal = m3Sub3(core, m3MulSV3(rRound, nHull));
+                }
+                else
+                {
+                    m3Vec3 nA = m3RotateVec3(qIn, nHull);
+                    nLocal = m3Neg3(nA);
+                    pALocal = m3Sub3(m3Add3(m3RotateVec3(qIn, core), pIn), m3MulSV3(rRound, nA));
+                    pBLocal = m3Add3(m3RotateVec3(qIn, onHull), pIn);
+                }
+            }
+            else
+            {
+                m3Vec3 axis;
+                m3Vec3 cA;
+                m3Vec3 cB;
+                if (proxyA.count == 2 && proxyB.count == 2)
+                {
+                    m3Vec3 dirA = m3Sub3(pointsA[1], pointsA[0]);
+                    m3Vec3 dirB = m3RotateVec3(qIn, m3Sub3(pointsB[1], pointsB[0]));
+                    axis = m3Cross3(dirA, dirB);
+                    cA = m3MulSV3(0.5f, m3Add3(pointsA[0], pointsA[1]));
+                    cB = m3Add3(m3RotateVec3(qIn, m3MulSV3(0.5f, m3Add3(pointsB[0], pointsB[1]))),
+                                pIn);
+                    if (m3Dot3(axis, axis) < 1.0e-10f)
+                    {
+                        axis = m3Sub3(cB, cA);
+                    }
+                }
+                else
+                {
+                    m3Vec3 dir = proxyA.count == 2
+                                     ? m3Sub3(pointsA[1], pointsA[0])
+                                     : m3RotateVec3(qIn, m3Sub3(pointsB[1], pointsB[0]));
+                    m3Vec3 t1;
+                    m3Vec3 t2;
+                    m3MakeTangentBasis(m3Normalize3(dir), &t1, &t2);
+                    axis = t1;
+                    cA = proxyA.count == 1 ? pointsA[0]
+                                           : m3MulSV3(0.5f, m3Add3(pointsA[0], pointsA[1]));
+                    cB = proxyB.count == 1
+                             ? m3Add3(m3RotateVec3(qIn, pointsB[0]), pIn)
+                             : m3Add3(m3RotateVec3(qIn, m3MulSV3(0.5f, m3Add3(pointsB[0], pointsB[1]))),
+                                      pIn);
+                }
+                nLocal = m3Normalize3(axis);
+                if (m3Dot3(nLocal, m3Sub3(cB, cA)) < 0.0f)
+                {
+                    nLocal = m3Neg3(nLocal);
+                }
+                m3Vec3 mid = m3MulSV3(0.5f, m3Add3(cA, cB));
+                pALocal = mid;
+                pBLocal = mid;
+                sep = -(rA + rB);
+            }
+            fresh.normal = m3RotateVec3(xfA.q, nLocal);
+            m3Vec3 wA = m3RotateVec3(xfA.q, pALocal);
+            m3Vec3 wB = m3RotateVec3(xfA.q, pBLocal);
+            fresh.points[0].anchorA = m3FromCom(w, bodyA, xfA.p.x + (double)wA.x,
+                                                xfA.p.y + (double)wA.y, xfA.p.z + (double)wA.z);
+            fresh.points[0].anchorB = m3FromCom(w, bodyB, xfA.p.x + (double)wB.x,
+                                                xfA.p.y + (double)wB.y, xfA.p.z + (double)wB.z);
+            fresh.points[0].separation = sep;
+            fresh.points[0].id = 0;
+            fresh.pointCount = 1;
+        }
     }
     else if (planePair)
     {
