@@ -1,0 +1,459 @@
+"""Benchmark: bit-exact body-substeps/s of the batched device step.
+
+Workload (default): the batched uneven-worlds configuration -- 4096
+independent worlds per GPU, dynamic body counts log-uniform in
+[32, 2048], each world 8-high box stacks (half extent U[0.25, 0.75]),
+loose spheres and three revolute chains of 8 capsules (r 0.1,
+half-height 0.4) hung from static anchors; dt 1/60, 4 substeps.  The
+worlds are seeded synthetic scenes built through the library's
+reference-compatible creation API (maul3d_b200/csrc/scenes.c).
+
+One "step" = one m3World_Step of every world in the batch.  The metric
+counts alive dynamic bodies x substeps x steps over all worlds and all
+ranks, divided by the max-over-ranks device time of exactly K steps.
+
+Lines printed by rank 0 (one JSON object):
+  value     device-resident throughput (CUDA events around K steps);
+  e2e       the same metric through the C ABI from host-built worlds:
+            the H2D upload of every world image, K steps and a D2H read
+            of every world's hash after each step, inside the timed
+            region;
+  roofline  the dominant kernel's algorithmic bytes / its device time,
+            against the measured HBM copy bandwidth;
+  plain_gpu the one-world-per-launch path on a sample of the worlds;
+  cpu_baseline  the reference engine (oracle/_ref, built from its own
+            sources) on the host cores, stepping a bounded sample of the
+            same worlds for the same W+K steps, every sampled world's
+            hash checked against the device's.
+
+Multi-GPU: one process per GPU (torchrun), each rank its own 4096
+worlds (weak scaling), no collective on the data path; the only NCCL
+calls are the timing barrier and the max/sum reductions of the result.
+
+--impl reference runs the reference engine alone on the host cores
+(all threads) for the same metric and config.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "bit-exact body-substeps/s"
+UNIT = "body-substeps/s"
+DT = 1.0 / 60.0
+SCENE_UNEVEN = 2
+
+# Algorithmic bytes per unit of work (the reference's record layouts):
+# per moving body per substep, integrate velocities 141 B + integrate
+# positions 173 B; per contact row per substep 3 passes x (456 B record +
+# 2 x 48 B v,w + 2 x 28 B dp,dq); per joint row per substep 3 x (472 +
+# 152); per candidate pair per step 2 x 40 B transforms + 2 x 32 B geom
+# + 188 B new + 188 B old manifold.
+BYTES_PER_MOVER_SUBSTEP = 314
+BYTES_PER_CONTACT_SUBSTEP = 3 * (456 + 2 * 48 + 2 * 28)
+BYTES_PER_JOINT_SUBSTEP = 3 * (472 + 152)
+BYTES_PER_PAIR_STEP = 2 * 40 + 2 * 32 + 188 + 188
+
+
+def env_int(name: str, default: int) -> int:
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def world_sizes(lib, seed: int, count: int, lo: int, hi: int) -> list[int]:
+    return [int(lib.m3s_uneven_size(seed, i, lo, hi)) for i in range(count)]
+
+
+def measured_peaks() -> tuple[float, str]:
+    path = ROOT / "MEASURED_PEAKS.json"
+    try:
+        data = json.loads(path.read_text())
+        return float(data["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self) -> None:
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200", "-f", self.path],
+                stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        try:
+            for line in Path(self.path).read_text().splitlines():
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+            os.unlink(self.path)
+        except Exception:
+            return None
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def build_worlds(m3, sizes: list[int], seed: int):
+    return [m3.World.scene(SCENE_UNEVEN, seed + i, n) for i, n in enumerate(sizes)]
+
+
+def body_substeps(sizes: list[int], substeps: int, steps: int) -> int:
+    return sum(sizes) * substeps * steps
+
+
+# ---------------------------------------------------------------------------
+# Reference engine on the host cores (oracle/_ref).  Worlds live in waves
+# of at most 64 (the reference's world table); each wave steps on
+# `threads` host threads, one world per task.  Only m3World_Step calls
+# are timed.
+# ---------------------------------------------------------------------------
+def reference_run(sizes, seed, substeps, steps, threads, time_budget_s, want_hashes=False):
+    from oracle import ref
+    lib = ref.lib()
+    done_bs = 0
+    busy = 0.0
+    hashes = {}
+    index = 0
+    t_start = time.perf_counter()
+    while index < len(sizes):
+        wave = list(range(index, min(index + 64, len(sizes))))
+        index = wave[-1] + 1
+        worlds = [ref.RefWorld.scene(SCENE_UNEVEN, seed + i, sizes[i]) for i in wave]
+        queue = list(range(len(wave)))
+        lock = threading.Lock()
+
+        def worker():
+            while True:
+                with lock:
+                    if not queue:
+                        return
+                    k = queue.pop(0)
+                lib.m3o_step_trace(worlds[k].id, DT, substeps, steps, None)
+
+        t0 = time.perf_counter()
+        pool = [threading.Thread(target=worker) for _ in range(threads)]
+        for t in pool:
+            t.start()
+        for t in pool:
+            t.join()
+        busy += time.perf_counter() - t0
+        for k, i in enumerate(wave):
+            if want_hashes:
+                hashes[i] = worlds[k].hash()
+            worlds[k].destroy()
+        done_bs += body_substeps([sizes[i] for i in wave], substeps, steps)
+        if time.perf_counter() - t_start > time_budget_s:
+            break
+    return done_bs, busy, hashes, index
+
+
+def run_reference_arm(args) -> None:
+    rank = env_int("RANK", 0)
+    if rank != 0:
+        return
+    from oracle import ref
+    if not ref.build():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "reference engine library oracle/_ref not built"}))
+        return
+    lib = ref.lib()
+    threads = os.cpu_count() or 1
+    sizes = world_sizes(lib, args.seed, args.worlds, args.lo, args.hi)
+    # Each step: one m3World_Step of every world of a bounded sample of
+    # the batch (its first worlds, at most the reference's 64-world
+    # table), spread over all host threads; the sample worlds persist
+    # across steps like the device's.
+    sample = min(len(sizes), args.ref_sample, 64)
+    worlds = [ref.RefWorld.scene(SCENE_UNEVEN, args.seed + i, sizes[i]) for i in range(sample)]
+
+    def step_all() -> float:
+        queue = list(range(sample))
+        lock = threading.Lock()
+
+        def worker():
+            while True:
+                with lock:
+                    if not queue:
+                        return
+                    k = queue.pop(0)
+                lib.m3o_step_trace(worlds[k].id, DT, args.substeps, 1, None)
+
+        t0 = time.perf_counter()
+        pool = [threading.Thread(target=worker) for _ in range(threads)]
+        for t in pool:
+            t.start()
+        for t in pool:
+            t.join()
+        return time.perf_counter() - t0
+
+    for _ in range(args.warmup):
+        step_all()
+    total_s = sum(step_all() for _ in range(args.steps))
+    total_bs = body_substeps(sizes[:sample], args.substeps, args.steps)
+    for w in worlds:
+        w.destroy()
+    value = total_bs / total_s
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
+        "n_gpus": env_int("WORLD_SIZE", 1), "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * total_s / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": config_block(args, sample_worlds=sample),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"first {sample} of {args.worlds} worlds, one step each per "
+                                   f"timed step, {threads} host threads"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def config_block(args, **extra) -> dict:
+    cfg = {"workload": f"batched uneven worlds: {args.worlds} worlds per GPU, dynamic bodies "
+                       f"log-uniform [{args.lo}, {args.hi}], box stacks + spheres + 3 revolute "
+                       f"capsule chains, dt 1/60, {args.substeps} substeps",
+           "worlds_per_gpu": args.worlds, "substeps": args.substeps, "dt": DT, "seed": args.seed,
+           "l2": "inputs larger than L2 (world slabs total several GB)",
+           "parallelism": "one block per world; worlds sharded across ranks (weak scaling)"}
+    cfg.update(extra)
+    return cfg
+
+
+# ---------------------------------------------------------------------------
+# Device arm
+# ---------------------------------------------------------------------------
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--worlds", type=int, default=4096)
+    ap.add_argument("--lo", type=int, default=32)
+    ap.add_argument("--hi", type=int, default=2048)
+    ap.add_argument("--substeps", type=int, default=4)
+    ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--plain-sample", type=int, default=64)
+    ap.add_argument("--ref-sample", type=int, default=64)
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+    import maul3d_b200 as m3
+
+    rank = env_int("RANK", 0)
+    world_size = env_int("WORLD_SIZE", 1)
+    local_rank = env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local_rank)
+    m3.set_device(local_rank)
+    if world_size > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+
+    rank_seed = args.seed + 1_000_003 * rank
+    sizes = world_sizes(m3.lib, rank_seed, args.worlds, args.lo, args.hi)
+    worlds = build_worlds(m3, sizes, rank_seed)
+    m3.reserve_worlds(worlds)
+    m3.upload_worlds(worlds)
+
+    # Warm-up steps (untimed).
+    m3.step_worlds(worlds, DT, args.substeps, args.warmup)
+    stats0 = np.stack([m3.world_stats(w) for w in worlds])
+
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    if world_size > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    m3.step_worlds(worlds, DT, args.substeps, args.steps)
+    e1.record()
+    torch.cuda.synchronize()
+    if world_size > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    collide_ms, solve_ms = m3.kernel_ms()
+    launches = 2 * args.steps + 1
+    stats1 = np.stack([m3.world_stats(w) for w in worlds])
+    work = (stats1 - stats0).astype(np.float64).sum(axis=0)
+    device_hashes = m3.hash_worlds(worlds)
+
+    local_bs = body_substeps(sizes, args.substeps, args.steps)
+    if world_size > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+        b = torch.tensor([float(local_bs)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(b, op=dist.ReduceOp.SUM)
+        total_bs = float(b.item())
+    else:
+        ms_max = ms
+        total_bs = float(local_bs)
+    value = total_bs / (ms_max / 1000.0)
+
+    # Roofline of the dominant kernel: algorithmic bytes / device time.
+    solve_bytes = (BYTES_PER_MOVER_SUBSTEP * work[0] + BYTES_PER_CONTACT_SUBSTEP * work[1] +
+                   BYTES_PER_JOINT_SUBSTEP * work[2])
+    collide_bytes = BYTES_PER_PAIR_STEP * work[3]
+    peak, peak_kind = measured_peaks()
+    if solve_ms >= collide_ms:
+        kname, kbytes, kms = "m3SolveKernel", solve_bytes, solve_ms
+    else:
+        kname, kbytes, kms = "m3CollideKernel", collide_bytes, collide_ms
+    achieved = (kbytes / args.steps) / (kms / args.steps / 1000.0) / 1e9
+    roofline = {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak,
+                "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None,
+                "bytes_per_launch": kbytes / args.steps,
+                "launch_ms": kms / args.steps,
+                "share": {"m3CollideKernel": collide_ms / ms, "m3SolveKernel": solve_ms / ms}}
+
+    # Plain path: one world per launch sequence, a sample of the worlds.
+    plain = None
+    if rank == 0 and args.plain_sample > 0:
+        psizes = sizes[:args.plain_sample]
+        pworlds = build_worlds(m3, psizes, rank_seed)
+        m3.reserve_worlds(pworlds)
+        m3.upload_worlds(pworlds)
+        for w in pworlds:
+            w.step(DT, args.substeps, 1)
+        torch.cuda.synchronize()
+        p0 = torch.cuda.Event(enable_timing=True)
+        p1 = torch.cuda.Event(enable_timing=True)
+        p0.record()
+        for _ in range(args.steps):
+            for w in pworlds:
+                m3.step_worlds([w], DT, args.substeps, 1)
+        p1.record()
+        torch.cuda.synchronize()
+        pms = p0.elapsed_time(p1)
+        plain = {"value": body_substeps(psizes, args.substeps, args.steps) / (pms / 1000.0),
+                 "unit": UNIT, "sample_worlds": len(psizes),
+                 "note": "each world stepped by its own launch sequence"}
+        for w in pworlds:
+            w.destroy()
+
+    # End to end through the C ABI: fresh host-built worlds, their upload,
+    # K steps and a D2H hash read of every world after every step.
+    e2e = None
+    if not args.no_e2e:
+        eworlds = build_worlds(m3, sizes, rank_seed)
+        m3.reserve_worlds(eworlds)
+        h2d = sum(m3.image_bytes(w) for w in eworlds)
+        if world_size > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        m3.upload_worlds(eworlds)
+        for _ in range(args.steps):
+            m3.step_worlds(eworlds, DT, args.substeps, 1)
+            m3.hash_worlds(eworlds)
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+        if world_size > 1:
+            t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e = {"value": total_bs / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d // args.steps),
+               "d2h_bytes_per_step": 8 * len(eworlds),
+               "note": "world images uploaded once inside the timed region (pageable host "
+                       "memory); per step: batched step + device hash of every world read back"}
+        for w in eworlds:
+            w.destroy()
+
+    # CPU baseline: the reference engine on the host cores, same worlds,
+    # same W+K steps; every sampled world's final hash must equal the
+    # device's (the bit-exact check behind the metric's name).
+    cpu = None
+    verified = None
+    if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
+        from oracle import ref
+        if ref.build():
+            threads = os.cpu_count() or 1
+            bs, busy, hashes, n = reference_run(sizes, rank_seed, args.substeps,
+                                                args.warmup + args.steps, threads,
+                                                args.cpu_seconds, want_hashes=True)
+            mismatched = [i for i, h in hashes.items() if int(device_hashes[i]) != h]
+            verified = {"worlds_checked": len(hashes), "mismatches": len(mismatched)}
+            cpu = {"value": bs / busy, "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": f"first {n} of {len(sizes)} worlds (waves of <= 64), "
+                             f"{args.warmup + args.steps} steps each, {threads} host threads; "
+                             f"every sampled world's final hash compared with the device's"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64", "data": "synthetic",
+            "config": config_block(args, total_dynamic_bodies_per_gpu=int(sum(sizes))),
+            "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
+            "cpu_baseline": cpu, "plain_gpu": plain, "bit_exact_check": verified,
+            "clocks": clocks,
+        }
+        print(json.dumps(line))
+    if world_size > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

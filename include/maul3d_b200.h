@@ -271,6 +271,21 @@ M3GPU_API int32_t m3gpu_step_worlds(const m3WorldId* worlds, int32_t count, floa
  * world), written to out[i].  Same values as m3World_Hash. */
 M3GPU_API int32_t m3gpu_hash_worlds(const m3WorldId* worlds, int32_t count, uint64_t* out);
 
+/* Select the CUDA device this library uses in the calling process (one
+ * process per GPU).  Call before the first device operation. */
+M3GPU_API int32_t m3gpu_set_device(int32_t device);
+
+/* Allocate the HBM slabs of `count` worlds without copying anything, so
+ * a later upload or step times only the copies and the work. */
+M3GPU_API int32_t m3gpu_reserve_worlds(const m3WorldId* worlds, int32_t count);
+
+/* Copy the host images of `count` worlds to their HBM slabs (worlds
+ * whose device copy is already current are skipped). */
+M3GPU_API int32_t m3gpu_upload_worlds(const m3WorldId* worlds, int32_t count);
+
+/* Bytes one world's host image occupies (what an upload copies). */
+M3GPU_API int64_t m3gpu_world_image_bytes(m3WorldId world);
+
 /* Wait for all device work of the library to finish. */
 M3GPU_API int32_t m3gpu_synchronize(void);
 
@@ -279,6 +294,17 @@ M3GPU_API int32_t m3gpu_synchronize(void);
  * the last m3gpu_step_worlds call measured with CUDA events. */
 M3GPU_API int64_t m3gpu_launch_count(void);
 M3GPU_API float m3gpu_last_step_ms(void);
+
+/* Device time in milliseconds of the last m3gpu_step_worlds call, split
+ * by kernel: out[0] the collide kernel (bounds, pairs, narrowphase),
+ * out[1] the solve kernel (islands through sleep), summed over steps. */
+M3GPU_API int32_t m3gpu_kernel_ms(float* out);
+
+/* Work counters of one world accumulated over its device steps:
+ * out[0] mover-substeps, out[1] contact-row-substeps, out[2]
+ * joint-row-substeps, out[3] candidate pairs, out[4] steps, out[5] the
+ * body slot count.  `out` holds 6 values. */
+M3GPU_API int32_t m3gpu_world_stats(m3WorldId world, uint64_t* out);
 
 /* White-box readback for parity tests.  Each copies [0, maxIndex) (or
  * [0, pairCount)) records in the reference's byte layout and returns the

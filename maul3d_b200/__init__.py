@@ -58,6 +58,17 @@ def _load() -> C.CDLL:
         fn.restype = C.c_int32
     lib.m3gpu_copy_mass.argtypes = [m3WorldId] + [C.c_void_p] * 6 + [C.c_int32]
     lib.m3gpu_copy_mass.restype = C.c_int32
+    lib.m3gpu_set_device.argtypes = [C.c_int32]
+    lib.m3gpu_set_device.restype = C.c_int32
+    for name in ("m3gpu_reserve_worlds", "m3gpu_upload_worlds"):
+        getattr(lib, name).argtypes = [C.POINTER(m3WorldId), C.c_int32]
+        getattr(lib, name).restype = C.c_int32
+    lib.m3gpu_world_image_bytes.argtypes = [m3WorldId]
+    lib.m3gpu_world_image_bytes.restype = C.c_int64
+    lib.m3gpu_kernel_ms.argtypes = [C.POINTER(C.c_float)]
+    lib.m3gpu_kernel_ms.restype = C.c_int32
+    lib.m3gpu_world_stats.argtypes = [m3WorldId, C.POINTER(C.c_uint64)]
+    lib.m3gpu_world_stats.restype = C.c_int32
     return lib
 
 
@@ -162,3 +173,34 @@ def launch_count() -> int:
 
 def last_step_ms() -> float:
     return float(lib.m3gpu_last_step_ms())
+
+
+def set_device(device: int) -> None:
+    _check(lib.m3gpu_set_device(device))
+
+
+def reserve_worlds(worlds) -> None:
+    _check(lib.m3gpu_reserve_worlds(_ids(worlds), len(worlds)))
+
+
+def upload_worlds(worlds) -> None:
+    _check(lib.m3gpu_upload_worlds(_ids(worlds), len(worlds)))
+
+
+def image_bytes(world) -> int:
+    return int(lib.m3gpu_world_image_bytes(world.id))
+
+
+def kernel_ms() -> tuple[float, float]:
+    """(collide, solve) device milliseconds of the last batched step call."""
+    out = (C.c_float * 2)()
+    _check(lib.m3gpu_kernel_ms(out))
+    return float(out[0]), float(out[1])
+
+
+def world_stats(world) -> np.ndarray:
+    """Work counters: mover-substeps, contact-row-substeps, joint-row-substeps,
+    candidate pairs, steps, body slots."""
+    out = (C.c_uint64 * 6)()
+    _check(lib.m3gpu_world_stats(world.id, out))
+    return np.array(list(out), dtype=np.uint64)

@@ -226,3 +226,42 @@ extern "C" int32_t m3gpu_copy_joints(m3WorldId world, void* impulse, void* perp,
     memcpy(angular, w->hv.jangular, (size_t)n * sizeof(m3Vec3));
     return n;
 }
+
+extern "C" int32_t m3gpu_reserve_worlds(const m3WorldId* worlds, int32_t count)
+{
+    m3gpuClearError();
+    std::vector<m3HostWorld*> ws;
+    int32_t rc = Resolve(worlds, count, ws);
+    for (int32_t i = 0; rc == M3GPU_OK && i < count; ++i)
+    {
+        rc = m3gpuReserve(ws[(size_t)i]);
+    }
+    return rc;
+}
+
+extern "C" int32_t m3gpu_upload_worlds(const m3WorldId* worlds, int32_t count)
+{
+    m3gpuClearError();
+    std::vector<m3HostWorld*> ws;
+    int32_t rc = Resolve(worlds, count, ws);
+    for (int32_t i = 0; rc == M3GPU_OK && i < count; ++i)
+    {
+        m3HostWorld* w = ws[(size_t)i];
+        if (w->hostDirty || w->dslab == nullptr)
+        {
+            w->hv.sc->status = 0;
+            rc = m3gpuUpload(w);
+        }
+    }
+    return rc;
+}
+
+extern "C" int64_t m3gpu_world_image_bytes(m3WorldId world)
+{
+    m3HostWorld* w = m3gpuWorldFromId(world);
+    if (w == nullptr)
+    {
+        return -1;
+    }
+    return w->persistentBytes + (int64_t)w->hulls.size() * (int64_t)sizeof(m3HullData);
+}

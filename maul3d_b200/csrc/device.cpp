@@ -13,6 +13,25 @@
 #include <string.h>
 
 static int s_deviceState = 0; // 0 unknown, 1 ready, -1 absent
+static int s_device = 0;
+
+extern "C" int32_t m3gpu_set_device(int32_t device)
+{
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count)
+    {
+        cudaGetLastError();
+        return m3gpuSetError(M3GPU_ERR_INVALID, "device %d is not visible", device);
+    }
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess)
+    {
+        return m3gpuSetError(M3GPU_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
+    }
+    s_device = device;
+    s_deviceState = 1;
+    return M3GPU_OK;
+}
 
 int32_t m3gpuEnsureDevice(void)
 {
@@ -34,6 +53,7 @@ int32_t m3gpuEnsureDevice(void)
                              cudaGetErrorString(e));
     }
     s_deviceState = 1;
+    cudaSetDevice(s_device);
     return M3GPU_OK;
 }
 
@@ -58,6 +78,23 @@ static void BuildDeviceView(m3HostWorld* w)
     w->dv.hulls = w->dhulls;
     w->dv.scratch = w->dslab + w->persistentBytes;
     w->dv.scratchBytes = w->scratchBytes;
+}
+
+int32_t m3gpuReserve(m3HostWorld* w)
+{
+    int32_t rc = m3gpuEnsureDevice();
+    if (rc != M3GPU_OK || w->dslab != nullptr)
+    {
+        return rc;
+    }
+    w->scratchBytes = m3gpuScratchBytes(w->bodyCap, w->shapeCap, w->jointCap, w->pairCap);
+    w->dslabBytes = w->persistentBytes + w->scratchBytes;
+    rc = CudaCheck(cudaMalloc((void**)&w->dslab, (size_t)w->dslabBytes), "cudaMalloc(slab)");
+    if (rc != M3GPU_OK)
+    {
+        w->dslab = nullptr;
+    }
+    return rc;
 }
 
 int32_t m3gpuUpload(m3HostWorld* w)

@@ -55,6 +55,11 @@ typedef struct m3WorldScalars
     int32_t moverCount;
     int32_t jointConstraintCount;
     int32_t pad1;
+    // Work counters accumulated over every device step (observer only,
+    // never hashed): the algorithmic-byte model of the roofline reads
+    // them.  [0] movers x substeps, [1] contact rows x substeps,
+    // [2] joint rows x substeps, [3] candidate pairs, [4] steps.
+    uint64_t work[5];
 } m3WorldScalars;
 
 // Per-body persistent arrays (capacity = bodyCap).

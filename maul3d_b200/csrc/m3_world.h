@@ -7,6 +7,7 @@
 #include "m3_layout.h"
 
 #include <stdint.h>
+#include <unordered_map>
 #include <vector>
 
 struct m3HostWorld
@@ -28,6 +29,7 @@ struct m3HostWorld
     // the reference's snapshot treats them).
     std::vector<m3HullData> hulls;
     std::vector<int32_t> hullRefs;
+    std::unordered_multimap<uint64_t, int32_t> hullIndexByContent;
 
     // Device residency.
     uint8_t* dslab = nullptr;        // persistent + scratch
@@ -46,6 +48,7 @@ m3HostWorld* m3gpuWorldFromIndex0(uint16_t index0);
 
 // Residency (device.cpp).
 int32_t m3gpuEnsureDevice(void);
+int32_t m3gpuReserve(m3HostWorld* w);
 int32_t m3gpuUpload(m3HostWorld* w);
 int32_t m3gpuDownload(m3HostWorld* w);
 void m3gpuRelease(m3HostWorld* w);

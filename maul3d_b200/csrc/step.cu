@@ -1184,6 +1184,25 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
     {
         sc->moverCount = moverCount;
         sc->stepCount += 1;
+        sc->work[0] += (uint64_t)moverCount * (uint64_t)substeps;
+        sc->work[1] += (uint64_t)constraintCount * (uint64_t)substeps;
+        sc->work[2] += (uint64_t)jointCount * (uint64_t)substeps;
+        sc->work[3] += (uint64_t)pairCount;
+        sc->work[4] += 1;
+    }
+}
+
+// Largest status word over the batch (0 when every world stepped).
+__global__ void m3StatusKernel(const m3WorldView* views, int32_t count, int32_t* out)
+{
+    int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count)
+    {
+        int32_t st = views[i].sc->status;
+        if (st != 0)
+        {
+            atomicMax(out, st);
+        }
     }
 }
 
@@ -1343,6 +1362,40 @@ static int32_t PrepareBatch(m3HostWorld** worlds, int32_t count)
     return M3GPU_OK;
 }
 
+static float s_kernelMs[2] = {0.0f, 0.0f};
+static std::vector<cudaEvent_t> s_events;
+static int32_t* s_dstatus = nullptr;
+
+extern "C" int32_t m3gpu_kernel_ms(float* out)
+{
+    if (out == nullptr)
+    {
+        return m3gpuSetError(M3GPU_ERR_INVALID, "null output");
+    }
+    out[0] = s_kernelMs[0];
+    out[1] = s_kernelMs[1];
+    return M3GPU_OK;
+}
+
+extern "C" int32_t m3gpu_world_stats(m3WorldId world, uint64_t* out)
+{
+    m3HostWorld* w = m3gpuWorldFromId(world);
+    if (w == nullptr || out == nullptr)
+    {
+        return m3gpuSetError(M3GPU_ERR_INVALID, "stale world or null output");
+    }
+    if (m3gpuSyncHost(w) != M3GPU_OK)
+    {
+        return m3gpu_last_error();
+    }
+    for (int32_t k = 0; k < 5; ++k)
+    {
+        out[k] = w->hv.sc->work[k];
+    }
+    out[5] = (uint64_t)w->hv.sc->bodyMax;
+    return M3GPU_OK;
+}
+
 int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t substeps,
                        int32_t steps)
 {
@@ -1356,27 +1409,46 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
     {
         return rc;
     }
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaEventRecord(e0);
+    // One event before the batch and one after each kernel, so the two
+    // kernels' device times are separable.
+    size_t needEvents = (size_t)(2 * steps + 1);
+    while (s_events.size() < needEvents)
+    {
+        cudaEvent_t e;
+        rc = Check(cudaEventCreate(&e), "cudaEventCreate");
+        if (rc != M3GPU_OK)
+        {
+            return rc;
+        }
+        s_events.push_back(e);
+    }
+    if (s_dstatus == nullptr)
+    {
+        rc = Check(cudaMalloc((void**)&s_dstatus, sizeof(int32_t)), "cudaMalloc(status)");
+        if (rc != M3GPU_OK)
+        {
+            return rc;
+        }
+    }
+    cudaEventRecord(s_events[0]);
     for (int32_t step = 0; step < steps; ++step)
     {
         m3CollideKernel<<<count, M3_BLOCK>>>(s_batch.dviews, s_batch.dorder, count);
+        cudaEventRecord(s_events[(size_t)(2 * step + 1)]);
         m3SolveKernel<<<count, M3_BLOCK>>>(s_batch.dviews, s_batch.dorder, count, dt, substeps);
+        cudaEventRecord(s_events[(size_t)(2 * step + 2)]);
         s_launches += 2;
     }
-    cudaEventRecord(e1);
+    cudaMemsetAsync(s_dstatus, 0, sizeof(int32_t));
+    m3StatusKernel<<<(count + 255) / 256, 256>>>(s_batch.dviews, count, s_dstatus);
+    s_launches += 1;
     rc = Check(cudaGetLastError(), "step launch");
+    int32_t status = 0;
     if (rc == M3GPU_OK)
     {
-        rc = Check(cudaEventSynchronize(e1), "step");
+        rc = Check(cudaMemcpy(&status, s_dstatus, sizeof(int32_t), cudaMemcpyDeviceToHost),
+                   "step");
     }
-    float ms = 0.0f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    s_lastStepMs = ms;
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     for (int32_t i = 0; i < count; ++i)
     {
         worlds[i]->deviceAhead = true;
@@ -1385,19 +1457,39 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
     {
         return rc;
     }
-    // Surface device-side refusals.
-    for (int32_t i = 0; i < count; ++i)
+    float total = 0.0f;
+    float collide = 0.0f;
+    float solve = 0.0f;
+    cudaEventElapsedTime(&total, s_events[0], s_events[(size_t)(2 * steps)]);
+    for (int32_t step = 0; step < steps; ++step)
     {
-        int32_t status = 0;
-        int32_t detail = 0;
-        cudaMemcpy(&status, &worlds[i]->dv.sc->status, sizeof(int32_t), cudaMemcpyDeviceToHost);
-        if (status != 0)
+        float a = 0.0f;
+        float b = 0.0f;
+        cudaEventElapsedTime(&a, s_events[(size_t)(2 * step)], s_events[(size_t)(2 * step + 1)]);
+        cudaEventElapsedTime(&b, s_events[(size_t)(2 * step + 1)], s_events[(size_t)(2 * step + 2)]);
+        collide += a;
+        solve += b;
+    }
+    s_lastStepMs = total;
+    s_kernelMs[0] = collide;
+    s_kernelMs[1] = solve;
+    if (status != 0)
+    {
+        // Name the first refusing world and its detail code.
+        for (int32_t i = 0; i < count; ++i)
         {
-            cudaMemcpy(&detail, &worlds[i]->dv.sc->statusDetail, sizeof(int32_t),
-                       cudaMemcpyDeviceToHost);
-            return m3gpuSetError(status, "world %d stalled on the device (status %d, detail %d)",
-                                 worlds[i]->slot, status, detail);
+            int32_t st = 0;
+            int32_t detail = 0;
+            cudaMemcpy(&st, &worlds[i]->dv.sc->status, sizeof(int32_t), cudaMemcpyDeviceToHost);
+            if (st != 0)
+            {
+                cudaMemcpy(&detail, &worlds[i]->dv.sc->statusDetail, sizeof(int32_t),
+                           cudaMemcpyDeviceToHost);
+                return m3gpuSetError(st, "world %d stalled on the device (status %d, detail %d)",
+                                     worlds[i]->slot, st, detail);
+            }
         }
+        return m3gpuSetError(status, "a world stalled on the device (status %d)", status);
     }
     return M3GPU_OK;
 }

@@ -717,11 +717,16 @@ static void BuildBoxHull(m3HullData* out, m3Vec3 he)
 }
 
 // Content-deduplicated interning in ascending slot order (hull.c:132-152).
+// Live slabs are pairwise distinct, so the first match in slot order is
+// the only match; a content-hash index finds it without scanning.
 static int32_t InternHull(m3HostWorld* w, const m3HullData* data)
 {
     m3WorldScalars* sc = w->hv.sc;
-    for (int32_t i = 0; i < sc->hullMax; ++i)
+    uint64_t key = m3Fnv(M3_HASH_INIT, data, (int32_t)sizeof(m3HullData));
+    auto range = w->hullIndexByContent.equal_range(key);
+    for (auto it = range.first; it != range.second; ++it)
     {
+        int32_t i = it->second;
         if (w->hullRefs[i] > 0 && memcmp(&w->hulls[i], data, sizeof(m3HullData)) == 0)
         {
             w->hullRefs[i] += 1;
@@ -736,6 +741,7 @@ static int32_t InternHull(m3HostWorld* w, const m3HullData* data)
     sc->hullMax += 1;
     w->hulls.push_back(*data);
     w->hullRefs.push_back(1);
+    w->hullIndexByContent.emplace(key, index);
     return index;
 }
 
