@@ -15,6 +15,11 @@
 static int s_deviceState = 0; // 0 unknown, 1 ready, -1 absent
 static int s_device = 0;
 
+// Bumped whenever any world's device allocations change (slab or hull
+// pool allocated, released): cached device views of a batch are valid
+// only for the epoch they were built in.
+uint64_t g_m3ResidencyEpoch = 1;
+
 extern "C" int32_t m3gpu_set_device(int32_t device)
 {
     int count = 0;
@@ -94,6 +99,7 @@ int32_t m3gpuReserve(m3HostWorld* w)
     {
         w->dslab = nullptr;
     }
+    g_m3ResidencyEpoch += 1;
     return rc;
 }
 
@@ -109,6 +115,7 @@ int32_t m3gpuUpload(m3HostWorld* w)
         w->scratchBytes = m3gpuScratchBytes(w->bodyCap, w->shapeCap, w->jointCap, w->pairCap);
         w->dslabBytes = w->persistentBytes + w->scratchBytes;
         rc = CudaCheck(cudaMalloc((void**)&w->dslab, (size_t)w->dslabBytes), "cudaMalloc(slab)");
+        g_m3ResidencyEpoch += 1;
         if (rc != M3GPU_OK)
         {
             w->dslab = nullptr;
@@ -123,6 +130,7 @@ int32_t m3gpuUpload(m3HostWorld* w)
             cudaFree(w->dhulls);
             w->dhulls = nullptr;
         }
+        g_m3ResidencyEpoch += 1;
         int32_t cap = hullCount < 4 ? 4 : hullCount;
         rc = CudaCheck(cudaMalloc((void**)&w->dhulls, (size_t)cap * sizeof(m3HullData)),
                        "cudaMalloc(hulls)");
@@ -135,6 +143,7 @@ int32_t m3gpuUpload(m3HostWorld* w)
     }
     if (w->dhulls == nullptr)
     {
+        g_m3ResidencyEpoch += 1;
         rc = CudaCheck(cudaMalloc((void**)&w->dhulls, 4 * sizeof(m3HullData)), "cudaMalloc(hulls)");
         if (rc != M3GPU_OK)
         {
@@ -223,6 +232,7 @@ int32_t m3gpuSyncHost(m3HostWorld* w)
 
 void m3gpuRelease(m3HostWorld* w)
 {
+    g_m3ResidencyEpoch += 1;
     if (w->dslab != nullptr)
     {
         cudaFree(w->dslab);

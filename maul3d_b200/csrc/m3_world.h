@@ -47,6 +47,7 @@ m3HostWorld* m3gpuWorldFromId(m3WorldId id);
 m3HostWorld* m3gpuWorldFromIndex0(uint16_t index0);
 
 // Residency (device.cpp).
+extern uint64_t g_m3ResidencyEpoch;
 int32_t m3gpuEnsureDevice(void);
 int32_t m3gpuReserve(m3HostWorld* w);
 int32_t m3gpuUpload(m3HostWorld* w);

@@ -1249,7 +1249,7 @@ extern "C" int32_t m3gpu_synchronize(void)
 struct m3BatchCache
 {
     std::vector<m3HostWorld*> worlds;
-    std::vector<void*> slabs;
+    uint64_t epoch = 0;
     m3WorldView* dviews = nullptr;
     int32_t* dorder = nullptr;
     uint64_t* dhash = nullptr;
@@ -1281,25 +1281,15 @@ static int32_t PrepareBatch(m3HostWorld** worlds, int32_t count)
             }
         }
     }
-    bool same = (int32_t)s_batch.worlds.size() == count;
+    bool same = s_batch.dviews != nullptr && s_batch.epoch == g_m3ResidencyEpoch &&
+                (int32_t)s_batch.worlds.size() == count;
     for (int32_t i = 0; same && i < count; ++i)
     {
-        same = s_batch.worlds[(size_t)i] == worlds[i] &&
-               s_batch.slabs[(size_t)i] == (void*)worlds[i]->dslab &&
-               true;
+        same = s_batch.worlds[(size_t)i] == worlds[i];
     }
-    if (same && s_batch.dviews != nullptr)
+    if (same)
     {
-        // Hull pools may have been reallocated by an upload.
-        bool hullsSame = true;
-        for (int32_t i = 0; i < count && hullsSame; ++i)
-        {
-            hullsSame = worlds[i]->dv.hulls == worlds[i]->dhulls;
-        }
-        if (hullsSame)
-        {
-            return M3GPU_OK;
-        }
+        return M3GPU_OK;
     }
     if (count > s_batch.cap)
     {
@@ -1354,11 +1344,7 @@ static int32_t PrepareBatch(m3HostWorld** worlds, int32_t count)
         return rc;
     }
     s_batch.worlds.assign(worlds, worlds + count);
-    s_batch.slabs.resize((size_t)count);
-    for (int32_t i = 0; i < count; ++i)
-    {
-        s_batch.slabs[(size_t)i] = worlds[i]->dslab;
-    }
+    s_batch.epoch = g_m3ResidencyEpoch;
     return M3GPU_OK;
 }
 
