@@ -322,16 +322,17 @@ def main() -> None:
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    launches0 = m3.launch_count()
     e0.record()
     m3.step_worlds(worlds, DT, args.substeps, args.steps)
     e1.record()
+    launches = m3.launch_count() - launches0
     torch.cuda.synchronize()
     if world_size > 1:
         dist.barrier()
     clocks = sampler.stop()
     ms = e0.elapsed_time(e1)
     collide_ms, solve_ms = m3.kernel_ms()
-    launches = 2 * args.steps + 1
     stats1 = np.stack([m3.world_stats(w) for w in worlds])
     work = (stats1 - stats0).astype(np.float64).sum(axis=0)
     device_hashes = m3.hash_worlds(worlds)

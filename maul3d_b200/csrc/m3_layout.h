@@ -54,7 +54,7 @@ typedef struct m3WorldScalars
     int32_t constraintCount;
     int32_t moverCount;
     int32_t jointConstraintCount;
-    int32_t pad1;
+    int32_t newPairCount; // pair list the running step is building
     // Work counters accumulated over every device step (observer only,
     // never hashed): the algorithmic-byte model of the roofline reads
     // them.  [0] movers x substeps, [1] contact rows x substeps,

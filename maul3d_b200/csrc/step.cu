@@ -44,7 +44,11 @@ struct m3Aabb
 struct m3Scratch
 {
     m3Aabb* aabb;          // per shape
-    int32_t* shapeCount;   // per shape, then exclusive offsets
+    int32_t* rowCount;     // per shape: pair count, then row offsets
+    int32_t* rowFill;      // per shape: row fill cursor
+    int32_t* planeFlag;    // per shape: plane row scan
+    uint64_t* sortKey;     // sweep order keys (power-of-two padded)
+    int32_t* sortIdx;      // sweep order shape indices
     m3Pos3* com0;          // per body
     m3Quat* rot0;          // per body
     int32_t* parent;       // per body (island union-find)
@@ -64,6 +68,16 @@ struct m3Scratch
     m3JointDev* joints;    // per joint
 };
 
+static __host__ __device__ inline int64_t NextPow2(int64_t n)
+{
+    int64_t p = 1;
+    while (p < n)
+    {
+        p <<= 1;
+    }
+    return p;
+}
+
 static __host__ __device__ inline int64_t ScratchCarve(m3Scratch* s, uint8_t* base, int32_t bodyCap,
                                                      int32_t shapeCap, int32_t jointCap,
                                                      int32_t pairCap)
@@ -76,7 +90,11 @@ static __host__ __device__ inline int64_t ScratchCarve(m3Scratch* s, uint8_t* ba
     }                                                                                              \
     off = m3AlignUp(off + (int64_t)sizeof(T) * (int64_t)(n), M3_SLAB_ALIGN);
     M3_CARVE(aabb, m3Aabb, shapeCap)
-    M3_CARVE(shapeCount, int32_t, shapeCap + 1)
+    M3_CARVE(rowCount, int32_t, shapeCap + 1)
+    M3_CARVE(rowFill, int32_t, shapeCap + 1)
+    M3_CARVE(planeFlag, int32_t, shapeCap + 1)
+    M3_CARVE(sortKey, uint64_t, NextPow2(shapeCap))
+    M3_CARVE(sortIdx, int32_t, NextPow2(shapeCap))
     M3_CARVE(com0, m3Pos3, bodyCap)
     M3_CARVE(rot0, m3Quat, bodyCap)
     M3_CARVE(parent, int32_t, bodyCap)
@@ -264,40 +282,54 @@ __device__ bool PairAllowed(const m3WorldView& w, int32_t i, int32_t j)
     return true;
 }
 
-// The candidate rule of the reference's brute-force referee
-// (broad_phase.c:641-681): every allowed plane/non-plane pair, and every
-// allowed non-plane pair whose fresh bounds overlap.  The tree path
-// (broad_phase.c:430-639) is held equal to it by the reference's own
-// referee test; this evaluates the rule directly, row i emitting its
-// partners j > i in ascending order, so the list comes out sorted.
-__device__ __forceinline__ bool PairCandidate(const m3WorldView& w, const m3Scratch& s, int32_t i,
-                                              int32_t j)
+// ---------------------------------------------------------------------
+// Kernel 1: fresh bounds and the canonical pair list (one block per
+// world).  Sort-and-sweep on the x lower bound finds every overlapping
+// non-plane pair exactly once; plane pairs are enumerated directly.
+// Each pair lands in the row of its smaller shape index; rows are then
+// ordered by the larger index, which yields the reference's ascending
+// key order (broad_phase.c:632-637) without a global sort.
+// ---------------------------------------------------------------------
+
+// Total order on doubles as unsigned integers (negative values flipped).
+__device__ __forceinline__ uint64_t OrderKey(double x)
 {
-    if (w.shapeAlive[j] == 0)
-    {
-        return false;
-    }
-    uint8_t ti = w.shapeType[i];
-    uint8_t tj = w.shapeType[j];
-    if (ti == M3_SHAPE_PLANE || tj == M3_SHAPE_PLANE)
-    {
-        if (ti == tj)
-        {
-            return false;
-        }
-    }
-    else if (!Overlap(s.aabb[i], s.aabb[j]))
-    {
-        return false;
-    }
-    return PairAllowed(w, i, j);
+    uint64_t b = (uint64_t)__double_as_longlong(x);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
 }
 
-// ---------------------------------------------------------------------
-// Kernel 1: bounds, pairs, narrowphase
-// ---------------------------------------------------------------------
-__global__ void __launch_bounds__(M3_BLOCK) m3CollideKernel(const m3WorldView* views,
-                                                            const int32_t* order, int32_t count)
+#define M3_MAX_PLANES 16
+
+// Visit every non-plane pair (a < b) whose fresh bounds overlap and that
+// the filter allows, from the sweep position `p` of the sorted order.
+template <typename F>
+__device__ __forceinline__ void SweepFrom(const m3WorldView& w, const m3Scratch& s, int32_t p,
+                                          int32_t n, F&& visit)
+{
+    const int32_t a = s.sortIdx[p];
+    const m3Aabb boxA = s.aabb[a];
+    for (int32_t q = p + 1; q < n; ++q)
+    {
+        const int32_t b = s.sortIdx[q];
+        const m3Aabb& boxB = s.aabb[b];
+        if (!(boxB.lo[0] <= boxA.hi[0]))
+        {
+            break;
+        }
+        if (Overlap(boxA, boxB))
+        {
+            int32_t lo = a < b ? a : b;
+            int32_t hi = a < b ? b : a;
+            if (PairAllowed(w, lo, hi))
+            {
+                visit(lo, hi);
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(M3_BLOCK) m3BroadKernel(const m3WorldView* views,
+                                                          const int32_t* order, int32_t count)
 {
     const int32_t wi = order[blockIdx.x];
     const m3WorldView& w = views[wi];
@@ -306,9 +338,14 @@ __global__ void __launch_bounds__(M3_BLOCK) m3CollideKernel(const m3WorldView* v
     ScratchCarve(&s, w.scratch, sc->bodyCap, sc->shapeCap, sc->jointCap, sc->pairCap);
     const int32_t tid = threadIdx.x;
     __shared__ int32_t s_status;
+    __shared__ int32_t s_planes[M3_MAX_PLANES];
+    __shared__ int32_t s_planeCount;
+    __shared__ int32_t s_sweepCount;
     if (tid == 0)
     {
         s_status = sc->status;
+        s_planeCount = 0;
+        s_sweepCount = 0;
     }
     __syncthreads();
     if (s_status != 0)
@@ -317,31 +354,111 @@ __global__ void __launch_bounds__(M3_BLOCK) m3CollideKernel(const m3WorldView* v
     }
     const int32_t shapeMax = sc->shapeMax;
 
-    // Fresh bounds once per shape (the reference's per-step cache).
+    // Fresh bounds once per shape; the sweep set and the plane list.
     for (int32_t i = tid; i < shapeMax; i += M3_BLOCK)
     {
-        if (w.shapeAlive[i] != 0 && w.shapeType[i] != M3_SHAPE_PLANE)
+        s.rowCount[i] = 0;
+        s.rowFill[i] = 0;
+        if (w.shapeAlive[i] == 0)
         {
-            s.aabb[i] = ShapeBounds(w, i);
+            continue;
+        }
+        if (w.shapeType[i] == M3_SHAPE_PLANE)
+        {
+            int32_t k = atomicAdd(&s_planeCount, 1);
+            if (k < M3_MAX_PLANES)
+            {
+                s_planes[k] = i;
+            }
+            continue;
+        }
+        s.aabb[i] = ShapeBounds(w, i);
+        int32_t k = atomicAdd(&s_sweepCount, 1);
+        s.sortIdx[k] = i;
+    }
+    __syncthreads();
+    if (s_planeCount > M3_MAX_PLANES)
+    {
+        if (tid == 0)
+        {
+            sc->status = M3GPU_ERR_UNSUPPORTED;
+            sc->statusDetail = 5001;
+        }
+        return;
+    }
+    const int32_t n = s_sweepCount;
+    int32_t pow2 = 1;
+    while (pow2 < n)
+    {
+        pow2 <<= 1;
+    }
+    for (int32_t i = tid; i < pow2; i += M3_BLOCK)
+    {
+        if (i < n)
+        {
+            s.sortKey[i] = OrderKey(s.aabb[s.sortIdx[i]].lo[0]);
+        }
+        else
+        {
+            s.sortKey[i] = ~0ull;
+            s.sortIdx[i] = 0x7FFFFFFF;
         }
     }
     __syncthreads();
+    // Bitonic sort by (x lower bound, shape index).
+    for (int32_t k = 2; k <= pow2; k <<= 1)
+    {
+        for (int32_t j = k >> 1; j > 0; j >>= 1)
+        {
+            for (int32_t i = tid; i < pow2; i += M3_BLOCK)
+            {
+                int32_t ixj = i ^ j;
+                if (ixj > i)
+                {
+                    uint64_t ka = s.sortKey[i];
+                    uint64_t kb = s.sortKey[ixj];
+                    int32_t ia = s.sortIdx[i];
+                    int32_t ib = s.sortIdx[ixj];
+                    bool greater = ka > kb || (ka == kb && ia > ib);
+                    bool ascending = (i & k) == 0;
+                    if (greater == ascending)
+                    {
+                        s.sortKey[i] = kb;
+                        s.sortKey[ixj] = ka;
+                        s.sortIdx[i] = ib;
+                        s.sortIdx[ixj] = ia;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
 
-    // Count each row's partners.
+    // Count every row's pairs.
+    const int32_t planeCount = s_planeCount;
+    for (int32_t p = tid; p < n; p += M3_BLOCK)
+    {
+        SweepFrom(w, s, p, n, [&](int32_t lo, int32_t hi) { atomicAdd(&s.rowCount[lo], 1); });
+    }
     for (int32_t i = tid; i < shapeMax; i += M3_BLOCK)
     {
-        int32_t n = 0;
-        if (w.shapeAlive[i] != 0)
+        if (w.shapeAlive[i] == 0 || w.shapeType[i] == M3_SHAPE_PLANE)
         {
-            for (int32_t j = i + 1; j < shapeMax; ++j)
+            continue;
+        }
+        for (int32_t k = 0; k < planeCount; ++k)
+        {
+            int32_t pl = s_planes[k];
+            int32_t lo = pl < i ? pl : i;
+            int32_t hi = pl < i ? i : pl;
+            if (PairAllowed(w, lo, hi))
             {
-                n += PairCandidate(w, s, i, j) ? 1 : 0;
+                atomicAdd(&s.rowCount[lo], 1);
             }
         }
-        s.shapeCount[i] = n;
     }
     __syncthreads();
-    int32_t total = BlockExclusiveScan(s.shapeCount, shapeMax);
+    const int32_t total = BlockExclusiveScan(s.rowCount, shapeMax);
     if (total > sc->pairCap)
     {
         // The reference's m3UpdatePairs refuses with m3_errorCapacity
@@ -354,57 +471,173 @@ __global__ void __launch_bounds__(M3_BLOCK) m3CollideKernel(const m3WorldView* v
         return;
     }
     const int32_t cur = sc->pairBuf;
-    const uint64_t* oldKeys = cur == 0 ? w.keys0 : w.keys1;
-    const m3Manifold* oldMan = cur == 0 ? w.man0 : w.man1;
-    const int32_t oldCount = sc->pairCount;
     uint64_t* newKeys = cur == 0 ? w.keys1 : w.keys0;
-    m3Manifold* newMan = cur == 0 ? w.man1 : w.man0;
 
-    // Emit keys in canonical ascending order.
+    // Fill rows: sweep pairs through per-row cursors, then each plane's
+    // own row in ascending partner order by a scan.
+    for (int32_t p = tid; p < n; p += M3_BLOCK)
+    {
+        SweepFrom(w, s, p, n, [&](int32_t lo, int32_t hi) {
+            int32_t slot = atomicAdd(&s.rowFill[lo], 1);
+            newKeys[s.rowCount[lo] + slot] = ((uint64_t)(uint32_t)lo << 32) | (uint64_t)(uint32_t)hi;
+        });
+    }
     for (int32_t i = tid; i < shapeMax; i += M3_BLOCK)
     {
-        if (w.shapeAlive[i] == 0)
+        if (w.shapeAlive[i] == 0 || w.shapeType[i] == M3_SHAPE_PLANE)
         {
             continue;
         }
-        int32_t o = s.shapeCount[i];
-        for (int32_t j = i + 1; j < shapeMax; ++j)
+        for (int32_t k = 0; k < planeCount; ++k)
         {
-            if (PairCandidate(w, s, i, j))
+            int32_t pl = s_planes[k];
+            if (pl < i || !PairAllowed(w, i, pl))
             {
-                newKeys[o++] = ((uint64_t)(uint32_t)i << 32) | (uint64_t)(uint32_t)j;
+                continue;
+            }
+            int32_t slot = atomicAdd(&s.rowFill[i], 1);
+            newKeys[s.rowCount[i] + slot] = ((uint64_t)(uint32_t)i << 32) | (uint64_t)(uint32_t)pl;
+        }
+    }
+    for (int32_t k = 0; k < planeCount; ++k)
+    {
+        const int32_t pl = s_planes[k];
+        __syncthreads();
+        for (int32_t i = tid; i < shapeMax; i += M3_BLOCK)
+        {
+            s.planeFlag[i] = (i > pl && w.shapeAlive[i] != 0 && w.shapeType[i] != M3_SHAPE_PLANE &&
+                              PairAllowed(w, pl, i))
+                                 ? 1
+                                 : 0;
+        }
+        __syncthreads();
+        BlockExclusiveScan(s.planeFlag, shapeMax);
+        const int32_t base = s.rowCount[pl];
+        for (int32_t i = tid; i < shapeMax; i += M3_BLOCK)
+        {
+            int32_t next = i + 1 < shapeMax ? s.planeFlag[i + 1] : -1;
+            bool flagged = i + 1 < shapeMax ? next != s.planeFlag[i]
+                                            : (i > pl && w.shapeAlive[i] != 0 &&
+                                               w.shapeType[i] != M3_SHAPE_PLANE &&
+                                               PairAllowed(w, pl, i));
+            if (flagged)
+            {
+                newKeys[base + s.planeFlag[i]] =
+                    ((uint64_t)(uint32_t)pl << 32) | (uint64_t)(uint32_t)i;
             }
         }
     }
     __syncthreads();
-
-    // Narrowphase and warm-start carry, one pair per thread.
-    for (int32_t k = tid; k < total; k += M3_BLOCK)
+    // Order each non-plane row by partner index (rows are short).
+    for (int32_t i = tid; i < shapeMax; i += M3_BLOCK)
     {
-        uint64_t key = newKeys[k];
+        if (w.shapeAlive[i] == 0 || w.shapeType[i] == M3_SHAPE_PLANE)
+        {
+            continue;
+        }
+        const int32_t a = s.rowCount[i];
+        const int32_t c = s.rowFill[i];
+        for (int32_t x = a + 1; x < a + c; ++x)
+        {
+            uint64_t key = newKeys[x];
+            int32_t y = x - 1;
+            while (y >= a && newKeys[y] > key)
+            {
+                newKeys[y + 1] = newKeys[y];
+                y -= 1;
+            }
+            newKeys[y + 1] = key;
+        }
+    }
+    if (tid == 0)
+    {
+        sc->newPairCount = total;
+    }
+}
+
+// Exclusive offsets of every world's new pair count, in batch order
+// (one block; the narrowphase grid strides over the flattened pairs).
+__global__ void m3PairOffsetsKernel(const m3WorldView* views, int32_t count, int32_t* offsets)
+{
+    __shared__ int32_t partial[M3_BLOCK];
+    const int32_t t = threadIdx.x;
+    const int32_t chunk = (count + M3_BLOCK - 1) / M3_BLOCK;
+    const int32_t lo = t * chunk < count ? t * chunk : count;
+    const int32_t hi = lo + chunk < count ? lo + chunk : count;
+    int32_t sum = 0;
+    for (int32_t i = lo; i < hi; ++i)
+    {
+        const m3WorldScalars* sc = views[i].sc;
+        sum += sc->status == 0 ? sc->newPairCount : 0;
+    }
+    partial[t] = sum;
+    __syncthreads();
+    if (t == 0)
+    {
+        int32_t run = 0;
+        for (int32_t k = 0; k < M3_BLOCK; ++k)
+        {
+            int32_t x = partial[k];
+            partial[k] = run;
+            run += x;
+        }
+        offsets[count] = run;
+    }
+    __syncthreads();
+    int32_t run = partial[t];
+    for (int32_t i = lo; i < hi; ++i)
+    {
+        offsets[i] = run;
+        const m3WorldScalars* sc = views[i].sc;
+        run += sc->status == 0 ? sc->newPairCount : 0;
+    }
+}
+
+// ---------------------------------------------------------------------
+// Kernel 2: the narrowphase and warm-start carry over the flattened
+// pairs of every world of the batch, one thread per pair.
+// ---------------------------------------------------------------------
+__global__ void __launch_bounds__(128) m3NarrowKernel(const m3WorldView* views,
+                                                      const int32_t* offsets, int32_t count)
+{
+    const int32_t total = offsets[count];
+    for (int32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total;
+         g += gridDim.x * blockDim.x)
+    {
+        // The world owning flattened pair g: last offset <= g.
+        int32_t lo = 0;
+        int32_t hi = count - 1;
+        while (lo < hi)
+        {
+            int32_t mid = (lo + hi + 1) >> 1;
+            if (offsets[mid] <= g)
+            {
+                lo = mid;
+            }
+            else
+            {
+                hi = mid - 1;
+            }
+        }
+        const m3WorldView& w = views[lo];
+        m3WorldScalars* sc = w.sc;
+        const int32_t k = g - offsets[lo];
+        const int32_t cur = sc->pairBuf;
+        const uint64_t* oldKeys = cur == 0 ? w.keys0 : w.keys1;
+        const m3Manifold* oldMan = cur == 0 ? w.man0 : w.man1;
+        const uint64_t* newKeys = cur == 0 ? w.keys1 : w.keys0;
+        m3Manifold* newMan = cur == 0 ? w.man1 : w.man0;
+        const uint64_t key = newKeys[k];
         m3Manifold fresh;
         int32_t st = m3CollidePair(w, key, &fresh);
         if (st != M3_NARROW_OK)
         {
-            s_status = M3GPU_ERR_UNSUPPORTED;
+            atomicMax(&sc->status, M3GPU_ERR_UNSUPPORTED);
             sc->statusDetail = 1000 + (int32_t)w.shapeType[(int32_t)(key >> 32)] * 10 +
                                (int32_t)w.shapeType[(int32_t)(key & 0xFFFFFFFFu)];
         }
-        m3WarmCarry(&fresh, key, oldKeys, oldMan, oldCount);
+        m3WarmCarry(&fresh, key, oldKeys, oldMan, sc->pairCount);
         newMan[k] = fresh;
-    }
-    __syncthreads();
-    if (tid == 0)
-    {
-        if (s_status != 0)
-        {
-            sc->status = s_status;
-        }
-        else
-        {
-            sc->pairBuf = 1 - cur;
-            sc->pairCount = total;
-        }
     }
 }
 
@@ -605,6 +838,13 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
     {
         s_status = sc->status;
         s_anyRestitution = 0;
+        if (s_status == 0)
+        {
+            // The pair list and manifolds built by the collide kernels
+            // become the current ones.
+            sc->pairBuf = 1 - sc->pairBuf;
+            sc->pairCount = sc->newPairCount;
+        }
     }
     __syncthreads();
     if (s_status != 0)
@@ -1252,6 +1492,7 @@ struct m3BatchCache
     uint64_t epoch = 0;
     m3WorldView* dviews = nullptr;
     int32_t* dorder = nullptr;
+    int32_t* doffsets = nullptr;
     uint64_t* dhash = nullptr;
     int32_t cap = 0;
 };
@@ -1296,6 +1537,8 @@ static int32_t PrepareBatch(m3HostWorld** worlds, int32_t count)
         cudaFree(s_batch.dviews);
         cudaFree(s_batch.dorder);
         cudaFree(s_batch.dhash);
+        cudaFree(s_batch.doffsets);
+        s_batch.doffsets = nullptr;
         s_batch.dviews = nullptr;
         s_batch.dorder = nullptr;
         s_batch.dhash = nullptr;
@@ -1310,6 +1553,11 @@ static int32_t PrepareBatch(m3HostWorld** worlds, int32_t count)
         {
             rc = Check(cudaMalloc((void**)&s_batch.dhash, sizeof(uint64_t) * (size_t)count),
                        "cudaMalloc(hash)");
+        }
+        if (rc == M3GPU_OK)
+        {
+            rc = Check(cudaMalloc((void**)&s_batch.doffsets, sizeof(int32_t) * (size_t)(count + 1)),
+                       "cudaMalloc(offsets)");
         }
         if (rc != M3GPU_OK)
         {
@@ -1349,6 +1597,9 @@ static int32_t PrepareBatch(m3HostWorld** worlds, int32_t count)
 }
 
 static float s_kernelMs[2] = {0.0f, 0.0f};
+// Narrowphase grid: enough 128-thread blocks to fill every SM several
+// times; the kernel strides over the batch's flattened pairs.
+static int32_t s_narrowGrid = 148 * 16;
 static std::vector<cudaEvent_t> s_events;
 static int32_t* s_dstatus = nullptr;
 
@@ -1419,11 +1670,13 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
     cudaEventRecord(s_events[0]);
     for (int32_t step = 0; step < steps; ++step)
     {
-        m3CollideKernel<<<count, M3_BLOCK>>>(s_batch.dviews, s_batch.dorder, count);
+        m3BroadKernel<<<count, M3_BLOCK>>>(s_batch.dviews, s_batch.dorder, count);
+        m3PairOffsetsKernel<<<1, M3_BLOCK>>>(s_batch.dviews, count, s_batch.doffsets);
+        m3NarrowKernel<<<s_narrowGrid, 128>>>(s_batch.dviews, s_batch.doffsets, count);
         cudaEventRecord(s_events[(size_t)(2 * step + 1)]);
         m3SolveKernel<<<count, M3_BLOCK>>>(s_batch.dviews, s_batch.dorder, count, dt, substeps);
         cudaEventRecord(s_events[(size_t)(2 * step + 2)]);
-        s_launches += 2;
+        s_launches += 4;
     }
     cudaMemsetAsync(s_dstatus, 0, sizeof(int32_t));
     m3StatusKernel<<<(count + 255) / 256, 256>>>(s_batch.dviews, count, s_dstatus);
