@@ -306,6 +306,14 @@ M3GPU_API int32_t m3gpu_kernel_ms(float* out);
  * body slot count.  `out` holds 6 values. */
 M3GPU_API int32_t m3gpu_world_stats(m3WorldId world, uint64_t* out);
 
+/* Device clock cycles one world's block spent in each step phase,
+ * accumulated over its device steps (the device counterpart of the
+ * reference's per-phase step profile, world.h:578-593).  `out` holds 16
+ * values: islands, prepare, colour+movers, integrate velocities, warm
+ * start, bias solve, integrate positions, relax, store, continuous,
+ * sleep, bounds, sweep sort, pair count, pair fill, unused. */
+M3GPU_API int32_t m3gpu_world_phase_cycles(m3WorldId world, uint64_t* out);
+
 /* White-box readback for parity tests.  Each copies [0, maxIndex) (or
  * [0, pairCount)) records in the reference's byte layout and returns the
  * record count, or -1 when `cap` is too small or the id is stale. */

@@ -69,6 +69,8 @@ def _load() -> C.CDLL:
     lib.m3gpu_kernel_ms.restype = C.c_int32
     lib.m3gpu_world_stats.argtypes = [m3WorldId, C.POINTER(C.c_uint64)]
     lib.m3gpu_world_stats.restype = C.c_int32
+    lib.m3gpu_world_phase_cycles.argtypes = [m3WorldId, C.POINTER(C.c_uint64)]
+    lib.m3gpu_world_phase_cycles.restype = C.c_int32
     return lib
 
 
@@ -196,6 +198,18 @@ def kernel_ms() -> tuple[float, float]:
     out = (C.c_float * 2)()
     _check(lib.m3gpu_kernel_ms(out))
     return float(out[0]), float(out[1])
+
+
+PHASES = ("islands", "prepare", "colour+movers", "integrate_v", "warm_start", "bias_solve",
+          "integrate_p", "relax", "store", "continuous", "sleep", "bounds", "sweep_sort",
+          "pair_count", "pair_fill")
+
+
+def world_phase_cycles(world) -> np.ndarray:
+    """Device clock cycles the world's block spent per step phase (PHASES)."""
+    out = (C.c_uint64 * 16)()
+    _check(lib.m3gpu_world_phase_cycles(world.id, out))
+    return np.array(list(out), dtype=np.uint64)
 
 
 def world_stats(world) -> np.ndarray:

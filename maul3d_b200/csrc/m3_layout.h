@@ -60,6 +60,10 @@ typedef struct m3WorldScalars
     // them.  [0] movers x substeps, [1] contact rows x substeps,
     // [2] joint rows x substeps, [3] candidate pairs, [4] steps.
     uint64_t work[5];
+    // Device clock cycles spent per step phase by the world's block,
+    // accumulated over steps (observer only, never hashed; the index
+    // list is M3_PHASE_* in step.cu).
+    uint64_t phase[16];
 } m3WorldScalars;
 
 // Per-body persistent arrays (capacity = bodyCap).

@@ -32,6 +32,35 @@
 
 #define M3_BLOCK 256
 
+// Step phases timed with the SM clock by thread 0 of each world's block
+// right after the barrier that closes the phase.
+enum
+{
+    M3_PHASE_ISLANDS = 0,
+    M3_PHASE_PREPARE = 1,
+    M3_PHASE_COLOR = 2,
+    M3_PHASE_INTEGRATE_V = 3,
+    M3_PHASE_WARM = 4,
+    M3_PHASE_SOLVE = 5,
+    M3_PHASE_INTEGRATE_P = 6,
+    M3_PHASE_RELAX = 7,
+    M3_PHASE_STORE = 8,
+    M3_PHASE_CONTINUOUS = 9,
+    M3_PHASE_SLEEP = 10,
+    M3_PHASE_BOUNDS = 11,
+    M3_PHASE_SORT = 12,
+    M3_PHASE_COUNT = 13,
+    M3_PHASE_FILL = 14,
+};
+
+#define M3_PHASE_MARK(k)                                                                           \
+    if (threadIdx.x == 0)                                                                          \
+    {                                                                                              \
+        long long now_ = clock64();                                                                \
+        sc->phase[k] += (uint64_t)(now_ - t_phase);                                                \
+        t_phase = now_;                                                                            \
+    }
+
 // ---------------------------------------------------------------------
 // Scratch layout (device only)
 // ---------------------------------------------------------------------
@@ -352,6 +381,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3BroadKernel(const m3WorldView* vie
     {
         return;
     }
+    long long t_phase = clock64();
     const int32_t shapeMax = sc->shapeMax;
 
     // Fresh bounds once per shape; the sweep set and the plane list.
@@ -386,6 +416,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3BroadKernel(const m3WorldView* vie
         }
         return;
     }
+    M3_PHASE_MARK(M3_PHASE_BOUNDS)
     const int32_t n = s_sweepCount;
     int32_t pow2 = 1;
     while (pow2 < n)
@@ -434,6 +465,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3BroadKernel(const m3WorldView* vie
         }
     }
 
+    M3_PHASE_MARK(M3_PHASE_SORT)
     // Count every row's pairs.
     const int32_t planeCount = s_planeCount;
     for (int32_t p = tid; p < n; p += M3_BLOCK)
@@ -473,6 +505,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3BroadKernel(const m3WorldView* vie
     const int32_t cur = sc->pairBuf;
     uint64_t* newKeys = cur == 0 ? w.keys1 : w.keys0;
 
+    M3_PHASE_MARK(M3_PHASE_COUNT)
     // Fill rows: sweep pairs through per-row cursors, then each plane's
     // own row in ascending partner order by a scan.
     for (int32_t p = tid; p < n; p += M3_BLOCK)
@@ -549,6 +582,8 @@ __global__ void __launch_bounds__(M3_BLOCK) m3BroadKernel(const m3WorldView* vie
             newKeys[y + 1] = key;
         }
     }
+    __syncthreads();
+    M3_PHASE_MARK(M3_PHASE_FILL)
     if (tid == 0)
     {
         sc->newPairCount = total;
@@ -821,9 +856,14 @@ __device__ void ContinuousVersusPlane(const m3WorldView& w, int32_t body, int32_
 // ---------------------------------------------------------------------
 // Kernel 2: islands, prepare, colour, substeps, store, continuous, sleep
 // ---------------------------------------------------------------------
+// Shared-memory bytes per body of the substep-loop cache: v, w, the
+// position delta (12 B each) and the rotation delta (16 B).
+#define M3_BODY_CACHE_BYTES 52
+
 __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* views,
                                                           const int32_t* order, int32_t count,
-                                                          float dt, int32_t substeps)
+                                                          float dt, int32_t substeps,
+                                                          int32_t cacheBytes)
 {
     const int32_t wi = order[blockIdx.x];
     const m3WorldView& w = views[wi];
@@ -851,6 +891,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
     {
         return;
     }
+    long long t_phase = clock64();
     const int32_t bodyMax = sc->bodyMax;
     const int32_t shapeMax = sc->shapeMax;
     const int32_t jointMax = sc->jointMax;
@@ -935,6 +976,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
     }
     __syncthreads();
 
+    M3_PHASE_MARK(M3_PHASE_ISLANDS)
     // Contact selection and preparation (solver.c:156-405).
     const m3real h = dt / (m3real)substeps;
     const m3real invH = h > 0.0f ? 1.0f / h : 0.0f;
@@ -995,6 +1037,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
         return;
     }
 
+    M3_PHASE_MARK(M3_PHASE_PREPARE)
     // Greedy 16-colour first-free-bit colouring in constraint order, the
     // overflow bucket last (solver.c:2750-2810).
     if (tid == 0)
@@ -1101,9 +1144,39 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
         }
     }
     __syncthreads();
+    M3_PHASE_MARK(M3_PHASE_COLOR)
     const int32_t jointCount = sc->jointConstraintCount;
     const m3real pushMax = sc->contactPushMaxSpeed;
 
+    // Body velocities and the substep deltas live in shared memory for
+    // the whole substep loop when the world fits: every solve row then
+    // reads and writes its two bodies at shared-memory latency.  One
+    // copy in here, one copy out after restitution; the arithmetic is
+    // unchanged.
+    extern __shared__ __align__(16) uint8_t s_bodyCache[];
+    m3WorldView wl = w;
+    m3Vec3* dP = s.deltaPos;
+    m3Quat* dQ = s.deltaRot;
+    const bool cached = (int64_t)bodyMax * M3_BODY_CACHE_BYTES <= (int64_t)cacheBytes;
+    if (cached)
+    {
+        m3Quat* cq = (m3Quat*)s_bodyCache;
+        m3Vec3* cv = (m3Vec3*)(cq + bodyMax);
+        m3Vec3* cw = cv + bodyMax;
+        m3Vec3* cp = cw + bodyMax;
+        for (int32_t i = tid; i < bodyMax; i += M3_BLOCK)
+        {
+            cv[i] = w.v[i];
+            cw[i] = w.w[i];
+            cp[i] = v3(0.0f, 0.0f, 0.0f);
+            cq[i] = m3IdentityQuat();
+        }
+        wl.v = cv;
+        wl.w = cw;
+        dP = cp;
+        dQ = cq;
+    }
+    __syncthreads();
     // The substep loop (solver.c:4085-4203).
     for (int32_t sub = 0; sub < substeps; ++sub)
     {
@@ -1112,13 +1185,14 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
             int32_t i = s.movers[m];
             if (w.btype[i] == M3_BODY_DYNAMIC)
             {
-                m3IntegrateVelocity(w, i, h);
+                m3IntegrateVelocity(wl, i, h);
             }
         }
         __syncthreads();
+        M3_PHASE_MARK(M3_PHASE_INTEGRATE_V)
         if (tid == 0 && jointCount > 0)
         {
-            m3WarmStartJoints(w, s.joints, jointCount, s.deltaRot);
+            m3WarmStartJoints(wl, s.joints, jointCount, dQ);
         }
         __syncthreads();
         // Warm start, colour by colour; the overflow bucket serially.
@@ -1132,7 +1206,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
             }
             for (int32_t k = a + tid; k < b; k += M3_BLOCK)
             {
-                m3WarmStartContact(w, &s.cons[s.lists[k]]);
+                m3WarmStartContact(wl, &s.cons[s.lists[k]]);
             }
             __syncthreads();
         }
@@ -1140,14 +1214,15 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
         {
             for (int32_t k = s_starts[M3_GRAPH_COLORS]; k < s_starts[M3_GRAPH_COLORS + 1]; ++k)
             {
-                m3WarmStartContact(w, &s.cons[s.lists[k]]);
+                m3WarmStartContact(wl, &s.cons[s.lists[k]]);
             }
             if (jointCount > 0)
             {
-                m3SolveJoints(w, s.joints, jointCount, s.deltaPos, s.deltaRot, h, invH, true);
+                m3SolveJoints(wl, s.joints, jointCount, dP, dQ, h, invH, true);
             }
         }
         __syncthreads();
+        M3_PHASE_MARK(M3_PHASE_WARM)
         for (int32_t color = 0; color < M3_GRAPH_COLORS; ++color)
         {
             int32_t a = s_starts[color];
@@ -1158,7 +1233,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
             }
             for (int32_t k = a + tid; k < b; k += M3_BLOCK)
             {
-                m3SolveContact(w, &s.cons[s.lists[k]], s.deltaPos, s.deltaRot, invH, pushMax, true);
+                m3SolveContact(wl, &s.cons[s.lists[k]], dP, dQ, invH, pushMax, true);
             }
             __syncthreads();
         }
@@ -1166,18 +1241,20 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
         {
             for (int32_t k = s_starts[M3_GRAPH_COLORS]; k < s_starts[M3_GRAPH_COLORS + 1]; ++k)
             {
-                m3SolveContact(w, &s.cons[s.lists[k]], s.deltaPos, s.deltaRot, invH, pushMax, true);
+                m3SolveContact(wl, &s.cons[s.lists[k]], dP, dQ, invH, pushMax, true);
             }
         }
         __syncthreads();
+        M3_PHASE_MARK(M3_PHASE_SOLVE)
         for (int32_t m = tid; m < moverCount; m += M3_BLOCK)
         {
-            m3IntegratePosition(w, s.movers[m], h, s.deltaPos, s.deltaRot);
+            m3IntegratePosition(wl, s.movers[m], h, dP, dQ);
         }
         __syncthreads();
+        M3_PHASE_MARK(M3_PHASE_INTEGRATE_P)
         if (tid == 0 && jointCount > 0)
         {
-            m3SolveJoints(w, s.joints, jointCount, s.deltaPos, s.deltaRot, h, invH, false);
+            m3SolveJoints(wl, s.joints, jointCount, dP, dQ, h, invH, false);
         }
         __syncthreads();
         for (int32_t color = 0; color < M3_GRAPH_COLORS; ++color)
@@ -1190,7 +1267,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
             }
             for (int32_t k = a + tid; k < b; k += M3_BLOCK)
             {
-                m3SolveContact(w, &s.cons[s.lists[k]], s.deltaPos, s.deltaRot, invH, pushMax,
+                m3SolveContact(wl, &s.cons[s.lists[k]], dP, dQ, invH, pushMax,
                                false);
             }
             __syncthreads();
@@ -1199,11 +1276,12 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
         {
             for (int32_t k = s_starts[M3_GRAPH_COLORS]; k < s_starts[M3_GRAPH_COLORS + 1]; ++k)
             {
-                m3SolveContact(w, &s.cons[s.lists[k]], s.deltaPos, s.deltaRot, invH, pushMax,
+                m3SolveContact(wl, &s.cons[s.lists[k]], dP, dQ, invH, pushMax,
                                false);
             }
         }
         __syncthreads();
+        M3_PHASE_MARK(M3_PHASE_RELAX)
     }
 
     // Forces live one step (solver.c:4207-4211).
@@ -1219,7 +1297,16 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
         const m3real threshold = sc->restitutionThreshold;
         for (int32_t i = 0; i < constraintCount; ++i)
         {
-            m3RestituteContact(w, &s.cons[i], threshold);
+            m3RestituteContact(wl, &s.cons[i], threshold);
+        }
+    }
+    __syncthreads();
+    if (cached)
+    {
+        for (int32_t i = tid; i < bodyMax; i += M3_BLOCK)
+        {
+            w.v[i] = wl.v[i];
+            w.w[i] = wl.w[i];
         }
     }
     __syncthreads();
@@ -1244,6 +1331,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
     }
     __syncthreads();
 
+    M3_PHASE_MARK(M3_PHASE_STORE)
     // Continuous phase (solver.c:3349-3425).  A non-bullet fast body
     // sweeps only against static targets, and a pull-back moves only the
     // fast body itself, so bodies are independent and run in parallel.
@@ -1354,6 +1442,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
         }
     }
 
+    M3_PHASE_MARK(M3_PHASE_CONTINUOUS)
     // Sleep pass (solver.c:3582-3660).
     if (sc->sleepEnabled != 0)
     {
@@ -1422,6 +1511,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
     }
     if (tid == 0)
     {
+        M3_PHASE_MARK(M3_PHASE_SLEEP)
         sc->moverCount = moverCount;
         sc->stepCount += 1;
         sc->work[0] += (uint64_t)moverCount * (uint64_t)substeps;
@@ -1490,6 +1580,7 @@ struct m3BatchCache
 {
     std::vector<m3HostWorld*> worlds;
     uint64_t epoch = 0;
+    int32_t cacheBytes = 0;
     m3WorldView* dviews = nullptr;
     int32_t* dorder = nullptr;
     int32_t* doffsets = nullptr;
@@ -1593,7 +1684,23 @@ static int32_t PrepareBatch(m3HostWorld** worlds, int32_t count)
     }
     s_batch.worlds.assign(worlds, worlds + count);
     s_batch.epoch = g_m3ResidencyEpoch;
-    return M3GPU_OK;
+    // Shared memory for the solve kernel's body cache: enough for the
+    // largest world of the batch, within the per-block limit.
+    int32_t maxBodies = 0;
+    for (int32_t i = 0; i < count; ++i)
+    {
+        maxBodies = worlds[i]->hv.sc->bodyMax > maxBodies ? worlds[i]->hv.sc->bodyMax : maxBodies;
+    }
+    int64_t want = (int64_t)maxBodies * M3_BODY_CACHE_BYTES;
+    const int64_t limit = 200 * 1024;
+    s_batch.cacheBytes = (int32_t)(want < limit ? want : limit);
+    if (s_batch.cacheBytes > 48 * 1024)
+    {
+        rc = Check(cudaFuncSetAttribute(m3SolveKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        s_batch.cacheBytes),
+                   "cudaFuncSetAttribute(solve smem)");
+    }
+    return rc;
 }
 
 static float s_kernelMs[2] = {0.0f, 0.0f};
@@ -1630,6 +1737,24 @@ extern "C" int32_t m3gpu_world_stats(m3WorldId world, uint64_t* out)
         out[k] = w->hv.sc->work[k];
     }
     out[5] = (uint64_t)w->hv.sc->bodyMax;
+    return M3GPU_OK;
+}
+
+extern "C" int32_t m3gpu_world_phase_cycles(m3WorldId world, uint64_t* out)
+{
+    m3HostWorld* w = m3gpuWorldFromId(world);
+    if (w == nullptr || out == nullptr)
+    {
+        return m3gpuSetError(M3GPU_ERR_INVALID, "stale world or null output");
+    }
+    if (m3gpuSyncHost(w) != M3GPU_OK)
+    {
+        return m3gpu_last_error();
+    }
+    for (int32_t k = 0; k < 16; ++k)
+    {
+        out[k] = w->hv.sc->phase[k];
+    }
     return M3GPU_OK;
 }
 
@@ -1674,7 +1799,9 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
         m3PairOffsetsKernel<<<1, M3_BLOCK>>>(s_batch.dviews, count, s_batch.doffsets);
         m3NarrowKernel<<<s_narrowGrid, 128>>>(s_batch.dviews, s_batch.doffsets, count);
         cudaEventRecord(s_events[(size_t)(2 * step + 1)]);
-        m3SolveKernel<<<count, M3_BLOCK>>>(s_batch.dviews, s_batch.dorder, count, dt, substeps);
+        m3SolveKernel<<<count, M3_BLOCK, s_batch.cacheBytes>>>(s_batch.dviews, s_batch.dorder,
+                                                               count, dt, substeps,
+                                                               s_batch.cacheBytes);
         cudaEventRecord(s_events[(size_t)(2 * step + 2)]);
         s_launches += 4;
     }
