@@ -305,8 +305,9 @@ def main() -> None:
         dist.init_process_group("nccl", timeout=timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
 
-    rank_seed = args.seed + 1_000_003 * rank
-    sizes = world_sizes(m3.lib, rank_seed, args.worlds, args.lo, args.hi)
+    from maul3d_b200.shard import rank_seed as shard_seed, shard_sizes
+    rank_seed = shard_seed(args.seed, rank)
+    sizes = shard_sizes(m3.lib, rank_seed, args.worlds, args.lo, args.hi)
     worlds = build_worlds(m3, sizes, rank_seed)
     m3.reserve_worlds(worlds)
     m3.upload_worlds(worlds)
