@@ -286,6 +286,23 @@ M3GPU_API int32_t m3gpu_upload_worlds(const m3WorldId* worlds, int32_t count);
 /* Bytes one world's host image occupies (what an upload copies). */
 M3GPU_API int64_t m3gpu_world_image_bytes(m3WorldId world);
 
+/* Allocation-free step of one resident world (no reference counterpart).
+ * For callers that must not allocate device memory when they step: a
+ * frame loop with a hard deadline (allocating and freeing can stall the
+ * whole device), code running while a CUDA graph is being captured, or
+ * a host whose device memory belongs to its own pool allocator.  The
+ * world must already be resident (m3gpu_reserve_worlds and
+ * m3gpu_upload_worlds, called earlier when allocating was allowed); the
+ * step then allocates nothing: its scratch lives in a fixed 4 MiB
+ * device array (held by every GPU that loads the library until exit).
+ * Worlds whose scratch exceeds that, or with more than about 800 bodies,
+ * are refused with M3GPU_ERR_CAPACITY before any device work.  The first
+ * call on a device looks up that array's address; make it before any
+ * stream capture.  Calls share the array: calls that overlap on the GPU
+ * race, so serialise them.  Same result, bit for bit, as
+ * m3gpu_step_worlds on the same world. */
+M3GPU_API int32_t m3gpu_step_world_noalloc(m3WorldId world, float dt, int32_t substeps);
+
 /* Wait for all device work of the library to finish. */
 M3GPU_API int32_t m3gpu_synchronize(void);
 

@@ -1883,3 +1883,159 @@ int32_t m3gpuHashBatch(m3HostWorld** worlds, int32_t count, uint64_t* out)
     }
     return rc;
 }
+
+// ---------------------------------------------------------------------
+// Allocation-free single-world step.
+//
+// Some callers cannot allocate device memory at the moment they need a
+// step: a frame loop with a hard deadline (cudaMalloc and cudaFree can
+// synchronise the whole device), code running while a CUDA graph is
+// being captured, or a host whose device memory is owned entirely by a
+// pool allocator.  For them m3gpu_step_world_noalloc steps one world
+// that is already resident in HBM (reserved and uploaded earlier, when
+// allocating was allowed) without allocating anything: the step's
+// scratch, the one-world launch table and the status word live in
+// file-scope __device__ arrays of fixed size instead of the world's own
+// slab scratch and the batch tables.
+//
+// Limits: the world's scratch need (bodies, shapes, joints and 8 pairs
+// per shape of the reference's pair capacity) must fit in
+// M3_NOALLOC_SCRATCH_BYTES (4 MiB, about 800 shape slots), and its
+// body-velocity cache in 48 KiB of shared memory (800 bodies); larger
+// worlds are refused with M3GPU_ERR_CAPACITY before any device work.
+// Every GPU that loads the library holds these arrays until exit.
+//
+// The first call on a device looks up the arrays' device addresses
+// (cudaGetSymbolAddress) with that device current and caches them; make
+// that first call before any stream capture.  All calls share the
+// arrays and leave the last call's contents behind (every field the
+// step reads is rewritten first), so calls that overlap on the GPU,
+// from several host threads or streams, race: serialise them.
+// ---------------------------------------------------------------------
+#define M3_NOALLOC_SCRATCH_BYTES (4 * 1024 * 1024)
+#define M3_NOALLOC_MAX_DEVICES 64
+
+static __device__ __align__(256) uint8_t g_noallocScratch[M3_NOALLOC_SCRATCH_BYTES];
+static __device__ __align__(256) m3WorldView g_noallocView;
+static __device__ __align__(256) int32_t g_noallocTable[4]; // order[1], offsets[2], spare
+
+struct m3NoallocSymbols
+{
+    uint8_t* scratch;
+    m3WorldView* view;
+    int32_t* table;
+};
+static m3NoallocSymbols s_noalloc[M3_NOALLOC_MAX_DEVICES];
+
+static int32_t NoallocSetup(int32_t device, m3NoallocSymbols* out)
+{
+    if (device < 0 || device >= M3_NOALLOC_MAX_DEVICES)
+    {
+        return m3gpuSetError(M3GPU_ERR_INVALID, "device %d beyond the supported range", device);
+    }
+    m3NoallocSymbols& sym = s_noalloc[device];
+    if (sym.scratch == nullptr)
+    {
+        int32_t rc = Check(cudaGetSymbolAddress((void**)&sym.scratch, g_noallocScratch),
+                           "cudaGetSymbolAddress(scratch)");
+        if (rc == M3GPU_OK)
+        {
+            rc = Check(cudaGetSymbolAddress((void**)&sym.view, g_noallocView),
+                       "cudaGetSymbolAddress(view)");
+        }
+        if (rc == M3GPU_OK)
+        {
+            rc = Check(cudaGetSymbolAddress((void**)&sym.table, g_noallocTable),
+                       "cudaGetSymbolAddress(table)");
+        }
+        if (rc != M3GPU_OK)
+        {
+            sym.scratch = nullptr;
+            return rc;
+        }
+    }
+    *out = sym;
+    return M3GPU_OK;
+}
+
+extern "C" int32_t m3gpu_step_world_noalloc(m3WorldId worldId, float dt, int32_t substeps)
+{
+    m3gpuClearError();
+    m3HostWorld* w = m3gpuWorldFromId(worldId);
+    if (w == nullptr || !(dt > 0.0f) || substeps < 1 || substeps > M3_MAX_SUBSTEPS)
+    {
+        return m3gpuSetError(M3GPU_ERR_INVALID, "stale world or invalid dt/substeps");
+    }
+    if (w->dslab == nullptr || w->hostDirty)
+    {
+        return m3gpuSetError(M3GPU_ERR_INVALID,
+                             "world is not resident on the device: reserve and upload it first "
+                             "(m3gpu_reserve_worlds, m3gpu_upload_worlds)");
+    }
+    const int64_t need = m3gpuScratchBytes(w->bodyCap, w->shapeCap, w->jointCap, w->pairCap);
+    const int64_t cache = (int64_t)w->hv.sc->bodyMax * M3_BODY_CACHE_BYTES;
+    if (need > M3_NOALLOC_SCRATCH_BYTES || cache > 48 * 1024)
+    {
+        return m3gpuSetError(M3GPU_ERR_CAPACITY,
+                             "world needs %lld scratch bytes and %lld cache bytes; the "
+                             "allocation-free step holds %d and %d",
+                             (long long)need, (long long)cache, M3_NOALLOC_SCRATCH_BYTES,
+                             48 * 1024);
+    }
+    int device = 0;
+    int32_t rc = Check(cudaGetDevice(&device), "cudaGetDevice");
+    m3NoallocSymbols sym;
+    if (rc == M3GPU_OK)
+    {
+        rc = NoallocSetup(device, &sym);
+    }
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
+    // The one-world launch table: the world's view with its scratch
+    // redirected to the static array, order {0}.
+    m3WorldView view = w->dv;
+    view.hulls = w->dhulls;
+    view.scratch = sym.scratch;
+    view.scratchBytes = M3_NOALLOC_SCRATCH_BYTES;
+    const int32_t zero = 0;
+    rc = Check(cudaMemcpy(sym.view, &view, sizeof(view), cudaMemcpyHostToDevice), "noalloc view");
+    if (rc == M3GPU_OK)
+    {
+        rc = Check(cudaMemcpy(sym.table, &zero, sizeof(zero), cudaMemcpyHostToDevice),
+                   "noalloc order");
+    }
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
+    int32_t* order = sym.table;
+    int32_t* offsets = sym.table + 1;
+    const int32_t cacheBytes = (int32_t)cache;
+    m3BroadKernel<<<1, M3_BLOCK>>>(sym.view, order, 1);
+    m3PairOffsetsKernel<<<1, M3_BLOCK>>>(sym.view, 1, offsets);
+    m3NarrowKernel<<<148, 128>>>(sym.view, offsets, 1);
+    m3SolveKernel<<<1, M3_BLOCK, cacheBytes>>>(sym.view, order, 1, dt, substeps, cacheBytes);
+    s_launches += 4;
+    rc = Check(cudaGetLastError(), "noalloc step launch");
+    int32_t status = 0;
+    if (rc == M3GPU_OK)
+    {
+        rc = Check(cudaMemcpy(&status, &w->dv.sc->status, sizeof(int32_t), cudaMemcpyDeviceToHost),
+                   "noalloc step");
+    }
+    w->deviceAhead = true;
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
+    if (status != 0)
+    {
+        int32_t detail = 0;
+        cudaMemcpy(&detail, &w->dv.sc->statusDetail, sizeof(int32_t), cudaMemcpyDeviceToHost);
+        return m3gpuSetError(status, "world %d stalled on the device (status %d, detail %d)",
+                             w->slot, status, detail);
+    }
+    return M3GPU_OK;
+}
