@@ -2,7 +2,7 @@
 // limits, motor, collinearity lock) and fixed (rotation lock + point
 // weld), prepared, warm-started, solved and stored exactly as the
 // reference does (src/solver.c:699-1042, :1044-1209, :1211-2702,
-// :2704-2730).  Joints solve serially in slot order between the contact
+// :2704-2730).  The reference runs joints serially in slot order between the contact
 // colours, the reference schedule, by one thread of the world's block.
 #ifndef M3_JOINTS_CUH
 #define M3_JOINTS_CUH
@@ -70,101 +70,120 @@ __device__ __forceinline__ m3Vec3 m3QuatToRotationVec(m3Quat relQ)
     return m3MulSV3(angle / len, v);
 }
 
-// PrepareJoints (solver.c:699-1042) for the device joint types.  Runs
-// on one thread; returns the joint-row count, or sets *status for a
-// joint the device path does not cover.
-__device__ int32_t m3PrepareJoints(const m3WorldView& w, m3JointDev* joints, m3real h,
-                                   int32_t* status, int32_t* detail)
+// Joint rows the device path covers: spherical without cone or twist
+// limits, revolute with limit and motor, fixed; no springs, no breaking
+// thresholds.  Returns 0, or a detail code for a refused joint.
+__device__ __forceinline__ int32_t m3JointRefusal(const m3WorldView& w, int32_t j)
 {
-    int32_t count = 0;
-    const int32_t maxJoint = w.sc->jointMax;
-    for (int32_t j = 0; j < maxJoint; ++j)
+    uint8_t type = w.jtype[j];
+    uint8_t flags = w.jflags[j];
+    if (w.jbreak[j].x != 0.0f || w.jbreak[j].y != 0.0f || (flags & 8) != 0 ||
+        (type != 0 && type != 1 && type != 3) || (type == 0 && (flags & 5) != 0))
     {
-        if (w.jointAlive[j] == 0)
-        {
-            continue;
-        }
-        uint8_t type = w.jtype[j];
-        uint8_t flags = w.jflags[j];
-        if (w.jbreak[j].x != 0.0f || w.jbreak[j].y != 0.0f || (flags & 8) != 0 ||
-            (type != 0 && type != 1 && type != 3) || (type == 0 && (flags & 5) != 0))
-        {
-            *status = M3GPU_ERR_UNSUPPORTED;
-            *detail = 4000 + type;
-            return 0;
-        }
-        int32_t bodyA = w.jbodyA[j];
-        int32_t bodyB = w.jbodyB[j];
-        int awakeDynA = w.btype[bodyA] == M3_BODY_DYNAMIC && w.awake[bodyA];
-        int awakeDynB = w.btype[bodyB] == M3_BODY_DYNAMIC && w.awake[bodyB];
-        if (!awakeDynA && !awakeDynB)
-        {
-            continue;
-        }
-        m3JointDev* c = &joints[count];
-        count += 1;
-        memset(c, 0, sizeof(*c));
-        c->joint = j;
-        c->bodyA = bodyA;
-        c->bodyB = bodyB;
-        const m3Transform xfA = w.xf[bodyA];
-        const m3Transform xfB = w.xf[bodyB];
-        c->rA = m3RotateVec3(xfA.q, m3Sub3(w.jlocalA[j], w.lc[bodyA]));
-        c->rB = m3RotateVec3(xfB.q, m3Sub3(w.jlocalB[j], w.lc[bodyB]));
-        m3Vec3 rlcA = m3RotateVec3(xfA.q, w.lc[bodyA]);
-        m3Vec3 rlcB = m3RotateVec3(xfB.q, w.lc[bodyB]);
-        c->deltaCenter = v3((m3real)(xfB.p.x + (double)rlcB.x - xfA.p.x - (double)rlcA.x),
-                            (m3real)(xfB.p.y + (double)rlcB.y - xfA.p.y - (double)rlcA.y),
-                            (m3real)(xfB.p.z + (double)rlcB.z - xfA.p.z - (double)rlcA.z));
-        c->invMassA = w.btype[bodyA] == M3_BODY_DYNAMIC ? w.invMass[bodyA] : 0.0f;
-        c->invMassB = w.btype[bodyB] == M3_BODY_DYNAMIC ? w.invMass[bodyB] : 0.0f;
-        c->invIA = m3WorldInvInertiaDev(w, bodyA);
-        c->invIB = m3WorldInvInertiaDev(w, bodyB);
-        c->softness = m3MakeSoft(60.0f, 2.0f, h);
-        c->impulse = w.jimpulse[j];
-        c->type = type;
-        c->flags = flags;
-        c->springImpulseV = w.jspringImp[j];
-        if (type == 1)
-        {
-            c->frameQA = m3MulQuat(xfA.q, w.jframeA[j]);
-            c->frameQB = m3MulQuat(xfB.q, w.jframeB[j]);
-            m3Vec3 axis = m3RotateVec3(c->frameQA, v3(0.0f, 0.0f, 1.0f));
-            c->rotationAxis = axis;
-            m3Vec3 sum = m3Add3(m3MulMV3(c->invIA, axis), m3MulMV3(c->invIB, axis));
-            m3real k = m3Dot3(axis, sum);
-            c->axialMass = k > 0.0f ? 1.0f / k : 0.0f;
-            m3Quat relQ = m3MulQuat(m3Conj(c->frameQA), c->frameQB);
-            c->perpAxisX = m3PerpColumn(c->frameQA, relQ, v3(1.0f, 0.0f, 0.0f));
-            c->perpAxisY = m3PerpColumn(c->frameQA, relQ, v3(0.0f, 1.0f, 0.0f));
-            c->perpImpulseX = w.jperp[j].x;
-            c->perpImpulseY = w.jperp[j].y;
-            c->motorImpulse = w.jperp[j].z;
-            c->lowerImpulse = w.jlimitImp[j].x;
-            c->upperImpulse = w.jlimitImp[j].y;
-            c->motorSpeed = w.jmotor[j].x;
-            c->maxMotorEffort = w.jmotor[j].y;
-            c->lowerLimit = w.jlimits[j].x;
-            c->upperLimit = w.jlimits[j].y;
-            c->angularImpulse = w.jangular[j];
-        }
-        else if (type == 3)
-        {
-            c->frameQA = m3MulQuat(xfA.q, w.jframeA[j]);
-            c->frameQB = m3MulQuat(xfB.q, w.jframeB[j]);
-            c->angularImpulse = w.jangular[j];
-        }
+        return 4000 + type;
     }
-    return count;
+    return 0;
 }
 
-// solver.c:1044-1209 for the device joint types.
-__device__ void m3WarmStartJoints(const m3WorldView& w, m3JointDev* joints, int32_t count,
-                                  const m3Quat* deltaRot)
+// A joint gets a row when either side is an awake dynamic body
+// (solver.c:705-725).
+__device__ __forceinline__ bool m3JointActive(const m3WorldView& w, int32_t j)
 {
-    for (int32_t i = 0; i < count; ++i)
+    if (w.jointAlive[j] == 0)
     {
-        m3JointDev* c = &joints[i];
+        return false;
+    }
+    int32_t bodyA = w.jbodyA[j];
+    int32_t bodyB = w.jbodyB[j];
+    int awakeDynA = w.btype[bodyA] == M3_BODY_DYNAMIC && w.awake[bodyA];
+    int awakeDynB = w.btype[bodyB] == M3_BODY_DYNAMIC && w.awake[bodyB];
+    return awakeDynA || awakeDynB;
+}
+
+// One joint's row, the body of PrepareJoints (solver.c:726-1042) for
+// the device joint types.  Every field the store writes back is set:
+// the reference zeroes the row first, so a spherical row stores zero
+// perpendicular, limit and angular impulses.
+__device__ void m3PrepareJoint(const m3WorldView& w, m3JointDev* c, int32_t j, m3real h)
+{
+    uint8_t type = w.jtype[j];
+    uint8_t flags = w.jflags[j];
+    int32_t bodyA = w.jbodyA[j];
+    int32_t bodyB = w.jbodyB[j];
+    c->joint = j;
+    c->bodyA = bodyA;
+    c->bodyB = bodyB;
+    const m3Transform xfA = w.xf[bodyA];
+    const m3Transform xfB = w.xf[bodyB];
+    c->rA = m3RotateVec3(xfA.q, m3Sub3(w.jlocalA[j], w.lc[bodyA]));
+    c->rB = m3RotateVec3(xfB.q, m3Sub3(w.jlocalB[j], w.lc[bodyB]));
+    m3Vec3 rlcA = m3RotateVec3(xfA.q, w.lc[bodyA]);
+    m3Vec3 rlcB = m3RotateVec3(xfB.q, w.lc[bodyB]);
+    c->deltaCenter = v3((m3real)(xfB.p.x + (double)rlcB.x - xfA.p.x - (double)rlcA.x),
+                        (m3real)(xfB.p.y + (double)rlcB.y - xfA.p.y - (double)rlcA.y),
+                        (m3real)(xfB.p.z + (double)rlcB.z - xfA.p.z - (double)rlcA.z));
+    c->invMassA = w.btype[bodyA] == M3_BODY_DYNAMIC ? w.invMass[bodyA] : 0.0f;
+    c->invMassB = w.btype[bodyB] == M3_BODY_DYNAMIC ? w.invMass[bodyB] : 0.0f;
+    c->invIA = m3WorldInvInertiaDev(w, bodyA);
+    c->invIB = m3WorldInvInertiaDev(w, bodyB);
+    c->softness = m3MakeSoft(60.0f, 2.0f, h);
+    c->impulse = w.jimpulse[j];
+    c->type = type;
+    c->flags = flags;
+    c->springImpulseV = w.jspringImp[j];
+    const m3Quat identity = m3IdentityQuat();
+    const m3Vec3 zero = v3(0.0f, 0.0f, 0.0f);
+    c->frameQA = identity;
+    c->frameQB = identity;
+    c->rotationAxis = zero;
+    c->axialMass = 0.0f;
+    c->perpAxisX = zero;
+    c->perpAxisY = zero;
+    c->perpImpulseX = 0.0f;
+    c->perpImpulseY = 0.0f;
+    c->motorImpulse = 0.0f;
+    c->lowerImpulse = 0.0f;
+    c->upperImpulse = 0.0f;
+    c->motorSpeed = 0.0f;
+    c->maxMotorEffort = 0.0f;
+    c->lowerLimit = 0.0f;
+    c->upperLimit = 0.0f;
+    c->angularImpulse = zero;
+    if (type == 1)
+    {
+        c->frameQA = m3MulQuat(xfA.q, w.jframeA[j]);
+        c->frameQB = m3MulQuat(xfB.q, w.jframeB[j]);
+        m3Vec3 axis = m3RotateVec3(c->frameQA, v3(0.0f, 0.0f, 1.0f));
+        c->rotationAxis = axis;
+        m3Vec3 sum = m3Add3(m3MulMV3(c->invIA, axis), m3MulMV3(c->invIB, axis));
+        m3real k = m3Dot3(axis, sum);
+        c->axialMass = k > 0.0f ? 1.0f / k : 0.0f;
+        m3Quat relQ = m3MulQuat(m3Conj(c->frameQA), c->frameQB);
+        c->perpAxisX = m3PerpColumn(c->frameQA, relQ, v3(1.0f, 0.0f, 0.0f));
+        c->perpAxisY = m3PerpColumn(c->frameQA, relQ, v3(0.0f, 1.0f, 0.0f));
+        c->perpImpulseX = w.jperp[j].x;
+        c->perpImpulseY = w.jperp[j].y;
+        c->motorImpulse = w.jperp[j].z;
+        c->lowerImpulse = w.jlimitImp[j].x;
+        c->upperImpulse = w.jlimitImp[j].y;
+        c->motorSpeed = w.jmotor[j].x;
+        c->maxMotorEffort = w.jmotor[j].y;
+        c->lowerLimit = w.jlimits[j].x;
+        c->upperLimit = w.jlimits[j].y;
+        c->angularImpulse = w.jangular[j];
+    }
+    else if (type == 3)
+    {
+        c->frameQA = m3MulQuat(xfA.q, w.jframeA[j]);
+        c->frameQB = m3MulQuat(xfB.q, w.jframeB[j]);
+        c->angularImpulse = w.jangular[j];
+    }
+}
+
+// One joint's warm start (solver.c:1044-1209 loop body).
+__device__ void m3WarmStartJoint(const m3WorldView& w, m3JointDev* c, const m3Quat* deltaRot)
+{
+    {
         m3Vec3 rA = m3RotateVec3(deltaRot[c->bodyA], c->rA);
         m3Vec3 rB = m3RotateVec3(deltaRot[c->bodyB], c->rB);
         m3Vec3 angularImpulse = v3(0.0f, 0.0f, 0.0f);
@@ -213,14 +232,12 @@ __device__ __forceinline__ m3real m3LimitRow(m3real cc, m3real cdot, m3real axia
     return *accum - old;
 }
 
-// solver.c:1211-2702 for the device joint types.
-__device__ void m3SolveJoints(const m3WorldView& w, m3JointDev* joints, int32_t count,
-                              const m3Vec3* deltaPos, const m3Quat* deltaRot, m3real hSub,
-                              m3real invHSub, bool useBias)
+// One joint's solve (solver.c:1211-2702 loop body) for the device joint
+// types.
+__device__ void m3SolveJoint(const m3WorldView& w, m3JointDev* c, const m3Vec3* deltaPos,
+                             const m3Quat* deltaRot, m3real hSub, m3real invHSub, bool useBias)
 {
-    for (int32_t i = 0; i < count; ++i)
     {
-        m3JointDev* c = &joints[i];
         m3Vec3 rA = m3RotateVec3(deltaRot[c->bodyA], c->rA);
         m3Vec3 rB = m3RotateVec3(deltaRot[c->bodyB], c->rB);
         m3Vec3 vA = w.v[c->bodyA];
@@ -380,12 +397,10 @@ __device__ void m3SolveJoints(const m3WorldView& w, m3JointDev* joints, int32_t 
     }
 }
 
-// solver.c:2704-2730
-__device__ void m3StoreJointImpulses(const m3WorldView& w, const m3JointDev* joints, int32_t count)
+// One joint's store (solver.c:2704-2730 loop body).
+__device__ void m3StoreJoint(const m3WorldView& w, const m3JointDev* c)
 {
-    for (int32_t i = 0; i < count; ++i)
     {
-        const m3JointDev* c = &joints[i];
         w.jimpulse[c->joint] = c->impulse;
         w.jperp[c->joint] = v3(c->perpImpulseX, c->perpImpulseY, c->motorImpulse);
         w.jlimitImp[c->joint] = v3(c->lowerImpulse, c->upperImpulse, 0.0f);

@@ -151,7 +151,9 @@ __device__ void m3PrepareContact(const m3WorldView& w, m3ContactDev* c, int32_t 
     int32_t shapeB = (int32_t)(key & 0xFFFFFFFFu);
     int32_t bodyA = w.shapeBody[shapeA];
     int32_t bodyB = w.shapeBody[shapeB];
-    memset(c, 0, sizeof(*c));
+    // Every field a later phase reads is written below (the reference
+    // zeroes the whole record first; rollingK is read only when rolling
+    // resistance is positive, points only below pointCount).
     c->bodyA = bodyA;
     c->bodyB = bodyB;
     c->manifoldIndex = pairIndex;

@@ -92,9 +92,14 @@ struct m3Scratch
     m3ContactDev* cons;    // per pair
     int32_t* pairFlag;     // per pair (compaction)
     uint8_t* colors;       // per pair
+    int2* conPair;         // per pair: colouring body pair
     int32_t* lists;        // per pair
     int32_t* starts;       // M3_GRAPH_COLORS + 2
-    m3JointDev* joints;    // per joint
+    m3JointDev* joints;    // per joint row
+    int32_t* jointFlag;    // per joint (selection scan)
+    int32_t* jointLevel;   // per joint row: dependency level
+    int32_t* jointOrder;   // joint rows grouped by level
+    int32_t* jointLevelStart; // level offsets into jointOrder
 };
 
 static __host__ __device__ inline int64_t NextPow2(int64_t n)
@@ -138,9 +143,14 @@ static __host__ __device__ inline int64_t ScratchCarve(m3Scratch* s, uint8_t* ba
     M3_CARVE(cons, m3ContactDev, pairCap)
     M3_CARVE(pairFlag, int32_t, pairCap + 1)
     M3_CARVE(colors, uint8_t, pairCap)
+    M3_CARVE(conPair, int2, pairCap)
     M3_CARVE(lists, int32_t, pairCap)
     M3_CARVE(starts, int32_t, M3_GRAPH_COLORS + 2)
     M3_CARVE(joints, m3JointDev, jointCap)
+    M3_CARVE(jointFlag, int32_t, jointCap + 1)
+    M3_CARVE(jointLevel, int32_t, jointCap)
+    M3_CARVE(jointOrder, int32_t, jointCap)
+    M3_CARVE(jointLevelStart, int32_t, jointCap + 2)
 #undef M3_CARVE
     return off;
 }
@@ -160,9 +170,11 @@ extern "C" int64_t m3gpuScratchBytes(int32_t bodyCap, int32_t shapeCap, int32_t 
 // memory.  Must be called by every thread of the block.
 __device__ int32_t BlockExclusiveScan(int32_t* a, int32_t n)
 {
-    __shared__ int32_t partial[M3_BLOCK];
+    __shared__ int32_t warpSums[M3_BLOCK / 32];
     __shared__ int32_t total;
     const int32_t t = threadIdx.x;
+    const int32_t lane = t & 31;
+    const int32_t warp = t >> 5;
     const int32_t chunk = (n + M3_BLOCK - 1) / M3_BLOCK;
     const int32_t lo = t * chunk < n ? t * chunk : n;
     const int32_t hi = lo + chunk < n ? lo + chunk : n;
@@ -171,26 +183,50 @@ __device__ int32_t BlockExclusiveScan(int32_t* a, int32_t n)
     {
         sum += a[i];
     }
-    partial[t] = sum;
-    __syncthreads();
-    if (t == 0)
+    // Inclusive scan of the chunk sums across the warp, then across the
+    // warps' totals.
+    int32_t x = sum;
+    for (int32_t o = 1; o < 32; o <<= 1)
     {
-        int32_t run = 0;
-        for (int32_t k = 0; k < M3_BLOCK; ++k)
+        int32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= o)
         {
-            int32_t x = partial[k];
-            partial[k] = run;
-            run += x;
+            x += y;
         }
-        total = run;
+    }
+    if (lane == 31)
+    {
+        warpSums[warp] = x;
     }
     __syncthreads();
-    int32_t run = partial[t];
+    if (warp == 0)
+    {
+        int32_t v = lane < M3_BLOCK / 32 ? warpSums[lane] : 0;
+        int32_t inc = v;
+        for (int32_t o = 1; o < 32; o <<= 1)
+        {
+            int32_t y = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+            if (lane >= o)
+            {
+                inc += y;
+            }
+        }
+        if (lane < M3_BLOCK / 32)
+        {
+            warpSums[lane] = inc - v;
+        }
+        if (lane == M3_BLOCK / 32 - 1)
+        {
+            total = inc;
+        }
+    }
+    __syncthreads();
+    int32_t run = warpSums[warp] + (x - sum);
     for (int32_t i = lo; i < hi; ++i)
     {
-        int32_t x = a[i];
+        int32_t y = a[i];
         a[i] = run;
-        run += x;
+        run += y;
     }
     __syncthreads();
     return total;
@@ -874,6 +910,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
     __shared__ int32_t s_status;
     __shared__ int32_t s_anyRestitution;
     __shared__ int32_t s_starts[M3_GRAPH_COLORS + 2];
+    __shared__ int32_t s_jointLevels;
     if (tid == 0)
     {
         s_status = sc->status;
@@ -1022,10 +1059,88 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
             sc->statusDetail = 2001;
         }
     }
-    // Joints prepare in slot order (solver.c:699-1042).
+    // Joint rows (solver.c:699-1042): selection in slot order, rows
+    // prepared in parallel, then grouped into dependency levels.  A
+    // joint's level is one past the latest earlier joint sharing either
+    // of its bodies (any body, static ones included), so the joints of
+    // one level touch disjoint bodies and solving level by level, each
+    // level in parallel, reproduces the reference's serial slot order.
+    for (int32_t j = tid; j < jointMax; j += M3_BLOCK)
+    {
+        int32_t flag = 0;
+        if (w.jointAlive[j] != 0)
+        {
+            int32_t refusal = m3JointRefusal(w, j);
+            if (refusal != 0)
+            {
+                s_status = M3GPU_ERR_UNSUPPORTED;
+                sc->statusDetail = refusal;
+            }
+            else if (m3JointActive(w, j))
+            {
+                flag = 1;
+            }
+        }
+        s.jointFlag[j] = flag;
+    }
+    __syncthreads();
+    const int32_t jointCount = BlockExclusiveScan(s.jointFlag, jointMax);
+    for (int32_t j = tid; j < jointMax; j += M3_BLOCK)
+    {
+        int32_t next = j + 1 < jointMax ? s.jointFlag[j + 1] : jointCount;
+        if (next != s.jointFlag[j])
+        {
+            m3PrepareJoint(w, &s.joints[s.jointFlag[j]], j, h);
+        }
+    }
+    __syncthreads();
     if (tid == 0)
     {
-        sc->jointConstraintCount = m3PrepareJoints(w, s.joints, h, &s_status, &sc->statusDetail);
+        int32_t levels = 0;
+        if (jointCount > 0)
+        {
+            for (int32_t i = 0; i < bodyMax; ++i)
+            {
+                s.ready[i] = -1;
+            }
+            for (int32_t r = 0; r < jointCount; ++r)
+            {
+                int32_t a = s.joints[r].bodyA;
+                int32_t b = s.joints[r].bodyB;
+                int32_t la = s.ready[a];
+                int32_t lb = s.ready[b];
+                int32_t level = 1 + (la > lb ? la : lb);
+                s.ready[a] = level;
+                s.ready[b] = level;
+                s.jointLevel[r] = level;
+                levels = level + 1 > levels ? level + 1 : levels;
+            }
+            for (int32_t k = 0; k <= levels; ++k)
+            {
+                s.jointLevelStart[k] = 0;
+            }
+            for (int32_t r = 0; r < jointCount; ++r)
+            {
+                s.jointLevelStart[s.jointLevel[r] + 1] += 1;
+            }
+            for (int32_t k = 0; k < levels; ++k)
+            {
+                s.jointLevelStart[k + 1] += s.jointLevelStart[k];
+            }
+            for (int32_t r = 0; r < jointCount; ++r)
+            {
+                int32_t level = s.jointLevel[r];
+                s.jointOrder[s.jointLevelStart[level]] = r;
+                s.jointLevelStart[level] += 1;
+            }
+            for (int32_t k = levels; k > 0; --k)
+            {
+                s.jointLevelStart[k] = s.jointLevelStart[k - 1];
+            }
+            s.jointLevelStart[0] = 0;
+        }
+        s_jointLevels = levels;
+        sc->jointConstraintCount = jointCount;
     }
     __syncthreads();
     if (s_status != 0)
@@ -1039,13 +1154,32 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
 
     M3_PHASE_MARK(M3_PHASE_PREPARE)
     // Greedy 16-colour first-free-bit colouring in constraint order, the
-    // overflow bucket last (solver.c:2750-2810).
+    // overflow bucket last (solver.c:2750-2810).  The walk is serial, so
+    // its inputs are staged first: each constraint's effective body pair
+    // (-1 for a side that is not an awake dynamic body), the body colour
+    // masks and the colours live in shared memory when they fit (the
+    // body cache's space is free until the substep loop).
+    extern __shared__ __align__(16) uint8_t s_colorStage[];
+    const int64_t maskBytes = 4 * (((int64_t)bodyMax + 1) & ~1LL);
+    const bool staged =
+        maskBytes + 9 * (int64_t)constraintCount <= (int64_t)cacheBytes;
+    uint32_t* cMask = staged ? (uint32_t*)s_colorStage : s.bodyMask;
+    int2* cPair = staged ? (int2*)(s_colorStage + maskBytes) : s.conPair;
+    uint8_t* cColor = staged ? (uint8_t*)(cPair + constraintCount) : s.colors;
+    for (int32_t i = tid; i < bodyMax; i += M3_BLOCK)
+    {
+        cMask[i] = 0u;
+    }
+    for (int32_t i = tid; i < constraintCount; i += M3_BLOCK)
+    {
+        const m3ContactDev* c = &s.cons[i];
+        int32_t a = c->dynA && w.awake[c->bodyA] ? c->bodyA : -1;
+        int32_t b = c->dynB && w.awake[c->bodyB] ? c->bodyB : -1;
+        cPair[i] = make_int2(a, b);
+    }
+    __syncthreads();
     if (tid == 0)
     {
-        for (int32_t i = 0; i < bodyMax; ++i)
-        {
-            s.bodyMask[i] = 0u;
-        }
         int32_t counts[M3_GRAPH_COLORS + 1];
         for (int32_t c = 0; c <= M3_GRAPH_COLORS; ++c)
         {
@@ -1053,29 +1187,22 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
         }
         for (int32_t i = 0; i < constraintCount; ++i)
         {
-            const m3ContactDev* c = &s.cons[i];
-            int dynA = c->dynA && w.awake[c->bodyA];
-            int dynB = c->dynB && w.awake[c->bodyB];
-            uint32_t mask = (dynA ? s.bodyMask[c->bodyA] : 0u) | (dynB ? s.bodyMask[c->bodyB] : 0u);
-            int32_t color = M3_GRAPH_COLORS;
-            for (int32_t bit = 0; bit < M3_GRAPH_COLORS; ++bit)
-            {
-                if ((mask & (1u << bit)) == 0u)
-                {
-                    color = bit;
-                    break;
-                }
-            }
-            s.colors[i] = (uint8_t)color;
+            const int2 p = cPair[i];
+            uint32_t mask = (p.x >= 0 ? cMask[p.x] : 0u) | (p.y >= 0 ? cMask[p.y] : 0u);
+            // First clear bit among the 16 colours; 16 = overflow.
+            int32_t color = __ffs((int)~mask) - 1;
+            color = color < M3_GRAPH_COLORS ? color : M3_GRAPH_COLORS;
+            cColor[i] = (uint8_t)color;
             if (color < M3_GRAPH_COLORS)
             {
-                if (dynA)
+                const uint32_t bit = 1u << color;
+                if (p.x >= 0)
                 {
-                    s.bodyMask[c->bodyA] |= 1u << color;
+                    cMask[p.x] |= bit;
                 }
-                if (dynB)
+                if (p.y >= 0)
                 {
-                    s.bodyMask[c->bodyB] |= 1u << color;
+                    cMask[p.y] |= bit;
                 }
             }
             counts[color] += 1;
@@ -1096,7 +1223,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
         }
         for (int32_t i = 0; i < constraintCount; ++i)
         {
-            s.lists[fill[s.colors[i]]++] = i;
+            s.lists[fill[cColor[i]]++] = i;
         }
         sc->lastColorCount = used;
         sc->constraintCount = constraintCount;
@@ -1145,7 +1272,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
     }
     __syncthreads();
     M3_PHASE_MARK(M3_PHASE_COLOR)
-    const int32_t jointCount = sc->jointConstraintCount;
+    const int32_t jointLevels = s_jointLevels;
     const m3real pushMax = sc->contactPushMaxSpeed;
 
     // Body velocities and the substep deltas live in shared memory for
@@ -1190,11 +1317,15 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
         }
         __syncthreads();
         M3_PHASE_MARK(M3_PHASE_INTEGRATE_V)
-        if (tid == 0 && jointCount > 0)
+        for (int32_t level = 0; level < jointLevels; ++level)
         {
-            m3WarmStartJoints(wl, s.joints, jointCount, dQ);
+            for (int32_t k = s.jointLevelStart[level] + tid; k < s.jointLevelStart[level + 1];
+                 k += M3_BLOCK)
+            {
+                m3WarmStartJoint(wl, &s.joints[s.jointOrder[k]], dQ);
+            }
+            __syncthreads();
         }
-        __syncthreads();
         // Warm start, colour by colour; the overflow bucket serially.
         for (int32_t color = 0; color < M3_GRAPH_COLORS; ++color)
         {
@@ -1216,12 +1347,17 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
             {
                 m3WarmStartContact(wl, &s.cons[s.lists[k]]);
             }
-            if (jointCount > 0)
-            {
-                m3SolveJoints(wl, s.joints, jointCount, dP, dQ, h, invH, true);
-            }
         }
         __syncthreads();
+        for (int32_t level = 0; level < jointLevels; ++level)
+        {
+            for (int32_t k = s.jointLevelStart[level] + tid; k < s.jointLevelStart[level + 1];
+                 k += M3_BLOCK)
+            {
+                m3SolveJoint(wl, &s.joints[s.jointOrder[k]], dP, dQ, h, invH, true);
+            }
+            __syncthreads();
+        }
         M3_PHASE_MARK(M3_PHASE_WARM)
         for (int32_t color = 0; color < M3_GRAPH_COLORS; ++color)
         {
@@ -1252,11 +1388,15 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
         }
         __syncthreads();
         M3_PHASE_MARK(M3_PHASE_INTEGRATE_P)
-        if (tid == 0 && jointCount > 0)
+        for (int32_t level = 0; level < jointLevels; ++level)
         {
-            m3SolveJoints(wl, s.joints, jointCount, dP, dQ, h, invH, false);
+            for (int32_t k = s.jointLevelStart[level] + tid; k < s.jointLevelStart[level + 1];
+                 k += M3_BLOCK)
+            {
+                m3SolveJoint(wl, &s.joints[s.jointOrder[k]], dP, dQ, h, invH, false);
+            }
+            __syncthreads();
         }
-        __syncthreads();
         for (int32_t color = 0; color < M3_GRAPH_COLORS; ++color)
         {
             int32_t a = s_starts[color];
@@ -1314,9 +1454,12 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
     {
         m3StoreContact(&s.cons[i], man);
     }
+    for (int32_t r = tid; r < jointCount; r += M3_BLOCK)
+    {
+        m3StoreJoint(w, &s.joints[r]);
+    }
     if (tid == 0)
     {
-        m3StoreJointImpulses(w, s.joints, jointCount);
         sc->lastInvH = invH;
         // Wind phase (solver.c:4220-4229).
         if (sc->windGustHertz > 0.0f)
@@ -1516,7 +1659,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
         sc->stepCount += 1;
         sc->work[0] += (uint64_t)moverCount * (uint64_t)substeps;
         sc->work[1] += (uint64_t)constraintCount * (uint64_t)substeps;
-        sc->work[2] += (uint64_t)jointCount * (uint64_t)substeps;
+        sc->work[2] += (uint64_t)sc->jointConstraintCount * (uint64_t)substeps;
         sc->work[3] += (uint64_t)pairCount;
         sc->work[4] += 1;
     }
