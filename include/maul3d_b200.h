@@ -204,8 +204,9 @@ M3GPU_API bool m3World_IsValid(m3WorldId worldId);
 /* solver.c:4322 (world.h:195): one step of `dt` seconds in `substeps`
  * substeps, computed on the GPU.  Refuses (no-op) a stale id, dt <= 0 or
  * substeps outside [1, 256], like the reference.  A device-side refusal
- * (a capacity or feature the device path does not cover) leaves the
- * world unstepped and is reported by m3gpu_last_error(). */
+ * (a capacity or feature the device path does not cover) is reported by
+ * m3gpu_last_error(); the world is then marked failed, its state is
+ * unspecified and every later step of it is refused the same way. */
 M3GPU_API void m3World_Step(m3WorldId worldId, float dt, int32_t substeps);
 
 /* snapshot.c:932 (world.h:510): FNV-1a over the curated world state,

@@ -2,8 +2,11 @@
 // limits, motor, collinearity lock) and fixed (rotation lock + point
 // weld), prepared, warm-started, solved and stored exactly as the
 // reference does (src/solver.c:699-1042, :1044-1209, :1211-2702,
-// :2704-2730).  The reference runs joints serially in slot order between the contact
-// colours, the reference schedule, by one thread of the world's block.
+// :2704-2730).  The reference runs joints serially in slot order before
+// the contact colours; the device groups them into dependency levels (a
+// joint's level is one past the last earlier joint sharing a body with
+// it), so rows of one level touch disjoint bodies and run on separate
+// threads while every body still sees its joints in slot order.
 #ifndef M3_JOINTS_CUH
 #define M3_JOINTS_CUH
 
