@@ -56,16 +56,14 @@ UNIT = "body-substeps/s"
 DT = 1.0 / 60.0
 SCENE_UNEVEN = 2
 
-# Algorithmic bytes per unit of work (the reference's record layouts):
-# per moving body per substep, integrate velocities 141 B + integrate
-# positions 173 B; per contact row per substep 3 passes x (456 B record +
-# 2 x 48 B v,w + 2 x 28 B dp,dq); per joint row per substep 3 x (472 +
-# 152); per candidate pair per step 2 x 40 B transforms + 2 x 32 B geom
-# + 188 B new + 188 B old manifold.
+# Algorithmic bytes per unit of work of the substep loop (the
+# reference's record layouts): per moving body per substep, integrate
+# velocities 141 B + integrate positions 173 B; per contact row per
+# substep 3 passes x (456 B record + 2 x 48 B v,w + 2 x 28 B dp,dq); per
+# joint row per substep 3 x (472 + 152).
 BYTES_PER_MOVER_SUBSTEP = 314
 BYTES_PER_CONTACT_SUBSTEP = 3 * (456 + 2 * 48 + 2 * 28)
 BYTES_PER_JOINT_SUBSTEP = 3 * (472 + 152)
-BYTES_PER_PAIR_STEP = 2 * 40 + 2 * 32 + 188 + 188
 
 
 def env_int(name: str, default: int) -> int:
@@ -333,7 +331,7 @@ def main() -> None:
         dist.barrier()
     clocks = sampler.stop()
     ms = e0.elapsed_time(e1)
-    collide_ms, solve_ms = m3.kernel_ms()
+    stage_ms = m3.kernel_ms()
     stats1 = np.stack([m3.world_stats(w) for w in worlds])
     work = (stats1 - stats0).astype(np.float64).sum(axis=0)
     device_hashes = m3.hash_worlds(worlds)
@@ -351,22 +349,21 @@ def main() -> None:
         total_bs = float(local_bs)
     value = total_bs / (ms_max / 1000.0)
 
-    # Roofline of the dominant kernel: algorithmic bytes / device time.
-    solve_bytes = (BYTES_PER_MOVER_SUBSTEP * work[0] + BYTES_PER_CONTACT_SUBSTEP * work[1] +
-                   BYTES_PER_JOINT_SUBSTEP * work[2])
-    collide_bytes = BYTES_PER_PAIR_STEP * work[3]
+    # Roofline of the dominant kernel (m3SubstepKernel, the substep loop:
+    # integrate, warm start, solve, relax, restitution, store):
+    # algorithmic bytes of its per-substep row and body passes / its
+    # device time from CUDA events around it on the launching stream.
+    sub_bytes = (BYTES_PER_MOVER_SUBSTEP * work[0] + BYTES_PER_CONTACT_SUBSTEP * work[1] +
+                 BYTES_PER_JOINT_SUBSTEP * work[2])
     peak, peak_kind = measured_peaks()
-    if solve_ms >= collide_ms:
-        kname, kbytes, kms = "m3SolveKernel", solve_bytes, solve_ms
-    else:
-        kname, kbytes, kms = "m3CollideKernel", collide_bytes, collide_ms
-    achieved = (kbytes / args.steps) / (kms / args.steps / 1000.0) / 1e9
-    roofline = {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak,
-                "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+    kms = stage_ms["substep"]
+    achieved = (sub_bytes / args.steps) / (kms / args.steps / 1000.0) / 1e9
+    roofline = {"kernel": "m3SubstepKernel", "bound": "hbm", "achieved": achieved,
+                "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": None,
-                "bytes_per_launch": kbytes / args.steps,
+                "bytes_per_launch": sub_bytes / args.steps,
                 "launch_ms": kms / args.steps,
-                "share": {"m3CollideKernel": collide_ms / ms, "m3SolveKernel": solve_ms / ms}}
+                "share": {k: v / ms for k, v in stage_ms.items()}}
 
     # Plain path: one world per launch sequence, a sample of the worlds.
     plain = None

@@ -314,8 +314,10 @@ M3GPU_API int64_t m3gpu_launch_count(void);
 M3GPU_API float m3gpu_last_step_ms(void);
 
 /* Device time in milliseconds of the last m3gpu_step_worlds call, split
- * by kernel: out[0] the collide kernel (bounds, pairs, narrowphase),
- * out[1] the solve kernel (islands through sleep), summed over steps. */
+ * by stage and summed over steps: out[0] collide (bounds, pairs,
+ * narrowphase), out[1] prepare (islands, colouring, rows), out[2] the
+ * substep loop with restitution and store, out[3] continuous and sleep.
+ * `out` holds 4 floats. */
 M3GPU_API int32_t m3gpu_kernel_ms(float* out);
 
 /* Work counters of one world accumulated over its device steps:

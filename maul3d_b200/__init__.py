@@ -193,11 +193,17 @@ def image_bytes(world) -> int:
     return int(lib.m3gpu_world_image_bytes(world.id))
 
 
-def kernel_ms() -> tuple[float, float]:
-    """(collide, solve) device milliseconds of the last batched step call."""
-    out = (C.c_float * 2)()
+STAGES = ("collide", "prepare", "substep", "finish")
+
+
+def kernel_ms() -> dict[str, float]:
+    """Device milliseconds of the last batched step call per stage:
+    collide (bounds, pairs, narrowphase), prepare (islands, colouring,
+    rows), substep (the substep loop, restitution, store) and finish
+    (continuous, sleep), each summed over the call's steps."""
+    out = (C.c_float * len(STAGES))()
     _check(lib.m3gpu_kernel_ms(out))
-    return float(out[0]), float(out[1])
+    return {name: float(out[k]) for k, name in enumerate(STAGES)}
 
 
 PHASES = ("islands", "prepare", "colour+movers", "integrate_v", "warm_start", "bias_solve",

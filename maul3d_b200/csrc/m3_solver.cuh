@@ -113,19 +113,145 @@ __device__ __forceinline__ m3Vec3 m3VelocityAt(const m3WorldView& w, int32_t bod
     return m3Add3(v, m3Cross3(om, arm));
 }
 
+// ---------------------------------------------------------------------
+// Contact rows in HBM, field-major: word `field` of the row in solve
+// slot `slot` sits at base[field * stride + slot].  Slots are the solve
+// order (colour by colour), so the threads of a warp working through a
+// colour read consecutive words of every field: one 128-byte line per
+// field per warp instead of one line per thread.  The fields a pass
+// only reads (written once by the preparation kernel) are fetched
+// through the read-only path; the impulse accumulators sit in a second
+// array and are loaded into registers once per row and written back
+// once.
+// ---------------------------------------------------------------------
+#define M3C_BODY_A 0
+#define M3C_BODY_B 1
+#define M3C_MANIFOLD 2
+#define M3C_POINTS 3
+#define M3C_FLAGS 4 // bit 0: side A dynamic, bit 1: side B dynamic
+#define M3C_NORMAL 5
+#define M3C_T1 8
+#define M3C_T2 11
+#define M3C_ORIGIN_A 14
+#define M3C_ORIGIN_B 17
+#define M3C_K11 20
+#define M3C_K12 21
+#define M3C_K22 22
+#define M3C_TWIST_MASS 23
+#define M3C_TANGENT_V1 24
+#define M3C_TANGENT_V2 25
+#define M3C_FRICTION 26
+#define M3C_RESTITUTION 27
+#define M3C_INV_MASS_A 28
+#define M3C_INV_MASS_B 29
+#define M3C_INV_I_A 30
+#define M3C_INV_I_B 39
+#define M3C_SOFT 48 // biasRate, massScale, impulseScale
+#define M3C_ROLLING 51
+#define M3C_ROLLING_K 52
+#define M3C_POINT0 61 // per point: rA, rB, baseSeparation, normalMass, leverArm, relativeVelocity
+#define M3C_POINT_WORDS 10
+#define M3C_WORDS (M3C_POINT0 + M3C_POINT_WORDS * M3_MANIFOLD_MAX_POINTS)
+
+#define M3A_NORMAL 0 // per point
+#define M3A_TOTAL_NORMAL 4 // per point
+#define M3A_FRICTION1 8
+#define M3A_FRICTION2 9
+#define M3A_TWIST 10
+#define M3A_ROLLING 11
+#define M3A_WORDS 14
+
+struct m3ConRows
+{
+    float* ro;
+    float* acc;
+    int32_t stride;
+};
+
+// One row of m3ConRows.  f/n/v/m read prepared words through the
+// read-only data path: valid only in kernels that never write them.
+struct m3ConRef
+{
+    const float* ro;
+    float* acc;
+    int32_t stride;
+
+    __device__ __forceinline__ m3real f(int32_t k) const
+    {
+        return __ldg(ro + (int64_t)k * stride);
+    }
+    __device__ __forceinline__ int32_t n(int32_t k) const
+    {
+        return __ldg(reinterpret_cast<const int32_t*>(ro) + (int64_t)k * stride);
+    }
+    __device__ __forceinline__ m3Vec3 v(int32_t k) const
+    {
+        return v3(f(k), f(k + 1), f(k + 2));
+    }
+    __device__ __forceinline__ m3Mat3 m(int32_t k) const
+    {
+        m3Mat3 r;
+        r.cx = v(k);
+        r.cy = v(k + 3);
+        r.cz = v(k + 6);
+        return r;
+    }
+    __device__ __forceinline__ m3real& a(int32_t k) const
+    {
+        return acc[(int64_t)k * stride];
+    }
+};
+
+__device__ __forceinline__ m3ConRef m3ConAt(const m3ConRows& r, int32_t slot)
+{
+    m3ConRef c;
+    c.ro = r.ro + slot;
+    c.acc = r.acc + slot;
+    c.stride = r.stride;
+    return c;
+}
+
+// The two bodies of a row and their mass terms, loaded once per row.
+struct m3ConBodies
+{
+    int32_t a;
+    int32_t b;
+    bool dynA;
+    bool dynB;
+    m3real mA;
+    m3real mB;
+    m3Mat3 iA;
+    m3Mat3 iB;
+};
+
+__device__ __forceinline__ m3ConBodies m3LoadConBodies(const m3ConRef& c)
+{
+    m3ConBodies cb;
+    cb.a = c.n(M3C_BODY_A);
+    cb.b = c.n(M3C_BODY_B);
+    const int32_t flags = c.n(M3C_FLAGS);
+    cb.dynA = (flags & 1) != 0;
+    cb.dynB = (flags & 2) != 0;
+    cb.mA = c.f(M3C_INV_MASS_A);
+    cb.mB = c.f(M3C_INV_MASS_B);
+    cb.iA = c.m(M3C_INV_I_A);
+    cb.iB = c.m(M3C_INV_I_B);
+    return cb;
+}
+
 // solver.c:105-121
-__device__ __forceinline__ void m3ApplyImpulseDev(const m3WorldView& w, const m3ContactDev* c,
+__device__ __forceinline__ void m3ApplyImpulseRow(const m3WorldView& w, const m3ConBodies& cb,
                                                   m3Vec3 impulse, m3Vec3 rsA, m3Vec3 rsB)
 {
-    if (c->dynA)
+    if (cb.dynA)
     {
-        w.v[c->bodyA] = m3Sub3(w.v[c->bodyA], m3MulSV3(c->invMassA, impulse));
-        w.w[c->bodyA] = m3Sub3(w.w[c->bodyA], m3MulMV3(c->invIA, m3Cross3(rsA, impulse)));
+        w.v[cb.a] = m3Sub3(w.v[cb.a], m3MulSV3(cb.mA, impulse));
+        w.w[cb.a] = m3Sub3(w.w[cb.a], m3MulMV3(cb.iA, m3Cross3(rsA, impulse)));
     }
-    if (c->dynB)
+    if (cb.dynB)
     {
-        w.v[c->bodyB] = m3Add3(w.v[c->bodyB], m3MulSV3(c->invMassB, impulse));
-        w.w[c->bodyB] = m3Add3(w.w[c->bodyB], m3MulMV3(c->invIB, m3Cross3(rsB, impulse)));
+        w.v[cb.b] = m3Add3(w.v[cb.b], m3MulSV3(cb.mB, impulse));
+        w.w[cb.b] = m3Add3(w.w[cb.b], m3MulMV3(cb.iB, m3Cross3(rsB, impulse)));
     }
 }
 
@@ -249,80 +375,193 @@ __device__ void m3PrepareContact(const m3WorldView& w, m3ContactDev* c, int32_t 
     c->twistImpulse = manifold->twistImpulse;
 }
 
-// solver.c:408-428
-__device__ void m3WarmStartContact(const m3WorldView& w, m3ContactDev* c)
+// Writes a prepared row into its solve slot: every word a later pass
+// reads (points only below the point count, the rolling matrix only
+// when rolling resistance is positive) and the starting accumulators.
+__device__ void m3WriteContactRow(const m3ConRows& r, int32_t slot, const m3ContactDev& c)
 {
-    for (int32_t k = 0; k < c->pointCount; ++k)
+    float* ro = r.ro + slot;
+    float* acc = r.acc + slot;
+    const int64_t st = r.stride;
+    auto put = [&](int32_t k, m3real x) { ro[k * st] = x; };
+    auto putv = [&](int32_t k, m3Vec3 x) {
+        put(k, x.x);
+        put(k + 1, x.y);
+        put(k + 2, x.z);
+    };
+    auto putm = [&](int32_t k, const m3Mat3& x) {
+        putv(k, x.cx);
+        putv(k + 3, x.cy);
+        putv(k + 6, x.cz);
+    };
+    int32_t* ri = reinterpret_cast<int32_t*>(ro);
+    ri[M3C_BODY_A * st] = c.bodyA;
+    ri[M3C_BODY_B * st] = c.bodyB;
+    ri[M3C_MANIFOLD * st] = c.manifoldIndex;
+    ri[M3C_POINTS * st] = c.pointCount;
+    ri[M3C_FLAGS * st] = (c.dynA ? 1 : 0) | (c.dynB ? 2 : 0);
+    putv(M3C_NORMAL, c.normal);
+    putv(M3C_T1, c.t1);
+    putv(M3C_T2, c.t2);
+    putv(M3C_ORIGIN_A, c.originA);
+    putv(M3C_ORIGIN_B, c.originB);
+    put(M3C_K11, c.frictionK11);
+    put(M3C_K12, c.frictionK12);
+    put(M3C_K22, c.frictionK22);
+    put(M3C_TWIST_MASS, c.twistMass);
+    put(M3C_TANGENT_V1, c.tangentVelocity1);
+    put(M3C_TANGENT_V2, c.tangentVelocity2);
+    put(M3C_FRICTION, c.friction);
+    put(M3C_RESTITUTION, c.restitution);
+    put(M3C_INV_MASS_A, c.invMassA);
+    put(M3C_INV_MASS_B, c.invMassB);
+    putm(M3C_INV_I_A, c.invIA);
+    putm(M3C_INV_I_B, c.invIB);
+    put(M3C_SOFT, c.softness.biasRate);
+    put(M3C_SOFT + 1, c.softness.massScale);
+    put(M3C_SOFT + 2, c.softness.impulseScale);
+    put(M3C_ROLLING, c.rollingResistance);
+    if (c.rollingResistance > 0.0f)
     {
-        m3ConstraintPointDev* cp = &c->points[k];
-        m3ApplyImpulseDev(w, c, m3MulSV3(cp->normalImpulse, c->normal), cp->rA, cp->rB);
+        putm(M3C_ROLLING_K, c.rollingK);
     }
-    m3Vec3 f = m3Add3(m3MulSV3(c->frictionImpulse1, c->t1), m3MulSV3(c->frictionImpulse2, c->t2));
-    m3ApplyImpulseDev(w, c, f, c->originA, c->originB);
-    m3Vec3 tw = m3Add3(m3MulSV3(c->twistImpulse, c->normal), c->rollingImpulse);
-    if (c->dynA)
+    for (int32_t k = 0; k < c.pointCount; ++k)
     {
-        w.w[c->bodyA] = m3Sub3(w.w[c->bodyA], m3MulMV3(c->invIA, tw));
+        const int32_t p = M3C_POINT0 + M3C_POINT_WORDS * k;
+        const m3ConstraintPointDev& cp = c.points[k];
+        putv(p, cp.rA);
+        putv(p + 3, cp.rB);
+        put(p + 6, cp.baseSeparation);
+        put(p + 7, cp.normalMass);
+        put(p + 8, cp.leverArm);
+        put(p + 9, cp.relativeVelocity);
+        acc[(M3A_NORMAL + k) * st] = cp.normalImpulse;
+        acc[(M3A_TOTAL_NORMAL + k) * st] = cp.totalNormalImpulse;
     }
-    if (c->dynB)
+    acc[M3A_FRICTION1 * st] = c.frictionImpulse1;
+    acc[M3A_FRICTION2 * st] = c.frictionImpulse2;
+    acc[M3A_TWIST * st] = c.twistImpulse;
+    acc[M3A_ROLLING * st] = c.rollingImpulse.x;
+    acc[(M3A_ROLLING + 1) * st] = c.rollingImpulse.y;
+    acc[(M3A_ROLLING + 2) * st] = c.rollingImpulse.z;
+}
+
+// solver.c:408-428
+__device__ void m3WarmStartContact(const m3WorldView& w, const m3ConRef& c)
+{
+    const m3ConBodies cb = m3LoadConBodies(c);
+    const int32_t pc = c.n(M3C_POINTS);
+    const m3Vec3 normal = c.v(M3C_NORMAL);
+    m3real imp[M3_MANIFOLD_MAX_POINTS];
+#pragma unroll
+    for (int32_t k = 0; k < M3_MANIFOLD_MAX_POINTS; ++k)
     {
-        w.w[c->bodyB] = m3Add3(w.w[c->bodyB], m3MulMV3(c->invIB, tw));
+        imp[k] = k < pc ? c.a(M3A_NORMAL + k) : 0.0f;
+    }
+    const m3real f1 = c.a(M3A_FRICTION1);
+    const m3real f2 = c.a(M3A_FRICTION2);
+    const m3real twist = c.a(M3A_TWIST);
+    const m3Vec3 rolling = v3(c.a(M3A_ROLLING), c.a(M3A_ROLLING + 1), c.a(M3A_ROLLING + 2));
+#pragma unroll
+    for (int32_t k = 0; k < M3_MANIFOLD_MAX_POINTS; ++k)
+    {
+        if (k < pc)
+        {
+            const int32_t p = M3C_POINT0 + M3C_POINT_WORDS * k;
+            m3ApplyImpulseRow(w, cb, m3MulSV3(imp[k], normal), c.v(p), c.v(p + 3));
+        }
+    }
+    m3Vec3 f = m3Add3(m3MulSV3(f1, c.v(M3C_T1)), m3MulSV3(f2, c.v(M3C_T2)));
+    m3ApplyImpulseRow(w, cb, f, c.v(M3C_ORIGIN_A), c.v(M3C_ORIGIN_B));
+    m3Vec3 tw = m3Add3(m3MulSV3(twist, normal), rolling);
+    if (cb.dynA)
+    {
+        w.w[cb.a] = m3Sub3(w.w[cb.a], m3MulMV3(cb.iA, tw));
+    }
+    if (cb.dynB)
+    {
+        w.w[cb.b] = m3Add3(w.w[cb.b], m3MulMV3(cb.iB, tw));
     }
 }
 
 // solver.c:430-574
-__device__ void m3SolveContact(const m3WorldView& w, m3ContactDev* c, const m3Vec3* deltaPos,
+__device__ void m3SolveContact(const m3WorldView& w, const m3ConRef& c, const m3Vec3* deltaPos,
                                const m3Quat* deltaRot, m3real invH, m3real pushMaxSpeed,
                                bool useBias)
 {
+    const m3ConBodies cb = m3LoadConBodies(c);
+    const int32_t pc = c.n(M3C_POINTS);
+    const m3Vec3 normal = c.v(M3C_NORMAL);
+    m3real imp[M3_MANIFOLD_MAX_POINTS];
+    m3real tot[M3_MANIFOLD_MAX_POINTS];
+#pragma unroll
+    for (int32_t k = 0; k < M3_MANIFOLD_MAX_POINTS; ++k)
+    {
+        imp[k] = k < pc ? c.a(M3A_NORMAL + k) : 0.0f;
+        tot[k] = k < pc ? c.a(M3A_TOTAL_NORMAL + k) : 0.0f;
+    }
     m3real passNormal = 0.0f;
     m3real twistLimit = 0.0f;
-    const m3Quat qA = deltaRot[c->bodyA];
-    const m3Quat qB = deltaRot[c->bodyB];
-    const m3Vec3 dpA = deltaPos[c->bodyA];
-    const m3Vec3 dpB = deltaPos[c->bodyB];
-    for (int32_t k = 0; k < c->pointCount; ++k)
+    const m3Quat qA = deltaRot[cb.a];
+    const m3Quat qB = deltaRot[cb.b];
+    const m3Vec3 dpA = deltaPos[cb.a];
+    const m3Vec3 dpB = deltaPos[cb.b];
+#pragma unroll
+    for (int32_t k = 0; k < M3_MANIFOLD_MAX_POINTS; ++k)
     {
-        m3ConstraintPointDev* cp = &c->points[k];
-        m3Vec3 rsA = m3RotateVec3(qA, cp->rA);
-        m3Vec3 rsB = m3RotateVec3(qB, cp->rB);
-        m3Vec3 ds = m3Add3(m3Sub3(dpB, dpA), m3Sub3(rsB, rsA));
-        m3real s = cp->baseSeparation + m3Dot3(ds, c->normal);
-        m3real bias = 0.0f;
-        m3real massScale = 1.0f;
-        m3real impulseScale = 0.0f;
-        if (s > 0.0f)
+        if (k < pc)
         {
-            bias = s * invH;
+            const int32_t p = M3C_POINT0 + M3C_POINT_WORDS * k;
+            const m3Vec3 rA = c.v(p);
+            const m3Vec3 rB = c.v(p + 3);
+            m3Vec3 rsA = m3RotateVec3(qA, rA);
+            m3Vec3 rsB = m3RotateVec3(qB, rB);
+            m3Vec3 ds = m3Add3(m3Sub3(dpB, dpA), m3Sub3(rsB, rsA));
+            m3real s = c.f(p + 6) + m3Dot3(ds, normal);
+            m3real bias = 0.0f;
+            m3real massScale = 1.0f;
+            m3real impulseScale = 0.0f;
+            if (s > 0.0f)
+            {
+                bias = s * invH;
+            }
+            else if (useBias)
+            {
+                bias = m3MaxF(c.f(M3C_SOFT) * s, -pushMaxSpeed);
+                massScale = c.f(M3C_SOFT + 1);
+                impulseScale = c.f(M3C_SOFT + 2);
+            }
+            m3real vn = m3Dot3(m3Sub3(m3VelocityAt(w, cb.b, rB), m3VelocityAt(w, cb.a, rA)), normal);
+            m3real impulse = -c.f(p + 7) * massScale * (vn + bias) - impulseScale * imp[k];
+            m3real newImpulse = m3MaxF(imp[k] + impulse, 0.0f);
+            impulse = newImpulse - imp[k];
+            imp[k] = newImpulse;
+            tot[k] += newImpulse;
+            passNormal += newImpulse;
+            twistLimit += c.f(p + 8) * newImpulse;
+            m3ApplyImpulseRow(w, cb, m3MulSV3(impulse, normal), rA, rB);
         }
-        else if (useBias)
+    }
+#pragma unroll
+    for (int32_t k = 0; k < M3_MANIFOLD_MAX_POINTS; ++k)
+    {
+        if (k < pc)
         {
-            bias = m3MaxF(c->softness.biasRate * s, -pushMaxSpeed);
-            massScale = c->softness.massScale;
-            impulseScale = c->softness.impulseScale;
+            c.a(M3A_NORMAL + k) = imp[k];
+            c.a(M3A_TOTAL_NORMAL + k) = tot[k];
         }
-        m3real vn = m3Dot3(
-            m3Sub3(m3VelocityAt(w, c->bodyB, cp->rB), m3VelocityAt(w, c->bodyA, cp->rA)),
-            c->normal);
-        m3real impulse = -cp->normalMass * massScale * (vn + bias) - impulseScale * cp->normalImpulse;
-        m3real newImpulse = m3MaxF(cp->normalImpulse + impulse, 0.0f);
-        impulse = newImpulse - cp->normalImpulse;
-        cp->normalImpulse = newImpulse;
-        cp->totalNormalImpulse += newImpulse;
-        passNormal += newImpulse;
-        twistLimit += cp->leverArm * newImpulse;
-        m3ApplyImpulseDev(w, c, m3MulSV3(impulse, c->normal), cp->rA, cp->rB);
     }
     if (useBias)
     {
         return;
     }
+    const m3real friction = c.f(M3C_FRICTION);
     {
-        m3Vec3 wRel = m3Sub3(w.w[c->bodyB], w.w[c->bodyA]);
-        m3real twistSpeed = m3Dot3(c->normal, wRel);
-        m3real maxTwist = c->friction * twistLimit;
-        m3real delta = -c->twistMass * twistSpeed;
-        m3real oldTwist = c->twistImpulse;
+        m3Vec3 wRel = m3Sub3(w.w[cb.b], w.w[cb.a]);
+        m3real twistSpeed = m3Dot3(normal, wRel);
+        m3real maxTwist = friction * twistLimit;
+        m3real delta = -c.f(M3C_TWIST_MASS) * twistSpeed;
+        m3real oldTwist = c.a(M3A_TWIST);
         m3real newTwist = oldTwist + delta;
         if (newTwist < -maxTwist)
         {
@@ -333,44 +572,58 @@ __device__ void m3SolveContact(const m3WorldView& w, m3ContactDev* c, const m3Ve
             newTwist = maxTwist;
         }
         delta = newTwist - oldTwist;
-        c->twistImpulse = newTwist;
-        m3Vec3 tw = m3MulSV3(delta, c->normal);
-        if (c->dynA)
+        c.a(M3A_TWIST) = newTwist;
+        m3Vec3 tw = m3MulSV3(delta, normal);
+        if (cb.dynA)
         {
-            w.w[c->bodyA] = m3Sub3(w.w[c->bodyA], m3MulMV3(c->invIA, tw));
+            w.w[cb.a] = m3Sub3(w.w[cb.a], m3MulMV3(cb.iA, tw));
         }
-        if (c->dynB)
+        if (cb.dynB)
         {
-            w.w[c->bodyB] = m3Add3(w.w[c->bodyB], m3MulMV3(c->invIB, tw));
+            w.w[cb.b] = m3Add3(w.w[cb.b], m3MulMV3(cb.iB, tw));
         }
     }
-    if (c->rollingResistance > 0.0f)
+    const m3real rollingResistance = c.f(M3C_ROLLING);
+    if (rollingResistance > 0.0f)
     {
         // The reference writes both bodies here whatever their type
         // (solver.c:542-545); the step refuses worlds where that would
         // touch a non-dynamic body, so both sides are dynamic here.
-        m3Vec3 wRel = m3Sub3(w.w[c->bodyB], w.w[c->bodyA]);
-        m3Vec3 delta = m3MulSV3(-1.0f, m3Solve3(&c->rollingK, wRel));
-        m3Vec3 accum = m3Add3(c->rollingImpulse, delta);
-        m3real maxRoll = c->rollingResistance * passNormal;
+        const m3Mat3 rollingK = c.m(M3C_ROLLING_K);
+        const m3Vec3 rollingImpulse =
+            v3(c.a(M3A_ROLLING), c.a(M3A_ROLLING + 1), c.a(M3A_ROLLING + 2));
+        m3Vec3 wRel = m3Sub3(w.w[cb.b], w.w[cb.a]);
+        m3Vec3 delta = m3MulSV3(-1.0f, m3Solve3(&rollingK, wRel));
+        m3Vec3 accum = m3Add3(rollingImpulse, delta);
+        m3real maxRoll = rollingResistance * passNormal;
         m3real mag2 = m3Dot3(accum, accum);
         if (mag2 > maxRoll * maxRoll && mag2 > 0.0f)
         {
             accum = m3MulSV3(maxRoll / sqrtf(mag2), accum);
         }
-        delta = m3Sub3(accum, c->rollingImpulse);
-        c->rollingImpulse = accum;
-        w.w[c->bodyA] = m3Sub3(w.w[c->bodyA], m3MulMV3(c->invIA, delta));
-        w.w[c->bodyB] = m3Add3(w.w[c->bodyB], m3MulMV3(c->invIB, delta));
+        delta = m3Sub3(accum, rollingImpulse);
+        c.a(M3A_ROLLING) = accum.x;
+        c.a(M3A_ROLLING + 1) = accum.y;
+        c.a(M3A_ROLLING + 2) = accum.z;
+        w.w[cb.a] = m3Sub3(w.w[cb.a], m3MulMV3(cb.iA, delta));
+        w.w[cb.b] = m3Add3(w.w[cb.b], m3MulMV3(cb.iB, delta));
     }
     {
-        m3Vec3 vrel = m3Sub3(m3VelocityAt(w, c->bodyB, c->originB),
-                             m3VelocityAt(w, c->bodyA, c->originA));
-        m3real vt1 = m3Dot3(vrel, c->t1) - c->tangentVelocity1;
-        m3real vt2 = m3Dot3(vrel, c->t2) - c->tangentVelocity2;
-        m3real f1 = c->frictionImpulse1 - (c->frictionK11 * vt1 + c->frictionK12 * vt2);
-        m3real f2 = c->frictionImpulse2 - (c->frictionK12 * vt1 + c->frictionK22 * vt2);
-        m3real maxFriction = c->friction * passNormal;
+        const m3Vec3 t1 = c.v(M3C_T1);
+        const m3Vec3 t2 = c.v(M3C_T2);
+        const m3Vec3 originA = c.v(M3C_ORIGIN_A);
+        const m3Vec3 originB = c.v(M3C_ORIGIN_B);
+        const m3real k11 = c.f(M3C_K11);
+        const m3real k12 = c.f(M3C_K12);
+        const m3real k22 = c.f(M3C_K22);
+        const m3real oldF1 = c.a(M3A_FRICTION1);
+        const m3real oldF2 = c.a(M3A_FRICTION2);
+        m3Vec3 vrel = m3Sub3(m3VelocityAt(w, cb.b, originB), m3VelocityAt(w, cb.a, originA));
+        m3real vt1 = m3Dot3(vrel, t1) - c.f(M3C_TANGENT_V1);
+        m3real vt2 = m3Dot3(vrel, t2) - c.f(M3C_TANGENT_V2);
+        m3real f1 = oldF1 - (k11 * vt1 + k12 * vt2);
+        m3real f2 = oldF2 - (k12 * vt1 + k22 * vt2);
+        m3real maxFriction = friction * passNormal;
         m3real mag2 = f1 * f1 + f2 * f2;
         if (mag2 > maxFriction * maxFriction)
         {
@@ -379,52 +632,58 @@ __device__ void m3SolveContact(const m3WorldView& w, m3ContactDev* c, const m3Ve
             f1 *= scale;
             f2 *= scale;
         }
-        m3real d1 = f1 - c->frictionImpulse1;
-        m3real d2 = f2 - c->frictionImpulse2;
-        c->frictionImpulse1 = f1;
-        c->frictionImpulse2 = f2;
-        m3ApplyImpulseDev(w, c, m3Add3(m3MulSV3(d1, c->t1), m3MulSV3(d2, c->t2)), c->originA,
-                          c->originB);
+        m3real d1 = f1 - oldF1;
+        m3real d2 = f2 - oldF2;
+        c.a(M3A_FRICTION1) = f1;
+        c.a(M3A_FRICTION2) = f2;
+        m3ApplyImpulseRow(w, cb, m3Add3(m3MulSV3(d1, t1), m3MulSV3(d2, t2)), originA, originB);
     }
 }
 
 // solver.c:2879-2906 (one constraint's points, in order).
-__device__ void m3RestituteContact(const m3WorldView& w, m3ContactDev* c, m3real threshold)
+__device__ void m3RestituteContact(const m3WorldView& w, const m3ConRef& c, m3real threshold)
 {
-    if (c->restitution == 0.0f)
+    const m3real restitution = c.f(M3C_RESTITUTION);
+    if (restitution == 0.0f)
     {
         return;
     }
-    for (int32_t k = 0; k < c->pointCount; ++k)
+    const m3ConBodies cb = m3LoadConBodies(c);
+    const int32_t pc = c.n(M3C_POINTS);
+    const m3Vec3 normal = c.v(M3C_NORMAL);
+    for (int32_t k = 0; k < pc; ++k)
     {
-        m3ConstraintPointDev* cp = &c->points[k];
-        if (cp->relativeVelocity > -threshold || cp->totalNormalImpulse == 0.0f)
+        const int32_t p = M3C_POINT0 + M3C_POINT_WORDS * k;
+        const m3real relativeVelocity = c.f(p + 9);
+        if (relativeVelocity > -threshold || c.a(M3A_TOTAL_NORMAL + k) == 0.0f)
         {
             continue;
         }
-        m3real vn = m3Dot3(
-            m3Sub3(m3VelocityAt(w, c->bodyB, cp->rB), m3VelocityAt(w, c->bodyA, cp->rA)),
-            c->normal);
-        m3real impulse = -cp->normalMass * (vn + c->restitution * cp->relativeVelocity);
-        m3real newImpulse = m3MaxF(cp->normalImpulse + impulse, 0.0f);
-        impulse = newImpulse - cp->normalImpulse;
-        cp->normalImpulse = newImpulse;
-        m3ApplyImpulseDev(w, c, m3MulSV3(impulse, c->normal), cp->rA, cp->rB);
+        const m3Vec3 rA = c.v(p);
+        const m3Vec3 rB = c.v(p + 3);
+        m3real vn = m3Dot3(m3Sub3(m3VelocityAt(w, cb.b, rB), m3VelocityAt(w, cb.a, rA)), normal);
+        m3real impulse = -c.f(p + 7) * (vn + restitution * relativeVelocity);
+        const m3real old = c.a(M3A_NORMAL + k);
+        m3real newImpulse = m3MaxF(old + impulse, 0.0f);
+        impulse = newImpulse - old;
+        c.a(M3A_NORMAL + k) = newImpulse;
+        m3ApplyImpulseRow(w, cb, m3MulSV3(impulse, normal), rA, rB);
     }
 }
 
 // solver.c:2979-3039 without the hit-event stream (observer only).
-__device__ void m3StoreContact(const m3ContactDev* c, m3Manifold* manifolds)
+__device__ void m3StoreContact(const m3ConRef& c, m3Manifold* manifolds)
 {
-    m3Manifold* manifold = &manifolds[c->manifoldIndex];
-    for (int32_t k = 0; k < c->pointCount; ++k)
+    m3Manifold* manifold = &manifolds[c.n(M3C_MANIFOLD)];
+    const int32_t pc = c.n(M3C_POINTS);
+    for (int32_t k = 0; k < pc; ++k)
     {
-        manifold->points[k].normalImpulse = c->points[k].normalImpulse;
+        manifold->points[k].normalImpulse = c.a(M3A_NORMAL + k);
     }
-    manifold->frictionImpulse =
-        m3Add3(m3MulSV3(c->frictionImpulse1, c->t1), m3MulSV3(c->frictionImpulse2, c->t2));
-    manifold->twistImpulse = c->twistImpulse;
-    manifold->rollingImpulse = c->rollingImpulse;
+    manifold->frictionImpulse = m3Add3(m3MulSV3(c.a(M3A_FRICTION1), c.v(M3C_T1)),
+                                       m3MulSV3(c.a(M3A_FRICTION2), c.v(M3C_T2)));
+    manifold->twistImpulse = c.a(M3A_TWIST);
+    manifold->rollingImpulse = v3(c.a(M3A_ROLLING), c.a(M3A_ROLLING + 1), c.a(M3A_ROLLING + 2));
 }
 
 // Implicit gyroscopic step, one Newton iteration in body coordinates,

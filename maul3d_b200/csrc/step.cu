@@ -1,14 +1,22 @@
 // The device step: m3StepInternal (src/solver.c:3662-4320) for a batch
 // of independent worlds, one thread block per world.
 //
-// Two kernels per step, each a grid of one block per world:
-//   m3CollideKernel  fresh bounds, the canonical pair list, and the
-//                    narrowphase with the warm-start carry;
-//   m3SolveKernel    islands and wake, contact preparation, graph
-//                    colouring, the substep loop (integrate, warm start,
-//                    colour-by-colour solve, integrate positions, relax),
-//                    restitution and store, the continuous pass against
-//                    planes, the sleep pass and the step counter.
+// Six launches per step:
+//   m3BroadKernel        one block per world: fresh bounds, sort-and-sweep
+//                        and the canonical (sorted) pair list;
+//   m3PairOffsetsKernel  prefix of the worlds' pair counts;
+//   m3NarrowKernel       one thread per pair of the whole batch: the
+//                        narrowphase with the warm-start carry;
+//   m3PrepareKernel      one block per world: islands and wake, contact
+//                        selection, graph colouring, contact rows written
+//                        into their solve slots, joint rows and their
+//                        dependency levels, movers;
+//   m3SubstepKernel      one block per world: the substep loop (integrate,
+//                        warm start, colour-by-colour solve, integrate
+//                        positions, relax) with body velocities in shared
+//                        memory, restitution and the impulse store;
+//   m3FinishKernel       one block per world: the continuous pass against
+//                        planes, the sleep pass and the step counter.
 // Block barriers separate every dependent phase, so inside a world the
 // order of every write is the reference's; across worlds nothing is
 // shared.  Worlds are ordered largest first so the long worlds start
@@ -16,8 +24,9 @@
 //
 // Refusals: a world that needs something this path does not implement
 // (a pair family, rolling resistance on a static contact, a bullet, a
-// breakable joint, ...) or whose pair list would exceed its capacity is
-// left unstepped with its status word set; the host reports it.
+// breakable joint, ...) or whose pair list would exceed its capacity gets
+// its status word set and is skipped by every later kernel; the host
+// reports it and the world stays failed.
 
 #include "m3_world.h"
 #include "m3_hash.h"
@@ -70,6 +79,17 @@ struct m3Aabb
     double hi[3];
 };
 
+// What the preparation kernel hands the substep and finish kernels.
+struct m3StepPlan
+{
+    int32_t constraintCount;
+    int32_t jointCount;
+    int32_t jointLevels;
+    int32_t moverCount;
+    int32_t anyRestitution;
+    int32_t starts[M3_GRAPH_COLORS + 2]; // colour offsets into the solve slots
+};
+
 struct m3Scratch
 {
     m3Aabb* aabb;          // per shape
@@ -89,7 +109,10 @@ struct m3Scratch
     int32_t* movers;       // per body
     int32_t* moverFlag;    // per body
     uint32_t* bodyMask;    // per body
-    m3ContactDev* cons;    // per pair
+    m3StepPlan* plan;      // counts and offsets handed between the step kernels
+    m3ConRows rows;        // contact rows, field-major, one slot per constraint
+    int32_t* conPairIndex; // per constraint: its pair
+    int32_t* conSlot;      // per constraint: its solve slot
     int32_t* pairFlag;     // per pair (compaction)
     uint8_t* colors;       // per pair
     int2* conPair;         // per pair: colouring body pair
@@ -140,7 +163,16 @@ static __host__ __device__ inline int64_t ScratchCarve(m3Scratch* s, uint8_t* ba
     M3_CARVE(movers, int32_t, bodyCap)
     M3_CARVE(moverFlag, int32_t, bodyCap + 1)
     M3_CARVE(bodyMask, uint32_t, bodyCap)
-    M3_CARVE(cons, m3ContactDev, pairCap)
+    M3_CARVE(plan, m3StepPlan, 1)
+    const int32_t rowStride = (int32_t)m3AlignUp(pairCap, 32);
+    if (s)
+    {
+        s->rows.stride = rowStride;
+    }
+    M3_CARVE(rows.ro, float, (int64_t)M3C_WORDS * rowStride)
+    M3_CARVE(rows.acc, float, (int64_t)M3A_WORDS * rowStride)
+    M3_CARVE(conPairIndex, int32_t, pairCap)
+    M3_CARVE(conSlot, int32_t, pairCap)
     M3_CARVE(pairFlag, int32_t, pairCap + 1)
     M3_CARVE(colors, uint8_t, pairCap)
     M3_CARVE(conPair, int2, pairCap)
@@ -890,16 +922,17 @@ __device__ void ContinuousVersusPlane(const m3WorldView& w, int32_t body, int32_
 }
 
 // ---------------------------------------------------------------------
-// Kernel 2: islands, prepare, colour, substeps, store, continuous, sleep
+// Kernel 2: islands and wake, contact selection, colouring, row
+// preparation, joint rows and their levels, movers
 // ---------------------------------------------------------------------
 // Shared-memory bytes per body of the substep-loop cache: v, w, the
 // position delta (12 B each) and the rotation delta (16 B).
 #define M3_BODY_CACHE_BYTES 52
 
-__global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* views,
-                                                          const int32_t* order, int32_t count,
-                                                          float dt, int32_t substeps,
-                                                          int32_t cacheBytes)
+__global__ void __launch_bounds__(M3_BLOCK) m3PrepareKernel(const m3WorldView* views,
+                                                            const int32_t* order, int32_t count,
+                                                            float dt, int32_t substeps,
+                                                            int32_t cacheBytes)
 {
     const int32_t wi = order[blockIdx.x];
     const m3WorldView& w = views[wi];
@@ -930,7 +963,6 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
     }
     long long t_phase = clock64();
     const int32_t bodyMax = sc->bodyMax;
-    const int32_t shapeMax = sc->shapeMax;
     const int32_t jointMax = sc->jointMax;
     const int32_t pairCount = sc->pairCount;
     const uint64_t* keys = sc->pairBuf == 0 ? w.keys0 : w.keys1;
@@ -1016,7 +1048,6 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
     M3_PHASE_MARK(M3_PHASE_ISLANDS)
     // Contact selection and preparation (solver.c:156-405).
     const m3real h = dt / (m3real)substeps;
-    const m3real invH = h > 0.0f ? 1.0f / h : 0.0f;
     const m3SoftDev soft = m3MakeSoft(sc->contactHertz, sc->contactDampingRatio, h);
     const m3SoftDev staticSoft = m3MakeSoft(2.0f * sc->contactHertz, sc->contactDampingRatio, h);
     for (int32_t k = tid; k < pairCount; k += M3_BLOCK)
@@ -1043,20 +1074,9 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
     for (int32_t k = tid; k < pairCount; k += M3_BLOCK)
     {
         int32_t next = k + 1 < pairCount ? s.pairFlag[k + 1] : constraintCount;
-        if (next == s.pairFlag[k])
+        if (next != s.pairFlag[k])
         {
-            continue; // not selected
-        }
-        m3ContactDev* c = &s.cons[s.pairFlag[k]];
-        m3PrepareContact(w, c, k, keys, man, soft, staticSoft);
-        if (c->restitution != 0.0f)
-        {
-            s_anyRestitution = 1;
-        }
-        if (c->rollingResistance > 0.0f && (!c->dynA || !c->dynB))
-        {
-            s_status = M3GPU_ERR_UNSUPPORTED;
-            sc->statusDetail = 2001;
+            s.conPairIndex[s.pairFlag[k]] = k;
         }
     }
     // Joint rows (solver.c:699-1042): selection in slot order, rows
@@ -1172,9 +1192,11 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
     }
     for (int32_t i = tid; i < constraintCount; i += M3_BLOCK)
     {
-        const m3ContactDev* c = &s.cons[i];
-        int32_t a = c->dynA && w.awake[c->bodyA] ? c->bodyA : -1;
-        int32_t b = c->dynB && w.awake[c->bodyB] ? c->bodyB : -1;
+        const uint64_t key = keys[s.conPairIndex[i]];
+        const int32_t bodyA = w.shapeBody[(int32_t)(key >> 32)];
+        const int32_t bodyB = w.shapeBody[(int32_t)(key & 0xFFFFFFFFu)];
+        int32_t a = w.btype[bodyA] == M3_BODY_DYNAMIC && w.awake[bodyA] ? bodyA : -1;
+        int32_t b = w.btype[bodyB] == M3_BODY_DYNAMIC && w.awake[bodyB] ? bodyB : -1;
         cPair[i] = make_int2(a, b);
     }
     __syncthreads();
@@ -1223,11 +1245,42 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
         }
         for (int32_t i = 0; i < constraintCount; ++i)
         {
-            s.lists[fill[cColor[i]]++] = i;
+            const int32_t slot = fill[cColor[i]]++;
+            s.lists[slot] = i;
+            s.conSlot[i] = slot;
         }
         sc->lastColorCount = used;
         sc->constraintCount = constraintCount;
     }
+    __syncthreads();
+    M3_PHASE_MARK(M3_PHASE_COLOR)
+    // Contact rows (solver.c:261-405), prepared straight into their
+    // solve slots; consecutive threads write consecutive slots.
+    for (int32_t slot = tid; slot < constraintCount; slot += M3_BLOCK)
+    {
+        m3ContactDev c;
+        m3PrepareContact(w, &c, s.conPairIndex[s.lists[slot]], keys, man, soft, staticSoft);
+        m3WriteContactRow(s.rows, slot, c);
+        if (c.restitution != 0.0f)
+        {
+            s_anyRestitution = 1;
+        }
+        if (c.rollingResistance > 0.0f && (!c.dynA || !c.dynB))
+        {
+            s_status = M3GPU_ERR_UNSUPPORTED;
+            sc->statusDetail = 2001;
+        }
+    }
+    __syncthreads();
+    if (s_status != 0)
+    {
+        if (tid == 0)
+        {
+            sc->status = s_status;
+        }
+        return;
+    }
+    M3_PHASE_MARK(M3_PHASE_PREPARE)
 
     // Movers: alive, enabled, kinematic or awake dynamic, ascending
     // (solver.c:3945-3983), with the kinematic servo.
@@ -1272,7 +1325,54 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
     }
     __syncthreads();
     M3_PHASE_MARK(M3_PHASE_COLOR)
-    const int32_t jointLevels = s_jointLevels;
+    if (tid == 0)
+    {
+        m3StepPlan* plan = s.plan;
+        plan->constraintCount = constraintCount;
+        plan->jointCount = sc->jointConstraintCount;
+        plan->jointLevels = s_jointLevels;
+        plan->moverCount = moverCount;
+        plan->anyRestitution = s_anyRestitution;
+        for (int32_t c = 0; c < M3_GRAPH_COLORS + 2; ++c)
+        {
+            plan->starts[c] = s_starts[c];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------
+// Kernel 3: the substep loop, restitution and the impulse store
+// ---------------------------------------------------------------------
+__global__ void __launch_bounds__(M3_BLOCK, 2) m3SubstepKernel(const m3WorldView* views,
+                                                            const int32_t* order, int32_t count,
+                                                            float dt, int32_t substeps,
+                                                            int32_t cacheBytes)
+{
+    const int32_t wi = order[blockIdx.x];
+    const m3WorldView& w = views[wi];
+    m3WorldScalars* sc = w.sc;
+    if (sc->status != 0)
+    {
+        return;
+    }
+    long long t_phase = clock64();
+    m3Scratch s;
+    ScratchCarve(&s, w.scratch, sc->bodyCap, sc->shapeCap, sc->jointCap, sc->pairCap);
+    const int32_t tid = threadIdx.x;
+    __shared__ int32_t s_starts[M3_GRAPH_COLORS + 2];
+    if (tid < M3_GRAPH_COLORS + 2)
+    {
+        s_starts[tid] = s.plan->starts[tid];
+    }
+    const int32_t bodyMax = sc->bodyMax;
+    const int32_t constraintCount = s.plan->constraintCount;
+    const int32_t jointCount = s.plan->jointCount;
+    const int32_t jointLevels = s.plan->jointLevels;
+    const int32_t moverCount = s.plan->moverCount;
+    const bool anyRestitution = s.plan->anyRestitution != 0;
+    m3Manifold* man = sc->pairBuf == 0 ? w.man0 : w.man1;
+    const m3real h = dt / (m3real)substeps;
+    const m3real invH = h > 0.0f ? 1.0f / h : 0.0f;
     const m3real pushMax = sc->contactPushMaxSpeed;
 
     // Body velocities and the substep deltas live in shared memory for
@@ -1337,7 +1437,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
             }
             for (int32_t k = a + tid; k < b; k += M3_BLOCK)
             {
-                m3WarmStartContact(wl, &s.cons[s.lists[k]]);
+                m3WarmStartContact(wl, m3ConAt(s.rows, k));
             }
             __syncthreads();
         }
@@ -1345,7 +1445,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
         {
             for (int32_t k = s_starts[M3_GRAPH_COLORS]; k < s_starts[M3_GRAPH_COLORS + 1]; ++k)
             {
-                m3WarmStartContact(wl, &s.cons[s.lists[k]]);
+                m3WarmStartContact(wl, m3ConAt(s.rows, k));
             }
         }
         __syncthreads();
@@ -1369,7 +1469,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
             }
             for (int32_t k = a + tid; k < b; k += M3_BLOCK)
             {
-                m3SolveContact(wl, &s.cons[s.lists[k]], dP, dQ, invH, pushMax, true);
+                m3SolveContact(wl, m3ConAt(s.rows, k), dP, dQ, invH, pushMax, true);
             }
             __syncthreads();
         }
@@ -1377,7 +1477,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
         {
             for (int32_t k = s_starts[M3_GRAPH_COLORS]; k < s_starts[M3_GRAPH_COLORS + 1]; ++k)
             {
-                m3SolveContact(wl, &s.cons[s.lists[k]], dP, dQ, invH, pushMax, true);
+                m3SolveContact(wl, m3ConAt(s.rows, k), dP, dQ, invH, pushMax, true);
             }
         }
         __syncthreads();
@@ -1407,7 +1507,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
             }
             for (int32_t k = a + tid; k < b; k += M3_BLOCK)
             {
-                m3SolveContact(wl, &s.cons[s.lists[k]], dP, dQ, invH, pushMax,
+                m3SolveContact(wl, m3ConAt(s.rows, k), dP, dQ, invH, pushMax,
                                false);
             }
             __syncthreads();
@@ -1416,7 +1516,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
         {
             for (int32_t k = s_starts[M3_GRAPH_COLORS]; k < s_starts[M3_GRAPH_COLORS + 1]; ++k)
             {
-                m3SolveContact(wl, &s.cons[s.lists[k]], dP, dQ, invH, pushMax,
+                m3SolveContact(wl, m3ConAt(s.rows, k), dP, dQ, invH, pushMax,
                                false);
             }
         }
@@ -1432,12 +1532,12 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
         w.torque[i] = v3(0.0f, 0.0f, 0.0f);
     }
     // Restitution is serial in constraint order (solver.c:2879-2906).
-    if (tid == 0 && s_anyRestitution)
+    if (tid == 0 && anyRestitution)
     {
         const m3real threshold = sc->restitutionThreshold;
         for (int32_t i = 0; i < constraintCount; ++i)
         {
-            m3RestituteContact(wl, &s.cons[i], threshold);
+            m3RestituteContact(wl, m3ConAt(s.rows, s.conSlot[i]), threshold);
         }
     }
     __syncthreads();
@@ -1452,7 +1552,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
     __syncthreads();
     for (int32_t i = tid; i < constraintCount; i += M3_BLOCK)
     {
-        m3StoreContact(&s.cons[i], man);
+        m3StoreContact(m3ConAt(s.rows, i), man);
     }
     for (int32_t r = tid; r < jointCount; r += M3_BLOCK)
     {
@@ -1472,9 +1572,38 @@ __global__ void __launch_bounds__(M3_BLOCK) m3SolveKernel(const m3WorldView* vie
             }
         }
     }
-    __syncthreads();
-
     M3_PHASE_MARK(M3_PHASE_STORE)
+}
+
+// ---------------------------------------------------------------------
+// Kernel 4: continuous collision against planes and the sleep pass
+// ---------------------------------------------------------------------
+__global__ void __launch_bounds__(M3_BLOCK) m3FinishKernel(const m3WorldView* views,
+                                                           const int32_t* order, int32_t count,
+                                                           float dt, int32_t substeps)
+{
+    const int32_t wi = order[blockIdx.x];
+    const m3WorldView& w = views[wi];
+    m3WorldScalars* sc = w.sc;
+    if (sc->status != 0)
+    {
+        return;
+    }
+    long long t_phase = clock64();
+    m3Scratch s;
+    ScratchCarve(&s, w.scratch, sc->bodyCap, sc->shapeCap, sc->jointCap, sc->pairCap);
+    const int32_t tid = threadIdx.x;
+    __shared__ int32_t s_status;
+    if (tid == 0)
+    {
+        s_status = 0;
+    }
+    __syncthreads();
+    const int32_t bodyMax = sc->bodyMax;
+    const int32_t shapeMax = sc->shapeMax;
+    const int32_t pairCount = sc->pairCount;
+    const int32_t constraintCount = s.plan->constraintCount;
+    const int32_t moverCount = s.plan->moverCount;
     // Continuous phase (solver.c:3349-3425).  A non-bullet fast body
     // sweeps only against static targets, and a pull-back moves only the
     // fast body itself, so bodies are independent and run in parallel.
@@ -1839,14 +1968,45 @@ static int32_t PrepareBatch(m3HostWorld** worlds, int32_t count)
     s_batch.cacheBytes = (int32_t)(want < limit ? want : limit);
     if (s_batch.cacheBytes > 48 * 1024)
     {
-        rc = Check(cudaFuncSetAttribute(m3SolveKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        rc = Check(cudaFuncSetAttribute(m3PrepareKernel,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         s_batch.cacheBytes),
-                   "cudaFuncSetAttribute(solve smem)");
+                   "cudaFuncSetAttribute(prepare smem)");
+        if (rc == M3GPU_OK)
+        {
+            rc = Check(cudaFuncSetAttribute(m3SubstepKernel,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            s_batch.cacheBytes),
+                       "cudaFuncSetAttribute(substep smem)");
+        }
     }
     return rc;
 }
 
-static float s_kernelMs[2] = {0.0f, 0.0f};
+// The three per-world solve kernels of one step, in order on the current
+// stream.  `marks`, when given, receives an event after the first two.
+static void LaunchSolve(const m3WorldView* views, const int32_t* order, int32_t count, float dt,
+                        int32_t substeps, int32_t cacheBytes, const cudaEvent_t* marks)
+{
+    m3PrepareKernel<<<count, M3_BLOCK, cacheBytes>>>(views, order, count, dt, substeps,
+                                                     cacheBytes);
+    if (marks != nullptr)
+    {
+        cudaEventRecord(marks[0]);
+    }
+    m3SubstepKernel<<<count, M3_BLOCK, cacheBytes>>>(views, order, count, dt, substeps,
+                                                     cacheBytes);
+    if (marks != nullptr)
+    {
+        cudaEventRecord(marks[1]);
+    }
+    m3FinishKernel<<<count, M3_BLOCK>>>(views, order, count, dt, substeps);
+}
+
+// Device milliseconds of the last batched call per stage: collide
+// (bounds, pairs, narrowphase), prepare, substeps, finish.
+#define M3_STAGES 4
+static float s_kernelMs[M3_STAGES] = {0.0f, 0.0f, 0.0f, 0.0f};
 // Narrowphase grid: enough 128-thread blocks to fill every SM several
 // times; the kernel strides over the batch's flattened pairs.
 static int32_t s_narrowGrid = 148 * 16;
@@ -1859,8 +2019,10 @@ extern "C" int32_t m3gpu_kernel_ms(float* out)
     {
         return m3gpuSetError(M3GPU_ERR_INVALID, "null output");
     }
-    out[0] = s_kernelMs[0];
-    out[1] = s_kernelMs[1];
+    for (int32_t k = 0; k < M3_STAGES; ++k)
+    {
+        out[k] = s_kernelMs[k];
+    }
     return M3GPU_OK;
 }
 
@@ -1914,9 +2076,10 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
     {
         return rc;
     }
-    // One event before the batch and one after each kernel, so the two
-    // kernels' device times are separable.
-    size_t needEvents = (size_t)(2 * steps + 1);
+    // Events: one before the batch, then per step one after the collide
+    // kernels and one after each solve kernel, so the stages' device
+    // times are separable.
+    size_t needEvents = (size_t)(M3_STAGES * steps + 1);
     while (s_events.size() < needEvents)
     {
         cudaEvent_t e;
@@ -1938,15 +2101,15 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
     cudaEventRecord(s_events[0]);
     for (int32_t step = 0; step < steps; ++step)
     {
+        const cudaEvent_t* ev = &s_events[(size_t)(M3_STAGES * step)];
         m3BroadKernel<<<count, M3_BLOCK>>>(s_batch.dviews, s_batch.dorder, count);
         m3PairOffsetsKernel<<<1, M3_BLOCK>>>(s_batch.dviews, count, s_batch.doffsets);
         m3NarrowKernel<<<s_narrowGrid, 128>>>(s_batch.dviews, s_batch.doffsets, count);
-        cudaEventRecord(s_events[(size_t)(2 * step + 1)]);
-        m3SolveKernel<<<count, M3_BLOCK, s_batch.cacheBytes>>>(s_batch.dviews, s_batch.dorder,
-                                                               count, dt, substeps,
-                                                               s_batch.cacheBytes);
-        cudaEventRecord(s_events[(size_t)(2 * step + 2)]);
-        s_launches += 4;
+        cudaEventRecord(ev[1]);
+        LaunchSolve(s_batch.dviews, s_batch.dorder, count, dt, substeps, s_batch.cacheBytes,
+                    ev + 2);
+        cudaEventRecord(ev[4]);
+        s_launches += 6;
     }
     cudaMemsetAsync(s_dstatus, 0, sizeof(int32_t));
     m3StatusKernel<<<(count + 255) / 256, 256>>>(s_batch.dviews, count, s_dstatus);
@@ -1967,21 +2130,22 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
         return rc;
     }
     float total = 0.0f;
-    float collide = 0.0f;
-    float solve = 0.0f;
-    cudaEventElapsedTime(&total, s_events[0], s_events[(size_t)(2 * steps)]);
+    cudaEventElapsedTime(&total, s_events[0], s_events[(size_t)(M3_STAGES * steps)]);
+    for (int32_t k = 0; k < M3_STAGES; ++k)
+    {
+        s_kernelMs[k] = 0.0f;
+    }
     for (int32_t step = 0; step < steps; ++step)
     {
-        float a = 0.0f;
-        float b = 0.0f;
-        cudaEventElapsedTime(&a, s_events[(size_t)(2 * step)], s_events[(size_t)(2 * step + 1)]);
-        cudaEventElapsedTime(&b, s_events[(size_t)(2 * step + 1)], s_events[(size_t)(2 * step + 2)]);
-        collide += a;
-        solve += b;
+        const cudaEvent_t* ev = &s_events[(size_t)(M3_STAGES * step)];
+        for (int32_t k = 0; k < M3_STAGES; ++k)
+        {
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+            s_kernelMs[k] += ms;
+        }
     }
     s_lastStepMs = total;
-    s_kernelMs[0] = collide;
-    s_kernelMs[1] = solve;
     if (status != 0)
     {
         // Name the first refusing world and its detail code.
@@ -2159,8 +2323,8 @@ extern "C" int32_t m3gpu_step_world_noalloc(m3WorldId worldId, float dt, int32_t
     m3BroadKernel<<<1, M3_BLOCK>>>(sym.view, order, 1);
     m3PairOffsetsKernel<<<1, M3_BLOCK>>>(sym.view, 1, offsets);
     m3NarrowKernel<<<148, 128>>>(sym.view, offsets, 1);
-    m3SolveKernel<<<1, M3_BLOCK, cacheBytes>>>(sym.view, order, 1, dt, substeps, cacheBytes);
-    s_launches += 4;
+    LaunchSolve(sym.view, order, 1, dt, substeps, cacheBytes, nullptr);
+    s_launches += 6;
     rc = Check(cudaGetLastError(), "noalloc step launch");
     int32_t status = 0;
     if (rc == M3GPU_OK)
