@@ -396,15 +396,23 @@ def main() -> None:
     if not args.no_e2e:
         eworlds = build_worlds(m3, sizes, rank_seed)
         m3.reserve_worlds(eworlds)
-        h2d = sum(m3.image_bytes(w) for w in eworlds)
+        up0 = m3.uploaded_bytes()
         if world_size > 1:
             dist.barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         m3.upload_worlds(eworlds)
+        t1 = time.perf_counter()
+        h2d = m3.uploaded_bytes() - up0
+        step_s = 0.0
+        hash_s = 0.0
         for _ in range(args.steps):
+            ta = time.perf_counter()
             m3.step_worlds(eworlds, DT, args.substeps, 1)
+            tb = time.perf_counter()
             m3.hash_worlds(eworlds)
+            step_s += tb - ta
+            hash_s += time.perf_counter() - tb
         torch.cuda.synchronize()
         e2e_s = time.perf_counter() - t0
         if world_size > 1:
@@ -414,6 +422,9 @@ def main() -> None:
         e2e = {"value": total_bs / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": int(h2d // args.steps),
                "d2h_bytes_per_step": 8 * len(eworlds),
+               "upload_ms": (t1 - t0) * 1e3,
+               "step_ms_per_step": step_s * 1e3 / args.steps,
+               "hash_ms_per_step": hash_s * 1e3 / args.steps,
                "note": "world images uploaded once inside the timed region (pageable host "
                        "memory); per step: batched step + device hash of every world read back"}
         for w in eworlds:

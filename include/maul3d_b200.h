@@ -284,8 +284,13 @@ M3GPU_API int32_t m3gpu_reserve_worlds(const m3WorldId* worlds, int32_t count);
  * whose device copy is already current are skipped). */
 M3GPU_API int32_t m3gpu_upload_worlds(const m3WorldId* worlds, int32_t count);
 
-/* Bytes one world's host image occupies (what an upload copies). */
+/* Bytes one world's host image occupies (an upload copies the part
+ * before the pair buffers, the current pair list and the hulls). */
 M3GPU_API int64_t m3gpu_world_image_bytes(m3WorldId world);
+
+/* Host-to-device bytes copied by world uploads since the library was
+ * loaded. */
+M3GPU_API int64_t m3gpu_uploaded_bytes(void);
 
 /* Allocation-free step of one resident world (no reference counterpart).
  * For callers that must not allocate device memory when they step: a

@@ -65,6 +65,8 @@ def _load() -> C.CDLL:
         getattr(lib, name).restype = C.c_int32
     lib.m3gpu_world_image_bytes.argtypes = [m3WorldId]
     lib.m3gpu_world_image_bytes.restype = C.c_int64
+    lib.m3gpu_uploaded_bytes.argtypes = []
+    lib.m3gpu_uploaded_bytes.restype = C.c_int64
     lib.m3gpu_kernel_ms.argtypes = [C.POINTER(C.c_float)]
     lib.m3gpu_kernel_ms.restype = C.c_int32
     lib.m3gpu_world_stats.argtypes = [m3WorldId, C.POINTER(C.c_uint64)]
@@ -191,6 +193,11 @@ def upload_worlds(worlds) -> None:
 
 def image_bytes(world) -> int:
     return int(lib.m3gpu_world_image_bytes(world.id))
+
+
+def uploaded_bytes() -> int:
+    """Host-to-device bytes copied by world uploads so far."""
+    return int(lib.m3gpu_uploaded_bytes())
 
 
 STAGES = ("collide", "prepare", "substep", "finish")

@@ -256,6 +256,11 @@ extern "C" int32_t m3gpu_upload_worlds(const m3WorldId* worlds, int32_t count)
     return rc;
 }
 
+extern "C" int64_t m3gpu_uploaded_bytes(void)
+{
+    return g_m3UploadedBytes;
+}
+
 extern "C" int64_t m3gpu_world_image_bytes(m3WorldId world)
 {
     m3HostWorld* w = m3gpuWorldFromId(world);

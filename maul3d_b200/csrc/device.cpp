@@ -19,6 +19,7 @@ static int s_device = 0;
 // pool allocated, released): cached device views of a batch are valid
 // only for the epoch they were built in.
 uint64_t g_m3ResidencyEpoch = 1;
+int64_t g_m3UploadedBytes = 0;
 
 extern "C" int32_t m3gpu_set_device(int32_t device)
 {
@@ -99,6 +100,20 @@ int32_t m3gpuReserve(m3HostWorld* w)
     {
         w->dslab = nullptr;
     }
+    // The hull pool too, sized for the hulls interned so far, so that the
+    // upload itself allocates nothing.
+    const int32_t hullCount = (int32_t)w->hulls.size();
+    if (rc == M3GPU_OK && w->dhulls == nullptr)
+    {
+        const int32_t cap = hullCount < 4 ? 4 : hullCount;
+        rc = CudaCheck(cudaMalloc((void**)&w->dhulls, (size_t)cap * sizeof(m3HullData)),
+                       "cudaMalloc(hulls)");
+        w->dhullCap = rc == M3GPU_OK ? cap : 0;
+        if (rc != M3GPU_OK)
+        {
+            w->dhulls = nullptr;
+        }
+    }
     g_m3ResidencyEpoch += 1;
     return rc;
 }
@@ -152,15 +167,38 @@ int32_t m3gpuUpload(m3HostWorld* w)
         w->dhullCap = 4;
     }
     BuildDeviceView(w);
-    rc = CudaCheck(cudaMemcpy(w->dslab, w->image.data(), (size_t)w->persistentBytes,
-                              cudaMemcpyHostToDevice),
+    // Everything before the pair buffers, then the current pair list up
+    // to its count: the other buffer and the unused tails are written by
+    // the step before anything reads them.
+    const int64_t head = Offset(w, w->hv.keys0);
+    rc = CudaCheck(cudaMemcpy(w->dslab, w->image.data(), (size_t)head, cudaMemcpyHostToDevice),
                    "upload world image");
+    int64_t bytes = head;
+    const int32_t n = w->hv.sc->pairCount;
+    if (rc == M3GPU_OK && n > 0)
+    {
+        const int32_t buf = w->hv.sc->pairBuf;
+        rc = CudaCheck(cudaMemcpy(buf == 0 ? w->dv.keys0 : w->dv.keys1,
+                                  buf == 0 ? w->hv.keys0 : w->hv.keys1,
+                                  (size_t)n * sizeof(uint64_t), cudaMemcpyHostToDevice),
+                       "upload pair keys");
+        if (rc == M3GPU_OK)
+        {
+            rc = CudaCheck(cudaMemcpy(buf == 0 ? w->dv.man0 : w->dv.man1,
+                                      buf == 0 ? w->hv.man0 : w->hv.man1,
+                                      (size_t)n * sizeof(m3Manifold), cudaMemcpyHostToDevice),
+                           "upload manifolds");
+        }
+        bytes += (int64_t)n * (int64_t)(sizeof(uint64_t) + sizeof(m3Manifold));
+    }
     if (rc == M3GPU_OK && hullCount > 0)
     {
         rc = CudaCheck(cudaMemcpy(w->dhulls, w->hulls.data(),
                                   (size_t)hullCount * sizeof(m3HullData), cudaMemcpyHostToDevice),
                        "upload hulls");
+        bytes += (int64_t)hullCount * (int64_t)sizeof(m3HullData);
     }
+    g_m3UploadedBytes += bytes;
     if (rc == M3GPU_OK)
     {
         w->hostDirty = false;

@@ -19,8 +19,10 @@
 
 #ifdef __CUDACC__
 #define M3_HD __host__ __device__ __forceinline__
+#define M3_HD_MEMBER __host__ __device__ __forceinline__
 #else
 #define M3_HD static inline
+#define M3_HD_MEMBER inline
 #endif
 
 #ifndef MAUL3D_B200_H

@@ -48,6 +48,8 @@ m3HostWorld* m3gpuWorldFromIndex0(uint16_t index0);
 
 // Residency (device.cpp).
 extern uint64_t g_m3ResidencyEpoch;
+// Host-to-device bytes copied by uploads (device.cpp).
+extern int64_t g_m3UploadedBytes;
 int32_t m3gpuEnsureDevice(void);
 int32_t m3gpuReserve(m3HostWorld* w);
 int32_t m3gpuUpload(m3HostWorld* w);
@@ -60,6 +62,10 @@ int32_t m3gpuSyncHost(m3HostWorld* w);
 int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t substeps,
                        int32_t steps);
 int32_t m3gpuHashBatch(m3HostWorld** worlds, int32_t count, uint64_t* out);
+// The parallel world hash (hash.cu): one block per world, blocks in
+// `order`, out[world] = that world's m3WorldHashView.
+int32_t m3gpuLaunchHash(const m3WorldView* views, const int32_t* order, int32_t count,
+                        uint64_t* out);
 
 // Error reporting (capi.cpp).
 int32_t m3gpuSetError(int32_t code, const char* fmt, ...);

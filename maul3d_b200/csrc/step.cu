@@ -1809,18 +1809,6 @@ __global__ void m3StatusKernel(const m3WorldView* views, int32_t count, int32_t*
 }
 
 // ---------------------------------------------------------------------
-// Hash kernel: one thread per world over its HBM slab.
-// ---------------------------------------------------------------------
-__global__ void m3HashKernel(const m3WorldView* views, int32_t count, uint64_t* out)
-{
-    int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < count)
-    {
-        out[i] = m3WorldHashView(&views[i]);
-    }
-}
-
-// ---------------------------------------------------------------------
 // Host launch
 // ---------------------------------------------------------------------
 static int64_t s_launches = 0;
@@ -2179,7 +2167,11 @@ int32_t m3gpuHashBatch(m3HostWorld** worlds, int32_t count, uint64_t* out)
     {
         return rc;
     }
-    m3HashKernel<<<(count + 127) / 128, 128>>>(s_batch.dviews, count, s_batch.dhash);
+    rc = m3gpuLaunchHash(s_batch.dviews, s_batch.dorder, count, s_batch.dhash);
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
     s_launches += 1;
     rc = Check(cudaGetLastError(), "hash launch");
     if (rc == M3GPU_OK)
