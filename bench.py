@@ -306,7 +306,7 @@ def main() -> None:
     from maul3d_b200.shard import rank_seed as shard_seed, shard_sizes
     rank_seed = shard_seed(args.seed, rank)
     sizes = shard_sizes(m3.lib, rank_seed, args.worlds, args.lo, args.hi)
-    worlds = build_worlds(m3, sizes, rank_seed)
+    worlds = m3.WorldBatch(build_worlds(m3, sizes, rank_seed))
     m3.reserve_worlds(worlds)
     m3.upload_worlds(worlds)
 
@@ -334,7 +334,14 @@ def main() -> None:
     stage_ms = m3.kernel_ms()
     stats1 = np.stack([m3.world_stats(w) for w in worlds])
     work = (stats1 - stats0).astype(np.float64).sum(axis=0)
-    device_hashes = m3.hash_worlds(worlds)
+    # The device hash of the whole batch, timed alone on the device.
+    h0 = torch.cuda.Event(enable_timing=True)
+    h1 = torch.cuda.Event(enable_timing=True)
+    h0.record()
+    device_hashes = m3.hash_worlds(worlds).copy()
+    h1.record()
+    torch.cuda.synchronize()
+    hash_ms = h0.elapsed_time(h1)
 
     local_bs = body_substeps(sizes, args.substeps, args.steps)
     if world_size > 1:
@@ -394,8 +401,10 @@ def main() -> None:
     # K steps and a D2H hash read of every world after every step.
     e2e = None
     if not args.no_e2e:
-        eworlds = build_worlds(m3, sizes, rank_seed)
+        eworlds = m3.WorldBatch(build_worlds(m3, sizes, rank_seed))
+        tr = time.perf_counter()
         m3.reserve_worlds(eworlds)
+        reserve_ms = (time.perf_counter() - tr) * 1e3
         up0 = m3.uploaded_bytes()
         if world_size > 1:
             dist.barrier()
@@ -422,10 +431,11 @@ def main() -> None:
         e2e = {"value": total_bs / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": int(h2d // args.steps),
                "d2h_bytes_per_step": 8 * len(eworlds),
+               "reserve_ms_untimed": reserve_ms,
                "upload_ms": (t1 - t0) * 1e3,
                "step_ms_per_step": step_s * 1e3 / args.steps,
                "hash_ms_per_step": hash_s * 1e3 / args.steps,
-               "note": "world images uploaded once inside the timed region (pageable host "
+               "note": "world images uploaded once inside the timed region (page-locked host "
                        "memory); per step: batched step + device hash of every world read back"}
         for w in eworlds:
             w.destroy()
@@ -458,7 +468,7 @@ def main() -> None:
             "config": config_block(args, total_dynamic_bodies_per_gpu=int(sum(sizes))),
             "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
             "cpu_baseline": cpu, "plain_gpu": plain, "bit_exact_check": verified,
-            "clocks": clocks,
+            "hash_ms": hash_ms, "clocks": clocks,
         }
         print(json.dumps(line))
     if world_size > 1:

@@ -35,7 +35,7 @@ class M3GpuError(RuntimeError):
 def _load() -> C.CDLL:
     if not _LIB_PATH.exists():
         raise ImportError(
-            f"{_LIB_PATH} is missing: build it with `python -m maul3d_b200.build` "
+            f"{_LIB_PATH} is missing: build it with `python maul3d_b200/build.py` "
             "(the CUDA path has no CPU fallback)")
     lib = C.CDLL(str(_LIB_PATH))
     abi.bind_common(lib)
@@ -90,10 +90,30 @@ def _check(rc: int) -> None:
 
 
 def _ids(worlds) -> "C.Array":
+    if isinstance(worlds, WorldBatch):
+        return worlds.ids
     arr = (m3WorldId * len(worlds))()
     for i, w in enumerate(worlds):
         arr[i] = w.id
     return arr
+
+
+class WorldBatch:
+    """A fixed list of worlds with its id array built once, for callers
+    that step and hash the same batch many times."""
+
+    def __init__(self, worlds):
+        self.worlds = list(worlds)
+        self.ids = (m3WorldId * len(self.worlds))()
+        for i, w in enumerate(self.worlds):
+            self.ids[i] = w.id
+        self.hashes = np.zeros(len(self.worlds), dtype=np.uint64)
+
+    def __len__(self) -> int:
+        return len(self.worlds)
+
+    def __iter__(self):
+        return iter(self.worlds)
 
 
 class World:
@@ -136,7 +156,9 @@ class World:
         got = lib.m3gpu_copy_bodies(self.id, xf.ctypes.data, lin.ctypes.data, ang.ctypes.data,
                                     awake.ctypes.data, sleep.ctypes.data, n)
         if got < 0:
-            raise M3GpuError(M3GPU_ERR_INVALID, "body readback failed")
+            code, msg = last_error()
+            raise M3GpuError(code or M3GPU_ERR_INVALID,
+                             f"body readback failed ({n} bodies asked): {msg}")
         p = int(lib.m3gpu_pair_count(self.id))
         keys = np.zeros(max(p, 0), np.uint64)
         man = np.zeros(max(p, 0), MANIFOLD)
@@ -161,10 +183,13 @@ def step_worlds(worlds, dt: float = 1.0 / 60.0, substeps: int = 4, steps: int = 
 
 
 def hash_worlds(worlds) -> np.ndarray:
-    """World hashes computed on the device, one thread per world."""
-    out = (C.c_uint64 * len(worlds))()
-    _check(lib.m3gpu_hash_worlds(_ids(worlds), len(worlds), out))
-    return np.array(list(out), dtype=np.uint64)
+    """World hashes computed on the device, one thread block per world.
+    For a WorldBatch the result is written into (and returned as) its
+    `hashes` array."""
+    out = worlds.hashes if isinstance(worlds, WorldBatch) else np.zeros(len(worlds), np.uint64)
+    _check(lib.m3gpu_hash_worlds(_ids(worlds), len(worlds),
+                                 out.ctypes.data_as(C.POINTER(C.c_uint64))))
+    return out
 
 
 def synchronize() -> None:

@@ -6,7 +6,7 @@ bit-exact contract needs: no fused multiply-add contraction
 -prec-sqrt=true) and denormals preserved (-ftz=false).  Host code is
 compiled with -ffp-contract=off, like the reference engine's own build.
 
-Run `python -m maul3d_b200.build` (or __graft_entry__.build()).  The
+Run `python maul3d_b200/build.py` (or __graft_entry__.build()).  The
 CUDA runtime is linked statically so the library has no runtime search
 path requirements beyond the driver.
 """
@@ -33,7 +33,7 @@ DET_DEVICE = ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"]
 DET_HOST = ["-ffp-contract=off", "-fno-fast-math", "-fno-unsafe-math-optimizations"]
 
 CU_SOURCES = ["step.cu", "hash.cu"]
-CPP_SOURCES = ["world.cpp", "device.cpp", "capi.cpp"]
+CPP_SOURCES = ["world.cpp", "device.cpp", "capi.cpp", "hostmem.cpp"]
 C_SOURCES = ["scenes.c"]
 
 

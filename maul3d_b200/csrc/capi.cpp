@@ -5,6 +5,8 @@
 #include "m3_world.h"
 #include "m3_hash.h"
 
+#include <cuda_runtime.h>
+
 #include <stdarg.h>
 #include <stdio.h>
 #include <string.h>
@@ -141,9 +143,14 @@ extern "C" int32_t m3gpu_hash_worlds(const m3WorldId* worlds, int32_t count, uin
 static m3HostWorld* Synced(m3WorldId id)
 {
     m3HostWorld* w = m3gpuWorldFromId(id);
-    if (w == nullptr || m3gpuSyncHost(w) != M3GPU_OK)
+    if (w == nullptr)
     {
+        m3gpuSetError(M3GPU_ERR_INVALID, "stale world id");
         return nullptr;
+    }
+    if (m3gpuSyncHost(w) != M3GPU_OK)
+    {
+        return nullptr; // the error is set by the failing copy
     }
     return w;
 }
@@ -164,8 +171,14 @@ extern "C" int32_t m3gpu_copy_bodies(m3WorldId world, void* transforms, void* li
                                      uint8_t* awake, float* sleepTimes, int32_t cap)
 {
     m3HostWorld* w = Synced(world);
-    if (w == nullptr || cap < w->hv.sc->bodyMax)
+    if (w == nullptr)
     {
+        return -1;
+    }
+    if (cap < w->hv.sc->bodyMax)
+    {
+        m3gpuSetError(M3GPU_ERR_CAPACITY, "readback room %d below %d body slots", cap,
+                      w->hv.sc->bodyMax);
         return -1;
     }
     int32_t n = w->hv.sc->bodyMax;
@@ -252,6 +265,13 @@ extern "C" int32_t m3gpu_upload_worlds(const m3WorldId* worlds, int32_t count)
             w->hv.sc->status = 0;
             rc = m3gpuUpload(w);
         }
+    }
+    // Uploads from page-locked images are asynchronous: the images must
+    // not change under the copies, so return only once they are done.
+    const cudaError_t e = cudaStreamSynchronize(0);
+    if (rc == M3GPU_OK && e != cudaSuccess)
+    {
+        rc = m3gpuSetError(M3GPU_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
     }
     return rc;
 }

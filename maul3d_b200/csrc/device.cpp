@@ -100,6 +100,12 @@ int32_t m3gpuReserve(m3HostWorld* w)
     {
         w->dslab = nullptr;
     }
+    // Page-lock the host memory of the images (chunk by chunk, see
+    // hostmem.cpp), so uploads are DMA copies straight from it.
+    if (rc == M3GPU_OK)
+    {
+        m3HostLockAll();
+    }
     // The hull pool too, sized for the hulls interned so far, so that the
     // upload itself allocates nothing.
     const int32_t hullCount = (int32_t)w->hulls.size();
@@ -171,8 +177,21 @@ int32_t m3gpuUpload(m3HostWorld* w)
     // to its count: the other buffer and the unused tails are written by
     // the step before anything reads them.
     const int64_t head = Offset(w, w->hv.keys0);
-    rc = CudaCheck(cudaMemcpy(w->dslab, w->image.data(), (size_t)head, cudaMemcpyHostToDevice),
-                   "upload world image");
+    if (m3HostIsLocked(w->image.data(), (size_t)head))
+    {
+        // Page-locked: an asynchronous DMA on the default stream, ordered
+        // before any later kernel; callers that return to the host
+        // synchronise first.
+        rc = CudaCheck(cudaMemcpyAsync(w->dslab, w->image.data(), (size_t)head,
+                                       cudaMemcpyHostToDevice, 0),
+                       "upload world image");
+    }
+    else
+    {
+        rc = CudaCheck(cudaMemcpy(w->dslab, w->image.data(), (size_t)head,
+                                  cudaMemcpyHostToDevice),
+                       "upload world image");
+    }
     int64_t bytes = head;
     const int32_t n = w->hv.sc->pairCount;
     if (rc == M3GPU_OK && n > 0)
@@ -193,10 +212,20 @@ int32_t m3gpuUpload(m3HostWorld* w)
     }
     if (rc == M3GPU_OK && hullCount > 0)
     {
-        rc = CudaCheck(cudaMemcpy(w->dhulls, w->hulls.data(),
-                                  (size_t)hullCount * sizeof(m3HullData), cudaMemcpyHostToDevice),
-                       "upload hulls");
-        bytes += (int64_t)hullCount * (int64_t)sizeof(m3HullData);
+        const size_t hullBytes = (size_t)hullCount * sizeof(m3HullData);
+        if (m3HostIsLocked(w->hulls.data(), hullBytes))
+        {
+            rc = CudaCheck(cudaMemcpyAsync(w->dhulls, w->hulls.data(), hullBytes,
+                                           cudaMemcpyHostToDevice, 0),
+                           "upload hulls");
+        }
+        else
+        {
+            rc = CudaCheck(cudaMemcpy(w->dhulls, w->hulls.data(), hullBytes,
+                                      cudaMemcpyHostToDevice),
+                           "upload hulls");
+        }
+        bytes += (int64_t)hullBytes;
     }
     g_m3UploadedBytes += bytes;
     if (rc == M3GPU_OK)
@@ -271,6 +300,11 @@ int32_t m3gpuSyncHost(m3HostWorld* w)
 void m3gpuRelease(m3HostWorld* w)
 {
     g_m3ResidencyEpoch += 1;
+    if (w->dslab != nullptr)
+    {
+        // No copy from the host image may be in flight when it is freed.
+        cudaDeviceSynchronize();
+    }
     if (w->dslab != nullptr)
     {
         cudaFree(w->dslab);

@@ -47,6 +47,7 @@ struct m3JointDev
     m3Vec3 angularImpulse;
     m3Vec3 springImpulseV;
 };
+static_assert(sizeof(m3JointDev) % 4 == 0, "joint rows are copied as 32-bit words");
 
 // Half-quaternion rotation of a frame axis (solver.c:690-696).
 __device__ __forceinline__ m3Vec3 m3PerpColumn(m3Quat qA, m3Quat relQ, m3Vec3 axis)

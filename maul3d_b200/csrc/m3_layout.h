@@ -178,6 +178,7 @@ typedef struct m3WorldView
 } m3WorldView;
 
 #define M3_SLAB_ALIGN 256
+#define M3_PAIR_SECTION_ALIGN 4096
 
 M3_HD int64_t m3AlignUp(int64_t x, int64_t a)
 {
@@ -208,6 +209,10 @@ static inline int64_t m3LayoutPersistent(m3WorldView* view, uint8_t* base, int32
     M3_BODY_FIELDS(M3_X_BODY)
     M3_SHAPE_FIELDS(M3_X_SHAPE)
     M3_JOINT_FIELDS(M3_X_JOINT)
+    // The pair buffers start on a fresh 4 KiB page: the host pages before
+    // them are page-locked for uploads, and a copy must not straddle the
+    // locked and unlocked parts.
+    off = m3AlignUp(off, M3_PAIR_SECTION_ALIGN);
     M3_PAIR_FIELDS(M3_X_PAIR)
 #undef M3_X_BODY
 #undef M3_X_SHAPE

@@ -470,27 +470,79 @@ __device__ __forceinline__ m3ProxyDev m3MakeProxyDev(const m3WorldView& w, int32
 
 // ---------------------------------------------------------------------
 // The pair dispatcher (manifold.c:2357-2911) for the shape families on
-// the device path.  Returns M3_NARROW_UNSUPPORTED for a pair family it
-// does not cover (the caller stalls the world loudly).
+// the device path, split by family so that each family runs as its own
+// kernel over a bucket of same-family pairs (uniform warps, and each
+// kernel only as large as its family's code).  m3PairFamily follows the
+// dispatcher's branch order; m3CollideFamily<F> is the branch for family
+// F.  A family the device does not cover reports M3_NARROW_UNSUPPORTED
+// (the caller stalls the world loudly).
 // ---------------------------------------------------------------------
-__device__ int32_t m3CollidePair(const m3WorldView& w, uint64_t key, m3Manifold* out)
+enum
+{
+    M3F_PLANE_HULL = 0,
+    M3F_HULL_HULL = 1,
+    M3F_PLANE_CAPSULE = 2,
+    M3F_CAPSULE_HULL = 3,
+    M3F_ROUND = 4, // hull-sphere, capsule-sphere, capsule-capsule: GJK on the cores
+    M3F_PLANE_SPHERE = 5,
+    M3F_SPHERE_SPHERE = 6,
+    M3F_UNSUPPORTED = 7,
+    M3F_COUNT = 8
+};
+
+__device__ __forceinline__ int32_t m3PairFamily(uint8_t typeA, uint8_t typeB)
+{
+    const bool planePair = typeA == M3_SHAPE_PLANE || typeB == M3_SHAPE_PLANE;
+    const bool hullPair = typeA == M3_SHAPE_HULL || typeB == M3_SHAPE_HULL;
+    const bool capsulePair = typeA == M3_SHAPE_CAPSULE || typeB == M3_SHAPE_CAPSULE;
+    if (typeA >= M3_SHAPE_MESH || typeB >= M3_SHAPE_MESH)
+    {
+        return M3F_UNSUPPORTED;
+    }
+    if (planePair && hullPair)
+    {
+        return M3F_PLANE_HULL;
+    }
+    if (typeA == M3_SHAPE_HULL && typeB == M3_SHAPE_HULL)
+    {
+        return M3F_HULL_HULL;
+    }
+    if (planePair && capsulePair)
+    {
+        return M3F_PLANE_CAPSULE;
+    }
+    if (hullPair && capsulePair)
+    {
+        return M3F_CAPSULE_HULL;
+    }
+    if (hullPair || capsulePair)
+    {
+        return M3F_ROUND;
+    }
+    if (planePair)
+    {
+        return M3F_PLANE_SPHERE;
+    }
+    return M3F_SPHERE_SPHERE;
+}
+
+template <int F>
+__device__ int32_t m3CollideFamily(const m3WorldView& w, uint64_t key, m3Manifold* out)
 {
     int32_t shapeA = (int32_t)(key >> 32);
     int32_t shapeB = (int32_t)(key & 0xFFFFFFFFu);
     uint8_t typeA = w.shapeType[shapeA];
     uint8_t typeB = w.shapeType[shapeB];
-    int planePair = typeA == M3_SHAPE_PLANE || typeB == M3_SHAPE_PLANE;
     int hullPair = typeA == M3_SHAPE_HULL || typeB == M3_SHAPE_HULL;
-    int capsulePair = typeA == M3_SHAPE_CAPSULE || typeB == M3_SHAPE_CAPSULE;
     int32_t status = M3_NARROW_OK;
     m3Manifold fresh = m3EmptyManifold();
 
-    if (typeA >= M3_SHAPE_MESH || typeB >= M3_SHAPE_MESH)
+    if (F == M3F_UNSUPPORTED)
     {
         *out = fresh;
         return M3_NARROW_UNSUPPORTED;
     }
-    if (planePair && hullPair)
+    if (F == M3F_PLANE_HULL)
     {
         // Plane versus hull (manifold.c:2415-2520): every vertex inside
         // the margin is a candidate; the four deepest survive (ties to
@@ -596,7 +648,7 @@ __device__ int32_t m3CollidePair(const m3WorldView& w, uint64_t key, m3Manifold*
             }
         }
     }
-    else if (typeA == M3_SHAPE_HULL && typeB == M3_SHAPE_HULL)
+    else if (F == M3F_HULL_HULL)
     {
         // Hull versus hull (manifold.c:2521-2558).
         int32_t bodyA = w.shapeBody[shapeA];
@@ -623,7 +675,7 @@ __device__ int32_t m3CollidePair(const m3WorldView& w, uint64_t key, m3Manifold*
             }
         }
     }
-    else if (planePair && capsulePair)
+    else if (F == M3F_PLANE_CAPSULE)
     {
         // Plane versus capsule (manifold.c:2559-2616): the two cap
         // centres are the only candidates, in cap order.
@@ -674,7 +726,7 @@ __device__ int32_t m3CollidePair(const m3WorldView& w, uint64_t key, m3Manifold*
             }
         }
     }
-    else if (hullPair && capsulePair)
+    else if (F == M3F_CAPSULE_HULL)
     {
         // Capsule versus hull: the segment SAT in the hull frame
         // (manifold.c:2617-2663).
@@ -712,7 +764,7 @@ __device__ int32_t m3CollidePair(const m3WorldView& w, uint64_t key, m3Manifold*
             }
         }
     }
-    else if (hullPair || capsulePair)
+    else if (F == M3F_ROUND)
     {
         // Hull-sphere, capsule-sphere, capsule-capsule: GJK on the
         // cores in A's frame, radii applied analytically, one point,
@@ -828,7 +880,7 @@ __device__ int32_t m3CollidePair(const m3WorldView& w, uint64_t key, m3Manifold*
             fresh.pointCount = 1;
         }
     }
-    else if (planePair)
+    else if (F == M3F_PLANE_SPHERE)
     {
         // Plane versus sphere (manifold.c:2808-2844).
         int32_t planeShape = typeA == M3_SHAPE_PLANE ? shapeA : shapeB;
@@ -858,7 +910,7 @@ __device__ int32_t m3CollidePair(const m3WorldView& w, uint64_t key, m3Manifold*
             }
         }
     }
-    else
+    else if (F == M3F_SPHERE_SPHERE)
     {
         // Sphere versus sphere (manifold.c:2845-2866).
         double ax, ay, az, bx, by, bz;
@@ -876,6 +928,33 @@ __device__ int32_t m3CollidePair(const m3WorldView& w, uint64_t key, m3Manifold*
     }
     *out = fresh;
     return status;
+}
+
+// All families through one entry (the allocation-free single-world path
+// and any caller without buckets).
+__device__ int32_t m3CollidePair(const m3WorldView& w, uint64_t key, m3Manifold* out)
+{
+    const uint8_t typeA = w.shapeType[(int32_t)(key >> 32)];
+    const uint8_t typeB = w.shapeType[(int32_t)(key & 0xFFFFFFFFu)];
+    switch (m3PairFamily(typeA, typeB))
+    {
+    case M3F_PLANE_HULL:
+        return m3CollideFamily<M3F_PLANE_HULL>(w, key, out);
+    case M3F_HULL_HULL:
+        return m3CollideFamily<M3F_HULL_HULL>(w, key, out);
+    case M3F_PLANE_CAPSULE:
+        return m3CollideFamily<M3F_PLANE_CAPSULE>(w, key, out);
+    case M3F_CAPSULE_HULL:
+        return m3CollideFamily<M3F_CAPSULE_HULL>(w, key, out);
+    case M3F_ROUND:
+        return m3CollideFamily<M3F_ROUND>(w, key, out);
+    case M3F_PLANE_SPHERE:
+        return m3CollideFamily<M3F_PLANE_SPHERE>(w, key, out);
+    case M3F_SPHERE_SPHERE:
+        return m3CollideFamily<M3F_SPHERE_SPHERE>(w, key, out);
+    default:
+        return m3CollideFamily<M3F_UNSUPPORTED>(w, key, out);
+    }
 }
 
 // Warm-start carry (manifold.c:2868-2908): binary search of the previous

@@ -7,8 +7,46 @@
 #include "m3_layout.h"
 
 #include <stdint.h>
+#include <stdlib.h>
+#include <new>
 #include <unordered_map>
 #include <vector>
+
+// Host memory for world images and hull buffers (hostmem.cpp): page-
+// granular blocks from large mappings, page-locked chunk by chunk when a
+// world becomes device-resident, so uploads are asynchronous DMA copies.
+#define M3_HOST_PAGE 4096
+void* m3HostAlloc(size_t bytes);
+void m3HostFree(void* p, size_t bytes);
+// Page-lock every chunk not locked yet (one driver call per chunk).
+int32_t m3HostLockAll(void);
+// Whether [p, p + bytes) lies in a locked chunk.
+bool m3HostIsLocked(const void* p, size_t bytes);
+
+template <class T> struct m3PageAllocator
+{
+    using value_type = T;
+    m3PageAllocator() = default;
+    template <class U> m3PageAllocator(const m3PageAllocator<U>&)
+    {
+    }
+    T* allocate(size_t n)
+    {
+        return (T*)m3HostAlloc(n * sizeof(T));
+    }
+    void deallocate(T* p, size_t n)
+    {
+        m3HostFree(p, n * sizeof(T));
+    }
+    template <class U> bool operator==(const m3PageAllocator<U>&) const
+    {
+        return true;
+    }
+    template <class U> bool operator!=(const m3PageAllocator<U>&) const
+    {
+        return false;
+    }
+};
 
 struct m3HostWorld
 {
@@ -20,14 +58,14 @@ struct m3HostWorld
     int32_t pairCap = 0;
 
     // Persistent image (host copy) and its view.
-    std::vector<uint8_t> image;
+    std::vector<uint8_t, m3PageAllocator<uint8_t>> image;
     int64_t persistentBytes = 0;
     m3WorldView hv{};
 
     // Interned hull slabs live outside the fixed-capacity image: the
     // pool is sized by the hulls actually interned (count-derived, as
     // the reference's snapshot treats them).
-    std::vector<m3HullData> hulls;
+    std::vector<m3HullData, m3PageAllocator<m3HullData>> hulls;
     std::vector<int32_t> hullRefs;
     std::unordered_multimap<uint64_t, int32_t> hullIndexByContent;
 

@@ -1,12 +1,16 @@
 // The device step: m3StepInternal (src/solver.c:3662-4320) for a batch
 // of independent worlds, one thread block per world.
 //
-// Six launches per step:
+// Launches per step:
 //   m3BroadKernel        one block per world: fresh bounds, sort-and-sweep
 //                        and the canonical (sorted) pair list;
 //   m3PairOffsetsKernel  prefix of the worlds' pair counts;
-//   m3NarrowKernel       one thread per pair of the whole batch: the
-//                        narrowphase with the warm-start carry;
+//   m3FamilyCount/ScatterKernel  bucket the batch's flattened pairs by
+//                        pair family;
+//   m3NarrowFamilyKernel<F>  one per covered family, one thread per pair
+//                        of its bucket: the narrowphase with the
+//                        warm-start carry (m3NarrowKernel, all families
+//                        in one, serves the single-world path);
 //   m3PrepareKernel      one block per world: islands and wake, contact
 //                        selection, graph colouring, contact rows written
 //                        into their solve slots, joint rows and their
@@ -40,6 +44,10 @@
 #include <vector>
 
 #define M3_BLOCK 256
+// Colouring: the marker of a constraint not coloured yet, and the
+// parallel rounds before the serial finish.
+#define M3_COLOR_PENDING 0xFF
+#define M3_COLOR_ROUNDS 64
 
 // Step phases timed with the SM clock by thread 0 of each world's block
 // right after the barrier that closes the phase.
@@ -109,6 +117,7 @@ struct m3Scratch
     int32_t* movers;       // per body
     int32_t* moverFlag;    // per body
     uint32_t* bodyMask;    // per body
+    int32_t* colorMin;     // 2 per body: colouring round claims
     m3StepPlan* plan;      // counts and offsets handed between the step kernels
     m3ConRows rows;        // contact rows, field-major, one slot per constraint
     int32_t* conPairIndex; // per constraint: its pair
@@ -163,6 +172,7 @@ static __host__ __device__ inline int64_t ScratchCarve(m3Scratch* s, uint8_t* ba
     M3_CARVE(movers, int32_t, bodyCap)
     M3_CARVE(moverFlag, int32_t, bodyCap + 1)
     M3_CARVE(bodyMask, uint32_t, bodyCap)
+    M3_CARVE(colorMin, int32_t, 2 * (int64_t)bodyCap)
     M3_CARVE(plan, m3StepPlan, 1)
     const int32_t rowStride = (int32_t)m3AlignUp(pairCap, 32);
     if (s)
@@ -745,6 +755,218 @@ __global__ void __launch_bounds__(128) m3NarrowKernel(const m3WorldView* views,
 }
 
 // ---------------------------------------------------------------------
+// Kernels 2b-2c: the batch's flattened pairs bucketed by pair family
+// (m3PairFamily), so that each family's narrowphase runs as its own
+// kernel over same-family warps.  A two-pass partition without global
+// atomics: each block counts the families of a contiguous range of the
+// flattened pairs, then scatters that range in order behind the counts
+// of all earlier blocks; the buckets hold flattened pair indices.
+// ---------------------------------------------------------------------
+#define M3_FAMILY_BLOCKS 592
+#define M3_FAMILY_THREADS 256
+
+// The world owning flattened pair g: the last world whose offset <= g.
+__device__ __forceinline__ int32_t FlatWorld(const int32_t* offsets, int32_t count, int32_t g)
+{
+    int32_t lo = 0;
+    int32_t hi = count - 1;
+    while (lo < hi)
+    {
+        const int32_t mid = (lo + hi + 1) >> 1;
+        if (offsets[mid] <= g)
+        {
+            lo = mid;
+        }
+        else
+        {
+            hi = mid - 1;
+        }
+    }
+    return lo;
+}
+
+__device__ __forceinline__ int32_t FlatFamily(const m3WorldView* views, const int32_t* offsets,
+                                              int32_t count, int32_t g, int32_t* world)
+{
+    const int32_t wi = FlatWorld(offsets, count, g);
+    const m3WorldView& w = views[wi];
+    const uint64_t* newKeys = w.sc->pairBuf == 0 ? w.keys1 : w.keys0;
+    const uint64_t key = newKeys[g - offsets[wi]];
+    *world = wi;
+    return m3PairFamily(w.shapeType[(int32_t)(key >> 32)],
+                        w.shapeType[(int32_t)(key & 0xFFFFFFFFu)]);
+}
+
+__device__ __forceinline__ void FamilyRange(int32_t total, int32_t* lo, int32_t* hi)
+{
+    const int32_t chunk = (total + (int32_t)gridDim.x - 1) / (int32_t)gridDim.x;
+    const int32_t a = (int32_t)blockIdx.x * chunk;
+    *lo = a < total ? a : total;
+    *hi = a + chunk < total ? a + chunk : total;
+}
+
+__global__ void __launch_bounds__(M3_FAMILY_THREADS)
+    m3FamilyCountKernel(const m3WorldView* views, const int32_t* offsets, int32_t count,
+                        int32_t* blockHist)
+{
+    __shared__ int32_t hist[M3F_COUNT];
+    const int32_t tid = threadIdx.x;
+    if (tid < M3F_COUNT)
+    {
+        hist[tid] = 0;
+    }
+    __syncthreads();
+    int32_t lo;
+    int32_t hi;
+    FamilyRange(offsets[count], &lo, &hi);
+    for (int32_t g = lo + tid; g < hi; g += M3_FAMILY_THREADS)
+    {
+        int32_t wi;
+        const int32_t f = FlatFamily(views, offsets, count, g, &wi);
+        if (f == M3F_UNSUPPORTED)
+        {
+            // A pair family the device does not cover: the world stalls.
+            const m3WorldView& w = views[wi];
+            const uint64_t* newKeys = w.sc->pairBuf == 0 ? w.keys1 : w.keys0;
+            const uint64_t key = newKeys[g - offsets[wi]];
+            atomicMax(&w.sc->status, M3GPU_ERR_UNSUPPORTED);
+            w.sc->statusDetail = 1000 + (int32_t)w.shapeType[(int32_t)(key >> 32)] * 10 +
+                                 (int32_t)w.shapeType[(int32_t)(key & 0xFFFFFFFFu)];
+        }
+        atomicAdd(&hist[f], 1);
+    }
+    __syncthreads();
+    if (tid < M3F_COUNT)
+    {
+        blockHist[blockIdx.x * M3F_COUNT + tid] = hist[tid];
+    }
+}
+
+__global__ void __launch_bounds__(M3_FAMILY_THREADS)
+    m3FamilyScatterKernel(const m3WorldView* views, const int32_t* offsets, int32_t count,
+                          const int32_t* blockHist, int32_t* famStart, int32_t* bucket)
+{
+    __shared__ int32_t base[M3F_COUNT];
+    __shared__ int32_t total[M3F_COUNT];
+    __shared__ int32_t warpCount[M3_FAMILY_THREADS / 32][M3F_COUNT];
+    const int32_t tid = threadIdx.x;
+    const int32_t lane = tid & 31;
+    const int32_t warp = tid >> 5;
+    if (tid < M3F_COUNT)
+    {
+        // Family totals over all blocks, and this family's pairs in the
+        // blocks before this one.
+        int32_t before = 0;
+        int32_t all = 0;
+        for (int32_t b = 0; b < (int32_t)gridDim.x; ++b)
+        {
+            const int32_t v = blockHist[b * M3F_COUNT + tid];
+            before += b < (int32_t)blockIdx.x ? v : 0;
+            all += v;
+        }
+        total[tid] = all;
+        base[tid] = before;
+    }
+    __syncthreads();
+    if (tid == 0)
+    {
+        int32_t start = 0;
+        for (int32_t f = 0; f < M3F_COUNT; ++f)
+        {
+            if (blockIdx.x == 0)
+            {
+                famStart[f] = start;
+            }
+            base[f] += start;
+            start += total[f];
+        }
+        if (blockIdx.x == 0)
+        {
+            famStart[M3F_COUNT] = start;
+        }
+    }
+    __syncthreads();
+    int32_t lo;
+    int32_t hi;
+    FamilyRange(offsets[count], &lo, &hi);
+    const uint32_t ltMask = (1u << lane) - 1u;
+    for (int32_t t0 = lo; t0 < hi; t0 += M3_FAMILY_THREADS)
+    {
+        const int32_t g = t0 + tid;
+        int32_t f = M3F_COUNT; // past the range: no family
+        if (g < hi)
+        {
+            int32_t wi;
+            f = FlatFamily(views, offsets, count, g, &wi);
+        }
+        int32_t rank = 0;
+#pragma unroll
+        for (int32_t k = 0; k < M3F_COUNT; ++k)
+        {
+            const uint32_t b = __ballot_sync(0xFFFFFFFFu, f == k);
+            if (f == k)
+            {
+                rank = __popc(b & ltMask);
+            }
+            if (lane == 0)
+            {
+                warpCount[warp][k] = __popc(b);
+            }
+        }
+        __syncthreads();
+        if (f < M3F_COUNT)
+        {
+            int32_t pos = base[f] + rank;
+            for (int32_t k = 0; k < warp; ++k)
+            {
+                pos += warpCount[k][f];
+            }
+            bucket[pos] = g;
+        }
+        __syncthreads();
+        if (tid < M3F_COUNT)
+        {
+            int32_t add = 0;
+            for (int32_t k = 0; k < M3_FAMILY_THREADS / 32; ++k)
+            {
+                add += warpCount[k][tid];
+            }
+            base[tid] += add;
+        }
+        __syncthreads();
+    }
+}
+
+// Kernel 2d: the narrowphase of one pair family over its bucket, with
+// the warm-start carry.
+template <int F>
+__global__ void __launch_bounds__(128)
+    m3NarrowFamilyKernel(const m3WorldView* views, const int32_t* offsets, int32_t count,
+                         const int32_t* famStart, const int32_t* bucket)
+{
+    const int32_t end = famStart[F + 1];
+    for (int32_t idx = famStart[F] + blockIdx.x * blockDim.x + threadIdx.x; idx < end;
+         idx += gridDim.x * blockDim.x)
+    {
+        const int32_t g = bucket[idx];
+        const int32_t wi = FlatWorld(offsets, count, g);
+        const m3WorldView& w = views[wi];
+        m3WorldScalars* sc = w.sc;
+        const int32_t k = g - offsets[wi];
+        const int32_t cur = sc->pairBuf;
+        const uint64_t* oldKeys = cur == 0 ? w.keys0 : w.keys1;
+        const m3Manifold* oldMan = cur == 0 ? w.man0 : w.man1;
+        const uint64_t* newKeys = cur == 0 ? w.keys1 : w.keys0;
+        m3Manifold* newMan = cur == 0 ? w.man1 : w.man0;
+        const uint64_t key = newKeys[k];
+        m3Manifold fresh;
+        m3CollideFamily<F>(w, key, &fresh);
+        m3WarmCarry(&fresh, key, oldKeys, oldMan, sc->pairCount);
+        newMan[k] = fresh;
+    }
+}
+
+// ---------------------------------------------------------------------
 // Islands (solver.c:3437-3578): a lock-free union-find whose links
 // always point a root at a smaller root, so each component's final
 // root is its smallest body index, the reference's "lower root wins".
@@ -928,6 +1150,9 @@ __device__ void ContinuousVersusPlane(const m3WorldView& w, int32_t body, int32_
 // Shared-memory bytes per body of the substep-loop cache: v, w, the
 // position delta (12 B each) and the rotation delta (16 B).
 #define M3_BODY_CACHE_BYTES 52
+// Dynamic shared memory per block that still lets two 256-thread blocks
+// share an SM (228 KB per SM, 1 KB reserved per block, static arrays).
+#define M3_TWO_BLOCK_SMEM (110 * 1024)
 
 __global__ void __launch_bounds__(M3_BLOCK) m3PrepareKernel(const m3WorldView* views,
                                                             const int32_t* order, int32_t count,
@@ -1174,21 +1399,31 @@ __global__ void __launch_bounds__(M3_BLOCK) m3PrepareKernel(const m3WorldView* v
 
     M3_PHASE_MARK(M3_PHASE_PREPARE)
     // Greedy 16-colour first-free-bit colouring in constraint order, the
-    // overflow bucket last (solver.c:2750-2810).  The walk is serial, so
-    // its inputs are staged first: each constraint's effective body pair
-    // (-1 for a side that is not an awake dynamic body), the body colour
-    // masks and the colours live in shared memory when they fit (the
-    // body cache's space is free until the substep loop).
+    // overflow bucket last (solver.c:2750-2810), computed in rounds.  In
+    // the serial walk a constraint's colour depends only on the colours
+    // of the earlier constraints that share one of its (awake dynamic)
+    // bodies.  So in each round every uncoloured constraint that is the
+    // earliest uncoloured one on each of its bodies takes its colour at
+    // once: exactly the masks the serial walk would see, and no two
+    // constraints of a round touch the same body.  Each round colours
+    // at least the earliest uncoloured constraint; after M3_COLOR_ROUNDS
+    // rounds thread 0 finishes any rest in order.  Slots are then
+    // assigned colour by colour in constraint order (a stable counting
+    // sort), as the serial list fill does.
     extern __shared__ __align__(16) uint8_t s_colorStage[];
-    const int64_t maskBytes = 4 * (((int64_t)bodyMax + 1) & ~1LL);
-    const bool staged =
-        maskBytes + 9 * (int64_t)constraintCount <= (int64_t)cacheBytes;
+    const int64_t bodyWords = ((int64_t)bodyMax + 1) & ~1LL;
+    const int64_t stageBytes = 12 * bodyWords + 9 * (int64_t)constraintCount;
+    const bool staged = stageBytes <= (int64_t)cacheBytes;
     uint32_t* cMask = staged ? (uint32_t*)s_colorStage : s.bodyMask;
-    int2* cPair = staged ? (int2*)(s_colorStage + maskBytes) : s.conPair;
+    int32_t* cMin0 = staged ? (int32_t*)(cMask + bodyWords) : s.colorMin;
+    int32_t* cMin1 = cMin0 + (staged ? bodyWords : (int64_t)sc->bodyCap);
+    int2* cPair = staged ? (int2*)(s_colorStage + 12 * bodyWords) : s.conPair;
     uint8_t* cColor = staged ? (uint8_t*)(cPair + constraintCount) : s.colors;
     for (int32_t i = tid; i < bodyMax; i += M3_BLOCK)
     {
         cMask[i] = 0u;
+        cMin0[i] = INT32_MAX;
+        cMin1[i] = INT32_MAX;
     }
     for (int32_t i = tid; i < constraintCount; i += M3_BLOCK)
     {
@@ -1198,19 +1433,55 @@ __global__ void __launch_bounds__(M3_BLOCK) m3PrepareKernel(const m3WorldView* v
         int32_t a = w.btype[bodyA] == M3_BODY_DYNAMIC && w.awake[bodyA] ? bodyA : -1;
         int32_t b = w.btype[bodyB] == M3_BODY_DYNAMIC && w.awake[bodyB] ? bodyB : -1;
         cPair[i] = make_int2(a, b);
+        cColor[i] = M3_COLOR_PENDING;
     }
     __syncthreads();
-    if (tid == 0)
+    bool pendingLeft = constraintCount > 0;
+    for (int32_t round = 0; pendingLeft && round < M3_COLOR_ROUNDS; ++round)
     {
-        int32_t counts[M3_GRAPH_COLORS + 1];
-        for (int32_t c = 0; c <= M3_GRAPH_COLORS; ++c)
+        int32_t* cur = (round & 1) ? cMin1 : cMin0;
+        int32_t* nxt = (round & 1) ? cMin0 : cMin1;
+        for (int32_t i = tid; i < constraintCount; i += M3_BLOCK)
         {
-            counts[c] = 0;
+            if (cColor[i] == M3_COLOR_PENDING)
+            {
+                const int2 p = cPair[i];
+                if (p.x >= 0)
+                {
+                    atomicMin(&cur[p.x], i);
+                }
+                if (p.y >= 0)
+                {
+                    atomicMin(&cur[p.y], i);
+                }
+            }
         }
-        for (int32_t i = 0; i < constraintCount; ++i)
+        __syncthreads();
+        int32_t waiting = 0;
+        for (int32_t i = tid; i < constraintCount; i += M3_BLOCK)
         {
+            if (cColor[i] != M3_COLOR_PENDING)
+            {
+                continue;
+            }
             const int2 p = cPair[i];
-            uint32_t mask = (p.x >= 0 ? cMask[p.x] : 0u) | (p.y >= 0 ? cMask[p.y] : 0u);
+            const bool ready = (p.x < 0 || cur[p.x] == i) && (p.y < 0 || cur[p.y] == i);
+            // The next round's claims start from empty on every body a
+            // pending constraint may touch.
+            if (p.x >= 0)
+            {
+                nxt[p.x] = INT32_MAX;
+            }
+            if (p.y >= 0)
+            {
+                nxt[p.y] = INT32_MAX;
+            }
+            if (!ready)
+            {
+                waiting = 1;
+                continue;
+            }
+            const uint32_t mask = (p.x >= 0 ? cMask[p.x] : 0u) | (p.y >= 0 ? cMask[p.y] : 0u);
             // First clear bit among the 16 colours; 16 = overflow.
             int32_t color = __ffs((int)~mask) - 1;
             color = color < M3_GRAPH_COLORS ? color : M3_GRAPH_COLORS;
@@ -1227,30 +1498,110 @@ __global__ void __launch_bounds__(M3_BLOCK) m3PrepareKernel(const m3WorldView* v
                     cMask[p.y] |= bit;
                 }
             }
-            counts[color] += 1;
         }
+        pendingLeft = __syncthreads_or(waiting) != 0;
+    }
+    if (pendingLeft && tid == 0)
+    {
+        // Long dependency chains: the rest in constraint order.
+        for (int32_t i = 0; i < constraintCount; ++i)
+        {
+            if (cColor[i] != M3_COLOR_PENDING)
+            {
+                continue;
+            }
+            const int2 p = cPair[i];
+            const uint32_t mask = (p.x >= 0 ? cMask[p.x] : 0u) | (p.y >= 0 ? cMask[p.y] : 0u);
+            int32_t color = __ffs((int)~mask) - 1;
+            color = color < M3_GRAPH_COLORS ? color : M3_GRAPH_COLORS;
+            cColor[i] = (uint8_t)color;
+            if (color < M3_GRAPH_COLORS)
+            {
+                const uint32_t bit = 1u << color;
+                if (p.x >= 0)
+                {
+                    cMask[p.x] |= bit;
+                }
+                if (p.y >= 0)
+                {
+                    cMask[p.y] |= bit;
+                }
+            }
+        }
+    }
+    // Colour sizes and offsets.
+    __shared__ int32_t s_colorFill[M3_GRAPH_COLORS + 1];
+    __shared__ int32_t s_warpColor[M3_BLOCK / 32][M3_GRAPH_COLORS + 1];
+    if (tid <= M3_GRAPH_COLORS)
+    {
+        s_colorFill[tid] = 0;
+    }
+    __syncthreads();
+    for (int32_t i = tid; i < constraintCount; i += M3_BLOCK)
+    {
+        atomicAdd(&s_colorFill[cColor[i]], 1);
+    }
+    __syncthreads();
+    if (tid == 0)
+    {
         int32_t cursor = 0;
         int32_t used = 0;
         for (int32_t c = 0; c <= M3_GRAPH_COLORS; ++c)
         {
+            const int32_t n = s_colorFill[c];
             s_starts[c] = cursor;
-            cursor += counts[c];
-            used += counts[c] > 0 ? 1 : 0;
+            s_colorFill[c] = cursor;
+            cursor += n;
+            used += n > 0 ? 1 : 0;
         }
         s_starts[M3_GRAPH_COLORS + 1] = cursor;
-        int32_t fill[M3_GRAPH_COLORS + 1];
-        for (int32_t c = 0; c <= M3_GRAPH_COLORS; ++c)
-        {
-            fill[c] = s_starts[c];
-        }
-        for (int32_t i = 0; i < constraintCount; ++i)
-        {
-            const int32_t slot = fill[cColor[i]]++;
-            s.lists[slot] = i;
-            s.conSlot[i] = slot;
-        }
         sc->lastColorCount = used;
         sc->constraintCount = constraintCount;
+    }
+    __syncthreads();
+    // Slots: colour by colour, constraint order inside a colour.
+    {
+        const int32_t lane = tid & 31;
+        const int32_t warp = tid >> 5;
+        const uint32_t ltMask = (1u << lane) - 1u;
+        for (int32_t c0 = 0; c0 < constraintCount; c0 += M3_BLOCK)
+        {
+            const int32_t i = c0 + tid;
+            const int32_t color = i < constraintCount ? (int32_t)cColor[i] : M3_GRAPH_COLORS + 1;
+            for (int32_t k = tid; k < (M3_BLOCK / 32) * (M3_GRAPH_COLORS + 1); k += M3_BLOCK)
+            {
+                (&s_warpColor[0][0])[k] = 0;
+            }
+            __syncthreads();
+            const uint32_t peers = __match_any_sync(0xFFFFFFFFu, color);
+            const int32_t rank = __popc(peers & ltMask);
+            if (rank == 0 && color <= M3_GRAPH_COLORS)
+            {
+                s_warpColor[warp][color] = __popc(peers);
+            }
+            __syncthreads();
+            if (color <= M3_GRAPH_COLORS)
+            {
+                int32_t slot = s_colorFill[color] + rank;
+                for (int32_t k = 0; k < warp; ++k)
+                {
+                    slot += s_warpColor[k][color];
+                }
+                s.lists[slot] = i;
+                s.conSlot[i] = slot;
+            }
+            __syncthreads();
+            if (tid <= M3_GRAPH_COLORS)
+            {
+                int32_t add = 0;
+                for (int32_t k = 0; k < M3_BLOCK / 32; ++k)
+                {
+                    add += s_warpColor[k][tid];
+                }
+                s_colorFill[tid] += add;
+            }
+            __syncthreads();
+        }
     }
     __syncthreads();
     M3_PHASE_MARK(M3_PHASE_COLOR)
@@ -1403,6 +1754,22 @@ __global__ void __launch_bounds__(M3_BLOCK, 2) m3SubstepKernel(const m3WorldView
         dP = cp;
         dQ = cq;
     }
+    // The joint rows join them when the world leaves room: a joint
+    // dependency chain is a sequence of single-thread row solves, each
+    // bound by the latency of its row reads.
+    m3JointDev* jrows = s.joints;
+    const int64_t jointOff =
+        m3AlignUp(cached ? (int64_t)bodyMax * M3_BODY_CACHE_BYTES : 0, 16);
+    if (jointCount > 0 &&
+        jointOff + (int64_t)jointCount * (int64_t)sizeof(m3JointDev) <= (int64_t)cacheBytes)
+    {
+        jrows = (m3JointDev*)(s_bodyCache + jointOff);
+        const int32_t words = jointCount * (int32_t)(sizeof(m3JointDev) / 4);
+        for (int32_t k = tid; k < words; k += M3_BLOCK)
+        {
+            ((uint32_t*)jrows)[k] = ((const uint32_t*)s.joints)[k];
+        }
+    }
     __syncthreads();
     // The substep loop (solver.c:4085-4203).
     for (int32_t sub = 0; sub < substeps; ++sub)
@@ -1422,7 +1789,7 @@ __global__ void __launch_bounds__(M3_BLOCK, 2) m3SubstepKernel(const m3WorldView
             for (int32_t k = s.jointLevelStart[level] + tid; k < s.jointLevelStart[level + 1];
                  k += M3_BLOCK)
             {
-                m3WarmStartJoint(wl, &s.joints[s.jointOrder[k]], dQ);
+                m3WarmStartJoint(wl, &jrows[s.jointOrder[k]], dQ);
             }
             __syncthreads();
         }
@@ -1454,7 +1821,7 @@ __global__ void __launch_bounds__(M3_BLOCK, 2) m3SubstepKernel(const m3WorldView
             for (int32_t k = s.jointLevelStart[level] + tid; k < s.jointLevelStart[level + 1];
                  k += M3_BLOCK)
             {
-                m3SolveJoint(wl, &s.joints[s.jointOrder[k]], dP, dQ, h, invH, true);
+                m3SolveJoint(wl, &jrows[s.jointOrder[k]], dP, dQ, h, invH, true);
             }
             __syncthreads();
         }
@@ -1493,7 +1860,7 @@ __global__ void __launch_bounds__(M3_BLOCK, 2) m3SubstepKernel(const m3WorldView
             for (int32_t k = s.jointLevelStart[level] + tid; k < s.jointLevelStart[level + 1];
                  k += M3_BLOCK)
             {
-                m3SolveJoint(wl, &s.joints[s.jointOrder[k]], dP, dQ, h, invH, false);
+                m3SolveJoint(wl, &jrows[s.jointOrder[k]], dP, dQ, h, invH, false);
             }
             __syncthreads();
         }
@@ -1556,7 +1923,7 @@ __global__ void __launch_bounds__(M3_BLOCK, 2) m3SubstepKernel(const m3WorldView
     }
     for (int32_t r = tid; r < jointCount; r += M3_BLOCK)
     {
-        m3StoreJoint(w, &s.joints[r]);
+        m3StoreJoint(w, &jrows[r]);
     }
     if (tid == 0)
     {
@@ -1846,6 +2213,12 @@ struct m3BatchCache
     int32_t* doffsets = nullptr;
     uint64_t* dhash = nullptr;
     int32_t cap = 0;
+    // Pair-family buckets of the flattened pairs: per-block counts and
+    // family offsets, and the bucket array (capacity: the batch's total
+    // pair capacity).
+    int32_t* dfamily = nullptr; // blockHist[M3_FAMILY_BLOCKS * M3F_COUNT], famStart[M3F_COUNT + 1]
+    int32_t* dbucket = nullptr;
+    int64_t bucketCap = 0;
 };
 static m3BatchCache s_batch;
 
@@ -1942,16 +2315,55 @@ static int32_t PrepareBatch(m3HostWorld** worlds, int32_t count)
     {
         return rc;
     }
-    s_batch.worlds.assign(worlds, worlds + count);
-    s_batch.epoch = g_m3ResidencyEpoch;
-    // Shared memory for the solve kernel's body cache: enough for the
-    // largest world of the batch, within the per-block limit.
-    int32_t maxBodies = 0;
+    int64_t pairTotal = 0;
     for (int32_t i = 0; i < count; ++i)
     {
-        maxBodies = worlds[i]->hv.sc->bodyMax > maxBodies ? worlds[i]->hv.sc->bodyMax : maxBodies;
+        pairTotal += worlds[i]->pairCap;
     }
-    int64_t want = (int64_t)maxBodies * M3_BODY_CACHE_BYTES;
+    if (s_batch.dfamily == nullptr)
+    {
+        rc = Check(cudaMalloc((void**)&s_batch.dfamily,
+                              sizeof(int32_t) * (size_t)(M3_FAMILY_BLOCKS * M3F_COUNT + M3F_COUNT + 1)),
+                   "cudaMalloc(family counts)");
+        if (rc != M3GPU_OK)
+        {
+            s_batch.dfamily = nullptr;
+            return rc;
+        }
+    }
+    if (pairTotal > s_batch.bucketCap)
+    {
+        cudaFree(s_batch.dbucket);
+        s_batch.dbucket = nullptr;
+        s_batch.bucketCap = 0;
+        rc = Check(cudaMalloc((void**)&s_batch.dbucket, sizeof(int32_t) * (size_t)pairTotal),
+                   "cudaMalloc(pair buckets)");
+        if (rc != M3GPU_OK)
+        {
+            s_batch.dbucket = nullptr;
+            return rc;
+        }
+        s_batch.bucketCap = pairTotal;
+    }
+    s_batch.worlds.assign(worlds, worlds + count);
+    s_batch.epoch = g_m3ResidencyEpoch;
+    // Shared memory for the substep kernel: the body cache of the
+    // largest world and, room permitting, each world's joint rows.  The
+    // joint rows never push a block past M3_TWO_BLOCK_SMEM (two blocks
+    // per SM); the body cache alone may go up to the per-block limit.
+    int64_t bodyOnly = 0;
+    int64_t want = 0;
+    for (int32_t i = 0; i < count; ++i)
+    {
+        const m3WorldScalars* sc = worlds[i]->hv.sc;
+        const int64_t bodies = (int64_t)sc->bodyMax * M3_BODY_CACHE_BYTES;
+        const int64_t withJoints =
+            m3AlignUp(bodies, 16) + (int64_t)sc->jointMax * (int64_t)sizeof(m3JointDev);
+        bodyOnly = bodies > bodyOnly ? bodies : bodyOnly;
+        want = withJoints > want ? withJoints : want;
+    }
+    const int64_t jointCap = bodyOnly > M3_TWO_BLOCK_SMEM ? bodyOnly : M3_TWO_BLOCK_SMEM;
+    want = want < jointCap ? want : jointCap;
     const int64_t limit = 200 * 1024;
     s_batch.cacheBytes = (int32_t)(want < limit ? want : limit);
     if (s_batch.cacheBytes > 48 * 1024)
@@ -1969,6 +2381,37 @@ static int32_t PrepareBatch(m3HostWorld** worlds, int32_t count)
         }
     }
     return rc;
+}
+
+// Narrowphase grid: enough 128-thread blocks to fill every SM several
+// times; the kernels stride over their pairs.
+static int32_t s_narrowGrid = 148 * 16;
+
+// The narrowphase of one step: family count and scatter, then one
+// kernel per covered family over its bucket.
+#define M3_NARROW_LAUNCHES (2 + M3F_UNSUPPORTED)
+static void LaunchNarrow(const m3WorldView* views, const int32_t* offsets, int32_t count)
+{
+    int32_t* blockHist = s_batch.dfamily;
+    int32_t* famStart = s_batch.dfamily + M3_FAMILY_BLOCKS * M3F_COUNT;
+    const int32_t* bucket = s_batch.dbucket;
+    m3FamilyCountKernel<<<M3_FAMILY_BLOCKS, M3_FAMILY_THREADS>>>(views, offsets, count, blockHist);
+    m3FamilyScatterKernel<<<M3_FAMILY_BLOCKS, M3_FAMILY_THREADS>>>(views, offsets, count,
+                                                                   blockHist, famStart,
+                                                                   s_batch.dbucket);
+    m3NarrowFamilyKernel<M3F_PLANE_HULL>
+        <<<s_narrowGrid, 128>>>(views, offsets, count, famStart, bucket);
+    m3NarrowFamilyKernel<M3F_HULL_HULL>
+        <<<s_narrowGrid, 128>>>(views, offsets, count, famStart, bucket);
+    m3NarrowFamilyKernel<M3F_PLANE_CAPSULE>
+        <<<s_narrowGrid, 128>>>(views, offsets, count, famStart, bucket);
+    m3NarrowFamilyKernel<M3F_CAPSULE_HULL>
+        <<<s_narrowGrid, 128>>>(views, offsets, count, famStart, bucket);
+    m3NarrowFamilyKernel<M3F_ROUND><<<s_narrowGrid, 128>>>(views, offsets, count, famStart, bucket);
+    m3NarrowFamilyKernel<M3F_PLANE_SPHERE>
+        <<<s_narrowGrid, 128>>>(views, offsets, count, famStart, bucket);
+    m3NarrowFamilyKernel<M3F_SPHERE_SPHERE>
+        <<<s_narrowGrid, 128>>>(views, offsets, count, famStart, bucket);
 }
 
 // The three per-world solve kernels of one step, in order on the current
@@ -1995,9 +2438,6 @@ static void LaunchSolve(const m3WorldView* views, const int32_t* order, int32_t 
 // (bounds, pairs, narrowphase), prepare, substeps, finish.
 #define M3_STAGES 4
 static float s_kernelMs[M3_STAGES] = {0.0f, 0.0f, 0.0f, 0.0f};
-// Narrowphase grid: enough 128-thread blocks to fill every SM several
-// times; the kernel strides over the batch's flattened pairs.
-static int32_t s_narrowGrid = 148 * 16;
 static std::vector<cudaEvent_t> s_events;
 static int32_t* s_dstatus = nullptr;
 
@@ -2092,12 +2532,12 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
         const cudaEvent_t* ev = &s_events[(size_t)(M3_STAGES * step)];
         m3BroadKernel<<<count, M3_BLOCK>>>(s_batch.dviews, s_batch.dorder, count);
         m3PairOffsetsKernel<<<1, M3_BLOCK>>>(s_batch.dviews, count, s_batch.doffsets);
-        m3NarrowKernel<<<s_narrowGrid, 128>>>(s_batch.dviews, s_batch.doffsets, count);
+        LaunchNarrow(s_batch.dviews, s_batch.doffsets, count);
         cudaEventRecord(ev[1]);
         LaunchSolve(s_batch.dviews, s_batch.dorder, count, dt, substeps, s_batch.cacheBytes,
                     ev + 2);
         cudaEventRecord(ev[4]);
-        s_launches += 6;
+        s_launches += 5 + M3_NARROW_LAUNCHES;
     }
     cudaMemsetAsync(s_dstatus, 0, sizeof(int32_t));
     m3StatusKernel<<<(count + 255) / 256, 256>>>(s_batch.dviews, count, s_dstatus);
