@@ -12,6 +12,10 @@
 
 #include <string.h>
 
+#include <map>
+#include <utility>
+#include <vector>
+
 static int s_deviceState = 0; // 0 unknown, 1 ready, -1 absent
 static int s_device = 0;
 
@@ -63,6 +67,106 @@ int32_t m3gpuEnsureDevice(void)
     return M3GPU_OK;
 }
 
+// Device memory for slabs and hull pools: blocks carved from large
+// cudaMalloc chunks of the current device and reused through exact-size
+// free lists (cudaMalloc is a slow driver call: one per 512 MiB instead
+// of two per world).  Chunks stay allocated until the process exits.
+namespace
+{
+constexpr size_t kDevChunkBytes = (size_t)512 << 20;
+
+struct DevChunk
+{
+    int device;
+    uint8_t* base;
+    size_t bytes;
+    size_t used;
+};
+
+struct DevArena
+{
+    std::vector<DevChunk> chunks;
+    std::map<std::pair<int, size_t>, std::vector<void*>> freeBlocks;
+};
+
+DevArena& TheDevArena()
+{
+    static DevArena* arena = new DevArena();
+    return *arena;
+}
+
+size_t RoundDev(size_t bytes)
+{
+    return bytes == 0 ? M3_SLAB_ALIGN : (bytes + M3_SLAB_ALIGN - 1) / M3_SLAB_ALIGN * M3_SLAB_ALIGN;
+}
+} // namespace
+
+static cudaError_t DevAlloc(void** out, size_t bytes)
+{
+    DevArena& a = TheDevArena();
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess)
+    {
+        return e;
+    }
+    const size_t size = RoundDev(bytes);
+    auto it = a.freeBlocks.find(std::make_pair(device, size));
+    if (it != a.freeBlocks.end() && !it->second.empty())
+    {
+        *out = it->second.back();
+        it->second.pop_back();
+        return cudaSuccess;
+    }
+    for (auto c = a.chunks.rbegin(); c != a.chunks.rend(); ++c)
+    {
+        if (c->device != device)
+        {
+            continue;
+        }
+        if (c->bytes - c->used >= size)
+        {
+            *out = c->base + c->used;
+            c->used += size;
+            return cudaSuccess;
+        }
+        break; // only the device's newest chunk is bumped
+    }
+    size_t chunkBytes = size > kDevChunkBytes ? size : kDevChunkBytes;
+    void* base = nullptr;
+    e = cudaMalloc(&base, chunkBytes);
+    if (e != cudaSuccess && chunkBytes > size)
+    {
+        cudaGetLastError();
+        chunkBytes = size; // memory is short: just this block
+        e = cudaMalloc(&base, chunkBytes);
+    }
+    if (e != cudaSuccess)
+    {
+        return e;
+    }
+    a.chunks.push_back(DevChunk{device, (uint8_t*)base, chunkBytes, size});
+    *out = base;
+    return cudaSuccess;
+}
+
+static void DevFree(void* p, size_t bytes)
+{
+    if (p == nullptr)
+    {
+        return;
+    }
+    DevArena& a = TheDevArena();
+    for (const DevChunk& c : a.chunks)
+    {
+        if ((uint8_t*)p >= c.base && (uint8_t*)p < c.base + c.bytes)
+        {
+            a.freeBlocks[std::make_pair(c.device, RoundDev(bytes))].push_back(p);
+            return;
+        }
+    }
+}
+
 static int32_t CudaCheck(cudaError_t e, const char* what)
 {
     if (e != cudaSuccess)
@@ -95,7 +199,7 @@ int32_t m3gpuReserve(m3HostWorld* w)
     }
     w->scratchBytes = m3gpuScratchBytes(w->bodyCap, w->shapeCap, w->jointCap, w->pairCap);
     w->dslabBytes = w->persistentBytes + w->scratchBytes;
-    rc = CudaCheck(cudaMalloc((void**)&w->dslab, (size_t)w->dslabBytes), "cudaMalloc(slab)");
+    rc = CudaCheck(DevAlloc((void**)&w->dslab, (size_t)w->dslabBytes), "allocate slab");
     if (rc != M3GPU_OK)
     {
         w->dslab = nullptr;
@@ -112,8 +216,8 @@ int32_t m3gpuReserve(m3HostWorld* w)
     if (rc == M3GPU_OK && w->dhulls == nullptr)
     {
         const int32_t cap = hullCount < 4 ? 4 : hullCount;
-        rc = CudaCheck(cudaMalloc((void**)&w->dhulls, (size_t)cap * sizeof(m3HullData)),
-                       "cudaMalloc(hulls)");
+        rc = CudaCheck(DevAlloc((void**)&w->dhulls, (size_t)cap * sizeof(m3HullData)),
+                       "allocate hull pool");
         w->dhullCap = rc == M3GPU_OK ? cap : 0;
         if (rc != M3GPU_OK)
         {
@@ -135,7 +239,7 @@ int32_t m3gpuUpload(m3HostWorld* w)
     {
         w->scratchBytes = m3gpuScratchBytes(w->bodyCap, w->shapeCap, w->jointCap, w->pairCap);
         w->dslabBytes = w->persistentBytes + w->scratchBytes;
-        rc = CudaCheck(cudaMalloc((void**)&w->dslab, (size_t)w->dslabBytes), "cudaMalloc(slab)");
+        rc = CudaCheck(DevAlloc((void**)&w->dslab, (size_t)w->dslabBytes), "allocate slab");
         g_m3ResidencyEpoch += 1;
         if (rc != M3GPU_OK)
         {
@@ -148,13 +252,13 @@ int32_t m3gpuUpload(m3HostWorld* w)
     {
         if (w->dhulls != nullptr)
         {
-            cudaFree(w->dhulls);
+            DevFree(w->dhulls, (size_t)w->dhullCap * sizeof(m3HullData));
             w->dhulls = nullptr;
         }
         g_m3ResidencyEpoch += 1;
         int32_t cap = hullCount < 4 ? 4 : hullCount;
-        rc = CudaCheck(cudaMalloc((void**)&w->dhulls, (size_t)cap * sizeof(m3HullData)),
-                       "cudaMalloc(hulls)");
+        rc = CudaCheck(DevAlloc((void**)&w->dhulls, (size_t)cap * sizeof(m3HullData)),
+                       "allocate hull pool");
         if (rc != M3GPU_OK)
         {
             w->dhullCap = 0;
@@ -165,7 +269,7 @@ int32_t m3gpuUpload(m3HostWorld* w)
     if (w->dhulls == nullptr)
     {
         g_m3ResidencyEpoch += 1;
-        rc = CudaCheck(cudaMalloc((void**)&w->dhulls, 4 * sizeof(m3HullData)), "cudaMalloc(hulls)");
+        rc = CudaCheck(DevAlloc((void**)&w->dhulls, 4 * sizeof(m3HullData)), "allocate hull pool");
         if (rc != M3GPU_OK)
         {
             return rc;
@@ -307,12 +411,12 @@ void m3gpuRelease(m3HostWorld* w)
     }
     if (w->dslab != nullptr)
     {
-        cudaFree(w->dslab);
+        DevFree(w->dslab, (size_t)w->dslabBytes);
         w->dslab = nullptr;
     }
     if (w->dhulls != nullptr)
     {
-        cudaFree(w->dhulls);
+        DevFree(w->dhulls, (size_t)w->dhullCap * sizeof(m3HullData));
         w->dhulls = nullptr;
     }
     w->dhullCap = 0;

@@ -1694,7 +1694,10 @@ __global__ void __launch_bounds__(M3_BLOCK) m3PrepareKernel(const m3WorldView* v
 // ---------------------------------------------------------------------
 // Kernel 3: the substep loop, restitution and the impulse store
 // ---------------------------------------------------------------------
-__global__ void __launch_bounds__(M3_BLOCK, 2) m3SubstepKernel(const m3WorldView* views,
+// NT threads per world (one of the size classes below); MIN_BLOCKS keeps
+// the register budget at 128 per thread for every class.
+template <int NT, int MIN_BLOCKS>
+__global__ void __launch_bounds__(NT, MIN_BLOCKS) m3SubstepKernel(const m3WorldView* views,
                                                             const int32_t* order, int32_t count,
                                                             float dt, int32_t substeps,
                                                             int32_t cacheBytes)
@@ -1742,7 +1745,7 @@ __global__ void __launch_bounds__(M3_BLOCK, 2) m3SubstepKernel(const m3WorldView
         m3Vec3* cv = (m3Vec3*)(cq + bodyMax);
         m3Vec3* cw = cv + bodyMax;
         m3Vec3* cp = cw + bodyMax;
-        for (int32_t i = tid; i < bodyMax; i += M3_BLOCK)
+        for (int32_t i = tid; i < bodyMax; i += NT)
         {
             cv[i] = w.v[i];
             cw[i] = w.w[i];
@@ -1765,7 +1768,7 @@ __global__ void __launch_bounds__(M3_BLOCK, 2) m3SubstepKernel(const m3WorldView
     {
         jrows = (m3JointDev*)(s_bodyCache + jointOff);
         const int32_t words = jointCount * (int32_t)(sizeof(m3JointDev) / 4);
-        for (int32_t k = tid; k < words; k += M3_BLOCK)
+        for (int32_t k = tid; k < words; k += NT)
         {
             ((uint32_t*)jrows)[k] = ((const uint32_t*)s.joints)[k];
         }
@@ -1774,7 +1777,7 @@ __global__ void __launch_bounds__(M3_BLOCK, 2) m3SubstepKernel(const m3WorldView
     // The substep loop (solver.c:4085-4203).
     for (int32_t sub = 0; sub < substeps; ++sub)
     {
-        for (int32_t m = tid; m < moverCount; m += M3_BLOCK)
+        for (int32_t m = tid; m < moverCount; m += NT)
         {
             int32_t i = s.movers[m];
             if (w.btype[i] == M3_BODY_DYNAMIC)
@@ -1787,7 +1790,7 @@ __global__ void __launch_bounds__(M3_BLOCK, 2) m3SubstepKernel(const m3WorldView
         for (int32_t level = 0; level < jointLevels; ++level)
         {
             for (int32_t k = s.jointLevelStart[level] + tid; k < s.jointLevelStart[level + 1];
-                 k += M3_BLOCK)
+                 k += NT)
             {
                 m3WarmStartJoint(wl, &jrows[s.jointOrder[k]], dQ);
             }
@@ -1802,7 +1805,7 @@ __global__ void __launch_bounds__(M3_BLOCK, 2) m3SubstepKernel(const m3WorldView
             {
                 continue;
             }
-            for (int32_t k = a + tid; k < b; k += M3_BLOCK)
+            for (int32_t k = a + tid; k < b; k += NT)
             {
                 m3WarmStartContact(wl, m3ConAt(s.rows, k));
             }
@@ -1819,7 +1822,7 @@ __global__ void __launch_bounds__(M3_BLOCK, 2) m3SubstepKernel(const m3WorldView
         for (int32_t level = 0; level < jointLevels; ++level)
         {
             for (int32_t k = s.jointLevelStart[level] + tid; k < s.jointLevelStart[level + 1];
-                 k += M3_BLOCK)
+                 k += NT)
             {
                 m3SolveJoint(wl, &jrows[s.jointOrder[k]], dP, dQ, h, invH, true);
             }
@@ -1834,7 +1837,7 @@ __global__ void __launch_bounds__(M3_BLOCK, 2) m3SubstepKernel(const m3WorldView
             {
                 continue;
             }
-            for (int32_t k = a + tid; k < b; k += M3_BLOCK)
+            for (int32_t k = a + tid; k < b; k += NT)
             {
                 m3SolveContact(wl, m3ConAt(s.rows, k), dP, dQ, invH, pushMax, true);
             }
@@ -1849,7 +1852,7 @@ __global__ void __launch_bounds__(M3_BLOCK, 2) m3SubstepKernel(const m3WorldView
         }
         __syncthreads();
         M3_PHASE_MARK(M3_PHASE_SOLVE)
-        for (int32_t m = tid; m < moverCount; m += M3_BLOCK)
+        for (int32_t m = tid; m < moverCount; m += NT)
         {
             m3IntegratePosition(wl, s.movers[m], h, dP, dQ);
         }
@@ -1858,7 +1861,7 @@ __global__ void __launch_bounds__(M3_BLOCK, 2) m3SubstepKernel(const m3WorldView
         for (int32_t level = 0; level < jointLevels; ++level)
         {
             for (int32_t k = s.jointLevelStart[level] + tid; k < s.jointLevelStart[level + 1];
-                 k += M3_BLOCK)
+                 k += NT)
             {
                 m3SolveJoint(wl, &jrows[s.jointOrder[k]], dP, dQ, h, invH, false);
             }
@@ -1872,7 +1875,7 @@ __global__ void __launch_bounds__(M3_BLOCK, 2) m3SubstepKernel(const m3WorldView
             {
                 continue;
             }
-            for (int32_t k = a + tid; k < b; k += M3_BLOCK)
+            for (int32_t k = a + tid; k < b; k += NT)
             {
                 m3SolveContact(wl, m3ConAt(s.rows, k), dP, dQ, invH, pushMax,
                                false);
@@ -1892,7 +1895,7 @@ __global__ void __launch_bounds__(M3_BLOCK, 2) m3SubstepKernel(const m3WorldView
     }
 
     // Forces live one step (solver.c:4207-4211).
-    for (int32_t m = tid; m < moverCount; m += M3_BLOCK)
+    for (int32_t m = tid; m < moverCount; m += NT)
     {
         int32_t i = s.movers[m];
         w.force[i] = v3(0.0f, 0.0f, 0.0f);
@@ -1910,18 +1913,18 @@ __global__ void __launch_bounds__(M3_BLOCK, 2) m3SubstepKernel(const m3WorldView
     __syncthreads();
     if (cached)
     {
-        for (int32_t i = tid; i < bodyMax; i += M3_BLOCK)
+        for (int32_t i = tid; i < bodyMax; i += NT)
         {
             w.v[i] = wl.v[i];
             w.w[i] = wl.w[i];
         }
     }
     __syncthreads();
-    for (int32_t i = tid; i < constraintCount; i += M3_BLOCK)
+    for (int32_t i = tid; i < constraintCount; i += NT)
     {
         m3StoreContact(m3ConAt(s.rows, i), man);
     }
-    for (int32_t r = tid; r < jointCount; r += M3_BLOCK)
+    for (int32_t r = tid; r < jointCount; r += NT)
     {
         m3StoreJoint(w, &jrows[r]);
     }
@@ -2219,6 +2222,10 @@ struct m3BatchCache
     int32_t* dfamily = nullptr; // blockHist[M3_FAMILY_BLOCKS * M3F_COUNT], famStart[M3F_COUNT + 1]
     int32_t* dbucket = nullptr;
     int64_t bucketCap = 0;
+    // Substep size classes: order[classFirst[c] .. classFirst[c + 1]) and
+    // each class's dynamic shared memory.
+    int32_t classFirst[4] = {0, 0, 0, 0};
+    int32_t classCache[3] = {0, 0, 0};
 };
 static m3BatchCache s_batch;
 
@@ -2228,6 +2235,104 @@ static int32_t Check(cudaError_t e, const char* what)
     {
         return m3gpuSetError(M3GPU_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
     }
+    return M3GPU_OK;
+}
+
+// Substep size classes: a world's threads follow its size (shape slots;
+// the batch order is by shape slots, largest first, so each class is a
+// contiguous run of the order).  Large worlds get 512 threads: twice the
+// rows per colour in flight and half as many worlds resident at once,
+// whose rows then stay in L2 across the passes.  Small worlds get 64:
+// eight worlds share an SM instead of two, hiding each other's joint
+// chains.  Every class keeps 128 registers per thread.
+#define M3_CLASSES 3
+static const int32_t s_classMinShapes[M3_CLASSES] = {769, 161, 0};
+
+static void LaunchSubstepClass(int32_t c, cudaStream_t stream, const m3WorldView* views,
+                               const int32_t* order, int32_t count, float dt, int32_t substeps,
+                               int32_t cacheBytes)
+{
+    if (count <= 0)
+    {
+        return;
+    }
+    if (c == 0)
+    {
+        m3SubstepKernel<512, 1><<<count, 512, cacheBytes, stream>>>(views, order, count, dt,
+                                                                    substeps, cacheBytes);
+    }
+    else if (c == 1)
+    {
+        m3SubstepKernel<256, 2><<<count, 256, cacheBytes, stream>>>(views, order, count, dt,
+                                                                    substeps, cacheBytes);
+    }
+    else
+    {
+        m3SubstepKernel<64, 8><<<count, 64, cacheBytes, stream>>>(views, order, count, dt,
+                                                                  substeps, cacheBytes);
+    }
+}
+
+static int32_t SetSubstepSmem(int32_t c, int32_t bytes)
+{
+    cudaError_t e = cudaSuccess;
+    if (c == 0)
+    {
+        e = cudaFuncSetAttribute(m3SubstepKernel<512, 1>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    }
+    else if (c == 1)
+    {
+        e = cudaFuncSetAttribute(m3SubstepKernel<256, 2>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    }
+    else
+    {
+        e = cudaFuncSetAttribute(m3SubstepKernel<64, 8>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    }
+    if (e != cudaSuccess)
+    {
+        return m3gpuSetError(M3GPU_ERR_CUDA, "cudaFuncSetAttribute(substep smem): %s",
+                             cudaGetErrorString(e));
+    }
+    return M3GPU_OK;
+}
+
+// Streams for the classes (they run side by side), and the events that
+// fork them off the default stream after the prepare kernel and join
+// them back before the finish kernel.
+struct m3ClassStreams
+{
+    int device = -1;
+    cudaStream_t stream[M3_CLASSES] = {};
+    cudaEvent_t fork = nullptr;
+    cudaEvent_t join[M3_CLASSES] = {};
+};
+static m3ClassStreams s_classStreams;
+
+static int32_t EnsureClassStreams()
+{
+    int device = 0;
+    cudaGetDevice(&device);
+    if (s_classStreams.device == device)
+    {
+        return M3GPU_OK;
+    }
+    cudaError_t e = cudaEventCreateWithFlags(&s_classStreams.fork, cudaEventDisableTiming);
+    for (int32_t c = 0; e == cudaSuccess && c < M3_CLASSES; ++c)
+    {
+        e = cudaStreamCreateWithFlags(&s_classStreams.stream[c], cudaStreamNonBlocking);
+        if (e == cudaSuccess)
+        {
+            e = cudaEventCreateWithFlags(&s_classStreams.join[c], cudaEventDisableTiming);
+        }
+    }
+    if (e != cudaSuccess)
+    {
+        return m3gpuSetError(M3GPU_ERR_CUDA, "class streams: %s", cudaGetErrorString(e));
+    }
+    s_classStreams.device = device;
     return M3GPU_OK;
 }
 
@@ -2372,12 +2477,46 @@ static int32_t PrepareBatch(m3HostWorld** worlds, int32_t count)
                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         s_batch.cacheBytes),
                    "cudaFuncSetAttribute(prepare smem)");
-        if (rc == M3GPU_OK)
+    }
+    // Size classes over the largest-first order, and each class's shared
+    // memory: its largest body cache, plus joint rows within the budget
+    // that keeps the class's blocks per SM (one 512-thread block, two
+    // 256-thread blocks, eight 64-thread blocks).
+    static const int64_t classSmem[M3_CLASSES] = {200 * 1024, M3_TWO_BLOCK_SMEM, 27 * 1024};
+    int32_t c = 0;
+    s_batch.classFirst[0] = 0;
+    for (int32_t k = 0; k < count; ++k)
+    {
+        const int32_t shapes = worlds[order[(size_t)k]]->hv.sc->shapeMax;
+        while (c < M3_CLASSES - 1 && shapes < s_classMinShapes[c])
         {
-            rc = Check(cudaFuncSetAttribute(m3SubstepKernel,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            s_batch.cacheBytes),
-                       "cudaFuncSetAttribute(substep smem)");
+            s_batch.classFirst[++c] = k;
+        }
+    }
+    while (c < M3_CLASSES)
+    {
+        s_batch.classFirst[++c] = count;
+    }
+    for (int32_t k = 0; rc == M3GPU_OK && k < M3_CLASSES; ++k)
+    {
+        int64_t cBodies = 0;
+        int64_t cWant = 0;
+        for (int32_t j = s_batch.classFirst[k]; j < s_batch.classFirst[k + 1]; ++j)
+        {
+            const m3WorldScalars* sc = worlds[order[(size_t)j]]->hv.sc;
+            const int64_t bodies = (int64_t)sc->bodyMax * M3_BODY_CACHE_BYTES;
+            const int64_t withJoints =
+                m3AlignUp(bodies, 16) + (int64_t)sc->jointMax * (int64_t)sizeof(m3JointDev);
+            cBodies = bodies > cBodies ? bodies : cBodies;
+            cWant = withJoints > cWant ? withJoints : cWant;
+        }
+        const int64_t cap = cBodies > classSmem[k] ? cBodies : classSmem[k];
+        cWant = cWant < cap ? cWant : cap;
+        cWant = cWant < limit ? cWant : limit;
+        s_batch.classCache[k] = (int32_t)cWant;
+        if (cWant > 48 * 1024)
+        {
+            rc = SetSubstepSmem(k, (int32_t)cWant);
         }
     }
     return rc;
@@ -2416,8 +2555,13 @@ static void LaunchNarrow(const m3WorldView* views, const int32_t* offsets, int32
 
 // The three per-world solve kernels of one step, in order on the current
 // stream.  `marks`, when given, receives an event after the first two.
+// The three per-world solve kernels of one step on the default stream,
+// the substep kernel split by size class when `classFirst` is given
+// (classFirst[c] .. classFirst[c + 1] index `order`).  `marks`, when
+// given, receives an event after the prepare and after the substep stage.
 static void LaunchSolve(const m3WorldView* views, const int32_t* order, int32_t count, float dt,
-                        int32_t substeps, int32_t cacheBytes, const cudaEvent_t* marks)
+                        int32_t substeps, int32_t cacheBytes, const cudaEvent_t* marks,
+                        const int32_t* classFirst = nullptr, const int32_t* classCache = nullptr)
 {
     m3PrepareKernel<<<count, M3_BLOCK, cacheBytes>>>(views, order, count, dt, substeps,
                                                      cacheBytes);
@@ -2425,8 +2569,28 @@ static void LaunchSolve(const m3WorldView* views, const int32_t* order, int32_t 
     {
         cudaEventRecord(marks[0]);
     }
-    m3SubstepKernel<<<count, M3_BLOCK, cacheBytes>>>(views, order, count, dt, substeps,
-                                                     cacheBytes);
+    if (classFirst == nullptr)
+    {
+        m3SubstepKernel<256, 2><<<count, 256, cacheBytes>>>(views, order, count, dt, substeps,
+                                                            cacheBytes);
+    }
+    else
+    {
+        cudaEventRecord(s_classStreams.fork, 0);
+        for (int32_t c = 0; c < M3_CLASSES; ++c)
+        {
+            const int32_t n = classFirst[c + 1] - classFirst[c];
+            if (n <= 0)
+            {
+                continue;
+            }
+            cudaStreamWaitEvent(s_classStreams.stream[c], s_classStreams.fork, 0);
+            LaunchSubstepClass(c, s_classStreams.stream[c], views, order + classFirst[c], n, dt,
+                               substeps, classCache[c]);
+            cudaEventRecord(s_classStreams.join[c], s_classStreams.stream[c]);
+            cudaStreamWaitEvent(0, s_classStreams.join[c], 0);
+        }
+    }
     if (marks != nullptr)
     {
         cudaEventRecord(marks[1]);
@@ -2500,6 +2664,10 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
         return rc;
     }
     rc = PrepareBatch(worlds, count);
+    if (rc == M3GPU_OK)
+    {
+        rc = EnsureClassStreams();
+    }
     if (rc != M3GPU_OK)
     {
         return rc;
@@ -2535,7 +2703,7 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
         LaunchNarrow(s_batch.dviews, s_batch.doffsets, count);
         cudaEventRecord(ev[1]);
         LaunchSolve(s_batch.dviews, s_batch.dorder, count, dt, substeps, s_batch.cacheBytes,
-                    ev + 2);
+                    ev + 2, s_batch.classFirst, s_batch.classCache);
         cudaEventRecord(ev[4]);
         s_launches += 5 + M3_NARROW_LAUNCHES;
     }
