@@ -210,14 +210,14 @@ extern "C" int64_t m3gpuScratchBytes(int32_t bodyCap, int32_t shapeCap, int32_t 
 // Exclusive prefix sum of a[0, n) in place; returns the total.  Each
 // thread scans a contiguous chunk, chunk totals are scanned in shared
 // memory.  Must be called by every thread of the block.
-__device__ int32_t BlockExclusiveScan(int32_t* a, int32_t n)
+template <int NT> __device__ int32_t BlockExclusiveScan(int32_t* a, int32_t n)
 {
-    __shared__ int32_t warpSums[M3_BLOCK / 32];
+    __shared__ int32_t warpSums[NT / 32];
     __shared__ int32_t total;
     const int32_t t = threadIdx.x;
     const int32_t lane = t & 31;
     const int32_t warp = t >> 5;
-    const int32_t chunk = (n + M3_BLOCK - 1) / M3_BLOCK;
+    const int32_t chunk = (n + NT - 1) / NT;
     const int32_t lo = t * chunk < n ? t * chunk : n;
     const int32_t hi = lo + chunk < n ? lo + chunk : n;
     int32_t sum = 0;
@@ -243,7 +243,7 @@ __device__ int32_t BlockExclusiveScan(int32_t* a, int32_t n)
     __syncthreads();
     if (warp == 0)
     {
-        int32_t v = lane < M3_BLOCK / 32 ? warpSums[lane] : 0;
+        int32_t v = lane < NT / 32 ? warpSums[lane] : 0;
         int32_t inc = v;
         for (int32_t o = 1; o < 32; o <<= 1)
         {
@@ -253,11 +253,11 @@ __device__ int32_t BlockExclusiveScan(int32_t* a, int32_t n)
                 inc += y;
             }
         }
-        if (lane < M3_BLOCK / 32)
+        if (lane < NT / 32)
         {
             warpSums[lane] = inc - v;
         }
-        if (lane == M3_BLOCK / 32 - 1)
+        if (lane == NT / 32 - 1)
         {
             total = inc;
         }
@@ -568,7 +568,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3BroadKernel(const m3WorldView* vie
         }
     }
     __syncthreads();
-    const int32_t total = BlockExclusiveScan(s.rowCount, shapeMax);
+    const int32_t total = BlockExclusiveScan<M3_BLOCK>(s.rowCount, shapeMax);
     if (total > sc->pairCap)
     {
         // The reference's m3UpdatePairs refuses with m3_errorCapacity
@@ -622,7 +622,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3BroadKernel(const m3WorldView* vie
                                  : 0;
         }
         __syncthreads();
-        BlockExclusiveScan(s.planeFlag, shapeMax);
+        BlockExclusiveScan<M3_BLOCK>(s.planeFlag, shapeMax);
         const int32_t base = s.rowCount[pl];
         for (int32_t i = tid; i < shapeMax; i += M3_BLOCK)
         {
@@ -1154,7 +1154,8 @@ __device__ void ContinuousVersusPlane(const m3WorldView& w, int32_t body, int32_
 // share an SM (228 KB per SM, 1 KB reserved per block, static arrays).
 #define M3_TWO_BLOCK_SMEM (110 * 1024)
 
-__global__ void __launch_bounds__(M3_BLOCK) m3PrepareKernel(const m3WorldView* views,
+template <int NT, int MIN_BLOCKS>
+__global__ void __launch_bounds__(NT, MIN_BLOCKS) m3PrepareKernel(const m3WorldView* views,
                                                             const int32_t* order, int32_t count,
                                                             float dt, int32_t substeps,
                                                             int32_t cacheBytes)
@@ -1195,7 +1196,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3PrepareKernel(const m3WorldView* v
 
     // Begin-of-step centres and rotations (solver.c:3866-3877); island
     // arrays reset.
-    for (int32_t i = tid; i < bodyMax; i += M3_BLOCK)
+    for (int32_t i = tid; i < bodyMax; i += NT)
     {
         s.parent[i] = i;
         s.forced[i] = 0;
@@ -1216,7 +1217,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3PrepareKernel(const m3WorldView* v
     __syncthreads();
 
     // Island wake pass (solver.c:3468-3578).
-    for (int32_t k = tid; k < pairCount; k += M3_BLOCK)
+    for (int32_t k = tid; k < pairCount; k += NT)
     {
         if (man[k].pointCount == 0)
         {
@@ -1231,7 +1232,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3PrepareKernel(const m3WorldView* v
         }
         MarkKinematicContact(w, s, w.shapeBody[shapeA], w.shapeBody[shapeB]);
     }
-    for (int32_t j = tid; j < jointMax; j += M3_BLOCK)
+    for (int32_t j = tid; j < jointMax; j += NT)
     {
         if (w.jointAlive[j] != 0)
         {
@@ -1239,7 +1240,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3PrepareKernel(const m3WorldView* v
         }
     }
     __syncthreads();
-    for (int32_t i = tid; i < bodyMax; i += M3_BLOCK)
+    for (int32_t i = tid; i < bodyMax; i += NT)
     {
         if (w.bodyAlive[i] == 0 || w.btype[i] != M3_BODY_DYNAMIC)
         {
@@ -1251,7 +1252,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3PrepareKernel(const m3WorldView* v
         }
     }
     __syncthreads();
-    for (int32_t i = tid; i < bodyMax; i += M3_BLOCK)
+    for (int32_t i = tid; i < bodyMax; i += NT)
     {
         if (w.bodyAlive[i] == 0 || w.btype[i] != M3_BODY_DYNAMIC)
         {
@@ -1263,7 +1264,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3PrepareKernel(const m3WorldView* v
             w.sleepTime[i] = 0.0f;
         }
     }
-    for (int32_t i = tid; i < bodyMax; i += M3_BLOCK)
+    for (int32_t i = tid; i < bodyMax; i += NT)
     {
         s.deltaPos[i] = v3(0.0f, 0.0f, 0.0f);
         s.deltaRot[i] = m3IdentityQuat();
@@ -1275,7 +1276,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3PrepareKernel(const m3WorldView* v
     const m3real h = dt / (m3real)substeps;
     const m3SoftDev soft = m3MakeSoft(sc->contactHertz, sc->contactDampingRatio, h);
     const m3SoftDev staticSoft = m3MakeSoft(2.0f * sc->contactHertz, sc->contactDampingRatio, h);
-    for (int32_t k = tid; k < pairCount; k += M3_BLOCK)
+    for (int32_t k = tid; k < pairCount; k += NT)
     {
         int32_t flag = 0;
         if (man[k].pointCount != 0)
@@ -1295,8 +1296,8 @@ __global__ void __launch_bounds__(M3_BLOCK) m3PrepareKernel(const m3WorldView* v
         s.pairFlag[k] = flag;
     }
     __syncthreads();
-    const int32_t constraintCount = BlockExclusiveScan(s.pairFlag, pairCount);
-    for (int32_t k = tid; k < pairCount; k += M3_BLOCK)
+    const int32_t constraintCount = BlockExclusiveScan<NT>(s.pairFlag, pairCount);
+    for (int32_t k = tid; k < pairCount; k += NT)
     {
         int32_t next = k + 1 < pairCount ? s.pairFlag[k + 1] : constraintCount;
         if (next != s.pairFlag[k])
@@ -1310,7 +1311,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3PrepareKernel(const m3WorldView* v
     // of its bodies (any body, static ones included), so the joints of
     // one level touch disjoint bodies and solving level by level, each
     // level in parallel, reproduces the reference's serial slot order.
-    for (int32_t j = tid; j < jointMax; j += M3_BLOCK)
+    for (int32_t j = tid; j < jointMax; j += NT)
     {
         int32_t flag = 0;
         if (w.jointAlive[j] != 0)
@@ -1329,8 +1330,8 @@ __global__ void __launch_bounds__(M3_BLOCK) m3PrepareKernel(const m3WorldView* v
         s.jointFlag[j] = flag;
     }
     __syncthreads();
-    const int32_t jointCount = BlockExclusiveScan(s.jointFlag, jointMax);
-    for (int32_t j = tid; j < jointMax; j += M3_BLOCK)
+    const int32_t jointCount = BlockExclusiveScan<NT>(s.jointFlag, jointMax);
+    for (int32_t j = tid; j < jointMax; j += NT)
     {
         int32_t next = j + 1 < jointMax ? s.jointFlag[j + 1] : jointCount;
         if (next != s.jointFlag[j])
@@ -1419,13 +1420,13 @@ __global__ void __launch_bounds__(M3_BLOCK) m3PrepareKernel(const m3WorldView* v
     int32_t* cMin1 = cMin0 + (staged ? bodyWords : (int64_t)sc->bodyCap);
     int2* cPair = staged ? (int2*)(s_colorStage + 12 * bodyWords) : s.conPair;
     uint8_t* cColor = staged ? (uint8_t*)(cPair + constraintCount) : s.colors;
-    for (int32_t i = tid; i < bodyMax; i += M3_BLOCK)
+    for (int32_t i = tid; i < bodyMax; i += NT)
     {
         cMask[i] = 0u;
         cMin0[i] = INT32_MAX;
         cMin1[i] = INT32_MAX;
     }
-    for (int32_t i = tid; i < constraintCount; i += M3_BLOCK)
+    for (int32_t i = tid; i < constraintCount; i += NT)
     {
         const uint64_t key = keys[s.conPairIndex[i]];
         const int32_t bodyA = w.shapeBody[(int32_t)(key >> 32)];
@@ -1441,7 +1442,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3PrepareKernel(const m3WorldView* v
     {
         int32_t* cur = (round & 1) ? cMin1 : cMin0;
         int32_t* nxt = (round & 1) ? cMin0 : cMin1;
-        for (int32_t i = tid; i < constraintCount; i += M3_BLOCK)
+        for (int32_t i = tid; i < constraintCount; i += NT)
         {
             if (cColor[i] == M3_COLOR_PENDING)
             {
@@ -1458,7 +1459,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3PrepareKernel(const m3WorldView* v
         }
         __syncthreads();
         int32_t waiting = 0;
-        for (int32_t i = tid; i < constraintCount; i += M3_BLOCK)
+        for (int32_t i = tid; i < constraintCount; i += NT)
         {
             if (cColor[i] != M3_COLOR_PENDING)
             {
@@ -1531,13 +1532,13 @@ __global__ void __launch_bounds__(M3_BLOCK) m3PrepareKernel(const m3WorldView* v
     }
     // Colour sizes and offsets.
     __shared__ int32_t s_colorFill[M3_GRAPH_COLORS + 1];
-    __shared__ int32_t s_warpColor[M3_BLOCK / 32][M3_GRAPH_COLORS + 1];
+    __shared__ int32_t s_warpColor[NT / 32][M3_GRAPH_COLORS + 1];
     if (tid <= M3_GRAPH_COLORS)
     {
         s_colorFill[tid] = 0;
     }
     __syncthreads();
-    for (int32_t i = tid; i < constraintCount; i += M3_BLOCK)
+    for (int32_t i = tid; i < constraintCount; i += NT)
     {
         atomicAdd(&s_colorFill[cColor[i]], 1);
     }
@@ -1564,11 +1565,11 @@ __global__ void __launch_bounds__(M3_BLOCK) m3PrepareKernel(const m3WorldView* v
         const int32_t lane = tid & 31;
         const int32_t warp = tid >> 5;
         const uint32_t ltMask = (1u << lane) - 1u;
-        for (int32_t c0 = 0; c0 < constraintCount; c0 += M3_BLOCK)
+        for (int32_t c0 = 0; c0 < constraintCount; c0 += NT)
         {
             const int32_t i = c0 + tid;
             const int32_t color = i < constraintCount ? (int32_t)cColor[i] : M3_GRAPH_COLORS + 1;
-            for (int32_t k = tid; k < (M3_BLOCK / 32) * (M3_GRAPH_COLORS + 1); k += M3_BLOCK)
+            for (int32_t k = tid; k < (NT / 32) * (M3_GRAPH_COLORS + 1); k += NT)
             {
                 (&s_warpColor[0][0])[k] = 0;
             }
@@ -1594,7 +1595,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3PrepareKernel(const m3WorldView* v
             if (tid <= M3_GRAPH_COLORS)
             {
                 int32_t add = 0;
-                for (int32_t k = 0; k < M3_BLOCK / 32; ++k)
+                for (int32_t k = 0; k < NT / 32; ++k)
                 {
                     add += s_warpColor[k][tid];
                 }
@@ -1607,7 +1608,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3PrepareKernel(const m3WorldView* v
     M3_PHASE_MARK(M3_PHASE_COLOR)
     // Contact rows (solver.c:261-405), prepared straight into their
     // solve slots; consecutive threads write consecutive slots.
-    for (int32_t slot = tid; slot < constraintCount; slot += M3_BLOCK)
+    for (int32_t slot = tid; slot < constraintCount; slot += NT)
     {
         m3ContactDev c;
         m3PrepareContact(w, &c, s.conPairIndex[s.lists[slot]], keys, man, soft, staticSoft);
@@ -1635,7 +1636,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3PrepareKernel(const m3WorldView* v
 
     // Movers: alive, enabled, kinematic or awake dynamic, ascending
     // (solver.c:3945-3983), with the kinematic servo.
-    for (int32_t i = tid; i < bodyMax; i += M3_BLOCK)
+    for (int32_t i = tid; i < bodyMax; i += NT)
     {
         int32_t flag = 0;
         if (w.bodyAlive[i] != 0 && w.enabled[i] != 0)
@@ -1665,8 +1666,8 @@ __global__ void __launch_bounds__(M3_BLOCK) m3PrepareKernel(const m3WorldView* v
         s.moverFlag[i] = flag;
     }
     __syncthreads();
-    const int32_t moverCount = BlockExclusiveScan(s.moverFlag, bodyMax);
-    for (int32_t i = tid; i < bodyMax; i += M3_BLOCK)
+    const int32_t moverCount = BlockExclusiveScan<NT>(s.moverFlag, bodyMax);
+    for (int32_t i = tid; i < bodyMax; i += NT)
     {
         int32_t next = i + 1 < bodyMax ? s.moverFlag[i + 1] : moverCount;
         if (next != s.moverFlag[i])
@@ -2248,52 +2249,72 @@ static int32_t Check(cudaError_t e, const char* what)
 #define M3_CLASSES 3
 static const int32_t s_classMinShapes[M3_CLASSES] = {769, 161, 0};
 
-static void LaunchSubstepClass(int32_t c, cudaStream_t stream, const m3WorldView* views,
-                               const int32_t* order, int32_t count, float dt, int32_t substeps,
-                               int32_t cacheBytes)
+// One class's prepare (stage 0) or substep (stage 1) kernel.
+static void LaunchClass(int32_t stage, int32_t c, cudaStream_t stream, const m3WorldView* views,
+                        const int32_t* order, int32_t count, float dt, int32_t substeps,
+                        int32_t cacheBytes)
 {
     if (count <= 0)
     {
         return;
     }
+#define M3_LAUNCH_CLASS(NT, MB)                                                                    \
+    if (stage == 0)                                                                                \
+    {                                                                                              \
+        m3PrepareKernel<NT, MB><<<count, NT, cacheBytes, stream>>>(views, order, count, dt,       \
+                                                                   substeps, cacheBytes);          \
+    }                                                                                              \
+    else                                                                                           \
+    {                                                                                              \
+        m3SubstepKernel<NT, MB><<<count, NT, cacheBytes, stream>>>(views, order, count, dt,       \
+                                                                   substeps, cacheBytes);          \
+    }
     if (c == 0)
     {
-        m3SubstepKernel<512, 1><<<count, 512, cacheBytes, stream>>>(views, order, count, dt,
-                                                                    substeps, cacheBytes);
+        M3_LAUNCH_CLASS(512, 1)
     }
     else if (c == 1)
     {
-        m3SubstepKernel<256, 2><<<count, 256, cacheBytes, stream>>>(views, order, count, dt,
-                                                                    substeps, cacheBytes);
+        M3_LAUNCH_CLASS(256, 2)
     }
     else
     {
-        m3SubstepKernel<64, 8><<<count, 64, cacheBytes, stream>>>(views, order, count, dt,
-                                                                  substeps, cacheBytes);
+        M3_LAUNCH_CLASS(64, 8)
     }
+#undef M3_LAUNCH_CLASS
 }
 
-static int32_t SetSubstepSmem(int32_t c, int32_t bytes)
+static int32_t SetClassSmem(int32_t c, int32_t bytes)
 {
     cudaError_t e = cudaSuccess;
+    const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
     if (c == 0)
     {
-        e = cudaFuncSetAttribute(m3SubstepKernel<512, 1>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        e = cudaFuncSetAttribute(m3PrepareKernel<512, 1>, a, bytes);
+        if (e == cudaSuccess)
+        {
+            e = cudaFuncSetAttribute(m3SubstepKernel<512, 1>, a, bytes);
+        }
     }
     else if (c == 1)
     {
-        e = cudaFuncSetAttribute(m3SubstepKernel<256, 2>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        e = cudaFuncSetAttribute(m3PrepareKernel<256, 2>, a, bytes);
+        if (e == cudaSuccess)
+        {
+            e = cudaFuncSetAttribute(m3SubstepKernel<256, 2>, a, bytes);
+        }
     }
     else
     {
-        e = cudaFuncSetAttribute(m3SubstepKernel<64, 8>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        e = cudaFuncSetAttribute(m3PrepareKernel<64, 8>, a, bytes);
+        if (e == cudaSuccess)
+        {
+            e = cudaFuncSetAttribute(m3SubstepKernel<64, 8>, a, bytes);
+        }
     }
     if (e != cudaSuccess)
     {
-        return m3gpuSetError(M3GPU_ERR_CUDA, "cudaFuncSetAttribute(substep smem): %s",
+        return m3gpuSetError(M3GPU_ERR_CUDA, "cudaFuncSetAttribute(class smem): %s",
                              cudaGetErrorString(e));
     }
     return M3GPU_OK;
@@ -2471,13 +2492,6 @@ static int32_t PrepareBatch(m3HostWorld** worlds, int32_t count)
     want = want < jointCap ? want : jointCap;
     const int64_t limit = 200 * 1024;
     s_batch.cacheBytes = (int32_t)(want < limit ? want : limit);
-    if (s_batch.cacheBytes > 48 * 1024)
-    {
-        rc = Check(cudaFuncSetAttribute(m3PrepareKernel,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        s_batch.cacheBytes),
-                   "cudaFuncSetAttribute(prepare smem)");
-    }
     // Size classes over the largest-first order, and each class's shared
     // memory: its largest body cache, plus joint rows within the budget
     // that keeps the class's blocks per SM (one 512-thread block, two
@@ -2516,7 +2530,7 @@ static int32_t PrepareBatch(m3HostWorld** worlds, int32_t count)
         s_batch.classCache[k] = (int32_t)cWant;
         if (cWant > 48 * 1024)
         {
-            rc = SetSubstepSmem(k, (int32_t)cWant);
+            rc = SetClassSmem(k, (int32_t)cWant);
         }
     }
     return rc;
@@ -2555,16 +2569,45 @@ static void LaunchNarrow(const m3WorldView* views, const int32_t* offsets, int32
 
 // The three per-world solve kernels of one step, in order on the current
 // stream.  `marks`, when given, receives an event after the first two.
-// The three per-world solve kernels of one step on the default stream,
-// the substep kernel split by size class when `classFirst` is given
-// (classFirst[c] .. classFirst[c + 1] index `order`).  `marks`, when
-// given, receives an event after the prepare and after the substep stage.
+// The three per-world solve kernels of one step on the default stream.
+// With `classFirst` (classFirst[c] .. classFirst[c + 1] index `order`)
+// the prepare and substep stages run per size class on the class
+// streams, forked off and joined back to the default stream around each
+// stage; without it (one world, the allocation-free path) every kernel
+// runs at 256 threads.  `marks`, when given, receives an event after the
+// prepare and after the substep stage.
+static void ClassStage(int32_t stage, const m3WorldView* views, const int32_t* order, float dt,
+                       int32_t substeps, const int32_t* classFirst, const int32_t* classCache)
+{
+    cudaEventRecord(s_classStreams.fork, 0);
+    for (int32_t c = 0; c < M3_CLASSES; ++c)
+    {
+        const int32_t n = classFirst[c + 1] - classFirst[c];
+        if (n <= 0)
+        {
+            continue;
+        }
+        cudaStreamWaitEvent(s_classStreams.stream[c], s_classStreams.fork, 0);
+        LaunchClass(stage, c, s_classStreams.stream[c], views, order + classFirst[c], n, dt,
+                    substeps, classCache[c]);
+        cudaEventRecord(s_classStreams.join[c], s_classStreams.stream[c]);
+        cudaStreamWaitEvent(0, s_classStreams.join[c], 0);
+    }
+}
+
 static void LaunchSolve(const m3WorldView* views, const int32_t* order, int32_t count, float dt,
                         int32_t substeps, int32_t cacheBytes, const cudaEvent_t* marks,
                         const int32_t* classFirst = nullptr, const int32_t* classCache = nullptr)
 {
-    m3PrepareKernel<<<count, M3_BLOCK, cacheBytes>>>(views, order, count, dt, substeps,
-                                                     cacheBytes);
+    if (classFirst == nullptr)
+    {
+        m3PrepareKernel<256, 2><<<count, 256, cacheBytes>>>(views, order, count, dt, substeps,
+                                                            cacheBytes);
+    }
+    else
+    {
+        ClassStage(0, views, order, dt, substeps, classFirst, classCache);
+    }
     if (marks != nullptr)
     {
         cudaEventRecord(marks[0]);
@@ -2576,20 +2619,7 @@ static void LaunchSolve(const m3WorldView* views, const int32_t* order, int32_t 
     }
     else
     {
-        cudaEventRecord(s_classStreams.fork, 0);
-        for (int32_t c = 0; c < M3_CLASSES; ++c)
-        {
-            const int32_t n = classFirst[c + 1] - classFirst[c];
-            if (n <= 0)
-            {
-                continue;
-            }
-            cudaStreamWaitEvent(s_classStreams.stream[c], s_classStreams.fork, 0);
-            LaunchSubstepClass(c, s_classStreams.stream[c], views, order + classFirst[c], n, dt,
-                               substeps, classCache[c]);
-            cudaEventRecord(s_classStreams.join[c], s_classStreams.stream[c]);
-            cudaStreamWaitEvent(0, s_classStreams.join[c], 0);
-        }
+        ClassStage(1, views, order, dt, substeps, classFirst, classCache);
     }
     if (marks != nullptr)
     {
