@@ -144,12 +144,10 @@ __device__ __forceinline__ m3Vec3 m3VelocityAt(const m3WorldView& w, int32_t bod
 #define M3C_RESTITUTION 27
 #define M3C_INV_MASS_A 28
 #define M3C_INV_MASS_B 29
-#define M3C_INV_I_A 30
-#define M3C_INV_I_B 39
-#define M3C_SOFT 48 // biasRate, massScale, impulseScale
-#define M3C_ROLLING 51
-#define M3C_ROLLING_K 52
-#define M3C_POINT0 61 // per point: rA, rB, baseSeparation, normalMass, leverArm, relativeVelocity
+#define M3C_SOFT 30 // biasRate, massScale, impulseScale
+#define M3C_ROLLING 33
+#define M3C_ROLLING_K 34
+#define M3C_POINT0 43 // per point: rA, rB, baseSeparation, normalMass, leverArm, relativeVelocity
 #define M3C_POINT_WORDS 10
 #define M3C_WORDS (M3C_POINT0 + M3C_POINT_WORDS * M3_MANIFOLD_MAX_POINTS)
 
@@ -212,6 +210,10 @@ __device__ __forceinline__ m3ConRef m3ConAt(const m3ConRows& r, int32_t slot)
 }
 
 // The two bodies of a row and their mass terms, loaded once per row.
+// The world-space inverse inertia tensors are not row words: every row
+// of a body uses the same prepare-time tensor (m3WorldInvInertiaDev), so
+// they come from a per-body table (shared memory in the substep loop),
+// read by body index.
 struct m3ConBodies
 {
     int32_t a;
@@ -224,7 +226,7 @@ struct m3ConBodies
     m3Mat3 iB;
 };
 
-__device__ __forceinline__ m3ConBodies m3LoadConBodies(const m3ConRef& c)
+__device__ __forceinline__ m3ConBodies m3LoadConBodies(const m3ConRef& c, const m3Mat3* invI)
 {
     m3ConBodies cb;
     cb.a = c.n(M3C_BODY_A);
@@ -234,8 +236,8 @@ __device__ __forceinline__ m3ConBodies m3LoadConBodies(const m3ConRef& c)
     cb.dynB = (flags & 2) != 0;
     cb.mA = c.f(M3C_INV_MASS_A);
     cb.mB = c.f(M3C_INV_MASS_B);
-    cb.iA = c.m(M3C_INV_I_A);
-    cb.iB = c.m(M3C_INV_I_B);
+    cb.iA = invI[cb.a];
+    cb.iB = invI[cb.b];
     return cb;
 }
 
@@ -269,7 +271,7 @@ __device__ __forceinline__ m3real m3EffectiveMass(const m3ContactDev* c, m3Vec3 
 // Per-constraint body of PrepareContacts (solver.c:261-405).
 __device__ void m3PrepareContact(const m3WorldView& w, m3ContactDev* c, int32_t pairIndex,
                                  const uint64_t* keys, const m3Manifold* manifolds,
-                                 m3SoftDev soft, m3SoftDev staticSoft)
+                                 m3SoftDev soft, m3SoftDev staticSoft, const m3Mat3* invI)
 {
     const m3Manifold* manifold = &manifolds[pairIndex];
     uint64_t key = keys[pairIndex];
@@ -290,8 +292,8 @@ __device__ void m3PrepareContact(const m3WorldView& w, m3ContactDev* c, int32_t 
     m3MakeTangentBasis(c->normal, &c->t1, &c->t2);
     c->invMassA = c->dynA ? w.invMass[bodyA] : 0.0f;
     c->invMassB = c->dynB ? w.invMass[bodyB] : 0.0f;
-    c->invIA = m3WorldInvInertiaDev(w, bodyA);
-    c->invIB = m3WorldInvInertiaDev(w, bodyB);
+    c->invIA = invI[bodyA];
+    c->invIB = invI[bodyB];
     float fricA = w.friction[shapeA];
     float fricB = w.friction[shapeB];
     float restA = w.restitution[shapeA];
@@ -415,8 +417,6 @@ __device__ void m3WriteContactRow(const m3ConRows& r, int32_t slot, const m3Cont
     put(M3C_RESTITUTION, c.restitution);
     put(M3C_INV_MASS_A, c.invMassA);
     put(M3C_INV_MASS_B, c.invMassB);
-    putm(M3C_INV_I_A, c.invIA);
-    putm(M3C_INV_I_B, c.invIB);
     put(M3C_SOFT, c.softness.biasRate);
     put(M3C_SOFT + 1, c.softness.massScale);
     put(M3C_SOFT + 2, c.softness.impulseScale);
@@ -447,9 +447,9 @@ __device__ void m3WriteContactRow(const m3ConRows& r, int32_t slot, const m3Cont
 }
 
 // solver.c:408-428
-__device__ void m3WarmStartContact(const m3WorldView& w, const m3ConRef& c)
+__device__ void m3WarmStartContact(const m3WorldView& w, const m3ConRef& c, const m3Mat3* invI)
 {
-    const m3ConBodies cb = m3LoadConBodies(c);
+    const m3ConBodies cb = m3LoadConBodies(c, invI);
     const int32_t pc = c.n(M3C_POINTS);
     const m3Vec3 normal = c.v(M3C_NORMAL);
     m3real imp[M3_MANIFOLD_MAX_POINTS];
@@ -485,11 +485,11 @@ __device__ void m3WarmStartContact(const m3WorldView& w, const m3ConRef& c)
 }
 
 // solver.c:430-574
-__device__ void m3SolveContact(const m3WorldView& w, const m3ConRef& c, const m3Vec3* deltaPos,
-                               const m3Quat* deltaRot, m3real invH, m3real pushMaxSpeed,
-                               bool useBias)
+__device__ void m3SolveContact(const m3WorldView& w, const m3ConRef& c, const m3Mat3* invI,
+                               const m3Vec3* deltaPos, const m3Quat* deltaRot, m3real invH,
+                               m3real pushMaxSpeed, bool useBias)
 {
-    const m3ConBodies cb = m3LoadConBodies(c);
+    const m3ConBodies cb = m3LoadConBodies(c, invI);
     const int32_t pc = c.n(M3C_POINTS);
     const m3Vec3 normal = c.v(M3C_NORMAL);
     m3real imp[M3_MANIFOLD_MAX_POINTS];
@@ -641,14 +641,15 @@ __device__ void m3SolveContact(const m3WorldView& w, const m3ConRef& c, const m3
 }
 
 // solver.c:2879-2906 (one constraint's points, in order).
-__device__ void m3RestituteContact(const m3WorldView& w, const m3ConRef& c, m3real threshold)
+__device__ void m3RestituteContact(const m3WorldView& w, const m3ConRef& c, const m3Mat3* invI,
+                                   m3real threshold)
 {
     const m3real restitution = c.f(M3C_RESTITUTION);
     if (restitution == 0.0f)
     {
         return;
     }
-    const m3ConBodies cb = m3LoadConBodies(c);
+    const m3ConBodies cb = m3LoadConBodies(c, invI);
     const int32_t pc = c.n(M3C_POINTS);
     const m3Vec3 normal = c.v(M3C_NORMAL);
     for (int32_t k = 0; k < pc; ++k)

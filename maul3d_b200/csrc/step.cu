@@ -114,6 +114,7 @@ struct m3Scratch
     int32_t* ready;        // per body
     m3Vec3* deltaPos;      // per body
     m3Quat* deltaRot;      // per body
+    m3Mat3* bodyInvI;      // per body: prepare-time world inverse inertia
     int32_t* movers;       // per body
     int32_t* moverFlag;    // per body
     uint32_t* bodyMask;    // per body
@@ -169,6 +170,7 @@ static __host__ __device__ inline int64_t ScratchCarve(m3Scratch* s, uint8_t* ba
     M3_CARVE(ready, int32_t, bodyCap)
     M3_CARVE(deltaPos, m3Vec3, bodyCap)
     M3_CARVE(deltaRot, m3Quat, bodyCap)
+    M3_CARVE(bodyInvI, m3Mat3, bodyCap)
     M3_CARVE(movers, int32_t, bodyCap)
     M3_CARVE(moverFlag, int32_t, bodyCap + 1)
     M3_CARVE(bodyMask, uint32_t, bodyCap)
@@ -435,7 +437,8 @@ __device__ __forceinline__ void SweepFrom(const m3WorldView& w, const m3Scratch&
     }
 }
 
-__global__ void __launch_bounds__(M3_BLOCK) m3BroadKernel(const m3WorldView* views,
+template <int NT, int MIN_BLOCKS>
+__global__ void __launch_bounds__(NT, MIN_BLOCKS) m3BroadKernel(const m3WorldView* views,
                                                           const int32_t* order, int32_t count)
 {
     const int32_t wi = order[blockIdx.x];
@@ -463,7 +466,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3BroadKernel(const m3WorldView* vie
     const int32_t shapeMax = sc->shapeMax;
 
     // Fresh bounds once per shape; the sweep set and the plane list.
-    for (int32_t i = tid; i < shapeMax; i += M3_BLOCK)
+    for (int32_t i = tid; i < shapeMax; i += NT)
     {
         s.rowCount[i] = 0;
         s.rowFill[i] = 0;
@@ -501,7 +504,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3BroadKernel(const m3WorldView* vie
     {
         pow2 <<= 1;
     }
-    for (int32_t i = tid; i < pow2; i += M3_BLOCK)
+    for (int32_t i = tid; i < pow2; i += NT)
     {
         if (i < n)
         {
@@ -519,7 +522,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3BroadKernel(const m3WorldView* vie
     {
         for (int32_t j = k >> 1; j > 0; j >>= 1)
         {
-            for (int32_t i = tid; i < pow2; i += M3_BLOCK)
+            for (int32_t i = tid; i < pow2; i += NT)
             {
                 int32_t ixj = i ^ j;
                 if (ixj > i)
@@ -546,11 +549,11 @@ __global__ void __launch_bounds__(M3_BLOCK) m3BroadKernel(const m3WorldView* vie
     M3_PHASE_MARK(M3_PHASE_SORT)
     // Count every row's pairs.
     const int32_t planeCount = s_planeCount;
-    for (int32_t p = tid; p < n; p += M3_BLOCK)
+    for (int32_t p = tid; p < n; p += NT)
     {
         SweepFrom(w, s, p, n, [&](int32_t lo, int32_t hi) { atomicAdd(&s.rowCount[lo], 1); });
     }
-    for (int32_t i = tid; i < shapeMax; i += M3_BLOCK)
+    for (int32_t i = tid; i < shapeMax; i += NT)
     {
         if (w.shapeAlive[i] == 0 || w.shapeType[i] == M3_SHAPE_PLANE)
         {
@@ -568,7 +571,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3BroadKernel(const m3WorldView* vie
         }
     }
     __syncthreads();
-    const int32_t total = BlockExclusiveScan<M3_BLOCK>(s.rowCount, shapeMax);
+    const int32_t total = BlockExclusiveScan<NT>(s.rowCount, shapeMax);
     if (total > sc->pairCap)
     {
         // The reference's m3UpdatePairs refuses with m3_errorCapacity
@@ -586,14 +589,14 @@ __global__ void __launch_bounds__(M3_BLOCK) m3BroadKernel(const m3WorldView* vie
     M3_PHASE_MARK(M3_PHASE_COUNT)
     // Fill rows: sweep pairs through per-row cursors, then each plane's
     // own row in ascending partner order by a scan.
-    for (int32_t p = tid; p < n; p += M3_BLOCK)
+    for (int32_t p = tid; p < n; p += NT)
     {
         SweepFrom(w, s, p, n, [&](int32_t lo, int32_t hi) {
             int32_t slot = atomicAdd(&s.rowFill[lo], 1);
             newKeys[s.rowCount[lo] + slot] = ((uint64_t)(uint32_t)lo << 32) | (uint64_t)(uint32_t)hi;
         });
     }
-    for (int32_t i = tid; i < shapeMax; i += M3_BLOCK)
+    for (int32_t i = tid; i < shapeMax; i += NT)
     {
         if (w.shapeAlive[i] == 0 || w.shapeType[i] == M3_SHAPE_PLANE)
         {
@@ -614,7 +617,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3BroadKernel(const m3WorldView* vie
     {
         const int32_t pl = s_planes[k];
         __syncthreads();
-        for (int32_t i = tid; i < shapeMax; i += M3_BLOCK)
+        for (int32_t i = tid; i < shapeMax; i += NT)
         {
             s.planeFlag[i] = (i > pl && w.shapeAlive[i] != 0 && w.shapeType[i] != M3_SHAPE_PLANE &&
                               PairAllowed(w, pl, i))
@@ -622,9 +625,9 @@ __global__ void __launch_bounds__(M3_BLOCK) m3BroadKernel(const m3WorldView* vie
                                  : 0;
         }
         __syncthreads();
-        BlockExclusiveScan<M3_BLOCK>(s.planeFlag, shapeMax);
+        BlockExclusiveScan<NT>(s.planeFlag, shapeMax);
         const int32_t base = s.rowCount[pl];
-        for (int32_t i = tid; i < shapeMax; i += M3_BLOCK)
+        for (int32_t i = tid; i < shapeMax; i += NT)
         {
             int32_t next = i + 1 < shapeMax ? s.planeFlag[i + 1] : -1;
             bool flagged = i + 1 < shapeMax ? next != s.planeFlag[i]
@@ -640,7 +643,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3BroadKernel(const m3WorldView* vie
     }
     __syncthreads();
     // Order each non-plane row by partner index (rows are short).
-    for (int32_t i = tid; i < shapeMax; i += M3_BLOCK)
+    for (int32_t i = tid; i < shapeMax; i += NT)
     {
         if (w.shapeAlive[i] == 0 || w.shapeType[i] == M3_SHAPE_PLANE)
         {
@@ -1203,6 +1206,7 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3PrepareKernel(const m3WorldV
         s.forcedRoot[i] = 0;
         if (w.bodyAlive[i] == 0)
         {
+            s.bodyInvI[i] = m3ZeroMat3();
             continue;
         }
         const m3Transform xf = w.xf[i];
@@ -1213,6 +1217,9 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3PrepareKernel(const m3WorldV
         c.z = xf.p.z + (double)rlc.z;
         s.com0[i] = c;
         s.rot0[i] = xf.q;
+        // The contact rows' world-space inverse inertia, once per body
+        // (the transforms do not change before the rows are prepared).
+        s.bodyInvI[i] = m3WorldInvInertiaDev(w, i);
     }
     __syncthreads();
 
@@ -1611,7 +1618,8 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3PrepareKernel(const m3WorldV
     for (int32_t slot = tid; slot < constraintCount; slot += NT)
     {
         m3ContactDev c;
-        m3PrepareContact(w, &c, s.conPairIndex[s.lists[slot]], keys, man, soft, staticSoft);
+        m3PrepareContact(w, &c, s.conPairIndex[s.lists[slot]], keys, man, soft, staticSoft,
+                         s.bodyInvI);
         m3WriteContactRow(s.rows, slot, c);
         if (c.restitution != 0.0f)
         {
@@ -1758,12 +1766,25 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3SubstepKernel(const m3WorldV
         dP = cp;
         dQ = cq;
     }
-    // The joint rows join them when the world leaves room: a joint
+    // Then the per-body inverse inertia table of the contact rows, when
+    // the world fits, and the joint rows when it leaves room: a joint
     // dependency chain is a sequence of single-thread row solves, each
     // bound by the latency of its row reads.
+    const m3Mat3* invI = s.bodyInvI;
+    int64_t smemUsed = m3AlignUp(cached ? (int64_t)bodyMax * M3_BODY_CACHE_BYTES : 0, 16);
+    if (cached && smemUsed + (int64_t)bodyMax * (int64_t)sizeof(m3Mat3) <= (int64_t)cacheBytes)
+    {
+        m3Mat3* table = (m3Mat3*)(s_bodyCache + smemUsed);
+        const int32_t words = bodyMax * (int32_t)(sizeof(m3Mat3) / 4);
+        for (int32_t k = tid; k < words; k += NT)
+        {
+            ((uint32_t*)table)[k] = ((const uint32_t*)s.bodyInvI)[k];
+        }
+        invI = table;
+        smemUsed = m3AlignUp(smemUsed + (int64_t)bodyMax * (int64_t)sizeof(m3Mat3), 16);
+    }
     m3JointDev* jrows = s.joints;
-    const int64_t jointOff =
-        m3AlignUp(cached ? (int64_t)bodyMax * M3_BODY_CACHE_BYTES : 0, 16);
+    const int64_t jointOff = smemUsed;
     if (jointCount > 0 &&
         jointOff + (int64_t)jointCount * (int64_t)sizeof(m3JointDev) <= (int64_t)cacheBytes)
     {
@@ -1808,7 +1829,7 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3SubstepKernel(const m3WorldV
             }
             for (int32_t k = a + tid; k < b; k += NT)
             {
-                m3WarmStartContact(wl, m3ConAt(s.rows, k));
+                m3WarmStartContact(wl, m3ConAt(s.rows, k), invI);
             }
             __syncthreads();
         }
@@ -1816,7 +1837,7 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3SubstepKernel(const m3WorldV
         {
             for (int32_t k = s_starts[M3_GRAPH_COLORS]; k < s_starts[M3_GRAPH_COLORS + 1]; ++k)
             {
-                m3WarmStartContact(wl, m3ConAt(s.rows, k));
+                m3WarmStartContact(wl, m3ConAt(s.rows, k), invI);
             }
         }
         __syncthreads();
@@ -1840,7 +1861,7 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3SubstepKernel(const m3WorldV
             }
             for (int32_t k = a + tid; k < b; k += NT)
             {
-                m3SolveContact(wl, m3ConAt(s.rows, k), dP, dQ, invH, pushMax, true);
+                m3SolveContact(wl, m3ConAt(s.rows, k), invI, dP, dQ, invH, pushMax, true);
             }
             __syncthreads();
         }
@@ -1848,7 +1869,7 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3SubstepKernel(const m3WorldV
         {
             for (int32_t k = s_starts[M3_GRAPH_COLORS]; k < s_starts[M3_GRAPH_COLORS + 1]; ++k)
             {
-                m3SolveContact(wl, m3ConAt(s.rows, k), dP, dQ, invH, pushMax, true);
+                m3SolveContact(wl, m3ConAt(s.rows, k), invI, dP, dQ, invH, pushMax, true);
             }
         }
         __syncthreads();
@@ -1878,7 +1899,7 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3SubstepKernel(const m3WorldV
             }
             for (int32_t k = a + tid; k < b; k += NT)
             {
-                m3SolveContact(wl, m3ConAt(s.rows, k), dP, dQ, invH, pushMax,
+                m3SolveContact(wl, m3ConAt(s.rows, k), invI, dP, dQ, invH, pushMax,
                                false);
             }
             __syncthreads();
@@ -1887,7 +1908,7 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3SubstepKernel(const m3WorldV
         {
             for (int32_t k = s_starts[M3_GRAPH_COLORS]; k < s_starts[M3_GRAPH_COLORS + 1]; ++k)
             {
-                m3SolveContact(wl, m3ConAt(s.rows, k), dP, dQ, invH, pushMax,
+                m3SolveContact(wl, m3ConAt(s.rows, k), invI, dP, dQ, invH, pushMax,
                                false);
             }
         }
@@ -1908,7 +1929,7 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3SubstepKernel(const m3WorldV
         const m3real threshold = sc->restitutionThreshold;
         for (int32_t i = 0; i < constraintCount; ++i)
         {
-            m3RestituteContact(wl, m3ConAt(s.rows, s.conSlot[i]), threshold);
+            m3RestituteContact(wl, m3ConAt(s.rows, s.conSlot[i]), invI, threshold);
         }
     }
     __syncthreads();
@@ -2493,9 +2514,10 @@ static int32_t PrepareBatch(m3HostWorld** worlds, int32_t count)
     const int64_t limit = 200 * 1024;
     s_batch.cacheBytes = (int32_t)(want < limit ? want : limit);
     // Size classes over the largest-first order, and each class's shared
-    // memory: its largest body cache, plus joint rows within the budget
-    // that keeps the class's blocks per SM (one 512-thread block, two
-    // 256-thread blocks, eight 64-thread blocks).
+    // memory: its largest body cache, plus the inverse inertia table and
+    // the joint rows within the budget that keeps the class's blocks per
+    // SM (one 512-thread block, two 256-thread blocks, eight 64-thread
+    // blocks).
     static const int64_t classSmem[M3_CLASSES] = {200 * 1024, M3_TWO_BLOCK_SMEM, 27 * 1024};
     int32_t c = 0;
     s_batch.classFirst[0] = 0;
@@ -2519,10 +2541,12 @@ static int32_t PrepareBatch(m3HostWorld** worlds, int32_t count)
         {
             const m3WorldScalars* sc = worlds[order[(size_t)j]]->hv.sc;
             const int64_t bodies = (int64_t)sc->bodyMax * M3_BODY_CACHE_BYTES;
-            const int64_t withJoints =
-                m3AlignUp(bodies, 16) + (int64_t)sc->jointMax * (int64_t)sizeof(m3JointDev);
+            const int64_t withTables =
+                m3AlignUp(m3AlignUp(bodies, 16) + (int64_t)sc->bodyMax * (int64_t)sizeof(m3Mat3),
+                          16) +
+                (int64_t)sc->jointMax * (int64_t)sizeof(m3JointDev);
             cBodies = bodies > cBodies ? bodies : cBodies;
-            cWant = withJoints > cWant ? withJoints : cWant;
+            cWant = withTables > cWant ? withTables : cWant;
         }
         const int64_t cap = cBodies > classSmem[k] ? cBodies : classSmem[k];
         cWant = cWant < cap ? cWant : cap;
@@ -2728,7 +2752,7 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
     for (int32_t step = 0; step < steps; ++step)
     {
         const cudaEvent_t* ev = &s_events[(size_t)(M3_STAGES * step)];
-        m3BroadKernel<<<count, M3_BLOCK>>>(s_batch.dviews, s_batch.dorder, count);
+        m3BroadKernel<M3_BLOCK, 2><<<count, M3_BLOCK>>>(s_batch.dviews, s_batch.dorder, count);
         m3PairOffsetsKernel<<<1, M3_BLOCK>>>(s_batch.dviews, count, s_batch.doffsets);
         LaunchNarrow(s_batch.dviews, s_batch.doffsets, count);
         cudaEventRecord(ev[1]);
@@ -2950,7 +2974,7 @@ extern "C" int32_t m3gpu_step_world_noalloc(m3WorldId worldId, float dt, int32_t
     int32_t* order = sym.table;
     int32_t* offsets = sym.table + 1;
     const int32_t cacheBytes = (int32_t)cache;
-    m3BroadKernel<<<1, M3_BLOCK>>>(sym.view, order, 1);
+    m3BroadKernel<M3_BLOCK, 1><<<1, M3_BLOCK>>>(sym.view, order, 1);
     m3PairOffsetsKernel<<<1, M3_BLOCK>>>(sym.view, 1, offsets);
     m3NarrowKernel<<<148, 128>>>(sym.view, offsets, 1);
     LaunchSolve(sym.view, order, 1, dt, substeps, cacheBytes, nullptr);
