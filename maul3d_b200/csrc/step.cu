@@ -95,7 +95,8 @@ struct m3StepPlan
     int32_t jointLevels;
     int32_t moverCount;
     int32_t anyRestitution;
-    int32_t starts[M3_GRAPH_COLORS + 2]; // colour offsets into the solve slots
+    int32_t levels; // joint/contact schedule levels; levelStart[levels] starts the overflow
+    int32_t starts[M3_GRAPH_COLORS + 2]; // colour sizes (as offsets) of the colouring
 };
 
 struct m3Scratch
@@ -106,6 +107,7 @@ struct m3Scratch
     int32_t* planeFlag;    // per shape: plane row scan
     uint64_t* sortKey;     // sweep order keys (power-of-two padded)
     int32_t* sortIdx;      // sweep order shape indices
+    uint64_t* sweepPairs;  // per pair: the sweep's pair keys, in discovery order
     m3Pos3* com0;          // per body
     m3Quat* rot0;          // per body
     int32_t* parent;       // per body (island union-find)
@@ -123,6 +125,9 @@ struct m3Scratch
     m3ConRows rows;        // contact rows, field-major, one slot per constraint
     int32_t* conPairIndex; // per constraint: its pair
     int32_t* conSlot;      // per constraint: its solve slot
+    int32_t* conLevel;     // per constraint: its level in the joint/contact schedule
+    int32_t* levelStart;   // level offsets into the solve slots (+ the overflow bucket)
+    int32_t* levelFill;    // level fill cursors
     int32_t* pairFlag;     // per pair (compaction)
     uint8_t* colors;       // per pair
     int2* conPair;         // per pair: colouring body pair
@@ -162,6 +167,7 @@ static __host__ __device__ inline int64_t ScratchCarve(m3Scratch* s, uint8_t* ba
     M3_CARVE(planeFlag, int32_t, shapeCap + 1)
     M3_CARVE(sortKey, uint64_t, NextPow2(shapeCap))
     M3_CARVE(sortIdx, int32_t, NextPow2(shapeCap))
+    M3_CARVE(sweepPairs, uint64_t, pairCap)
     M3_CARVE(com0, m3Pos3, bodyCap)
     M3_CARVE(rot0, m3Quat, bodyCap)
     M3_CARVE(parent, int32_t, bodyCap)
@@ -185,6 +191,9 @@ static __host__ __device__ inline int64_t ScratchCarve(m3Scratch* s, uint8_t* ba
     M3_CARVE(rows.acc, float, (int64_t)M3A_WORDS * rowStride)
     M3_CARVE(conPairIndex, int32_t, pairCap)
     M3_CARVE(conSlot, int32_t, pairCap)
+    M3_CARVE(conLevel, int32_t, pairCap)
+    M3_CARVE(levelStart, int32_t, (int64_t)jointCap + M3_GRAPH_COLORS + 3)
+    M3_CARVE(levelFill, int32_t, (int64_t)jointCap + M3_GRAPH_COLORS + 3)
     M3_CARVE(pairFlag, int32_t, pairCap + 1)
     M3_CARVE(colors, uint8_t, pairCap)
     M3_CARVE(conPair, int2, pairCap)
@@ -451,11 +460,13 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3BroadKernel(const m3WorldVie
     __shared__ int32_t s_planes[M3_MAX_PLANES];
     __shared__ int32_t s_planeCount;
     __shared__ int32_t s_sweepCount;
+    __shared__ int32_t s_sweepPairs;
     if (tid == 0)
     {
         s_status = sc->status;
         s_planeCount = 0;
         s_sweepCount = 0;
+        s_sweepPairs = 0;
     }
     __syncthreads();
     if (s_status != 0)
@@ -547,11 +558,20 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3BroadKernel(const m3WorldVie
     }
 
     M3_PHASE_MARK(M3_PHASE_SORT)
-    // Count every row's pairs.
+    // Count every row's pairs; the sweep's pairs are recorded on the way
+    // so the fill below need not sweep again.
     const int32_t planeCount = s_planeCount;
+    const int32_t pairCap = sc->pairCap;
     for (int32_t p = tid; p < n; p += NT)
     {
-        SweepFrom(w, s, p, n, [&](int32_t lo, int32_t hi) { atomicAdd(&s.rowCount[lo], 1); });
+        SweepFrom(w, s, p, n, [&](int32_t lo, int32_t hi) {
+            atomicAdd(&s.rowCount[lo], 1);
+            const int32_t r = atomicAdd(&s_sweepPairs, 1);
+            if (r < pairCap)
+            {
+                s.sweepPairs[r] = ((uint64_t)(uint32_t)lo << 32) | (uint64_t)(uint32_t)hi;
+            }
+        });
     }
     for (int32_t i = tid; i < shapeMax; i += NT)
     {
@@ -589,12 +609,13 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3BroadKernel(const m3WorldVie
     M3_PHASE_MARK(M3_PHASE_COUNT)
     // Fill rows: sweep pairs through per-row cursors, then each plane's
     // own row in ascending partner order by a scan.
-    for (int32_t p = tid; p < n; p += NT)
+    const int32_t swept = s_sweepPairs;
+    for (int32_t r = tid; r < swept; r += NT)
     {
-        SweepFrom(w, s, p, n, [&](int32_t lo, int32_t hi) {
-            int32_t slot = atomicAdd(&s.rowFill[lo], 1);
-            newKeys[s.rowCount[lo] + slot] = ((uint64_t)(uint32_t)lo << 32) | (uint64_t)(uint32_t)hi;
-        });
+        const uint64_t key = s.sweepPairs[r];
+        const int32_t lo = (int32_t)(key >> 32);
+        const int32_t slot = atomicAdd(&s.rowFill[lo], 1);
+        newKeys[s.rowCount[lo] + slot] = key;
     }
     for (int32_t i = tid; i < shapeMax; i += NT)
     {
@@ -1173,6 +1194,8 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3PrepareKernel(const m3WorldV
     __shared__ int32_t s_anyRestitution;
     __shared__ int32_t s_starts[M3_GRAPH_COLORS + 2];
     __shared__ int32_t s_jointLevels;
+    __shared__ int32_t s_contactLevels;
+    __shared__ int32_t s_totalLevels;
     if (tid == 0)
     {
         s_status = sc->status;
@@ -1612,6 +1635,110 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3PrepareKernel(const m3WorldV
         }
     }
     __syncthreads();
+    // One schedule for joints and contacts.  Per body, the reference
+    // applies its joints (slot order) and then its contacts (colour
+    // order) in each pass.  A contact's level is therefore at least one
+    // past the last joint level on either of its awake dynamic bodies and
+    // one past the level of the previous contact on either of them; the
+    // substep loop then runs level by level, joint rows and contact rows
+    // of a level together, so contacts away from the joint chains no
+    // longer wait for them.  The overflow colour stays last and serial.
+    // Contacts are re-slotted by level (any order inside a level: its
+    // rows touch disjoint bodies).
+    {
+        int32_t* cLast = cMin0; // per body: first level free for its next contact
+        for (int32_t i = tid; i < bodyMax; i += NT)
+        {
+            cLast[i] = jointCount > 0 ? s.ready[i] + 1 : 0;
+        }
+        if (tid == 0)
+        {
+            s_contactLevels = 0;
+        }
+        __syncthreads();
+        for (int32_t color = 0; color < M3_GRAPH_COLORS; ++color)
+        {
+            for (int32_t k = s_starts[color] + tid; k < s_starts[color + 1]; k += NT)
+            {
+                const int32_t i = s.lists[k];
+                const int2 p = cPair[i];
+                int32_t level = 0;
+                if (p.x >= 0)
+                {
+                    level = cLast[p.x] > level ? cLast[p.x] : level;
+                }
+                if (p.y >= 0)
+                {
+                    level = cLast[p.y] > level ? cLast[p.y] : level;
+                }
+                s.conLevel[i] = level;
+                if (p.x >= 0)
+                {
+                    cLast[p.x] = level + 1;
+                }
+                if (p.y >= 0)
+                {
+                    cLast[p.y] = level + 1;
+                }
+                atomicMax(&s_contactLevels, level + 1);
+            }
+            __syncthreads();
+        }
+        const int32_t levels = s_contactLevels > s_jointLevels ? s_contactLevels : s_jointLevels;
+        // Counts per level (the overflow colour is bucket `levels`),
+        // offsets, then each constraint claims a slot in its level.
+        for (int32_t k = tid; k <= levels + 1; k += NT)
+        {
+            s.levelStart[k] = 0;
+        }
+        __syncthreads();
+        for (int32_t i = tid; i < constraintCount; i += NT)
+        {
+            const int32_t level = cColor[i] == M3_GRAPH_COLORS ? levels : s.conLevel[i];
+            s.conLevel[i] = level;
+            atomicAdd(&s.levelStart[level + 1], 1);
+        }
+        __syncthreads();
+        if (tid == 0)
+        {
+            for (int32_t k = 0; k <= levels; ++k)
+            {
+                s.levelStart[k + 1] += s.levelStart[k];
+            }
+            s_totalLevels = levels;
+        }
+        __syncthreads();
+        for (int32_t k = tid; k <= levels; k += NT)
+        {
+            s.levelFill[k] = s.levelStart[k];
+        }
+        __syncthreads();
+        // The overflow bucket keeps constraint order (it runs serially).
+        for (int32_t i = tid; i < constraintCount; i += NT)
+        {
+            const int32_t level = s.conLevel[i];
+            if (level < levels)
+            {
+                const int32_t slot = atomicAdd(&s.levelFill[level], 1);
+                s.lists[slot] = i;
+                s.conSlot[i] = slot;
+            }
+        }
+        if (tid == 0 && s.levelStart[levels + 1] > s.levelStart[levels])
+        {
+            int32_t slot = s.levelStart[levels];
+            for (int32_t i = 0; i < constraintCount; ++i)
+            {
+                if (s.conLevel[i] == levels)
+                {
+                    s.lists[slot] = i;
+                    s.conSlot[i] = slot;
+                    slot += 1;
+                }
+            }
+        }
+    }
+    __syncthreads();
     M3_PHASE_MARK(M3_PHASE_COLOR)
     // Contact rows (solver.c:261-405), prepared straight into their
     // solve slots; consecutive threads write consecutive slots.
@@ -1693,6 +1820,7 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3PrepareKernel(const m3WorldV
         plan->jointLevels = s_jointLevels;
         plan->moverCount = moverCount;
         plan->anyRestitution = s_anyRestitution;
+        plan->levels = s_totalLevels;
         for (int32_t c = 0; c < M3_GRAPH_COLORS + 2; ++c)
         {
             plan->starts[c] = s_starts[c];
@@ -1796,6 +1924,69 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3SubstepKernel(const m3WorldV
         }
     }
     __syncthreads();
+    // One pass over the joint/contact schedule (pass 0 warm start, 1 the
+    // biased solve, 2 relax): level by level, the level's joint rows on
+    // the first warps and its contact rows on the remaining warps (whole
+    // warps apart, so the two kinds of row never diverge inside a warp),
+    // then the overflow colour serially.
+    const int32_t levels = s.plan->levels;
+    auto mergedPass = [&](int32_t pass) {
+        for (int32_t level = 0; level < levels; ++level)
+        {
+            int32_t jointThreads = 0;
+            if (level < jointLevels)
+            {
+                const int32_t j0 = s.jointLevelStart[level];
+                const int32_t j1 = s.jointLevelStart[level + 1];
+                const int32_t warps = (j1 - j0 + 31) / 32;
+                jointThreads = 32 * (warps < NT / 32 - 1 ? warps : NT / 32 - 1);
+                for (int32_t k = j0 + tid; tid < jointThreads && k < j1; k += jointThreads)
+                {
+                    m3JointDev* row = &jrows[s.jointOrder[k]];
+                    if (pass == 0)
+                    {
+                        m3WarmStartJoint(wl, row, dQ);
+                    }
+                    else
+                    {
+                        m3SolveJoint(wl, row, dP, dQ, h, invH, pass == 1);
+                    }
+                }
+            }
+            const int32_t c1 = s.levelStart[level + 1];
+            const int32_t contactThreads = NT - jointThreads;
+            for (int32_t k = s.levelStart[level] + tid - jointThreads;
+                 tid >= jointThreads && k < c1; k += contactThreads)
+            {
+                if (pass == 0)
+                {
+                    m3WarmStartContact(wl, m3ConAt(s.rows, k), invI);
+                }
+                else
+                {
+                    m3SolveContact(wl, m3ConAt(s.rows, k), invI, dP, dQ, invH, pushMax,
+                                   pass == 1);
+                }
+            }
+            __syncthreads();
+        }
+        if (tid == 0)
+        {
+            for (int32_t k = s.levelStart[levels]; k < s.levelStart[levels + 1]; ++k)
+            {
+                if (pass == 0)
+                {
+                    m3WarmStartContact(wl, m3ConAt(s.rows, k), invI);
+                }
+                else
+                {
+                    m3SolveContact(wl, m3ConAt(s.rows, k), invI, dP, dQ, invH, pushMax,
+                                   pass == 1);
+                }
+            }
+        }
+        __syncthreads();
+    };
     // The substep loop (solver.c:4085-4203).
     for (int32_t sub = 0; sub < substeps; ++sub)
     {
@@ -1809,70 +2000,9 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3SubstepKernel(const m3WorldV
         }
         __syncthreads();
         M3_PHASE_MARK(M3_PHASE_INTEGRATE_V)
-        for (int32_t level = 0; level < jointLevels; ++level)
-        {
-            for (int32_t k = s.jointLevelStart[level] + tid; k < s.jointLevelStart[level + 1];
-                 k += NT)
-            {
-                m3WarmStartJoint(wl, &jrows[s.jointOrder[k]], dQ);
-            }
-            __syncthreads();
-        }
-        // Warm start, colour by colour; the overflow bucket serially.
-        for (int32_t color = 0; color < M3_GRAPH_COLORS; ++color)
-        {
-            int32_t a = s_starts[color];
-            int32_t b = s_starts[color + 1];
-            if (a == b)
-            {
-                continue;
-            }
-            for (int32_t k = a + tid; k < b; k += NT)
-            {
-                m3WarmStartContact(wl, m3ConAt(s.rows, k), invI);
-            }
-            __syncthreads();
-        }
-        if (tid == 0)
-        {
-            for (int32_t k = s_starts[M3_GRAPH_COLORS]; k < s_starts[M3_GRAPH_COLORS + 1]; ++k)
-            {
-                m3WarmStartContact(wl, m3ConAt(s.rows, k), invI);
-            }
-        }
-        __syncthreads();
-        for (int32_t level = 0; level < jointLevels; ++level)
-        {
-            for (int32_t k = s.jointLevelStart[level] + tid; k < s.jointLevelStart[level + 1];
-                 k += NT)
-            {
-                m3SolveJoint(wl, &jrows[s.jointOrder[k]], dP, dQ, h, invH, true);
-            }
-            __syncthreads();
-        }
+        mergedPass(0); // warm start
         M3_PHASE_MARK(M3_PHASE_WARM)
-        for (int32_t color = 0; color < M3_GRAPH_COLORS; ++color)
-        {
-            int32_t a = s_starts[color];
-            int32_t b = s_starts[color + 1];
-            if (a == b)
-            {
-                continue;
-            }
-            for (int32_t k = a + tid; k < b; k += NT)
-            {
-                m3SolveContact(wl, m3ConAt(s.rows, k), invI, dP, dQ, invH, pushMax, true);
-            }
-            __syncthreads();
-        }
-        if (tid == 0)
-        {
-            for (int32_t k = s_starts[M3_GRAPH_COLORS]; k < s_starts[M3_GRAPH_COLORS + 1]; ++k)
-            {
-                m3SolveContact(wl, m3ConAt(s.rows, k), invI, dP, dQ, invH, pushMax, true);
-            }
-        }
-        __syncthreads();
+        mergedPass(1); // solve with bias
         M3_PHASE_MARK(M3_PHASE_SOLVE)
         for (int32_t m = tid; m < moverCount; m += NT)
         {
@@ -1880,39 +2010,7 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3SubstepKernel(const m3WorldV
         }
         __syncthreads();
         M3_PHASE_MARK(M3_PHASE_INTEGRATE_P)
-        for (int32_t level = 0; level < jointLevels; ++level)
-        {
-            for (int32_t k = s.jointLevelStart[level] + tid; k < s.jointLevelStart[level + 1];
-                 k += NT)
-            {
-                m3SolveJoint(wl, &jrows[s.jointOrder[k]], dP, dQ, h, invH, false);
-            }
-            __syncthreads();
-        }
-        for (int32_t color = 0; color < M3_GRAPH_COLORS; ++color)
-        {
-            int32_t a = s_starts[color];
-            int32_t b = s_starts[color + 1];
-            if (a == b)
-            {
-                continue;
-            }
-            for (int32_t k = a + tid; k < b; k += NT)
-            {
-                m3SolveContact(wl, m3ConAt(s.rows, k), invI, dP, dQ, invH, pushMax,
-                               false);
-            }
-            __syncthreads();
-        }
-        if (tid == 0)
-        {
-            for (int32_t k = s_starts[M3_GRAPH_COLORS]; k < s_starts[M3_GRAPH_COLORS + 1]; ++k)
-            {
-                m3SolveContact(wl, m3ConAt(s.rows, k), invI, dP, dQ, invH, pushMax,
-                               false);
-            }
-        }
-        __syncthreads();
+        mergedPass(2); // relax
         M3_PHASE_MARK(M3_PHASE_RELAX)
     }
 
@@ -2264,9 +2362,10 @@ static int32_t Check(cudaError_t e, const char* what)
 // the batch order is by shape slots, largest first, so each class is a
 // contiguous run of the order).  Large worlds get 512 threads: twice the
 // rows per colour in flight and half as many worlds resident at once,
-// whose rows then stay in L2 across the passes.  Small worlds get 64:
-// eight worlds share an SM instead of two, hiding each other's joint
-// chains.  Every class keeps 128 registers per thread.
+// whose rows then stay in L2 across the passes.  Small worlds get 128:
+// four worlds share an SM instead of two, hiding each other's joint
+// chains, with one warp for a level's joint rows and three for its
+// contact rows.  Every class keeps 128 registers per thread.
 #define M3_CLASSES 3
 static const int32_t s_classMinShapes[M3_CLASSES] = {769, 161, 0};
 
@@ -2300,7 +2399,7 @@ static void LaunchClass(int32_t stage, int32_t c, cudaStream_t stream, const m3W
     }
     else
     {
-        M3_LAUNCH_CLASS(64, 8)
+        M3_LAUNCH_CLASS(128, 4)
     }
 #undef M3_LAUNCH_CLASS
 }
@@ -2327,10 +2426,10 @@ static int32_t SetClassSmem(int32_t c, int32_t bytes)
     }
     else
     {
-        e = cudaFuncSetAttribute(m3PrepareKernel<64, 8>, a, bytes);
+        e = cudaFuncSetAttribute(m3PrepareKernel<128, 4>, a, bytes);
         if (e == cudaSuccess)
         {
-            e = cudaFuncSetAttribute(m3SubstepKernel<64, 8>, a, bytes);
+            e = cudaFuncSetAttribute(m3SubstepKernel<128, 4>, a, bytes);
         }
     }
     if (e != cudaSuccess)
@@ -2516,9 +2615,9 @@ static int32_t PrepareBatch(m3HostWorld** worlds, int32_t count)
     // Size classes over the largest-first order, and each class's shared
     // memory: its largest body cache, plus the inverse inertia table and
     // the joint rows within the budget that keeps the class's blocks per
-    // SM (one 512-thread block, two 256-thread blocks, eight 64-thread
+    // SM (one 512-thread block, two 256-thread blocks, four 128-thread
     // blocks).
-    static const int64_t classSmem[M3_CLASSES] = {200 * 1024, M3_TWO_BLOCK_SMEM, 27 * 1024};
+    static const int64_t classSmem[M3_CLASSES] = {200 * 1024, M3_TWO_BLOCK_SMEM, 54 * 1024};
     int32_t c = 0;
     s_batch.classFirst[0] = 0;
     for (int32_t k = 0; k < count; ++k)
