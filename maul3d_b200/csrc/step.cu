@@ -984,7 +984,13 @@ __global__ void __launch_bounds__(128)
         m3Manifold* newMan = cur == 0 ? w.man1 : w.man0;
         const uint64_t key = newKeys[k];
         m3Manifold fresh;
-        m3CollideFamily<F>(w, key, &fresh);
+        if (m3CollideFamily<F>(w, key, &fresh) != M3_NARROW_OK)
+        {
+            // A clip polygon beyond the device's bound: the world stalls.
+            atomicMax(&sc->status, M3GPU_ERR_UNSUPPORTED);
+            sc->statusDetail = 1000 + (int32_t)w.shapeType[(int32_t)(key >> 32)] * 10 +
+                               (int32_t)w.shapeType[(int32_t)(key & 0xFFFFFFFFu)];
+        }
         m3WarmCarry(&fresh, key, oldKeys, oldMan, sc->pairCount);
         newMan[k] = fresh;
     }
