@@ -32,7 +32,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 DET_DEVICE = ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"]
 DET_HOST = ["-ffp-contract=off", "-fno-fast-math", "-fno-unsafe-math-optimizations"]
 
-CU_SOURCES = ["step.cu", "hash.cu"]
+CU_SOURCES = ["step.cu", "hash.cu", "upload.cu"]
 CPP_SOURCES = ["world.cpp", "device.cpp", "capi.cpp", "hostmem.cpp"]
 C_SOURCES = ["scenes.c"]
 

@@ -257,14 +257,19 @@ extern "C" int32_t m3gpu_upload_worlds(const m3WorldId* worlds, int32_t count)
     m3gpuClearError();
     std::vector<m3HostWorld*> ws;
     int32_t rc = Resolve(worlds, count, ws);
+    std::vector<m3HostWorld*> dirty;
     for (int32_t i = 0; rc == M3GPU_OK && i < count; ++i)
     {
         m3HostWorld* w = ws[(size_t)i];
         if (w->hostDirty || w->dslab == nullptr)
         {
             w->hv.sc->status = 0;
-            rc = m3gpuUpload(w);
+            dirty.push_back(w);
         }
+    }
+    if (rc == M3GPU_OK && !dirty.empty())
+    {
+        rc = m3gpuUploadBatch(dirty.data(), (int32_t)dirty.size());
     }
     // Uploads from page-locked images are asynchronous: the images must
     // not change under the copies, so return only once they are done.

@@ -228,7 +228,8 @@ int32_t m3gpuReserve(m3HostWorld* w)
     return rc;
 }
 
-int32_t m3gpuUpload(m3HostWorld* w)
+// Device allocations and the device view for an upload.
+static int32_t UploadPrepare(m3HostWorld* w)
 {
     int32_t rc = m3gpuEnsureDevice();
     if (rc != M3GPU_OK)
@@ -277,6 +278,14 @@ int32_t m3gpuUpload(m3HostWorld* w)
         w->dhullCap = 4;
     }
     BuildDeviceView(w);
+    return M3GPU_OK;
+}
+
+// The copies of one world's upload, one call per part.
+static int32_t UploadCopies(m3HostWorld* w)
+{
+    int32_t rc = M3GPU_OK;
+    const int32_t hullCount = (int32_t)w->hulls.size();
     // Everything before the pair buffers, then the current pair list up
     // to its count: the other buffer and the unused tails are written by
     // the step before anything reads them.
@@ -337,6 +346,123 @@ int32_t m3gpuUpload(m3HostWorld* w)
         w->hostDirty = false;
     }
     return rc;
+}
+
+int32_t m3gpuUpload(m3HostWorld* w)
+{
+    int32_t rc = UploadPrepare(w);
+    return rc == M3GPU_OK ? UploadCopies(w) : rc;
+}
+
+// Batched upload: worlds whose host memory the GPU can read (page-locked,
+// mapped chunks) become items of one upload kernel; the others copy one
+// call per part.  The item table goes through a page-locked staging
+// buffer; callers synchronise before returning to the host, so a later
+// call finds the staging free.
+static m3UploadItem* s_itemHost = nullptr;
+static m3UploadItem* s_itemDev = nullptr;
+static int32_t s_itemCap = 0;
+
+int32_t m3gpuUploadBatch(m3HostWorld** worlds, int32_t count)
+{
+    std::vector<m3UploadItem> items;
+    std::vector<m3HostWorld*> batched;
+    int64_t bytes = 0;
+    for (int32_t i = 0; i < count; ++i)
+    {
+        m3HostWorld* w = worlds[i];
+        int32_t rc = UploadPrepare(w);
+        if (rc != M3GPU_OK)
+        {
+            return rc;
+        }
+        const int64_t head = Offset(w, w->hv.keys0);
+        const int32_t n = w->hv.sc->pairCount;
+        const int32_t buf = w->hv.sc->pairBuf;
+        const uint64_t* hk = buf == 0 ? w->hv.keys0 : w->hv.keys1;
+        const m3Manifold* hm = buf == 0 ? w->hv.man0 : w->hv.man1;
+        const int32_t hullCount = (int32_t)w->hulls.size();
+        const uint8_t* srcHead = m3HostDevicePointer(w->image.data(), (size_t)head);
+        const uint8_t* srcKeys = n > 0 ? m3HostDevicePointer(hk, (size_t)n * sizeof(uint64_t)) : nullptr;
+        const uint8_t* srcMan = n > 0 ? m3HostDevicePointer(hm, (size_t)n * sizeof(m3Manifold)) : nullptr;
+        const uint8_t* srcHulls =
+            hullCount > 0 ? m3HostDevicePointer(w->hulls.data(), (size_t)hullCount * sizeof(m3HullData))
+                          : nullptr;
+        if (srcHead == nullptr || (n > 0 && (srcKeys == nullptr || srcMan == nullptr)) ||
+            (hullCount > 0 && srcHulls == nullptr))
+        {
+            rc = UploadCopies(w);
+            if (rc != M3GPU_OK)
+            {
+                return rc;
+            }
+            continue;
+        }
+        items.push_back(m3UploadItem{srcHead, w->dslab, head, 0, 0});
+        bytes += head;
+        if (n > 0)
+        {
+            items.push_back(m3UploadItem{srcKeys, (uint8_t*)(buf == 0 ? w->dv.keys0 : w->dv.keys1),
+                                         (int64_t)n * (int64_t)sizeof(uint64_t), 0, 0});
+            items.push_back(m3UploadItem{srcMan, (uint8_t*)(buf == 0 ? w->dv.man0 : w->dv.man1),
+                                         (int64_t)n * (int64_t)sizeof(m3Manifold), 0, 0});
+            bytes += (int64_t)n * (int64_t)(sizeof(uint64_t) + sizeof(m3Manifold));
+        }
+        if (hullCount > 0)
+        {
+            items.push_back(m3UploadItem{srcHulls, (uint8_t*)w->dhulls, 0, hullCount, 0});
+            for (int32_t h = 0; h < hullCount; ++h)
+            {
+                bytes += m3HullUsedBytes(&w->hulls[(size_t)h]);
+            }
+        }
+        batched.push_back(w);
+    }
+    const int32_t n = (int32_t)items.size();
+    if (n == 0)
+    {
+        return M3GPU_OK;
+    }
+    if (n > s_itemCap)
+    {
+        cudaDeviceSynchronize();
+        cudaFreeHost(s_itemHost);
+        cudaFree(s_itemDev);
+        s_itemHost = nullptr;
+        s_itemDev = nullptr;
+        s_itemCap = 0;
+        int32_t rc = CudaCheck(cudaMallocHost((void**)&s_itemHost, sizeof(m3UploadItem) * (size_t)n),
+                               "allocate upload table");
+        if (rc == M3GPU_OK)
+        {
+            rc = CudaCheck(cudaMalloc((void**)&s_itemDev, sizeof(m3UploadItem) * (size_t)n),
+                           "allocate upload table");
+        }
+        if (rc != M3GPU_OK)
+        {
+            return rc;
+        }
+        s_itemCap = n;
+    }
+    memcpy(s_itemHost, items.data(), sizeof(m3UploadItem) * (size_t)n);
+    int32_t rc = CudaCheck(cudaMemcpyAsync(s_itemDev, s_itemHost, sizeof(m3UploadItem) * (size_t)n,
+                                           cudaMemcpyHostToDevice, 0),
+                           "upload table");
+    if (rc == M3GPU_OK)
+    {
+        m3gpuLaunchUpload(s_itemDev, n);
+        rc = CudaCheck(cudaGetLastError(), "upload kernel");
+    }
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
+    for (m3HostWorld* w : batched)
+    {
+        w->hostDirty = false;
+    }
+    g_m3UploadedBytes += bytes;
+    return M3GPU_OK;
 }
 
 int32_t m3gpuDownload(m3HostWorld* w)

@@ -27,6 +27,7 @@ struct Chunk
     size_t bytes;
     size_t used;
     bool locked;
+    uint8_t* deviceBase; // the chunk as the GPU addresses it (locked chunks)
 };
 
 struct Arena
@@ -80,7 +81,7 @@ void* m3HostAlloc(size_t bytes)
     {
         throw std::bad_alloc();
     }
-    Chunk c{(uint8_t*)m, chunkBytes, size, false};
+    Chunk c{(uint8_t*)m, chunkBytes, size, false, nullptr};
     a.chunks.push_back(c);
     return m;
 }
@@ -106,9 +107,20 @@ int32_t m3HostLockAll(void)
         {
             continue;
         }
-        if (cudaHostRegister(c.base, c.bytes, cudaHostRegisterDefault) == cudaSuccess)
+        // Mapped too: the upload kernel reads the images straight from here.
+        if (cudaHostRegister(c.base, c.bytes, cudaHostRegisterMapped | cudaHostRegisterPortable) ==
+            cudaSuccess)
         {
             c.locked = true;
+            void* dev = nullptr;
+            if (cudaHostGetDevicePointer(&dev, c.base, 0) == cudaSuccess)
+            {
+                c.deviceBase = (uint8_t*)dev;
+            }
+            else
+            {
+                cudaGetLastError();
+            }
         }
         else
         {
@@ -131,4 +143,19 @@ bool m3HostIsLocked(const void* p, size_t bytes)
         }
     }
     return false;
+}
+
+const uint8_t* m3HostDevicePointer(const void* p, size_t bytes)
+{
+    Arena& a = TheArena();
+    std::lock_guard<std::mutex> lock(a.mu);
+    const uint8_t* q = (const uint8_t*)p;
+    for (const Chunk& c : a.chunks)
+    {
+        if (q >= c.base && q + bytes <= c.base + c.bytes)
+        {
+            return c.locked && c.deviceBase != nullptr ? c.deviceBase + (q - c.base) : nullptr;
+        }
+    }
+    return nullptr;
 }

@@ -22,6 +22,25 @@ void m3HostFree(void* p, size_t bytes);
 int32_t m3HostLockAll(void);
 // Whether [p, p + bytes) lies in a locked chunk.
 bool m3HostIsLocked(const void* p, size_t bytes);
+// The device's address of [p, p + bytes) when it lies in a locked (and
+// mapped) chunk, else null.
+const uint8_t* m3HostDevicePointer(const void* p, size_t bytes);
+
+// One copy of a batched upload, done on the GPU from page-locked, mapped
+// host memory (upload.cu): `bytes` raw bytes, or, when `hulls` > 0, that
+// many interned hull slabs of which only the parts their counts use.
+struct m3UploadItem
+{
+    const uint8_t* src;
+    uint8_t* dst;
+    int64_t bytes;
+    int32_t hulls;
+    int32_t pad;
+};
+int32_t m3gpuLaunchUpload(const m3UploadItem* items, int32_t count);
+// Bytes of one hull slab an upload copies (the parts its counts use).
+int64_t m3HullUsedBytes(const m3HullData* h);
+
 
 template <class T> struct m3PageAllocator
 {
@@ -91,6 +110,9 @@ extern int64_t g_m3UploadedBytes;
 int32_t m3gpuEnsureDevice(void);
 int32_t m3gpuReserve(m3HostWorld* w);
 int32_t m3gpuUpload(m3HostWorld* w);
+// Upload many worlds with one kernel where their host memory allows; the
+// rest one world at a time.
+int32_t m3gpuUploadBatch(m3HostWorld** worlds, int32_t count);
 int32_t m3gpuDownload(m3HostWorld* w);
 void m3gpuRelease(m3HostWorld* w);
 // Make the host image current before a host read or write.

@@ -2485,17 +2485,22 @@ static int32_t EnsureClassStreams()
 
 static int32_t PrepareBatch(m3HostWorld** worlds, int32_t count)
 {
+    std::vector<m3HostWorld*> dirty;
     for (int32_t i = 0; i < count; ++i)
     {
         m3HostWorld* w = worlds[i];
         if (w->hostDirty || w->dslab == nullptr)
         {
             w->hv.sc->status = 0;
-            int32_t rc = m3gpuUpload(w);
-            if (rc != M3GPU_OK)
-            {
-                return rc;
-            }
+            dirty.push_back(w);
+        }
+    }
+    if (!dirty.empty())
+    {
+        int32_t rc = m3gpuUploadBatch(dirty.data(), (int32_t)dirty.size());
+        if (rc != M3GPU_OK)
+        {
+            return rc;
         }
     }
     bool same = s_batch.dviews != nullptr && s_batch.epoch == g_m3ResidencyEpoch &&
