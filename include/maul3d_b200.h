@@ -241,6 +241,11 @@ M3GPU_API bool m3Shape_IsValid(m3ShapeId shapeId);
  * fixed joints are stepped on the device. */
 M3GPU_API m3JointDef m3DefaultJointDef(void);
 M3GPU_API m3JointId m3CreateJoint(const m3JointDef* def);
+/* joint.c:914 (joint.h:216): breaking thresholds in N and N*m (0 = no
+ * limit); a joint whose reaction exceeds one is destroyed by the step,
+ * in ascending joint order, and its slot is recycled.  Wakes the joint's
+ * dynamic bodies.  Negative or non-finite values are refused (no-op). */
+M3GPU_API void m3Joint_SetBreakThresholds(m3JointId jointId, float maxForce, float maxTorque);
 M3GPU_API bool m3Joint_IsValid(m3JointId jointId);
 
 /* ---------------------------------------------------------------------

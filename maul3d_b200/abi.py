@@ -46,6 +46,7 @@ SCENE_SPHERE_PYRAMID = 0
 SCENE_BOX_PYRAMID = 1
 SCENE_UNEVEN = 2
 SCENE_FREEFALL = 3
+SCENE_TOWERS = 4
 
 
 def _ptr(a: np.ndarray) -> C.c_void_p:
@@ -154,7 +155,24 @@ class m3Capsule(C.Structure):
     _fields_ = [("point1", m3Vec3), ("point2", m3Vec3), ("radius", C.c_float)]
 
 
+class m3JointDef(C.Structure):
+    """joint.h:85-132 of the reference."""
+    _fields_ = [("type", C.c_int32), ("bodyA", m3BodyId), ("bodyB", m3BodyId),
+                ("localAnchorA", m3Vec3), ("localAnchorB", m3Vec3), ("localAxisA", m3Vec3),
+                ("localAxisB", m3Vec3), ("enableLimit", C.c_bool), ("lowerLimit", C.c_float),
+                ("upperLimit", C.c_float), ("enableMotor", C.c_bool), ("motorSpeed", C.c_float),
+                ("maxMotorEffort", C.c_float), ("enableCone", C.c_bool), ("coneAngle", C.c_float),
+                ("collideConnected", C.c_bool), ("genericLinear", C.c_uint8 * 3),
+                ("genericAngular", C.c_uint8 * 3), ("genericMotorAxis", C.c_uint8),
+                ("genericReserved", C.c_uint8), ("genericLinearLower", C.c_float * 3),
+                ("genericLinearUpper", C.c_float * 3), ("genericAngularLower", C.c_float * 3),
+                ("genericAngularUpper", C.c_float * 3), ("ratio", C.c_float),
+                ("groundAnchorA", m3Pos3), ("groundAnchorB", m3Pos3), ("internalValue", C.c_int32)]
+
+
 assert C.sizeof(m3WorldDef) == 112 and C.sizeof(m3BodyDef) == 104 and C.sizeof(m3ShapeDef) == 88
+assert C.sizeof(m3JointDef) == 224 and m3JointDef.ratio.offset == 160
+assert m3JointDef.groundAnchorA.offset == 168 and m3JointDef.internalValue.offset == 216
 
 
 def bind_create(lib: C.CDLL) -> C.CDLL:
@@ -174,4 +192,11 @@ def bind_create(lib: C.CDLL) -> C.CDLL:
     lib.m3CreateCapsuleShape.restype = m3ShapeId
     lib.m3CreateBoxShape.argtypes = [m3BodyId, C.POINTER(m3ShapeDef), m3Vec3]
     lib.m3CreateBoxShape.restype = m3ShapeId
+    lib.m3DefaultJointDef.restype = m3JointDef
+    lib.m3CreateJoint.argtypes = [C.POINTER(m3JointDef)]
+    lib.m3CreateJoint.restype = m3JointId
+    lib.m3Joint_SetBreakThresholds.argtypes = [m3JointId, C.c_float, C.c_float]
+    lib.m3Joint_SetBreakThresholds.restype = None
+    lib.m3Joint_IsValid.argtypes = [m3JointId]
+    lib.m3Joint_IsValid.restype = C.c_bool
     return lib

@@ -514,6 +514,7 @@ int32_t m3gpuDownload(m3HostWorld* w)
     if (rc == M3GPU_OK)
     {
         w->deviceAhead = false;
+        m3DrainBrokenJoints(w);
     }
     return rc;
 }

@@ -75,14 +75,15 @@ __device__ __forceinline__ m3Vec3 m3QuatToRotationVec(m3Quat relQ)
 }
 
 // Joint rows the device path covers: spherical without cone or twist
-// limits, revolute with limit and motor, fixed; no springs, no breaking
-// thresholds.  Returns 0, or a detail code for a refused joint.
+// limits, revolute with limit and motor, fixed, each with or without
+// breaking thresholds; no springs.  Returns 0, or a detail code for a
+// refused joint.
 __device__ __forceinline__ int32_t m3JointRefusal(const m3WorldView& w, int32_t j)
 {
     uint8_t type = w.jtype[j];
     uint8_t flags = w.jflags[j];
-    if (w.jbreak[j].x != 0.0f || w.jbreak[j].y != 0.0f || (flags & 8) != 0 ||
-        (type != 0 && type != 1 && type != 3) || (type == 0 && (flags & 5) != 0))
+    if ((flags & 8) != 0 || (type != 0 && type != 1 && type != 3) ||
+        (type == 0 && (flags & 5) != 0))
     {
         return 4000 + type;
     }
@@ -410,6 +411,127 @@ __device__ void m3StoreJoint(const m3WorldView& w, const m3JointDev* c)
         w.jlimitImp[c->joint] = v3(c->lowerImpulse, c->upperImpulse, 0.0f);
         w.jangular[c->joint] = c->angularImpulse;
         w.jspringImp[c->joint] = c->springImpulseV;
+    }
+}
+
+// Reaction magnitudes of a stored joint for the device joint types
+// (joint.c:635-711): revolute -- the cross-axis locks, motor and limits
+// as torque; spherical -- its twist/swing rows; fixed -- the weld's
+// angular impulse; the point impulse as force.  Both scaled by invH.
+__device__ __forceinline__ void m3JointReactionDev(const m3WorldView& w, int32_t j, m3real invH,
+                                                   m3real* outForce, m3real* outTorque)
+{
+    const m3Vec3 lin = w.jimpulse[j];
+    const m3Vec3 perp = w.jperp[j];
+    const m3Vec3 lim = w.jlimitImp[j];
+    const m3Vec3 ang = w.jangular[j];
+    const m3real force = m3Length3(lin);
+    m3real torque;
+    if (w.jtype[j] == 1)
+    {
+        torque = sqrtf(perp.x * perp.x + perp.y * perp.y) + fabsf(perp.z) + fabsf(lim.x) +
+                 fabsf(lim.y);
+    }
+    else if (w.jtype[j] == 0)
+    {
+        torque = fabsf(lim.x) + fabsf(lim.y) + fabsf(lim.z);
+    }
+    else
+    {
+        torque = m3Length3(ang);
+    }
+    *outForce = force * invH;
+    *outTorque = torque * invH;
+}
+
+// Removes joint j from one body's joint list (joint.c:324-337).
+__device__ __forceinline__ void m3UnlinkJointDev(const m3WorldView& w, int32_t body, int32_t j)
+{
+    int32_t* cursor = &w.jointHead[body];
+    while (*cursor != -1)
+    {
+        const int32_t k = *cursor;
+        if (k == j)
+        {
+            *cursor = w.jbodyA[k] == body ? w.jnextA[k] : w.jnextB[k];
+            return;
+        }
+        cursor = w.jbodyA[k] == body ? &w.jnextA[k] : &w.jnextB[k];
+    }
+}
+
+// Joint breakage after the impulse store (solver.c:4228-4257): serially
+// in ascending joint order, a joint whose reaction exceeds a set
+// threshold is destroyed (joint.c:339-385): unlinked from both bodies,
+// which wake, its record reset, its slot freed (generation bumped unless
+// retired at 0xFFFF) and queued for the host's free list.
+__device__ void m3BreakJointsDev(const m3WorldView& w, m3real invH)
+{
+    m3WorldScalars* sc = w.sc;
+    const int32_t jointMax = sc->jointMax;
+    for (int32_t j = 0; j < jointMax; ++j)
+    {
+        if (w.jointAlive[j] == 0)
+        {
+            continue;
+        }
+        const m3real maxForce = w.jbreak[j].x;
+        const m3real maxTorque = w.jbreak[j].y;
+        if (maxForce == 0.0f && maxTorque == 0.0f)
+        {
+            continue;
+        }
+        m3real force;
+        m3real torque;
+        m3JointReactionDev(w, j, invH, &force, &torque);
+        if (!((maxForce > 0.0f && force > maxForce) || (maxTorque > 0.0f && torque > maxTorque)))
+        {
+            continue;
+        }
+        const int32_t bodyA = w.jbodyA[j];
+        const int32_t bodyB = w.jbodyB[j];
+        m3UnlinkJointDev(w, bodyA, j);
+        m3UnlinkJointDev(w, bodyB, j);
+        if (w.btype[bodyA] == M3_BODY_DYNAMIC && w.bodyAlive[bodyA] != 0)
+        {
+            w.awake[bodyA] = 1;
+            w.sleepTime[bodyA] = 0.0f;
+        }
+        if (w.btype[bodyB] == M3_BODY_DYNAMIC && w.bodyAlive[bodyB] != 0)
+        {
+            w.awake[bodyB] = 1;
+            w.sleepTime[bodyB] = 0.0f;
+        }
+        const m3Vec3 zero = v3(0.0f, 0.0f, 0.0f);
+        w.jtype[j] = 0;
+        w.jbodyA[j] = -1;
+        w.jbodyB[j] = -1;
+        w.jlocalA[j] = zero;
+        w.jlocalB[j] = zero;
+        w.jcollide[j] = 0;
+        w.jimpulse[j] = zero;
+        w.jperp[j] = zero;
+        w.jlimitImp[j] = zero;
+        w.jangular[j] = zero;
+        w.jframeA[j] = m3IdentityQuat();
+        w.jframeB[j] = m3IdentityQuat();
+        w.jflags[j] = 0;
+        w.jmotor[j] = zero;
+        w.jbreak[j] = zero;
+        w.jspring[j] = zero;
+        w.jtargetScalar[j] = 0.0f;
+        w.jtargetQ[j] = m3IdentityQuat();
+        w.jspringImp[j] = zero;
+        w.jlimits[j] = zero;
+        w.jnextA[j] = -1;
+        w.jnextB[j] = -1;
+        w.jointAlive[j] = 0;
+        if (w.jointGen[j] != 0xFFFF)
+        {
+            w.jointGen[j] = (uint16_t)(w.jointGen[j] + 1);
+            w.jbroken[sc->brokenCount % sc->jointCap] = j;
+            sc->brokenCount += 1;
+        }
     }
 }
 

@@ -55,6 +55,10 @@ typedef struct m3WorldScalars
     int32_t moverCount;
     int32_t jointConstraintCount;
     int32_t newPairCount; // pair list the running step is building
+    // Joints the device destroyed (breakage), as a ring over jbroken:
+    // the host drains entries [drained, brokenCount) into its free queue.
+    int32_t brokenCount;
+    int32_t pad1;
     // Work counters accumulated over every device step (observer only,
     // never hashed): the algorithmic-byte model of the roofline reads
     // them.  [0] movers x substeps, [1] contact rows x substeps,
@@ -148,7 +152,8 @@ typedef struct m3WorldScalars
     X(int32_t, jnextA)                                                                             \
     X(int32_t, jnextB)                                                                             \
     X(uint8_t, jointAlive)                                                                         \
-    X(uint16_t, jointGen)
+    X(uint16_t, jointGen)                                                                          \
+    X(int32_t, jbroken)
 
 // Candidate pairs and manifolds, double-buffered: the step reads the
 // previous step's lists for the warm-start carry while it writes the

@@ -8,6 +8,7 @@
 
 #include <stdint.h>
 #include <stdlib.h>
+#include <deque>
 #include <new>
 #include <unordered_map>
 #include <vector>
@@ -85,6 +86,11 @@ struct m3HostWorld
     // pool is sized by the hulls actually interned (count-derived, as
     // the reference's snapshot treats them).
     std::vector<m3HullData, m3PageAllocator<m3HullData>> hulls;
+    // Recycled joint slots, reused first in FIFO order (allocator.c:178-
+    // 218); the device's breakage appends to it through the jbroken ring,
+    // drained up to `brokenDrained` at each download.
+    std::deque<int32_t> jointFree;
+    int32_t brokenDrained = 0;
     std::vector<int32_t> hullRefs;
     std::unordered_multimap<uint64_t, int32_t> hullIndexByContent;
 
@@ -117,6 +123,8 @@ int32_t m3gpuDownload(m3HostWorld* w);
 void m3gpuRelease(m3HostWorld* w);
 // Make the host image current before a host read or write.
 int32_t m3gpuSyncHost(m3HostWorld* w);
+// Queue the joint slots the device freed since the last call (world.cpp).
+void m3DrainBrokenJoints(m3HostWorld* w);
 
 // Step and hash entry points (step.cu).
 int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t substeps,

@@ -21,6 +21,11 @@
 //                       hung from static anchors, laid out from `seed`.
 //   M3S_FREEFALL        `param` spheres and boxes in free fall, no
 //                       contacts for the first steps (integration only).
+//   M3S_TOWERS          `param` towers of 2x2x4 unit boxes welded to
+//                       their face neighbours by breakable fixed joints
+//                       (28 a tower), each hit by a sphere launched at
+//                       20-40 m/s: joints break on impact and their
+//                       slots are recycled.
 
 #include <m3_scene_api.h> // resolved by -I: product or oracle shim
 
@@ -33,6 +38,7 @@ enum
     M3S_BOX_PYRAMID = 1,
     M3S_UNEVEN = 2,
     M3S_FREEFALL = 3,
+    M3S_TOWERS = 4,
 };
 
 static uint64_t SceneSplitMix(uint64_t* state)
@@ -240,6 +246,85 @@ static m3WorldId FreeFall(int32_t count)
     return world;
 }
 
+// Towers of 2x2x4 unit boxes 6 m apart along x.  Each box is welded to
+// its +x, +y and +z neighbours by a fixed joint with a 500 N force
+// threshold; every third joint also gets a 150 N*m torque threshold.  A
+// dense sphere (radius 0.5, density 40) starts 8 m before each tower,
+// 1-3.5 m up, flying at it at 20-40 m/s.
+static m3WorldId Towers(uint64_t seed, int32_t towers)
+{
+    m3WorldDef def = m3DefaultWorldDef();
+    def.bodyCapacity = 17 * towers + 4;
+    def.shapeCapacity = 17 * towers + 4;
+    def.jointCapacity = 28 * towers + 4;
+    m3WorldId world = m3CreateWorld(&def);
+    SceneGround(world, 0.6f);
+    uint64_t rng = seed ^ 0x70BE125ull;
+    m3BodyDef bd = m3DefaultBodyDef();
+    bd.type = m3_dynamicBody;
+    m3ShapeDef sd = m3DefaultShapeDef();
+    sd.friction = 0.6f;
+    int32_t jointCount = 0;
+    for (int32_t t = 0; t < towers; ++t)
+    {
+        double cx = 6.0 * (double)t;
+        m3BodyId box[4][2][2];
+        for (int32_t k = 0; k < 4; ++k)
+        {
+            for (int32_t j = 0; j < 2; ++j)
+            {
+                for (int32_t i = 0; i < 2; ++i)
+                {
+                    bd.position = (m3Pos3){cx + (double)i - 0.5, 0.5 + (double)k, (double)j - 0.5};
+                    box[k][j][i] = m3CreateBody(world, &bd);
+                    m3CreateBoxShape(box[k][j][i], &sd, (m3Vec3){0.5f, 0.5f, 0.5f});
+                }
+            }
+        }
+        for (int32_t k = 0; k < 4; ++k)
+        {
+            for (int32_t j = 0; j < 2; ++j)
+            {
+                for (int32_t i = 0; i < 2; ++i)
+                {
+                    for (int32_t axis = 0; axis < 3; ++axis)
+                    {
+                        int32_t ni = i + (axis == 0 ? 1 : 0);
+                        int32_t nk = k + (axis == 1 ? 1 : 0);
+                        int32_t nj = j + (axis == 2 ? 1 : 0);
+                        if (ni > 1 || nk > 3 || nj > 1)
+                        {
+                            continue;
+                        }
+                        m3Vec3 half = {axis == 0 ? 0.5f : 0.0f, axis == 1 ? 0.5f : 0.0f,
+                                       axis == 2 ? 0.5f : 0.0f};
+                        m3JointDef jd = m3DefaultJointDef();
+                        jd.type = m3_fixedJoint;
+                        jd.bodyA = box[k][j][i];
+                        jd.bodyB = box[nk][nj][ni];
+                        jd.localAnchorA = half;
+                        jd.localAnchorB = (m3Vec3){-half.x, -half.y, -half.z};
+                        m3JointId joint = m3CreateJoint(&jd);
+                        m3Joint_SetBreakThresholds(joint, 500.0f,
+                                                   jointCount % 3 == 0 ? 150.0f : 0.0f);
+                        jointCount += 1;
+                    }
+                }
+            }
+        }
+        bd.position = (m3Pos3){cx - 8.0, SceneRand(&rng, 1.0, 3.5), SceneRand(&rng, -0.5, 0.5)};
+        bd.linearVelocity = (m3Vec3){(float)SceneRand(&rng, 20.0, 40.0),
+                                     (float)SceneRand(&rng, 0.0, 2.0), 0.0f};
+        m3BodyId ball = m3CreateBody(world, &bd);
+        m3Sphere shape = {{0.0f, 0.0f, 0.0f}, 0.5f};
+        m3ShapeDef heavy = sd;
+        heavy.density = 40.0f;
+        m3CreateSphereShape(ball, &heavy, &shape);
+        bd.linearVelocity = (m3Vec3){0.0f, 0.0f, 0.0f};
+    }
+    return world;
+}
+
 // Build one seeded scene; returns the null world id for an unknown
 // scene number.
 M3S_API m3WorldId m3s_build(int32_t scene, uint64_t seed, int32_t param)
@@ -254,6 +339,8 @@ M3S_API m3WorldId m3s_build(int32_t scene, uint64_t seed, int32_t param)
         return UnevenWorld(seed, param);
     case M3S_FREEFALL:
         return FreeFall(param > 0 ? param : 8);
+    case M3S_TOWERS:
+        return Towers(seed, param > 0 ? param : 4);
     default:
     {
         m3WorldId none = {0, 0};

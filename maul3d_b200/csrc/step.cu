@@ -2054,6 +2054,7 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3SubstepKernel(const m3WorldV
     {
         m3StoreJoint(w, &jrows[r]);
     }
+    __syncthreads(); // breakage reads the stored joint impulses
     if (tid == 0)
     {
         sc->lastInvH = invH;
@@ -2066,6 +2067,10 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3SubstepKernel(const m3WorldV
                 sc->windPhase -=
                     2.0f * M3_PI * (m3real)(int32_t)(sc->windPhase / (2.0f * M3_PI));
             }
+        }
+        if (sc->jointMax > 0)
+        {
+            m3BreakJointsDev(w, invH);
         }
     }
     M3_PHASE_MARK(M3_PHASE_STORE)

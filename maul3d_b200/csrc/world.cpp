@@ -1069,13 +1069,23 @@ extern "C" m3JointId m3CreateJoint(const m3JointDef* def)
         m3gpuSetError(M3GPU_ERR_INVALID, "m3CreateJoint: a joint between immovables");
         return nullId;
     }
-    if (v.sc->jointMax >= w->jointCap)
+    // Recycled slots first, FIFO, then a fresh one (allocator.c:178-198).
+    int32_t j = -1;
+    if (!w->jointFree.empty())
+    {
+        j = w->jointFree.front();
+        w->jointFree.pop_front();
+    }
+    else if (v.sc->jointMax < w->jointCap)
+    {
+        j = v.sc->jointMax;
+        v.sc->jointMax += 1;
+    }
+    else
     {
         m3gpuSetError(M3GPU_ERR_CAPACITY, "m3CreateJoint: joint pool exhausted");
         return nullId;
     }
-    int32_t j = v.sc->jointMax;
-    v.sc->jointMax += 1;
     v.jointAlive[j] = 1;
     v.jtype[j] = (uint8_t)def->type;
     v.jbodyA[j] = a;
@@ -1127,10 +1137,60 @@ extern "C" m3JointId m3CreateJoint(const m3JointDef* def)
     return id;
 }
 
+void m3DrainBrokenJoints(m3HostWorld* w)
+{
+    const int32_t cap = w->jointCap > 0 ? w->jointCap : 1;
+    while (w->brokenDrained < w->hv.sc->brokenCount)
+    {
+        w->jointFree.push_back(w->hv.jbroken[w->brokenDrained % cap]);
+        w->brokenDrained += 1;
+    }
+}
+
+// joint.c:914-938 (joint.h:216): breaking thresholds (0 = none); wakes
+// the joint's dynamic bodies.  Refuses negative or non-finite values.
+extern "C" void m3Joint_SetBreakThresholds(m3JointId jointId, float maxForce, float maxTorque)
+{
+    m3HostWorld* w = m3gpuWorldFromIndex0(jointId.world0);
+    const int32_t j = jointId.index1 - 1;
+    if (w == nullptr || !isfinite(maxForce) || maxForce < 0.0f || !isfinite(maxTorque) ||
+        maxTorque < 0.0f)
+    {
+        return;
+    }
+    if (m3gpuSyncHost(w) != M3GPU_OK)
+    {
+        return;
+    }
+    m3WorldView& v = w->hv;
+    if (j < 0 || j >= v.sc->jointMax || v.jointAlive[j] == 0 ||
+        v.jointGen[j] != jointId.generation)
+    {
+        return;
+    }
+    v.jbreak[j] = v3(maxForce, maxTorque, 0.0f);
+    const int32_t bodies[2] = {v.jbodyA[j], v.jbodyB[j]};
+    for (int32_t k = 0; k < 2; ++k)
+    {
+        const int32_t b = bodies[k];
+        if (b >= 0 && v.btype[b] == M3_BODY_DYNAMIC)
+        {
+            v.awake[b] = 1;
+            v.sleepTime[b] = 0.0f;
+        }
+    }
+    w->hostDirty = true;
+}
+
 extern "C" bool m3Joint_IsValid(m3JointId jointId)
 {
     m3HostWorld* w = m3gpuWorldFromIndex0(jointId.world0);
     int32_t index = jointId.index1 - 1;
+    // The step may have broken the joint on the device.
+    if (w != nullptr && m3gpuSyncHost(w) != M3GPU_OK)
+    {
+        return false;
+    }
     return w != nullptr && index >= 0 && index < w->hv.sc->jointMax &&
            w->hv.jointAlive[index] != 0 && w->hv.jointGen[index] == jointId.generation;
 }

@@ -16,6 +16,10 @@ if str(ROOT) not in sys.path:
     sys.path.insert(0, str(ROOT))
 
 
+# Number of golden trace cases in tests/golden/traces.json.
+GOLDEN_CASES = len(json.loads((ROOT / "tests" / "golden" / "traces.json").read_text())["cases"])
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
 

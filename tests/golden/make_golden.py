@@ -28,6 +28,8 @@ CASES = [
     ("uneven_200_s3", 2, 3, 200, 1.0 / 60.0, 4, 300, [1, 10, 100, 300]),
     ("uneven_600_s4", 2, 4, 600, 1.0 / 60.0, 4, 300, [1, 10, 100, 300]),
     ("uneven_2048_s5", 2, 5, 2048, 1.0 / 60.0, 4, 120, [1, 10, 60, 120]),
+    ("towers_4_s7", 4, 7, 4, 1.0 / 60.0, 4, 240, [1, 10, 20, 60, 240]),
+    ("towers_16_s8", 4, 8, 16, 1.0 / 60.0, 4, 180, [1, 15, 30, 90, 180]),
 ]
 
 

@@ -11,6 +11,8 @@ import subprocess
 
 import pytest
 
+from conftest import GOLDEN_CASES
+
 # bench/pins.txt:1-7 of the reference.
 BENCH_PINS = {
     "pyramid": "975f319f2f44cc5d",
@@ -49,7 +51,7 @@ def test_oracle_sphere_pyramid_matches_bench_pin(oracle):
     w.destroy()
 
 
-@pytest.mark.parametrize("idx", range(8))
+@pytest.mark.parametrize("idx", range(GOLDEN_CASES))
 def test_oracle_reproduces_golden_traces(oracle, golden, idx):
     case = golden["cases"][idx]
     w = oracle.RefWorld.scene(case["scene"], case["seed"], case["param"])

@@ -12,14 +12,15 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from conftest import cuda_available
-from maul3d_b200.abi import SCENE_BOX_PYRAMID, SCENE_FREEFALL, SCENE_SPHERE_PYRAMID, SCENE_UNEVEN
+from conftest import GOLDEN_CASES, cuda_available
+from maul3d_b200.abi import (SCENE_BOX_PYRAMID, SCENE_FREEFALL, SCENE_SPHERE_PYRAMID, SCENE_TOWERS,
+                             SCENE_UNEVEN)
 
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not cuda_available(), reason="needs a CUDA device")]
 
 
-@pytest.mark.parametrize("idx", range(8))
+@pytest.mark.parametrize("idx", range(GOLDEN_CASES))
 def test_golden_trace_on_device(m3, golden, idx):
     case = golden["cases"][idx]
     w = m3.World.scene(case["scene"], case["seed"], case["param"])
@@ -44,6 +45,8 @@ def test_sphere_pyramid_reaches_reference_bench_pin(m3):
     (SCENE_BOX_PYRAMID, 0, 20, 120),
     (SCENE_UNEVEN, 11, 48, 150),
     (SCENE_UNEVEN, 12, 300, 100),
+    (SCENE_TOWERS, 7, 4, 120),
+    (SCENE_TOWERS, 9, 24, 90),
 ])
 def test_every_step_matches_oracle(m3, oracle, scene, seed, param, steps):
     g = m3.World.scene(scene, seed, param)
@@ -109,3 +112,52 @@ def test_unsupported_feature_fails_loudly(m3):
     # The world stays failed: every later step reports the refusal.
     with pytest.raises(m3.M3GpuError):
         w.step()
+
+
+def _joint_ids(lib, world, count):
+    from maul3d_b200 import abi
+    w0 = world.id.index1 - 1
+    return [bool(lib.m3Joint_IsValid(abi.m3JointId(j + 1, w0, 0))) for j in range(count)]
+
+
+def test_broken_joint_slots_recycle_like_the_reference(m3, oracle):
+    # Towers of welded boxes hit by dense spheres: the step destroys the
+    # joints whose reaction passes their threshold (solver.c:4228-4257),
+    # in ascending order, and a joint created afterwards takes the first
+    # freed slot with its generation bumped (allocator.c:178-218).
+    from maul3d_b200 import abi
+    glib = abi.bind_create(m3.lib)
+    rlib = abi.bind_create(oracle.lib())
+    g = m3.World.scene(SCENE_TOWERS, 7, 4)
+    r = oracle.RefWorld.scene(SCENE_TOWERS, 7, 4)
+    for s in range(40):
+        g.step(1.0 / 60.0, 4, 1)
+        r.step(1.0 / 60.0, 4, 1)
+        assert g.hash() == r.hash(), f"step {s + 1}"
+    alive_g = _joint_ids(glib, g, 112)
+    alive_r = _joint_ids(rlib, r, 112)
+    assert alive_g == alive_r
+    assert 0 < sum(alive_g) < 112, "the scene must break some joints and keep others"
+    made = []
+    for lib, world in ((glib, g), (rlib, r)):
+        ids = []
+        w0 = world.id.index1 - 1
+        for k in range(3):
+            jd = lib.m3DefaultJointDef()
+            jd.type = 3
+            jd.bodyA = abi.m3BodyId(2 + 4 * k, w0, 0)
+            jd.bodyB = abi.m3BodyId(3 + 4 * k, w0, 0)
+            jd.localAnchorA = abi.m3Vec3(0.5, 0.0, 0.0)
+            jd.localAnchorB = abi.m3Vec3(-0.5, 0.0, 0.0)
+            j = lib.m3CreateJoint(C.byref(jd))
+            lib.m3Joint_SetBreakThresholds(j, 800.0, 0.0)
+            ids.append((j.index1, j.generation))
+        made.append(ids)
+    assert made[0] == made[1]
+    assert all(gen == 1 for _, gen in made[0]), made[0]
+    assert g.hash() == r.hash()
+    for s in range(60):
+        g.step(1.0 / 60.0, 4, 1)
+        r.step(1.0 / 60.0, 4, 1)
+        if g.hash() != r.hash():
+            pytest.fail(f"step {s + 41}: {g.state().first_difference(r.state())}")
