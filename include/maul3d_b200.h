@@ -201,6 +201,32 @@ M3GPU_API void m3DestroyWorld(m3WorldId worldId);
 /* world.h:94 */
 M3GPU_API bool m3World_IsValid(m3WorldId worldId);
 
+/* snapshot.c:603 (world.h:203): the exact byte count m3World_Snapshot
+ * writes, -1 for a stale id. */
+M3GPU_API int32_t m3World_SnapshotSize(m3WorldId worldId);
+/* snapshot.c:613 (world.h:204): writes the world's snapshot (format
+ * v54), byte for byte what the reference engine writes for the same
+ * world: the persistent state including the broadphase tree and the id
+ * pools.  Returns the size, or -1 for a stale id, a null buffer or a
+ * capacity below m3World_SnapshotSize. */
+M3GPU_API int32_t m3World_Snapshot(m3WorldId worldId, void* out, int32_t capacity);
+
+/* snapshot.c:680 (world.h:205): restores a snapshot (format v54, taken
+ * by the reference engine or by this library) into a world created with
+ * the same capacities.  False, with the world untouched, on a foreign
+ * format or build, mismatched capacities or corrupt content; false with
+ * m3gpu_last_error() == M3GPU_ERR_UNSUPPORTED when the snapshot holds
+ * content the device path does not model (meshes, voxels, heightfields,
+ * characters, vehicles, soft bodies, water volumes). */
+M3GPU_API bool m3World_Restore(m3WorldId worldId, const void* data, int32_t size);
+
+/* world.c:3187 (world.h:606): replays a recorded command stream.  Steps
+ * run on the GPU; velocity sets, forces, torques and impulses apply
+ * between them.  The whole stream is validated first, so a refusal
+ * leaves the world untouched; other ops are refused with
+ * M3GPU_ERR_UNSUPPORTED. */
+M3GPU_API bool m3World_JournalReplay(m3WorldId worldId, const void* data, int32_t size);
+
 /* solver.c:4322 (world.h:195): one step of `dt` seconds in `substeps`
  * substeps, computed on the GPU.  Refuses (no-op) a stale id, dt <= 0 or
  * substeps outside [1, 256], like the reference.  A device-side refusal
@@ -224,6 +250,17 @@ M3GPU_API m3Vec3 m3Body_GetLinearVelocity(m3BodyId bodyId);
 M3GPU_API m3Vec3 m3Body_GetAngularVelocity(m3BodyId bodyId);
 /* body.h: awake query (dynamic bodies sleep; others report true) */
 M3GPU_API bool m3Body_IsAwake(m3BodyId bodyId);
+
+/* body.h:115-123 (body.c:818-1014): commands between steps.  Forces,
+ * torques and impulses act on dynamic bodies with mass; velocity sets on
+ * any live body; a nonzero command (any velocity set) wakes the body.
+ * Stale ids and non-finite vectors are no-ops. */
+M3GPU_API void m3Body_ApplyForce(m3BodyId bodyId, m3Vec3 force);
+M3GPU_API void m3Body_ApplyTorque(m3BodyId bodyId, m3Vec3 torque);
+M3GPU_API void m3Body_ApplyLinearImpulse(m3BodyId bodyId, m3Vec3 impulse);
+M3GPU_API void m3Body_ApplyAngularImpulse(m3BodyId bodyId, m3Vec3 impulse);
+M3GPU_API void m3Body_SetLinearVelocity(m3BodyId bodyId, m3Vec3 velocity);
+M3GPU_API void m3Body_SetAngularVelocity(m3BodyId bodyId, m3Vec3 velocity);
 
 /* shape.c:31 (shape.h:78) and the creators shape.c:763/782/802/1334 */
 M3GPU_API m3ShapeDef m3DefaultShapeDef(void);

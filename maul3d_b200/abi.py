@@ -7,6 +7,7 @@ reference build; `bind_common` declares them on any handle.
 from __future__ import annotations
 
 import ctypes as C
+import struct
 
 import numpy as np
 
@@ -71,6 +72,43 @@ def bind_common(lib: C.CDLL) -> C.CDLL:
     lib.m3Hash64.restype = C.c_uint64
     lib.m3GetVersion.argtypes = []
     lib.m3GetVersion.restype = C.c_int
+    return lib
+
+
+# Journal op codes (the reference's m3JournalOp numbering).
+OP_STEP = 1
+OP_SET_LINEAR_VELOCITY = 4
+OP_SET_ANGULAR_VELOCITY = 5
+OP_APPLY_FORCE = 26
+OP_APPLY_TORQUE = 27
+OP_APPLY_LINEAR_IMPULSE = 28
+OP_APPLY_ANGULAR_IMPULSE = 29
+
+
+def journal_step(dt: float, substeps: int) -> bytes:
+    """One step record: {float dt; int32 substeps} (world.c:1623)."""
+    return struct.pack("<ii", OP_STEP, 8) + struct.pack("<fi", dt, substeps)
+
+
+def journal_body_command(op: int, index1: int, generation: int, v) -> bytes:
+    """One body command record: {m3BodyId id; m3Vec3 v} (world.c:2286)."""
+    payload = struct.pack("<iHH3f", index1, 0, generation, *v)
+    return struct.pack("<ii", op, len(payload)) + payload
+
+
+def bind_snapshot(lib: C.CDLL) -> C.CDLL:
+    """Declare the snapshot, restore and journal entry points a handle has."""
+    for name, args, res in (("m3World_SnapshotSize", [m3WorldId], C.c_int32),
+                            ("m3World_Snapshot", [m3WorldId, C.c_void_p, C.c_int32], C.c_int32),
+                            ("m3World_Restore", [m3WorldId, C.c_void_p, C.c_int32], C.c_bool),
+                            ("m3World_JournalReplay", [m3WorldId, C.c_void_p, C.c_int32],
+                             C.c_bool)):
+        try:
+            fn = getattr(lib, name)
+        except AttributeError:
+            continue
+        fn.argtypes = args
+        fn.restype = res
     return lib
 
 
@@ -199,4 +237,9 @@ def bind_create(lib: C.CDLL) -> C.CDLL:
     lib.m3Joint_SetBreakThresholds.restype = None
     lib.m3Joint_IsValid.argtypes = [m3JointId]
     lib.m3Joint_IsValid.restype = C.c_bool
+    for name in ("m3Body_ApplyForce", "m3Body_ApplyTorque", "m3Body_ApplyLinearImpulse",
+                 "m3Body_ApplyAngularImpulse", "m3Body_SetLinearVelocity",
+                 "m3Body_SetAngularVelocity"):
+        getattr(lib, name).argtypes = [m3BodyId, m3Vec3]
+        getattr(lib, name).restype = None
     return lib

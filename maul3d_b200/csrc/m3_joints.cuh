@@ -526,12 +526,16 @@ __device__ void m3BreakJointsDev(const m3WorldView& w, m3real invH)
         w.jnextA[j] = -1;
         w.jnextB[j] = -1;
         w.jointAlive[j] = 0;
+        // The host's free queue learns of the slot through the ring:
+        // j when freed, -1 - j when retired at generation 0xFFFF.
+        int32_t entry = -1 - j;
         if (w.jointGen[j] != 0xFFFF)
         {
             w.jointGen[j] = (uint16_t)(w.jointGen[j] + 1);
-            w.jbroken[sc->brokenCount % sc->jointCap] = j;
-            sc->brokenCount += 1;
+            entry = j;
         }
+        w.jbroken[sc->brokenCount % sc->jointCap] = entry;
+        sc->brokenCount += 1;
     }
 }
 

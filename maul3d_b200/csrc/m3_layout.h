@@ -58,6 +58,9 @@ typedef struct m3WorldScalars
     // Joints the device destroyed (breakage), as a ring over jbroken:
     // the host drains entries [drained, brokenCount) into its free queue.
     int32_t brokenCount;
+    // The broadphase tree's root and free-list head (nodes: treeNodes).
+    int32_t treeRoot;
+    int32_t treeFreeList;
     int32_t pad1;
     // Work counters accumulated over every device step (observer only,
     // never hashed): the algorithmic-byte model of the roofline reads
@@ -69,6 +72,21 @@ typedef struct m3WorldScalars
     // list is M3_PHASE_* in step.cu).
     uint64_t phase[16];
 } m3WorldScalars;
+
+// One broadphase tree node, the reference's 72-byte record
+// (dynamic_tree.h:18-28): bounds, links (parent doubles as the free-list
+// next), the shape index on leaves, height (-1 free, 0 leaf).
+typedef struct m3TreeNode
+{
+    double lo[3];
+    double hi[3];
+    int32_t parent;
+    int32_t child1;
+    int32_t child2;
+    int32_t userData;
+    int32_t height;
+    int32_t pad;
+} m3TreeNode;
 
 // Per-body persistent arrays (capacity = bodyCap).
 #define M3_BODY_FIELDS(X)                                                                          \
@@ -122,6 +140,7 @@ typedef struct m3WorldScalars
     X(uint64_t, mask)                                                                              \
     X(int32_t, group)                                                                              \
     X(int32_t, shapeNext)                                                                          \
+    X(int32_t, proxyId)                                                                            \
     X(int32_t, hullIndex)                                                                          \
     X(uint8_t, shapeAlive)                                                                         \
     X(uint16_t, shapeGen)                                                                          \
@@ -155,6 +174,9 @@ typedef struct m3WorldScalars
     X(uint16_t, jointGen)                                                                          \
     X(int32_t, jbroken)
 
+// Broadphase tree nodes (capacity = 2 * shapeCap).
+#define M3_TREE_FIELDS(X) X(m3TreeNode, treeNodes)
+
 // Candidate pairs and manifolds, double-buffered: the step reads the
 // previous step's lists for the warm-start carry while it writes the
 // new ones (capacity = pairCap each).
@@ -172,6 +194,7 @@ typedef struct m3WorldView
     M3_BODY_FIELDS(M3_X_PTR)
     M3_SHAPE_FIELDS(M3_X_PTR)
     M3_JOINT_FIELDS(M3_X_PTR)
+    M3_TREE_FIELDS(M3_X_PTR)
     M3_PAIR_FIELDS(M3_X_PTR)
 #undef M3_X_PTR
     // Interned hull slabs (count-derived pool, outside the slab).
@@ -211,9 +234,11 @@ static inline int64_t m3LayoutPersistent(m3WorldView* view, uint8_t* base, int32
 #define M3_X_SHAPE(T, name) M3_X_OFF(T, name, shapeCap)
 #define M3_X_JOINT(T, name) M3_X_OFF(T, name, jointCap)
 #define M3_X_PAIR(T, name) M3_X_OFF(T, name, pairCap)
+#define M3_X_TREE(T, name) M3_X_OFF(T, name, 2 * (int64_t)shapeCap)
     M3_BODY_FIELDS(M3_X_BODY)
     M3_SHAPE_FIELDS(M3_X_SHAPE)
     M3_JOINT_FIELDS(M3_X_JOINT)
+    M3_TREE_FIELDS(M3_X_TREE)
     // The pair buffers start on a fresh 4 KiB page: the host pages before
     // them are page-locked for uploads, and a copy must not straddle the
     // locked and unlocked parts.
@@ -223,6 +248,7 @@ static inline int64_t m3LayoutPersistent(m3WorldView* view, uint8_t* base, int32
 #undef M3_X_SHAPE
 #undef M3_X_JOINT
 #undef M3_X_PAIR
+#undef M3_X_TREE
 #undef M3_X_OFF
     return off;
 }

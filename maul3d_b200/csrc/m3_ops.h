@@ -1,0 +1,105 @@
+// Body commands between steps: forces, torques, impulses and velocity
+// sets (body.c:335-418).  One definition serves the host API, the
+// journal replay and the device command kernel of the serving path, so
+// a command lands on the same bits wherever it is applied.
+#ifndef M3_OPS_H
+#define M3_OPS_H
+
+#include "m3_layout.h"
+
+// Journal op codes of the commands this path applies (the reference's
+// m3JournalOp numbering, world_internal.h:108-147).
+enum
+{
+    M3_OP_STEP = 1,
+    M3_OP_SET_LINEAR_VELOCITY = 4,
+    M3_OP_SET_ANGULAR_VELOCITY = 5,
+    M3_OP_APPLY_FORCE = 26,
+    M3_OP_APPLY_TORQUE = 27,
+    M3_OP_APPLY_LINEAR_IMPULSE = 28,
+    M3_OP_APPLY_ANGULAR_IMPULSE = 29,
+};
+
+// One command for the device kernel: `world` indexes the batch, `body`
+// the world's body slot.
+typedef struct m3BodyOp
+{
+    int32_t world;
+    int32_t op;
+    int32_t body;
+    m3Vec3 v;
+} m3BodyOp;
+
+M3_HD bool m3IsBodyOp(int32_t op)
+{
+    return op == M3_OP_SET_LINEAR_VELOCITY || op == M3_OP_SET_ANGULAR_VELOCITY ||
+           op == M3_OP_APPLY_FORCE || op == M3_OP_APPLY_TORQUE ||
+           op == M3_OP_APPLY_LINEAR_IMPULSE || op == M3_OP_APPLY_ANGULAR_IMPULSE;
+}
+
+// World-space inverse inertia R Il^-1 R^T, column by column
+// (solver.c:141-154).
+M3_HD m3Mat3 m3WorldInvInertiaHD(const m3WorldView& w, int32_t body)
+{
+    if (w.btype[body] != M3_BODY_DYNAMIC)
+    {
+        return m3ZeroMat3();
+    }
+    const m3Quat q = w.xf[body].q;
+    const m3Mat3 il = w.invI[body];
+    m3Mat3 r;
+    r.cx = m3RotateVec3(q, m3MulMV3(il, m3InvRotateVec3(q, v3(1.0f, 0.0f, 0.0f))));
+    r.cy = m3RotateVec3(q, m3MulMV3(il, m3InvRotateVec3(q, v3(0.0f, 1.0f, 0.0f))));
+    r.cz = m3RotateVec3(q, m3MulMV3(il, m3InvRotateVec3(q, v3(0.0f, 0.0f, 1.0f))));
+    return r;
+}
+
+// A nonzero command wakes the body (body.c:342-349).
+M3_HD void m3WakeOnCommand(const m3WorldView& w, int32_t body, m3Vec3 a)
+{
+    if (a.x != 0.0f || a.y != 0.0f || a.z != 0.0f)
+    {
+        w.awake[body] = 1;
+        w.sleepTime[body] = 0.0f;
+    }
+}
+
+// Applies one command to a live body slot (body.c:351-418).  The
+// caller has validated the slot and the vector (and, for the public
+// force and impulse entry points, that the body is dynamic with mass).
+M3_HD void m3ApplyBodyOp(const m3WorldView& w, int32_t op, int32_t body, m3Vec3 v)
+{
+    switch (op)
+    {
+    case M3_OP_SET_LINEAR_VELOCITY:
+        w.awake[body] = 1;
+        w.sleepTime[body] = 0.0f;
+        w.v[body] = v;
+        break;
+    case M3_OP_SET_ANGULAR_VELOCITY:
+        w.awake[body] = 1;
+        w.sleepTime[body] = 0.0f;
+        w.w[body] = v;
+        break;
+    case M3_OP_APPLY_FORCE:
+        w.force[body] = m3Add3(w.force[body], v);
+        m3WakeOnCommand(w, body, v);
+        break;
+    case M3_OP_APPLY_TORQUE:
+        w.torque[body] = m3Add3(w.torque[body], v);
+        m3WakeOnCommand(w, body, v);
+        break;
+    case M3_OP_APPLY_LINEAR_IMPULSE:
+        w.v[body] = m3Add3(w.v[body], m3MulSV3(w.invMass[body], v));
+        m3WakeOnCommand(w, body, v);
+        break;
+    case M3_OP_APPLY_ANGULAR_IMPULSE:
+        w.w[body] = m3Add3(w.w[body], m3MulMV3(m3WorldInvInertiaHD(w, body), v));
+        m3WakeOnCommand(w, body, v);
+        break;
+    default:
+        break;
+    }
+}
+
+#endif // M3_OPS_H

@@ -1,0 +1,411 @@
+// The broadphase tree the reference keeps as world state (its nodes and
+// proxy ids are snapshot bytes, snapshot.c:245-247): a dynamic AABB tree
+// of fat shape bounds, grown by surface-area-heuristic descent and kept
+// balanced by AVL-style rotations (dynamic_tree.c:16-363).  This path
+// does not query it (candidate pairs come from a sort-and-sweep over
+// fresh bounds, the same set); it maintains it so a snapshot carries the
+// reference's tree byte for byte.  Every bound is a double and every
+// decision a strict comparison, so the same sequence of inserts and
+// removes gives the same nodes on the host (shape creation) and on the
+// device (the per-step refresh).
+#ifndef M3_TREE_H
+#define M3_TREE_H
+
+#include "m3_layout.h"
+
+#define M3_TREE_NULL (-1)
+
+typedef struct m3Aabb
+{
+    double lo[3];
+    double hi[3];
+} m3Aabb;
+
+// A tree over a node array of fixed capacity; root and free-list head
+// live in the world scalars.
+typedef struct m3TreeRef
+{
+    m3TreeNode* nodes;
+    int32_t capacity;
+    int32_t* root;
+    int32_t* freeList;
+} m3TreeRef;
+
+M3_HD m3TreeRef m3WorldTree(const m3WorldView& w)
+{
+    m3TreeRef t;
+    t.nodes = w.treeNodes;
+    t.capacity = 2 * w.sc->shapeCap;
+    t.root = &w.sc->treeRoot;
+    t.freeList = &w.sc->treeFreeList;
+    return t;
+}
+
+// An empty tree: every node free, chained in index order
+// (dynamic_tree.c:41-55).
+M3_HD void m3TreeInit(m3TreeRef t)
+{
+    for (int32_t i = 0; i < t.capacity; ++i)
+    {
+        m3TreeNode n;
+        for (int32_t k = 0; k < 3; ++k)
+        {
+            n.lo[k] = 0.0;
+            n.hi[k] = 0.0;
+        }
+        n.parent = i + 1 < t.capacity ? i + 1 : M3_TREE_NULL;
+        n.child1 = 0;
+        n.child2 = 0;
+        n.userData = 0;
+        n.height = -1;
+        n.pad = 0;
+        t.nodes[i] = n;
+    }
+    *t.root = M3_TREE_NULL;
+    *t.freeList = t.capacity > 0 ? 0 : M3_TREE_NULL;
+}
+
+M3_HD double m3TreeArea(const double lo[3], const double hi[3])
+{
+    const double dx = hi[0] - lo[0];
+    const double dy = hi[1] - lo[1];
+    const double dz = hi[2] - lo[2];
+    return 2.0 * (dx * dy + dy * dz + dz * dx);
+}
+
+M3_HD void m3TreeUnion(const double aLo[3], const double aHi[3], const double bLo[3],
+                       const double bHi[3], double outLo[3], double outHi[3])
+{
+    for (int32_t k = 0; k < 3; ++k)
+    {
+        outLo[k] = aLo[k] < bLo[k] ? aLo[k] : bLo[k];
+        outHi[k] = aHi[k] > bHi[k] ? aHi[k] : bHi[k];
+    }
+}
+
+M3_HD int32_t m3TreeTakeNode(m3TreeRef t)
+{
+    const int32_t id = *t.freeList;
+    if (id == M3_TREE_NULL)
+    {
+        return M3_TREE_NULL;
+    }
+    m3TreeNode* n = t.nodes + id;
+    *t.freeList = n->parent;
+    n->parent = M3_TREE_NULL;
+    n->child1 = M3_TREE_NULL;
+    n->child2 = M3_TREE_NULL;
+    n->height = 0;
+    n->userData = -1;
+    n->pad = 0;
+    return id;
+}
+
+// A freed node is zeroed and pushed on the free chain (dynamic_tree.c:83-90).
+M3_HD void m3TreeGiveNode(m3TreeRef t, int32_t id)
+{
+    m3TreeNode* n = t.nodes + id;
+    for (int32_t k = 0; k < 3; ++k)
+    {
+        n->lo[k] = 0.0;
+        n->hi[k] = 0.0;
+    }
+    n->child1 = 0;
+    n->child2 = 0;
+    n->userData = 0;
+    n->pad = 0;
+    n->parent = *t.freeList;
+    n->height = -1;
+    *t.freeList = id;
+}
+
+M3_HD int32_t m3TreeMaxI(int32_t a, int32_t b)
+{
+    return a > b ? a : b;
+}
+
+// Re-links `child` under `parent` in place of `old` (or as the root).
+M3_HD void m3TreeReplaceChild(m3TreeRef t, int32_t parent, int32_t old, int32_t child)
+{
+    if (parent != M3_TREE_NULL)
+    {
+        if (t.nodes[parent].child1 == old)
+        {
+            t.nodes[parent].child1 = child;
+        }
+        else
+        {
+            t.nodes[parent].child2 = child;
+        }
+    }
+    else
+    {
+        *t.root = child;
+    }
+}
+
+// Rotates the subtree at a when its children's heights differ by more
+// than one: the taller child (p) rises, a becomes its child, and a keeps
+// the shorter of p's children while p keeps the taller one
+// (dynamic_tree.c:92-203).  Returns the subtree's new root.
+M3_HD int32_t m3TreeRotate(m3TreeRef t, int32_t a)
+{
+    m3TreeNode* nodes = t.nodes;
+    if (nodes[a].height < 2 || nodes[a].child1 == M3_TREE_NULL)
+    {
+        return a;
+    }
+    const int32_t b = nodes[a].child1;
+    const int32_t c = nodes[a].child2;
+    const int32_t balance = nodes[c].height - nodes[b].height;
+    if (balance > -2 && balance < 2)
+    {
+        return a;
+    }
+    // p rises; q is a's other child, which a keeps.
+    const bool right = balance > 1;
+    const int32_t p = right ? c : b;
+    const int32_t q = right ? b : c;
+    const int32_t p1 = nodes[p].child1;
+    const int32_t p2 = nodes[p].child2;
+    nodes[p].child1 = a;
+    nodes[p].parent = nodes[a].parent;
+    nodes[a].parent = p;
+    m3TreeReplaceChild(t, nodes[p].parent, a, p);
+    // keep: p's taller child stays with p; move: the other goes to a.
+    const bool firstTaller = nodes[p1].height > nodes[p2].height;
+    const int32_t keep = firstTaller ? p1 : p2;
+    const int32_t move = firstTaller ? p2 : p1;
+    nodes[p].child2 = keep;
+    if (right)
+    {
+        nodes[a].child2 = move;
+    }
+    else
+    {
+        nodes[a].child1 = move;
+    }
+    nodes[move].parent = a;
+    m3TreeUnion(nodes[q].lo, nodes[q].hi, nodes[move].lo, nodes[move].hi, nodes[a].lo,
+                nodes[a].hi);
+    m3TreeUnion(nodes[a].lo, nodes[a].hi, nodes[keep].lo, nodes[keep].hi, nodes[p].lo,
+                nodes[p].hi);
+    nodes[a].height = 1 + m3TreeMaxI(nodes[q].height, nodes[move].height);
+    nodes[p].height = 1 + m3TreeMaxI(nodes[a].height, nodes[keep].height);
+    return p;
+}
+
+// Walks from `index` to the root, rebalancing and refitting heights and
+// bounds (dynamic_tree.c:205-219).
+M3_HD void m3TreeRefit(m3TreeRef t, int32_t index)
+{
+    m3TreeNode* nodes = t.nodes;
+    while (index != M3_TREE_NULL)
+    {
+        index = m3TreeRotate(t, index);
+        m3TreeNode* n = nodes + index;
+        const int32_t c1 = n->child1;
+        const int32_t c2 = n->child2;
+        n->height = 1 + m3TreeMaxI(nodes[c1].height, nodes[c2].height);
+        m3TreeUnion(nodes[c1].lo, nodes[c1].hi, nodes[c2].lo, nodes[c2].hi, n->lo, n->hi);
+        index = n->parent;
+    }
+}
+
+// Surface-area cost of pairing the new box with a child: the area of
+// the union, less the child's own area when the child is internal (a
+// leaf gains a new parent whose area all counts), plus the inherited
+// cost of growing the ancestors (dynamic_tree.c:245-273).
+M3_HD double m3TreeChildCost(const m3TreeNode& child, const double lo[3], const double hi[3],
+                             double inherited)
+{
+    double ulo[3];
+    double uhi[3];
+    m3TreeUnion(child.lo, child.hi, lo, hi, ulo, uhi);
+    if (child.height == 0)
+    {
+        return m3TreeArea(ulo, uhi) + inherited;
+    }
+    return m3TreeArea(ulo, uhi) - m3TreeArea(child.lo, child.hi) + inherited;
+}
+
+// Inserts a leaf for `userData` with bounds [lo, hi]; returns its node or
+// M3_TREE_NULL when the node pool is exhausted (dynamic_tree.c:221-322).
+M3_HD int32_t m3TreeInsert(m3TreeRef t, const double lo[3], const double hi[3], int32_t userData)
+{
+    const int32_t leaf = m3TreeTakeNode(t);
+    if (leaf == M3_TREE_NULL)
+    {
+        return M3_TREE_NULL;
+    }
+    m3TreeNode* nodes = t.nodes;
+    for (int32_t k = 0; k < 3; ++k)
+    {
+        nodes[leaf].lo[k] = lo[k];
+        nodes[leaf].hi[k] = hi[k];
+    }
+    nodes[leaf].userData = userData;
+    nodes[leaf].height = 0;
+    if (*t.root == M3_TREE_NULL)
+    {
+        *t.root = leaf;
+        return leaf;
+    }
+    // Descend while a child is cheaper than pairing here.
+    int32_t index = *t.root;
+    while (nodes[index].height > 0)
+    {
+        double ulo[3];
+        double uhi[3];
+        m3TreeUnion(nodes[index].lo, nodes[index].hi, lo, hi, ulo, uhi);
+        const double area = m3TreeArea(ulo, uhi);
+        const double here = 2.0 * area;
+        const double inherited = 2.0 * (area - m3TreeArea(nodes[index].lo, nodes[index].hi));
+        const int32_t c1 = nodes[index].child1;
+        const int32_t c2 = nodes[index].child2;
+        const double cost1 = m3TreeChildCost(nodes[c1], lo, hi, inherited);
+        const double cost2 = m3TreeChildCost(nodes[c2], lo, hi, inherited);
+        if (here < cost1 && here < cost2)
+        {
+            break;
+        }
+        index = cost1 < cost2 ? c1 : c2;
+    }
+    // A new parent takes the sibling's place; sibling and leaf hang
+    // under it in that order.
+    const int32_t sibling = index;
+    const int32_t oldParent = nodes[sibling].parent;
+    const int32_t parent = m3TreeTakeNode(t);
+    if (parent == M3_TREE_NULL)
+    {
+        m3TreeGiveNode(t, leaf);
+        return M3_TREE_NULL;
+    }
+    nodes[parent].parent = oldParent;
+    nodes[parent].userData = -1;
+    m3TreeUnion(lo, hi, nodes[sibling].lo, nodes[sibling].hi, nodes[parent].lo, nodes[parent].hi);
+    nodes[parent].height = nodes[sibling].height + 1;
+    m3TreeReplaceChild(t, oldParent, sibling, parent);
+    nodes[parent].child1 = sibling;
+    nodes[parent].child2 = leaf;
+    nodes[sibling].parent = parent;
+    nodes[leaf].parent = parent;
+    m3TreeRefit(t, parent);
+    return leaf;
+}
+
+// Removes a leaf; its parent is freed and the sibling takes the parent's
+// place (dynamic_tree.c:324-358).
+M3_HD void m3TreeRemove(m3TreeRef t, int32_t leaf)
+{
+    m3TreeNode* nodes = t.nodes;
+    if (leaf == *t.root)
+    {
+        *t.root = M3_TREE_NULL;
+        m3TreeGiveNode(t, leaf);
+        return;
+    }
+    const int32_t parent = nodes[leaf].parent;
+    const int32_t grand = nodes[parent].parent;
+    const int32_t sibling =
+        nodes[parent].child1 == leaf ? nodes[parent].child2 : nodes[parent].child1;
+    if (grand != M3_TREE_NULL)
+    {
+        m3TreeReplaceChild(t, grand, parent, sibling);
+        nodes[sibling].parent = grand;
+        m3TreeGiveNode(t, parent);
+        m3TreeRefit(t, grand);
+    }
+    else
+    {
+        *t.root = sibling;
+        nodes[sibling].parent = M3_TREE_NULL;
+        m3TreeGiveNode(t, parent);
+    }
+    m3TreeGiveNode(t, leaf);
+}
+
+M3_HD bool m3TreeContains(const m3TreeNode& n, const m3Aabb& b)
+{
+    return n.lo[0] <= b.lo[0] && n.lo[1] <= b.lo[1] && n.lo[2] <= b.lo[2] && b.hi[0] <= n.hi[0] &&
+           b.hi[1] <= n.hi[1] && b.hi[2] <= n.hi[2];
+}
+
+// Shape pose in the world: body pose composed with the compound offset
+// (world_internal.h:1276-1290).
+M3_HD m3Transform m3ShapePose(const m3WorldView& w, int32_t shape)
+{
+    const int32_t body = w.shapeBody[shape];
+    m3Transform xf = w.xf[body];
+    if (w.hasOffset[shape] != 0)
+    {
+        const m3Vec3 r = m3RotateVec3(xf.q, w.localPos[shape]);
+        xf.p.x += (double)r.x;
+        xf.p.y += (double)r.y;
+        xf.p.z += (double)r.z;
+        xf.q = m3MulQuat(xf.q, w.localRot[shape]);
+    }
+    return xf;
+}
+
+// Fresh bounds of one non-plane shape, tight plus the margin
+// (broad_phase.c:22-135): hull vertices rotated out, capsule cap
+// centres, sphere centre, min and max in double.
+M3_HD m3Aabb m3ShapeFreshBounds(const m3WorldView& w, int32_t shape)
+{
+    const m3Transform xf = m3ShapePose(w, shape);
+    m3Aabb box;
+    const uint8_t type = w.shapeType[shape];
+    if (type == M3_SHAPE_HULL)
+    {
+        const m3HullData* hull = &w.hulls[w.hullIndex[shape]];
+        for (int32_t k = 0; k < 3; ++k)
+        {
+            box.lo[k] = 1.0e30;
+            box.hi[k] = -1.0e30;
+        }
+        const int32_t nv = hull->vertexCount;
+        for (int32_t v = 0; v < nv; ++v)
+        {
+            const m3Vec3 r = m3RotateVec3(xf.q, hull->vertices[v]);
+            const double p[3] = {xf.p.x + (double)r.x, xf.p.y + (double)r.y,
+                                 xf.p.z + (double)r.z};
+            for (int32_t k = 0; k < 3; ++k)
+            {
+                box.lo[k] = p[k] < box.lo[k] ? p[k] : box.lo[k];
+                box.hi[k] = p[k] > box.hi[k] ? p[k] : box.hi[k];
+            }
+        }
+        for (int32_t k = 0; k < 3; ++k)
+        {
+            box.lo[k] -= (double)M3_AABB_MARGIN;
+            box.hi[k] += (double)M3_AABB_MARGIN;
+        }
+        return box;
+    }
+    if (type == M3_SHAPE_CAPSULE)
+    {
+        const m3Vec3 r1 = m3RotateVec3(xf.q, w.geom[shape].v);
+        const m3Vec3 r2 = m3RotateVec3(xf.q, w.geom[shape].v2);
+        const double c1[3] = {xf.p.x + (double)r1.x, xf.p.y + (double)r1.y, xf.p.z + (double)r1.z};
+        const double c2[3] = {xf.p.x + (double)r2.x, xf.p.y + (double)r2.y, xf.p.z + (double)r2.z};
+        const double fat = (double)(w.geom[shape].s + M3_AABB_MARGIN);
+        for (int32_t k = 0; k < 3; ++k)
+        {
+            box.lo[k] = (c1[k] < c2[k] ? c1[k] : c2[k]) - fat;
+            box.hi[k] = (c1[k] > c2[k] ? c1[k] : c2[k]) + fat;
+        }
+        return box;
+    }
+    const m3Vec3 r = m3RotateVec3(xf.q, w.geom[shape].v);
+    const double c[3] = {xf.p.x + (double)r.x, xf.p.y + (double)r.y, xf.p.z + (double)r.z};
+    const double fat = (double)(w.geom[shape].s + M3_AABB_MARGIN);
+    for (int32_t k = 0; k < 3; ++k)
+    {
+        box.lo[k] = c[k] - fat;
+        box.hi[k] = c[k] + fat;
+    }
+    return box;
+}
+
+#endif // M3_TREE_H

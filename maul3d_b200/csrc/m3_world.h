@@ -8,7 +8,6 @@
 
 #include <stdint.h>
 #include <stdlib.h>
-#include <deque>
 #include <new>
 #include <unordered_map>
 #include <vector>
@@ -68,6 +67,42 @@ template <class T> struct m3PageAllocator
     }
 };
 
+// A slot pool's free queue as the reference keeps it (allocator.c:178-
+// 218): a ring over `capacity` entries read from `head`, so a snapshot
+// carries it byte for byte.  Slots whose generation reached 0xFFFF are
+// retired instead of queued.
+struct m3FreeRing
+{
+    std::vector<int32_t> queue;
+    int32_t head = 0;
+    int32_t count = 0;
+    int32_t retired = 0;
+
+    void Init(int32_t capacity)
+    {
+        queue.assign((size_t)capacity, 0);
+        head = 0;
+        count = 0;
+        retired = 0;
+    }
+    bool Pop(int32_t* index)
+    {
+        if (count <= 0)
+        {
+            return false;
+        }
+        *index = queue[(size_t)head];
+        head = (head + 1) % (int32_t)queue.size();
+        count -= 1;
+        return true;
+    }
+    void Push(int32_t index)
+    {
+        queue[(size_t)((head + count) % (int32_t)queue.size())] = index;
+        count += 1;
+    }
+};
+
 struct m3HostWorld
 {
     int32_t slot = -1;
@@ -86,11 +121,29 @@ struct m3HostWorld
     // pool is sized by the hulls actually interned (count-derived, as
     // the reference's snapshot treats them).
     std::vector<m3HullData, m3PageAllocator<m3HullData>> hulls;
-    // Recycled joint slots, reused first in FIFO order (allocator.c:178-
-    // 218); the device's breakage appends to it through the jbroken ring,
+    // Recycled slots of each pool, reused first (FIFO).  The device's
+    // joint breakage appends to jointFree through the jbroken ring,
     // drained up to `brokenDrained` at each download.
-    std::deque<int32_t> jointFree;
+    m3FreeRing bodyFree;
+    m3FreeRing shapeFree;
+    m3FreeRing hullFree;
+    m3FreeRing jointFree;
     int32_t brokenDrained = 0;
+    // Hull slot generations (the pool's liveness is the reference count).
+    std::vector<uint16_t> hullGen;
+    // Snapshot bytes of the state this path does not model, as the last
+    // restore read them, written back by the next snapshot (empty for a
+    // world built here: it writes a fresh world's values).
+    std::vector<uint8_t> snapshotCarry;
+    std::vector<uint8_t> snapshotHeaderCarry;
+    std::vector<float> heightFieldCellCarry;
+    // Capacities of the pools this path does not model; they size the
+    // snapshot's blocks (snapshot.c:161-600).
+    int32_t meshCap = 0;
+    int32_t voxelCap = 0;
+    int32_t charCap = 0;
+    int32_t vehicleCap = 0;
+    int32_t softCap = 0;
     std::vector<int32_t> hullRefs;
     std::unordered_multimap<uint64_t, int32_t> hullIndexByContent;
 
@@ -123,6 +176,20 @@ int32_t m3gpuDownload(m3HostWorld* w);
 void m3gpuRelease(m3HostWorld* w);
 // Make the host image current before a host read or write.
 int32_t m3gpuSyncHost(m3HostWorld* w);
+// One validated journal record (snapshot.cpp): a step or a body command.
+struct m3JournalRecordView
+{
+    int32_t op;
+    int32_t body;
+    m3Vec3 v;
+    float dt;
+    int32_t substeps;
+};
+// Parses and validates a whole journal against a world's bodies; false
+// (with the error set) on the first bad or unsupported record.
+bool m3ParseJournal(const m3HostWorld* w, const uint8_t* stream, int32_t size,
+                    std::vector<m3JournalRecordView>* out);
+
 // Queue the joint slots the device freed since the last call (world.cpp).
 void m3DrainBrokenJoints(m3HostWorld* w);
 

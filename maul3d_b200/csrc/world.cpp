@@ -13,6 +13,8 @@
 // frames, create).
 
 #include "m3_world.h"
+#include "m3_ops.h"
+#include "m3_tree.h"
 #include "m3_hash.h"
 
 #include <math.h>
@@ -152,6 +154,16 @@ extern "C" m3WorldId m3CreateWorld(const m3WorldDef* def)
     w->shapeCap = def->shapeCapacity;
     w->jointCap = def->jointCapacity;
     w->pairCap = 8 * def->shapeCapacity; // world.c:429
+    w->meshCap = def->meshCapacity;
+    w->voxelCap = def->voxelCapacity;
+    w->charCap = def->characterCapacity;
+    w->vehicleCap = def->vehicleCapacity;
+    w->softCap = def->softBodyCapacity;
+    w->bodyFree.Init(w->bodyCap);
+    w->shapeFree.Init(w->shapeCap);
+    w->hullFree.Init(w->shapeCap);
+    w->hullGen.assign((size_t)w->shapeCap, 0);
+    w->jointFree.Init(w->jointCap);
     w->persistentBytes =
         m3LayoutPersistent(nullptr, nullptr, w->bodyCap, w->shapeCap, w->jointCap, w->pairCap);
     w->image.assign((size_t)w->persistentBytes, 0);
@@ -183,8 +195,10 @@ extern "C" m3WorldId m3CreateWorld(const m3WorldDef* def)
         w->hv.shapeHead[i] = -1;
         w->hv.jointHead[i] = -1;
     }
+    m3TreeInit(m3WorldTree(w->hv));
     for (int32_t i = 0; i < w->shapeCap; ++i)
     {
+        w->hv.proxyId[i] = M3_TREE_NULL;
         w->hv.shapeNext[i] = -1;
         w->hv.hullIndex[i] = -1;
         w->hv.shapeBody[i] = -1;
@@ -195,9 +209,6 @@ extern "C" m3WorldId m3CreateWorld(const m3WorldDef* def)
         w->hv.jbodyB[i] = -1;
         w->hv.jnextA[i] = -1;
         w->hv.jnextB[i] = -1;
-        w->hv.jtargetQ[i] = m3IdentityQuat();
-        w->hv.jframeA[i] = m3IdentityQuat();
-        w->hv.jframeB[i] = m3IdentityQuat();
     }
     s_worlds[slot] = w;
     m3WorldId id = {slot + 1, w->generation};
@@ -283,13 +294,18 @@ extern "C" m3BodyId m3CreateBody(m3WorldId worldId, const m3BodyDef* def)
         return nullId;
     }
     m3WorldView& v = w->hv;
-    if (v.sc->bodyMax >= w->bodyCap)
+    // Recycled slots first, then a fresh one (allocator.c:178-198).
+    int32_t i = -1;
+    if (!w->bodyFree.Pop(&i))
     {
-        m3gpuSetError(M3GPU_ERR_CAPACITY, "m3CreateBody: body pool exhausted");
-        return nullId;
+        if (v.sc->bodyMax >= w->bodyCap)
+        {
+            m3gpuSetError(M3GPU_ERR_CAPACITY, "m3CreateBody: body pool exhausted");
+            return nullId;
+        }
+        i = v.sc->bodyMax;
+        v.sc->bodyMax += 1;
     }
-    int32_t i = v.sc->bodyMax;
-    v.sc->bodyMax += 1;
     v.bodyAlive[i] = 1;
     v.xf[i].p = def->position;
     v.xf[i].q = m3NormalizeQuat(def->rotation);
@@ -371,6 +387,55 @@ extern "C" bool m3Body_IsAwake(m3BodyId bodyId)
     return ReadBody(bodyId, false, [](const m3WorldView& v, int32_t i) {
         return v.btype[i] != M3_BODY_DYNAMIC || v.awake[i] != 0;
     });
+}
+
+// Commands between steps (body.c:818-1014): forces, torques and
+// impulses reach dynamic bodies with mass only; velocity sets reach any
+// live body.  A stale id or a non-finite vector is a no-op.
+static void BodyCommand(m3BodyId id, int32_t op, m3Vec3 v, bool needsMass)
+{
+    int32_t index;
+    m3HostWorld* w = ResolveBody(id, &index);
+    if (w == nullptr || !FiniteV3(v) || m3gpuSyncHost(w) != M3GPU_OK)
+    {
+        return;
+    }
+    if (needsMass && !(w->hv.btype[index] == M3_BODY_DYNAMIC && w->hv.invMass[index] > 0.0f))
+    {
+        return;
+    }
+    m3ApplyBodyOp(w->hv, op, index, v);
+    w->hostDirty = true;
+}
+
+extern "C" void m3Body_ApplyForce(m3BodyId bodyId, m3Vec3 force)
+{
+    BodyCommand(bodyId, M3_OP_APPLY_FORCE, force, true);
+}
+
+extern "C" void m3Body_ApplyTorque(m3BodyId bodyId, m3Vec3 torque)
+{
+    BodyCommand(bodyId, M3_OP_APPLY_TORQUE, torque, true);
+}
+
+extern "C" void m3Body_ApplyLinearImpulse(m3BodyId bodyId, m3Vec3 impulse)
+{
+    BodyCommand(bodyId, M3_OP_APPLY_LINEAR_IMPULSE, impulse, true);
+}
+
+extern "C" void m3Body_ApplyAngularImpulse(m3BodyId bodyId, m3Vec3 impulse)
+{
+    BodyCommand(bodyId, M3_OP_APPLY_ANGULAR_IMPULSE, impulse, true);
+}
+
+extern "C" void m3Body_SetLinearVelocity(m3BodyId bodyId, m3Vec3 velocity)
+{
+    BodyCommand(bodyId, M3_OP_SET_LINEAR_VELOCITY, velocity, false);
+}
+
+extern "C" void m3Body_SetAngularVelocity(m3BodyId bodyId, m3Vec3 velocity)
+{
+    BodyCommand(bodyId, M3_OP_SET_ANGULAR_VELOCITY, velocity, false);
 }
 
 // ---------------------------------------------------------------------
@@ -733,14 +798,23 @@ static int32_t InternHull(m3HostWorld* w, const m3HullData* data)
             return i;
         }
     }
-    if (sc->hullMax >= w->shapeCap)
+    int32_t index = -1;
+    if (w->hullFree.Pop(&index))
     {
-        return -1;
+        w->hulls[(size_t)index] = *data;
+        w->hullRefs[(size_t)index] = 1;
     }
-    int32_t index = sc->hullMax;
-    sc->hullMax += 1;
-    w->hulls.push_back(*data);
-    w->hullRefs.push_back(1);
+    else
+    {
+        if (sc->hullMax >= w->shapeCap)
+        {
+            return -1;
+        }
+        index = sc->hullMax;
+        sc->hullMax += 1;
+        w->hulls.push_back(*data);
+        w->hullRefs.push_back(1);
+    }
     w->hullIndexByContent.emplace(key, index);
     return index;
 }
@@ -792,7 +866,7 @@ static m3ShapeId CreateShapeCommon(m3BodyId bodyId, const m3ShapeDef* def, uint8
         return nullId;
     }
     m3WorldView& v = w->hv;
-    if (v.sc->shapeMax >= w->shapeCap)
+    if (v.sc->shapeMax >= w->shapeCap && w->shapeFree.count == 0)
     {
         m3gpuSetError(M3GPU_ERR_CAPACITY, "create shape: shape pool exhausted");
         return nullId;
@@ -809,8 +883,12 @@ static m3ShapeId CreateShapeCommon(m3BodyId bodyId, const m3ShapeDef* def, uint8
             return nullId;
         }
     }
-    int32_t s = v.sc->shapeMax;
-    v.sc->shapeMax += 1;
+    int32_t s = -1;
+    if (!w->shapeFree.Pop(&s))
+    {
+        s = v.sc->shapeMax;
+        v.sc->shapeMax += 1;
+    }
     v.shapeAlive[s] = 1;
     v.shapeBody[s] = b;
     v.shapeType[s] = type;
@@ -838,6 +916,15 @@ static m3ShapeId CreateShapeCommon(m3BodyId bodyId, const m3ShapeDef* def, uint8
     v.shapeNext[s] = v.shapeHead[b];
     v.shapeHead[b] = s;
     v.hullIndex[s] = hullIndex;
+    // Every shape but a plane enters the broadphase tree with its fresh
+    // bounds (shape.c:589-606).
+    if (type != M3_SHAPE_PLANE)
+    {
+        m3WorldView tv = v;
+        tv.hulls = w->hulls.empty() ? nullptr : w->hulls.data();
+        const m3Aabb box = m3ShapeFreshBounds(tv, s);
+        v.proxyId[s] = m3TreeInsert(m3WorldTree(v), box.lo, box.hi, s);
+    }
     RecomputeMass(w, b);
     w->hostDirty = true;
     m3ShapeId id = {s + 1, (uint16_t)w->slot, v.shapeGen[s]};
@@ -1071,10 +1158,8 @@ extern "C" m3JointId m3CreateJoint(const m3JointDef* def)
     }
     // Recycled slots first, FIFO, then a fresh one (allocator.c:178-198).
     int32_t j = -1;
-    if (!w->jointFree.empty())
+    if (w->jointFree.Pop(&j))
     {
-        j = w->jointFree.front();
-        w->jointFree.pop_front();
     }
     else if (v.sc->jointMax < w->jointCap)
     {
@@ -1142,7 +1227,17 @@ void m3DrainBrokenJoints(m3HostWorld* w)
     const int32_t cap = w->jointCap > 0 ? w->jointCap : 1;
     while (w->brokenDrained < w->hv.sc->brokenCount)
     {
-        w->jointFree.push_back(w->hv.jbroken[w->brokenDrained % cap]);
+        // Entry j: slot j freed; entry -1 - j: slot j retired (its
+        // generation had reached 0xFFFF).
+        const int32_t e = w->hv.jbroken[w->brokenDrained % cap];
+        if (e >= 0)
+        {
+            w->jointFree.Push(e);
+        }
+        else
+        {
+            w->jointFree.retired += 1;
+        }
         w->brokenDrained += 1;
     }
 }

@@ -1,0 +1,215 @@
+"""Snapshot restore and journal ingestion (CPU): a snapshot the reference
+engine takes (format v54, snapshot.c:613-678) restores into a world of
+this library with the reference's hash, pools and free queues; corrupt,
+foreign or unsupported snapshots are refused with the world untouched
+(snapshot.c:680-826).  Journal records of body commands apply with the
+reference's arithmetic (body.c:351-418, world.c:2283-2321); stepping
+journals run on the GPU (tests/test_serving_gpu.py).
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from maul3d_b200 import abi
+from maul3d_b200.abi import SCENE_BOX_PYRAMID, SCENE_TOWERS, SCENE_UNEVEN
+
+
+def _snapshot(lib, wid) -> bytes:
+    n = lib.m3World_SnapshotSize(wid)
+    assert n > 0
+    buf = (C.c_uint8 * n)()
+    assert lib.m3World_Snapshot(wid, buf, n) == n
+    return bytes(buf)
+
+
+def _restore(lib, wid, data: bytes) -> bool:
+    buf = (C.c_uint8 * len(data)).from_buffer_copy(data)
+    return bool(lib.m3World_Restore(wid, buf, len(data)))
+
+
+def _replay(lib, wid, data: bytes) -> bool:
+    buf = (C.c_uint8 * max(len(data), 1)).from_buffer_copy(data or b"\0")
+    return bool(lib.m3World_JournalReplay(wid, buf, len(data)))
+
+
+@pytest.fixture(scope="module")
+def libs(m3, oracle):
+    ref = abi.bind_snapshot(abi.bind_create(oracle.lib()))
+    ours = abi.bind_snapshot(abi.bind_create(m3.lib))
+    return ours, ref
+
+
+@pytest.mark.parametrize("scene,seed,param,steps", [
+    (SCENE_BOX_PYRAMID, 0, 20, 40),
+    (SCENE_UNEVEN, 21, 64, 90),
+    (SCENE_TOWERS, 7, 4, 40),
+])
+def test_reference_snapshot_restores_with_the_reference_hash(m3, oracle, libs, scene, seed,
+                                                            param, steps):
+    ours, ref = libs
+    r = oracle.RefWorld.scene(scene, seed, param)
+    r.step(1.0 / 60.0, 4, steps)
+    snap = _snapshot(ref, r.id)
+    # A fresh world of the same scene (same capacities), never stepped.
+    g = m3.World.scene(scene, seed, param)
+    assert _restore(ours, g.id, snap), m3.last_error()
+    assert g.hash() == r.hash()
+    assert g.state().first_difference(r.state()) is None
+    g.destroy()
+    r.destroy()
+
+
+def test_restore_recycles_slots_like_the_reference(m3, oracle, libs):
+    # Joints broken before the snapshot sit in its free queue: a joint
+    # created after the restore takes the first one, with its generation.
+    ours, ref = libs
+    r = oracle.RefWorld.scene(SCENE_TOWERS, 7, 4)
+    r.step(1.0 / 60.0, 4, 40)
+    snap = _snapshot(ref, r.id)
+    g = m3.World.scene(SCENE_TOWERS, 7, 4)
+    assert _restore(ours, g.id, snap)
+    made = []
+    for lib, wid in ((ours, g.id), (ref, r.id)):
+        jd = lib.m3DefaultJointDef()
+        jd.type = 3
+        jd.bodyA = abi.m3BodyId(2, wid.index1 - 1, 0)
+        jd.bodyB = abi.m3BodyId(3, wid.index1 - 1, 0)
+        jd.localAnchorA = abi.m3Vec3(0.5, 0.0, 0.0)
+        jd.localAnchorB = abi.m3Vec3(-0.5, 0.0, 0.0)
+        j = lib.m3CreateJoint(C.byref(jd))
+        made.append((j.index1, j.generation))
+    assert made[0] == made[1] and made[0][1] == 1
+    assert g.hash() == r.hash()
+
+
+def test_corrupt_or_foreign_snapshots_are_refused_untouched(m3, oracle, libs):
+    ours, ref = libs
+    r = oracle.RefWorld.scene(SCENE_UNEVEN, 3, 48)
+    r.step(1.0 / 60.0, 4, 10)
+    snap = _snapshot(ref, r.id)
+    g = m3.World.scene(SCENE_UNEVEN, 4, 48)
+    before = g.hash()
+    bad_magic = b"X" + snap[1:]
+    assert not _restore(ours, g.id, bad_magic)
+    assert not _restore(ours, g.id, snap[:-1])
+    assert not _restore(ours, g.id, snap + b"\0")
+    # A flipped pool cursor (body maxIndex beyond capacity).
+    cur = bytearray(snap)
+    cur[28:32] = (10 ** 6).to_bytes(4, "little")
+    assert not _restore(ours, g.id, bytes(cur))
+    assert m3.last_error()[0] == m3.M3GPU_ERR_INVALID
+    assert g.hash() == before
+    # A world of other capacities.
+    other = m3.World.scene(SCENE_UNEVEN, 3, 64)
+    assert not _restore(ours, other.id, snap)
+    # The same bytes restore fine into the right world.
+    assert _restore(ours, g.id, snap)
+    assert g.hash() == r.hash()
+
+
+class _WaterVolumeDef(C.Structure):
+    # world.h:107-116 of the reference.
+    _fields_ = [("lo", abi.m3Pos3), ("hi", abi.m3Pos3), ("density", C.c_float),
+                ("linearDrag", C.c_float), ("angularDrag", C.c_float), ("flow", abi.m3Vec3),
+                ("internalValue", C.c_int32)]
+
+
+class _WaterVolumeId(C.Structure):
+    _fields_ = [("index1", C.c_int32), ("world0", C.c_uint16), ("generation", C.c_uint16)]
+
+
+def test_unmodelled_content_is_refused(m3, oracle, libs):
+    # A live water volume (a pool this path does not model) in the
+    # snapshot: refused as unsupported, the world untouched.
+    ours, ref = libs
+    lib = oracle.lib()
+    lib.m3DefaultWaterVolumeDef.restype = _WaterVolumeDef
+    lib.m3CreateWaterVolume.argtypes = [abi.m3WorldId, C.POINTER(_WaterVolumeDef)]
+    lib.m3CreateWaterVolume.restype = _WaterVolumeId
+    r = oracle.RefWorld.scene(SCENE_UNEVEN, 3, 48)
+    wd = lib.m3DefaultWaterVolumeDef()
+    wd.lo = abi.m3Pos3(-5.0, -1.0, -5.0)
+    wd.hi = abi.m3Pos3(5.0, 0.5, 5.0)
+    vol = lib.m3CreateWaterVolume(r.id, C.byref(wd))
+    assert vol.index1 > 0
+    snap = _snapshot(ref, r.id)
+    g = m3.World.scene(SCENE_UNEVEN, 3, 48)
+    before = g.hash()
+    assert not _restore(ours, g.id, snap)
+    assert m3.last_error()[0] == m3.M3GPU_ERR_UNSUPPORTED
+    assert g.hash() == before
+
+
+def test_body_commands_replay_like_the_reference(m3, oracle, libs):
+    ours, ref = libs
+    r = oracle.RefWorld.scene(SCENE_UNEVEN, 5, 64)
+    r.step(1.0 / 60.0, 4, 20)
+    snap = _snapshot(ref, r.id)
+    g = m3.World.scene(SCENE_UNEVEN, 5, 64)
+    assert _restore(ours, g.id, snap)
+    rng = np.random.default_rng(5)
+    journal = b""
+    ops = [abi.OP_APPLY_LINEAR_IMPULSE, abi.OP_APPLY_ANGULAR_IMPULSE, abi.OP_APPLY_FORCE,
+           abi.OP_APPLY_TORQUE, abi.OP_SET_LINEAR_VELOCITY, abi.OP_SET_ANGULAR_VELOCITY]
+    for k in range(40):
+        body = int(rng.integers(2, 60))
+        v = [float(x) for x in rng.uniform(-50, 50, 3).astype(np.float32)]
+        journal += abi.journal_body_command(ops[k % len(ops)], body, 0, v)
+    assert _replay(ref, r.id, journal)
+    assert _replay(ours, g.id, journal)
+    assert g.hash() == r.hash()
+    assert g.state().first_difference(r.state()) is None
+
+
+def test_bad_or_unsupported_journals_are_refused_untouched(m3, libs):
+    ours, _ = libs
+    g = m3.World.scene(SCENE_UNEVEN, 5, 64)
+    before = g.hash()
+    good = abi.journal_body_command(abi.OP_APPLY_LINEAR_IMPULSE, 3, 0, [1.0, 2.0, 3.0])
+    # Truncated, stale body, non-finite vector, unknown and unsupported ops.
+    assert not _replay(ours, g.id, good + good[:-1])
+    assert not _replay(ours, g.id, good + abi.journal_body_command(28, 9999, 0, [1, 1, 1]))
+    assert not _replay(ours, g.id, good + abi.journal_body_command(28, 3, 0, [float("nan"), 0, 0]))
+    assert not _replay(ours, g.id, good + abi.journal_step(0.0, 4))
+    assert not _replay(ours, g.id, good + abi.journal_step(1 / 60, 300))
+    unsupported = C.c_int32(32).value.to_bytes(4, "little") + (0).to_bytes(4, "little")
+    assert not _replay(ours, g.id, good + unsupported)
+    assert m3.last_error()[0] == m3.M3GPU_ERR_UNSUPPORTED
+    assert g.hash() == before
+    assert _replay(ours, g.id, good)
+    assert g.hash() != before
+
+
+@pytest.mark.parametrize("scene,seed,param", [
+    (SCENE_BOX_PYRAMID, 0, 20),
+    (SCENE_UNEVEN, 1, 32),
+    (SCENE_UNEVEN, 7, 600),
+    (SCENE_TOWERS, 7, 4),
+])
+def test_snapshot_of_a_new_world_is_the_references_bytes(m3, oracle, libs, scene, seed, param):
+    # Every block, the broadphase tree built by the creation inserts
+    # (dynamic_tree.c:221-322) and the id pools included.
+    ours, ref = libs
+    r = oracle.RefWorld.scene(scene, seed, param)
+    g = m3.World.scene(scene, seed, param)
+    assert ours.m3World_SnapshotSize(g.id) == ref.m3World_SnapshotSize(r.id)
+    assert _snapshot(ours, g.id) == _snapshot(ref, r.id)
+
+
+@pytest.mark.parametrize("scene,seed,param,steps", [
+    (SCENE_UNEVEN, 21, 64, 90),
+    (SCENE_TOWERS, 7, 4, 40),
+])
+def test_restored_world_snapshots_the_same_bytes(m3, oracle, libs, scene, seed, param, steps):
+    # Restore then snapshot gives back the input byte for byte, the state
+    # this path does not model included.
+    ours, ref = libs
+    r = oracle.RefWorld.scene(scene, seed, param)
+    r.step(1.0 / 60.0, 4, steps)
+    snap = _snapshot(ref, r.id)
+    g = m3.World.scene(scene, seed, param)
+    assert _restore(ours, g.id, snap)
+    assert _snapshot(ours, g.id) == snap
+    small = (C.c_uint8 * 16)()
+    assert ours.m3World_Snapshot(g.id, small, 16) == -1
