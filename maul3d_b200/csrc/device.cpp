@@ -204,6 +204,15 @@ int32_t m3gpuReserve(m3HostWorld* w)
     {
         w->dslab = nullptr;
     }
+    // Both pair buffers start as the host's do at creation: zero (the
+    // step keeps their parts past the live list equal to the reference's
+    // single array, which starts zeroed).
+    if (rc == M3GPU_OK)
+    {
+        const int64_t pairs = Offset(w, w->hv.keys0);
+        rc = CudaCheck(cudaMemsetAsync(w->dslab + pairs, 0, (size_t)(w->persistentBytes - pairs), 0),
+                       "clear pair buffers");
+    }
     // Page-lock the host memory of the images (chunk by chunk, see
     // hostmem.cpp), so uploads are DMA copies straight from it.
     if (rc == M3GPU_OK)
@@ -245,6 +254,13 @@ static int32_t UploadPrepare(m3HostWorld* w)
         if (rc != M3GPU_OK)
         {
             w->dslab = nullptr;
+            return rc;
+        }
+        const int64_t pairs = Offset(w, w->hv.keys0);
+        rc = CudaCheck(cudaMemsetAsync(w->dslab + pairs, 0, (size_t)(w->persistentBytes - pairs), 0),
+                       "clear pair buffers");
+        if (rc != M3GPU_OK)
+        {
             return rc;
         }
     }
@@ -306,8 +322,41 @@ static int32_t UploadCopies(m3HostWorld* w)
                        "upload world image");
     }
     int64_t bytes = head;
-    const int32_t n = w->hv.sc->pairCount;
-    if (rc == M3GPU_OK && n > 0)
+    const int32_t n = w->pairTailsToDevice ? w->pairCap : w->hv.sc->pairCount;
+    if (rc == M3GPU_OK && w->pairTailsToDevice)
+    {
+        // A restore set the whole arrays: both device buffers take the
+        // host's current one.
+        const int32_t buf = w->hv.sc->pairBuf;
+        const size_t kb = (size_t)w->pairCap * sizeof(uint64_t);
+        const size_t mb = (size_t)w->pairCap * sizeof(m3Manifold);
+        rc = CudaCheck(cudaMemcpy(w->dv.keys0, buf == 0 ? w->hv.keys0 : w->hv.keys1, kb,
+                                  cudaMemcpyHostToDevice),
+                       "upload pair arrays");
+        if (rc == M3GPU_OK)
+        {
+            rc = CudaCheck(cudaMemcpy(w->dv.man0, buf == 0 ? w->hv.man0 : w->hv.man1, mb,
+                                      cudaMemcpyHostToDevice),
+                           "upload pair arrays");
+        }
+        if (rc == M3GPU_OK)
+        {
+            rc = CudaCheck(cudaMemcpy(w->dv.keys1, w->dv.keys0, kb, cudaMemcpyDeviceToDevice),
+                           "copy pair arrays");
+        }
+        if (rc == M3GPU_OK)
+        {
+            rc = CudaCheck(cudaMemcpy(w->dv.man1, w->dv.man0, mb, cudaMemcpyDeviceToDevice),
+                           "copy pair arrays");
+        }
+        bytes += (int64_t)(kb + mb);
+        if (rc == M3GPU_OK)
+        {
+            w->pairTailsToDevice = false;
+            w->pairTailsOnDevice = false;
+        }
+    }
+    else if (rc == M3GPU_OK && n > 0)
     {
         const int32_t buf = w->hv.sc->pairBuf;
         rc = CudaCheck(cudaMemcpy(buf == 0 ? w->dv.keys0 : w->dv.keys1,
@@ -382,6 +431,15 @@ int32_t m3gpuUploadBatch(m3HostWorld** worlds, int32_t count)
         const uint64_t* hk = buf == 0 ? w->hv.keys0 : w->hv.keys1;
         const m3Manifold* hm = buf == 0 ? w->hv.man0 : w->hv.man1;
         const int32_t hullCount = (int32_t)w->hulls.size();
+        if (w->pairTailsToDevice)
+        {
+            rc = UploadCopies(w);
+            if (rc != M3GPU_OK)
+            {
+                return rc;
+            }
+            continue;
+        }
         const uint8_t* srcHead = m3HostDevicePointer(w->image.data(), (size_t)head);
         const uint8_t* srcKeys = n > 0 ? m3HostDevicePointer(hk, (size_t)n * sizeof(uint64_t)) : nullptr;
         const uint8_t* srcMan = n > 0 ? m3HostDevicePointer(hm, (size_t)n * sizeof(m3Manifold)) : nullptr;
@@ -515,6 +573,32 @@ int32_t m3gpuDownload(m3HostWorld* w)
     {
         w->deviceAhead = false;
         m3DrainBrokenJoints(w);
+    }
+    return rc;
+}
+
+int32_t m3gpuDownloadPairTails(m3HostWorld* w)
+{
+    if (w->dslab == nullptr || !w->pairTailsOnDevice)
+    {
+        return M3GPU_OK;
+    }
+    const int32_t buf = w->hv.sc->pairBuf;
+    int32_t rc = CudaCheck(cudaMemcpy(buf == 0 ? w->hv.keys0 : w->hv.keys1,
+                                      buf == 0 ? w->dv.keys0 : w->dv.keys1,
+                                      (size_t)w->pairCap * sizeof(uint64_t),
+                                      cudaMemcpyDeviceToHost),
+                           "download pair arrays");
+    if (rc == M3GPU_OK)
+    {
+        rc = CudaCheck(cudaMemcpy(buf == 0 ? w->hv.man0 : w->hv.man1,
+                                  buf == 0 ? w->dv.man0 : w->dv.man1,
+                                  (size_t)w->pairCap * sizeof(m3Manifold), cudaMemcpyDeviceToHost),
+                       "download pair arrays");
+    }
+    if (rc == M3GPU_OK)
+    {
+        w->pairTailsOnDevice = false;
     }
     return rc;
 }

@@ -196,11 +196,12 @@ M3_HD int32_t m3TreeRotate(m3TreeRef t, int32_t a)
 }
 
 // Walks from `index` to the root, rebalancing and refitting heights and
-// bounds (dynamic_tree.c:205-219).
+// bounds (dynamic_tree.c:205-219).  A walk longer than the node count
+// can only come from a malformed tree; it stops there.
 M3_HD void m3TreeRefit(m3TreeRef t, int32_t index)
 {
     m3TreeNode* nodes = t.nodes;
-    while (index != M3_TREE_NULL)
+    for (int32_t guard = 0; index != M3_TREE_NULL && guard < t.capacity; ++guard)
     {
         index = m3TreeRotate(t, index);
         m3TreeNode* n = nodes + index;
@@ -251,25 +252,44 @@ M3_HD int32_t m3TreeInsert(m3TreeRef t, const double lo[3], const double hi[3], 
         *t.root = leaf;
         return leaf;
     }
-    // Descend while a child is cheaper than pairing here.
+    // Descend while a child is cheaper than pairing here (at most one
+    // level per node: a longer descent means a malformed tree).  The
+    // chosen child's record is carried down, so each level loads only
+    // the two children.
     int32_t index = *t.root;
-    while (nodes[index].height > 0)
+    m3TreeNode cur = nodes[index];
+    for (int32_t guard = 0; cur.height > 0; ++guard)
     {
+        if (guard >= t.capacity)
+        {
+            return M3_TREE_NULL;
+        }
+        const int32_t c1 = cur.child1;
+        const int32_t c2 = cur.child2;
+        const m3TreeNode n1 = nodes[c1];
+        const m3TreeNode n2 = nodes[c2];
         double ulo[3];
         double uhi[3];
-        m3TreeUnion(nodes[index].lo, nodes[index].hi, lo, hi, ulo, uhi);
+        m3TreeUnion(cur.lo, cur.hi, lo, hi, ulo, uhi);
         const double area = m3TreeArea(ulo, uhi);
         const double here = 2.0 * area;
-        const double inherited = 2.0 * (area - m3TreeArea(nodes[index].lo, nodes[index].hi));
-        const int32_t c1 = nodes[index].child1;
-        const int32_t c2 = nodes[index].child2;
-        const double cost1 = m3TreeChildCost(nodes[c1], lo, hi, inherited);
-        const double cost2 = m3TreeChildCost(nodes[c2], lo, hi, inherited);
+        const double inherited = 2.0 * (area - m3TreeArea(cur.lo, cur.hi));
+        const double cost1 = m3TreeChildCost(n1, lo, hi, inherited);
+        const double cost2 = m3TreeChildCost(n2, lo, hi, inherited);
         if (here < cost1 && here < cost2)
         {
             break;
         }
-        index = cost1 < cost2 ? c1 : c2;
+        if (cost1 < cost2)
+        {
+            index = c1;
+            cur = n1;
+        }
+        else
+        {
+            index = c2;
+            cur = n2;
+        }
     }
     // A new parent takes the sibling's place; sibling and leaf hang
     // under it in that order.
@@ -407,5 +427,101 @@ M3_HD m3Aabb m3ShapeFreshBounds(const m3WorldView& w, int32_t shape)
     }
     return box;
 }
+
+#ifndef __CUDACC__
+#include <vector>
+
+// Structural check of a tree read from outside (a restored snapshot):
+// every link in range, parents and children agreeing, heights and
+// bounds as the tree keeps them, no node reached twice, the free chain
+// of free nodes only, together covering every node, and each live
+// non-plane shape's proxy a leaf naming it.  The device trusts a tree
+// that passed.
+static inline bool m3TreeValid(const m3TreeNode* nodes, int32_t capacity, int32_t root,
+                               int32_t freeList, const int32_t* proxyId, const uint8_t* alive,
+                               const uint8_t* type, int32_t shapeMax)
+{
+    std::vector<uint8_t> seen((size_t)capacity, 0);
+    int32_t reached = 0;
+    std::vector<int32_t> stack;
+    if (root != M3_TREE_NULL)
+    {
+        if (root < 0 || root >= capacity || nodes[root].parent != M3_TREE_NULL)
+        {
+            return false;
+        }
+        stack.push_back(root);
+    }
+    while (!stack.empty())
+    {
+        const int32_t i = stack.back();
+        stack.pop_back();
+        if (seen[(size_t)i] != 0)
+        {
+            return false;
+        }
+        seen[(size_t)i] = 1;
+        reached += 1;
+        const m3TreeNode& n = nodes[i];
+        if (n.height == 0)
+        {
+            if (n.userData < 0 || n.userData >= shapeMax || proxyId[n.userData] != i)
+            {
+                return false;
+            }
+            continue;
+        }
+        if (n.height < 0)
+        {
+            return false;
+        }
+        const int32_t c[2] = {n.child1, n.child2};
+        for (int32_t k = 0; k < 2; ++k)
+        {
+            if (c[k] < 0 || c[k] >= capacity || nodes[c[k]].parent != i)
+            {
+                return false;
+            }
+            stack.push_back(c[k]);
+        }
+        if (n.height != 1 + m3TreeMaxI(nodes[c[0]].height, nodes[c[1]].height))
+        {
+            return false;
+        }
+    }
+    for (int32_t i = freeList, guard = 0; i != M3_TREE_NULL; i = nodes[i].parent, ++guard)
+    {
+        if (i < 0 || i >= capacity || guard >= capacity || seen[(size_t)i] != 0 ||
+            nodes[i].height != -1)
+        {
+            return false;
+        }
+        seen[(size_t)i] = 1;
+        reached += 1;
+    }
+    if (reached != capacity)
+    {
+        return false;
+    }
+    for (int32_t s = 0; s < shapeMax; ++s)
+    {
+        const int32_t leaf = proxyId[s];
+        const bool wantsLeaf = alive[s] != 0 && type[s] != M3_SHAPE_PLANE;
+        if (leaf == M3_TREE_NULL)
+        {
+            if (wantsLeaf)
+            {
+                return false;
+            }
+            continue;
+        }
+        if (leaf < 0 || leaf >= capacity || nodes[leaf].height != 0 || nodes[leaf].userData != s)
+        {
+            return false;
+        }
+    }
+    return true;
+}
+#endif
 
 #endif // M3_TREE_H

@@ -156,6 +156,12 @@ struct m3HostWorld
     m3WorldView dv{};                // device view (device addresses)
     bool hostDirty = true;           // host image newer than device
     bool deviceAhead = false;        // device newer than host image
+    // The pair arrays past the live list are snapshot bytes (what longer
+    // lists of earlier steps left there).  A restore sets them on the
+    // host, and the next upload copies the whole current buffer; a step
+    // changes them on the device, and a snapshot downloads them.
+    bool pairTailsToDevice = false;
+    bool pairTailsOnDevice = false;
 };
 
 // Registry (world.cpp).
@@ -173,6 +179,8 @@ int32_t m3gpuUpload(m3HostWorld* w);
 // rest one world at a time.
 int32_t m3gpuUploadBatch(m3HostWorld** worlds, int32_t count);
 int32_t m3gpuDownload(m3HostWorld* w);
+// The current pair buffer in full, device to host (for a snapshot).
+int32_t m3gpuDownloadPairTails(m3HostWorld* w);
 void m3gpuRelease(m3HostWorld* w);
 // Make the host image current before a host read or write.
 int32_t m3gpuSyncHost(m3HostWorld* w);

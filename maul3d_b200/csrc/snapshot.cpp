@@ -220,6 +220,8 @@ struct PoolBlocks
     std::vector<int32_t> jointQueue;
     const uint8_t* shapeType = nullptr;
     const uint8_t* shapeAlive = nullptr;
+    const uint8_t* proxyId = nullptr;
+    const uint8_t* treeNodes = nullptr;
 
     void Size(const m3HostWorld* w)
     {
@@ -327,7 +329,9 @@ void WalkFixed(BlockWalk& b, const m3HostWorld* w, const m3WorldView& v, PoolBlo
 
     b.Keep(v.keys0, 8 * np);
     // The broadphase: proxy ids and tree nodes.
+    pb.proxyId = b.Here();
     b.Keep(v.proxyId, 4 * ns);
+    pb.treeNodes = b.Here();
     b.Keep(v.treeNodes, (int64_t)sizeof(m3TreeNode) * 2 * ns);
     b.Keep(v.hullIndex, 4 * ns);
     // Hull reference counts and pool.
@@ -523,7 +527,8 @@ extern "C" int32_t m3World_Snapshot(m3WorldId worldId, void* out, int32_t capaci
 {
     m3gpuClearError();
     m3HostWorld* w = m3gpuWorldFromId(worldId);
-    if (w == nullptr || out == nullptr || m3gpuSyncHost(w) != M3GPU_OK)
+    if (w == nullptr || out == nullptr || m3gpuSyncHost(w) != M3GPU_OK ||
+        m3gpuDownloadPairTails(w) != M3GPU_OK)
     {
         return -1;
     }
@@ -795,6 +800,21 @@ extern "C" bool m3World_Restore(m3WorldId worldId, const void* data, int32_t siz
                       unsupported);
         return false;
     }
+    {
+        // The broadphase tree must be well formed before the device
+        // walks it (copied out of the input: it may be unaligned).
+        const int32_t cap = 2 * w->shapeCap;
+        std::vector<m3TreeNode> nodes((size_t)cap);
+        std::vector<int32_t> proxy((size_t)w->shapeCap);
+        memcpy(nodes.data(), pb.treeNodes, sizeof(m3TreeNode) * (size_t)cap);
+        memcpy(proxy.data(), pb.proxyId, 4 * (size_t)w->shapeCap);
+        if (!m3TreeValid(nodes.data(), cap, hd.treeRoot, hd.treeFreeList, proxy.data(),
+                         pb.shapeAlive, pb.shapeType, hd.shapeMaxIndex))
+        {
+            m3gpuSetError(M3GPU_ERR_INVALID, "m3World_Restore: malformed broadphase tree");
+            return false;
+        }
+    }
 
     // Read pass.
     std::vector<uint8_t> carry;
@@ -856,9 +876,12 @@ extern "C" bool m3World_Restore(m3WorldId worldId, const void* data, int32_t siz
     {
         memcpy(&w->heightFieldCellCarry[(size_t)f], raw + heightFieldAt + 12LL * f + 8, 4);
     }
-    // The image on the host is now the world; the next step uploads it.
+    // The image on the host is now the world; the next step uploads it,
+    // the pair arrays in full.
     w->deviceAhead = false;
     w->hostDirty = true;
+    w->pairTailsToDevice = true;
+    w->pairTailsOnDevice = false;
     return true;
 }
 

@@ -37,6 +37,7 @@
 #include "m3_narrow.cuh"
 #include "m3_solver.cuh"
 #include "m3_joints.cuh"
+#include "m3_tree.h"
 
 #include <cuda_runtime.h>
 
@@ -48,6 +49,9 @@
 // parallel rounds before the serial finish.
 #define M3_COLOR_PENDING 0xFF
 #define M3_COLOR_ROUNDS 64
+// Steps the broadphase tree kernel may trail the step (the depth of the
+// ring of per-step move lists).
+#define M3_TREE_LAG 8
 
 // Step phases timed with the SM clock by thread 0 of each world's block
 // right after the barrier that closes the phase.
@@ -81,12 +85,6 @@ enum
 // ---------------------------------------------------------------------
 // Scratch layout (device only)
 // ---------------------------------------------------------------------
-struct m3Aabb
-{
-    double lo[3];
-    double hi[3];
-};
-
 // What the preparation kernel hands the substep and finish kernels.
 struct m3StepPlan
 {
@@ -138,6 +136,12 @@ struct m3Scratch
     int32_t* jointLevel;   // per joint row: dependency level
     int32_t* jointOrder;   // joint rows grouped by level
     int32_t* jointLevelStart; // level offsets into jointOrder
+    int32_t* treeMove;     // per shape: leaf-escape flags, then their scan
+    m3Aabb* leafBox;       // per shape: its tree leaf's bounds (kept by the broadphase)
+    int32_t* hasLeaf;      // per shape: whether it has a tree leaf
+    int32_t* treeMoveCount; // M3_TREE_LAG: moves of each step in the ring
+    int32_t* treeMoveShape; // M3_TREE_LAG x shapeCap: a step's moves (shapes, ascending)
+    m3Aabb* treeMoveBox;   // M3_TREE_LAG x shapeCap: the fat bounds they are inserted with
 };
 
 static __host__ __device__ inline int64_t NextPow2(int64_t n)
@@ -150,9 +154,12 @@ static __host__ __device__ inline int64_t NextPow2(int64_t n)
     return p;
 }
 
+// The ring of tree move lists comes last and is `treeLag` steps deep:
+// only the kernels that touch it need the depth the scratch was sized
+// with; for every other array the offsets do not depend on it.
 static __host__ __device__ inline int64_t ScratchCarve(m3Scratch* s, uint8_t* base, int32_t bodyCap,
                                                      int32_t shapeCap, int32_t jointCap,
-                                                     int32_t pairCap)
+                                                     int32_t pairCap, int32_t treeLag = 1)
 {
     int64_t off = 0;
 #define M3_CARVE(field, T, n)                                                                      \
@@ -204,6 +211,12 @@ static __host__ __device__ inline int64_t ScratchCarve(m3Scratch* s, uint8_t* ba
     M3_CARVE(jointLevel, int32_t, jointCap)
     M3_CARVE(jointOrder, int32_t, jointCap)
     M3_CARVE(jointLevelStart, int32_t, jointCap + 2)
+    M3_CARVE(treeMove, int32_t, shapeCap + 1)
+    M3_CARVE(leafBox, m3Aabb, shapeCap)
+    M3_CARVE(hasLeaf, int32_t, shapeCap)
+    M3_CARVE(treeMoveCount, int32_t, M3_TREE_LAG)
+    M3_CARVE(treeMoveBox, m3Aabb, (int64_t)treeLag * shapeCap)
+    M3_CARVE(treeMoveShape, int32_t, (int64_t)treeLag * shapeCap)
 #undef M3_CARVE
     return off;
 }
@@ -211,7 +224,7 @@ static __host__ __device__ inline int64_t ScratchCarve(m3Scratch* s, uint8_t* ba
 extern "C" int64_t m3gpuScratchBytes(int32_t bodyCap, int32_t shapeCap, int32_t jointCap,
                                      int32_t pairCap)
 {
-    return ScratchCarve(nullptr, nullptr, bodyCap, shapeCap, jointCap, pairCap);
+    return ScratchCarve(nullptr, nullptr, bodyCap, shapeCap, jointCap, pairCap, M3_TREE_LAG);
 }
 
 // ---------------------------------------------------------------------
@@ -290,63 +303,9 @@ template <int NT> __device__ int32_t BlockExclusiveScan(int32_t* a, int32_t n)
 // ---------------------------------------------------------------------
 
 // Fresh bounds of one shape, tight plus the margin (broad_phase.c:22-135).
-__device__ m3Aabb ShapeBounds(const m3WorldView& w, int32_t shape)
+__device__ __forceinline__ m3Aabb ShapeBounds(const m3WorldView& w, int32_t shape)
 {
-    m3Transform xf = m3ShapeXf(w, shape);
-    m3Aabb box;
-    uint8_t type = w.shapeType[shape];
-    if (type == M3_SHAPE_HULL)
-    {
-        const m3HullData* hull = &w.hulls[w.hullIndex[shape]];
-        for (int32_t k = 0; k < 3; ++k)
-        {
-            box.lo[k] = 1.0e30;
-            box.hi[k] = -1.0e30;
-        }
-        const int32_t nv = hull->vertexCount;
-        for (int32_t v = 0; v < nv; ++v)
-        {
-            m3Vec3 r = m3RotateVec3(xf.q, hull->vertices[v]);
-            double p[3] = {xf.p.x + (double)r.x, xf.p.y + (double)r.y, xf.p.z + (double)r.z};
-            for (int32_t k = 0; k < 3; ++k)
-            {
-                box.lo[k] = p[k] < box.lo[k] ? p[k] : box.lo[k];
-                box.hi[k] = p[k] > box.hi[k] ? p[k] : box.hi[k];
-            }
-        }
-        for (int32_t k = 0; k < 3; ++k)
-        {
-            box.lo[k] -= (double)M3_AABB_MARGIN;
-            box.hi[k] += (double)M3_AABB_MARGIN;
-        }
-        return box;
-    }
-    if (type == M3_SHAPE_CAPSULE)
-    {
-        m3Vec3 r1 = m3RotateVec3(xf.q, w.geom[shape].v);
-        m3Vec3 r2 = m3RotateVec3(xf.q, w.geom[shape].v2);
-        double c1[3] = {xf.p.x + (double)r1.x, xf.p.y + (double)r1.y, xf.p.z + (double)r1.z};
-        double c2[3] = {xf.p.x + (double)r2.x, xf.p.y + (double)r2.y, xf.p.z + (double)r2.z};
-        double fat = (double)(w.geom[shape].s + M3_AABB_MARGIN);
-        for (int32_t k = 0; k < 3; ++k)
-        {
-            box.lo[k] = (c1[k] < c2[k] ? c1[k] : c2[k]) - fat;
-            box.hi[k] = (c1[k] > c2[k] ? c1[k] : c2[k]) + fat;
-        }
-        return box;
-    }
-    m3Vec3 r = m3RotateVec3(xf.q, w.geom[shape].v);
-    double cx = xf.p.x + (double)r.x;
-    double cy = xf.p.y + (double)r.y;
-    double cz = xf.p.z + (double)r.z;
-    double fat = (double)(w.geom[shape].s + M3_AABB_MARGIN);
-    box.lo[0] = cx - fat;
-    box.lo[1] = cy - fat;
-    box.lo[2] = cz - fat;
-    box.hi[0] = cx + fat;
-    box.hi[1] = cy + fat;
-    box.hi[2] = cz + fat;
-    return box;
+    return m3ShapeFreshBounds(w, shape);
 }
 
 __device__ __forceinline__ bool Overlap(const m3Aabb& a, const m3Aabb& b)
@@ -418,6 +377,100 @@ __device__ __forceinline__ uint64_t OrderKey(double x)
 
 #define M3_MAX_PLANES 16
 
+// The broadphase tree's leaves as the broadphase reads them: each
+// shape's leaf bounds, copied out of the tree once per batch; the
+// broadphase keeps the copy current as it moves leaves, so its
+// containment tests never wait for the tree kernel.
+__global__ void __launch_bounds__(M3_BLOCK) m3LeafBoxKernel(const m3WorldView* views,
+                                                           int32_t count)
+{
+    const m3WorldView& w = views[blockIdx.x];
+    const m3WorldScalars* sc = w.sc;
+    m3Scratch s;
+    ScratchCarve(&s, w.scratch, sc->bodyCap, sc->shapeCap, sc->jointCap, sc->pairCap);
+    const int32_t shapeMax = sc->shapeMax;
+    for (int32_t i = threadIdx.x; i < shapeMax; i += blockDim.x)
+    {
+        const int32_t leaf = w.proxyId[i];
+        s.hasLeaf[i] = leaf != M3_TREE_NULL ? 1 : 0;
+        if (leaf != M3_TREE_NULL)
+        {
+            const m3TreeNode& n = w.treeNodes[leaf];
+            m3Aabb b;
+            for (int32_t k = 0; k < 3; ++k)
+            {
+                b.lo[k] = n.lo[k];
+                b.hi[k] = n.hi[k];
+            }
+            s.leafBox[i] = b;
+        }
+    }
+}
+
+// Broadphase tree refresh, second half (broad_phase.c:516-538): one warp
+// per world replays one step's moves in ascending shape order, each a
+// leaf removal and the insertion of its fat bounds.  The tree is state
+// only a snapshot reads, so this runs on its own low-priority stream
+// beside the following steps, up to M3_TREE_LAG steps behind (the move
+// lists sit in a ring of that depth).
+#define M3_TREE_WORLDS_PER_BLOCK 4
+__global__ void __launch_bounds__(32 * M3_TREE_WORLDS_PER_BLOCK)
+    m3TreeKernel(const m3WorldView* views, const int32_t* order, int32_t count, int32_t slot,
+                 int32_t treeLag)
+{
+    const int32_t k = blockIdx.x * M3_TREE_WORLDS_PER_BLOCK + (int32_t)(threadIdx.x >> 5);
+    const int32_t lane = (int32_t)(threadIdx.x & 31);
+    if (k >= count)
+    {
+        return;
+    }
+    const m3WorldView& w = views[order[k]];
+    m3WorldScalars* sc = w.sc;
+    m3Scratch s;
+    ScratchCarve(&s, w.scratch, sc->bodyCap, sc->shapeCap, sc->jointCap, sc->pairCap, treeLag);
+    const m3TreeRef tree = m3WorldTree(w);
+    const int32_t moves = s.treeMoveCount[slot];
+    if (moves == 0)
+    {
+        return;
+    }
+    // The walk below is a chain of dependent loads: bring the world's
+    // nodes into L2 first, one bulk prefetch per 64 KiB piece (the array
+    // is 256-byte aligned and 144 bytes a shape, so every piece is a
+    // multiple of 16 bytes).
+    {
+        const int64_t bytes = (int64_t)sizeof(m3TreeNode) * 2 * sc->shapeCap;
+        const uint8_t* base = (const uint8_t*)w.treeNodes;
+        for (int64_t off = (int64_t)lane << 16; off < bytes; off += (int64_t)32 << 16)
+        {
+            const int64_t left = bytes - off;
+            const uint32_t piece = (uint32_t)(left < 65536 ? left : 65536);
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(base + off), "r"(piece)
+                         : "memory");
+        }
+    }
+    if (lane != 0)
+    {
+        return;
+    }
+    const int32_t* shapes = s.treeMoveShape + (int64_t)slot * sc->shapeCap;
+    const m3Aabb* boxes = s.treeMoveBox + (int64_t)slot * sc->shapeCap;
+    for (int32_t m = 0; m < moves; ++m)
+    {
+        const int32_t shape = shapes[m];
+        const m3Aabb box = boxes[m];
+        m3TreeRemove(tree, w.proxyId[shape]);
+        const int32_t leaf = m3TreeInsert(tree, box.lo, box.hi, shape);
+        w.proxyId[shape] = leaf;
+        if (leaf == M3_TREE_NULL)
+        {
+            // The reference's pair update refuses with m3_errorCapacity.
+            atomicExch(&sc->status, M3GPU_ERR_CAPACITY);
+            return;
+        }
+    }
+}
+
 // Visit every non-plane pair (a < b) whose fresh bounds overlap and that
 // the filter allows, from the sweep position `p` of the sorted order.
 template <typename F>
@@ -448,13 +501,14 @@ __device__ __forceinline__ void SweepFrom(const m3WorldView& w, const m3Scratch&
 
 template <int NT, int MIN_BLOCKS>
 __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3BroadKernel(const m3WorldView* views,
-                                                          const int32_t* order, int32_t count)
+                                                          const int32_t* order, int32_t count,
+                                                          int32_t treeSlot, int32_t treeLag)
 {
     const int32_t wi = order[blockIdx.x];
     const m3WorldView& w = views[wi];
     m3WorldScalars* sc = w.sc;
     m3Scratch s;
-    ScratchCarve(&s, w.scratch, sc->bodyCap, sc->shapeCap, sc->jointCap, sc->pairCap);
+    ScratchCarve(&s, w.scratch, sc->bodyCap, sc->shapeCap, sc->jointCap, sc->pairCap, treeLag);
     const int32_t tid = threadIdx.x;
     __shared__ int32_t s_status;
     __shared__ int32_t s_planes[M3_MAX_PLANES];
@@ -507,6 +561,50 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3BroadKernel(const m3WorldVie
             sc->statusDetail = 5001;
         }
         return;
+    }
+    // Broadphase tree refresh, first half (broad_phase.c:500-539): the
+    // awake shapes whose fresh bounds left their leaf, ascending, with
+    // the fat bounds they are reinserted with.  A leaf moves only when
+    // its own shape is reinserted, so every containment test can run
+    // here at once; m3TreeKernel replays the moves in order.
+    for (int32_t i = tid; i < shapeMax; i += NT)
+    {
+        int32_t move = 0;
+        if (w.shapeAlive[i] != 0 && s.hasLeaf[i] != 0 && w.awake[w.shapeBody[i]] != 0)
+        {
+            const m3Aabb& leaf = s.leafBox[i];
+            const m3Aabb& b = s.aabb[i];
+            move = leaf.lo[0] <= b.lo[0] && leaf.lo[1] <= b.lo[1] && leaf.lo[2] <= b.lo[2] &&
+                           b.hi[0] <= leaf.hi[0] && b.hi[1] <= leaf.hi[1] && b.hi[2] <= leaf.hi[2]
+                       ? 0
+                       : 1;
+        }
+        s.treeMove[i] = move;
+    }
+    __syncthreads();
+    const int32_t treeMoves = BlockExclusiveScan<NT>(s.treeMove, shapeMax);
+    int32_t* moveShape = s.treeMoveShape + (int64_t)treeSlot * sc->shapeCap;
+    m3Aabb* moveBox = s.treeMoveBox + (int64_t)treeSlot * sc->shapeCap;
+    for (int32_t i = tid; i < shapeMax; i += NT)
+    {
+        const int32_t at = s.treeMove[i];
+        const int32_t next = i + 1 < shapeMax ? s.treeMove[i + 1] : treeMoves;
+        if (next != at)
+        {
+            m3Aabb fat = s.aabb[i];
+            for (int32_t k = 0; k < 3; ++k)
+            {
+                fat.lo[k] -= (double)M3_AABB_MARGIN;
+                fat.hi[k] += (double)M3_AABB_MARGIN;
+            }
+            moveShape[at] = i;
+            moveBox[at] = fat;
+            s.leafBox[i] = fat;
+        }
+    }
+    if (tid == 0)
+    {
+        s.treeMoveCount[treeSlot] = treeMoves;
     }
     M3_PHASE_MARK(M3_PHASE_BOUNDS)
     const int32_t n = s_sweepCount;
@@ -605,6 +703,22 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3BroadKernel(const m3WorldVie
     }
     const int32_t cur = sc->pairBuf;
     uint64_t* newKeys = cur == 0 ? w.keys1 : w.keys0;
+    {
+        // The reference keeps one pair array: past the new list it still
+        // holds what longer lists of earlier steps left there, and a
+        // snapshot carries those bytes.  The old buffer agrees with it
+        // past the old list and holds the old list itself, so the new
+        // buffer takes [total, old count) from it.
+        const int32_t oldCount = sc->pairCount;
+        const uint64_t* oldKeys = cur == 0 ? w.keys0 : w.keys1;
+        const m3Manifold* oldMan = cur == 0 ? w.man0 : w.man1;
+        m3Manifold* newMan = cur == 0 ? w.man1 : w.man0;
+        for (int32_t i = total + tid; i < oldCount; i += NT)
+        {
+            newKeys[i] = oldKeys[i];
+            newMan[i] = oldMan[i];
+        }
+    }
 
     M3_PHASE_MARK(M3_PHASE_COUNT)
     // Fill rows: sweep pairs through per-row cursors, then each plane's
@@ -2460,6 +2574,11 @@ struct m3ClassStreams
     cudaStream_t stream[M3_CLASSES] = {};
     cudaEvent_t fork = nullptr;
     cudaEvent_t join[M3_CLASSES] = {};
+    // The broadphase tree's stream and its per-step events: the
+    // broadphase of step k done, the tree kernel of step k done.
+    cudaStream_t tree = nullptr;
+    std::vector<cudaEvent_t> broadDone;
+    std::vector<cudaEvent_t> treeDone;
 };
 static m3ClassStreams s_classStreams;
 
@@ -2480,11 +2599,41 @@ static int32_t EnsureClassStreams()
             e = cudaEventCreateWithFlags(&s_classStreams.join[c], cudaEventDisableTiming);
         }
     }
+    if (e == cudaSuccess)
+    {
+        // The lowest priority: the step's own kernels take free SMs first.
+        int least = 0;
+        int greatest = 0;
+        cudaDeviceGetStreamPriorityRange(&least, &greatest);
+        e = cudaStreamCreateWithPriority(&s_classStreams.tree, cudaStreamNonBlocking, least);
+    }
     if (e != cudaSuccess)
     {
         return m3gpuSetError(M3GPU_ERR_CUDA, "class streams: %s", cudaGetErrorString(e));
     }
     s_classStreams.device = device;
+    return M3GPU_OK;
+}
+
+// Events for `steps` steps of the tree pipeline.
+static int32_t EnsureTreeEvents(int32_t steps)
+{
+    while ((int32_t)s_classStreams.treeDone.size() < steps)
+    {
+        cudaEvent_t a = nullptr;
+        cudaEvent_t b = nullptr;
+        cudaError_t e = cudaEventCreateWithFlags(&a, cudaEventDisableTiming);
+        if (e == cudaSuccess)
+        {
+            e = cudaEventCreateWithFlags(&b, cudaEventDisableTiming);
+        }
+        if (e != cudaSuccess)
+        {
+            return m3gpuSetError(M3GPU_ERR_CUDA, "tree events: %s", cudaGetErrorString(e));
+        }
+        s_classStreams.broadDone.push_back(a);
+        s_classStreams.treeDone.push_back(b);
+    }
     return M3GPU_OK;
 }
 
@@ -2863,19 +3012,47 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
             return rc;
         }
     }
+    rc = EnsureTreeEvents(steps);
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
     cudaEventRecord(s_events[0]);
+    // The broadphase tree: the leaves' bounds once per batch, then per
+    // step the tree kernel on its own stream, at most M3_TREE_LAG steps
+    // behind (the move lists sit in a ring of that depth).
+    m3LeafBoxKernel<<<count, M3_BLOCK>>>(s_batch.dviews, count);
+    const cudaStream_t treeStream = s_classStreams.tree;
     for (int32_t step = 0; step < steps; ++step)
     {
         const cudaEvent_t* ev = &s_events[(size_t)(M3_STAGES * step)];
-        m3BroadKernel<M3_BLOCK, 2><<<count, M3_BLOCK>>>(s_batch.dviews, s_batch.dorder, count);
+        if (step >= M3_TREE_LAG)
+        {
+            cudaStreamWaitEvent(0, s_classStreams.treeDone[(size_t)(step - M3_TREE_LAG)], 0);
+        }
+        m3BroadKernel<M3_BLOCK, 2><<<count, M3_BLOCK>>>(s_batch.dviews, s_batch.dorder, count,
+                                                        step % M3_TREE_LAG, M3_TREE_LAG);
+        cudaEventRecord(s_classStreams.broadDone[(size_t)step], 0);
+        cudaStreamWaitEvent(treeStream, s_classStreams.broadDone[(size_t)step], 0);
+        m3TreeKernel<<<(count + M3_TREE_WORLDS_PER_BLOCK - 1) / M3_TREE_WORLDS_PER_BLOCK,
+                       32 * M3_TREE_WORLDS_PER_BLOCK, 0, treeStream>>>(
+            s_batch.dviews, s_batch.dorder, count, step % M3_TREE_LAG, M3_TREE_LAG);
+        cudaEventRecord(s_classStreams.treeDone[(size_t)step], treeStream);
         m3PairOffsetsKernel<<<1, M3_BLOCK>>>(s_batch.dviews, count, s_batch.doffsets);
         LaunchNarrow(s_batch.dviews, s_batch.doffsets, count);
         cudaEventRecord(ev[1]);
         LaunchSolve(s_batch.dviews, s_batch.dorder, count, dt, substeps, s_batch.cacheBytes,
                     ev + 2, s_batch.classFirst, s_batch.classCache);
         cudaEventRecord(ev[4]);
-        s_launches += 5 + M3_NARROW_LAUNCHES;
+        s_launches += 6 + M3_NARROW_LAUNCHES;
     }
+    if (steps > 0)
+    {
+        // Everything after the batch (status, readbacks, snapshots) sees
+        // the finished tree.
+        cudaStreamWaitEvent(0, s_classStreams.treeDone[(size_t)(steps - 1)], 0);
+    }
+    s_launches += 1;
     cudaMemsetAsync(s_dstatus, 0, sizeof(int32_t));
     m3StatusKernel<<<(count + 255) / 256, 256>>>(s_batch.dviews, count, s_dstatus);
     s_launches += 1;
@@ -2889,6 +3066,7 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
     for (int32_t i = 0; i < count; ++i)
     {
         worlds[i]->deviceAhead = true;
+        worlds[i]->pairTailsOnDevice = true;
     }
     if (rc != M3GPU_OK)
     {
@@ -3048,7 +3226,9 @@ extern "C" int32_t m3gpu_step_world_noalloc(m3WorldId worldId, float dt, int32_t
                              "world is not resident on the device: reserve and upload it first "
                              "(m3gpu_reserve_worlds, m3gpu_upload_worlds)");
     }
-    const int64_t need = m3gpuScratchBytes(w->bodyCap, w->shapeCap, w->jointCap, w->pairCap);
+    // One slot of tree moves: this path runs the tree kernel in order.
+    const int64_t need =
+        ScratchCarve(nullptr, nullptr, w->bodyCap, w->shapeCap, w->jointCap, w->pairCap, 1);
     const int64_t cache = (int64_t)w->hv.sc->bodyMax * M3_BODY_CACHE_BYTES;
     if (need > M3_NOALLOC_SCRATCH_BYTES || cache > 48 * 1024)
     {
@@ -3089,11 +3269,13 @@ extern "C" int32_t m3gpu_step_world_noalloc(m3WorldId worldId, float dt, int32_t
     int32_t* order = sym.table;
     int32_t* offsets = sym.table + 1;
     const int32_t cacheBytes = (int32_t)cache;
-    m3BroadKernel<M3_BLOCK, 1><<<1, M3_BLOCK>>>(sym.view, order, 1);
+    m3LeafBoxKernel<<<1, M3_BLOCK>>>(sym.view, 1);
+    m3BroadKernel<M3_BLOCK, 1><<<1, M3_BLOCK>>>(sym.view, order, 1, 0, 1);
+    m3TreeKernel<<<1, 32 * M3_TREE_WORLDS_PER_BLOCK>>>(sym.view, order, 1, 0, 1);
     m3PairOffsetsKernel<<<1, M3_BLOCK>>>(sym.view, 1, offsets);
     m3NarrowKernel<<<148, 128>>>(sym.view, offsets, 1);
     LaunchSolve(sym.view, order, 1, dt, substeps, cacheBytes, nullptr);
-    s_launches += 6;
+    s_launches += 8;
     rc = Check(cudaGetLastError(), "noalloc step launch");
     int32_t status = 0;
     if (rc == M3GPU_OK)
@@ -3102,6 +3284,7 @@ extern "C" int32_t m3gpu_step_world_noalloc(m3WorldId worldId, float dt, int32_t
                    "noalloc step");
     }
     w->deviceAhead = true;
+    w->pairTailsOnDevice = true;
     if (rc != M3GPU_OK)
     {
         return rc;
