@@ -261,6 +261,71 @@ def run_reference_arm(args) -> None:
     print(json.dumps(line))
 
 
+def serving_run(m3, requests: int, seed: int, rates: list[float]) -> dict:
+    """Serving: replay containers (a snapshot of a world of 200-5000
+    bodies plus a journal of 4-16 frames, each frame 1-8 linear impulses
+    of 1-50 N s and one step of 1/60 s in 4 substeps) arrive as a Poisson
+    process; one server on this GPU batches every active request's frame
+    per tick.  Latency is arrival to final hash; the saturated run
+    submits everything at once."""
+    from maul3d_b200 import abi
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(200), np.log(5000), requests)).astype(int)
+    worlds = [m3.World.scene(abi.SCENE_UNEVEN, seed + i, int(n)) for i, n in enumerate(sizes)]
+    m3.step_worlds(worlds, DT, 4, 5)  # in motion, with contacts and warm starts
+    containers, work = [], []
+    for w, n in zip(worlds, sizes):
+        bodies = w.body_count()
+        frames = int(rng.integers(4, 17))
+        journal = b""
+        for _ in range(frames):
+            for _ in range(int(rng.integers(1, 9))):
+                d = rng.normal(size=3)
+                d = d / np.linalg.norm(d) * rng.uniform(1.0, 50.0)
+                journal += abi.journal_body_command(abi.OP_APPLY_LINEAR_IMPULSE,
+                                                    int(rng.integers(2, bodies + 1)), 0,
+                                                    [float(x) for x in d.astype(np.float32)])
+            journal += abi.journal_step(DT, 4)
+        containers.append(abi.encode_container(m3.lib, m3.snapshot(w), journal))
+        work.append(int(n) * frames * 4)
+        w.destroy()
+    out = {"requests": requests, "bodies": "log-uniform [200, 5000]", "frames": "U{4..16}",
+           "impulses_per_frame": "U{1..8}, 1-50 N s", "runs": []}
+    for rate in rates:
+        server = m3.Server()
+        arrivals = (np.cumsum(rng.exponential(1.0 / rate, requests)) if rate > 0
+                    else np.zeros(requests))
+        latency = np.zeros(requests)
+        ticket_of = {}
+        submitted = 0
+        finished = 0
+        ticks = 0
+        t0 = time.perf_counter()
+        while finished < requests:
+            now = time.perf_counter() - t0
+            while submitted < requests and arrivals[submitted] <= now:
+                ticket_of[server.submit(containers[submitted])] = submitted
+                submitted += 1
+            if server.tick() == 0 and submitted < requests:
+                time.sleep(max(0.0, arrivals[submitted] - (time.perf_counter() - t0)))
+            ticks += 1
+            t, h, st = server.poll()
+            done_at = time.perf_counter() - t0
+            for k in range(len(t)):
+                i = ticket_of[int(t[k])]
+                latency[i] = done_at - arrivals[i]
+                finished += 1
+        wall = time.perf_counter() - t0
+        server.close()
+        out["runs"].append({
+            "arrival_rate_per_s": rate if rate > 0 else "all at once",
+            "p50_latency_ms": float(np.percentile(latency, 50) * 1e3),
+            "p99_latency_ms": float(np.percentile(latency, 99) * 1e3),
+            "requests_per_s": requests / wall,
+            "body_substeps_per_s": float(sum(work)) / wall, "ticks": ticks})
+    return out
+
+
 def config_block(args, **extra) -> dict:
     cfg = {"workload": f"batched uneven worlds: {args.worlds} worlds per GPU, dynamic bodies "
                        f"log-uniform [{args.lo}, {args.hi}], box stacks + spheres + 3 revolute "
@@ -291,6 +356,7 @@ def main() -> None:
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--serving-requests", type=int, default=256)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -469,6 +535,10 @@ def main() -> None:
                              f"{args.warmup + args.steps} steps each, {threads} host threads; "
                              f"every sampled world's final hash compared with the device's"}
 
+    serving = None
+    if args.serving_requests > 0:
+        serving = serving_run(m3, args.serving_requests, rank_seed + 77, [400.0, 0.0])
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size,
@@ -478,7 +548,7 @@ def main() -> None:
             "config": config_block(args, total_dynamic_bodies_per_gpu=int(sum(sizes))),
             "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
             "cpu_baseline": cpu, "plain_gpu": plain, "bit_exact_check": verified,
-            "hash_ms": hash_ms, "clocks": clocks,
+            "hash_ms": hash_ms, "clocks": clocks, "serving": serving,
         }
         print(json.dumps(line))
     if world_size > 1:

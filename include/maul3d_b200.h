@@ -297,6 +297,25 @@ M3GPU_API bool m3Joint_IsValid(m3JointId jointId);
 #define M3GPU_ERR_UNSUPPORTED 4  /* a feature the device path does not cover */
 #define M3GPU_ERR_NO_DEVICE 5    /* no CUDA device visible */
 
+/* replay.h:28-62 (replay.c): the M3J1 replay container, a snapshot and
+ * the journal recorded after it.  Pure memory codecs, same layout,
+ * validation and refusals as the reference's. */
+typedef struct m3JournalInfo { int32_t opCount; int32_t stepCount; } m3JournalInfo;
+typedef struct m3ReplayView {
+    const void* snapshot;
+    int32_t snapshotBytes;
+    const void* journal;
+    int32_t journalBytes;
+    uint64_t finalHash;
+    m3JournalInfo info;
+} m3ReplayView;
+M3GPU_API bool m3JournalDescribe(const void* journal, int32_t bytes, m3JournalInfo* out);
+M3GPU_API int32_t m3ReplayEncodeSize(int32_t snapshotBytes, int32_t journalBytes);
+M3GPU_API int32_t m3ReplayEncode(const void* snapshot, int32_t snapshotBytes, const void* journal,
+                                 int32_t journalBytes, uint64_t finalHash, void* out,
+                                 int32_t capacity);
+M3GPU_API bool m3ReplayDecode(const void* data, int32_t bytes, m3ReplayView* out);
+
 /* Last error raised on the calling thread's most recent m3gpu or drop-in
  * call, and a one-line message for it (never NULL). */
 M3GPU_API int32_t m3gpu_last_error(void);
@@ -395,6 +414,31 @@ M3GPU_API int32_t m3gpu_copy_pairs(m3WorldId world, uint64_t* keys, void* manifo
                                    int32_t cap);
 M3GPU_API int32_t m3gpu_copy_joints(m3WorldId world, void* impulse, void* perp, void* limit,
                                     void* angular, int32_t cap);
+
+/* Serving: replay containers in, final world hashes out.  A server
+ * admits queued requests while their device memory fits `deviceBudget`
+ * bytes (and at most `maxActive` at once): each is restored into a fresh
+ * world and its journal validated whole.  Every m3gpu_serve_tick then
+ * advances every active request by one frame (its body commands and the
+ * step that closes them) in one batched launch sequence, and retires the
+ * requests whose journal is done with the world hash the reference's
+ * m3World_Restore + m3World_JournalReplay would give.  A request's result
+ * does not depend on the others in the batch. */
+typedef struct m3gpuServer m3gpuServer;
+M3GPU_API m3gpuServer* m3gpu_serve_create(int64_t deviceBudget, int32_t maxActive);
+M3GPU_API void m3gpu_serve_destroy(m3gpuServer* server);
+/* Queues a container; returns its ticket (> 0), or -1 for bytes that are
+ * not a valid container. */
+M3GPU_API int64_t m3gpu_serve_submit(m3gpuServer* server, const void* container, int32_t bytes);
+/* Admits, runs one frame, retires; returns the requests still queued or
+ * active, or a negative error code. */
+M3GPU_API int32_t m3gpu_serve_tick(m3gpuServer* server);
+/* Drains up to `capacity` finished requests: ticket, final hash, status
+ * (M3GPU_OK, or the refusal: an invalid snapshot or journal, content
+ * the device path does not model). */
+M3GPU_API int32_t m3gpu_serve_poll(m3gpuServer* server, int64_t* tickets, uint64_t* hashes,
+                                   int32_t* status, int32_t capacity);
+M3GPU_API int32_t m3gpu_serve_active(const m3gpuServer* server);
 
 #ifdef __cplusplus
 }

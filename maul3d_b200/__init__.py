@@ -58,6 +58,20 @@ def _load() -> C.CDLL:
         fn.restype = C.c_int32
     lib.m3gpu_copy_mass.argtypes = [m3WorldId] + [C.c_void_p] * 6 + [C.c_int32]
     lib.m3gpu_copy_mass.restype = C.c_int32
+    abi.bind_snapshot(lib)
+    abi.bind_replay(lib)
+    lib.m3gpu_serve_create.argtypes = [C.c_int64, C.c_int32]
+    lib.m3gpu_serve_create.restype = C.c_void_p
+    lib.m3gpu_serve_destroy.argtypes = [C.c_void_p]
+    lib.m3gpu_serve_destroy.restype = None
+    lib.m3gpu_serve_submit.argtypes = [C.c_void_p, C.c_void_p, C.c_int32]
+    lib.m3gpu_serve_submit.restype = C.c_int64
+    lib.m3gpu_serve_tick.argtypes = [C.c_void_p]
+    lib.m3gpu_serve_tick.restype = C.c_int32
+    lib.m3gpu_serve_poll.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]
+    lib.m3gpu_serve_poll.restype = C.c_int32
+    lib.m3gpu_serve_active.argtypes = [C.c_void_p]
+    lib.m3gpu_serve_active.restype = C.c_int32
     lib.m3gpu_set_device.argtypes = [C.c_int32]
     lib.m3gpu_set_device.restype = C.c_int32
     for name in ("m3gpu_reserve_worlds", "m3gpu_upload_worlds"):
@@ -256,3 +270,69 @@ def world_stats(world) -> np.ndarray:
     out = (C.c_uint64 * 6)()
     _check(lib.m3gpu_world_stats(world.id, out))
     return np.array(list(out), dtype=np.uint64)
+
+
+class Server:
+    """Batched serving of replay containers (snapshot + journal): submit,
+    tick until idle, poll the final hashes (m3gpu_serve_*)."""
+
+    def __init__(self, device_budget: int = 64 << 30, max_active: int = 4096):
+        self.handle = lib.m3gpu_serve_create(device_budget, max_active)
+        if not self.handle:
+            raise M3GpuError(*last_error())
+
+    def submit(self, container: bytes) -> int:
+        buf = (C.c_uint8 * len(container)).from_buffer_copy(container)
+        ticket = int(lib.m3gpu_serve_submit(self.handle, buf, len(container)))
+        if ticket < 0:
+            raise M3GpuError(*last_error())
+        return ticket
+
+    def tick(self) -> int:
+        """One frame for every active request; returns queued + active."""
+        n = int(lib.m3gpu_serve_tick(self.handle))
+        if n < 0:
+            raise M3GpuError(-n, last_error()[1])
+        return n
+
+    def active(self) -> int:
+        return int(lib.m3gpu_serve_active(self.handle))
+
+    def poll(self, capacity: int = 4096):
+        """Finished requests: arrays of tickets, hashes and statuses."""
+        t = np.zeros(capacity, np.int64)
+        h = np.zeros(capacity, np.uint64)
+        st = np.zeros(capacity, np.int32)
+        n = int(lib.m3gpu_serve_poll(self.handle, t.ctypes.data, h.ctypes.data, st.ctypes.data,
+                                     capacity))
+        return t[:n], h[:n], st[:n]
+
+    def run(self) -> dict[int, tuple[int, int]]:
+        """Tick until idle; {ticket: (hash, status)} of everything finished."""
+        out = {}
+        while True:
+            left = self.tick()
+            t, h, st = self.poll()
+            for k in range(len(t)):
+                out[int(t[k])] = (int(h[k]), int(st[k]))
+            if left == 0:
+                t, h, st = self.poll()
+                for k in range(len(t)):
+                    out[int(t[k])] = (int(h[k]), int(st[k]))
+                return out
+
+    def close(self) -> None:
+        if self.handle:
+            lib.m3gpu_serve_destroy(self.handle)
+            self.handle = None
+
+
+def snapshot(world) -> bytes:
+    """The world's snapshot bytes (m3World_Snapshot)."""
+    n = int(lib.m3World_SnapshotSize(world.id))
+    if n < 0:
+        raise M3GpuError(*last_error())
+    buf = (C.c_uint8 * n)()
+    if lib.m3World_Snapshot(world.id, buf, n) != n:
+        raise M3GpuError(*last_error())
+    return bytes(buf)

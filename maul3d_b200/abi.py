@@ -112,6 +112,39 @@ def bind_snapshot(lib: C.CDLL) -> C.CDLL:
     return lib
 
 
+class m3JournalInfo(C.Structure):
+    _fields_ = [("opCount", C.c_int32), ("stepCount", C.c_int32)]
+
+
+class m3ReplayView(C.Structure):
+    _fields_ = [("snapshot", C.c_void_p), ("snapshotBytes", C.c_int32), ("journal", C.c_void_p),
+                ("journalBytes", C.c_int32), ("finalHash", C.c_uint64), ("info", m3JournalInfo)]
+
+
+def bind_replay(lib: C.CDLL) -> C.CDLL:
+    """Declare the M3J1 container codecs (replay.h:34-62)."""
+    lib.m3JournalDescribe.argtypes = [C.c_void_p, C.c_int32, C.POINTER(m3JournalInfo)]
+    lib.m3JournalDescribe.restype = C.c_bool
+    lib.m3ReplayEncodeSize.argtypes = [C.c_int32, C.c_int32]
+    lib.m3ReplayEncodeSize.restype = C.c_int32
+    lib.m3ReplayEncode.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_uint64,
+                                   C.c_void_p, C.c_int32]
+    lib.m3ReplayEncode.restype = C.c_int32
+    lib.m3ReplayDecode.argtypes = [C.c_void_p, C.c_int32, C.POINTER(m3ReplayView)]
+    lib.m3ReplayDecode.restype = C.c_bool
+    return lib
+
+
+def encode_container(lib: C.CDLL, snapshot: bytes, journal: bytes, final_hash: int = 0) -> bytes:
+    """An M3J1 container through a library's m3ReplayEncode."""
+    n = lib.m3ReplayEncodeSize(len(snapshot), len(journal))
+    out = (C.c_uint8 * n)()
+    s = (C.c_uint8 * len(snapshot)).from_buffer_copy(snapshot)
+    j = (C.c_uint8 * max(len(journal), 1)).from_buffer_copy(journal or b"\0")
+    assert lib.m3ReplayEncode(s, len(snapshot), j, len(journal), final_hash, out, n) == n
+    return bytes(out)
+
+
 class WorldState:
     """Readback of one world's per-step state in the reference layouts."""
 

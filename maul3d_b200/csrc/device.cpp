@@ -327,26 +327,30 @@ static int32_t UploadCopies(m3HostWorld* w)
     {
         // A restore set the whole arrays: both device buffers take the
         // host's current one.
+        // Asynchronous on the default stream (ordered before any later
+        // kernel) when the image is page-locked, as the head copy above.
         const int32_t buf = w->hv.sc->pairBuf;
         const size_t kb = (size_t)w->pairCap * sizeof(uint64_t);
         const size_t mb = (size_t)w->pairCap * sizeof(m3Manifold);
-        rc = CudaCheck(cudaMemcpy(w->dv.keys0, buf == 0 ? w->hv.keys0 : w->hv.keys1, kb,
-                                  cudaMemcpyHostToDevice),
-                       "upload pair arrays");
+        const uint64_t* hk = buf == 0 ? w->hv.keys0 : w->hv.keys1;
+        const m3Manifold* hm = buf == 0 ? w->hv.man0 : w->hv.man1;
+        const bool locked = m3HostIsLocked(hk, kb) && m3HostIsLocked(hm, mb);
+        auto copy = [locked](void* dst, const void* src, size_t n, cudaMemcpyKind kind) {
+            return locked ? cudaMemcpyAsync(dst, src, n, kind, 0) : cudaMemcpy(dst, src, n, kind);
+        };
+        rc = CudaCheck(copy(w->dv.keys0, hk, kb, cudaMemcpyHostToDevice), "upload pair arrays");
         if (rc == M3GPU_OK)
         {
-            rc = CudaCheck(cudaMemcpy(w->dv.man0, buf == 0 ? w->hv.man0 : w->hv.man1, mb,
-                                      cudaMemcpyHostToDevice),
-                           "upload pair arrays");
+            rc = CudaCheck(copy(w->dv.man0, hm, mb, cudaMemcpyHostToDevice), "upload pair arrays");
         }
         if (rc == M3GPU_OK)
         {
-            rc = CudaCheck(cudaMemcpy(w->dv.keys1, w->dv.keys0, kb, cudaMemcpyDeviceToDevice),
+            rc = CudaCheck(cudaMemcpyAsync(w->dv.keys1, w->dv.keys0, kb, cudaMemcpyDeviceToDevice, 0),
                            "copy pair arrays");
         }
         if (rc == M3GPU_OK)
         {
-            rc = CudaCheck(cudaMemcpy(w->dv.man1, w->dv.man0, mb, cudaMemcpyDeviceToDevice),
+            rc = CudaCheck(cudaMemcpyAsync(w->dv.man1, w->dv.man0, mb, cudaMemcpyDeviceToDevice, 0),
                            "copy pair arrays");
         }
         bytes += (int64_t)(kb + mb);
@@ -575,6 +579,21 @@ int32_t m3gpuDownload(m3HostWorld* w)
         m3DrainBrokenJoints(w);
     }
     return rc;
+}
+
+int32_t m3gpuWorldStatus(m3HostWorld* w)
+{
+    if (w->dslab == nullptr || !w->deviceAhead)
+    {
+        return w->hv.sc->status;
+    }
+    int32_t status = 0;
+    if (CudaCheck(cudaMemcpy(&status, &w->dv.sc->status, sizeof(int32_t), cudaMemcpyDeviceToHost),
+                  "read status") != M3GPU_OK)
+    {
+        return M3GPU_ERR_CUDA;
+    }
+    return status;
 }
 
 int32_t m3gpuDownloadPairTails(m3HostWorld* w)

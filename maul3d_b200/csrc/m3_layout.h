@@ -61,7 +61,9 @@ typedef struct m3WorldScalars
     // The broadphase tree's root and free-list head (nodes: treeNodes).
     int32_t treeRoot;
     int32_t treeFreeList;
-    int32_t pad1;
+    // Whether the step keeps the broadphase tree (snapshot state).  Off
+    // only for worlds nobody can snapshot (the serving path's own).
+    int32_t treeTracked;
     // Work counters accumulated over every device step (observer only,
     // never hashed): the algorithmic-byte model of the roofline reads
     // them.  [0] movers x substeps, [1] contact rows x substeps,

@@ -83,39 +83,51 @@ M3_HD void m3TreeUnion(const double aLo[3], const double aHi[3], const double bL
     }
 }
 
-M3_HD int32_t m3TreeTakeNode(m3TreeRef t)
+// Node storage the tree operations go through, one whole record at a
+// time: the plain node array (host), or the array behind a cache in
+// shared memory (the device's tree kernel, m3TreeCachedStore).
+struct m3TreeArrayStore
+{
+    m3TreeNode* nodes;
+    M3_HD_MEMBER m3TreeNode Get(int32_t i) const { return nodes[i]; }
+    M3_HD_MEMBER void Put(int32_t i, const m3TreeNode& n) const { nodes[i] = n; }
+};
+
+template <class Store> M3_HD int32_t m3TreeTakeNode(m3TreeRef t, const Store& st)
 {
     const int32_t id = *t.freeList;
     if (id == M3_TREE_NULL)
     {
         return M3_TREE_NULL;
     }
-    m3TreeNode* n = t.nodes + id;
-    *t.freeList = n->parent;
-    n->parent = M3_TREE_NULL;
-    n->child1 = M3_TREE_NULL;
-    n->child2 = M3_TREE_NULL;
-    n->height = 0;
-    n->userData = -1;
-    n->pad = 0;
+    m3TreeNode n = st.Get(id);
+    *t.freeList = n.parent;
+    n.parent = M3_TREE_NULL;
+    n.child1 = M3_TREE_NULL;
+    n.child2 = M3_TREE_NULL;
+    n.height = 0;
+    n.userData = -1;
+    n.pad = 0;
+    st.Put(id, n);
     return id;
 }
 
 // A freed node is zeroed and pushed on the free chain (dynamic_tree.c:83-90).
-M3_HD void m3TreeGiveNode(m3TreeRef t, int32_t id)
+template <class Store> M3_HD void m3TreeGiveNode(m3TreeRef t, const Store& st, int32_t id)
 {
-    m3TreeNode* n = t.nodes + id;
+    m3TreeNode n;
     for (int32_t k = 0; k < 3; ++k)
     {
-        n->lo[k] = 0.0;
-        n->hi[k] = 0.0;
+        n.lo[k] = 0.0;
+        n.hi[k] = 0.0;
     }
-    n->child1 = 0;
-    n->child2 = 0;
-    n->userData = 0;
-    n->pad = 0;
-    n->parent = *t.freeList;
-    n->height = -1;
+    n.child1 = 0;
+    n.child2 = 0;
+    n.userData = 0;
+    n.pad = 0;
+    n.parent = *t.freeList;
+    n.height = -1;
+    st.Put(id, n);
     *t.freeList = id;
 }
 
@@ -125,18 +137,22 @@ M3_HD int32_t m3TreeMaxI(int32_t a, int32_t b)
 }
 
 // Re-links `child` under `parent` in place of `old` (or as the root).
-M3_HD void m3TreeReplaceChild(m3TreeRef t, int32_t parent, int32_t old, int32_t child)
+template <class Store>
+M3_HD void m3TreeReplaceChild(m3TreeRef t, const Store& st, int32_t parent, int32_t old,
+                              int32_t child)
 {
     if (parent != M3_TREE_NULL)
     {
-        if (t.nodes[parent].child1 == old)
+        m3TreeNode n = st.Get(parent);
+        if (n.child1 == old)
         {
-            t.nodes[parent].child1 = child;
+            n.child1 = child;
         }
         else
         {
-            t.nodes[parent].child2 = child;
+            n.child2 = child;
         }
+        st.Put(parent, n);
     }
     else
     {
@@ -148,16 +164,18 @@ M3_HD void m3TreeReplaceChild(m3TreeRef t, int32_t parent, int32_t old, int32_t 
 // than one: the taller child (p) rises, a becomes its child, and a keeps
 // the shorter of p's children while p keeps the taller one
 // (dynamic_tree.c:92-203).  Returns the subtree's new root.
-M3_HD int32_t m3TreeRotate(m3TreeRef t, int32_t a)
+template <class Store> M3_HD int32_t m3TreeRotate(m3TreeRef t, const Store& st, int32_t a)
 {
-    m3TreeNode* nodes = t.nodes;
-    if (nodes[a].height < 2 || nodes[a].child1 == M3_TREE_NULL)
+    m3TreeNode A = st.Get(a);
+    if (A.height < 2 || A.child1 == M3_TREE_NULL)
     {
         return a;
     }
-    const int32_t b = nodes[a].child1;
-    const int32_t c = nodes[a].child2;
-    const int32_t balance = nodes[c].height - nodes[b].height;
+    const int32_t b = A.child1;
+    const int32_t c = A.child2;
+    const m3TreeNode B = st.Get(b);
+    const m3TreeNode C = st.Get(c);
+    const int32_t balance = C.height - B.height;
     if (balance > -2 && balance < 2)
     {
         return a;
@@ -165,51 +183,57 @@ M3_HD int32_t m3TreeRotate(m3TreeRef t, int32_t a)
     // p rises; q is a's other child, which a keeps.
     const bool right = balance > 1;
     const int32_t p = right ? c : b;
-    const int32_t q = right ? b : c;
-    const int32_t p1 = nodes[p].child1;
-    const int32_t p2 = nodes[p].child2;
-    nodes[p].child1 = a;
-    nodes[p].parent = nodes[a].parent;
-    nodes[a].parent = p;
-    m3TreeReplaceChild(t, nodes[p].parent, a, p);
+    m3TreeNode P = right ? C : B;
+    const m3TreeNode Q = right ? B : C;
+    const int32_t p1 = P.child1;
+    const int32_t p2 = P.child2;
+    const m3TreeNode P1 = st.Get(p1);
+    const m3TreeNode P2 = st.Get(p2);
+    P.child1 = a;
+    P.parent = A.parent;
+    A.parent = p;
+    m3TreeReplaceChild(t, st, P.parent, a, p);
     // keep: p's taller child stays with p; move: the other goes to a.
-    const bool firstTaller = nodes[p1].height > nodes[p2].height;
+    const bool firstTaller = P1.height > P2.height;
     const int32_t keep = firstTaller ? p1 : p2;
     const int32_t move = firstTaller ? p2 : p1;
-    nodes[p].child2 = keep;
+    const m3TreeNode K = firstTaller ? P1 : P2;
+    m3TreeNode M = firstTaller ? P2 : P1;
+    P.child2 = keep;
     if (right)
     {
-        nodes[a].child2 = move;
+        A.child2 = move;
     }
     else
     {
-        nodes[a].child1 = move;
+        A.child1 = move;
     }
-    nodes[move].parent = a;
-    m3TreeUnion(nodes[q].lo, nodes[q].hi, nodes[move].lo, nodes[move].hi, nodes[a].lo,
-                nodes[a].hi);
-    m3TreeUnion(nodes[a].lo, nodes[a].hi, nodes[keep].lo, nodes[keep].hi, nodes[p].lo,
-                nodes[p].hi);
-    nodes[a].height = 1 + m3TreeMaxI(nodes[q].height, nodes[move].height);
-    nodes[p].height = 1 + m3TreeMaxI(nodes[a].height, nodes[keep].height);
+    M.parent = a;
+    m3TreeUnion(Q.lo, Q.hi, M.lo, M.hi, A.lo, A.hi);
+    m3TreeUnion(A.lo, A.hi, K.lo, K.hi, P.lo, P.hi);
+    A.height = 1 + m3TreeMaxI(Q.height, M.height);
+    P.height = 1 + m3TreeMaxI(A.height, K.height);
+    st.Put(move, M);
+    st.Put(a, A);
+    st.Put(p, P);
     return p;
 }
 
 // Walks from `index` to the root, rebalancing and refitting heights and
 // bounds (dynamic_tree.c:205-219).  A walk longer than the node count
 // can only come from a malformed tree; it stops there.
-M3_HD void m3TreeRefit(m3TreeRef t, int32_t index)
+template <class Store> M3_HD void m3TreeRefit(m3TreeRef t, const Store& st, int32_t index)
 {
-    m3TreeNode* nodes = t.nodes;
     for (int32_t guard = 0; index != M3_TREE_NULL && guard < t.capacity; ++guard)
     {
-        index = m3TreeRotate(t, index);
-        m3TreeNode* n = nodes + index;
-        const int32_t c1 = n->child1;
-        const int32_t c2 = n->child2;
-        n->height = 1 + m3TreeMaxI(nodes[c1].height, nodes[c2].height);
-        m3TreeUnion(nodes[c1].lo, nodes[c1].hi, nodes[c2].lo, nodes[c2].hi, n->lo, n->hi);
-        index = n->parent;
+        index = m3TreeRotate(t, st, index);
+        m3TreeNode n = st.Get(index);
+        const m3TreeNode c1 = st.Get(n.child1);
+        const m3TreeNode c2 = st.Get(n.child2);
+        n.height = 1 + m3TreeMaxI(c1.height, c2.height);
+        m3TreeUnion(c1.lo, c1.hi, c2.lo, c2.hi, n.lo, n.hi);
+        st.Put(index, n);
+        index = n.parent;
     }
 }
 
@@ -232,23 +256,26 @@ M3_HD double m3TreeChildCost(const m3TreeNode& child, const double lo[3], const 
 
 // Inserts a leaf for `userData` with bounds [lo, hi]; returns its node or
 // M3_TREE_NULL when the node pool is exhausted (dynamic_tree.c:221-322).
-M3_HD int32_t m3TreeInsert(m3TreeRef t, const double lo[3], const double hi[3], int32_t userData)
+template <class Store>
+M3_HD int32_t m3TreeInsert(m3TreeRef t, const Store& st, const double lo[3], const double hi[3],
+                           int32_t userData)
 {
-    const int32_t leaf = m3TreeTakeNode(t);
+    const int32_t leaf = m3TreeTakeNode(t, st);
     if (leaf == M3_TREE_NULL)
     {
         return M3_TREE_NULL;
     }
-    m3TreeNode* nodes = t.nodes;
+    m3TreeNode L = st.Get(leaf);
     for (int32_t k = 0; k < 3; ++k)
     {
-        nodes[leaf].lo[k] = lo[k];
-        nodes[leaf].hi[k] = hi[k];
+        L.lo[k] = lo[k];
+        L.hi[k] = hi[k];
     }
-    nodes[leaf].userData = userData;
-    nodes[leaf].height = 0;
+    L.userData = userData;
+    L.height = 0;
     if (*t.root == M3_TREE_NULL)
     {
+        st.Put(leaf, L);
         *t.root = leaf;
         return leaf;
     }
@@ -257,7 +284,7 @@ M3_HD int32_t m3TreeInsert(m3TreeRef t, const double lo[3], const double hi[3], 
     // chosen child's record is carried down, so each level loads only
     // the two children.
     int32_t index = *t.root;
-    m3TreeNode cur = nodes[index];
+    m3TreeNode cur = st.Get(index);
     for (int32_t guard = 0; cur.height > 0; ++guard)
     {
         if (guard >= t.capacity)
@@ -266,8 +293,8 @@ M3_HD int32_t m3TreeInsert(m3TreeRef t, const double lo[3], const double hi[3], 
         }
         const int32_t c1 = cur.child1;
         const int32_t c2 = cur.child2;
-        const m3TreeNode n1 = nodes[c1];
-        const m3TreeNode n2 = nodes[c2];
+        const m3TreeNode n1 = st.Get(c1);
+        const m3TreeNode n2 = st.Get(c2);
         double ulo[3];
         double uhi[3];
         m3TreeUnion(cur.lo, cur.hi, lo, hi, ulo, uhi);
@@ -294,55 +321,62 @@ M3_HD int32_t m3TreeInsert(m3TreeRef t, const double lo[3], const double hi[3], 
     // A new parent takes the sibling's place; sibling and leaf hang
     // under it in that order.
     const int32_t sibling = index;
-    const int32_t oldParent = nodes[sibling].parent;
-    const int32_t parent = m3TreeTakeNode(t);
+    m3TreeNode S = cur;
+    const int32_t oldParent = S.parent;
+    const int32_t parent = m3TreeTakeNode(t, st);
     if (parent == M3_TREE_NULL)
     {
-        m3TreeGiveNode(t, leaf);
+        m3TreeGiveNode(t, st, leaf);
         return M3_TREE_NULL;
     }
-    nodes[parent].parent = oldParent;
-    nodes[parent].userData = -1;
-    m3TreeUnion(lo, hi, nodes[sibling].lo, nodes[sibling].hi, nodes[parent].lo, nodes[parent].hi);
-    nodes[parent].height = nodes[sibling].height + 1;
-    m3TreeReplaceChild(t, oldParent, sibling, parent);
-    nodes[parent].child1 = sibling;
-    nodes[parent].child2 = leaf;
-    nodes[sibling].parent = parent;
-    nodes[leaf].parent = parent;
-    m3TreeRefit(t, parent);
+    m3TreeNode N = st.Get(parent);
+    N.parent = oldParent;
+    N.userData = -1;
+    m3TreeUnion(lo, hi, S.lo, S.hi, N.lo, N.hi);
+    N.height = S.height + 1;
+    m3TreeReplaceChild(t, st, oldParent, sibling, parent);
+    N.child1 = sibling;
+    N.child2 = leaf;
+    S.parent = parent;
+    L.parent = parent;
+    st.Put(parent, N);
+    st.Put(sibling, S);
+    st.Put(leaf, L);
+    m3TreeRefit(t, st, parent);
     return leaf;
 }
 
 // Removes a leaf; its parent is freed and the sibling takes the parent's
 // place (dynamic_tree.c:324-358).
-M3_HD void m3TreeRemove(m3TreeRef t, int32_t leaf)
+template <class Store> M3_HD void m3TreeRemove(m3TreeRef t, const Store& st, int32_t leaf)
 {
-    m3TreeNode* nodes = t.nodes;
     if (leaf == *t.root)
     {
         *t.root = M3_TREE_NULL;
-        m3TreeGiveNode(t, leaf);
+        m3TreeGiveNode(t, st, leaf);
         return;
     }
-    const int32_t parent = nodes[leaf].parent;
-    const int32_t grand = nodes[parent].parent;
-    const int32_t sibling =
-        nodes[parent].child1 == leaf ? nodes[parent].child2 : nodes[parent].child1;
+    const int32_t parent = st.Get(leaf).parent;
+    const m3TreeNode P = st.Get(parent);
+    const int32_t grand = P.parent;
+    const int32_t sibling = P.child1 == leaf ? P.child2 : P.child1;
+    m3TreeNode S = st.Get(sibling);
     if (grand != M3_TREE_NULL)
     {
-        m3TreeReplaceChild(t, grand, parent, sibling);
-        nodes[sibling].parent = grand;
-        m3TreeGiveNode(t, parent);
-        m3TreeRefit(t, grand);
+        m3TreeReplaceChild(t, st, grand, parent, sibling);
+        S.parent = grand;
+        st.Put(sibling, S);
+        m3TreeGiveNode(t, st, parent);
+        m3TreeRefit(t, st, grand);
     }
     else
     {
         *t.root = sibling;
-        nodes[sibling].parent = M3_TREE_NULL;
-        m3TreeGiveNode(t, parent);
+        S.parent = M3_TREE_NULL;
+        st.Put(sibling, S);
+        m3TreeGiveNode(t, st, parent);
     }
-    m3TreeGiveNode(t, leaf);
+    m3TreeGiveNode(t, st, leaf);
 }
 
 M3_HD bool m3TreeContains(const m3TreeNode& n, const m3Aabb& b)

@@ -40,6 +40,10 @@ struct m3UploadItem
 int32_t m3gpuLaunchUpload(const m3UploadItem* items, int32_t count);
 // Bytes of one hull slab an upload copies (the parts its counts use).
 int64_t m3HullUsedBytes(const m3HullData* h);
+// Content key of an interned hull slab for the dedup index: FNV-1a over
+// its counts and used vertices (equal slabs give equal keys; lookups
+// confirm with a full compare).
+uint64_t m3HullKey(const m3HullData* h);
 
 
 template <class T> struct m3PageAllocator
@@ -56,6 +60,16 @@ template <class T> struct m3PageAllocator
     void deallocate(T* p, size_t n)
     {
         m3HostFree(p, n * sizeof(T));
+    }
+    // Elements are default-initialised (no zeroing on resize): the owners
+    // clear what they allocate with one memset.
+    template <class U> void construct(U* p)
+    {
+        ::new ((void*)p) U;
+    }
+    template <class U, class... Args> void construct(U* p, Args&&... args)
+    {
+        ::new ((void*)p) U(static_cast<Args&&>(args)...);
     }
     template <class U> bool operator==(const m3PageAllocator<U>&) const
     {
@@ -179,6 +193,9 @@ int32_t m3gpuUpload(m3HostWorld* w);
 // rest one world at a time.
 int32_t m3gpuUploadBatch(m3HostWorld** worlds, int32_t count);
 int32_t m3gpuDownload(m3HostWorld* w);
+// The world's step status word (M3GPU_OK or its refusal), read from the
+// device when it is resident.
+int32_t m3gpuWorldStatus(m3HostWorld* w);
 // The current pair buffer in full, device to host (for a snapshot).
 int32_t m3gpuDownloadPairTails(m3HostWorld* w);
 void m3gpuRelease(m3HostWorld* w);
@@ -202,8 +219,11 @@ bool m3ParseJournal(const m3HostWorld* w, const uint8_t* stream, int32_t size,
 void m3DrainBrokenJoints(m3HostWorld* w);
 
 // Step and hash entry points (step.cu).
+// `ops` (optional) are body commands applied on the device before the
+// first step: m3BodyOp.world indexes `worlds`; per world they apply in
+// array order.
 int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t substeps,
-                       int32_t steps);
+                       int32_t steps, const struct m3BodyOp* ops = nullptr, int32_t opCount = 0);
 int32_t m3gpuHashBatch(m3HostWorld** worlds, int32_t count, uint64_t* out);
 // The parallel world hash (hash.cu): one block per world, blocks in
 // `order`, out[world] = that world's m3WorldHashView.

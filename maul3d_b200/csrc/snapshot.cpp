@@ -532,6 +532,11 @@ extern "C" int32_t m3World_Snapshot(m3WorldId worldId, void* out, int32_t capaci
     {
         return -1;
     }
+    if (w->hv.sc->treeTracked == 0)
+    {
+        m3gpuSetError(M3GPU_ERR_UNSUPPORTED, "m3World_Snapshot: the world keeps no tree");
+        return -1;
+    }
     const int64_t fixed = FixedBytes(w);
     const int64_t size = (int64_t)sizeof(SnapshotHeader) + fixed + TailBytes(w);
     if (capacity < size)
@@ -848,13 +853,16 @@ extern "C" bool m3World_Restore(m3WorldId worldId, const void* data, int32_t siz
             hd.jointRetiredCount);
     SetRing(w->hullFree, pb.hullQueue, hd.hullFreeHead, hd.hullFreeCount, hd.hullRetiredCount);
     w->hullGen = pb.hullGens;
-    w->hulls.assign((size_t)hd.hullMaxIndex, m3HullData{});
+    w->hulls.resize((size_t)hd.hullMaxIndex);
+    if (hd.hullMaxIndex > 0)
+    {
+        memset(w->hulls.data(), 0, sizeof(m3HullData) * (size_t)hd.hullMaxIndex);
+    }
     w->hullRefs.assign(pb.hullRefs.begin(), pb.hullRefs.begin() + hd.hullMaxIndex);
     w->hullIndexByContent.clear();
     for (int32_t h = 0; h < hd.hullMaxIndex; ++h)
     {
-        m3HullData* d = &w->hulls[(size_t)h];
-        memset(d, 0, sizeof(*d));
+        m3HullData* d = &w->hulls[(size_t)h]; // zeroed by the assign above
         const uint8_t* p = raw + hullAt[(size_t)h];
         d->vertexCount = ReadI32(p);
         d->faceCount = ReadI32(p + 4);
@@ -866,7 +874,7 @@ extern "C" bool m3World_Restore(m3WorldId worldId, const void* data, int32_t siz
         }
         if (w->hullRefs[(size_t)h] > 0)
         {
-            w->hullIndexByContent.emplace(m3Fnv(M3_HASH_INIT, d, (int32_t)sizeof(m3HullData)), h);
+            w->hullIndexByContent.emplace(m3HullKey(d), h);
         }
     }
     w->snapshotCarry.swap(carry);

@@ -38,6 +38,7 @@
 #include "m3_solver.cuh"
 #include "m3_joints.cuh"
 #include "m3_tree.h"
+#include "m3_ops.h"
 
 #include <cuda_runtime.h>
 
@@ -453,14 +454,15 @@ __global__ void __launch_bounds__(32 * M3_TREE_WORLDS_PER_BLOCK)
     {
         return;
     }
+    const m3TreeArrayStore store{w.treeNodes};
     const int32_t* shapes = s.treeMoveShape + (int64_t)slot * sc->shapeCap;
     const m3Aabb* boxes = s.treeMoveBox + (int64_t)slot * sc->shapeCap;
     for (int32_t m = 0; m < moves; ++m)
     {
         const int32_t shape = shapes[m];
         const m3Aabb box = boxes[m];
-        m3TreeRemove(tree, w.proxyId[shape]);
-        const int32_t leaf = m3TreeInsert(tree, box.lo, box.hi, shape);
+        m3TreeRemove(tree, store, w.proxyId[shape]);
+        const int32_t leaf = m3TreeInsert(tree, store, box.lo, box.hi, shape);
         w.proxyId[shape] = leaf;
         if (leaf == M3_TREE_NULL)
         {
@@ -567,10 +569,11 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3BroadKernel(const m3WorldVie
     // the fat bounds they are reinserted with.  A leaf moves only when
     // its own shape is reinserted, so every containment test can run
     // here at once; m3TreeKernel replays the moves in order.
+    const bool tracked = sc->treeTracked != 0;
     for (int32_t i = tid; i < shapeMax; i += NT)
     {
         int32_t move = 0;
-        if (w.shapeAlive[i] != 0 && s.hasLeaf[i] != 0 && w.awake[w.shapeBody[i]] != 0)
+        if (tracked && w.shapeAlive[i] != 0 && s.hasLeaf[i] != 0 && w.awake[w.shapeBody[i]] != 0)
         {
             const m3Aabb& leaf = s.leafBox[i];
             const m3Aabb& b = s.aabb[i];
@@ -2973,8 +2976,101 @@ extern "C" int32_t m3gpu_world_phase_cycles(m3WorldId world, uint64_t* out)
     return M3GPU_OK;
 }
 
+// Body commands between steps (body.c:351-418), for the serving path:
+// one thread per world applies its commands in order.
+__global__ void __launch_bounds__(M3_BLOCK) m3BodyOpKernel(const m3WorldView* views, int32_t count,
+                                                          const m3BodyOp* ops,
+                                                          const int32_t* offsets)
+{
+    const int32_t wi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (wi >= count)
+    {
+        return;
+    }
+    const m3WorldView& w = views[wi];
+    if (w.sc->status != 0)
+    {
+        return;
+    }
+    for (int32_t k = offsets[wi]; k < offsets[wi + 1]; ++k)
+    {
+        const m3BodyOp o = ops[k];
+        if (o.body >= 0 && o.body < w.sc->bodyMax)
+        {
+            m3ApplyBodyOp(w, o.op, o.body, o.v);
+        }
+    }
+}
+
+// Page-locked staging and device copies of a batch's body commands.
+struct m3OpStaging
+{
+    uint8_t* host = nullptr;
+    uint8_t* dev = nullptr;
+    int64_t cap = 0;
+};
+static m3OpStaging s_ops;
+
+static int32_t LaunchBodyOps(int32_t count, const m3BodyOp* ops, int32_t opCount)
+{
+    // Ops sorted by world (stable), and each world's range.
+    std::vector<int32_t> offsets((size_t)count + 1, 0);
+    for (int32_t k = 0; k < opCount; ++k)
+    {
+        if (ops[k].world < 0 || ops[k].world >= count)
+        {
+            return m3gpuSetError(M3GPU_ERR_INVALID, "body command names world %d of %d",
+                                 ops[k].world, count);
+        }
+        offsets[(size_t)ops[k].world + 1] += 1;
+    }
+    for (int32_t i = 0; i < count; ++i)
+    {
+        offsets[(size_t)i + 1] += offsets[(size_t)i];
+    }
+    std::vector<int32_t> fill(offsets.begin(), offsets.end() - 1);
+    std::vector<m3BodyOp> sorted((size_t)opCount);
+    for (int32_t k = 0; k < opCount; ++k)
+    {
+        sorted[(size_t)fill[(size_t)ops[k].world]++] = ops[k];
+    }
+    const int64_t opBytes = (int64_t)sizeof(m3BodyOp) * opCount;
+    const int64_t offBytes = (int64_t)sizeof(int32_t) * (count + 1);
+    const int64_t need = m3AlignUp(opBytes, 256) + offBytes;
+    if (need > s_ops.cap)
+    {
+        cudaDeviceSynchronize();
+        cudaFreeHost(s_ops.host);
+        cudaFree(s_ops.dev);
+        s_ops = m3OpStaging{};
+        int32_t rc = Check(cudaMallocHost((void**)&s_ops.host, (size_t)need), "op staging");
+        if (rc == M3GPU_OK)
+        {
+            rc = Check(cudaMalloc((void**)&s_ops.dev, (size_t)need), "op staging");
+        }
+        if (rc != M3GPU_OK)
+        {
+            return rc;
+        }
+        s_ops.cap = need;
+    }
+    memcpy(s_ops.host, sorted.data(), (size_t)opBytes);
+    memcpy(s_ops.host + m3AlignUp(opBytes, 256), offsets.data(), (size_t)offBytes);
+    int32_t rc = Check(cudaMemcpyAsync(s_ops.dev, s_ops.host, (size_t)need, cudaMemcpyHostToDevice, 0),
+                       "upload body commands");
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
+    m3BodyOpKernel<<<(count + M3_BLOCK - 1) / M3_BLOCK, M3_BLOCK>>>(
+        s_batch.dviews, count, (const m3BodyOp*)s_ops.dev,
+        (const int32_t*)(s_ops.dev + m3AlignUp(opBytes, 256)));
+    s_launches += 1;
+    return Check(cudaGetLastError(), "body command kernel");
+}
+
 int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t substeps,
-                       int32_t steps)
+                       int32_t steps, const m3BodyOp* ops, int32_t opCount)
 {
     int32_t rc = m3gpuEnsureDevice();
     if (rc != M3GPU_OK)
@@ -2985,6 +3081,12 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
     if (rc == M3GPU_OK)
     {
         rc = EnsureClassStreams();
+    }
+    if (rc == M3GPU_OK && opCount > 0)
+    {
+        // The staging buffer is reused by the next call only after this
+        // one synchronised (below, reading the status).
+        rc = LaunchBodyOps(count, ops, opCount);
     }
     if (rc != M3GPU_OK)
     {
@@ -3020,39 +3122,52 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
     cudaEventRecord(s_events[0]);
     // The broadphase tree: the leaves' bounds once per batch, then per
     // step the tree kernel on its own stream, at most M3_TREE_LAG steps
-    // behind (the move lists sit in a ring of that depth).
-    m3LeafBoxKernel<<<count, M3_BLOCK>>>(s_batch.dviews, count);
+    // behind (the move lists sit in a ring of that depth).  Batches of
+    // worlds that keep no tree skip both.
+    bool anyTracked = false;
+    for (int32_t i = 0; i < count; ++i)
+    {
+        anyTracked = anyTracked || worlds[i]->hv.sc->treeTracked != 0;
+    }
+    if (anyTracked)
+    {
+        m3LeafBoxKernel<<<count, M3_BLOCK>>>(s_batch.dviews, count);
+    }
     const cudaStream_t treeStream = s_classStreams.tree;
     for (int32_t step = 0; step < steps; ++step)
     {
         const cudaEvent_t* ev = &s_events[(size_t)(M3_STAGES * step)];
-        if (step >= M3_TREE_LAG)
+        if (anyTracked && step >= M3_TREE_LAG)
         {
             cudaStreamWaitEvent(0, s_classStreams.treeDone[(size_t)(step - M3_TREE_LAG)], 0);
         }
         m3BroadKernel<M3_BLOCK, 2><<<count, M3_BLOCK>>>(s_batch.dviews, s_batch.dorder, count,
                                                         step % M3_TREE_LAG, M3_TREE_LAG);
-        cudaEventRecord(s_classStreams.broadDone[(size_t)step], 0);
-        cudaStreamWaitEvent(treeStream, s_classStreams.broadDone[(size_t)step], 0);
-        m3TreeKernel<<<(count + M3_TREE_WORLDS_PER_BLOCK - 1) / M3_TREE_WORLDS_PER_BLOCK,
-                       32 * M3_TREE_WORLDS_PER_BLOCK, 0, treeStream>>>(
-            s_batch.dviews, s_batch.dorder, count, step % M3_TREE_LAG, M3_TREE_LAG);
-        cudaEventRecord(s_classStreams.treeDone[(size_t)step], treeStream);
+        if (anyTracked)
+        {
+            cudaEventRecord(s_classStreams.broadDone[(size_t)step], 0);
+            cudaStreamWaitEvent(treeStream, s_classStreams.broadDone[(size_t)step], 0);
+            m3TreeKernel<<<(count + M3_TREE_WORLDS_PER_BLOCK - 1) / M3_TREE_WORLDS_PER_BLOCK,
+                           32 * M3_TREE_WORLDS_PER_BLOCK, 0, treeStream>>>(
+                s_batch.dviews, s_batch.dorder, count, step % M3_TREE_LAG, M3_TREE_LAG);
+            cudaEventRecord(s_classStreams.treeDone[(size_t)step], treeStream);
+            s_launches += 1;
+        }
         m3PairOffsetsKernel<<<1, M3_BLOCK>>>(s_batch.dviews, count, s_batch.doffsets);
         LaunchNarrow(s_batch.dviews, s_batch.doffsets, count);
         cudaEventRecord(ev[1]);
         LaunchSolve(s_batch.dviews, s_batch.dorder, count, dt, substeps, s_batch.cacheBytes,
                     ev + 2, s_batch.classFirst, s_batch.classCache);
         cudaEventRecord(ev[4]);
-        s_launches += 6 + M3_NARROW_LAUNCHES;
+        s_launches += 5 + M3_NARROW_LAUNCHES;
     }
-    if (steps > 0)
+    if (anyTracked && steps > 0)
     {
         // Everything after the batch (status, readbacks, snapshots) sees
         // the finished tree.
         cudaStreamWaitEvent(0, s_classStreams.treeDone[(size_t)(steps - 1)], 0);
     }
-    s_launches += 1;
+    s_launches += anyTracked ? 1 : 0;
     cudaMemsetAsync(s_dstatus, 0, sizeof(int32_t));
     m3StatusKernel<<<(count + 255) / 256, 256>>>(s_batch.dviews, count, s_dstatus);
     s_launches += 1;

@@ -18,6 +18,7 @@
 #include "m3_hash.h"
 
 #include <math.h>
+#include <stddef.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -166,7 +167,8 @@ extern "C" m3WorldId m3CreateWorld(const m3WorldDef* def)
     w->jointFree.Init(w->jointCap);
     w->persistentBytes =
         m3LayoutPersistent(nullptr, nullptr, w->bodyCap, w->shapeCap, w->jointCap, w->pairCap);
-    w->image.assign((size_t)w->persistentBytes, 0);
+    w->image.resize((size_t)w->persistentBytes);
+    memset(w->image.data(), 0, (size_t)w->persistentBytes);
     m3LayoutPersistent(&w->hv, w->image.data(), w->bodyCap, w->shapeCap, w->jointCap, w->pairCap);
     w->hv.hulls = nullptr;
     w->hv.scratch = nullptr;
@@ -187,6 +189,7 @@ extern "C" m3WorldId m3CreateWorld(const m3WorldDef* def)
     sc->shapeCap = w->shapeCap;
     sc->jointCap = w->jointCap;
     sc->pairCap = w->pairCap;
+    sc->treeTracked = 1;
 
     // Array initial values of the reference's create (world.c:160-440):
     // empty list heads and unset slots read -1; joint targets identity.
@@ -781,13 +784,22 @@ static void BuildBoxHull(m3HullData* out, m3Vec3 he)
     BuildHalfEdges(out);
 }
 
+uint64_t m3HullKey(const m3HullData* h)
+{
+    const int32_t nv = h->vertexCount < 0 ? 0
+                                          : (h->vertexCount > M3_HULL_MAX_VERTS ? M3_HULL_MAX_VERTS
+                                                                                : h->vertexCount);
+    uint64_t key = m3Fnv(M3_HASH_INIT, h, (int32_t)offsetof(m3HullData, vertices));
+    return m3Fnv(key, h->vertices, 12 * nv);
+}
+
 // Content-deduplicated interning in ascending slot order (hull.c:132-152).
 // Live slabs are pairwise distinct, so the first match in slot order is
 // the only match; a content-hash index finds it without scanning.
 static int32_t InternHull(m3HostWorld* w, const m3HullData* data)
 {
     m3WorldScalars* sc = w->hv.sc;
-    uint64_t key = m3Fnv(M3_HASH_INIT, data, (int32_t)sizeof(m3HullData));
+    uint64_t key = m3HullKey(data);
     auto range = w->hullIndexByContent.equal_range(key);
     for (auto it = range.first; it != range.second; ++it)
     {
@@ -923,7 +935,8 @@ static m3ShapeId CreateShapeCommon(m3BodyId bodyId, const m3ShapeDef* def, uint8
         m3WorldView tv = v;
         tv.hulls = w->hulls.empty() ? nullptr : w->hulls.data();
         const m3Aabb box = m3ShapeFreshBounds(tv, s);
-        v.proxyId[s] = m3TreeInsert(m3WorldTree(v), box.lo, box.hi, s);
+        v.proxyId[s] =
+            m3TreeInsert(m3WorldTree(v), m3TreeArrayStore{v.treeNodes}, box.lo, box.hi, s);
     }
     RecomputeMass(w, b);
     w->hostDirty = true;

@@ -1,0 +1,144 @@
+"""Serving (C4): replay containers in, final hashes out.
+
+CPU: the M3J1 container codec (replay.c:15-136) encodes the reference's
+bytes and refuses what it refuses.  GPU: a server fed containers of
+reference snapshots and impulse journals answers each with the hash the
+reference gives after m3World_Restore + m3World_JournalReplay, whatever
+else shares the batch.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import cuda_available
+from maul3d_b200 import abi
+from maul3d_b200.abi import SCENE_TOWERS, SCENE_UNEVEN
+
+
+def _snapshot(lib, wid) -> bytes:
+    n = lib.m3World_SnapshotSize(wid)
+    buf = (C.c_uint8 * n)()
+    assert lib.m3World_Snapshot(wid, buf, n) == n
+    return bytes(buf)
+
+
+def _journal(rng, bodies: int, frames: int) -> bytes:
+    """`frames` frames of 1-8 linear impulses of 1-50 N s on random bodies,
+    each closed by a step of 1/60 s in 4 substeps."""
+    out = b""
+    for _ in range(frames):
+        for _ in range(int(rng.integers(1, 9))):
+            d = rng.normal(size=3)
+            d = d / np.linalg.norm(d) * rng.uniform(1.0, 50.0)
+            out += abi.journal_body_command(abi.OP_APPLY_LINEAR_IMPULSE,
+                                            int(rng.integers(2, bodies + 1)), 0,
+                                            [float(x) for x in d.astype(np.float32)])
+        out += abi.journal_step(1.0 / 60.0, 4)
+    return out
+
+
+@pytest.fixture(scope="module")
+def ref(oracle):
+    return abi.bind_replay(abi.bind_snapshot(abi.bind_create(oracle.lib())))
+
+
+def test_container_codec_matches_the_reference(m3, ref):
+    rng = np.random.default_rng(3)
+    snap = bytes(rng.integers(0, 256, 400, dtype=np.uint8))
+    journal = _journal(rng, 50, 5)
+    ours = abi.encode_container(m3.lib, snap, journal, 0x1234)
+    theirs = abi.encode_container(ref, snap, journal, 0x1234)
+    assert ours == theirs
+    for lib in (m3.lib, ref):
+        view = abi.m3ReplayView()
+        buf = (C.c_uint8 * len(ours)).from_buffer_copy(ours)
+        assert lib.m3ReplayDecode(buf, len(ours), C.byref(view))
+        assert view.snapshotBytes == 400 and view.finalHash == 0x1234
+        assert view.info.stepCount == 5
+        bad = bytearray(ours)
+        bad[16] ^= 1  # a header that lies about its step count
+        buf = (C.c_uint8 * len(bad)).from_buffer_copy(bytes(bad))
+        assert not lib.m3ReplayDecode(buf, len(bad), C.byref(view))
+        info = abi.m3JournalInfo()
+        j = (C.c_uint8 * len(journal)).from_buffer_copy(journal)
+        assert lib.m3JournalDescribe(j, len(journal), C.byref(info))
+        assert not lib.m3JournalDescribe(j, len(journal) - 1, C.byref(info))
+
+
+def test_submit_refuses_a_bad_container(m3):
+    server = m3.Server()
+    with pytest.raises(m3.M3GpuError):
+        server.submit(b"not a container at all, not even close....")
+    server.close()
+
+
+def _requests(oracle, ref, count, seed):
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for i in range(count):
+        scene, param = (SCENE_TOWERS, 2) if i % 5 == 4 else (SCENE_UNEVEN,
+                                                              int(rng.integers(200, 700)))
+        r = oracle.RefWorld.scene(scene, 900 + i, param)
+        r.step(1.0 / 60.0, 4, int(rng.integers(1, 30)))
+        snap = _snapshot(ref, r.id)
+        journal = _journal(rng, r.body_count() - 1, int(rng.integers(4, 17)))
+        jb = (C.c_uint8 * len(journal)).from_buffer_copy(journal)
+        assert ref.m3World_JournalReplay(r.id, jb, len(journal))
+        reqs.append((abi.encode_container(ref, snap, journal, r.hash()), r.hash()))
+        r.destroy()
+    return reqs
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not cuda_available(), reason="needs a CUDA device")
+def test_served_hashes_equal_restore_and_replay_on_the_reference(m3, oracle, ref):
+    reqs = _requests(oracle, ref, 24, 7)
+    server = m3.Server(max_active=10)
+    tickets = [server.submit(c) for c, _ in reqs]
+    done = server.run()
+    server.close()
+    for t, (_, expected) in zip(tickets, reqs):
+        h, status = done[t]
+        assert status == m3.M3GPU_OK
+        assert h == expected, f"ticket {t}"
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not cuda_available(), reason="needs a CUDA device")
+def test_a_request_alone_and_in_a_crowd_gives_the_same_hash(m3, oracle, ref):
+    reqs = _requests(oracle, ref, 6, 11)
+    alone = m3.Server()
+    t = alone.submit(reqs[0][0])
+    h_alone = alone.run()[t][0]
+    alone.close()
+    crowd = m3.Server(max_active=3)
+    ts = [crowd.submit(c) for c, _ in reqs]
+    done = crowd.run()
+    crowd.close()
+    assert done[ts[0]][0] == h_alone == reqs[0][1]
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not cuda_available(), reason="needs a CUDA device")
+def test_unmodelled_content_completes_with_its_refusal(m3, oracle, ref):
+    # A snapshot with a live water volume: restored nowhere, reported.
+    from test_snapshot import _WaterVolumeDef, _WaterVolumeId
+    lib = oracle.lib()
+    lib.m3DefaultWaterVolumeDef.restype = _WaterVolumeDef
+    lib.m3CreateWaterVolume.argtypes = [abi.m3WorldId, C.POINTER(_WaterVolumeDef)]
+    lib.m3CreateWaterVolume.restype = _WaterVolumeId
+    r = oracle.RefWorld.scene(SCENE_UNEVEN, 5, 64)
+    wd = lib.m3DefaultWaterVolumeDef()
+    wd.lo = abi.m3Pos3(-5.0, -1.0, -5.0)
+    wd.hi = abi.m3Pos3(5.0, 0.5, 5.0)
+    assert lib.m3CreateWaterVolume(r.id, C.byref(wd)).index1 > 0
+    container = abi.encode_container(ref, _snapshot(ref, r.id), abi.journal_step(1 / 60, 4))
+    good = _requests(oracle, ref, 1, 13)[0]
+    server = m3.Server()
+    bad_t = server.submit(container)
+    good_t = server.submit(good[0])
+    done = server.run()
+    server.close()
+    assert done[bad_t][1] == m3.M3GPU_ERR_UNSUPPORTED
+    assert done[good_t] == (good[1], m3.M3GPU_OK)
