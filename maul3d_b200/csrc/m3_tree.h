@@ -160,31 +160,21 @@ M3_HD void m3TreeReplaceChild(m3TreeRef t, const Store& st, int32_t parent, int3
     }
 }
 
-// Rotates the subtree at a when its children's heights differ by more
-// than one: the taller child (p) rises, a becomes its child, and a keeps
-// the shorter of p's children while p keeps the taller one
-// (dynamic_tree.c:92-203).  Returns the subtree's new root.
-template <class Store> M3_HD int32_t m3TreeRotate(m3TreeRef t, const Store& st, int32_t a)
+// Rotates the subtree at a (record A, children records B and C) whose
+// children's heights differ by more than one: the taller child (p)
+// rises, a becomes its child, and a keeps the shorter of p's children
+// while p keeps the taller one (dynamic_tree.c:92-203).  Writes a, p and
+// the moved grandchild; returns p's record (bounds and height final).
+template <class Store>
+M3_HD m3TreeNode m3TreeRotate(m3TreeRef t, const Store& st, int32_t a, m3TreeNode A,
+                              const m3TreeNode& B, const m3TreeNode& C, int32_t* newRoot)
 {
-    m3TreeNode A = st.Get(a);
-    if (A.height < 2 || A.child1 == M3_TREE_NULL)
-    {
-        return a;
-    }
     const int32_t b = A.child1;
     const int32_t c = A.child2;
-    const m3TreeNode B = st.Get(b);
-    const m3TreeNode C = st.Get(c);
-    const int32_t balance = C.height - B.height;
-    if (balance > -2 && balance < 2)
-    {
-        return a;
-    }
-    // p rises; q is a's other child, which a keeps.
-    const bool right = balance > 1;
+    const bool right = C.height - B.height > 1;
     const int32_t p = right ? c : b;
     m3TreeNode P = right ? C : B;
-    const m3TreeNode Q = right ? B : C;
+    const m3TreeNode& Q = right ? B : C;
     const int32_t p1 = P.child1;
     const int32_t p2 = P.child2;
     const m3TreeNode P1 = st.Get(p1);
@@ -197,7 +187,7 @@ template <class Store> M3_HD int32_t m3TreeRotate(m3TreeRef t, const Store& st, 
     const bool firstTaller = P1.height > P2.height;
     const int32_t keep = firstTaller ? p1 : p2;
     const int32_t move = firstTaller ? p2 : p1;
-    const m3TreeNode K = firstTaller ? P1 : P2;
+    const m3TreeNode& K = firstTaller ? P1 : P2;
     m3TreeNode M = firstTaller ? P2 : P1;
     P.child2 = keep;
     if (right)
@@ -216,42 +206,37 @@ template <class Store> M3_HD int32_t m3TreeRotate(m3TreeRef t, const Store& st, 
     st.Put(move, M);
     st.Put(a, A);
     st.Put(p, P);
-    return p;
+    *newRoot = p;
+    return P;
 }
 
 // Walks from `index` to the root, rebalancing and refitting heights and
-// bounds (dynamic_tree.c:205-219).  A walk longer than the node count
-// can only come from a malformed tree; it stops there.
+// bounds (dynamic_tree.c:205-219).  The balance test reads the node's
+// stored height, as the reference's does before its refit; after a
+// rotation the risen node's height and bounds are already what the
+// refit would compute (the union of its two children, in order).  A
+// walk longer than the node count can only come from a malformed tree;
+// it stops there.
 template <class Store> M3_HD void m3TreeRefit(m3TreeRef t, const Store& st, int32_t index)
 {
     for (int32_t guard = 0; index != M3_TREE_NULL && guard < t.capacity; ++guard)
     {
-        index = m3TreeRotate(t, st, index);
         m3TreeNode n = st.Get(index);
         const m3TreeNode c1 = st.Get(n.child1);
         const m3TreeNode c2 = st.Get(n.child2);
+        const int32_t balance = c2.height - c1.height;
+        if (n.height >= 2 && n.child1 != M3_TREE_NULL && (balance > 1 || balance < -1))
+        {
+            int32_t root = index;
+            n = m3TreeRotate(t, st, index, n, c1, c2, &root);
+            index = n.parent;
+            continue;
+        }
         n.height = 1 + m3TreeMaxI(c1.height, c2.height);
         m3TreeUnion(c1.lo, c1.hi, c2.lo, c2.hi, n.lo, n.hi);
         st.Put(index, n);
         index = n.parent;
     }
-}
-
-// Surface-area cost of pairing the new box with a child: the area of
-// the union, less the child's own area when the child is internal (a
-// leaf gains a new parent whose area all counts), plus the inherited
-// cost of growing the ancestors (dynamic_tree.c:245-273).
-M3_HD double m3TreeChildCost(const m3TreeNode& child, const double lo[3], const double hi[3],
-                             double inherited)
-{
-    double ulo[3];
-    double uhi[3];
-    m3TreeUnion(child.lo, child.hi, lo, hi, ulo, uhi);
-    if (child.height == 0)
-    {
-        return m3TreeArea(ulo, uhi) + inherited;
-    }
-    return m3TreeArea(ulo, uhi) - m3TreeArea(child.lo, child.hi) + inherited;
 }
 
 // Inserts a leaf for `userData` with bounds [lo, hi]; returns its node or
@@ -281,10 +266,20 @@ M3_HD int32_t m3TreeInsert(m3TreeRef t, const Store& st, const double lo[3], con
     }
     // Descend while a child is cheaper than pairing here (at most one
     // level per node: a longer descent means a malformed tree).  The
-    // chosen child's record is carried down, so each level loads only
-    // the two children.
+    // chosen child's record, its own area and the area of its union
+    // with the new box (both computed for its cost) are carried down,
+    // so each level loads and measures only the two children.
     int32_t index = *t.root;
     m3TreeNode cur = st.Get(index);
+    double curUnion;
+    double curArea;
+    {
+        double ulo[3];
+        double uhi[3];
+        m3TreeUnion(cur.lo, cur.hi, lo, hi, ulo, uhi);
+        curUnion = m3TreeArea(ulo, uhi);
+        curArea = m3TreeArea(cur.lo, cur.hi);
+    }
     for (int32_t guard = 0; cur.height > 0; ++guard)
     {
         if (guard >= t.capacity)
@@ -295,14 +290,20 @@ M3_HD int32_t m3TreeInsert(m3TreeRef t, const Store& st, const double lo[3], con
         const int32_t c2 = cur.child2;
         const m3TreeNode n1 = st.Get(c1);
         const m3TreeNode n2 = st.Get(c2);
+        const double here = 2.0 * curUnion;
+        const double inherited = 2.0 * (curUnion - curArea);
         double ulo[3];
         double uhi[3];
-        m3TreeUnion(cur.lo, cur.hi, lo, hi, ulo, uhi);
-        const double area = m3TreeArea(ulo, uhi);
-        const double here = 2.0 * area;
-        const double inherited = 2.0 * (area - m3TreeArea(cur.lo, cur.hi));
-        const double cost1 = m3TreeChildCost(n1, lo, hi, inherited);
-        const double cost2 = m3TreeChildCost(n2, lo, hi, inherited);
+        m3TreeUnion(n1.lo, n1.hi, lo, hi, ulo, uhi);
+        const double union1 = m3TreeArea(ulo, uhi);
+        const double area1 = n1.height == 0 ? 0.0 : m3TreeArea(n1.lo, n1.hi);
+        m3TreeUnion(n2.lo, n2.hi, lo, hi, ulo, uhi);
+        const double union2 = m3TreeArea(ulo, uhi);
+        const double area2 = n2.height == 0 ? 0.0 : m3TreeArea(n2.lo, n2.hi);
+        // dynamic_tree.c:245-273: a leaf child's cost is its union's area
+        // plus the inherited cost; an internal child's subtracts its area.
+        const double cost1 = n1.height == 0 ? union1 + inherited : union1 - area1 + inherited;
+        const double cost2 = n2.height == 0 ? union2 + inherited : union2 - area2 + inherited;
         if (here < cost1 && here < cost2)
         {
             break;
@@ -311,11 +312,15 @@ M3_HD int32_t m3TreeInsert(m3TreeRef t, const Store& st, const double lo[3], con
         {
             index = c1;
             cur = n1;
+            curUnion = union1;
+            curArea = area1; // a leaf ends the descent: its area is not read
         }
         else
         {
             index = c2;
             cur = n2;
+            curUnion = union2;
+            curArea = area2;
         }
     }
     // A new parent takes the sibling's place; sibling and leaf hang
