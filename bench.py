@@ -8,9 +8,11 @@ half-height 0.4) hung from static anchors; dt 1/60, 4 substeps.  The
 worlds are seeded synthetic scenes built through the library's
 reference-compatible creation API (maul3d_b200/csrc/scenes.c).
 
-One "step" = one m3World_Step of every world in the batch.  The metric
-counts alive dynamic bodies x substeps x steps over all worlds and all
-ranks, divided by the max-over-ranks device time of exactly K steps.
+One "step" = one m3World_Step of every world in the batch, everything
+the reference's step does included (the broadphase tree it keeps as
+snapshot state too).  The metric counts alive dynamic bodies x substeps
+x steps over all worlds and all ranks, divided by the max-over-ranks
+device time of exactly K steps.
 
 Lines printed by rank 0 (one JSON object):
   value     device-resident throughput (CUDA events around K steps);
@@ -24,7 +26,11 @@ Lines printed by rank 0 (one JSON object):
   cpu_baseline  the reference engine (oracle/_ref, built from its own
             sources) on the host cores, stepping a bounded sample of the
             same worlds for the same W+K steps, every sampled world's
-            hash checked against the device's.
+            hash checked against the device's;
+  serving   the serving path: replay containers (snapshot + journal of
+            impulse frames) of worlds of 200-5000 bodies arriving as a
+            Poisson process, p50/p99 latency from arrival to final hash
+            and throughput, plus a run with every request at once.
 
 Multi-GPU: one process per GPU (torchrun), each rank its own 4096
 worlds (weak scaling), no collective on the data path; the only NCCL

@@ -220,9 +220,17 @@ M3GPU_API int32_t m3World_Snapshot(m3WorldId worldId, void* out, int32_t capacit
  * characters, vehicles, soft bodies, water volumes). */
 M3GPU_API bool m3World_Restore(m3WorldId worldId, const void* data, int32_t size);
 
+/* world.c:1369-1398 (world.h:600-601): journal recording into the
+ * caller's buffer: steps, velocity sets, forces, torques, impulses and
+ * joint break thresholds are recorded in the reference's record formats.
+ * End returns the byte count, or -1 after an overflow or after a call
+ * this path does not record (body, shape or joint creation). */
+M3GPU_API bool m3World_JournalBegin(m3WorldId worldId, void* buffer, int32_t capacity);
+M3GPU_API int32_t m3World_JournalEnd(m3WorldId worldId);
+
 /* world.c:3187 (world.h:606): replays a recorded command stream.  Steps
- * run on the GPU; velocity sets, forces, torques and impulses apply
- * between them.  The whole stream is validated first, so a refusal
+ * run on the GPU; velocity sets, forces, torques, impulses and joint
+ * break thresholds apply between them.  The whole stream is validated first, so a refusal
  * leaves the world untouched; other ops are refused with
  * M3GPU_ERR_UNSUPPORTED. */
 M3GPU_API bool m3World_JournalReplay(m3WorldId worldId, const void* data, int32_t size);

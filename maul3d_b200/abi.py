@@ -96,13 +96,24 @@ def journal_body_command(op: int, index1: int, generation: int, v) -> bytes:
     return struct.pack("<ii", op, len(payload)) + payload
 
 
+OP_JOINT_SET_BREAK = 55
+
+
+def journal_joint_break(index1: int, generation: int, max_force: float, max_torque: float) -> bytes:
+    """One joint threshold record: {m3JointId id; float maxForce, maxTorque} (world.c:3111)."""
+    payload = struct.pack("<iHHff", index1, 0, generation, max_force, max_torque)
+    return struct.pack("<ii", OP_JOINT_SET_BREAK, len(payload)) + payload
+
+
 def bind_snapshot(lib: C.CDLL) -> C.CDLL:
     """Declare the snapshot, restore and journal entry points a handle has."""
     for name, args, res in (("m3World_SnapshotSize", [m3WorldId], C.c_int32),
                             ("m3World_Snapshot", [m3WorldId, C.c_void_p, C.c_int32], C.c_int32),
                             ("m3World_Restore", [m3WorldId, C.c_void_p, C.c_int32], C.c_bool),
                             ("m3World_JournalReplay", [m3WorldId, C.c_void_p, C.c_int32],
-                             C.c_bool)):
+                             C.c_bool),
+                            ("m3World_JournalBegin", [m3WorldId, C.c_void_p, C.c_int32], C.c_bool),
+                            ("m3World_JournalEnd", [m3WorldId], C.c_int32)):
         try:
             fn = getattr(lib, name)
         except AttributeError:

@@ -4,6 +4,7 @@
 
 #include "m3_world.h"
 #include "m3_hash.h"
+#include "m3_ops.h"
 
 #include <cuda_runtime.h>
 
@@ -52,6 +53,20 @@ extern "C" uint64_t m3Hash64(uint64_t h, const void* bytes, int32_t count)
     return m3Fnv(h, bytes, count);
 }
 
+// solver.c:4332-4354: a step is recorded after it ran ({dt, substeps}).
+static void RecordSteps(m3HostWorld* w, float dt, int32_t substeps, int32_t steps)
+{
+    struct
+    {
+        float dt;
+        int32_t substeps;
+    } record = {dt, substeps};
+    for (int32_t k = 0; k < steps && w->journalActive; ++k)
+    {
+        m3JournalAppend(w, M3_OP_STEP, &record, (int32_t)sizeof(record));
+    }
+}
+
 extern "C" void m3World_Step(m3WorldId worldId, float dt, int32_t substeps)
 {
     m3gpuClearError();
@@ -61,7 +76,10 @@ extern "C" void m3World_Step(m3WorldId worldId, float dt, int32_t substeps)
         m3gpuSetError(M3GPU_ERR_INVALID, "m3World_Step: stale world or invalid dt/substeps");
         return;
     }
-    m3gpuStepBatch(&w, 1, dt, substeps, 1);
+    if (m3gpuStepBatch(&w, 1, dt, substeps, 1) == M3GPU_OK)
+    {
+        RecordSteps(w, dt, substeps, 1);
+    }
 }
 
 extern "C" uint64_t m3World_Hash(m3WorldId worldId)
@@ -122,7 +140,15 @@ extern "C" int32_t m3gpu_step_worlds(const m3WorldId* worlds, int32_t count, flo
     {
         return M3GPU_OK;
     }
-    return m3gpuStepBatch(ws.data(), count, dt, substeps, steps);
+    rc = m3gpuStepBatch(ws.data(), count, dt, substeps, steps);
+    if (rc == M3GPU_OK)
+    {
+        for (m3HostWorld* w : ws)
+        {
+            RecordSteps(w, dt, substeps, steps);
+        }
+    }
+    return rc;
 }
 
 extern "C" int32_t m3gpu_hash_worlds(const m3WorldId* worlds, int32_t count, uint64_t* out)

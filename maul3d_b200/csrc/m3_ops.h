@@ -18,6 +18,7 @@ enum
     M3_OP_APPLY_TORQUE = 27,
     M3_OP_APPLY_LINEAR_IMPULSE = 28,
     M3_OP_APPLY_ANGULAR_IMPULSE = 29,
+    M3_OP_JOINT_SET_BREAK = 55,
 };
 
 // One command for the device kernel: `world` indexes the batch, `body`
@@ -29,6 +30,12 @@ typedef struct m3BodyOp
     int32_t body;
     m3Vec3 v;
 } m3BodyOp;
+
+// Joint commands ride the same record: `body` is then the joint slot.
+M3_HD bool m3IsJointOp(int32_t op)
+{
+    return op == M3_OP_JOINT_SET_BREAK;
+}
 
 M3_HD bool m3IsBodyOp(int32_t op)
 {
@@ -97,6 +104,23 @@ M3_HD void m3ApplyBodyOp(const m3WorldView& w, int32_t op, int32_t body, m3Vec3 
         w.w[body] = m3Add3(w.w[body], m3MulMV3(m3WorldInvInertiaHD(w, body), v));
         m3WakeOnCommand(w, body, v);
         break;
+    case M3_OP_JOINT_SET_BREAK:
+    {
+        // joint.c:626-630, 548-560: thresholds (maxForce, maxTorque), then
+        // the joint's dynamic bodies wake.
+        const int32_t j = body;
+        w.jbreak[j] = v3(v.x, v.y, 0.0f);
+        const int32_t ends[2] = {w.jbodyA[j], w.jbodyB[j]};
+        for (int32_t k = 0; k < 2; ++k)
+        {
+            if (ends[k] >= 0 && w.btype[ends[k]] == M3_BODY_DYNAMIC)
+            {
+                w.awake[ends[k]] = 1;
+                w.sleepTime[ends[k]] = 0.0f;
+            }
+        }
+        break;
+    }
     default:
         break;
     }

@@ -151,6 +151,13 @@ struct m3HostWorld
     std::vector<uint8_t> snapshotCarry;
     std::vector<uint8_t> snapshotHeaderCarry;
     std::vector<float> heightFieldCellCarry;
+    // Journal recording (world.c:1348-1398): records appended to the
+    // caller's buffer while active; overflow latches and ends it.
+    uint8_t* journalBuffer = nullptr;
+    int32_t journalCapacity = 0;
+    int32_t journalCursor = 0;
+    bool journalActive = false;
+    bool journalOverflow = false;
     // Capacities of the pools this path does not model; they size the
     // snapshot's blocks (snapshot.c:161-600).
     int32_t meshCap = 0;
@@ -205,15 +212,22 @@ int32_t m3gpuSyncHost(m3HostWorld* w);
 struct m3JournalRecordView
 {
     int32_t op;
-    int32_t body;
-    m3Vec3 v;
+    int32_t body; // body slot, or joint slot for a joint record
+    m3Vec3 v;     // command vector, or (maxForce, maxTorque) of a joint record
     float dt;
     int32_t substeps;
+    uint16_t generation; // joint records
 };
 // Parses and validates a whole journal against a world's bodies; false
 // (with the error set) on the first bad or unsupported record.
 bool m3ParseJournal(const m3HostWorld* w, const uint8_t* stream, int32_t size,
                     std::vector<m3JournalRecordView>* out);
+
+// Appends one record to the world's active journal (snapshot.cpp).
+void m3JournalAppend(m3HostWorld* w, int32_t op, const void* payload, int32_t bytes);
+// Ends an active journal as unrecordable: a call this path cannot record
+// happened during the session (snapshot.cpp).
+void m3JournalUnrecordable(m3HostWorld* w);
 
 // Queue the joint slots the device freed since the last call (world.cpp).
 void m3DrainBrokenJoints(m3HostWorld* w);

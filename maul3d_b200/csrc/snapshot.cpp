@@ -1000,6 +1000,29 @@ bool m3ParseJournal(const m3HostWorld* w, const uint8_t* stream, int32_t size,
             }
             r.body = index;
         }
+        else if (op == M3_OP_JOINT_SET_BREAK)
+        {
+            // world.c:3111-3133: {m3JointId id; float maxForce, maxTorque}.
+            if (bytes != 16)
+            {
+                m3gpuSetError(M3GPU_ERR_INVALID, "journal: bad joint break record");
+                return false;
+            }
+            m3JointId id;
+            memcpy(&id, payload, 8);
+            memcpy(&r.v.x, payload + 8, 4);
+            memcpy(&r.v.y, payload + 12, 4);
+            const int32_t j = id.index1 - 1;
+            if (j < 0 || j >= w->hv.sc->jointMax || w->hv.jointAlive[j] == 0 ||
+                w->hv.jointGen[j] != id.generation || !isfinite(r.v.x) || !isfinite(r.v.y) ||
+                r.v.x < 0.0f || r.v.y < 0.0f)
+            {
+                m3gpuSetError(M3GPU_ERR_INVALID, "journal: stale joint or bad thresholds");
+                return false;
+            }
+            r.body = j;
+            r.generation = id.generation;
+        }
         else if (op <= 0)
         {
             m3gpuSetError(M3GPU_ERR_INVALID, "journal: unknown op %d", op);
@@ -1013,4 +1036,71 @@ bool m3ParseJournal(const m3HostWorld* w, const uint8_t* stream, int32_t size,
         out->push_back(r);
     }
     return true;
+}
+
+void m3JournalAppend(m3HostWorld* w, int32_t op, const void* payload, int32_t bytes)
+{
+    if (!w->journalActive)
+    {
+        return;
+    }
+    const int64_t need = 8 + (int64_t)bytes;
+    if (w->journalCursor + need > w->journalCapacity)
+    {
+        w->journalOverflow = true;
+        w->journalActive = false;
+        return;
+    }
+    uint8_t* out = w->journalBuffer + w->journalCursor;
+    memcpy(out, &op, 4);
+    memcpy(out + 4, &bytes, 4);
+    memcpy(out + 8, payload, (size_t)bytes);
+    w->journalCursor += (int32_t)need;
+}
+
+void m3JournalUnrecordable(m3HostWorld* w)
+{
+    if (w->journalActive)
+    {
+        w->journalOverflow = true;
+        w->journalActive = false;
+    }
+}
+
+// world.c:1369-1382 (world.h:600): starts recording into the caller's
+// buffer; false for a stale id, a null or tiny buffer, or a session
+// already running.
+extern "C" bool m3World_JournalBegin(m3WorldId worldId, void* buffer, int32_t capacity)
+{
+    m3gpuClearError();
+    m3HostWorld* w = m3gpuWorldFromId(worldId);
+    if (w == nullptr || buffer == nullptr || capacity < 8 || w->journalActive)
+    {
+        return false;
+    }
+    w->journalBuffer = (uint8_t*)buffer;
+    w->journalCapacity = capacity;
+    w->journalCursor = 0;
+    w->journalActive = true;
+    w->journalOverflow = false;
+    return true;
+}
+
+// world.c:1384-1398 (world.h:601): ends the session; the recorded byte
+// count, or -1 after an overflow (or, here, after a call this path does
+// not record: world, body, shape or joint creation).
+extern "C" int32_t m3World_JournalEnd(m3WorldId worldId)
+{
+    m3HostWorld* w = m3gpuWorldFromId(worldId);
+    if (w == nullptr)
+    {
+        return -1;
+    }
+    const int32_t bytes = w->journalOverflow ? -1 : w->journalCursor;
+    w->journalBuffer = nullptr;
+    w->journalCapacity = 0;
+    w->journalCursor = 0;
+    w->journalActive = false;
+    w->journalOverflow = false;
+    return bytes;
 }

@@ -414,7 +414,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3LeafBoxKernel(const m3WorldView* v
 // only a snapshot reads, so this runs on its own low-priority stream
 // beside the following steps, up to M3_TREE_LAG steps behind (the move
 // lists sit in a ring of that depth).
-#define M3_TREE_WORLDS_PER_BLOCK 4
+#define M3_TREE_WORLDS_PER_BLOCK 1
 __global__ void __launch_bounds__(32 * M3_TREE_WORLDS_PER_BLOCK)
     m3TreeKernel(const m3WorldView* views, const int32_t* order, int32_t count, int32_t slot,
                  int32_t treeLag)
@@ -2995,7 +2995,8 @@ __global__ void __launch_bounds__(M3_BLOCK) m3BodyOpKernel(const m3WorldView* vi
     for (int32_t k = offsets[wi]; k < offsets[wi + 1]; ++k)
     {
         const m3BodyOp o = ops[k];
-        if (o.body >= 0 && o.body < w.sc->bodyMax)
+        const int32_t slots = m3IsJointOp(o.op) ? w.sc->jointMax : w.sc->bodyMax;
+        if (o.body >= 0 && o.body < slots)
         {
             m3ApplyBodyOp(w, o.op, o.body, o.v);
         }

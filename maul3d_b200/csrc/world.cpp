@@ -340,6 +340,7 @@ extern "C" m3BodyId m3CreateBody(m3WorldId worldId, const m3BodyDef* def)
     v.shapeHead[i] = -1;
     v.jointHead[i] = -1;
     w->hostDirty = true;
+    m3JournalUnrecordable(w); // creation is not recorded by this path
     m3BodyId id = {i + 1, (uint16_t)w->slot, v.bodyGen[i]};
     return id;
 }
@@ -407,6 +408,12 @@ static void BodyCommand(m3BodyId id, int32_t op, m3Vec3 v, bool needsMass)
     {
         return;
     }
+    struct
+    {
+        m3BodyId id;
+        m3Vec3 v;
+    } record = {id, v};
+    m3JournalAppend(w, op, &record, (int32_t)sizeof(record));
     m3ApplyBodyOp(w->hv, op, index, v);
     w->hostDirty = true;
 }
@@ -940,6 +947,7 @@ static m3ShapeId CreateShapeCommon(m3BodyId bodyId, const m3ShapeDef* def, uint8
     }
     RecomputeMass(w, b);
     w->hostDirty = true;
+    m3JournalUnrecordable(w); // creation is not recorded by this path
     m3ShapeId id = {s + 1, (uint16_t)w->slot, v.shapeGen[s]};
     return id;
 }
@@ -1231,6 +1239,7 @@ extern "C" m3JointId m3CreateJoint(const m3JointDef* def)
         v.sleepTime[b] = 0.0f;
     }
     w->hostDirty = true;
+    m3JournalUnrecordable(w); // creation is not recorded by this path
     m3JointId id = {j + 1, (uint16_t)w->slot, v.jointGen[j]};
     return id;
 }
@@ -1276,17 +1285,14 @@ extern "C" void m3Joint_SetBreakThresholds(m3JointId jointId, float maxForce, fl
     {
         return;
     }
-    v.jbreak[j] = v3(maxForce, maxTorque, 0.0f);
-    const int32_t bodies[2] = {v.jbodyA[j], v.jbodyB[j]};
-    for (int32_t k = 0; k < 2; ++k)
+    struct
     {
-        const int32_t b = bodies[k];
-        if (b >= 0 && v.btype[b] == M3_BODY_DYNAMIC)
-        {
-            v.awake[b] = 1;
-            v.sleepTime[b] = 0.0f;
-        }
-    }
+        m3JointId id;
+        float maxForce;
+        float maxTorque;
+    } record = {jointId, maxForce, maxTorque};
+    m3JournalAppend(w, M3_OP_JOINT_SET_BREAK, &record, (int32_t)sizeof(record));
+    m3ApplyBodyOp(v, M3_OP_JOINT_SET_BREAK, j, v3(maxForce, maxTorque, 0.0f));
     w->hostDirty = true;
 }
 

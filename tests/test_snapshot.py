@@ -7,6 +7,7 @@ reference's arithmetic (body.c:351-418, world.c:2283-2321); stepping
 journals run on the GPU (tests/test_serving_gpu.py).
 """
 import ctypes as C
+import struct
 
 import numpy as np
 import pytest
@@ -213,3 +214,68 @@ def test_restored_world_snapshots_the_same_bytes(m3, oracle, libs, scene, seed, 
     assert _snapshot(ours, g.id) == snap
     small = (C.c_uint8 * 16)()
     assert ours.m3World_Snapshot(g.id, small, 16) == -1
+
+
+def _record_session(lib, wid, joints=()):
+    """Body commands and joint thresholds on one world, recorded."""
+    buf = (C.c_uint8 * 4096)()
+    assert lib.m3World_JournalBegin(wid, buf, 4096)
+    w0 = wid.index1 - 1
+    for k in range(6):
+        b = abi.m3BodyId(3 + k, w0, 0)
+        lib.m3Body_ApplyLinearImpulse(b, abi.m3Vec3(1.5 * k, 2.0, -0.5))
+        lib.m3Body_ApplyAngularImpulse(b, abi.m3Vec3(0.1, -0.2 * k, 0.3))
+        lib.m3Body_SetLinearVelocity(b, abi.m3Vec3(0.0, 0.5 * k, 0.0))
+        lib.m3Body_ApplyForce(b, abi.m3Vec3(3.0, 0.0, 1.0))
+        lib.m3Body_ApplyTorque(b, abi.m3Vec3(0.0, 1.0, 0.0))
+        lib.m3Body_SetAngularVelocity(b, abi.m3Vec3(0.2, 0.0, 0.1))
+    lib.m3Body_ApplyLinearImpulse(abi.m3BodyId(1, w0, 0), abi.m3Vec3(1.0, 1.0, 1.0))  # static: no-op
+    for j in joints:
+        lib.m3Joint_SetBreakThresholds(abi.m3JointId(j, w0, 0), 300.0, 50.0)
+    n = lib.m3World_JournalEnd(wid)
+    assert n > 0
+    return bytes(buf[:n])
+
+
+def _without_world_index(journal: bytes) -> bytes:
+    """The records with the recording world's index (the world0 half of
+    every body or joint id, which replay retargets) cleared."""
+    out = bytearray(journal)
+    cursor = 0
+    while cursor < len(out):
+        op, n = struct.unpack_from("<ii", out, cursor)
+        if op != abi.OP_STEP:
+            out[cursor + 12:cursor + 14] = b"\0\0"
+        cursor += 8 + n
+    return bytes(out)
+
+
+def test_recorded_journals_are_the_references_bytes(m3, oracle, libs):
+    ours, ref = libs
+    g = m3.World.scene(SCENE_TOWERS, 7, 2)
+    r = oracle.RefWorld.scene(SCENE_TOWERS, 7, 2)
+    a = _record_session(ours, g.id, joints=(1, 5, 9))
+    b = _record_session(ref, r.id, joints=(1, 5, 9))
+    assert _without_world_index(a) == _without_world_index(b)
+    assert g.hash() == r.hash()
+    # Our recording replays in the reference, and the reference's in ours.
+    g2 = m3.World.scene(SCENE_TOWERS, 7, 2)
+    r2 = oracle.RefWorld.scene(SCENE_TOWERS, 7, 2)
+    assert _replay(ours, g2.id, b) and _replay(ref, r2.id, a)
+    assert g2.hash() == r2.hash() == r.hash()
+
+
+def test_creation_during_a_recording_ends_it_unrecordable(m3, libs):
+    ours, _ = libs
+    g = m3.World.scene(SCENE_UNEVEN, 1, 32)
+    buf = (C.c_uint8 * 1024)()
+    assert ours.m3World_JournalBegin(g.id, buf, 1024)
+    assert not ours.m3World_JournalBegin(g.id, buf, 1024)  # one session at a time
+    bd = ours.m3DefaultBodyDef()
+    ours.m3CreateBody(g.id, C.byref(bd))
+    assert ours.m3World_JournalEnd(g.id) == -1
+    # Overflow ends a session the same way.
+    small = (C.c_uint8 * 16)()
+    assert ours.m3World_JournalBegin(g.id, small, 16)
+    ours.m3Body_ApplyLinearImpulse(abi.m3BodyId(3, g.id.index1 - 1, 0), abi.m3Vec3(1.0, 0.0, 0.0))
+    assert ours.m3World_JournalEnd(g.id) == -1
