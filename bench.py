@@ -67,11 +67,13 @@ SCENE_UNEVEN = 2
 # velocities 141 B + integrate positions 173 B; per contact row per
 # substep 3 passes x (456 B record + 2 x 48 B v,w + 2 x 28 B dp,dq); per
 # joint row per substep 3 x (472 + 152).
-# DRAM bytes (read + write) of one m3SubstepKernel launch on the default
-# workload, from ncu (dram__bytes_read.sum + dram__bytes_write.sum, one
-# pass; profiles/m3SubstepKernel_uneven296x1024.txt gives the command).
-# Reported only for that workload.
-SUBSTEP_TRAFFIC_DEFAULT = 3.70e9 + 0.967e9
+# DRAM bytes (read + write) of one step's m3SubstepKernel launches (the
+# three size classes) on the default workload, from ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum, one pass each;
+# profiles/m3SubstepKernel_uneven4096.txt gives the command):
+# 875.0 + 345.2 MB (512-thread class), 342.7 + 130.1 MB (256), 79.8 +
+# 95.9 MB (128).  Reported for that workload only.
+SUBSTEP_TRAFFIC_DEFAULT = (875.0 + 345.2 + 342.7 + 130.1 + 79.8 + 95.9) * 1e6
 BYTES_PER_MOVER_SUBSTEP = 314
 BYTES_PER_CONTACT_SUBSTEP = 3 * (456 + 2 * 48 + 2 * 28)
 BYTES_PER_JOINT_SUBSTEP = 3 * (472 + 152)
@@ -449,7 +451,8 @@ def main() -> None:
     roofline = {"kernel": "m3SubstepKernel", "bound": "hbm", "achieved": achieved,
                 "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": SUBSTEP_TRAFFIC_DEFAULT if default_workload(args) else None,
-                "traffic_source": "ncu dram bytes of one launch on this workload",
+                "traffic_source": "ncu dram bytes of one step's three size-class launches on "
+                                  "this workload",
                 "bytes_per_launch": sub_bytes / args.steps,
                 "launch_ms": kms / args.steps,
                 "share": {k: v / ms for k, v in stage_ms.items()}}

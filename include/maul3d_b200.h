@@ -448,6 +448,12 @@ M3GPU_API int32_t m3gpu_serve_poll(m3gpuServer* server, int64_t* tickets, uint64
                                    int32_t* status, int32_t capacity);
 M3GPU_API int32_t m3gpu_serve_active(const m3gpuServer* server);
 
+/* White-box test hook: one broadphase tree move on the host image (remove
+ * the shape's leaf, insert [lo, hi]), as the step's tree refresh makes
+ * it; the new leaf or -1. */
+M3GPU_API int32_t m3gpu_tree_move(m3WorldId world, int32_t shape, const double* lo,
+                                  const double* hi);
+
 #ifdef __cplusplus
 }
 #endif

@@ -214,28 +214,74 @@ M3_HD m3TreeNode m3TreeRotate(m3TreeRef t, const Store& st, int32_t a, m3TreeNod
 // bounds (dynamic_tree.c:205-219).  The balance test reads the node's
 // stored height, as the reference's does before its refit; after a
 // rotation the risen node's height and bounds are already what the
-// refit would compute (the union of its two children, in order).  A
-// walk longer than the node count can only come from a malformed tree;
-// it stops there.
-template <class Store> M3_HD void m3TreeRefit(m3TreeRef t, const Store& st, int32_t index)
+// refit would compute (the union of its two children, in order).
+// `from`, when not M3_TREE_NULL, is a child of `index` whose current
+// record is `fromRec`: the walk carries each level's record up to the
+// next instead of reading it again, and asks for the parent's record
+// before the level's arithmetic, so a level waits on one load (the
+// other child).  A walk longer than the node count can only come from a
+// malformed tree; it stops there.
+template <class Store>
+M3_HD void m3TreeRefit(m3TreeRef t, const Store& st, int32_t index, int32_t from,
+                       m3TreeNode fromRec)
 {
-    for (int32_t guard = 0; index != M3_TREE_NULL && guard < t.capacity; ++guard)
+    if (index == M3_TREE_NULL)
     {
-        m3TreeNode n = st.Get(index);
-        const m3TreeNode c1 = st.Get(n.child1);
-        const m3TreeNode c2 = st.Get(n.child2);
+        return;
+    }
+    m3TreeNode n = st.Get(index);
+    for (int32_t guard = 0; guard < t.capacity; ++guard)
+    {
+        m3TreeNode c1;
+        m3TreeNode c2;
+        if (n.child1 == from)
+        {
+            c1 = fromRec;
+            c2 = st.Get(n.child2);
+        }
+        else if (n.child2 == from)
+        {
+            c1 = st.Get(n.child1);
+            c2 = fromRec;
+        }
+        else
+        {
+            c1 = st.Get(n.child1);
+            c2 = st.Get(n.child2);
+        }
+        const int32_t up = n.parent;
+        m3TreeNode upRec = n;
+        if (up != M3_TREE_NULL)
+        {
+            upRec = st.Get(up);
+        }
         const int32_t balance = c2.height - c1.height;
         if (n.height >= 2 && n.child1 != M3_TREE_NULL && (balance > 1 || balance < -1))
         {
             int32_t root = index;
-            n = m3TreeRotate(t, st, index, n, c1, c2, &root);
-            index = n.parent;
+            const m3TreeNode risen = m3TreeRotate(t, st, index, n, c1, c2, &root);
+            if (risen.parent == M3_TREE_NULL)
+            {
+                return;
+            }
+            // The rotation re-linked the parent's child: read it again.
+            from = root;
+            fromRec = risen;
+            index = risen.parent;
+            n = st.Get(index);
             continue;
         }
         n.height = 1 + m3TreeMaxI(c1.height, c2.height);
         m3TreeUnion(c1.lo, c1.hi, c2.lo, c2.hi, n.lo, n.hi);
         st.Put(index, n);
-        index = n.parent;
+        if (up == M3_TREE_NULL)
+        {
+            return;
+        }
+        from = index;
+        fromRec = n;
+        index = up;
+        n = upRec;
     }
 }
 
@@ -280,47 +326,74 @@ M3_HD int32_t m3TreeInsert(m3TreeRef t, const Store& st, const double lo[3], con
         curUnion = m3TreeArea(ulo, uhi);
         curArea = m3TreeArea(cur.lo, cur.hi);
     }
-    for (int32_t guard = 0; cur.height > 0; ++guard)
+    if (cur.height > 0)
     {
-        if (guard >= t.capacity)
+        m3TreeNode n1 = st.Get(cur.child1);
+        m3TreeNode n2 = st.Get(cur.child2);
+        for (int32_t guard = 0;; ++guard)
         {
-            return M3_TREE_NULL;
-        }
-        const int32_t c1 = cur.child1;
-        const int32_t c2 = cur.child2;
-        const m3TreeNode n1 = st.Get(c1);
-        const m3TreeNode n2 = st.Get(c2);
-        const double here = 2.0 * curUnion;
-        const double inherited = 2.0 * (curUnion - curArea);
-        double ulo[3];
-        double uhi[3];
-        m3TreeUnion(n1.lo, n1.hi, lo, hi, ulo, uhi);
-        const double union1 = m3TreeArea(ulo, uhi);
-        const double area1 = n1.height == 0 ? 0.0 : m3TreeArea(n1.lo, n1.hi);
-        m3TreeUnion(n2.lo, n2.hi, lo, hi, ulo, uhi);
-        const double union2 = m3TreeArea(ulo, uhi);
-        const double area2 = n2.height == 0 ? 0.0 : m3TreeArea(n2.lo, n2.hi);
-        // dynamic_tree.c:245-273: a leaf child's cost is its union's area
-        // plus the inherited cost; an internal child's subtracts its area.
-        const double cost1 = n1.height == 0 ? union1 + inherited : union1 - area1 + inherited;
-        const double cost2 = n2.height == 0 ? union2 + inherited : union2 - area2 + inherited;
-        if (here < cost1 && here < cost2)
-        {
-            break;
-        }
-        if (cost1 < cost2)
-        {
-            index = c1;
-            cur = n1;
-            curUnion = union1;
-            curArea = area1; // a leaf ends the descent: its area is not read
-        }
-        else
-        {
-            index = c2;
-            cur = n2;
-            curUnion = union2;
-            curArea = area2;
+            if (guard >= t.capacity)
+            {
+                return M3_TREE_NULL;
+            }
+            // Ask for the grandchildren before the arithmetic that picks
+            // between them: the next level's loads then overlap this
+            // level's work.
+            m3TreeNode g11 = n1;
+            m3TreeNode g12 = n1;
+            m3TreeNode g21 = n2;
+            m3TreeNode g22 = n2;
+            if (n1.height > 0)
+            {
+                g11 = st.Get(n1.child1);
+                g12 = st.Get(n1.child2);
+            }
+            if (n2.height > 0)
+            {
+                g21 = st.Get(n2.child1);
+                g22 = st.Get(n2.child2);
+            }
+            const double here = 2.0 * curUnion;
+            const double inherited = 2.0 * (curUnion - curArea);
+            double ulo[3];
+            double uhi[3];
+            m3TreeUnion(n1.lo, n1.hi, lo, hi, ulo, uhi);
+            const double union1 = m3TreeArea(ulo, uhi);
+            const double area1 = n1.height == 0 ? 0.0 : m3TreeArea(n1.lo, n1.hi);
+            m3TreeUnion(n2.lo, n2.hi, lo, hi, ulo, uhi);
+            const double union2 = m3TreeArea(ulo, uhi);
+            const double area2 = n2.height == 0 ? 0.0 : m3TreeArea(n2.lo, n2.hi);
+            // dynamic_tree.c:245-273: a leaf child's cost is its union's
+            // area plus the inherited cost; an internal child's subtracts
+            // its own area.
+            const double cost1 = n1.height == 0 ? union1 + inherited : union1 - area1 + inherited;
+            const double cost2 = n2.height == 0 ? union2 + inherited : union2 - area2 + inherited;
+            if (here < cost1 && here < cost2)
+            {
+                break;
+            }
+            if (cost1 < cost2)
+            {
+                index = cur.child1;
+                cur = n1;
+                curUnion = union1;
+                curArea = area1;
+                n1 = g11;
+                n2 = g12;
+            }
+            else
+            {
+                index = cur.child2;
+                cur = n2;
+                curUnion = union2;
+                curArea = area2;
+                n1 = g21;
+                n2 = g22;
+            }
+            if (cur.height == 0)
+            {
+                break;
+            }
         }
     }
     // A new parent takes the sibling's place; sibling and leaf hang
@@ -347,7 +420,7 @@ M3_HD int32_t m3TreeInsert(m3TreeRef t, const Store& st, const double lo[3], con
     st.Put(parent, N);
     st.Put(sibling, S);
     st.Put(leaf, L);
-    m3TreeRefit(t, st, parent);
+    m3TreeRefit(t, st, parent, leaf, L);
     return leaf;
 }
 
@@ -372,7 +445,7 @@ template <class Store> M3_HD void m3TreeRemove(m3TreeRef t, const Store& st, int
         S.parent = grand;
         st.Put(sibling, S);
         m3TreeGiveNode(t, st, parent);
-        m3TreeRefit(t, st, grand);
+        m3TreeRefit(t, st, grand, sibling, S);
     }
     else
     {

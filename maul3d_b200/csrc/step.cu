@@ -411,9 +411,9 @@ __global__ void __launch_bounds__(M3_BLOCK) m3LeafBoxKernel(const m3WorldView* v
 // Broadphase tree refresh, second half (broad_phase.c:516-538): one warp
 // per world replays one step's moves in ascending shape order, each a
 // leaf removal and the insertion of its fat bounds.  The tree is state
-// only a snapshot reads, so this runs on its own low-priority stream
-// beside the following steps, up to M3_TREE_LAG steps behind (the move
-// lists sit in a ring of that depth).
+// only a snapshot reads, so this runs on its own stream beside the
+// following steps, up to M3_TREE_LAG steps behind (the move lists sit in
+// a ring of that depth).
 #define M3_TREE_WORLDS_PER_BLOCK 1
 __global__ void __launch_bounds__(32 * M3_TREE_WORLDS_PER_BLOCK)
     m3TreeKernel(const m3WorldView* views, const int32_t* order, int32_t count, int32_t slot,
@@ -2604,11 +2604,10 @@ static int32_t EnsureClassStreams()
     }
     if (e == cudaSuccess)
     {
-        // The lowest priority: the step's own kernels take free SMs first.
-        int least = 0;
-        int greatest = 0;
-        cudaDeviceGetStreamPriorityRange(&least, &greatest);
-        e = cudaStreamCreateWithPriority(&s_classStreams.tree, cudaStreamNonBlocking, least);
+        // Default priority: the tree's single-warp blocks then interleave
+        // with the step's kernels instead of waiting for idle SMs, which
+        // a busy batch never leaves.
+        e = cudaStreamCreateWithFlags(&s_classStreams.tree, cudaStreamNonBlocking);
     }
     if (e != cudaSuccess)
     {

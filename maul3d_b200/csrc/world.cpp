@@ -1296,6 +1296,30 @@ extern "C" void m3Joint_SetBreakThresholds(m3JointId jointId, float maxForce, fl
     w->hostDirty = true;
 }
 
+// White-box hook for the tests: one broadphase tree move on the host
+// image, as the step's tree kernel makes it (remove the shape's leaf,
+// insert `lo`..`hi`).  Returns the new leaf, or -1.
+extern "C" int32_t m3gpu_tree_move(m3WorldId worldId, int32_t shape, const double* lo,
+                                   const double* hi)
+{
+    m3HostWorld* w = m3gpuWorldFromId(worldId);
+    if (w == nullptr || lo == nullptr || hi == nullptr || m3gpuSyncHost(w) != M3GPU_OK)
+    {
+        return -1;
+    }
+    m3WorldView& v = w->hv;
+    if (shape < 0 || shape >= v.sc->shapeMax || v.proxyId[shape] == M3_TREE_NULL)
+    {
+        return -1;
+    }
+    const m3TreeRef tree = m3WorldTree(v);
+    const m3TreeArrayStore store{v.treeNodes};
+    m3TreeRemove(tree, store, v.proxyId[shape]);
+    v.proxyId[shape] = m3TreeInsert(tree, store, lo, hi, shape);
+    w->hostDirty = true;
+    return v.proxyId[shape];
+}
+
 extern "C" bool m3Joint_IsValid(m3JointId jointId)
 {
     m3HostWorld* w = m3gpuWorldFromIndex0(jointId.world0);

@@ -279,3 +279,56 @@ def test_creation_during_a_recording_ends_it_unrecordable(m3, libs):
     assert ours.m3World_JournalBegin(g.id, small, 16)
     ours.m3Body_ApplyLinearImpulse(abi.m3BodyId(3, g.id.index1 - 1, 0), abi.m3Vec3(1.0, 0.0, 0.0))
     assert ours.m3World_JournalEnd(g.id) == -1
+
+
+def _tree_blocks(snap: bytes):
+    """(root, free list, proxy ids, nodes) of a snapshot: the header
+    cursors and the blocks after the pair keys (snapshot.c:243-247)."""
+    h = np.frombuffer(snap[:192], dtype=np.int32)
+    body_cap, shape_cap = int(h[6]), int(h[11])
+    per_body = 40 + 12 + 12 + 4 + 36 + 36 + 12 + 4 + 4 + 4 + 1 + 1 + 4 + 1 + 4 + 4 + 8 + 32 \
+        + 12 + 12 + 1 + 1 + 4 + 1 + 1 + 40
+    off = 192 + per_body * body_cap + 58 + (2 + 1 + 4 + 4) * body_cap
+    off += (4 + 1 + 32 + 4 + 4 + 4 + 8 + 4 + 2 + 1 + 4) * shape_cap + 8 * 8 * shape_cap
+    proxies = np.frombuffer(snap[off:off + 4 * shape_cap], dtype=np.int32)
+    nodes = np.frombuffer(snap[off + 4 * shape_cap:off + 4 * shape_cap + 144 * shape_cap],
+                          dtype=np.uint8).reshape(2 * shape_cap, 72)
+    return int(h[17]), int(h[18]), proxies, nodes
+
+
+def test_tree_moves_on_the_host_rebuild_the_references_tree(m3, oracle, libs):
+    # Each reference step reinserts the leaves its shapes escaped, in
+    # shape order (broad_phase.c:500-539).  Read those moves off two
+    # consecutive reference snapshots and make them with this library's
+    # tree code on the restored earlier one: the tree must come out as
+    # the reference's, byte for byte (removals, insertions, rotations).
+    ours, ref = libs
+    m3.lib.m3gpu_tree_move.argtypes = [abi.m3WorldId, C.c_int32, C.c_void_p, C.c_void_p]
+    m3.lib.m3gpu_tree_move.restype = C.c_int32
+    r = oracle.RefWorld.scene(SCENE_UNEVEN, 9, 300)
+    g = m3.World.scene(SCENE_UNEVEN, 9, 300)
+    total = 0
+    before = _snapshot(ref, r.id)
+    for step in range(12):
+        r.step(1.0 / 60.0, 4, 1)
+        after = _snapshot(ref, r.id)
+        _, _, p0, n0 = _tree_blocks(before)
+        root1, free1, p1, n1 = _tree_blocks(after)
+        assert _restore(ours, g.id, before)
+        for shape in range(len(p1)):
+            if p1[shape] < 0:
+                continue
+            old = n0[p0[shape]][:48].tobytes()
+            new = n1[p1[shape]][:48].tobytes()
+            if old != new or p0[shape] != p1[shape]:
+                bounds = np.frombuffer(new, dtype=np.float64)
+                lo = np.ascontiguousarray(bounds[:3])
+                hi = np.ascontiguousarray(bounds[3:])
+                assert m3.lib.m3gpu_tree_move(g.id, shape, lo.ctypes.data, hi.ctypes.data) >= 0
+                total += 1
+        root, free, p, n = _tree_blocks(_snapshot(ours, g.id))
+        assert (root, free) == (root1, free1), f"step {step + 1}"
+        assert np.array_equal(p, p1), f"step {step + 1}"
+        assert np.array_equal(n, n1), f"step {step + 1}"
+        before = after
+    assert total > 100
