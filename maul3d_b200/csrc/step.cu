@@ -2833,8 +2833,18 @@ static int32_t s_narrowGrid = 148 * 16;
 // The narrowphase of one step: family count and scatter, then one
 // kernel per covered family over its bucket.
 #define M3_NARROW_LAUNCHES (2 + M3F_UNSUPPORTED)
+// Batches of at most this many worlds take the single narrowphase kernel.
+#define M3_NARROW_SMALL_BATCH 4
+
 static void LaunchNarrow(const m3WorldView* views, const int32_t* offsets, int32_t count)
 {
+    if (count <= M3_NARROW_SMALL_BATCH)
+    {
+        // A handful of worlds: one kernel over every family beats the
+        // bucketing's nine launches.
+        m3NarrowKernel<<<148, 128>>>(views, offsets, count);
+        return;
+    }
     int32_t* blockHist = s_batch.dfamily;
     int32_t* famStart = s_batch.dfamily + M3_FAMILY_BLOCKS * M3F_COUNT;
     const int32_t* bucket = s_batch.dbucket;
@@ -3159,7 +3169,7 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
         LaunchSolve(s_batch.dviews, s_batch.dorder, count, dt, substeps, s_batch.cacheBytes,
                     ev + 2, s_batch.classFirst, s_batch.classCache);
         cudaEventRecord(ev[4]);
-        s_launches += 5 + M3_NARROW_LAUNCHES;
+        s_launches += 5 + (count <= M3_NARROW_SMALL_BATCH ? 1 : M3_NARROW_LAUNCHES);
     }
     if (anyTracked && steps > 0)
     {
