@@ -339,10 +339,11 @@ M3_HD int32_t m3TreeInsert(m3TreeRef t, const Store& st, const double lo[3], con
             // Ask for the grandchildren before the arithmetic that picks
             // between them: the next level's loads then overlap this
             // level's work.
-            m3TreeNode g11 = n1;
-            m3TreeNode g12 = n1;
-            m3TreeNode g21 = n2;
-            m3TreeNode g22 = n2;
+            // (A leaf's slots stay unread: choosing a leaf ends the walk.)
+            m3TreeNode g11;
+            m3TreeNode g12;
+            m3TreeNode g21;
+            m3TreeNode g22;
             if (n1.height > 0)
             {
                 g11 = st.Get(n1.child1);
