@@ -314,7 +314,10 @@ M3_HD int32_t m3TreeInsert(m3TreeRef t, const Store& st, const double lo[3], con
     // level per node: a longer descent means a malformed tree).  The
     // chosen child's record, its own area and the area of its union
     // with the new box (both computed for its cost) are carried down,
-    // so each level loads and measures only the two children.
+    // so each level loads and measures only the two children.  (Asking
+    // for the grandchildren before choosing hid the loads but doubled the
+    // instructions, and the walk runs beside the step's own kernels,
+    // where instructions cost more than latency.)
     int32_t index = *t.root;
     m3TreeNode cur = st.Get(index);
     double curUnion;
@@ -326,75 +329,48 @@ M3_HD int32_t m3TreeInsert(m3TreeRef t, const Store& st, const double lo[3], con
         curUnion = m3TreeArea(ulo, uhi);
         curArea = m3TreeArea(cur.lo, cur.hi);
     }
-    if (cur.height > 0)
+    for (int32_t guard = 0; cur.height > 0; ++guard)
     {
-        m3TreeNode n1 = st.Get(cur.child1);
-        m3TreeNode n2 = st.Get(cur.child2);
-        for (int32_t guard = 0;; ++guard)
+        if (guard >= t.capacity)
         {
-            if (guard >= t.capacity)
-            {
-                return M3_TREE_NULL;
-            }
-            // Ask for the grandchildren before the arithmetic that picks
-            // between them: the next level's loads then overlap this
-            // level's work.
-            // (A leaf's slots stay unread: choosing a leaf ends the walk.)
-            m3TreeNode g11;
-            m3TreeNode g12;
-            m3TreeNode g21;
-            m3TreeNode g22;
-            if (n1.height > 0)
-            {
-                g11 = st.Get(n1.child1);
-                g12 = st.Get(n1.child2);
-            }
-            if (n2.height > 0)
-            {
-                g21 = st.Get(n2.child1);
-                g22 = st.Get(n2.child2);
-            }
-            const double here = 2.0 * curUnion;
-            const double inherited = 2.0 * (curUnion - curArea);
-            double ulo[3];
-            double uhi[3];
-            m3TreeUnion(n1.lo, n1.hi, lo, hi, ulo, uhi);
-            const double union1 = m3TreeArea(ulo, uhi);
-            const double area1 = n1.height == 0 ? 0.0 : m3TreeArea(n1.lo, n1.hi);
-            m3TreeUnion(n2.lo, n2.hi, lo, hi, ulo, uhi);
-            const double union2 = m3TreeArea(ulo, uhi);
-            const double area2 = n2.height == 0 ? 0.0 : m3TreeArea(n2.lo, n2.hi);
-            // dynamic_tree.c:245-273: a leaf child's cost is its union's
-            // area plus the inherited cost; an internal child's subtracts
-            // its own area.
-            const double cost1 = n1.height == 0 ? union1 + inherited : union1 - area1 + inherited;
-            const double cost2 = n2.height == 0 ? union2 + inherited : union2 - area2 + inherited;
-            if (here < cost1 && here < cost2)
-            {
-                break;
-            }
-            if (cost1 < cost2)
-            {
-                index = cur.child1;
-                cur = n1;
-                curUnion = union1;
-                curArea = area1;
-                n1 = g11;
-                n2 = g12;
-            }
-            else
-            {
-                index = cur.child2;
-                cur = n2;
-                curUnion = union2;
-                curArea = area2;
-                n1 = g21;
-                n2 = g22;
-            }
-            if (cur.height == 0)
-            {
-                break;
-            }
+            return M3_TREE_NULL;
+        }
+        const int32_t c1 = cur.child1;
+        const int32_t c2 = cur.child2;
+        const m3TreeNode n1 = st.Get(c1);
+        const m3TreeNode n2 = st.Get(c2);
+        const double here = 2.0 * curUnion;
+        const double inherited = 2.0 * (curUnion - curArea);
+        double ulo[3];
+        double uhi[3];
+        m3TreeUnion(n1.lo, n1.hi, lo, hi, ulo, uhi);
+        const double union1 = m3TreeArea(ulo, uhi);
+        const double area1 = n1.height == 0 ? 0.0 : m3TreeArea(n1.lo, n1.hi);
+        m3TreeUnion(n2.lo, n2.hi, lo, hi, ulo, uhi);
+        const double union2 = m3TreeArea(ulo, uhi);
+        const double area2 = n2.height == 0 ? 0.0 : m3TreeArea(n2.lo, n2.hi);
+        // dynamic_tree.c:245-273: a leaf child's cost is its union's area
+        // plus the inherited cost; an internal child's subtracts its own
+        // area.
+        const double cost1 = n1.height == 0 ? union1 + inherited : union1 - area1 + inherited;
+        const double cost2 = n2.height == 0 ? union2 + inherited : union2 - area2 + inherited;
+        if (here < cost1 && here < cost2)
+        {
+            break;
+        }
+        if (cost1 < cost2)
+        {
+            index = c1;
+            cur = n1;
+            curUnion = union1;
+            curArea = area1; // a leaf ends the descent: its area is not read
+        }
+        else
+        {
+            index = c2;
+            cur = n2;
+            curUnion = union2;
+            curArea = area2;
         }
     }
     // A new parent takes the sibling's place; sibling and leaf hang

@@ -415,11 +415,7 @@ __global__ void __launch_bounds__(M3_BLOCK) m3LeafBoxKernel(const m3WorldView* v
 // following steps, up to M3_TREE_LAG steps behind (the move lists sit in
 // a ring of that depth).
 #define M3_TREE_WORLDS_PER_BLOCK 1
-// Registers of a tree warp are capped (65536 / (32 x 16) = 128) so the
-// tree's many latency-bound warps leave room on each SM for the step's
-// own blocks, which run beside them.
-#define M3_TREE_BLOCKS_PER_SM 16
-__global__ void __launch_bounds__(32 * M3_TREE_WORLDS_PER_BLOCK, M3_TREE_BLOCKS_PER_SM)
+__global__ void __launch_bounds__(32 * M3_TREE_WORLDS_PER_BLOCK)
     m3TreeKernel(const m3WorldView* views, const int32_t* order, int32_t count, int32_t slot,
                  int32_t treeLag)
 {
