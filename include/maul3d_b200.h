@@ -280,6 +280,13 @@ M3GPU_API m3ShapeId m3CreateCapsuleShape(m3BodyId bodyId, const m3ShapeDef* def,
                                          const m3Capsule* capsule);
 M3GPU_API m3ShapeId m3CreateBoxShape(m3BodyId bodyId, const m3ShapeDef* def,
                                      m3Vec3 halfExtents);
+/* Replaces m3CreateHeightFieldGridShape (include/maul3d/shape.h:194-202,
+ * shape.c:1175-1262): a native grid heightfield of nx x nz samples
+ * (2..255 each way, x fastest, `cellSize` apart) on a static body, its
+ * minimum corner at the shape's origin.  Null id on invalid input. */
+M3GPU_API m3ShapeId m3CreateHeightFieldGridShape(m3BodyId bodyId, const m3ShapeDef* def,
+                                                 const float* heights, int32_t nx, int32_t nz,
+                                                 float cellSize);
 M3GPU_API bool m3Shape_IsValid(m3ShapeId shapeId);
 
 /* joint.c:15 (joint.h:134) and joint.h:136: spherical, revolute and

@@ -48,6 +48,7 @@ SCENE_BOX_PYRAMID = 1
 SCENE_UNEVEN = 2
 SCENE_FREEFALL = 3
 SCENE_TOWERS = 4
+SCENE_TERRAIN = 5
 
 
 def _ptr(a: np.ndarray) -> C.c_void_p:

@@ -185,9 +185,52 @@ static int64_t Offset(const m3HostWorld* w, const void* hostPtr)
 static void BuildDeviceView(m3HostWorld* w)
 {
     m3LayoutPersistent(&w->dv, w->dslab, w->bodyCap, w->shapeCap, w->jointCap, w->pairCap);
-    w->dv.hulls = w->dhulls;
+    m3AttachDevicePools(w, &w->dv);
     w->dv.scratch = w->dslab + w->persistentBytes;
     w->dv.scratchBytes = w->scratchBytes;
+}
+
+// The heightfield slots and samples, copied whole when their content
+// changed since the last copy (heightfields are static: in practice
+// once, before the first step).
+static int32_t UploadHeightFields(m3HostWorld* w)
+{
+    if (w->hfHeaders.empty() || (w->dhf != nullptr && w->dhfVersion == w->hfVersion))
+    {
+        return M3GPU_OK;
+    }
+    const size_t headers = (size_t)m3AlignUp(
+        (int64_t)(w->hfHeaders.size() * sizeof(m3HeightFieldDev)), 16);
+    const size_t bytes = headers + w->hfSamples.size() * sizeof(float);
+    if (w->dhf != nullptr && w->dhfBytes < bytes)
+    {
+        cudaDeviceSynchronize();
+        DevFree(w->dhf, w->dhfBytes);
+        w->dhf = nullptr;
+        w->dhfBytes = 0;
+    }
+    int32_t rc = M3GPU_OK;
+    if (w->dhf == nullptr)
+    {
+        g_m3ResidencyEpoch += 1;
+        rc = CudaCheck(DevAlloc((void**)&w->dhf, bytes), "allocate heightfields");
+        if (rc != M3GPU_OK)
+        {
+            w->dhf = nullptr;
+            return rc;
+        }
+        w->dhfBytes = bytes;
+    }
+    std::vector<uint8_t> blob(bytes, 0);
+    memcpy(blob.data(), w->hfHeaders.data(), w->hfHeaders.size() * sizeof(m3HeightFieldDev));
+    memcpy(blob.data() + headers, w->hfSamples.data(), w->hfSamples.size() * sizeof(float));
+    rc = CudaCheck(cudaMemcpy(w->dhf, blob.data(), bytes, cudaMemcpyHostToDevice),
+                   "upload heightfields");
+    if (rc == M3GPU_OK)
+    {
+        w->dhfVersion = w->hfVersion;
+    }
+    return rc;
 }
 
 int32_t m3gpuReserve(m3HostWorld* w)
@@ -232,6 +275,10 @@ int32_t m3gpuReserve(m3HostWorld* w)
         {
             w->dhulls = nullptr;
         }
+    }
+    if (rc == M3GPU_OK)
+    {
+        rc = UploadHeightFields(w);
     }
     g_m3ResidencyEpoch += 1;
     return rc;
@@ -292,6 +339,11 @@ static int32_t UploadPrepare(m3HostWorld* w)
             return rc;
         }
         w->dhullCap = 4;
+    }
+    rc = UploadHeightFields(w);
+    if (rc != M3GPU_OK)
+    {
+        return rc;
     }
     BuildDeviceView(w);
     return M3GPU_OK;
@@ -650,6 +702,13 @@ void m3gpuRelease(m3HostWorld* w)
         w->dhulls = nullptr;
     }
     w->dhullCap = 0;
+    if (w->dhf != nullptr)
+    {
+        DevFree(w->dhf, w->dhfBytes);
+        w->dhf = nullptr;
+    }
+    w->dhfBytes = 0;
+    w->dhfVersion = 0;
     w->hostDirty = true;
     w->deviceAhead = false;
 }

@@ -73,6 +73,7 @@ typedef struct m3Mat3 { m3Vec3 cx, cy, cz; } m3Mat3;
 #define M3_SHAPE_MESH 4
 #define M3_SHAPE_VOXEL 5
 #define M3_SHAPE_HEIGHTFIELD 6
+#define M3_HEIGHTFIELD_MAX_DIM 255 // samples per grid axis (world_internal.h:305)
 
 // ---------------------------------------------------------------------
 // Persistent record layouts (byte-identical to the reference)
@@ -172,6 +173,14 @@ M3_HD m3Quat q4(m3real x, m3real y, m3real z, m3real w)
 M3_HD m3real m3MinF(m3real a, m3real b) { return a < b ? a : b; }
 M3_HD m3real m3MaxF(m3real a, m3real b) { return a > b ? a : b; }
 M3_HD m3real m3ClampF(m3real a, m3real lo, m3real hi) { return m3MaxF(lo, m3MinF(a, hi)); }
+// A float cell coordinate to an integer: NaN parks at `nanPark`, the rest
+// clamps to +-2e9 and truncates (world_internal.h:30-35).
+M3_HD int32_t m3CellFromF(m3real f, m3real nanPark)
+{
+    f = f != f ? nanPark : f;
+    f = f < -2.0e9f ? -2.0e9f : (f > 2.0e9f ? 2.0e9f : f);
+    return (int32_t)f;
+}
 M3_HD m3real m3AbsF(m3real a) { return a < 0.0f ? -a : a; }
 
 M3_HD m3Vec3 m3Add3(m3Vec3 a, m3Vec3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }

@@ -356,10 +356,17 @@ __device__ void m3Witness(const m3SimplexDev* s, m3Vec3* pointA, m3Vec3* pointB)
 
 // m3ShapeDistance with an empty cache and useRadii = false, the form the
 // narrowphase calls (manifold.c:2664-2700, distance.c:505-709).  B's
-// pose in A's frame is (q, p).
+// pose in A's frame is (q, p).  `cacheMaskA`, when given, receives the
+// bit mask of A's vertices in the simplex cache the call writes back:
+// the final simplex's (at most three) A indices on the regular exit,
+// 0 on the two early exits, which leave the empty cache as it was.
 __device__ m3DistanceOutDev m3ShapeDistanceDev(const m3ProxyDev& proxyA, const m3ProxyDev& proxyB,
-                                               m3Quat q, m3Vec3 p)
+                                               m3Quat q, m3Vec3 p, int32_t* cacheMaskA = nullptr)
 {
+    if (cacheMaskA != nullptr)
+    {
+        *cacheMaskA = 0;
+    }
     m3DistanceOutDev output;
     output.pointA = v3(0.0f, 0.0f, 0.0f);
     output.pointB = v3(0.0f, 0.0f, 0.0f);
@@ -494,6 +501,15 @@ __device__ m3DistanceOutDev m3ShapeDistanceDev(const m3ProxyDev& proxyA, const m
     m3Vec3 pointA;
     m3Vec3 pointB;
     m3Witness(&simplex, &pointA, &pointB);
+    if (cacheMaskA != nullptr)
+    {
+        int32_t mask = 0;
+        for (int32_t i = 0; i < simplex.count && i < 3; ++i)
+        {
+            mask |= 1 << vs[i].indexA;
+        }
+        *cacheMaskA = mask;
+    }
     output.pointA = pointA;
     output.pointB = pointB;
     output.distance = m3Length3(m3Sub3(pointA, pointB));

@@ -90,6 +90,19 @@ typedef struct m3TreeNode
     int32_t pad;
 } m3TreeNode;
 
+// One heightfield slot (world_internal.h:307-315): an nx x nz grid of
+// samples, row-major with x fastest, starting at `sampleStart` in the
+// world's sample pool; the sample extremes are baked at creation.
+typedef struct m3HeightFieldDev
+{
+    int32_t nx;
+    int32_t nz;
+    float cellSize;
+    float minHeight;
+    float maxHeight;
+    int32_t sampleStart;
+} m3HeightFieldDev;
+
 // Per-body persistent arrays (capacity = bodyCap).
 #define M3_BODY_FIELDS(X)                                                                          \
     X(m3Transform, xf)                                                                             \
@@ -144,6 +157,7 @@ typedef struct m3TreeNode
     X(int32_t, shapeNext)                                                                          \
     X(int32_t, proxyId)                                                                            \
     X(int32_t, hullIndex)                                                                          \
+    X(int32_t, hfIndex)                                                                            \
     X(uint8_t, shapeAlive)                                                                         \
     X(uint16_t, shapeGen)                                                                          \
     X(uint64_t, shapeUserData)
@@ -201,6 +215,10 @@ typedef struct m3WorldView
 #undef M3_X_PTR
     // Interned hull slabs (count-derived pool, outside the slab).
     m3HullData* hulls;
+    // Heightfield slots and their samples (count-derived, outside the
+    // slab; null in a world without heightfields).
+    const m3HeightFieldDev* hfs;
+    const float* hfSamples;
     // Device-only scratch (null in host views), laid out by the step
     // module which owns its record types.
     uint8_t* scratch;

@@ -437,6 +437,7 @@ __device__ m3Manifold m3CollideHullsDev(const m3HullData* hullA, const m3HullDat
 }
 
 #include "m3_distance.cuh"
+#include "m3_terrain.cuh"
 
 // GJK proxy of a shape in its own frame (manifold.c:463-499).
 __device__ __forceinline__ m3ProxyDev m3MakeProxyDev(const m3WorldView& w, int32_t shape,
@@ -486,8 +487,9 @@ enum
     M3F_ROUND = 4, // hull-sphere, capsule-sphere, capsule-capsule: GJK on the cores
     M3F_PLANE_SPHERE = 5,
     M3F_SPHERE_SPHERE = 6,
-    M3F_UNSUPPORTED = 7,
-    M3F_COUNT = 8
+    M3F_TERRAIN = 7, // heightfield versus sphere, capsule or hull
+    M3F_UNSUPPORTED = 8,
+    M3F_COUNT = 9
 };
 
 __device__ __forceinline__ int32_t m3PairFamily(uint8_t typeA, uint8_t typeB)
@@ -495,6 +497,16 @@ __device__ __forceinline__ int32_t m3PairFamily(uint8_t typeA, uint8_t typeB)
     const bool planePair = typeA == M3_SHAPE_PLANE || typeB == M3_SHAPE_PLANE;
     const bool hullPair = typeA == M3_SHAPE_HULL || typeB == M3_SHAPE_HULL;
     const bool capsulePair = typeA == M3_SHAPE_CAPSULE || typeB == M3_SHAPE_CAPSULE;
+    // The dispatcher's order: voxel pairs, then heightfield pairs, then
+    // mesh pairs (manifold.c:2372-2413).
+    if (typeA == M3_SHAPE_VOXEL || typeB == M3_SHAPE_VOXEL)
+    {
+        return M3F_UNSUPPORTED;
+    }
+    if (typeA == M3_SHAPE_HEIGHTFIELD || typeB == M3_SHAPE_HEIGHTFIELD)
+    {
+        return M3F_TERRAIN;
+    }
     if (typeA >= M3_SHAPE_MESH || typeB >= M3_SHAPE_MESH)
     {
         return M3F_UNSUPPORTED;
@@ -541,6 +553,20 @@ __device__ int32_t m3CollideFamily(const m3WorldView& w, uint64_t key, m3Manifol
     {
         *out = fresh;
         return M3_NARROW_UNSUPPORTED;
+    }
+    if (F == M3F_TERRAIN)
+    {
+        // manifold.c:2391-2402: only spheres, capsules and hulls collide
+        // with a heightfield; any other partner leaves the manifold empty.
+        const int32_t hfShape = typeA == M3_SHAPE_HEIGHTFIELD ? shapeA : shapeB;
+        const int32_t otherShape = hfShape == shapeA ? shapeB : shapeA;
+        const uint8_t ot = w.shapeType[otherShape];
+        if (ot == M3_SHAPE_SPHERE || ot == M3_SHAPE_CAPSULE || ot == M3_SHAPE_HULL)
+        {
+            m3CollideTerrainDev(w, hfShape, otherShape, hfShape == shapeA, &fresh);
+        }
+        *out = fresh;
+        return status;
     }
     if (F == M3F_PLANE_HULL)
     {
@@ -952,6 +978,8 @@ __device__ int32_t m3CollidePair(const m3WorldView& w, uint64_t key, m3Manifold*
         return m3CollideFamily<M3F_PLANE_SPHERE>(w, key, out);
     case M3F_SPHERE_SPHERE:
         return m3CollideFamily<M3F_SPHERE_SPHERE>(w, key, out);
+    case M3F_TERRAIN:
+        return m3CollideFamily<M3F_TERRAIN>(w, key, out);
     default:
         return m3CollideFamily<M3F_UNSUPPORTED>(w, key, out);
     }

@@ -492,6 +492,24 @@ M3_HD m3Aabb m3ShapeFreshBounds(const m3WorldView& w, int32_t shape)
         }
         return box;
     }
+    if (type == M3_SHAPE_HEIGHTFIELD)
+    {
+        // The grid's box from the shape's origin and the baked sample
+        // extremes, rotation ignored (broad_phase.c:52-67).
+        const m3HeightFieldDev hf = w.hfs[w.hfIndex[shape]];
+        box.lo[0] = xf.p.x;
+        box.lo[1] = xf.p.y + (double)hf.minHeight;
+        box.lo[2] = xf.p.z;
+        box.hi[0] = xf.p.x + (double)((float)(hf.nx - 1) * hf.cellSize);
+        box.hi[1] = xf.p.y + (double)hf.maxHeight;
+        box.hi[2] = xf.p.z + (double)((float)(hf.nz - 1) * hf.cellSize);
+        for (int32_t k = 0; k < 3; ++k)
+        {
+            box.lo[k] -= (double)M3_AABB_MARGIN;
+            box.hi[k] += (double)M3_AABB_MARGIN;
+        }
+        return box;
+    }
     if (type == M3_SHAPE_CAPSULE)
     {
         const m3Vec3 r1 = m3RotateVec3(xf.q, w.geom[shape].v);
@@ -514,6 +532,28 @@ M3_HD m3Aabb m3ShapeFreshBounds(const m3WorldView& w, int32_t shape)
         box.lo[k] = c[k] - fat;
         box.hi[k] = c[k] + fat;
     }
+    return box;
+}
+
+// The box a shape enters the tree with at creation (broad_phase.c:
+// 149-173): the fresh bounds, except for a heightfield, whose box hangs
+// from its BODY's origin with a fixed 0.1 margin.
+M3_HD m3Aabb m3ShapeCreationBounds(const m3WorldView& w, int32_t shape)
+{
+    if (w.shapeType[shape] != M3_SHAPE_HEIGHTFIELD)
+    {
+        return m3ShapeFreshBounds(w, shape);
+    }
+    const m3HeightFieldDev hf = w.hfs[w.hfIndex[shape]];
+    const m3Transform xf = w.xf[w.shapeBody[shape]];
+    const double margin = 0.1;
+    m3Aabb box;
+    box.lo[0] = xf.p.x - margin;
+    box.lo[1] = xf.p.y + (double)hf.minHeight - margin;
+    box.lo[2] = xf.p.z - margin;
+    box.hi[0] = xf.p.x + (double)((float)(hf.nx - 1) * hf.cellSize) + margin;
+    box.hi[1] = xf.p.y + (double)hf.maxHeight + margin;
+    box.hi[2] = xf.p.z + (double)((float)(hf.nz - 1) * hf.cellSize) + margin;
     return box;
 }
 

@@ -167,6 +167,12 @@ struct m3HostWorld
     int32_t softCap = 0;
     std::vector<int32_t> hullRefs;
     std::unordered_multimap<uint64_t, int32_t> hullIndexByContent;
+    // Heightfield slots (hfMax in use) and their samples; hfVersion
+    // counts content changes, so the device copy is refreshed only then.
+    std::vector<m3HeightFieldDev> hfHeaders;
+    std::vector<float> hfSamples;
+    uint64_t hfVersion = 0;
+    size_t hfAtRestore = 0; // slots the last restore left
 
     // Device residency.
     uint8_t* dslab = nullptr;        // persistent + scratch
@@ -174,6 +180,9 @@ struct m3HostWorld
     int64_t scratchBytes = 0;
     m3HullData* dhulls = nullptr;    // device hull pool
     int32_t dhullCap = 0;
+    uint8_t* dhf = nullptr;          // device heightfield slots + samples
+    size_t dhfBytes = 0;
+    uint64_t dhfVersion = 0;
     m3WorldView dv{};                // device view (device addresses)
     bool hostDirty = true;           // host image newer than device
     bool deviceAhead = false;        // device newer than host image
@@ -184,6 +193,15 @@ struct m3HostWorld
     bool pairTailsToDevice = false;
     bool pairTailsOnDevice = false;
 };
+
+// Points a device view at the world's pools outside the slab.
+inline void m3AttachDevicePools(m3HostWorld* w, m3WorldView* view)
+{
+    view->hulls = w->dhulls;
+    const size_t headers = m3AlignUp((int64_t)(w->hfHeaders.size() * sizeof(m3HeightFieldDev)), 16);
+    view->hfs = w->dhf != nullptr ? (const m3HeightFieldDev*)w->dhf : nullptr;
+    view->hfSamples = w->dhf != nullptr ? (const float*)(w->dhf + headers) : nullptr;
+}
 
 // Registry (world.cpp).
 m3HostWorld* m3gpuWorldFromId(m3WorldId id);

@@ -26,6 +26,10 @@
 //                       (28 a tower), each hit by a sphere launched at
 //                       20-40 m/s: joints break on impact and their
 //                       slots are recycled.
+//   M3S_TERRAIN         `param` spheres, capsules and boxes dropped a
+//                       short way onto a seeded heightfield (1 m cells,
+//                       a sum of three sine waves, about 0.6 m high),
+//                       the heightfield versus convex contacts.
 
 #include <m3_scene_api.h> // resolved by -I: product or oracle shim
 
@@ -39,6 +43,7 @@ enum
     M3S_UNEVEN = 2,
     M3S_FREEFALL = 3,
     M3S_TOWERS = 4,
+    M3S_TERRAIN = 5,
 };
 
 static uint64_t SceneSplitMix(uint64_t* state)
@@ -325,6 +330,111 @@ static m3WorldId Towers(uint64_t seed, int32_t towers)
     return world;
 }
 
+// Terrain height at (x, z) from six seeded phases.
+static double TerrainWave(const double* ph, double x, double z)
+{
+    return 0.3 * sin(0.45 * x + ph[0]) * cos(0.38 * z + ph[1]) +
+           0.18 * sin(0.83 * (x + z) + ph[2]) + 0.12 * cos(1.31 * x - 0.97 * z + ph[3]);
+}
+
+static m3WorldId Terrain(uint64_t seed, int32_t bodies)
+{
+    if (bodies < 3)
+    {
+        bodies = 3;
+    }
+    int32_t side = 1;
+    while (side * side < bodies)
+    {
+        side += 1;
+    }
+    const float cell = 1.0f;
+    int32_t n = (int32_t)(1.6 * (double)side) + 7;
+    n = n > 255 ? 255 : n;
+    const double half = 0.5 * (double)(n - 1) * (double)cell;
+
+    m3WorldDef def = m3DefaultWorldDef();
+    def.bodyCapacity = bodies + 4;
+    def.shapeCapacity = bodies + 4;
+    def.jointCapacity = 4;
+    m3WorldId world = m3CreateWorld(&def);
+
+    uint64_t rng = seed;
+    double ph[4];
+    for (int32_t k = 0; k < 4; ++k)
+    {
+        ph[k] = SceneRand(&rng, 0.0, 6.283185307179586);
+    }
+    static float heights[255 * 255];
+    for (int32_t iz = 0; iz < n; ++iz)
+    {
+        for (int32_t ix = 0; ix < n; ++ix)
+        {
+            heights[iz * n + ix] = (float)TerrainWave(ph, (double)ix, (double)iz);
+        }
+    }
+    m3BodyDef gd = m3DefaultBodyDef();
+    gd.position = (m3Pos3){-half, 0.0, -half};
+    m3BodyId ground = m3CreateBody(world, &gd);
+    m3ShapeDef sd = m3DefaultShapeDef();
+    sd.friction = 0.6f;
+    m3CreateHeightFieldGridShape(ground, &sd, heights, n, n, cell);
+
+    m3BodyDef bd = m3DefaultBodyDef();
+    bd.type = m3_dynamicBody;
+    for (int32_t b = 0; b < bodies; ++b)
+    {
+        // Grid coordinates in the heightfield's frame, jittered.
+        double gx = 3.0 + 1.6 * (double)(b % side) + SceneRand(&rng, -0.3, 0.3);
+        double gz = 3.0 + 1.6 * (double)(b / side) + SceneRand(&rng, -0.3, 0.3);
+        // The highest sample of the cells around keeps the start clear.
+        float top = -1.0e30f;
+        for (int32_t dz = -1; dz <= 2; ++dz)
+        {
+            for (int32_t dx = -1; dx <= 2; ++dx)
+            {
+                int32_t ix = (int32_t)gx + dx;
+                int32_t iz = (int32_t)gz + dz;
+                ix = ix < 0 ? 0 : (ix > n - 1 ? n - 1 : ix);
+                iz = iz < 0 ? 0 : (iz > n - 1 ? n - 1 : iz);
+                top = heights[iz * n + ix] > top ? heights[iz * n + ix] : top;
+            }
+        }
+        double drop = SceneRand(&rng, 0.02, 0.15);
+        int32_t kind = b % 3;
+        double lift;
+        if (kind == 0)
+        {
+            float r = (float)SceneRand(&rng, 0.3, 0.5);
+            lift = (double)r;
+            bd.position = (m3Pos3){gx - half, (double)top + lift + drop, gz - half};
+            m3BodyId body = m3CreateBody(world, &bd);
+            m3Sphere ball = {{0.0f, 0.0f, 0.0f}, r};
+            m3CreateSphereShape(body, &sd, &ball);
+        }
+        else if (kind == 1)
+        {
+            float r = (float)SceneRand(&rng, 0.25, 0.35);
+            float hh = (float)SceneRand(&rng, 0.2, 0.45);
+            lift = (double)r;
+            bd.position = (m3Pos3){gx - half, (double)top + lift + drop, gz - half};
+            m3BodyId body = m3CreateBody(world, &bd);
+            m3Capsule cap = {{-hh, 0.0f, 0.0f}, {hh, 0.0f, 0.0f}, r};
+            m3CreateCapsuleShape(body, &sd, &cap);
+        }
+        else
+        {
+            m3Vec3 he = {(float)SceneRand(&rng, 0.3, 0.45), (float)SceneRand(&rng, 0.3, 0.45),
+                         (float)SceneRand(&rng, 0.3, 0.45)};
+            lift = (double)he.y;
+            bd.position = (m3Pos3){gx - half, (double)top + lift + drop, gz - half};
+            m3BodyId body = m3CreateBody(world, &bd);
+            m3CreateBoxShape(body, &sd, he);
+        }
+    }
+    return world;
+}
+
 // Build one seeded scene; returns the null world id for an unknown
 // scene number.
 M3S_API m3WorldId m3s_build(int32_t scene, uint64_t seed, int32_t param)
@@ -341,6 +451,8 @@ M3S_API m3WorldId m3s_build(int32_t scene, uint64_t seed, int32_t param)
         return FreeFall(param > 0 ? param : 8);
     case M3S_TOWERS:
         return Towers(seed, param > 0 ? param : 4);
+    case M3S_TERRAIN:
+        return Terrain(seed, param > 0 ? param : 60);
     default:
     {
         m3WorldId none = {0, 0};

@@ -49,7 +49,7 @@ constexpr int32_t kWaterVolumes = 8;
 constexpr int32_t kMeshMaxVerts = 65535;
 constexpr int32_t kMeshMaxTris = 65535;
 constexpr int32_t kMeshMaterialBytes = 8 * 24;
-constexpr int32_t kHeightFieldMaxDim = 255;
+constexpr int32_t kHeightFieldMaxDim = M3_HEIGHTFIELD_MAX_DIM;
 
 #pragma pack(push, 1)
 struct SnapshotHeader // snapshot.c:88-127
@@ -195,6 +195,11 @@ public:
     const uint8_t* Here() const { return mode_ == Mode::kCheck ? in_ + cursor_ : nullptr; }
     int64_t cursor() const { return cursor_; }
     const char* unsupported() const { return unsupported_; }
+    // Writing a world built here (no restored bytes to carry).
+    bool WritesOwn() const
+    {
+        return mode_ == Mode::kWrite && (carry_ == nullptr || carry_->empty());
+    }
 
 private:
     Mode mode_;
@@ -218,8 +223,15 @@ struct PoolBlocks
     std::vector<int32_t> shapeQueue;
     std::vector<int32_t> hullQueue;
     std::vector<int32_t> jointQueue;
+    // The heightfield pool of a world built here (shape.c:549-566): slots
+    // 0 .. count-1 live, reference count 1, generation 0, queue empty.
+    std::vector<int32_t> hfRefs;
+    std::vector<uint16_t> hfGens;
+    std::vector<uint8_t> hfAlive;
+    std::vector<int32_t> hfQueue;
     const uint8_t* shapeType = nullptr;
     const uint8_t* shapeAlive = nullptr;
+    const uint8_t* hfIndex = nullptr;
     const uint8_t* proxyId = nullptr;
     const uint8_t* treeNodes = nullptr;
 
@@ -232,6 +244,10 @@ struct PoolBlocks
         shapeQueue.assign((size_t)w->shapeCap, 0);
         hullQueue.assign((size_t)w->shapeCap, 0);
         jointQueue.assign((size_t)w->jointCap, 0);
+        hfRefs.assign((size_t)w->shapeCap, 0);
+        hfGens.assign((size_t)w->shapeCap, 0);
+        hfAlive.assign((size_t)w->shapeCap, 0);
+        hfQueue.assign((size_t)w->shapeCap, 0);
     }
     // The world's pools as the walk writes them.
     void From(const m3HostWorld* w)
@@ -247,6 +263,11 @@ struct PoolBlocks
         shapeQueue = w->shapeFree.queue;
         hullQueue = w->hullFree.queue;
         jointQueue = w->jointFree.queue;
+        for (size_t f = 0; f < w->hfHeaders.size(); ++f)
+        {
+            hfRefs[f] = 1;
+            hfAlive[f] = 1;
+        }
     }
 };
 
@@ -356,10 +377,23 @@ void WalkFixed(BlockWalk& b, const m3HostWorld* w, const m3WorldView& v, PoolBlo
     b.Carry(kVoxelChunkBytes * nv + 4 * nv + 2 * nv, Fill::kZero);
     b.Empty(nv, "voxel chunks");
     b.Carry(4 * nv, Fill::kZero);
-    b.Carry(4 * ns + 4 * ns, Fill::kMinusOne); // voxel and heightfield index per shape
-    b.Carry(4 * ns + 2 * ns, Fill::kZero);
-    b.Empty(ns, "heightfields");
-    b.Carry(4 * ns, Fill::kZero);
+    b.Carry(4 * ns, Fill::kMinusOne); // voxel index per shape
+    pb.hfIndex = b.Here();
+    b.Keep(v.hfIndex, 4 * ns); // heightfield index per shape
+    if (b.WritesOwn() && !w->hfHeaders.empty())
+    {
+        // The heightfield pool of a world built here.
+        b.Keep(pb.hfRefs.data(), 4 * ns);
+        b.Keep(pb.hfGens.data(), 2 * ns);
+        b.Keep(pb.hfAlive.data(), ns);
+        b.Keep(pb.hfQueue.data(), 4 * ns);
+    }
+    else
+    {
+        // As restored (or a fresh world's empty pool): reference counts,
+        // generations, liveness, free queue.
+        b.Carry(4 * ns + 2 * ns + ns + 4 * ns, Fill::kZero);
+    }
     // Characters.
     b.Carry(4 * nc, Fill::kMinusOne); // body
     b.Carry(nc * (4 * 6 + 1 + 12 + 4 + 4 + 4 + 2 + 2), Fill::kZero);
@@ -494,6 +528,10 @@ int64_t FixedBytes(const m3HostWorld* w)
 int64_t TailBytes(const m3HostWorld* w)
 {
     int64_t n = 8LL * w->meshCap + 12LL * w->shapeCap;
+    for (const m3HeightFieldDev& hf : w->hfHeaders)
+    {
+        n += hf.nx > 0 ? 8 + 4LL * hf.nx * hf.nz : 0;
+    }
     for (int32_t h = 0; h < w->shapeCap; ++h)
     {
         n += 16;
@@ -535,6 +573,12 @@ extern "C" int32_t m3World_Snapshot(m3WorldId worldId, void* out, int32_t capaci
     if (w->hv.sc->treeTracked == 0)
     {
         m3gpuSetError(M3GPU_ERR_UNSUPPORTED, "m3World_Snapshot: the world keeps no tree");
+        return -1;
+    }
+    if (w->hfHeaders.size() != w->hfAtRestore && !w->snapshotCarry.empty())
+    {
+        m3gpuSetError(M3GPU_ERR_UNSUPPORTED,
+                      "m3World_Snapshot: heightfields created after a restore");
         return -1;
     }
     const int64_t fixed = FixedBytes(w);
@@ -618,6 +662,20 @@ extern "C" int32_t m3World_Snapshot(m3WorldId worldId, void* out, int32_t capaci
     }
     for (int32_t f = 0; f < w->shapeCap; ++f)
     {
+        if (f < (int32_t)w->hfHeaders.size() && w->hfHeaders[(size_t)f].nx > 0)
+        {
+            // A heightfield: counts, cell, extremes, samples.
+            const m3HeightFieldDev& hf = w->hfHeaders[(size_t)f];
+            memcpy(p, &hf.nx, 4);
+            memcpy(p + 4, &hf.nz, 4);
+            memcpy(p + 8, &hf.cellSize, 4);
+            memcpy(p + 12, &hf.minHeight, 4);
+            memcpy(p + 16, &hf.maxHeight, 4);
+            const size_t samples = (size_t)hf.nx * (size_t)hf.nz;
+            memcpy(p + 20, w->hfSamples.data() + hf.sampleStart, 4 * samples);
+            p += 20 + 4 * samples;
+            continue;
+        }
         // An empty heightfield slot: no samples, its cell size as carried.
         memset(p, 0, 12);
         if (w->heightFieldCellCarry.size() == (size_t)w->shapeCap)
@@ -746,7 +804,8 @@ extern "C" bool m3World_Restore(m3WorldId worldId, const void* data, int32_t siz
             cursor += content;
         }
     }
-    const int64_t heightFieldAt = cursor;
+    std::vector<m3HeightFieldDev> hfSlots; // nx == 0: an empty slot
+    std::vector<float> hfCells((size_t)w->shapeCap, 0.0f);
     for (int32_t f = 0; f < w->shapeCap; ++f)
     {
         if (size - cursor < 12)
@@ -756,6 +815,7 @@ extern "C" bool m3World_Restore(m3WorldId worldId, const void* data, int32_t siz
         }
         const int32_t nx = ReadI32(raw + cursor);
         const int32_t nz = ReadI32(raw + cursor + 4);
+        memcpy(&hfCells[(size_t)f], raw + cursor + 8, 4);
         cursor += 12;
         if (nx < 0 || nx > kHeightFieldMaxDim || nz < 0 || nz > kHeightFieldMaxDim ||
             (nx == 0) != (nz == 0) || (nx > 0 && (nx < 2 || nz < 2)))
@@ -771,8 +831,21 @@ extern "C" bool m3World_Restore(m3WorldId worldId, const void* data, int32_t siz
                 m3gpuSetError(M3GPU_ERR_INVALID, "m3World_Restore: truncated heightfield");
                 return false;
             }
+            m3HeightFieldDev hf;
+            hf.nx = nx;
+            hf.nz = nz;
+            memcpy(&hf.cellSize, raw + cursor - 4, 4);
+            memcpy(&hf.minHeight, raw + cursor, 4);
+            memcpy(&hf.maxHeight, raw + cursor + 4, 4);
+            hf.sampleStart = (int32_t)(cursor + 8); // byte offset, rebased at commit
+            if (!(hf.cellSize > 0.0f) || !(hf.cellSize < 3.4e38f))
+            {
+                m3gpuSetError(M3GPU_ERR_INVALID, "m3World_Restore: corrupt heightfield cell");
+                return false;
+            }
+            hfSlots.resize((size_t)f + 1);
+            hfSlots[(size_t)f] = hf;
             cursor += content;
-            unsupported = "heightfields";
         }
     }
     if (cursor != size)
@@ -794,9 +867,19 @@ extern "C" bool m3World_Restore(m3WorldId worldId, const void* data, int32_t siz
     {
         const uint8_t t = pb.shapeType[s];
         if (pb.shapeAlive[s] != 0 && t != M3_SHAPE_SPHERE && t != M3_SHAPE_PLANE &&
-            t != M3_SHAPE_HULL && t != M3_SHAPE_CAPSULE)
+            t != M3_SHAPE_HULL && t != M3_SHAPE_CAPSULE && t != M3_SHAPE_HEIGHTFIELD)
         {
-            unsupported = "mesh, voxel or heightfield shapes";
+            unsupported = "mesh or voxel shapes";
+        }
+        if (pb.shapeAlive[s] != 0 && t == M3_SHAPE_HEIGHTFIELD)
+        {
+            // A live heightfield shape names a slot holding samples.
+            const int32_t f = ReadI32(pb.hfIndex + 4LL * s);
+            if (f < 0 || f >= (int32_t)hfSlots.size() || hfSlots[(size_t)f].nx == 0)
+            {
+                m3gpuSetError(M3GPU_ERR_INVALID, "m3World_Restore: corrupt heightfield index");
+                return false;
+            }
         }
     }
     if (unsupported != nullptr)
@@ -879,11 +962,29 @@ extern "C" bool m3World_Restore(m3WorldId worldId, const void* data, int32_t siz
     }
     w->snapshotCarry.swap(carry);
     w->snapshotHeaderCarry.assign(raw, raw + sizeof(SnapshotHeader));
-    w->heightFieldCellCarry.assign((size_t)w->shapeCap, 0.0f);
-    for (int32_t f = 0; f < w->shapeCap; ++f)
+    w->heightFieldCellCarry = hfCells;
+    // The heightfield slots and samples (the index per shape came with
+    // the fixed blocks).
+    w->hfHeaders.clear();
+    w->hfSamples.clear();
+    for (m3HeightFieldDev hf : hfSlots)
     {
-        memcpy(&w->heightFieldCellCarry[(size_t)f], raw + heightFieldAt + 12LL * f + 8, 4);
+        if (hf.nx > 0)
+        {
+            const size_t samples = (size_t)hf.nx * (size_t)hf.nz;
+            const size_t at = w->hfSamples.size();
+            w->hfSamples.resize(at + samples);
+            memcpy(w->hfSamples.data() + at, raw + hf.sampleStart, 4 * samples);
+            hf.sampleStart = (int32_t)at;
+        }
+        else
+        {
+            memset(&hf, 0, sizeof(hf));
+        }
+        w->hfHeaders.push_back(hf);
     }
+    w->hfVersion += 1;
+    w->hfAtRestore = w->hfHeaders.size();
     // The image on the host is now the world; the next step uploads it,
     // the pair arrays in full.
     w->deviceAhead = false;

@@ -2707,7 +2707,7 @@ static int32_t PrepareBatch(m3HostWorld** worlds, int32_t count)
     std::vector<int32_t> order((size_t)count);
     for (int32_t i = 0; i < count; ++i)
     {
-        worlds[i]->dv.hulls = worlds[i]->dhulls;
+        m3AttachDevicePools(worlds[i], &worlds[i]->dv);
         views[(size_t)i] = worlds[i]->dv;
         order[(size_t)i] = i;
     }
@@ -2832,11 +2832,12 @@ static int32_t s_narrowGrid = 148 * 16;
 
 // The narrowphase of one step: family count and scatter, then one
 // kernel per covered family over its bucket.
-#define M3_NARROW_LAUNCHES (2 + M3F_UNSUPPORTED)
+#define M3_NARROW_LAUNCHES (2 + M3F_TERRAIN)
 // Batches of at most this many worlds take the single narrowphase kernel.
 #define M3_NARROW_SMALL_BATCH 4
 
-static void LaunchNarrow(const m3WorldView* views, const int32_t* offsets, int32_t count)
+static void LaunchNarrow(const m3WorldView* views, const int32_t* offsets, int32_t count,
+                         bool terrain)
 {
     if (count <= M3_NARROW_SMALL_BATCH)
     {
@@ -2865,6 +2866,12 @@ static void LaunchNarrow(const m3WorldView* views, const int32_t* offsets, int32
         <<<s_narrowGrid, 128>>>(views, offsets, count, famStart, bucket);
     m3NarrowFamilyKernel<M3F_SPHERE_SPHERE>
         <<<s_narrowGrid, 128>>>(views, offsets, count, famStart, bucket);
+    if (terrain)
+    {
+        // Heightfield pairs, only in batches holding a heightfield.
+        m3NarrowFamilyKernel<M3F_TERRAIN>
+            <<<s_narrowGrid, 128>>>(views, offsets, count, famStart, bucket);
+    }
 }
 
 // The three per-world solve kernels of one step, in order on the current
@@ -3135,9 +3142,11 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
     // behind (the move lists sit in a ring of that depth).  Batches of
     // worlds that keep no tree skip both.
     bool anyTracked = false;
+    bool anyTerrain = false;
     for (int32_t i = 0; i < count; ++i)
     {
         anyTracked = anyTracked || worlds[i]->hv.sc->treeTracked != 0;
+        anyTerrain = anyTerrain || !worlds[i]->hfHeaders.empty();
     }
     if (anyTracked)
     {
@@ -3164,12 +3173,12 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
             s_launches += 1;
         }
         m3PairOffsetsKernel<<<1, M3_BLOCK>>>(s_batch.dviews, count, s_batch.doffsets);
-        LaunchNarrow(s_batch.dviews, s_batch.doffsets, count);
+        LaunchNarrow(s_batch.dviews, s_batch.doffsets, count, anyTerrain);
         cudaEventRecord(ev[1]);
         LaunchSolve(s_batch.dviews, s_batch.dorder, count, dt, substeps, s_batch.cacheBytes,
                     ev + 2, s_batch.classFirst, s_batch.classCache);
         cudaEventRecord(ev[4]);
-        s_launches += 5 + (count <= M3_NARROW_SMALL_BATCH ? 1 : M3_NARROW_LAUNCHES);
+        s_launches += 5 + (count <= M3_NARROW_SMALL_BATCH ? 1 : M3_NARROW_LAUNCHES + (anyTerrain ? 1 : 0));
     }
     if (anyTracked && steps > 0)
     {
@@ -3377,7 +3386,7 @@ extern "C" int32_t m3gpu_step_world_noalloc(m3WorldId worldId, float dt, int32_t
     // The one-world launch table: the world's view with its scratch
     // redirected to the static array, order {0}.
     m3WorldView view = w->dv;
-    view.hulls = w->dhulls;
+    m3AttachDevicePools(w, &view);
     view.scratch = sym.scratch;
     view.scratchBytes = M3_NOALLOC_SCRATCH_BYTES;
     const int32_t zero = 0;

@@ -204,6 +204,7 @@ extern "C" m3WorldId m3CreateWorld(const m3WorldDef* def)
         w->hv.proxyId[i] = M3_TREE_NULL;
         w->hv.shapeNext[i] = -1;
         w->hv.hullIndex[i] = -1;
+        w->hv.hfIndex[i] = -1;
         w->hv.shapeBody[i] = -1;
     }
     for (int32_t i = 0; i < w->jointCap; ++i)
@@ -857,7 +858,8 @@ extern "C" m3ShapeDef m3DefaultShapeDef(void)
 }
 
 static m3ShapeId CreateShapeCommon(m3BodyId bodyId, const m3ShapeDef* def, uint8_t type,
-                                   const m3ShapeGeom* geom)
+                                   const m3ShapeGeom* geom, const m3HeightFieldDev* grid = nullptr,
+                                   const float* heights = nullptr)
 {
     m3ShapeId nullId = {0, 0, 0};
     int32_t b;
@@ -935,13 +937,27 @@ static m3ShapeId CreateShapeCommon(m3BodyId bodyId, const m3ShapeDef* def, uint8
     v.shapeNext[s] = v.shapeHead[b];
     v.shapeHead[b] = s;
     v.hullIndex[s] = hullIndex;
-    // Every shape but a plane enters the broadphase tree with its fresh
-    // bounds (shape.c:589-606).
+    v.hfIndex[s] = -1;
+    if (type == M3_SHAPE_HEIGHTFIELD)
+    {
+        // A fresh heightfield slot holding the caller's samples
+        // (shape.c:549-566).
+        m3HeightFieldDev slot = *grid;
+        slot.sampleStart = (int32_t)w->hfSamples.size();
+        v.hfIndex[s] = (int32_t)w->hfHeaders.size();
+        w->hfHeaders.push_back(slot);
+        w->hfSamples.insert(w->hfSamples.end(), heights, heights + (size_t)grid->nx * grid->nz);
+        w->hfVersion += 1;
+    }
+    // Every shape but a plane enters the broadphase tree with its
+    // creation bounds (shape.c:589-606).
     if (type != M3_SHAPE_PLANE)
     {
         m3WorldView tv = v;
         tv.hulls = w->hulls.empty() ? nullptr : w->hulls.data();
-        const m3Aabb box = m3ShapeFreshBounds(tv, s);
+        tv.hfs = w->hfHeaders.empty() ? nullptr : w->hfHeaders.data();
+        tv.hfSamples = w->hfSamples.empty() ? nullptr : w->hfSamples.data();
+        const m3Aabb box = m3ShapeCreationBounds(tv, s);
         v.proxyId[s] =
             m3TreeInsert(m3WorldTree(v), m3TreeArrayStore{v.treeNodes}, box.lo, box.hi, s);
     }
@@ -1038,6 +1054,54 @@ extern "C" m3ShapeId m3CreateBoxShape(m3BodyId bodyId, const m3ShapeDef* def, m3
     geom.v2 = v3(0.0f, 0.0f, 0.0f);
     geom.s2 = 0.0f;
     return CreateShapeCommon(bodyId, def, M3_SHAPE_HULL, &geom);
+}
+
+// shape.c:1175-1262: a native heightfield on a static body, an nx x nz
+// grid of samples (x fastest) with square cells, its minimum corner at
+// the shape's origin.
+extern "C" m3ShapeId m3CreateHeightFieldGridShape(m3BodyId bodyId, const m3ShapeDef* def,
+                                                  const float* heights, int32_t nx, int32_t nz,
+                                                  float cellSize)
+{
+    m3ShapeId nullId = {0, 0, 0};
+    m3gpuClearError();
+    int32_t b;
+    m3HostWorld* w = ResolveBody(bodyId, &b);
+    if (w == nullptr || def == nullptr || def->internalValue != M3_SHAPE_COOKIE ||
+        heights == nullptr || m3gpuSyncHost(w) != M3GPU_OK || w->hv.btype[b] != M3_BODY_STATIC)
+    {
+        m3gpuSetError(M3GPU_ERR_INVALID,
+                      "m3CreateHeightFieldGridShape: heightfields need a static body");
+        return nullId;
+    }
+    if (nx < 2 || nx > M3_HEIGHTFIELD_MAX_DIM || nz < 2 || nz > M3_HEIGHTFIELD_MAX_DIM ||
+        !FiniteF(cellSize) || !(cellSize > 0.0f))
+    {
+        m3gpuSetError(M3GPU_ERR_INVALID, "m3CreateHeightFieldGridShape: invalid grid");
+        return nullId;
+    }
+    float lo = heights[0];
+    float hi = heights[0];
+    for (int32_t i = 0; i < nx * nz; ++i)
+    {
+        if (!FiniteF(heights[i]))
+        {
+            m3gpuSetError(M3GPU_ERR_INVALID, "m3CreateHeightFieldGridShape: non-finite sample");
+            return nullId;
+        }
+        lo = heights[i] < lo ? heights[i] : lo;
+        hi = heights[i] > hi ? heights[i] : hi;
+    }
+    m3HeightFieldDev grid;
+    grid.nx = nx;
+    grid.nz = nz;
+    grid.cellSize = cellSize;
+    grid.minHeight = lo;
+    grid.maxHeight = hi;
+    grid.sampleStart = 0;
+    m3ShapeGeom geom;
+    memset(&geom, 0, sizeof(geom));
+    return CreateShapeCommon(bodyId, def, M3_SHAPE_HEIGHTFIELD, &geom, &grid, heights);
 }
 
 extern "C" bool m3Shape_IsValid(m3ShapeId shapeId)

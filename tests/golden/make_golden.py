@@ -30,6 +30,8 @@ CASES = [
     ("uneven_2048_s5", 2, 5, 2048, 1.0 / 60.0, 4, 120, [1, 10, 60, 120]),
     ("towers_4_s7", 4, 7, 4, 1.0 / 60.0, 4, 240, [1, 10, 20, 60, 240]),
     ("towers_16_s8", 4, 8, 16, 1.0 / 60.0, 4, 180, [1, 15, 30, 90, 180]),
+    ("terrain_30_s1", 5, 1, 30, 1.0 / 60.0, 4, 200, [1, 10, 50, 200]),
+    ("terrain_60_s2", 5, 2, 60, 1.0 / 60.0, 4, 120, [1, 30, 120]),
 ]
 
 
