@@ -49,6 +49,7 @@ SCENE_UNEVEN = 2
 SCENE_FREEFALL = 3
 SCENE_TOWERS = 4
 SCENE_TERRAIN = 5
+SCENE_SHOTS = 6
 
 
 def _ptr(a: np.ndarray) -> C.c_void_p:

@@ -354,19 +354,57 @@ __device__ void m3Witness(const m3SimplexDev* s, m3Vec3* pointA, m3Vec3* pointB)
     }
 }
 
-// m3ShapeDistance with an empty cache and useRadii = false, the form the
-// narrowphase calls (manifold.c:2664-2700, distance.c:505-709).  B's
-// pose in A's frame is (q, p).  `cacheMaskA`, when given, receives the
-// bit mask of A's vertices in the simplex cache the call writes back:
-// the final simplex's (at most three) A indices on the regular exit,
-// 0 on the two early exits, which leave the empty cache as it was.
-__device__ m3DistanceOutDev m3ShapeDistanceDev(const m3ProxyDev& proxyA, const m3ProxyDev& proxyB,
-                                               m3Quat q, m3Vec3 p, int32_t* cacheMaskA = nullptr)
+// The simplex cache (distance.c:60-132): the vertex indices of the last
+// simplex and its size metric.
+struct m3SimplexCacheDev
 {
-    if (cacheMaskA != nullptr)
+    int32_t count;
+    m3real metric;
+    uint8_t indexA[4];
+    uint8_t indexB[4];
+};
+
+// distance.c:100-121
+__device__ __forceinline__ m3real m3SimplexMetric(const m3SimplexDev& s)
+{
+    const m3SimplexVertexDev* vs = s.v;
+    switch (s.count)
     {
-        *cacheMaskA = 0;
+    case 2:
+        return m3Length3(m3Sub3(vs[1].w, vs[0].w));
+    case 3:
+        return 0.5f * m3Length3(m3Cross3(m3Sub3(vs[1].w, vs[0].w), m3Sub3(vs[2].w, vs[0].w)));
+    case 4:
+        return m3Triple(m3Sub3(vs[1].w, vs[0].w), m3Sub3(vs[2].w, vs[0].w),
+                        m3Sub3(vs[3].w, vs[0].w)) /
+               6.0f;
+    default:
+        return 0.0f;
     }
+}
+
+// The A indices of a cache written back, as a bit mask over at most its
+// first three vertices (the triangle kernels' feature).
+__device__ __forceinline__ int32_t m3CacheMaskA(const m3SimplexCacheDev& c)
+{
+    int32_t mask = 0;
+    for (int32_t i = 0; i < c.count && i < 3; ++i)
+    {
+        mask |= 1 << c.indexA[i];
+    }
+    return mask;
+}
+
+// m3ShapeDistance with useRadii = false (distance.c:505-709).  B's pose
+// in A's frame is (q, p).  Without a cache the simplex starts from
+// vertex pair (0, 0), the form the narrowphase calls (manifold.c:2664-
+// 2700); with one it starts from the cached simplex unless the metric
+// moved (flushed then), and the regular exit writes the final simplex
+// back (the two early exits leave the cache as it was).
+__device__ m3DistanceOutDev m3ShapeDistanceDev(const m3ProxyDev& proxyA, const m3ProxyDev& proxyB,
+                                               m3Quat q, m3Vec3 p,
+                                               m3SimplexCacheDev* cache = nullptr)
+{
     m3DistanceOutDev output;
     output.pointA = v3(0.0f, 0.0f, 0.0f);
     output.pointB = v3(0.0f, 0.0f, 0.0f);
@@ -375,13 +413,46 @@ __device__ m3DistanceOutDev m3ShapeDistanceDev(const m3ProxyDev& proxyA, const m
     m3SimplexDev simplex;
     memset(&simplex, 0, sizeof(simplex));
     m3SimplexVertexDev* vs = simplex.v;
-    simplex.count = 1;
-    vs[0].indexA = 0;
-    vs[0].indexB = 0;
-    vs[0].wA = proxyA.points[0];
-    vs[0].wB = m3Add3(m3RotateVec3(q, proxyB.points[0]), p);
-    vs[0].w = m3Sub3(vs[0].wB, vs[0].wA);
-    vs[0].a = 0.0f;
+    simplex.count = 0;
+    if (cache != nullptr)
+    {
+        simplex.count = cache->count <= 4 ? cache->count : 0;
+        for (int32_t i = 0; i < simplex.count; ++i)
+        {
+            const int32_t indexA = cache->indexA[i];
+            const int32_t indexB = cache->indexB[i];
+            if (indexA >= proxyA.count || indexB >= proxyB.count)
+            {
+                simplex.count = 0;
+                break;
+            }
+            vs[i].indexA = indexA;
+            vs[i].indexB = indexB;
+            vs[i].wA = proxyA.points[indexA];
+            vs[i].wB = m3Add3(m3RotateVec3(q, proxyB.points[indexB]), p);
+            vs[i].w = m3Sub3(vs[i].wB, vs[i].wA);
+            vs[i].a = 0.0f;
+        }
+        if (simplex.count > 0)
+        {
+            const m3real metric1 = cache->metric;
+            const m3real metric2 = m3SimplexMetric(simplex);
+            if (2.0f * metric1 < metric2 || metric2 < 0.5f * metric1 || metric2 < M3_FLT_EPSILON)
+            {
+                simplex.count = 0;
+            }
+        }
+    }
+    if (simplex.count == 0)
+    {
+        simplex.count = 1;
+        vs[0].indexA = 0;
+        vs[0].indexB = 0;
+        vs[0].wA = proxyA.points[0];
+        vs[0].wB = m3Add3(m3RotateVec3(q, proxyB.points[0]), p);
+        vs[0].w = m3Sub3(vs[0].wB, vs[0].wA);
+        vs[0].a = 0.0f;
+    }
 
     m3SimplexDev backup;
     memset(&backup, 0, sizeof(backup));
@@ -501,14 +572,15 @@ __device__ m3DistanceOutDev m3ShapeDistanceDev(const m3ProxyDev& proxyA, const m
     m3Vec3 pointA;
     m3Vec3 pointB;
     m3Witness(&simplex, &pointA, &pointB);
-    if (cacheMaskA != nullptr)
+    if (cache != nullptr)
     {
-        int32_t mask = 0;
-        for (int32_t i = 0; i < simplex.count && i < 3; ++i)
+        cache->metric = m3SimplexMetric(simplex);
+        cache->count = simplex.count;
+        for (int32_t i = 0; i < simplex.count; ++i)
         {
-            mask |= 1 << vs[i].indexA;
+            cache->indexA[i] = (uint8_t)vs[i].indexA;
+            cache->indexB[i] = (uint8_t)vs[i].indexB;
         }
-        *cacheMaskA = mask;
     }
     output.pointA = pointA;
     output.pointB = pointB;

@@ -261,9 +261,12 @@ __device__ void m3CapsuleTriangleDev(m3TriManifoldDev* out, m3Vec3 c1, m3Vec3 c2
     proxyB.points = segPts;
     proxyB.count = 2;
     proxyB.radius = 0.0f;
-    int32_t cacheMask = 0;
+    m3SimplexCacheDev cache;
+    cache.count = 0;
+    cache.metric = 0.0f;
     const m3DistanceOutDev dOut = m3ShapeDistanceDev(proxyA, proxyB, q4(0.0f, 0.0f, 0.0f, 1.0f),
-                                                     v3(0.0f, 0.0f, 0.0f), &cacheMask);
+                                                     v3(0.0f, 0.0f, 0.0f), &cache);
+    const int32_t cacheMask = m3CacheMaskA(cache);
     if (dOut.distance > radius + M3_SPECULATIVE_DISTANCE)
     {
         return;
@@ -743,9 +746,12 @@ __device__ void m3HullTriangleDev(m3TriManifoldDev* out, const m3HullData* hull,
         proxyB.points = hull->vertices;
         proxyB.count = hull->vertexCount;
         proxyB.radius = 0.0f;
-        int32_t cacheMask = 0;
+        m3SimplexCacheDev cache;
+        cache.count = 0;
+        cache.metric = 0.0f;
         const m3DistanceOutDev dOut = m3ShapeDistanceDev(
-            proxyA, proxyB, q4(0.0f, 0.0f, 0.0f, 1.0f), v3(0.0f, 0.0f, 0.0f), &cacheMask);
+            proxyA, proxyB, q4(0.0f, 0.0f, 0.0f, 1.0f), v3(0.0f, 0.0f, 0.0f), &cache);
+        const int32_t cacheMask = m3CacheMaskA(cache);
         if (dOut.distance > 0.0f && dOut.distance <= M3_SPECULATIVE_DISTANCE)
         {
             out->pointCount = 1;

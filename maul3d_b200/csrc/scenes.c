@@ -30,6 +30,11 @@
 //                       short way onto a seeded heightfield (1 m cells,
 //                       a sum of three sine waves, about 0.6 m high),
 //                       the heightfield versus convex contacts.
+//   M3S_SHOTS           `param` small spheres, boxes and capsules shot at
+//                       25-60 m/s across a ring of static boxes, spheres
+//                       and capsules above a ground plane (odd seeds add
+//                       a heightfield patch): the continuous phase's time
+//                       of impact against static targets.
 
 #include <m3_scene_api.h> // resolved by -I: product or oracle shim
 
@@ -44,6 +49,7 @@ enum
     M3S_FREEFALL = 3,
     M3S_TOWERS = 4,
     M3S_TERRAIN = 5,
+    M3S_SHOTS = 6,
 };
 
 static uint64_t SceneSplitMix(uint64_t* state)
@@ -435,6 +441,111 @@ static m3WorldId Terrain(uint64_t seed, int32_t bodies)
     return world;
 }
 
+static m3WorldId Shots(uint64_t seed, int32_t shots)
+{
+    if (shots < 1)
+    {
+        shots = 1;
+    }
+    int32_t targets = shots / 3 < 4 ? 4 : shots / 3;
+    m3WorldDef def = m3DefaultWorldDef();
+    def.bodyCapacity = shots + targets + 4;
+    def.shapeCapacity = shots + targets + 4;
+    def.jointCapacity = 4;
+    m3WorldId world = m3CreateWorld(&def);
+    SceneGround(world, 0.6f);
+    uint64_t rng = seed;
+    m3ShapeDef sd = m3DefaultShapeDef();
+    sd.friction = 0.6f;
+    if ((seed & 1u) != 0)
+    {
+        static float patch[12 * 12];
+        for (int32_t k = 0; k < 12 * 12; ++k)
+        {
+            patch[k] = (float)SceneRand(&rng, 0.0, 0.4);
+        }
+        m3BodyDef pd = m3DefaultBodyDef();
+        pd.position = (m3Pos3){-5.5, 0.05, -5.5};
+        m3BodyId pb = m3CreateBody(world, &pd);
+        m3CreateHeightFieldGridShape(pb, &sd, patch, 12, 12, 1.0f);
+    }
+
+    // Static targets on a ring of radius 12 (a ring's width apart).
+    const double ring = 12.0 + 0.5 * (double)targets;
+    double tx[4096];
+    double ty[4096];
+    double tz[4096];
+    targets = targets > 4096 ? 4096 : targets;
+    m3BodyDef td = m3DefaultBodyDef();
+    for (int32_t t = 0; t < targets; ++t)
+    {
+        double a = 6.283185307179586 * (double)t / (double)targets;
+        tx[t] = ring * cos(a);
+        tz[t] = ring * sin(a);
+        ty[t] = SceneRand(&rng, 1.5, 3.0);
+        td.position = (m3Pos3){tx[t], ty[t], tz[t]};
+        m3BodyId body = m3CreateBody(world, &td);
+        int32_t kind = t % 3;
+        if (kind == 0)
+        {
+            float h = (float)SceneRand(&rng, 0.6, 1.2);
+            m3CreateBoxShape(body, &sd, (m3Vec3){h, h, h});
+        }
+        else if (kind == 1)
+        {
+            m3Sphere ball = {{0.0f, 0.0f, 0.0f}, (float)SceneRand(&rng, 0.6, 1.2)};
+            m3CreateSphereShape(body, &sd, &ball);
+        }
+        else
+        {
+            float hh = (float)SceneRand(&rng, 0.5, 1.0);
+            m3Capsule cap = {{0.0f, -hh, 0.0f}, {0.0f, hh, 0.0f}, (float)SceneRand(&rng, 0.4, 0.7)};
+            m3CreateCapsuleShape(body, &sd, &cap);
+        }
+    }
+
+    // Projectiles: each aimed at one target from outside the ring,
+    // spread by height so no two start together.
+    m3BodyDef bd = m3DefaultBodyDef();
+    bd.type = m3_dynamicBody;
+    for (int32_t j = 0; j < shots; ++j)
+    {
+        int32_t t = j % targets;
+        double a = 6.283185307179586 * (double)t / (double)targets;
+        double dist = SceneRand(&rng, 5.0, 9.0);
+        double sx = tx[t] + dist * cos(a) + SceneRand(&rng, -0.2, 0.2);
+        double sz = tz[t] + dist * sin(a) + SceneRand(&rng, -0.2, 0.2);
+        double sy = ty[t] + 0.9 * (double)(j / targets) + SceneRand(&rng, -0.2, 0.2);
+        double speed = SceneRand(&rng, 25.0, 60.0);
+        double dx = tx[t] - sx;
+        double dy = ty[t] - sy;
+        double dz = tz[t] - sz;
+        double len = sqrt(dx * dx + dy * dy + dz * dz);
+        bd.position = (m3Pos3){sx, sy, sz};
+        bd.linearVelocity =
+            (m3Vec3){(float)(speed * dx / len), (float)(speed * dy / len), (float)(speed * dz / len)};
+        m3BodyId body = m3CreateBody(world, &bd);
+        int32_t kind = j % 3;
+        if (kind == 0)
+        {
+            m3Sphere ball = {{0.0f, 0.0f, 0.0f}, (float)SceneRand(&rng, 0.15, 0.35)};
+            m3CreateSphereShape(body, &sd, &ball);
+        }
+        else if (kind == 1)
+        {
+            float h = (float)SceneRand(&rng, 0.15, 0.3);
+            m3CreateBoxShape(body, &sd, (m3Vec3){h, h, h});
+        }
+        else
+        {
+            float hh = (float)SceneRand(&rng, 0.15, 0.3);
+            m3Capsule cap = {{-hh, 0.0f, 0.0f}, {hh, 0.0f, 0.0f}, (float)SceneRand(&rng, 0.1, 0.2)};
+            m3CreateCapsuleShape(body, &sd, &cap);
+        }
+    }
+    return world;
+}
+
 // Build one seeded scene; returns the null world id for an unknown
 // scene number.
 M3S_API m3WorldId m3s_build(int32_t scene, uint64_t seed, int32_t param)
@@ -453,6 +564,8 @@ M3S_API m3WorldId m3s_build(int32_t scene, uint64_t seed, int32_t param)
         return Towers(seed, param > 0 ? param : 4);
     case M3S_TERRAIN:
         return Terrain(seed, param > 0 ? param : 60);
+    case M3S_SHOTS:
+        return Shots(seed, param > 0 ? param : 24);
     default:
     {
         m3WorldId none = {0, 0};

@@ -39,6 +39,7 @@
 #include "m3_joints.cuh"
 #include "m3_tree.h"
 #include "m3_ops.h"
+#include "m3_toi.cuh"
 
 #include <cuda_runtime.h>
 
@@ -2194,9 +2195,99 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3SubstepKernel(const m3WorldV
 }
 
 // ---------------------------------------------------------------------
+// The tree arm of the continuous phase for one shape of a fast body
+// (solver.c:3081-3274): every static target whose tree leaf touches the
+// swept box [lo, hi], swept by the time of impact bounded by `*fraction`.
+// Returns how many targets hit before `*fraction`; with exactly one,
+// `*fraction` becomes its fraction.  `*refusal` is set for a mesh or
+// voxel target.
+__device__ __noinline__ int32_t SweepStaticTargets(const m3WorldView& w, const m3Pos3* com0,
+                                                   const m3Quat* rot0, int32_t i, int32_t sh,
+                                                   int32_t shapeMax, const double* lo,
+                                                   const double* hi, const m3Pos3& base,
+                                                   const m3ProxyDev& proxyB,
+                                                   const m3SweepDev& fastSweep, m3real* fraction,
+                                                   int32_t* refusal)
+{
+    const m3real limit = *fraction;
+    int32_t hits = 0;
+    m3real hitFraction = limit;
+    for (int32_t o = 0; o < shapeMax; ++o)
+    {
+        if (w.shapeAlive[o] == 0 || w.shapeType[o] == M3_SHAPE_PLANE || o == sh ||
+            w.proxyId[o] == M3_TREE_NULL)
+        {
+            continue;
+        }
+        const int32_t ob = w.shapeBody[o];
+        if (ob == i || w.enabled[ob] == 0 || w.bullet[ob] != 0 || w.sensor[o] != 0)
+        {
+            continue;
+        }
+        const m3TreeNode& leaf = w.treeNodes[w.proxyId[o]];
+        if (!(leaf.lo[0] <= hi[0] && lo[0] <= leaf.hi[0] && leaf.lo[1] <= hi[1] &&
+              lo[1] <= leaf.hi[1] && leaf.lo[2] <= hi[2] && lo[2] <= leaf.hi[2]))
+        {
+            continue;
+        }
+        if (w.shapeType[o] == M3_SHAPE_MESH || w.shapeType[o] == M3_SHAPE_VOXEL)
+        {
+            *refusal = 3003;
+            continue;
+        }
+        if (w.btype[ob] != M3_BODY_STATIC)
+        {
+            continue; // only bullets sweep against moving bodies
+        }
+        const int32_t gi = w.group[o];
+        if (gi != 0 && gi == w.group[sh])
+        {
+            if (gi < 0)
+            {
+                continue;
+            }
+        }
+        else if (!((w.category[o] & w.mask[sh]) != 0 &&
+                   (w.category[sh] & w.mask[o]) != 0))
+        {
+            continue;
+        }
+        m3Vec3 scratchA[2];
+        m3ProxyDev proxyA;
+        proxyA.count = ProxyPoints(w, o, &proxyA.points, scratchA, &proxyA.radius);
+        // The target's sweep relative to the fast body's base
+        // (solver.c:3065-3079).
+        const m3Pos3 oc0 = com0[ob];
+        const m3Transform oxf = w.xf[ob];
+        const m3Vec3 orlc = m3RotateVec3(oxf.q, w.lc[ob]);
+        m3SweepDev sweepA;
+        sweepA.localCenter = w.lc[ob];
+        sweepA.c1 = v3((m3real)(oc0.x - base.x), (m3real)(oc0.y - base.y),
+                       (m3real)(oc0.z - base.z));
+        sweepA.c2 = v3((m3real)(oxf.p.x + (double)orlc.x - base.x),
+                       (m3real)(oxf.p.y + (double)orlc.y - base.y),
+                       (m3real)(oxf.p.z + (double)orlc.z - base.z));
+        sweepA.q1 = rot0[ob];
+        sweepA.q2 = oxf.q;
+        int32_t state;
+        const m3real t =
+            m3TimeOfImpactDev(proxyA, sweepA, proxyB, fastSweep, limit, &state);
+        if (state == M3_TOI_HIT && 0.0f < t && t < limit)
+        {
+            hits += 1;
+            hitFraction = t;
+        }
+    }
+    if (hits == 1)
+    {
+        *fraction = hitFraction;
+    }
+    return hits;
+}
+
 // Kernel 4: continuous collision against planes and the sleep pass
 // ---------------------------------------------------------------------
-__global__ void __launch_bounds__(M3_BLOCK) m3FinishKernel(const m3WorldView* views,
+__global__ void __launch_bounds__(M3_BLOCK, 2) m3FinishKernel(const m3WorldView* views,
                                                            const int32_t* order, int32_t count,
                                                            float dt, int32_t substeps)
 {
@@ -2225,8 +2316,8 @@ __global__ void __launch_bounds__(M3_BLOCK) m3FinishKernel(const m3WorldView* vi
     // Continuous phase (solver.c:3349-3425).  A non-bullet fast body
     // sweeps only against static targets, and a pull-back moves only the
     // fast body itself, so bodies are independent and run in parallel.
-    // Planes are swept here; a static non-plane target in range, or a
-    // bullet, is refused.
+    // Static tree targets and then planes are swept per shape; a bullet,
+    // a mesh or voxel target, or two tree hits for one shape are refused.
     if (sc->continuousEnabled != 0)
     {
         for (int32_t i = tid; i < bodyMax; i += M3_BLOCK)
@@ -2270,36 +2361,42 @@ __global__ void __launch_bounds__(M3_BLOCK) m3FinishKernel(const m3WorldView* vi
                             (c0.z < cz ? c0.z : cz) - pad};
             double hi[3] = {(c0.x > cx ? c0.x : cx) + pad, (c0.y > cy ? c0.y : cy) + pad,
                             (c0.z > cz ? c0.z : cz) + pad};
+            m3SweepDev fastSweep;
+            fastSweep.localCenter = lc;
+            fastSweep.c1 = sc1;
+            fastSweep.c2 = sc2;
+            fastSweep.q1 = q0;
+            fastSweep.q2 = xfEnd.q;
             for (int32_t sh = w.shapeHead[i]; sh != -1; sh = w.shapeNext[sh])
             {
                 if (w.sensor[sh] != 0)
                 {
                     continue;
                 }
-                // Static non-plane shapes whose fresh bounds touch the
-                // swept box would need the general time of impact.
-                for (int32_t o = 0; o < shapeMax; ++o)
+                // The tree query (solver.c:3081-3274): static targets whose
+                // tree leaf touches the swept box, each swept by the time
+                // of impact.  Static leaves never move, so their boxes are
+                // read straight from the tree.  The reference visits them
+                // in tree order, each call bounded by the fraction so far;
+                // with one hit the order does not matter (every target
+                // sees the fraction of the earlier shapes), with two or
+                // more it would, and the world is refused.
+                m3Vec3 scratchB[2];
+                m3ProxyDev proxyB;
+                proxyB.count = ProxyPoints(w, sh, &proxyB.points, scratchB, &proxyB.radius);
+                int32_t refusal = 0;
+                const int32_t hits = SweepStaticTargets(w, s.com0, s.rot0, i, sh, shapeMax, lo, hi,
+                                                        base, proxyB, fastSweep, &fraction,
+                                                        &refusal);
+                if (refusal != 0)
                 {
-                    if (w.shapeAlive[o] == 0 || w.shapeType[o] == M3_SHAPE_PLANE)
-                    {
-                        continue;
-                    }
-                    int32_t ob = w.shapeBody[o];
-                    if (ob == i || w.btype[ob] != M3_BODY_STATIC || w.enabled[ob] == 0)
-                    {
-                        continue;
-                    }
-                    const m3Aabb& ab = s.aabb[o];
-                    if (ab.hi[0] + (double)M3_AABB_MARGIN >= lo[0] &&
-                        ab.lo[0] - (double)M3_AABB_MARGIN <= hi[0] &&
-                        ab.hi[1] + (double)M3_AABB_MARGIN >= lo[1] &&
-                        ab.lo[1] - (double)M3_AABB_MARGIN <= hi[1] &&
-                        ab.hi[2] + (double)M3_AABB_MARGIN >= lo[2] &&
-                        ab.lo[2] - (double)M3_AABB_MARGIN <= hi[2])
-                    {
-                        s_status = M3GPU_ERR_UNSUPPORTED;
-                        sc->statusDetail = 3002;
-                    }
+                    s_status = M3GPU_ERR_UNSUPPORTED;
+                    sc->statusDetail = refusal;
+                }
+                if (hits > 1)
+                {
+                    s_status = M3GPU_ERR_UNSUPPORTED;
+                    sc->statusDetail = 3002;
                 }
                 for (int32_t p = 0; p < shapeMax; ++p)
                 {

@@ -32,6 +32,7 @@ CASES = [
     ("towers_16_s8", 4, 8, 16, 1.0 / 60.0, 4, 180, [1, 15, 30, 90, 180]),
     ("terrain_30_s1", 5, 1, 30, 1.0 / 60.0, 4, 200, [1, 10, 50, 200]),
     ("terrain_60_s2", 5, 2, 60, 1.0 / 60.0, 4, 120, [1, 30, 120]),
+    ("shots_24_s3", 6, 3, 24, 1.0 / 60.0, 4, 60, [1, 10, 30, 60]),
 ]
 
 
