@@ -61,6 +61,7 @@ METRIC = "bit-exact body-substeps/s"
 UNIT = "body-substeps/s"
 DT = 1.0 / 60.0
 SCENE_UNEVEN = 2
+SCENE_TERRAIN = 5
 
 # Algorithmic bytes per unit of work of the substep loop (the
 # reference's record layouts): per moving body per substep, integrate
@@ -269,6 +270,67 @@ def run_reference_arm(args) -> None:
     print(json.dumps(line))
 
 
+def terrain_run(m3, args, seed: int) -> dict:
+    """Batched heightfield worlds: spheres, capsules and boxes settling on
+    seeded terrain (the heightfield narrowphase), body counts log-uniform
+    in [32, 512].  Device-resident steps timed with CUDA events; the
+    reference steps a bounded sample of the same worlds on the host cores,
+    and every sampled world's hash is compared with the device's."""
+    import torch
+    from oracle import ref
+    count = args.terrain_worlds
+    sizes = world_sizes(m3.lib, seed, count, 32, 512)
+    batch = m3.WorldBatch([m3.World.scene(SCENE_TERRAIN, seed + i, n)
+                           for i, n in enumerate(sizes)])
+    m3.reserve_worlds(batch)
+    m3.upload_worlds(batch)
+    steps = args.terrain_steps
+    m3.step_worlds(batch, DT, args.substeps, 3)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    m3.step_worlds(batch, DT, args.substeps, steps)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    value = body_substeps(sizes, args.substeps, steps) / (ms / 1000.0)
+    got = m3.hash_worlds(batch)
+    # Reference: the first worlds, each stepped the same 3 + `steps` steps.
+    lib = ref.lib()
+    threads = min(16, os.cpu_count() or 1)
+    sample = []
+    budget = max(2.0, args.cpu_seconds / 2)
+    busy = 0.0
+    mismatches = 0
+    k = 0
+    while k < count and busy < budget:
+        wave = list(range(k, min(k + threads, count)))
+        k = wave[-1] + 1
+        worlds = [ref.RefWorld.scene(SCENE_TERRAIN, seed + i, sizes[i]) for i in wave]
+        pool = [threading.Thread(target=lib.m3o_step_trace,
+                                 args=(w.id, DT, args.substeps, 3 + steps, None)) for w in worlds]
+        t0 = time.perf_counter()
+        for t in pool:
+            t.start()
+        for t in pool:
+            t.join()
+        busy += time.perf_counter() - t0
+        for i, w in zip(wave, worlds):
+            mismatches += int(w.hash() != int(got[i]))
+            w.destroy()
+        sample.extend(wave)
+    cpu = body_substeps([sizes[i] for i in sample], args.substeps, 3 + steps) / busy
+    for w in batch:
+        w.destroy()
+    return {"workload": f"{count} heightfield worlds, bodies log-uniform [32, 512] "
+                        "(spheres, capsules, boxes on seeded terrain)",
+            "value": value, "unit": UNIT, "steps": steps, "ms_per_step": ms / steps,
+            "cpu_reference": {"value": cpu, "unit": UNIT, "cores": threads,
+                              "sample": f"first {len(sample)} worlds, {3 + steps} steps each"},
+            "bit_exact_check": {"worlds_checked": len(sample), "mismatches": mismatches}}
+
+
 def serving_run(m3, requests: int, seed: int, rates: list[float]) -> dict:
     """Serving: replay containers (a snapshot of a world of 200-5000
     bodies plus a journal of 4-16 frames, each frame 1-8 linear impulses
@@ -365,6 +427,8 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--serving-requests", type=int, default=256)
+    ap.add_argument("--terrain-worlds", type=int, default=1024)
+    ap.add_argument("--terrain-steps", type=int, default=20)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -544,6 +608,9 @@ def main() -> None:
                              f"{args.warmup + args.steps} steps each, {threads} host threads; "
                              f"every sampled world's final hash compared with the device's"}
 
+    terrain = None
+    if rank == 0 and args.terrain_worlds > 0 and not args.no_cpu_baseline:
+        terrain = terrain_run(m3, args, rank_seed + 91)
     serving = None
     if args.serving_requests > 0:
         serving = serving_run(m3, args.serving_requests, rank_seed + 77, [400.0, 0.0])
@@ -557,7 +624,7 @@ def main() -> None:
             "config": config_block(args, total_dynamic_bodies_per_gpu=int(sum(sizes))),
             "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
             "cpu_baseline": cpu, "plain_gpu": plain, "bit_exact_check": verified,
-            "hash_ms": hash_ms, "clocks": clocks, "serving": serving,
+            "hash_ms": hash_ms, "clocks": clocks, "terrain": terrain, "serving": serving,
         }
         print(json.dumps(line))
     if world_size > 1:

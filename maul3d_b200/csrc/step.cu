@@ -502,6 +502,12 @@ __device__ __forceinline__ void SweepFrom(const m3WorldView& w, const m3Scratch&
     }
 }
 
+// Rows longer than this are ordered by the whole block (at most
+// M3_LONG_ROWS of them per world per step; any further ones by their
+// thread).
+#define M3_LONG_ROW 64
+#define M3_LONG_ROWS 16
+
 template <int NT, int MIN_BLOCKS>
 __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3BroadKernel(const m3WorldView* views,
                                                           const int32_t* order, int32_t count,
@@ -780,8 +786,17 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3BroadKernel(const m3WorldVie
             }
         }
     }
+    // Order each non-plane row by partner index: a short row by one
+    // thread's insertion sort; a long one (a heightfield's, or a large
+    // static shape's, pairs with much of the world) by the whole block,
+    // each key written at its rank (keys in a row are distinct).
+    __shared__ int32_t s_longRows[M3_LONG_ROWS];
+    __shared__ int32_t s_longCount;
+    if (tid == 0)
+    {
+        s_longCount = 0;
+    }
     __syncthreads();
-    // Order each non-plane row by partner index (rows are short).
     for (int32_t i = tid; i < shapeMax; i += NT)
     {
         if (w.shapeAlive[i] == 0 || w.shapeType[i] == M3_SHAPE_PLANE)
@@ -790,6 +805,15 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3BroadKernel(const m3WorldVie
         }
         const int32_t a = s.rowCount[i];
         const int32_t c = s.rowFill[i];
+        if (c > M3_LONG_ROW)
+        {
+            const int32_t slot = atomicAdd(&s_longCount, 1);
+            if (slot < M3_LONG_ROWS)
+            {
+                s_longRows[slot] = i;
+                continue;
+            }
+        }
         for (int32_t x = a + 1; x < a + c; ++x)
         {
             uint64_t key = newKeys[x];
@@ -803,6 +827,30 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3BroadKernel(const m3WorldVie
         }
     }
     __syncthreads();
+    // The long rows; the sweep's pair list is spent and holds each row's
+    // sorted copy (a row is no longer than the pair capacity).
+    const int32_t longRows = s_longCount < M3_LONG_ROWS ? s_longCount : M3_LONG_ROWS;
+    for (int32_t r = 0; r < longRows; ++r)
+    {
+        const int32_t a = s.rowCount[s_longRows[r]];
+        const int32_t c = s.rowFill[s_longRows[r]];
+        for (int32_t x = tid; x < c; x += NT)
+        {
+            const uint64_t key = newKeys[a + x];
+            int32_t rank = 0;
+            for (int32_t y = 0; y < c; ++y)
+            {
+                rank += newKeys[a + y] < key ? 1 : 0;
+            }
+            s.sweepPairs[rank] = key;
+        }
+        __syncthreads();
+        for (int32_t x = tid; x < c; x += NT)
+        {
+            newKeys[a + x] = s.sweepPairs[x];
+        }
+        __syncthreads();
+    }
     M3_PHASE_MARK(M3_PHASE_FILL)
     if (tid == 0)
     {
