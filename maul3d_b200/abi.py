@@ -276,6 +276,10 @@ def bind_create(lib: C.CDLL) -> C.CDLL:
     lib.m3CreateCapsuleShape.restype = m3ShapeId
     lib.m3CreateBoxShape.argtypes = [m3BodyId, C.POINTER(m3ShapeDef), m3Vec3]
     lib.m3CreateBoxShape.restype = m3ShapeId
+    lib.m3CreateHeightFieldGridShape.argtypes = [m3BodyId, C.POINTER(m3ShapeDef),
+                                                 C.POINTER(C.c_float), C.c_int32, C.c_int32,
+                                                 C.c_float]
+    lib.m3CreateHeightFieldGridShape.restype = m3ShapeId
     lib.m3DefaultJointDef.restype = m3JointDef
     lib.m3CreateJoint.argtypes = [C.POINTER(m3JointDef)]
     lib.m3CreateJoint.restype = m3JointId
