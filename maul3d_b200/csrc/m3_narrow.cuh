@@ -487,9 +487,14 @@ enum
     M3F_ROUND = 4, // hull-sphere, capsule-sphere, capsule-capsule: GJK on the cores
     M3F_PLANE_SPHERE = 5,
     M3F_SPHERE_SPHERE = 6,
-    M3F_TERRAIN = 7, // heightfield versus sphere, capsule or hull
-    M3F_UNSUPPORTED = 8,
-    M3F_COUNT = 9
+    // Heightfield pairs, bucketed by partner so that a warp runs one
+    // triangle kernel (any other partner joins the sphere bucket and
+    // collides with nothing).
+    M3F_TERRAIN_SPHERE = 7,
+    M3F_TERRAIN_CAPSULE = 8,
+    M3F_TERRAIN_HULL = 9,
+    M3F_UNSUPPORTED = 10,
+    M3F_COUNT = 11
 };
 
 __device__ __forceinline__ int32_t m3PairFamily(uint8_t typeA, uint8_t typeB)
@@ -505,7 +510,10 @@ __device__ __forceinline__ int32_t m3PairFamily(uint8_t typeA, uint8_t typeB)
     }
     if (typeA == M3_SHAPE_HEIGHTFIELD || typeB == M3_SHAPE_HEIGHTFIELD)
     {
-        return M3F_TERRAIN;
+        const uint8_t other = typeA == M3_SHAPE_HEIGHTFIELD ? typeB : typeA;
+        return other == M3_SHAPE_HULL      ? M3F_TERRAIN_HULL
+               : other == M3_SHAPE_CAPSULE ? M3F_TERRAIN_CAPSULE
+                                           : M3F_TERRAIN_SPHERE;
     }
     if (typeA >= M3_SHAPE_MESH || typeB >= M3_SHAPE_MESH)
     {
@@ -554,7 +562,7 @@ __device__ int32_t m3CollideFamily(const m3WorldView& w, uint64_t key, m3Manifol
         *out = fresh;
         return M3_NARROW_UNSUPPORTED;
     }
-    if (F == M3F_TERRAIN)
+    if (F == M3F_TERRAIN_SPHERE || F == M3F_TERRAIN_CAPSULE || F == M3F_TERRAIN_HULL)
     {
         // manifold.c:2391-2402: only spheres, capsules and hulls collide
         // with a heightfield; any other partner leaves the manifold empty.
@@ -978,8 +986,12 @@ __device__ int32_t m3CollidePair(const m3WorldView& w, uint64_t key, m3Manifold*
         return m3CollideFamily<M3F_PLANE_SPHERE>(w, key, out);
     case M3F_SPHERE_SPHERE:
         return m3CollideFamily<M3F_SPHERE_SPHERE>(w, key, out);
-    case M3F_TERRAIN:
-        return m3CollideFamily<M3F_TERRAIN>(w, key, out);
+    case M3F_TERRAIN_SPHERE:
+        return m3CollideFamily<M3F_TERRAIN_SPHERE>(w, key, out);
+    case M3F_TERRAIN_CAPSULE:
+        return m3CollideFamily<M3F_TERRAIN_CAPSULE>(w, key, out);
+    case M3F_TERRAIN_HULL:
+        return m3CollideFamily<M3F_TERRAIN_HULL>(w, key, out);
     default:
         return m3CollideFamily<M3F_UNSUPPORTED>(w, key, out);
     }

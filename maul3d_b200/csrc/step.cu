@@ -2977,7 +2977,8 @@ static int32_t s_narrowGrid = 148 * 16;
 
 // The narrowphase of one step: family count and scatter, then one
 // kernel per covered family over its bucket.
-#define M3_NARROW_LAUNCHES (2 + M3F_TERRAIN)
+#define M3_NARROW_LAUNCHES (2 + M3F_TERRAIN_SPHERE)
+#define M3_TERRAIN_LAUNCHES 3
 // Batches of at most this many worlds take the single narrowphase kernel.
 #define M3_NARROW_SMALL_BATCH 4
 
@@ -3014,7 +3015,11 @@ static void LaunchNarrow(const m3WorldView* views, const int32_t* offsets, int32
     if (terrain)
     {
         // Heightfield pairs, only in batches holding a heightfield.
-        m3NarrowFamilyKernel<M3F_TERRAIN>
+        m3NarrowFamilyKernel<M3F_TERRAIN_SPHERE>
+            <<<s_narrowGrid, 128>>>(views, offsets, count, famStart, bucket);
+        m3NarrowFamilyKernel<M3F_TERRAIN_CAPSULE>
+            <<<s_narrowGrid, 128>>>(views, offsets, count, famStart, bucket);
+        m3NarrowFamilyKernel<M3F_TERRAIN_HULL>
             <<<s_narrowGrid, 128>>>(views, offsets, count, famStart, bucket);
     }
 }
@@ -3323,7 +3328,7 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
         LaunchSolve(s_batch.dviews, s_batch.dorder, count, dt, substeps, s_batch.cacheBytes,
                     ev + 2, s_batch.classFirst, s_batch.classCache);
         cudaEventRecord(ev[4]);
-        s_launches += 5 + (count <= M3_NARROW_SMALL_BATCH ? 1 : M3_NARROW_LAUNCHES + (anyTerrain ? 1 : 0));
+        s_launches += 5 + (count <= M3_NARROW_SMALL_BATCH ? 1 : M3_NARROW_LAUNCHES + (anyTerrain ? M3_TERRAIN_LAUNCHES : 0));
     }
     if (anyTracked && steps > 0)
     {
