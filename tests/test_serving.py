@@ -13,7 +13,7 @@ import pytest
 
 from conftest import cuda_available
 from maul3d_b200 import abi
-from maul3d_b200.abi import SCENE_TOWERS, SCENE_UNEVEN
+from maul3d_b200.abi import SCENE_TERRAIN, SCENE_TOWERS, SCENE_UNEVEN
 
 
 def _snapshot(lib, wid) -> bytes:
@@ -77,8 +77,12 @@ def _requests(oracle, ref, count, seed):
     rng = np.random.default_rng(seed)
     reqs = []
     for i in range(count):
-        scene, param = (SCENE_TOWERS, 2) if i % 5 == 4 else (SCENE_UNEVEN,
-                                                              int(rng.integers(200, 700)))
+        if i % 5 == 4:
+            scene, param = SCENE_TOWERS, 2
+        elif i % 5 == 3:
+            scene, param = SCENE_TERRAIN, int(rng.integers(40, 200))
+        else:
+            scene, param = SCENE_UNEVEN, int(rng.integers(200, 700))
         r = oracle.RefWorld.scene(scene, 900 + i, param)
         r.step(1.0 / 60.0, 4, int(rng.integers(1, 30)))
         snap = _snapshot(ref, r.id)

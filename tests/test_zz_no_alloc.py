@@ -12,7 +12,7 @@ import ctypes as C
 import pytest
 
 from conftest import cuda_available
-from maul3d_b200.abi import SCENE_BOX_PYRAMID, SCENE_UNEVEN, m3WorldId
+from maul3d_b200.abi import SCENE_BOX_PYRAMID, SCENE_SHOTS, SCENE_TERRAIN, SCENE_UNEVEN, m3WorldId
 
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not cuda_available(), reason="needs a CUDA device")]
@@ -25,7 +25,8 @@ def _bind(m3):
     return fn
 
 
-@pytest.mark.parametrize("scene,seed,param", [(SCENE_UNEVEN, 41, 200), (SCENE_UNEVEN, 42, 700)])
+@pytest.mark.parametrize("scene,seed,param", [(SCENE_UNEVEN, 41, 200), (SCENE_UNEVEN, 42, 700),
+                                              (SCENE_TERRAIN, 44, 60), (SCENE_SHOTS, 45, 24)])
 def test_noalloc_step_equals_regular_step_twice(m3, scene, seed, param):
     step_noalloc = _bind(m3)
     regular = m3.World.scene(scene, seed, param)
