@@ -608,12 +608,14 @@ def main() -> None:
                              f"{args.warmup + args.steps} steps each, {threads} host threads; "
                              f"every sampled world's final hash compared with the device's"}
 
-    terrain = None
-    if rank == 0 and args.terrain_worlds > 0 and not args.no_cpu_baseline:
-        terrain = terrain_run(m3, args, rank_seed + 91)
     serving = None
     if args.serving_requests > 0:
         serving = serving_run(m3, args.serving_requests, rank_seed + 77, [400.0, 0.0])
+    # The terrain batch runs after the serving loop, so that its host
+    # threads and device memory leave the latency figures alone.
+    terrain = None
+    if rank == 0 and args.terrain_worlds > 0 and not args.no_cpu_baseline:
+        terrain = terrain_run(m3, args, rank_seed + 91)
 
     if rank == 0:
         line = {
