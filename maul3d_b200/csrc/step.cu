@@ -2272,6 +2272,14 @@ __device__ __noinline__ int32_t SweepStaticTargets(const m3WorldView& w, const m
         {
             continue;
         }
+        // Only bullets sweep against moving bodies.  (The reference tests
+        // this after the mesh and voxel cases; those shapes live on static
+        // bodies only, so testing it first, before the leaf is read,
+        // changes nothing.)
+        if (w.btype[ob] != M3_BODY_STATIC)
+        {
+            continue;
+        }
         const m3TreeNode& leaf = w.treeNodes[w.proxyId[o]];
         if (!(leaf.lo[0] <= hi[0] && lo[0] <= leaf.hi[0] && leaf.lo[1] <= hi[1] &&
               lo[1] <= leaf.hi[1] && leaf.lo[2] <= hi[2] && lo[2] <= leaf.hi[2]))
@@ -2282,10 +2290,6 @@ __device__ __noinline__ int32_t SweepStaticTargets(const m3WorldView& w, const m
         {
             *refusal = 3003;
             continue;
-        }
-        if (w.btype[ob] != M3_BODY_STATIC)
-        {
-            continue; // only bullets sweep against moving bodies
         }
         const int32_t gi = w.group[o];
         if (gi != 0 && gi == w.group[sh])
@@ -2368,6 +2372,24 @@ __global__ void __launch_bounds__(M3_BLOCK, 2) m3FinishKernel(const m3WorldView*
     // a mesh or voxel target, or two tree hits for one shape are refused.
     if (sc->continuousEnabled != 0)
     {
+        // Whether the world holds any static non-plane shape: without one
+        // the tree arm finds nothing, and fast bodies meet only planes.
+        __shared__ int32_t s_targets;
+        if (tid == 0)
+        {
+            s_targets = 0;
+        }
+        __syncthreads();
+        for (int32_t o = tid; o < shapeMax; o += M3_BLOCK)
+        {
+            if (w.shapeAlive[o] != 0 && w.shapeType[o] != M3_SHAPE_PLANE &&
+                w.btype[w.shapeBody[o]] == M3_BODY_STATIC)
+            {
+                s_targets = 1;
+            }
+        }
+        __syncthreads();
+        const bool staticTargets = s_targets != 0;
         for (int32_t i = tid; i < bodyMax; i += M3_BLOCK)
         {
             if (w.bodyAlive[i] == 0 || w.btype[i] != M3_BODY_DYNAMIC)
@@ -2433,9 +2455,10 @@ __global__ void __launch_bounds__(M3_BLOCK, 2) m3FinishKernel(const m3WorldView*
                 m3ProxyDev proxyB;
                 proxyB.count = ProxyPoints(w, sh, &proxyB.points, scratchB, &proxyB.radius);
                 int32_t refusal = 0;
-                const int32_t hits = SweepStaticTargets(w, s.com0, s.rot0, i, sh, shapeMax, lo, hi,
-                                                        base, proxyB, fastSweep, &fraction,
-                                                        &refusal);
+                const int32_t hits =
+                    staticTargets ? SweepStaticTargets(w, s.com0, s.rot0, i, sh, shapeMax, lo, hi,
+                                                       base, proxyB, fastSweep, &fraction, &refusal)
+                                  : 0;
                 if (refusal != 0)
                 {
                     s_status = M3GPU_ERR_UNSUPPORTED;
