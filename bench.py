@@ -156,8 +156,12 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def build_worlds(m3, sizes: list[int], seed: int):
-    return [m3.World.scene(SCENE_UNEVEN, seed + i, n) for i, n in enumerate(sizes)]
+def build_worlds(m3, sizes: list[int], seeds):
+    """Seeded uneven worlds; `seeds` is a list (one per world) or a base
+    seed (world i gets seed + i)."""
+    if isinstance(seeds, int):
+        seeds = [seeds + i for i in range(len(sizes))]
+    return [m3.World.scene(SCENE_UNEVEN, s, n) for s, n in zip(seeds, sizes)]
 
 
 def body_substeps(sizes: list[int], substeps: int, steps: int) -> int:
@@ -211,6 +215,14 @@ def reference_run(sizes, seed, substeps, steps, threads, time_budget_s, want_has
 
 
 def run_reference_arm(args) -> None:
+    """The reference engine alone (oracle/_ref, built from its own
+    sources; this library is never loaded) on every host thread, for the
+    device arm's metric and workload: all of the batch's worlds, in waves
+    of at most 64 (the reference's world table).  Per wave the worlds are
+    built (untimed), stepped W warm-up steps (untimed), then K timed
+    steps, one world per task, largest first; the value is the K steps'
+    body-substeps of every world over the summed wall time of the waves'
+    timed phases."""
     rank = env_int("RANK", 0)
     if rank != 0:
         return
@@ -221,16 +233,16 @@ def run_reference_arm(args) -> None:
         return
     lib = ref.lib()
     threads = os.cpu_count() or 1
-    sizes = world_sizes(lib, args.seed, args.worlds, args.lo, args.hi)
-    # Each step: one m3World_Step of every world of a bounded sample of
-    # the batch (its first worlds, at most the reference's 64-world
-    # table), spread over all host threads; the sample worlds persist
-    # across steps like the device's.
-    sample = min(len(sizes), args.ref_sample, 64)
-    worlds = [ref.RefWorld.scene(SCENE_UNEVEN, args.seed + i, sizes[i]) for i in range(sample)]
+    # Rank 0's shard of the job's world list (the whole list at N=1).
+    from maul3d_b200.shard import partition, shard_sizes, world_cost
+    world_size = env_int("WORLD_SIZE", 1)
+    all_sizes = shard_sizes(lib, args.seed, args.worlds * world_size, args.lo, args.hi)
+    mine = partition([world_cost(n) for n in all_sizes], world_size)[0]
+    sizes = [all_sizes[i] for i in mine]
+    seeds = [args.seed + i for i in mine]
 
-    def step_all() -> float:
-        queue = list(range(sample))
+    def run_pool(worlds, order, steps) -> float:
+        queue = list(order)
         lock = threading.Lock()
 
         def worker():
@@ -239,32 +251,40 @@ def run_reference_arm(args) -> None:
                     if not queue:
                         return
                     k = queue.pop(0)
-                lib.m3o_step_trace(worlds[k].id, DT, args.substeps, 1, None)
+                lib.m3o_step_trace(worlds[k].id, DT, args.substeps, steps, None)
 
         t0 = time.perf_counter()
-        pool = [threading.Thread(target=worker) for _ in range(threads)]
+        pool = [threading.Thread(target=worker) for _ in range(min(threads, len(order)))]
         for t in pool:
             t.start()
         for t in pool:
             t.join()
         return time.perf_counter() - t0
 
-    for _ in range(args.warmup):
-        step_all()
-    total_s = sum(step_all() for _ in range(args.steps))
-    total_bs = body_substeps(sizes[:sample], args.substeps, args.steps)
-    for w in worlds:
-        w.destroy()
+    total_s = 0.0
+    waves = 0
+    for first in range(0, len(sizes), 64):
+        wave = list(range(first, min(first + 64, len(sizes))))
+        worlds = [ref.RefWorld.scene(SCENE_UNEVEN, seeds[i], sizes[i]) for i in wave]
+        order = sorted(range(len(wave)), key=lambda k: -sizes[wave[k]])
+        run_pool(worlds, order, args.warmup)
+        total_s += run_pool(worlds, order, args.steps)
+        for w in worlds:
+            w.destroy()
+        waves += 1
+    total_bs = body_substeps(sizes, args.substeps, args.steps)
     value = total_bs / total_s
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
-        "n_gpus": env_int("WORLD_SIZE", 1), "steps": args.steps, "warmup": args.warmup,
+        "n_gpus": world_size, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * total_s / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-        "config": config_block(args, sample_worlds=sample),
+        "config": config_block(args, total_dynamic_bodies_per_gpu=int(sum(sizes))),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
-                         "sample": f"first {sample} of {args.worlds} worlds, one step each per "
-                                   f"timed step, {threads} host threads"},
+                         "sample": f"all {len(sizes)} worlds in {waves} waves of <= 64 (the "
+                                   f"reference's world table), {args.warmup} untimed + "
+                                   f"{args.steps} timed steps each, {threads} host threads, "
+                                   f"one world per task, largest first"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -402,7 +422,8 @@ def config_block(args, **extra) -> dict:
                        f"capsule chains, dt 1/60, {args.substeps} substeps",
            "worlds_per_gpu": args.worlds, "substeps": args.substeps, "dt": DT, "seed": args.seed,
            "l2": "inputs larger than L2 (world slabs total several GB)",
-           "parallelism": "one block per world; worlds sharded across ranks (weak scaling)"}
+           "parallelism": "one block per world; worlds split across ranks by estimated cost, "
+                          "bodies + pairs (weak scaling)"}
     cfg.update(extra)
     return cfg
 
@@ -450,10 +471,16 @@ def main() -> None:
         dist.init_process_group("nccl", timeout=timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
 
-    from maul3d_b200.shard import rank_seed as shard_seed, shard_sizes
-    rank_seed = shard_seed(args.seed, rank)
-    sizes = shard_sizes(m3.lib, rank_seed, args.worlds, args.lo, args.hi)
-    worlds = m3.WorldBatch(build_worlds(m3, sizes, rank_seed))
+    # Weak scaling: the job's world list holds `worlds` per GPU; every
+    # rank computes the same cost-balanced split of it and builds only its
+    # own shard (at N=1 the shard is the whole list, in order).
+    from maul3d_b200.shard import partition, shard_sizes, world_cost
+    all_sizes = shard_sizes(m3.lib, args.seed, args.worlds * world_size, args.lo, args.hi)
+    mine = partition([world_cost(n) for n in all_sizes], world_size)[rank]
+    sizes = [all_sizes[i] for i in mine]
+    seeds = [args.seed + i for i in mine]
+    rank_seed = args.seed + 1_000_003 * rank
+    worlds = m3.WorldBatch(build_worlds(m3, sizes, seeds))
     m3.reserve_worlds(worlds)
     m3.upload_worlds(worlds)
 
@@ -525,7 +552,7 @@ def main() -> None:
     plain = None
     if rank == 0 and args.plain_sample > 0:
         psizes = sizes[:args.plain_sample]
-        pworlds = build_worlds(m3, psizes, rank_seed)
+        pworlds = build_worlds(m3, psizes, seeds[:len(psizes)])
         m3.reserve_worlds(pworlds)
         m3.upload_worlds(pworlds)
         for w in pworlds:
@@ -550,7 +577,7 @@ def main() -> None:
     # K steps and a D2H hash read of every world after every step.
     e2e = None
     if not args.no_e2e:
-        eworlds = m3.WorldBatch(build_worlds(m3, sizes, rank_seed))
+        eworlds = m3.WorldBatch(build_worlds(m3, sizes, seeds))
         tr = time.perf_counter()
         m3.reserve_worlds(eworlds)
         reserve_ms = (time.perf_counter() - tr) * 1e3
@@ -598,7 +625,7 @@ def main() -> None:
         from oracle import ref
         if ref.build():
             threads = os.cpu_count() or 1
-            bs, busy, hashes, n = reference_run(sizes, rank_seed, args.substeps,
+            bs, busy, hashes, n = reference_run(sizes, args.seed, args.substeps,
                                                 args.warmup + args.steps, threads,
                                                 args.cpu_seconds, want_hashes=True)
             mismatched = [i for i, h in hashes.items() if int(device_hashes[i]) != h]

@@ -248,6 +248,61 @@ M3GPU_API void m3World_Step(m3WorldId worldId, float dt, int32_t substeps);
  * stale id. */
 M3GPU_API uint64_t m3World_Hash(m3WorldId worldId);
 
+/* world.h:531-554 (world.c:917-951): the world's live counts and the
+ * last step's solver figures.  colorCount counts the non-empty graph
+ * colours of the last step, the overflow colour included (17 when it was
+ * used).  scratchPeak and scratchCapacity report the world's device
+ * scratch bytes (the device step carves all of it each step);
+ * allocCalls/freeCalls count the library's device block allocations and
+ * frees.  Zeroes for a stale id. */
+typedef struct m3Counters
+{
+    int32_t bodyCount;
+    int32_t shapeCount;
+    int32_t jointCount;
+    int32_t contactCount;
+    int32_t awakeCount;
+    int32_t islandCount;
+    int32_t colorCount;
+    int32_t characterCount;
+    int32_t vehicleCount;
+    int32_t softBodyCount;
+    int32_t voxelChunkCount;
+    int32_t hullCount;
+    int32_t meshCount;
+    int32_t treeHeight;
+    int32_t scratchPeak;
+    int32_t scratchCapacity;
+    int32_t snapshotBytes;
+    int64_t allocCalls;
+    int64_t freeCalls;
+} m3Counters;
+M3GPU_API m3Counters m3World_GetCounters(m3WorldId worldId);
+
+/* world.h:578-593 (world.c:955-965): milliseconds of the world's last
+ * step by phase, measured on the device with CUDA events around the
+ * stages of the batch the world was stepped in: broadphase (bounds and
+ * pairs), narrowphase, prepare (islands, colouring, constraint rows),
+ * solve (the substep loop, restitution, store) and continuous (the
+ * continuous phase and the sleep pass, one kernel); step is their sum.
+ * Stages this path does not run report 0.  Zeroes before the first
+ * device step and for a stale id. */
+typedef struct m3Profile
+{
+    float step;
+    float vehicles;
+    float broadphase;
+    float narrowphase;
+    float events;
+    float prepare;
+    float solve;
+    float continuous;
+    float sleep;
+    float characters;
+    float softBodies;
+} m3Profile;
+M3GPU_API m3Profile m3World_GetProfile(m3WorldId worldId);
+
 /* body.c:35 (body.h:43) / body.h:49 / body.h:56-59 */
 M3GPU_API m3BodyDef m3DefaultBodyDef(void);
 M3GPU_API m3BodyId m3CreateBody(m3WorldId worldId, const m3BodyDef* def);
@@ -337,14 +392,15 @@ M3GPU_API int32_t m3gpu_last_error(void);
 M3GPU_API const char* m3gpu_last_error_message(void);
 
 /* Step `count` independent worlds `steps` times each in ONE batched
- * launch sequence (one CTA per world; a CUDA graph captures the step).
+ * launch sequence (one CTA per world in the per-world stages, the
+ * flattened pairs of every world in the narrowphase).
  * Equivalent, world by world and bit for bit, to calling m3World_Step on
  * each world in turn.  Returns M3GPU_OK or an error code; on error no
  * world is partially stepped past the failing step. */
 M3GPU_API int32_t m3gpu_step_worlds(const m3WorldId* worlds, int32_t count, float dt,
                                     int32_t substeps, int32_t steps);
 
-/* World hashes of `count` worlds computed on the device (one thread per
+/* World hashes of `count` worlds computed on the device (one block per
  * world), written to out[i].  Same values as m3World_Hash. */
 M3GPU_API int32_t m3gpu_hash_worlds(const m3WorldId* worlds, int32_t count, uint64_t* out);
 
@@ -371,8 +427,8 @@ M3GPU_API int64_t m3gpu_uploaded_bytes(void);
 /* Allocation-free step of one resident world (no reference counterpart).
  * For callers that must not allocate device memory when they step: a
  * frame loop with a hard deadline (allocating and freeing can stall the
- * whole device), code running while a CUDA graph is being captured, or
- * a host whose device memory belongs to its own pool allocator.  The
+ * whole device), or a host whose device memory belongs to its own pool
+ * allocator.  The
  * world must already be resident (m3gpu_reserve_worlds and
  * m3gpu_upload_worlds, called earlier when allocating was allowed); the
  * step then allocates nothing: its scratch lives in a fixed 4 MiB
@@ -380,9 +436,11 @@ M3GPU_API int64_t m3gpu_uploaded_bytes(void);
  * Worlds whose scratch exceeds that, or with more than about 800 bodies,
  * are refused with M3GPU_ERR_CAPACITY before any device work.  The first
  * call on a device looks up that array's address; make it before any
- * stream capture.  Calls share the array: calls that overlap on the GPU
- * race, so serialise them.  Same result, bit for bit, as
- * m3gpu_step_worlds on the same world. */
+ * stream capture.  The call uses blocking copies on the legacy default
+ * stream, so it must not run while any stream of the process is being
+ * captured.  Calls share the array: the library serialises the calls of
+ * one process, and calls that overlapped on the GPU would race.  Same
+ * result, bit for bit, as m3gpu_step_worlds on the same world. */
 M3GPU_API int32_t m3gpu_step_world_noalloc(m3WorldId world, float dt, int32_t substeps);
 
 /* Wait for all device work of the library to finish. */
@@ -395,10 +453,10 @@ M3GPU_API int64_t m3gpu_launch_count(void);
 M3GPU_API float m3gpu_last_step_ms(void);
 
 /* Device time in milliseconds of the last m3gpu_step_worlds call, split
- * by stage and summed over steps: out[0] collide (bounds, pairs,
- * narrowphase), out[1] prepare (islands, colouring, rows), out[2] the
- * substep loop with restitution and store, out[3] continuous and sleep.
- * `out` holds 4 floats. */
+ * by stage and summed over steps: out[0] broadphase (bounds, pairs),
+ * out[1] narrowphase, out[2] prepare (islands, colouring, rows), out[3]
+ * the substep loop with restitution and store, out[4] continuous and
+ * sleep.  `out` holds 5 floats. */
 M3GPU_API int32_t m3gpu_kernel_ms(float* out);
 
 /* Work counters of one world accumulated over its device steps:

@@ -239,17 +239,32 @@ def uploaded_bytes() -> int:
     return int(lib.m3gpu_uploaded_bytes())
 
 
-STAGES = ("collide", "prepare", "substep", "finish")
+STAGES = ("broad", "narrow", "prepare", "substep", "finish")
 
 
 def kernel_ms() -> dict[str, float]:
     """Device milliseconds of the last batched step call per stage:
-    collide (bounds, pairs, narrowphase), prepare (islands, colouring,
-    rows), substep (the substep loop, restitution, store) and finish
-    (continuous, sleep), each summed over the call's steps."""
+    broad (bounds, pairs), narrow (narrowphase), prepare (islands,
+    colouring, rows), substep (the substep loop, restitution, store) and
+    finish (continuous, sleep), each summed over the call's steps;
+    collide = broad + narrow."""
     out = (C.c_float * len(STAGES))()
     _check(lib.m3gpu_kernel_ms(out))
-    return {name: float(out[k]) for k, name in enumerate(STAGES)}
+    ms = {name: float(out[k]) for k, name in enumerate(STAGES)}
+    ms["collide"] = ms["broad"] + ms["narrow"]
+    return ms
+
+
+def counters(world) -> dict[str, int]:
+    """m3World_GetCounters of one world, as a dict."""
+    c = lib.m3World_GetCounters(world.id)
+    return {name: getattr(c, name) for name, _ in c._fields_}
+
+
+def profile(world) -> dict[str, float]:
+    """m3World_GetProfile of one world (milliseconds of its last step)."""
+    p = lib.m3World_GetProfile(world.id)
+    return {name: getattr(p, name) for name, _ in p._fields_}
 
 
 PHASES = ("islands", "prepare", "colour+movers", "integrate_v", "warm_start", "bias_solve",

@@ -50,14 +50,39 @@ SCENE_FREEFALL = 3
 SCENE_TOWERS = 4
 SCENE_TERRAIN = 5
 SCENE_SHOTS = 6
+SCENE_PLANK = 7
+SCENE_BOUNCE = 8
 
 
 def _ptr(a: np.ndarray) -> C.c_void_p:
     return C.c_void_p(a.ctypes.data)
 
 
+class m3Counters(C.Structure):
+    """world.h:531-552 of the reference."""
+    _fields_ = [(name, C.c_int32) for name in (
+        "bodyCount", "shapeCount", "jointCount", "contactCount", "awakeCount", "islandCount",
+        "colorCount", "characterCount", "vehicleCount", "softBodyCount", "voxelChunkCount",
+        "hullCount", "meshCount", "treeHeight", "scratchPeak", "scratchCapacity",
+        "snapshotBytes")] + [("allocCalls", C.c_int64), ("freeCalls", C.c_int64)]
+
+
+class m3Profile(C.Structure):
+    """world.h:578-591 of the reference (milliseconds)."""
+    _fields_ = [(name, C.c_float) for name in (
+        "step", "vehicles", "broadphase", "narrowphase", "events", "prepare", "solve",
+        "continuous", "sleep", "characters", "softBodies")]
+
+
+assert C.sizeof(m3Counters) == 88 and C.sizeof(m3Profile) == 44
+
+
 def bind_common(lib: C.CDLL) -> C.CDLL:
     """Declare the reference-named entry points shared by both engines."""
+    lib.m3World_GetCounters.argtypes = [m3WorldId]
+    lib.m3World_GetCounters.restype = m3Counters
+    lib.m3World_GetProfile.argtypes = [m3WorldId]
+    lib.m3World_GetProfile.restype = m3Profile
     lib.m3World_Step.argtypes = [m3WorldId, C.c_float, C.c_int32]
     lib.m3World_Step.restype = None
     lib.m3World_Hash.argtypes = [m3WorldId]

@@ -5,6 +5,7 @@
 #include "m3_world.h"
 #include "m3_hash.h"
 #include "m3_ops.h"
+#include "m3_tree.h"
 
 #include <cuda_runtime.h>
 
@@ -102,6 +103,77 @@ extern "C" uint64_t m3World_Hash(m3WorldId worldId)
     m3WorldView view = w->hv;
     view.hulls = w->hulls.empty() ? nullptr : w->hulls.data();
     return m3WorldHashView(&view);
+}
+
+// world.c:917-951: live counts from the (synced) host image, the last
+// step's island and colour counts from the device's scalars.
+extern "C" m3Counters m3World_GetCounters(m3WorldId worldId)
+{
+    m3Counters c;
+    memset(&c, 0, sizeof(c));
+    m3gpuClearError();
+    m3HostWorld* w = m3gpuWorldFromId(worldId);
+    if (w == nullptr || m3gpuSyncHost(w) != M3GPU_OK)
+    {
+        return c;
+    }
+    const m3WorldView& v = w->hv;
+    const m3WorldScalars* sc = v.sc;
+    for (int32_t i = 0; i < sc->bodyMax; ++i)
+    {
+        if (v.bodyAlive[i] != 0)
+        {
+            c.bodyCount += 1;
+            if (v.btype[i] == M3_BODY_DYNAMIC && v.awake[i] != 0)
+            {
+                c.awakeCount += 1;
+            }
+        }
+    }
+    for (int32_t i = 0; i < sc->shapeMax; ++i)
+    {
+        c.shapeCount += v.shapeAlive[i] != 0 ? 1 : 0;
+    }
+    for (int32_t i = 0; i < sc->jointMax; ++i)
+    {
+        c.jointCount += v.jointAlive[i] != 0 ? 1 : 0;
+    }
+    for (int32_t r : w->hullRefs)
+    {
+        c.hullCount += r > 0 ? 1 : 0;
+    }
+    c.contactCount = sc->pairCount;
+    c.islandCount = sc->lastIslandCount;
+    c.colorCount = sc->lastColorCount;
+    c.treeHeight = sc->treeRoot != M3_TREE_NULL ? v.treeNodes[sc->treeRoot].height : 0;
+    const int64_t scratch =
+        w->scratchBytes > 0 ? w->scratchBytes
+                            : m3gpuScratchBytes(w->bodyCap, w->shapeCap, w->jointCap, w->pairCap);
+    c.scratchCapacity = scratch > INT32_MAX ? INT32_MAX : (int32_t)scratch;
+    c.scratchPeak = c.scratchCapacity;
+    c.snapshotBytes = m3World_SnapshotSize(worldId);
+    c.allocCalls = g_m3DevAllocCalls;
+    c.freeCalls = g_m3DevFreeCalls;
+    return c;
+}
+
+// world.c:955-965: the last device step's stage times.
+extern "C" m3Profile m3World_GetProfile(m3WorldId worldId)
+{
+    m3Profile p;
+    memset(&p, 0, sizeof(p));
+    m3HostWorld* w = m3gpuWorldFromId(worldId);
+    if (w == nullptr || !w->profile.valid)
+    {
+        return p;
+    }
+    p.step = w->profile.step;
+    p.broadphase = w->profile.broadphase;
+    p.narrowphase = w->profile.narrowphase;
+    p.prepare = w->profile.prepare;
+    p.solve = w->profile.solve;
+    p.continuous = w->profile.finish;
+    return p;
 }
 
 static int32_t Resolve(const m3WorldId* ids, int32_t count, std::vector<m3HostWorld*>& out)

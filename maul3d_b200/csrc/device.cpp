@@ -25,8 +25,15 @@ static int s_device = 0;
 uint64_t g_m3ResidencyEpoch = 1;
 int64_t g_m3UploadedBytes = 0;
 
+std::recursive_mutex& m3gpuDeviceMutex()
+{
+    static std::recursive_mutex* mu = new std::recursive_mutex(); // lives until exit
+    return *mu;
+}
+
 extern "C" int32_t m3gpu_set_device(int32_t device)
 {
+    M3_DEVICE_GUARD;
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count)
     {
@@ -43,10 +50,19 @@ extern "C" int32_t m3gpu_set_device(int32_t device)
     return M3GPU_OK;
 }
 
+// The current device is a property of the calling host thread: every
+// entry makes the library's device current for its caller, so a thread
+// other than the one that selected it launches on the same GPU.
 int32_t m3gpuEnsureDevice(void)
 {
+    M3_DEVICE_GUARD;
     if (s_deviceState == 1)
     {
+        const cudaError_t e = cudaSetDevice(s_device);
+        if (e != cudaSuccess)
+        {
+            return m3gpuSetError(M3GPU_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
+        }
         return M3GPU_OK;
     }
     if (s_deviceState == -1)
@@ -101,9 +117,13 @@ size_t RoundDev(size_t bytes)
 }
 } // namespace
 
+int64_t g_m3DevAllocCalls = 0;
+int64_t g_m3DevFreeCalls = 0;
+
 static cudaError_t DevAlloc(void** out, size_t bytes)
 {
     DevArena& a = TheDevArena();
+    g_m3DevAllocCalls += 1;
     int device = 0;
     cudaError_t e = cudaGetDevice(&device);
     if (e != cudaSuccess)
@@ -156,6 +176,7 @@ static void DevFree(void* p, size_t bytes)
     {
         return;
     }
+    g_m3DevFreeCalls += 1;
     DevArena& a = TheDevArena();
     for (const DevChunk& c : a.chunks)
     {
@@ -235,6 +256,7 @@ static int32_t UploadHeightFields(m3HostWorld* w)
 
 int32_t m3gpuReserve(m3HostWorld* w)
 {
+    M3_DEVICE_GUARD;
     int32_t rc = m3gpuEnsureDevice();
     if (rc != M3GPU_OK || w->dslab != nullptr)
     {
@@ -455,6 +477,7 @@ static int32_t UploadCopies(m3HostWorld* w)
 
 int32_t m3gpuUpload(m3HostWorld* w)
 {
+    M3_DEVICE_GUARD;
     int32_t rc = UploadPrepare(w);
     return rc == M3GPU_OK ? UploadCopies(w) : rc;
 }
@@ -470,6 +493,7 @@ static int32_t s_itemCap = 0;
 
 int32_t m3gpuUploadBatch(m3HostWorld** worlds, int32_t count)
 {
+    M3_DEVICE_GUARD;
     std::vector<m3UploadItem> items;
     std::vector<m3HostWorld*> batched;
     int64_t bytes = 0;
@@ -581,9 +605,15 @@ int32_t m3gpuUploadBatch(m3HostWorld** worlds, int32_t count)
 
 int32_t m3gpuDownload(m3HostWorld* w)
 {
+    M3_DEVICE_GUARD;
     if (w->dslab == nullptr)
     {
         return M3GPU_OK;
+    }
+    int32_t rc0 = m3gpuEnsureDevice();
+    if (rc0 != M3GPU_OK)
+    {
+        return rc0;
     }
     // Scalars first: they say which pair buffer is current and how long.
     int32_t rc = CudaCheck(cudaMemcpy(w->hv.sc, w->dv.sc, sizeof(m3WorldScalars),
@@ -635,9 +665,14 @@ int32_t m3gpuDownload(m3HostWorld* w)
 
 int32_t m3gpuWorldStatus(m3HostWorld* w)
 {
+    M3_DEVICE_GUARD;
     if (w->dslab == nullptr || !w->deviceAhead)
     {
         return w->hv.sc->status;
+    }
+    if (m3gpuEnsureDevice() != M3GPU_OK)
+    {
+        return m3gpu_last_error();
     }
     int32_t status = 0;
     if (CudaCheck(cudaMemcpy(&status, &w->dv.sc->status, sizeof(int32_t), cudaMemcpyDeviceToHost),
@@ -650,9 +685,14 @@ int32_t m3gpuWorldStatus(m3HostWorld* w)
 
 int32_t m3gpuDownloadPairTails(m3HostWorld* w)
 {
+    M3_DEVICE_GUARD;
     if (w->dslab == nullptr || !w->pairTailsOnDevice)
     {
         return M3GPU_OK;
+    }
+    if (m3gpuEnsureDevice() != M3GPU_OK)
+    {
+        return m3gpu_last_error();
     }
     const int32_t buf = w->hv.sc->pairBuf;
     int32_t rc = CudaCheck(cudaMemcpy(buf == 0 ? w->hv.keys0 : w->hv.keys1,
@@ -676,6 +716,7 @@ int32_t m3gpuDownloadPairTails(m3HostWorld* w)
 
 int32_t m3gpuSyncHost(m3HostWorld* w)
 {
+    M3_DEVICE_GUARD;
     if (!w->deviceAhead)
     {
         return M3GPU_OK;
@@ -685,10 +726,12 @@ int32_t m3gpuSyncHost(m3HostWorld* w)
 
 void m3gpuRelease(m3HostWorld* w)
 {
+    M3_DEVICE_GUARD;
     g_m3ResidencyEpoch += 1;
-    if (w->dslab != nullptr)
+    if (w->dslab != nullptr || w->dhulls != nullptr || w->dhf != nullptr)
     {
         // No copy from the host image may be in flight when it is freed.
+        m3gpuEnsureDevice();
         cudaDeviceSynchronize();
     }
     if (w->dslab != nullptr)

@@ -10,6 +10,7 @@
 #include <stdlib.h>
 #include <new>
 #include <unordered_map>
+#include <mutex>
 #include <vector>
 
 // Host memory for world images and hull buffers (hostmem.cpp): page-
@@ -117,6 +118,19 @@ struct m3FreeRing
     }
 };
 
+// Device milliseconds of a world's last step, per stage (the batch it
+// was stepped in), for m3World_GetProfile.
+struct m3StepProfile
+{
+    float step = 0.0f;
+    float broadphase = 0.0f;
+    float narrowphase = 0.0f;
+    float prepare = 0.0f;
+    float solve = 0.0f;
+    float finish = 0.0f; // continuous phase and sleep
+    bool valid = false;
+};
+
 struct m3HostWorld
 {
     int32_t slot = -1;
@@ -192,6 +206,7 @@ struct m3HostWorld
     // changes them on the device, and a snapshot downloads them.
     bool pairTailsToDevice = false;
     bool pairTailsOnDevice = false;
+    m3StepProfile profile;
 };
 
 // Points a device view at the world's pools outside the slab.
@@ -207,10 +222,23 @@ inline void m3AttachDevicePools(m3HostWorld* w, m3WorldView* view)
 m3HostWorld* m3gpuWorldFromId(m3WorldId id);
 m3HostWorld* m3gpuWorldFromIndex0(uint16_t index0);
 
+// The library's shared device state (the selected device, the batch
+// tables, streams, events, staging buffers, the device chunk allocator
+// and every world's residency) sits behind one process-wide recursive
+// lock, taken by each internal entry below that touches it.  Distinct
+// worlds may therefore be stepped, hashed, snapshotted and restored from
+// distinct host threads (the reference's threading contract): their
+// device work is serialised, each call's result is the one it gets alone.
+std::recursive_mutex& m3gpuDeviceMutex();
+#define M3_DEVICE_GUARD std::lock_guard<std::recursive_mutex> m3DeviceGuard_(m3gpuDeviceMutex())
+
 // Residency (device.cpp).
 extern uint64_t g_m3ResidencyEpoch;
 // Host-to-device bytes copied by uploads (device.cpp).
 extern int64_t g_m3UploadedBytes;
+// Device blocks allocated and freed (device.cpp).
+extern int64_t g_m3DevAllocCalls;
+extern int64_t g_m3DevFreeCalls;
 int32_t m3gpuEnsureDevice(void);
 int32_t m3gpuReserve(m3HostWorld* w);
 int32_t m3gpuUpload(m3HostWorld* w);

@@ -35,6 +35,13 @@
 //                       and capsules above a ground plane (odd seeds add
 //                       a heightfield patch): the continuous phase's time
 //                       of impact against static targets.
+//   M3S_PLANK           `param` small boxes (at least 17) resting on one
+//                       dynamic plank on the ground: the plank carries
+//                       more constraints than there are graph colours,
+//                       so the solver's overflow colour is used.
+//   M3S_BOUNCE          `param` spheres and boxes with restitution 0.3-0.8
+//                       dropped from 2-8 m onto a bouncy ground and onto
+//                       each other: the restitution pass.
 
 #include <m3_scene_api.h> // resolved by -I: product or oracle shim
 
@@ -50,6 +57,8 @@ enum
     M3S_TOWERS = 4,
     M3S_TERRAIN = 5,
     M3S_SHOTS = 6,
+    M3S_PLANK = 7,
+    M3S_BOUNCE = 8,
 };
 
 static uint64_t SceneSplitMix(uint64_t* state)
@@ -546,6 +555,120 @@ static m3WorldId Shots(uint64_t seed, int32_t shots)
     return world;
 }
 
+// A plank (half extents 4.5 x 0.25 x 4.5) on the ground with `boxes`
+// small boxes (half extent 0.35) on a grid on top of it, jittered by the
+// seed, and a few spheres on top of the first boxes.  Every box touches
+// the plank, so the plank's constraints outnumber the 16 graph colours.
+static m3WorldId Plank(uint64_t seed, int32_t boxes)
+{
+    if (boxes < 17)
+    {
+        boxes = 17;
+    }
+    const int32_t spheres = 4;
+    m3WorldDef def = m3DefaultWorldDef();
+    def.bodyCapacity = boxes + spheres + 4;
+    def.shapeCapacity = boxes + spheres + 4;
+    m3WorldId world = m3CreateWorld(&def);
+    SceneGround(world, 0.6f);
+    uint64_t rng = seed ^ 0x9A4Cull;
+    m3ShapeDef sd = m3DefaultShapeDef();
+    sd.friction = 0.6f;
+    m3BodyDef bd = m3DefaultBodyDef();
+    bd.type = m3_dynamicBody;
+    bd.position = (m3Pos3){0.0, 0.25, 0.0};
+    m3BodyId plank = m3CreateBody(world, &bd);
+    m3ShapeDef heavy = sd;
+    heavy.density = 4.0f;
+    m3CreateBoxShape(plank, &heavy, (m3Vec3){4.5f, 0.25f, 4.5f});
+    int32_t side = 1;
+    while (side * side < boxes)
+    {
+        side += 1;
+    }
+    const double pitch = 8.0 / (double)side;
+    for (int32_t b = 0; b < boxes; ++b)
+    {
+        double x = -4.0 + pitch * (0.5 + (double)(b % side)) + SceneRand(&rng, -0.05, 0.05);
+        double z = -4.0 + pitch * (0.5 + (double)(b / side)) + SceneRand(&rng, -0.05, 0.05);
+        bd.position = (m3Pos3){x, 0.5 + 0.35 + SceneRand(&rng, 0.0, 0.02), z};
+        m3BodyId body = m3CreateBody(world, &bd);
+        m3CreateBoxShape(body, &sd, (m3Vec3){0.35f, 0.35f, 0.35f});
+    }
+    for (int32_t k = 0; k < spheres; ++k)
+    {
+        double x = -4.0 + pitch * (0.5 + (double)(k % side));
+        double z = -4.0 + pitch * 0.5;
+        bd.position = (m3Pos3){x, 1.2 + 0.3 + SceneRand(&rng, 0.0, 0.5), z};
+        m3BodyId body = m3CreateBody(world, &bd);
+        m3Sphere ball = {{0.0f, 0.0f, 0.0f}, 0.3f};
+        m3CreateSphereShape(body, &sd, &ball);
+    }
+    return world;
+}
+
+// `count` spheres (radius U[0.3, 0.6]) and boxes (half extent U[0.3,
+// 0.5]) with restitution U[0.3, 0.8] on a 1.6 m grid, dropped from 2-8 m
+// onto a ground of restitution 0.5; every fourth body starts right above
+// its neighbour so the two bounce off each other.
+static m3WorldId Bounce(uint64_t seed, int32_t count)
+{
+    if (count < 2)
+    {
+        count = 2;
+    }
+    m3WorldDef def = m3DefaultWorldDef();
+    def.bodyCapacity = count + 4;
+    def.shapeCapacity = count + 4;
+    m3WorldId world = m3CreateWorld(&def);
+    m3BodyDef gd = m3DefaultBodyDef();
+    m3BodyId ground = m3CreateBody(world, &gd);
+    m3ShapeDef floorDef = m3DefaultShapeDef();
+    floorDef.friction = 0.5f;
+    floorDef.restitution = 0.5f;
+    m3Plane floor = {{0.0f, 1.0f, 0.0f}, 0.0f};
+    m3CreatePlaneShape(ground, &floorDef, &floor);
+    uint64_t rng = seed ^ 0xB0B0ull;
+    int32_t side = 1;
+    while (side * side < count)
+    {
+        side += 1;
+    }
+    m3BodyDef bd = m3DefaultBodyDef();
+    bd.type = m3_dynamicBody;
+    for (int32_t k = 0; k < count; ++k)
+    {
+        m3ShapeDef sd = m3DefaultShapeDef();
+        sd.friction = (float)SceneRand(&rng, 0.2, 0.8);
+        sd.restitution = (float)SceneRand(&rng, 0.3, 0.8);
+        double x = 1.6 * (double)(k % side);
+        double z = 1.6 * (double)(k / side);
+        double y = SceneRand(&rng, 2.0, 8.0);
+        if (k % 4 == 3)
+        {
+            // Above the previous body, a little off its axis.
+            x = 1.6 * (double)((k - 1) % side) + 0.15;
+            z = 1.6 * (double)((k - 1) / side) - 0.1;
+            y = 9.5 + SceneRand(&rng, 0.0, 1.5);
+        }
+        bd.position = (m3Pos3){x, y, z};
+        bd.angularVelocity = (m3Vec3){(float)SceneRand(&rng, -1.0, 1.0), 0.0f,
+                                      (float)SceneRand(&rng, -1.0, 1.0)};
+        m3BodyId body = m3CreateBody(world, &bd);
+        if (k % 2 == 0)
+        {
+            m3Sphere ball = {{0.0f, 0.0f, 0.0f}, (float)SceneRand(&rng, 0.3, 0.6)};
+            m3CreateSphereShape(body, &sd, &ball);
+        }
+        else
+        {
+            float h = (float)SceneRand(&rng, 0.3, 0.5);
+            m3CreateBoxShape(body, &sd, (m3Vec3){h, h, h});
+        }
+    }
+    return world;
+}
+
 // Build one seeded scene; returns the null world id for an unknown
 // scene number.
 M3S_API m3WorldId m3s_build(int32_t scene, uint64_t seed, int32_t param)
@@ -566,6 +689,10 @@ M3S_API m3WorldId m3s_build(int32_t scene, uint64_t seed, int32_t param)
         return Terrain(seed, param > 0 ? param : 60);
     case M3S_SHOTS:
         return Shots(seed, param > 0 ? param : 24);
+    case M3S_PLANK:
+        return Plank(seed, param > 0 ? param : 25);
+    case M3S_BOUNCE:
+        return Bounce(seed, param > 0 ? param : 40);
     default:
     {
         m3WorldId none = {0, 0};

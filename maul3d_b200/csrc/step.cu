@@ -432,7 +432,10 @@ __global__ void __launch_bounds__(32 * M3_TREE_WORLDS_PER_BLOCK)
     ScratchCarve(&s, w.scratch, sc->bodyCap, sc->shapeCap, sc->jointCap, sc->pairCap, treeLag);
     const m3TreeRef tree = m3WorldTree(w);
     const int32_t moves = s.treeMoveCount[slot];
-    if (moves == 0)
+    // A refused world's tree is not kept (its state is unspecified after
+    // a refusal), and a move count above the shape slots cannot come
+    // from this world's broadphase.
+    if (moves <= 0 || sc->status != 0 || moves > sc->shapeMax)
     {
         return;
     }
@@ -458,11 +461,21 @@ __global__ void __launch_bounds__(32 * M3_TREE_WORLDS_PER_BLOCK)
     const m3TreeArrayStore store{w.treeNodes};
     const int32_t* shapes = s.treeMoveShape + (int64_t)slot * sc->shapeCap;
     const m3Aabb* boxes = s.treeMoveBox + (int64_t)slot * sc->shapeCap;
+    const int32_t shapeMax = sc->shapeMax;
+    const int32_t nodeCap = 2 * sc->shapeCap;
     for (int32_t m = 0; m < moves; ++m)
     {
         const int32_t shape = shapes[m];
         const m3Aabb box = boxes[m];
-        m3TreeRemove(tree, store, w.proxyId[shape]);
+        const int32_t old = shape >= 0 && shape < shapeMax ? w.proxyId[shape] : M3_TREE_NULL;
+        if (old == M3_TREE_NULL || old < 0 || old >= nodeCap)
+        {
+            // Only shapes with a leaf are ever recorded as moves.
+            atomicExch(&sc->status, M3GPU_ERR_INVALID);
+            sc->statusDetail = 6001;
+            return;
+        }
+        m3TreeRemove(tree, store, old);
         const int32_t leaf = m3TreeInsert(tree, store, box.lo, box.hi, shape);
         w.proxyId[shape] = leaf;
         if (leaf == M3_TREE_NULL)
@@ -530,6 +543,10 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3BroadKernel(const m3WorldVie
         s_planeCount = 0;
         s_sweepCount = 0;
         s_sweepPairs = 0;
+        // No moves recorded unless this step reaches the containment
+        // tests below: the tree kernel must never replay a ring slot
+        // (or scratch shared with another world) left by an older step.
+        s.treeMoveCount[treeSlot] = 0;
     }
     __syncthreads();
     if (s_status != 0)
@@ -2612,6 +2629,11 @@ extern "C" float m3gpu_last_step_ms(void)
 
 extern "C" int32_t m3gpu_synchronize(void)
 {
+    M3_DEVICE_GUARD;
+    if (m3gpuEnsureDevice() != M3GPU_OK)
+    {
+        return m3gpu_last_error();
+    }
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess)
     {
@@ -3108,15 +3130,16 @@ static void LaunchSolve(const m3WorldView* views, const int32_t* order, int32_t 
     m3FinishKernel<<<count, M3_BLOCK>>>(views, order, count, dt, substeps);
 }
 
-// Device milliseconds of the last batched call per stage: collide
-// (bounds, pairs, narrowphase), prepare, substeps, finish.
-#define M3_STAGES 4
-static float s_kernelMs[M3_STAGES] = {0.0f, 0.0f, 0.0f, 0.0f};
+// Device milliseconds of the last batched call per stage: broadphase
+// (bounds, pairs), narrowphase, prepare, substeps, finish.
+#define M3_STAGES 5
+static float s_kernelMs[M3_STAGES] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
 static std::vector<cudaEvent_t> s_events;
 static int32_t* s_dstatus = nullptr;
 
 extern "C" int32_t m3gpu_kernel_ms(float* out)
 {
+    M3_DEVICE_GUARD;
     if (out == nullptr)
     {
         return m3gpuSetError(M3GPU_ERR_INVALID, "null output");
@@ -3130,6 +3153,7 @@ extern "C" int32_t m3gpu_kernel_ms(float* out)
 
 extern "C" int32_t m3gpu_world_stats(m3WorldId world, uint64_t* out)
 {
+    M3_DEVICE_GUARD;
     m3HostWorld* w = m3gpuWorldFromId(world);
     if (w == nullptr || out == nullptr)
     {
@@ -3149,6 +3173,7 @@ extern "C" int32_t m3gpu_world_stats(m3WorldId world, uint64_t* out)
 
 extern "C" int32_t m3gpu_world_phase_cycles(m3WorldId world, uint64_t* out)
 {
+    M3_DEVICE_GUARD;
     m3HostWorld* w = m3gpuWorldFromId(world);
     if (w == nullptr || out == nullptr)
     {
@@ -3262,6 +3287,7 @@ static int32_t LaunchBodyOps(int32_t count, const m3BodyOp* ops, int32_t opCount
 int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t substeps,
                        int32_t steps, const m3BodyOp* ops, int32_t opCount)
 {
+    M3_DEVICE_GUARD;
     int32_t rc = m3gpuEnsureDevice();
     if (rc != M3GPU_OK)
     {
@@ -3335,6 +3361,7 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
         }
         m3BroadKernel<M3_BLOCK, 2><<<count, M3_BLOCK>>>(s_batch.dviews, s_batch.dorder, count,
                                                         step % M3_TREE_LAG, M3_TREE_LAG);
+        cudaEventRecord(ev[1]);
         if (anyTracked)
         {
             cudaEventRecord(s_classStreams.broadDone[(size_t)step], 0);
@@ -3347,10 +3374,10 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
         }
         m3PairOffsetsKernel<<<1, M3_BLOCK>>>(s_batch.dviews, count, s_batch.doffsets);
         LaunchNarrow(s_batch.dviews, s_batch.doffsets, count, anyTerrain);
-        cudaEventRecord(ev[1]);
+        cudaEventRecord(ev[2]);
         LaunchSolve(s_batch.dviews, s_batch.dorder, count, dt, substeps, s_batch.cacheBytes,
-                    ev + 2, s_batch.classFirst, s_batch.classCache);
-        cudaEventRecord(ev[4]);
+                    ev + 3, s_batch.classFirst, s_batch.classCache);
+        cudaEventRecord(ev[5]);
         s_launches += 5 + (count <= M3_NARROW_SMALL_BATCH ? 1 : M3_NARROW_LAUNCHES + (anyTerrain ? M3_TERRAIN_LAUNCHES : 0));
     }
     if (anyTracked && steps > 0)
@@ -3385,6 +3412,7 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
     {
         s_kernelMs[k] = 0.0f;
     }
+    float last[M3_STAGES] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
     for (int32_t step = 0; step < steps; ++step)
     {
         const cudaEvent_t* ev = &s_events[(size_t)(M3_STAGES * step)];
@@ -3393,9 +3421,31 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
             float ms = 0.0f;
             cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
             s_kernelMs[k] += ms;
+            last[k] = ms;
         }
     }
     s_lastStepMs = total;
+    // Every world's profile (m3World_GetProfile) is its batch's last
+    // step: the device runs the batch's worlds together, stage by stage.
+    if (steps > 0)
+    {
+        float stepMs = 0.0f;
+        for (int32_t k = 0; k < M3_STAGES; ++k)
+        {
+            stepMs += last[k];
+        }
+        for (int32_t i = 0; i < count; ++i)
+        {
+            m3StepProfile& p = worlds[i]->profile;
+            p.step = stepMs;
+            p.broadphase = last[0];
+            p.narrowphase = last[1];
+            p.prepare = last[2];
+            p.solve = last[3];
+            p.finish = last[4];
+            p.valid = true;
+        }
+    }
     if (status != 0)
     {
         // Name the first refusing world and its detail code.
@@ -3419,6 +3469,7 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
 
 int32_t m3gpuHashBatch(m3HostWorld** worlds, int32_t count, uint64_t* out)
 {
+    M3_DEVICE_GUARD;
     int32_t rc = m3gpuEnsureDevice();
     if (rc != M3GPU_OK)
     {
@@ -3450,9 +3501,9 @@ int32_t m3gpuHashBatch(m3HostWorld** worlds, int32_t count, uint64_t* out)
 //
 // Some callers cannot allocate device memory at the moment they need a
 // step: a frame loop with a hard deadline (cudaMalloc and cudaFree can
-// synchronise the whole device), code running while a CUDA graph is
-// being captured, or a host whose device memory is owned entirely by a
-// pool allocator.  For them m3gpu_step_world_noalloc steps one world
+// synchronise the whole device), or a host whose device memory is owned
+// entirely by its own pool allocator.  For them m3gpu_step_world_noalloc
+// steps one world
 // that is already resident in HBM (reserved and uploaded earlier, when
 // allocating was allowed) without allocating anything: the step's
 // scratch, the one-world launch table and the status word live in
@@ -3468,10 +3519,15 @@ int32_t m3gpuHashBatch(m3HostWorld** worlds, int32_t count, uint64_t* out)
 //
 // The first call on a device looks up the arrays' device addresses
 // (cudaGetSymbolAddress) with that device current and caches them; make
-// that first call before any stream capture.  All calls share the
-// arrays and leave the last call's contents behind (every field the
-// step reads is rewritten first), so calls that overlap on the GPU,
-// from several host threads or streams, race: serialise them.
+// that first call before any stream capture.  The call itself copies the
+// launch table and reads the status with blocking copies on the legacy
+// default stream, so it must not run while any stream of the process is
+// being captured.  All calls share the arrays and leave the last call's
+// contents behind (every field the step reads is rewritten first, and
+// the tree's move count is zeroed before anything can return early), so
+// calls that overlap on the GPU race: the library's lock serialises the
+// calls of one process; callers in several processes sharing a GPU each
+// hold their own copy of the arrays.
 // ---------------------------------------------------------------------
 #define M3_NOALLOC_SCRATCH_BYTES (4 * 1024 * 1024)
 #define M3_NOALLOC_MAX_DEVICES 64
@@ -3521,6 +3577,7 @@ static int32_t NoallocSetup(int32_t device, m3NoallocSymbols* out)
 
 extern "C" int32_t m3gpu_step_world_noalloc(m3WorldId worldId, float dt, int32_t substeps)
 {
+    M3_DEVICE_GUARD;
     m3gpuClearError();
     m3HostWorld* w = m3gpuWorldFromId(worldId);
     if (w == nullptr || !(dt > 0.0f) || substeps < 1 || substeps > M3_MAX_SUBSTEPS)
@@ -3545,8 +3602,14 @@ extern "C" int32_t m3gpu_step_world_noalloc(m3WorldId worldId, float dt, int32_t
                              (long long)need, (long long)cache, M3_NOALLOC_SCRATCH_BYTES,
                              48 * 1024);
     }
+    // The library's device, made current for this thread (the world's
+    // slab lives there); the static arrays are looked up on it.
+    int32_t rc = m3gpuEnsureDevice();
     int device = 0;
-    int32_t rc = Check(cudaGetDevice(&device), "cudaGetDevice");
+    if (rc == M3GPU_OK)
+    {
+        rc = Check(cudaGetDevice(&device), "cudaGetDevice");
+    }
     m3NoallocSymbols sym;
     if (rc == M3GPU_OK)
     {

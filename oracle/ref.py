@@ -10,21 +10,48 @@ bench.py's CPU legs import this module; the product never does.
 from __future__ import annotations
 
 import ctypes as C
+import importlib.util
 import os
 import subprocess
+import sys
 from pathlib import Path
 
 import numpy as np
 
-from maul3d_b200 import abi
-from maul3d_b200.abi import MANIFOLD, MAT3, TRANSFORM, VEC3, WorldState, m3WorldId
-
 HERE = Path(__file__).resolve().parent
+REPO = HERE.parent
+
+
+def _records():
+    """The ctypes record types and value layouts (maul3d_b200/abi.py).
+
+    abi.py depends on ctypes and numpy only.  When the package is already
+    imported (the tests) its module is shared; otherwise the file is
+    loaded on its own, so that driving the oracle never runs the
+    package's __init__ and never maps this library's shared object (the
+    reference arm of the bench loads the reference engine alone)."""
+    mod = sys.modules.get("maul3d_b200.abi")
+    if mod is not None:
+        return mod
+    spec = importlib.util.spec_from_file_location("m3_oracle_records",
+                                                  REPO / "maul3d_b200" / "abi.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+abi = _records()
+MANIFOLD, MAT3, TRANSFORM, VEC3 = abi.MANIFOLD, abi.MAT3, abi.TRANSFORM, abi.VEC3
+WorldState, m3WorldId = abi.WorldState, abi.m3WorldId
+
 REF_DIR = HERE / "_ref"
 LIB_PATH = REF_DIR / "libmaul3d_ref.so"
 BENCH_PATH = REF_DIR / "maul3d_bench"
 DET_PATH = REF_DIR / "test_determinism"
-REFERENCE_SRC = Path(os.environ.get("M3_REFERENCE_SRC", "/root/reference"))
+# The reference's sources: M3_REFERENCE_SRC, else a checkout named
+# `reference` beside this repository.  Absent on hosts that only use the
+# prebuilt oracle/_ref.
+REFERENCE_SRC = Path(os.environ.get("M3_REFERENCE_SRC") or (REPO.parent / "reference"))
 
 
 def build(force: bool = False) -> bool:

@@ -71,3 +71,21 @@ def test_refusals_return_null_ids(m3):
 def test_unknown_scene_is_null(m3):
     with pytest.raises(m3.M3GpuError):
         m3.World.scene(99)
+
+
+@pytest.mark.parametrize("scene,seed,param", SCENES[:4])
+def test_counters_at_creation_match_reference(m3, oracle, scene, seed, param):
+    """m3World_GetCounters on a freshly built world: the live counts, the
+    tree height and the snapshot size equal the reference's (the scratch
+    and allocation figures are engine-specific)."""
+    g = m3.World.scene(scene, seed, param)
+    r = oracle.RefWorld.scene(scene, seed, param)
+    gc = m3.counters(g)
+    rc = oracle.lib().m3World_GetCounters(r.id)
+    for name in ("bodyCount", "shapeCount", "jointCount", "contactCount", "awakeCount",
+                 "islandCount", "colorCount", "hullCount", "meshCount", "treeHeight",
+                 "snapshotBytes"):
+        assert gc[name] == getattr(rc, name), name
+    assert m3.profile(g)["step"] == 0.0
+    g.destroy()
+    r.destroy()
