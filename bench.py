@@ -311,6 +311,7 @@ def terrain_run(m3, args, seed: int) -> dict:
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record()
     m3.step_worlds(batch, DT, args.substeps, steps)
+    m3.synchronize()
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
@@ -498,6 +499,9 @@ def main() -> None:
     launches0 = m3.launch_count()
     e0.record()
     m3.step_worlds(worlds, DT, args.substeps, args.steps)
+    # The trees finish on their own stream behind the call: the timed
+    # region ends when every stream of the device is idle.
+    m3.synchronize()
     e1.record()
     launches = m3.launch_count() - launches0
     torch.cuda.synchronize()
@@ -564,6 +568,7 @@ def main() -> None:
         for _ in range(args.steps):
             for w in pworlds:
                 m3.step_worlds([w], DT, args.substeps, 1)
+        m3.synchronize()
         p1.record()
         torch.cuda.synchronize()
         pms = p0.elapsed_time(p1)

@@ -314,6 +314,10 @@ static int32_t UploadPrepare(m3HostWorld* w)
     {
         return rc;
     }
+    // The upload overwrites the device tree: no replay of the old one may
+    // still be running.  The scratch's leaf bounds are then stale.
+    m3gpuWaitTree(w);
+    w->leafBoxValid = false;
     if (w->dslab == nullptr)
     {
         w->scratchBytes = m3gpuScratchBytes(w->bodyCap, w->shapeCap, w->jointCap, w->pairCap);
@@ -615,6 +619,9 @@ int32_t m3gpuDownload(m3HostWorld* w)
     {
         return rc0;
     }
+    // The tree nodes are in the joint section below: its pending
+    // replays first.
+    m3gpuWaitTree(w);
     // Scalars first: they say which pair buffer is current and how long.
     int32_t rc = CudaCheck(cudaMemcpy(w->hv.sc, w->dv.sc, sizeof(m3WorldScalars),
                                       cudaMemcpyDeviceToHost),
@@ -734,6 +741,8 @@ void m3gpuRelease(m3HostWorld* w)
         m3gpuEnsureDevice();
         cudaDeviceSynchronize();
     }
+    w->treePendingCount = 0;
+    w->leafBoxValid = false;
     if (w->dslab != nullptr)
     {
         DevFree(w->dslab, (size_t)w->dslabBytes);

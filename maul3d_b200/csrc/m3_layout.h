@@ -64,6 +64,12 @@ typedef struct m3WorldScalars
     // Whether the step keeps the broadphase tree (snapshot state).  Off
     // only for worlds nobody can snapshot (the serving path's own).
     int32_t treeTracked;
+    // Cursors of the ring of per-step tree move lists (device scratch):
+    // the broadphase writes slot treeHead % depth and advances treeHead,
+    // the tree kernel replays slot treeTail % depth and advances
+    // treeTail.  Equal whenever no tree work is pending.
+    int32_t treeHead;
+    int32_t treeTail;
     // Work counters accumulated over every device step (observer only,
     // never hashed): the algorithmic-byte model of the roofline reads
     // them.  [0] movers x substeps, [1] contact rows x substeps,

@@ -131,6 +131,10 @@ struct m3StepProfile
     bool valid = false;
 };
 
+// Steps the broadphase tree kernel may trail the step: the depth of the
+// ring of per-step move lists in each world's scratch.
+#define M3_TREE_LAG 8
+
 struct m3HostWorld
 {
     int32_t slot = -1;
@@ -207,6 +211,14 @@ struct m3HostWorld
     bool pairTailsToDevice = false;
     bool pairTailsOnDevice = false;
     m3StepProfile profile;
+    // Tree launches (their sequence numbers, oldest first) that have yet
+    // to replay this world's recorded moves, one per ring slot in use;
+    // and whether the scratch's copy of the tree leaves' bounds is
+    // current (it is kept by the broadphase once made).
+    uint64_t treePending[M3_TREE_LAG] = {};
+    int32_t treePendingFirst = 0;
+    int32_t treePendingCount = 0;
+    bool leafBoxValid = false;
 };
 
 // Points a device view at the world's pools outside the slab.
@@ -285,6 +297,10 @@ void m3DrainBrokenJoints(m3HostWorld* w);
 int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t substeps,
                        int32_t steps, const struct m3BodyOp* ops = nullptr, int32_t opCount = 0);
 int32_t m3gpuHashBatch(m3HostWorld** worlds, int32_t count, uint64_t* out);
+// Orders the default stream after every tree launch still pending for
+// the world (step.cu): anything that reads or overwrites its tree or its
+// scratch on the default stream calls this first.
+void m3gpuWaitTree(m3HostWorld* w);
 // The parallel world hash (hash.cu): one block per world, blocks in
 // `order`, out[world] = that world's m3WorldHashView.
 int32_t m3gpuLaunchHash(const m3WorldView* views, const int32_t* order, int32_t count,

@@ -51,9 +51,8 @@
 // parallel rounds before the serial finish.
 #define M3_COLOR_PENDING 0xFF
 #define M3_COLOR_ROUNDS 64
-// Steps the broadphase tree kernel may trail the step (the depth of the
-// ring of per-step move lists).
-#define M3_TREE_LAG 8
+// Threads (worlds) per block of the tree kernel, at most.
+#define M3_TREE_THREADS_MAX 512
 
 // Step phases timed with the SM clock by thread 0 of each world's block
 // right after the barrier that closes the phase.
@@ -409,28 +408,38 @@ __global__ void __launch_bounds__(M3_BLOCK) m3LeafBoxKernel(const m3WorldView* v
     }
 }
 
-// Broadphase tree refresh, second half (broad_phase.c:516-538): one warp
-// per world replays one step's moves in ascending shape order, each a
-// leaf removal and the insertion of its fat bounds.  The tree is state
-// only a snapshot reads, so this runs on its own stream beside the
-// following steps, up to M3_TREE_LAG steps behind (the move lists sit in
-// a ring of that depth).
-#define M3_TREE_WORLDS_PER_BLOCK 1
-__global__ void __launch_bounds__(32 * M3_TREE_WORLDS_PER_BLOCK)
-    m3TreeKernel(const m3WorldView* views, const int32_t* order, int32_t count, int32_t slot,
-                 int32_t treeLag)
+// Broadphase tree refresh, second half (broad_phase.c:516-538): one
+// thread per world replays one step's moves in ascending shape order,
+// each a leaf removal and the insertion of its fat bounds.  The walk is
+// a serial chain of dependent loads per world, so a world needs one
+// lane, not a warp: the worlds of a warp walk side by side (neighbours
+// in the largest-first order, so of similar size), and the whole batch's
+// walks fit on a few SMs instead of holding a warp's registers on every
+// SM the step's own blocks need.  The tree is state only a snapshot
+// reads, so this runs on its own stream beside the following steps, up
+// to M3_TREE_LAG steps behind (the move lists sit in a ring of that
+// depth).
+__global__ void __launch_bounds__(M3_TREE_THREADS_MAX)
+    m3TreeKernel(const m3WorldView* views, const int32_t* order, int32_t count, int32_t treeLag)
 {
-    const int32_t k = blockIdx.x * M3_TREE_WORLDS_PER_BLOCK + (int32_t)(threadIdx.x >> 5);
-    const int32_t lane = (int32_t)(threadIdx.x & 31);
+    const int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= count)
     {
         return;
     }
     const m3WorldView& w = views[order[k]];
     m3WorldScalars* sc = w.sc;
+    if (sc->treeTracked == 0)
+    {
+        return;
+    }
     m3Scratch s;
     ScratchCarve(&s, w.scratch, sc->bodyCap, sc->shapeCap, sc->jointCap, sc->pairCap, treeLag);
     const m3TreeRef tree = m3WorldTree(w);
+    // The oldest recorded step: one launch replays one step of each of
+    // its worlds, in the order the broadphase recorded them.
+    const int32_t slot = (int32_t)((uint32_t)sc->treeTail % (uint32_t)treeLag);
+    sc->treeTail += 1;
     const int32_t moves = s.treeMoveCount[slot];
     // A refused world's tree is not kept (its state is unspecified after
     // a refusal), and a move count above the shape slots cannot come
@@ -446,17 +455,13 @@ __global__ void __launch_bounds__(32 * M3_TREE_WORLDS_PER_BLOCK)
     {
         const int64_t bytes = (int64_t)sizeof(m3TreeNode) * 2 * sc->shapeCap;
         const uint8_t* base = (const uint8_t*)w.treeNodes;
-        for (int64_t off = (int64_t)lane << 16; off < bytes; off += (int64_t)32 << 16)
+        for (int64_t off = 0; off < bytes; off += (int64_t)1 << 16)
         {
             const int64_t left = bytes - off;
             const uint32_t piece = (uint32_t)(left < 65536 ? left : 65536);
             asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(base + off), "r"(piece)
                          : "memory");
         }
-    }
-    if (lane != 0)
-    {
-        return;
     }
     const m3TreeArrayStore store{w.treeNodes};
     const int32_t* shapes = s.treeMoveShape + (int64_t)slot * sc->shapeCap;
@@ -524,7 +529,7 @@ __device__ __forceinline__ void SweepFrom(const m3WorldView& w, const m3Scratch&
 template <int NT, int MIN_BLOCKS>
 __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3BroadKernel(const m3WorldView* views,
                                                           const int32_t* order, int32_t count,
-                                                          int32_t treeSlot, int32_t treeLag)
+                                                          int32_t treeLag)
 {
     const int32_t wi = order[blockIdx.x];
     const m3WorldView& w = views[wi];
@@ -537,18 +542,29 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3BroadKernel(const m3WorldVie
     __shared__ int32_t s_planeCount;
     __shared__ int32_t s_sweepCount;
     __shared__ int32_t s_sweepPairs;
+    __shared__ int32_t s_treeSlot;
     if (tid == 0)
     {
         s_status = sc->status;
         s_planeCount = 0;
         s_sweepCount = 0;
         s_sweepPairs = 0;
-        // No moves recorded unless this step reaches the containment
-        // tests below: the tree kernel must never replay a ring slot
-        // (or scratch shared with another world) left by an older step.
-        s.treeMoveCount[treeSlot] = 0;
+        // A world that keeps the tree records one ring slot per step, read
+        // back by exactly one tree launch.  No moves are recorded unless
+        // this step reaches the containment tests below: the tree kernel
+        // must never replay a slot (or scratch shared with another world)
+        // left by an older step.
+        int32_t slot = 0;
+        if (sc->treeTracked != 0)
+        {
+            slot = (int32_t)((uint32_t)sc->treeHead % (uint32_t)treeLag);
+            sc->treeHead += 1;
+            s.treeMoveCount[slot] = 0;
+        }
+        s_treeSlot = slot;
     }
     __syncthreads();
+    const int32_t treeSlot = s_treeSlot;
     if (s_status != 0)
     {
         return;
@@ -2768,10 +2784,10 @@ struct m3ClassStreams
     cudaEvent_t fork = nullptr;
     cudaEvent_t join[M3_CLASSES] = {};
     // The broadphase tree's stream and its per-step events: the
-    // broadphase of step k done, the tree kernel of step k done.
+    // broadphase of step k done (the tree launches' own events are a
+    // ring by launch, below).
     cudaStream_t tree = nullptr;
     std::vector<cudaEvent_t> broadDone;
-    std::vector<cudaEvent_t> treeDone;
 };
 static m3ClassStreams s_classStreams;
 
@@ -2794,9 +2810,9 @@ static int32_t EnsureClassStreams()
     }
     if (e == cudaSuccess)
     {
-        // Default priority: the tree's single-warp blocks then interleave
-        // with the step's kernels instead of waiting for idle SMs, which
-        // a busy batch never leaves.
+        // Default priority: the tree's blocks then take SMs as the step's
+        // kernels free them instead of waiting for idle SMs, which a busy
+        // batch never leaves.
         e = cudaStreamCreateWithFlags(&s_classStreams.tree, cudaStreamNonBlocking);
     }
     if (e != cudaSuccess)
@@ -2810,21 +2826,15 @@ static int32_t EnsureClassStreams()
 // Events for `steps` steps of the tree pipeline.
 static int32_t EnsureTreeEvents(int32_t steps)
 {
-    while ((int32_t)s_classStreams.treeDone.size() < steps)
+    while ((int32_t)s_classStreams.broadDone.size() < steps)
     {
         cudaEvent_t a = nullptr;
-        cudaEvent_t b = nullptr;
         cudaError_t e = cudaEventCreateWithFlags(&a, cudaEventDisableTiming);
-        if (e == cudaSuccess)
-        {
-            e = cudaEventCreateWithFlags(&b, cudaEventDisableTiming);
-        }
         if (e != cudaSuccess)
         {
             return m3gpuSetError(M3GPU_ERR_CUDA, "tree events: %s", cudaGetErrorString(e));
         }
         s_classStreams.broadDone.push_back(a);
-        s_classStreams.treeDone.push_back(b);
     }
     return M3GPU_OK;
 }
@@ -3284,6 +3294,72 @@ static int32_t LaunchBodyOps(int32_t count, const m3BodyOp* ops, int32_t opCount
     return Check(cudaGetLastError(), "body command kernel");
 }
 
+// Every tree launch gets a sequence number (from 1) and an event in a
+// ring; waiting for launch q waits on its event, or, once the ring has
+// moved past it, on the oldest event still in the ring (the tree stream
+// runs its launches in order, so a later launch done means q is done).
+#define M3_TREE_EVENTS 64
+static cudaEvent_t s_treeEvents[M3_TREE_EVENTS] = {};
+static uint64_t s_treeSeq = 0;
+
+static cudaEvent_t TreeEventFor(uint64_t q)
+{
+    if (s_treeSeq - q >= M3_TREE_EVENTS)
+    {
+        q = s_treeSeq - M3_TREE_EVENTS + 1;
+    }
+    return s_treeEvents[q % M3_TREE_EVENTS];
+}
+
+static uint64_t RecordTreeLaunch(cudaStream_t stream)
+{
+    const uint64_t q = s_treeSeq + 1;
+    cudaEvent_t& e = s_treeEvents[q % M3_TREE_EVENTS];
+    if (e == nullptr)
+    {
+        cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    }
+    cudaEventRecord(e, stream);
+    s_treeSeq = q;
+    return q;
+}
+
+void m3gpuWaitTree(m3HostWorld* w)
+{
+    M3_DEVICE_GUARD;
+    if (w->treePendingCount > 0)
+    {
+        const uint64_t last =
+            w->treePending[(w->treePendingFirst + w->treePendingCount - 1) % M3_TREE_LAG];
+        cudaStreamWaitEvent(0, TreeEventFor(last), 0);
+        w->treePendingCount = 0;
+        w->treePendingFirst = 0;
+    }
+}
+
+// Worlds per block of the tree kernel: each block's worlds walk on one
+// SM, so this sets how many SMs the batch's tree walks hold (4096
+// worlds at 128 a block: 32 blocks of four warps).  M3GPU_TREE_THREADS
+// (32 to M3_TREE_THREADS_MAX, a multiple of 32) overrides it.
+static int32_t TreeThreads()
+{
+    static int32_t threads = 0;
+    if (threads == 0)
+    {
+        threads = 128;
+        const char* env = getenv("M3GPU_TREE_THREADS");
+        if (env != nullptr)
+        {
+            const int32_t v = atoi(env);
+            if (v >= 32 && v <= M3_TREE_THREADS_MAX && v % 32 == 0)
+            {
+                threads = v;
+            }
+        }
+    }
+    return threads;
+}
+
 int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t substeps,
                        int32_t steps, const m3BodyOp* ops, int32_t opCount)
 {
@@ -3336,40 +3412,83 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
         return rc;
     }
     cudaEventRecord(s_events[0]);
-    // The broadphase tree: the leaves' bounds once per batch, then per
-    // step the tree kernel on its own stream, at most M3_TREE_LAG steps
-    // behind (the move lists sit in a ring of that depth).  Batches of
-    // worlds that keep no tree skip both.
+    // The broadphase tree: the leaves' bounds once per fresh slab, then
+    // per step the tree kernel on its own stream, each world at most
+    // M3_TREE_LAG steps behind its own step (the move lists sit in a ring
+    // of that depth in its scratch), across calls.  Batches of worlds
+    // that keep no tree skip both.
     bool anyTracked = false;
     bool anyTerrain = false;
+    bool leafBoxes = false;
+    std::vector<m3HostWorld*> tracked;
     for (int32_t i = 0; i < count; ++i)
     {
-        anyTracked = anyTracked || worlds[i]->hv.sc->treeTracked != 0;
+        if (worlds[i]->hv.sc->treeTracked != 0)
+        {
+            anyTracked = true;
+            tracked.push_back(worlds[i]);
+            leafBoxes = leafBoxes || !worlds[i]->leafBoxValid;
+        }
         anyTerrain = anyTerrain || !worlds[i]->hfHeaders.empty();
     }
-    if (anyTracked)
+    if (leafBoxes)
     {
+        // Fresh slabs: copy every leaf's bounds out of the (finished)
+        // trees once; the broadphase keeps the copy current afterwards.
+        for (m3HostWorld* w : tracked)
+        {
+            m3gpuWaitTree(w);
+        }
         m3LeafBoxKernel<<<count, M3_BLOCK>>>(s_batch.dviews, count);
+        s_launches += 1;
+        for (m3HostWorld* w : tracked)
+        {
+            w->leafBoxValid = true;
+        }
     }
     const cudaStream_t treeStream = s_classStreams.tree;
     for (int32_t step = 0; step < steps; ++step)
     {
         const cudaEvent_t* ev = &s_events[(size_t)(M3_STAGES * step)];
-        if (anyTracked && step >= M3_TREE_LAG)
+        if (anyTracked)
         {
-            cudaStreamWaitEvent(0, s_classStreams.treeDone[(size_t)(step - M3_TREE_LAG)], 0);
+            // The step reuses each world's oldest ring slot once the ring
+            // is full: the launch replaying that slot must be done.
+            uint64_t need = 0;
+            for (m3HostWorld* w : tracked)
+            {
+                if (w->treePendingCount == M3_TREE_LAG)
+                {
+                    const uint64_t q = w->treePending[w->treePendingFirst];
+                    need = q > need ? q : need;
+                }
+            }
+            if (need != 0)
+            {
+                cudaStreamWaitEvent(0, TreeEventFor(need), 0);
+            }
         }
         m3BroadKernel<M3_BLOCK, 2><<<count, M3_BLOCK>>>(s_batch.dviews, s_batch.dorder, count,
-                                                        step % M3_TREE_LAG, M3_TREE_LAG);
+                                                        M3_TREE_LAG);
         cudaEventRecord(ev[1]);
         if (anyTracked)
         {
             cudaEventRecord(s_classStreams.broadDone[(size_t)step], 0);
             cudaStreamWaitEvent(treeStream, s_classStreams.broadDone[(size_t)step], 0);
-            m3TreeKernel<<<(count + M3_TREE_WORLDS_PER_BLOCK - 1) / M3_TREE_WORLDS_PER_BLOCK,
-                           32 * M3_TREE_WORLDS_PER_BLOCK, 0, treeStream>>>(
-                s_batch.dviews, s_batch.dorder, count, step % M3_TREE_LAG, M3_TREE_LAG);
-            cudaEventRecord(s_classStreams.treeDone[(size_t)step], treeStream);
+            const int32_t tt = TreeThreads();
+            m3TreeKernel<<<(count + tt - 1) / tt, tt, 0, treeStream>>>(
+                s_batch.dviews, s_batch.dorder, count, M3_TREE_LAG);
+            const uint64_t q = RecordTreeLaunch(treeStream);
+            for (m3HostWorld* w : tracked)
+            {
+                if (w->treePendingCount == M3_TREE_LAG)
+                {
+                    w->treePendingFirst = (w->treePendingFirst + 1) % M3_TREE_LAG;
+                    w->treePendingCount -= 1;
+                }
+                w->treePending[(w->treePendingFirst + w->treePendingCount) % M3_TREE_LAG] = q;
+                w->treePendingCount += 1;
+            }
             s_launches += 1;
         }
         m3PairOffsetsKernel<<<1, M3_BLOCK>>>(s_batch.dviews, count, s_batch.doffsets);
@@ -3380,13 +3499,10 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
         cudaEventRecord(ev[5]);
         s_launches += 5 + (count <= M3_NARROW_SMALL_BATCH ? 1 : M3_NARROW_LAUNCHES + (anyTerrain ? M3_TERRAIN_LAUNCHES : 0));
     }
-    if (anyTracked && steps > 0)
-    {
-        // Everything after the batch (status, readbacks, snapshots) sees
-        // the finished tree.
-        cudaStreamWaitEvent(0, s_classStreams.treeDone[(size_t)(steps - 1)], 0);
-    }
-    s_launches += anyTracked ? 1 : 0;
+    // The trees finish behind this call, on their own stream: a later
+    // step waits only for a ring slot it reuses, and anything reading or
+    // overwriting a world's tree waits for that world's launches
+    // (m3gpuWaitTree); m3gpu_synchronize waits for everything.
     cudaMemsetAsync(s_dstatus, 0, sizeof(int32_t));
     m3StatusKernel<<<(count + 255) / 256, 256>>>(s_batch.dviews, count, s_dstatus);
     s_launches += 1;
@@ -3639,9 +3755,14 @@ extern "C" int32_t m3gpu_step_world_noalloc(m3WorldId worldId, float dt, int32_t
     int32_t* order = sym.table;
     int32_t* offsets = sym.table + 1;
     const int32_t cacheBytes = (int32_t)cache;
+    // Tree replays of earlier regular steps first; this call replays its
+    // own moves in order on the default stream, and moves leaves the
+    // slab scratch's copy of their bounds does not see.
+    m3gpuWaitTree(w);
+    w->leafBoxValid = false;
     m3LeafBoxKernel<<<1, M3_BLOCK>>>(sym.view, 1);
-    m3BroadKernel<M3_BLOCK, 1><<<1, M3_BLOCK>>>(sym.view, order, 1, 0, 1);
-    m3TreeKernel<<<1, 32 * M3_TREE_WORLDS_PER_BLOCK>>>(sym.view, order, 1, 0, 1);
+    m3BroadKernel<M3_BLOCK, 1><<<1, M3_BLOCK>>>(sym.view, order, 1, 1);
+    m3TreeKernel<<<1, 32>>>(sym.view, order, 1, 1);
     m3PairOffsetsKernel<<<1, M3_BLOCK>>>(sym.view, 1, offsets);
     m3NarrowKernel<<<148, 128>>>(sym.view, offsets, 1);
     LaunchSolve(sym.view, order, 1, dt, substeps, cacheBytes, nullptr);
