@@ -3324,6 +3324,69 @@ static uint64_t RecordTreeLaunch(cudaStream_t stream)
     return q;
 }
 
+// The tree launches of a call read their own copy of the call's world
+// table: they finish behind the call, after the next call may have
+// rebuilt the batch table.  A copy is reused (oldest first) once the
+// last launch reading it is done.
+#define M3_TREE_TABLES 8
+struct m3TreeTable
+{
+    m3WorldView* views = nullptr;
+    int32_t* order = nullptr;
+    int32_t cap = 0;
+    uint64_t lastSeq = 0;
+};
+static m3TreeTable s_treeTables[M3_TREE_TABLES];
+static int32_t s_treeTableNext = 0;
+
+static int32_t TakeTreeTable(int32_t count, m3TreeTable** out)
+{
+    m3TreeTable& t = s_treeTables[s_treeTableNext];
+    s_treeTableNext = (s_treeTableNext + 1) % M3_TREE_TABLES;
+    if (t.lastSeq != 0)
+    {
+        const cudaError_t e = cudaEventSynchronize(TreeEventFor(t.lastSeq));
+        if (e != cudaSuccess)
+        {
+            return m3gpuSetError(M3GPU_ERR_CUDA, "tree table: %s", cudaGetErrorString(e));
+        }
+        t.lastSeq = 0;
+    }
+    if (count > t.cap)
+    {
+        cudaFree(t.views);
+        cudaFree(t.order);
+        t.views = nullptr;
+        t.order = nullptr;
+        t.cap = 0;
+        cudaError_t e = cudaMalloc((void**)&t.views, sizeof(m3WorldView) * (size_t)count);
+        if (e == cudaSuccess)
+        {
+            e = cudaMalloc((void**)&t.order, sizeof(int32_t) * (size_t)count);
+        }
+        if (e != cudaSuccess)
+        {
+            return m3gpuSetError(M3GPU_ERR_CUDA, "tree table: %s", cudaGetErrorString(e));
+        }
+        t.cap = count;
+    }
+    // Ordered on the default stream after the batch table's upload and
+    // before the broadphase the tree launches wait for.
+    cudaError_t e = cudaMemcpyAsync(t.views, s_batch.dviews, sizeof(m3WorldView) * (size_t)count,
+                                    cudaMemcpyDeviceToDevice, 0);
+    if (e == cudaSuccess)
+    {
+        e = cudaMemcpyAsync(t.order, s_batch.dorder, sizeof(int32_t) * (size_t)count,
+                            cudaMemcpyDeviceToDevice, 0);
+    }
+    if (e != cudaSuccess)
+    {
+        return m3gpuSetError(M3GPU_ERR_CUDA, "tree table: %s", cudaGetErrorString(e));
+    }
+    *out = &t;
+    return M3GPU_OK;
+}
+
 void m3gpuWaitTree(m3HostWorld* w)
 {
     M3_DEVICE_GUARD;
@@ -3447,6 +3510,15 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
         }
     }
     const cudaStream_t treeStream = s_classStreams.tree;
+    m3TreeTable* treeTable = nullptr;
+    if (anyTracked && steps > 0)
+    {
+        rc = TakeTreeTable(count, &treeTable);
+        if (rc != M3GPU_OK)
+        {
+            return rc;
+        }
+    }
     for (int32_t step = 0; step < steps; ++step)
     {
         const cudaEvent_t* ev = &s_events[(size_t)(M3_STAGES * step)];
@@ -3477,8 +3549,9 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
             cudaStreamWaitEvent(treeStream, s_classStreams.broadDone[(size_t)step], 0);
             const int32_t tt = TreeThreads();
             m3TreeKernel<<<(count + tt - 1) / tt, tt, 0, treeStream>>>(
-                s_batch.dviews, s_batch.dorder, count, M3_TREE_LAG);
+                treeTable->views, treeTable->order, count, M3_TREE_LAG);
             const uint64_t q = RecordTreeLaunch(treeStream);
+            treeTable->lastSeq = q;
             for (m3HostWorld* w : tracked)
             {
                 if (w->treePendingCount == M3_TREE_LAG)
