@@ -51,8 +51,6 @@
 // parallel rounds before the serial finish.
 #define M3_COLOR_PENDING 0xFF
 #define M3_COLOR_ROUNDS 64
-// Threads (worlds) per block of the tree kernel, at most.
-#define M3_TREE_THREADS_MAX 512
 
 // Step phases timed with the SM clock by thread 0 of each world's block
 // right after the barrier that closes the phase.
@@ -408,21 +406,20 @@ __global__ void __launch_bounds__(M3_BLOCK) m3LeafBoxKernel(const m3WorldView* v
     }
 }
 
-// Broadphase tree refresh, second half (broad_phase.c:516-538): one
-// thread per world replays one step's moves in ascending shape order,
-// each a leaf removal and the insertion of its fat bounds.  The walk is
-// a serial chain of dependent loads per world, so a world needs one
-// lane, not a warp: the worlds of a warp walk side by side (neighbours
-// in the largest-first order, so of similar size), and the whole batch's
-// walks fit on a few SMs instead of holding a warp's registers on every
-// SM the step's own blocks need.  The tree is state only a snapshot
-// reads, so this runs on its own stream beside the following steps, up
-// to M3_TREE_LAG steps behind (the move lists sit in a ring of that
-// depth).
-__global__ void __launch_bounds__(M3_TREE_THREADS_MAX)
+// Broadphase tree refresh, second half (broad_phase.c:516-538): one warp
+// per world replays one step's moves in ascending shape order, each a
+// leaf removal and the insertion of its fat bounds; the warp's lanes
+// prefetch the world's nodes into L2, lane 0 walks.  (One lane per world,
+// 32 worlds to a warp, measured several times slower: the worlds' walks
+// diverge and their dependent loads serialise.)  The tree is state only a
+// snapshot reads, so this runs on its own stream beside the following
+// steps, each world up to M3_TREE_LAG steps behind (the move lists sit in
+// a ring of that depth).
+__global__ void __launch_bounds__(32)
     m3TreeKernel(const m3WorldView* views, const int32_t* order, int32_t count, int32_t treeLag)
 {
-    const int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int32_t k = blockIdx.x;
+    const int32_t lane = (int32_t)threadIdx.x;
     if (k >= count)
     {
         return;
@@ -439,8 +436,12 @@ __global__ void __launch_bounds__(M3_TREE_THREADS_MAX)
     // The oldest recorded step: one launch replays one step of each of
     // its worlds, in the order the broadphase recorded them.
     const int32_t slot = (int32_t)((uint32_t)sc->treeTail % (uint32_t)treeLag);
-    sc->treeTail += 1;
     const int32_t moves = s.treeMoveCount[slot];
+    __syncwarp();
+    if (lane == 0)
+    {
+        sc->treeTail += 1;
+    }
     // A refused world's tree is not kept (its state is unspecified after
     // a refusal), and a move count above the shape slots cannot come
     // from this world's broadphase.
@@ -455,13 +456,17 @@ __global__ void __launch_bounds__(M3_TREE_THREADS_MAX)
     {
         const int64_t bytes = (int64_t)sizeof(m3TreeNode) * 2 * sc->shapeCap;
         const uint8_t* base = (const uint8_t*)w.treeNodes;
-        for (int64_t off = 0; off < bytes; off += (int64_t)1 << 16)
+        for (int64_t off = (int64_t)lane << 16; off < bytes; off += (int64_t)32 << 16)
         {
             const int64_t left = bytes - off;
             const uint32_t piece = (uint32_t)(left < 65536 ? left : 65536);
             asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(base + off), "r"(piece)
                          : "memory");
         }
+    }
+    if (lane != 0)
+    {
+        return;
     }
     const m3TreeArrayStore store{w.treeNodes};
     const int32_t* shapes = s.treeMoveShape + (int64_t)slot * sc->shapeCap;
@@ -3400,29 +3405,6 @@ void m3gpuWaitTree(m3HostWorld* w)
     }
 }
 
-// Worlds per block of the tree kernel: each block's worlds walk on one
-// SM, so this sets how many SMs the batch's tree walks hold (4096
-// worlds at 128 a block: 32 blocks of four warps).  M3GPU_TREE_THREADS
-// (32 to M3_TREE_THREADS_MAX, a multiple of 32) overrides it.
-static int32_t TreeThreads()
-{
-    static int32_t threads = 0;
-    if (threads == 0)
-    {
-        threads = 128;
-        const char* env = getenv("M3GPU_TREE_THREADS");
-        if (env != nullptr)
-        {
-            const int32_t v = atoi(env);
-            if (v >= 32 && v <= M3_TREE_THREADS_MAX && v % 32 == 0)
-            {
-                threads = v;
-            }
-        }
-    }
-    return threads;
-}
-
 int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t substeps,
                        int32_t steps, const m3BodyOp* ops, int32_t opCount)
 {
@@ -3547,8 +3529,7 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
         {
             cudaEventRecord(s_classStreams.broadDone[(size_t)step], 0);
             cudaStreamWaitEvent(treeStream, s_classStreams.broadDone[(size_t)step], 0);
-            const int32_t tt = TreeThreads();
-            m3TreeKernel<<<(count + tt - 1) / tt, tt, 0, treeStream>>>(
+            m3TreeKernel<<<count, 32, 0, treeStream>>>(
                 treeTable->views, treeTable->order, count, M3_TREE_LAG);
             const uint64_t q = RecordTreeLaunch(treeStream);
             treeTable->lastSeq = q;
