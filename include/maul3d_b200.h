@@ -459,6 +459,15 @@ M3GPU_API float m3gpu_last_step_ms(void);
  * sleep.  `out` holds 5 floats. */
 M3GPU_API int32_t m3gpu_kernel_ms(float* out);
 
+/* Wide worlds (no reference counterpart; the reference spreads one
+ * world's same-colour constraint batches over host threads, solver.c:
+ * 2845-2877).  A step of a single world with at least `shapes` shape
+ * slots runs its substep loop over a cooperative grid of many blocks
+ * instead of one block, the schedule's levels separated by grid
+ * barriers; results are bit-identical either way.  Default 4096; returns
+ * the previous value (a value <= 0 only queries). */
+M3GPU_API int32_t m3gpu_set_wide_min_shapes(int32_t shapes);
+
 /* Work counters of one world accumulated over its device steps:
  * out[0] mover-substeps, out[1] contact-row-substeps, out[2]
  * joint-row-substeps, out[3] candidate pairs, out[4] steps, out[5] the

@@ -87,6 +87,8 @@ def _load() -> C.CDLL:
     lib.m3gpu_world_stats.restype = C.c_int32
     lib.m3gpu_world_phase_cycles.argtypes = [m3WorldId, C.POINTER(C.c_uint64)]
     lib.m3gpu_world_phase_cycles.restype = C.c_int32
+    lib.m3gpu_set_wide_min_shapes.argtypes = [C.c_int32]
+    lib.m3gpu_set_wide_min_shapes.restype = C.c_int32
     return lib
 
 
@@ -253,6 +255,12 @@ def kernel_ms() -> dict[str, float]:
     ms = {name: float(out[k]) for k, name in enumerate(STAGES)}
     ms["collide"] = ms["broad"] + ms["narrow"]
     return ms
+
+
+def set_wide_min_shapes(shapes: int) -> int:
+    """A single world with at least `shapes` shape slots steps its
+    substep loop over the whole grid; returns the previous threshold."""
+    return int(lib.m3gpu_set_wide_min_shapes(shapes))
 
 
 def counters(world) -> dict[str, int]:

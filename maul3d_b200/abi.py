@@ -52,6 +52,7 @@ SCENE_TERRAIN = 5
 SCENE_SHOTS = 6
 SCENE_PLANK = 7
 SCENE_BOUNCE = 8
+SCENE_CITY = 9
 
 
 def _ptr(a: np.ndarray) -> C.c_void_p:

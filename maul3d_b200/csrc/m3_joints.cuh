@@ -465,77 +465,95 @@ __device__ __forceinline__ void m3UnlinkJointDev(const m3WorldView& w, int32_t b
 // threshold is destroyed (joint.c:339-385): unlinked from both bodies,
 // which wake, its record reset, its slot freed (generation bumped unless
 // retired at 0xFFFF) and queued for the host's free list.
-__device__ void m3BreakJointsDev(const m3WorldView& w, m3real invH)
+// Whether joint j breaks at the end of this step: alive, breakable and
+// its reaction above a threshold (solver.c:4233-4245).  Independent of
+// every other joint's fate: the reaction reads only j's own impulses.
+__device__ bool m3JointBreaksDev(const m3WorldView& w, int32_t j, m3real invH)
+{
+    if (w.jointAlive[j] == 0)
+    {
+        return false;
+    }
+    const m3real maxForce = w.jbreak[j].x;
+    const m3real maxTorque = w.jbreak[j].y;
+    if (maxForce == 0.0f && maxTorque == 0.0f)
+    {
+        return false;
+    }
+    m3real force;
+    m3real torque;
+    m3JointReactionDev(w, j, invH, &force, &torque);
+    return (maxForce > 0.0f && force > maxForce) || (maxTorque > 0.0f && torque > maxTorque);
+}
+
+// Destroys broken joint j (m3DestroyJointInternal, joint.c:339-385):
+// unlinks it, wakes its bodies, clears its record and queues the slot.
+// Order dependent (the body joint lists, the slot queue): ascending j.
+__device__ void m3DestroyBrokenJointDev(const m3WorldView& w, int32_t j)
 {
     m3WorldScalars* sc = w.sc;
-    const int32_t jointMax = sc->jointMax;
+    const int32_t bodyA = w.jbodyA[j];
+    const int32_t bodyB = w.jbodyB[j];
+    m3UnlinkJointDev(w, bodyA, j);
+    m3UnlinkJointDev(w, bodyB, j);
+    if (w.btype[bodyA] == M3_BODY_DYNAMIC && w.bodyAlive[bodyA] != 0)
+    {
+        w.awake[bodyA] = 1;
+        w.sleepTime[bodyA] = 0.0f;
+    }
+    if (w.btype[bodyB] == M3_BODY_DYNAMIC && w.bodyAlive[bodyB] != 0)
+    {
+        w.awake[bodyB] = 1;
+        w.sleepTime[bodyB] = 0.0f;
+    }
+    const m3Vec3 zero = v3(0.0f, 0.0f, 0.0f);
+    w.jtype[j] = 0;
+    w.jbodyA[j] = -1;
+    w.jbodyB[j] = -1;
+    w.jlocalA[j] = zero;
+    w.jlocalB[j] = zero;
+    w.jcollide[j] = 0;
+    w.jimpulse[j] = zero;
+    w.jperp[j] = zero;
+    w.jlimitImp[j] = zero;
+    w.jangular[j] = zero;
+    w.jframeA[j] = m3IdentityQuat();
+    w.jframeB[j] = m3IdentityQuat();
+    w.jflags[j] = 0;
+    w.jmotor[j] = zero;
+    w.jbreak[j] = zero;
+    w.jspring[j] = zero;
+    w.jtargetScalar[j] = 0.0f;
+    w.jtargetQ[j] = m3IdentityQuat();
+    w.jspringImp[j] = zero;
+    w.jlimits[j] = zero;
+    w.jnextA[j] = -1;
+    w.jnextB[j] = -1;
+    w.jointAlive[j] = 0;
+    // The host's free queue learns of the slot through the ring:
+    // j when freed, -1 - j when retired at generation 0xFFFF.
+    int32_t entry = -1 - j;
+    if (w.jointGen[j] != 0xFFFF)
+    {
+        w.jointGen[j] = (uint16_t)(w.jointGen[j] + 1);
+        entry = j;
+    }
+    w.jbroken[sc->brokenCount % sc->jointCap] = entry;
+    sc->brokenCount += 1;
+}
+
+// Joint breakage of one world on one thread (solver.c:4233-4257):
+// reactions against thresholds, broken joints destroyed in ascending
+// order.
+__device__ void m3BreakJointsDev(const m3WorldView& w, m3real invH)
+{
+    const int32_t jointMax = w.sc->jointMax;
     for (int32_t j = 0; j < jointMax; ++j)
     {
-        if (w.jointAlive[j] == 0)
+        if (m3JointBreaksDev(w, j, invH))
         {
-            continue;
+            m3DestroyBrokenJointDev(w, j);
         }
-        const m3real maxForce = w.jbreak[j].x;
-        const m3real maxTorque = w.jbreak[j].y;
-        if (maxForce == 0.0f && maxTorque == 0.0f)
-        {
-            continue;
-        }
-        m3real force;
-        m3real torque;
-        m3JointReactionDev(w, j, invH, &force, &torque);
-        if (!((maxForce > 0.0f && force > maxForce) || (maxTorque > 0.0f && torque > maxTorque)))
-        {
-            continue;
-        }
-        const int32_t bodyA = w.jbodyA[j];
-        const int32_t bodyB = w.jbodyB[j];
-        m3UnlinkJointDev(w, bodyA, j);
-        m3UnlinkJointDev(w, bodyB, j);
-        if (w.btype[bodyA] == M3_BODY_DYNAMIC && w.bodyAlive[bodyA] != 0)
-        {
-            w.awake[bodyA] = 1;
-            w.sleepTime[bodyA] = 0.0f;
-        }
-        if (w.btype[bodyB] == M3_BODY_DYNAMIC && w.bodyAlive[bodyB] != 0)
-        {
-            w.awake[bodyB] = 1;
-            w.sleepTime[bodyB] = 0.0f;
-        }
-        const m3Vec3 zero = v3(0.0f, 0.0f, 0.0f);
-        w.jtype[j] = 0;
-        w.jbodyA[j] = -1;
-        w.jbodyB[j] = -1;
-        w.jlocalA[j] = zero;
-        w.jlocalB[j] = zero;
-        w.jcollide[j] = 0;
-        w.jimpulse[j] = zero;
-        w.jperp[j] = zero;
-        w.jlimitImp[j] = zero;
-        w.jangular[j] = zero;
-        w.jframeA[j] = m3IdentityQuat();
-        w.jframeB[j] = m3IdentityQuat();
-        w.jflags[j] = 0;
-        w.jmotor[j] = zero;
-        w.jbreak[j] = zero;
-        w.jspring[j] = zero;
-        w.jtargetScalar[j] = 0.0f;
-        w.jtargetQ[j] = m3IdentityQuat();
-        w.jspringImp[j] = zero;
-        w.jlimits[j] = zero;
-        w.jnextA[j] = -1;
-        w.jnextB[j] = -1;
-        w.jointAlive[j] = 0;
-        // The host's free queue learns of the slot through the ring:
-        // j when freed, -1 - j when retired at generation 0xFFFF.
-        int32_t entry = -1 - j;
-        if (w.jointGen[j] != 0xFFFF)
-        {
-            w.jointGen[j] = (uint16_t)(w.jointGen[j] + 1);
-            entry = j;
-        }
-        w.jbroken[sc->brokenCount % sc->jointCap] = entry;
-        sc->brokenCount += 1;
     }
 }
 

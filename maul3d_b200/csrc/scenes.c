@@ -42,6 +42,14 @@
 //   M3S_BOUNCE          `param` spheres and boxes with restitution 0.3-0.8
 //                       dropped from 2-8 m onto a bouncy ground and onto
 //                       each other: the restitution pass.
+//   M3S_CITY            the large single world: `param` towers of
+//                       10 x 10 x 2 unit boxes (10 wide, 10 high, 2 deep)
+//                       welded to their six neighbours by fixed joints
+//                       that break at 500 N (460 joints a tower), on a
+//                       grid 16 m apart, and four spheres (radius 0.5)
+//                       per tower launched at 20-40 m/s toward seeded
+//                       towers: 1000 towers are 204,000 bodies and
+//                       460,000 joints.
 
 #include <m3_scene_api.h> // resolved by -I: product or oracle shim
 
@@ -59,6 +67,7 @@ enum
     M3S_SHOTS = 6,
     M3S_PLANK = 7,
     M3S_BOUNCE = 8,
+    M3S_CITY = 9,
 };
 
 static uint64_t SceneSplitMix(uint64_t* state)
@@ -669,6 +678,109 @@ static m3WorldId Bounce(uint64_t seed, int32_t count)
     return world;
 }
 
+// Towers of 10 x 10 x 2 welded unit boxes on a grid of 16 m cells (the
+// grid as square as the count allows), each box joined to its +x, +y
+// and +z neighbours by a fixed joint with a 500 N force threshold, and
+// four dense spheres per tower, each starting 12 m in front of a seeded
+// target tower (+z side), 1-9 m up, flying at it at 20-40 m/s.
+static m3WorldId City(uint64_t seed, int32_t towers)
+{
+    if (towers < 1)
+    {
+        towers = 1;
+    }
+    const int32_t nx = 10;
+    const int32_t ny = 10;
+    const int32_t nz = 2;
+    const int32_t boxes = nx * ny * nz;
+    const int32_t joints = (nx - 1) * ny * nz + nx * (ny - 1) * nz + nx * ny * (nz - 1);
+    const int32_t shots = 4 * towers;
+    m3WorldDef def = m3DefaultWorldDef();
+    def.bodyCapacity = boxes * towers + shots + 4;
+    def.shapeCapacity = boxes * towers + shots + 4;
+    def.jointCapacity = joints * towers + 4;
+    m3WorldId world = m3CreateWorld(&def);
+    SceneGround(world, 0.6f);
+    uint64_t rng = seed ^ 0xC17Cull;
+    int32_t side = 1;
+    while (side * side < towers)
+    {
+        side += 1;
+    }
+    m3BodyDef bd = m3DefaultBodyDef();
+    bd.type = m3_dynamicBody;
+    m3ShapeDef sd = m3DefaultShapeDef();
+    sd.friction = 0.6f;
+    // One tower's bodies, indexed [y][z][x], reused per tower.
+    static m3BodyId box[10][2][10];
+    for (int32_t t = 0; t < towers; ++t)
+    {
+        const double cx = 16.0 * (double)(t % side);
+        const double cz = 16.0 * (double)(t / side);
+        for (int32_t y = 0; y < ny; ++y)
+        {
+            for (int32_t z = 0; z < nz; ++z)
+            {
+                for (int32_t x = 0; x < nx; ++x)
+                {
+                    bd.position = (m3Pos3){cx + (double)x - 4.5, 0.5 + (double)y,
+                                           cz + (double)z - 0.5};
+                    box[y][z][x] = m3CreateBody(world, &bd);
+                    m3CreateBoxShape(box[y][z][x], &sd, (m3Vec3){0.5f, 0.5f, 0.5f});
+                }
+            }
+        }
+        for (int32_t y = 0; y < ny; ++y)
+        {
+            for (int32_t z = 0; z < nz; ++z)
+            {
+                for (int32_t x = 0; x < nx; ++x)
+                {
+                    for (int32_t axis = 0; axis < 3; ++axis)
+                    {
+                        const int32_t x2 = x + (axis == 0 ? 1 : 0);
+                        const int32_t y2 = y + (axis == 1 ? 1 : 0);
+                        const int32_t z2 = z + (axis == 2 ? 1 : 0);
+                        if (x2 >= nx || y2 >= ny || z2 >= nz)
+                        {
+                            continue;
+                        }
+                        const m3Vec3 half = {axis == 0 ? 0.5f : 0.0f, axis == 1 ? 0.5f : 0.0f,
+                                             axis == 2 ? 0.5f : 0.0f};
+                        m3JointDef jd = m3DefaultJointDef();
+                        jd.type = m3_fixedJoint;
+                        jd.bodyA = box[y][z][x];
+                        jd.bodyB = box[y2][z2][x2];
+                        jd.localAnchorA = half;
+                        jd.localAnchorB = (m3Vec3){-half.x, -half.y, -half.z};
+                        m3JointId joint = m3CreateJoint(&jd);
+                        m3Joint_SetBreakThresholds(joint, 500.0f, 0.0f);
+                    }
+                }
+            }
+        }
+    }
+    m3ShapeDef heavy = sd;
+    heavy.density = 20.0f;
+    for (int32_t k = 0; k < shots; ++k)
+    {
+        const int32_t target = (int32_t)(SceneSplitMix(&rng) % (uint64_t)towers);
+        const double tx = 16.0 * (double)(target % side) + SceneRand(&rng, -4.0, 4.0);
+        const double tz = 16.0 * (double)(target / side);
+        const double y = SceneRand(&rng, 1.0, 9.0);
+        const double speed = SceneRand(&rng, 20.0, 40.0);
+        // Start 12 m out on the +z side, a little off line, aimed at the
+        // tower's face.
+        bd.position = (m3Pos3){tx + SceneRand(&rng, -1.0, 1.0), y, tz + 12.0 + 0.25 * (double)(k % 4)};
+        bd.linearVelocity = (m3Vec3){0.0f, (float)SceneRand(&rng, 0.0, 2.0), (float)(-speed)};
+        m3BodyId ball = m3CreateBody(world, &bd);
+        m3Sphere shape = {{0.0f, 0.0f, 0.0f}, 0.5f};
+        m3CreateSphereShape(ball, &heavy, &shape);
+    }
+    bd.linearVelocity = (m3Vec3){0.0f, 0.0f, 0.0f};
+    return world;
+}
+
 // Build one seeded scene; returns the null world id for an unknown
 // scene number.
 M3S_API m3WorldId m3s_build(int32_t scene, uint64_t seed, int32_t param)
@@ -693,6 +805,8 @@ M3S_API m3WorldId m3s_build(int32_t scene, uint64_t seed, int32_t param)
         return Plank(seed, param > 0 ? param : 25);
     case M3S_BOUNCE:
         return Bounce(seed, param > 0 ? param : 40);
+    case M3S_CITY:
+        return City(seed, param > 0 ? param : 1000);
     default:
     {
         m3WorldId none = {0, 0};

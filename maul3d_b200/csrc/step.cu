@@ -141,6 +141,9 @@ struct m3Scratch
     int32_t* treeMoveCount; // M3_TREE_LAG: moves of each step in the ring
     int32_t* treeMoveShape; // M3_TREE_LAG x shapeCap: a step's moves (shapes, ascending)
     m3Aabb* treeMoveBox;   // M3_TREE_LAG x shapeCap: the fat bounds they are inserted with
+    uint32_t* gridBar;     // 4 words: the wide kernels' grid barrier (count, generation, error)
+    int32_t* staticList;   // per shape: static-target flags, then their scan
+    int32_t* targetList;   // the continuous phase's static targets, ascending
 };
 
 static __host__ __device__ inline int64_t NextPow2(int64_t n)
@@ -214,6 +217,9 @@ static __host__ __device__ inline int64_t ScratchCarve(m3Scratch* s, uint8_t* ba
     M3_CARVE(leafBox, m3Aabb, shapeCap)
     M3_CARVE(hasLeaf, int32_t, shapeCap)
     M3_CARVE(treeMoveCount, int32_t, M3_TREE_LAG)
+    M3_CARVE(gridBar, uint32_t, 4)
+    M3_CARVE(staticList, int32_t, shapeCap + 1)
+    M3_CARVE(targetList, int32_t, shapeCap)
     M3_CARVE(treeMoveBox, m3Aabb, (int64_t)treeLag * shapeCap)
     M3_CARVE(treeMoveShape, int32_t, (int64_t)treeLag * shapeCap)
 #undef M3_CARVE
@@ -1410,6 +1416,10 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3PrepareKernel(const m3WorldV
     {
         s_status = sc->status;
         s_anyRestitution = 0;
+        // A wide substep kernel may follow: its grid barrier starts with
+        // no arrivals and no error.
+        s.gridBar[0] = 0;
+        s.gridBar[2] = 0;
         if (s_status == 0)
         {
             // The pair list and manifolds built by the collide kernels
@@ -2281,6 +2291,312 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3SubstepKernel(const m3WorldV
 }
 
 // ---------------------------------------------------------------------
+// Wide worlds: one world across the whole grid
+// ---------------------------------------------------------------------
+// A world of tens of thousands of bodies gets one thread block, and so
+// one SM, in the per-world kernels above.  Its substep loop instead runs
+// here over a cooperative grid of many blocks: the rows of one schedule
+// level (disjoint awake dynamic bodies, the reference's same-colour
+// batches that RunColored fans out to host threads, solver.c:2845-2877)
+// are spread over every thread of the grid, and a grid barrier separates
+// the levels, as the reference's barrier between colours does.  The
+// serial parts (the overflow colour, restitution, the destruction of
+// broken joints) run on one thread between barriers.  Body state stays
+// in global memory (L2), every row's arithmetic is the per-world
+// kernel's.
+
+// Grid barrier over `blocks` co-resident blocks (a cooperative launch).
+// Thread 0 of each block arrives on a counter; the last arrival resets it
+// and advances the generation the others wait on.  A wait that lasts
+// longer than `limitNs` (a block that never arrives) sets the error word
+// instead of spinning on: every block then leaves the kernel at its next
+// barrier, and the host reports the world as failed.
+#define M3_GRID_WAIT_NS (4000000000ull)
+
+__device__ __forceinline__ uint64_t m3GlobalTimerNs()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ bool m3GridSync(uint32_t* bar, uint32_t blocks)
+{
+    __shared__ uint32_t s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        volatile uint32_t* vbar = bar;
+        const uint32_t gen = vbar[1];
+        __threadfence();
+        if (atomicAdd(&bar[0], 1u) == blocks - 1)
+        {
+            bar[0] = 0;
+            __threadfence();
+            atomicAdd(&bar[1], 1u);
+        }
+        else
+        {
+            const uint64_t start = m3GlobalTimerNs();
+            while (vbar[1] == gen && vbar[2] == 0)
+            {
+                __nanosleep(64);
+                if (m3GlobalTimerNs() - start > M3_GRID_WAIT_NS)
+                {
+                    atomicExch(&bar[2], 1u);
+                    break;
+                }
+            }
+        }
+        __threadfence();
+        s_ok = vbar[2] == 0 ? 1u : 0u;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT, 2) m3WideSubstepKernel(const m3WorldView* views,
+                                                           const int32_t* order, float dt,
+                                                           int32_t substeps)
+{
+    const m3WorldView& w = views[order[0]];
+    m3WorldScalars* sc = w.sc;
+    if (sc->status != 0)
+    {
+        return;
+    }
+    m3Scratch s;
+    ScratchCarve(&s, w.scratch, sc->bodyCap, sc->shapeCap, sc->jointCap, sc->pairCap);
+    uint32_t* bar = s.gridBar;
+    const uint32_t blocks = gridDim.x;
+    const int32_t tid = threadIdx.x;
+    const int32_t gtid = (int32_t)blockIdx.x * NT + tid;
+    const int32_t gstride = (int32_t)blocks * NT;
+    const bool lead = blockIdx.x == 0 && tid == 0;
+    const int32_t constraintCount = s.plan->constraintCount;
+    const int32_t jointCount = s.plan->jointCount;
+    const int32_t jointLevels = s.plan->jointLevels;
+    const int32_t moverCount = s.plan->moverCount;
+    const int32_t levels = s.plan->levels;
+    const bool anyRestitution = s.plan->anyRestitution != 0;
+    m3Manifold* man = sc->pairBuf == 0 ? w.man0 : w.man1;
+    const m3real h = dt / (m3real)substeps;
+    const m3real invH = h > 0.0f ? 1.0f / h : 0.0f;
+    const m3real pushMax = sc->contactPushMaxSpeed;
+    m3Vec3* dP = s.deltaPos;
+    m3Quat* dQ = s.deltaRot;
+    const m3Mat3* invI = s.bodyInvI;
+    m3JointDev* jrows = s.joints;
+    long long t_phase = clock64();
+#define M3_WIDE_MARK(k)                                                                            \
+    if (lead)                                                                                      \
+    {                                                                                              \
+        long long now_ = clock64();                                                                \
+        sc->phase[k] += (uint64_t)(now_ - t_phase);                                                \
+        t_phase = now_;                                                                            \
+    }
+    // (The substep deltas were cleared by the prepare kernel.)
+    // One pass over the joint/contact schedule: per level, the level's
+    // joint rows then its contact rows, over the whole grid; the overflow
+    // colour serially.
+    auto pass = [&](int32_t which) -> bool {
+        for (int32_t level = 0; level < levels; ++level)
+        {
+            int32_t j0 = 0;
+            int32_t nj = 0;
+            if (level < jointLevels)
+            {
+                j0 = s.jointLevelStart[level];
+                nj = s.jointLevelStart[level + 1] - j0;
+            }
+            const int32_t c0 = s.levelStart[level];
+            const int32_t nc = s.levelStart[level + 1] - c0;
+            for (int32_t r = gtid; r < nj + nc; r += gstride)
+            {
+                if (r < nj)
+                {
+                    m3JointDev* row = &jrows[s.jointOrder[j0 + r]];
+                    if (which == 0)
+                    {
+                        m3WarmStartJoint(w, row, dQ);
+                    }
+                    else
+                    {
+                        m3SolveJoint(w, row, dP, dQ, h, invH, which == 1);
+                    }
+                }
+                else
+                {
+                    const m3ConRef c = m3ConAt(s.rows, c0 + (r - nj));
+                    if (which == 0)
+                    {
+                        m3WarmStartContact(w, c, invI);
+                    }
+                    else
+                    {
+                        m3SolveContact(w, c, invI, dP, dQ, invH, pushMax, which == 1);
+                    }
+                }
+            }
+            if (!m3GridSync(bar, blocks))
+            {
+                return false;
+            }
+        }
+        const int32_t o0 = s.levelStart[levels];
+        const int32_t o1 = s.levelStart[levels + 1];
+        if (o1 > o0)
+        {
+            if (lead)
+            {
+                for (int32_t k = o0; k < o1; ++k)
+                {
+                    if (which == 0)
+                    {
+                        m3WarmStartContact(w, m3ConAt(s.rows, k), invI);
+                    }
+                    else
+                    {
+                        m3SolveContact(w, m3ConAt(s.rows, k), invI, dP, dQ, invH, pushMax,
+                                       which == 1);
+                    }
+                }
+            }
+            if (!m3GridSync(bar, blocks))
+            {
+                return false;
+            }
+        }
+        return true;
+    };
+    // The substep loop (solver.c:4085-4203).
+    for (int32_t sub = 0; sub < substeps; ++sub)
+    {
+        for (int32_t m = gtid; m < moverCount; m += gstride)
+        {
+            const int32_t i = s.movers[m];
+            if (w.btype[i] == M3_BODY_DYNAMIC)
+            {
+                m3IntegrateVelocity(w, i, h);
+            }
+        }
+        if (!m3GridSync(bar, blocks))
+        {
+            return;
+        }
+        M3_WIDE_MARK(M3_PHASE_INTEGRATE_V)
+        if (!pass(0))
+        {
+            return;
+        }
+        M3_WIDE_MARK(M3_PHASE_WARM)
+        if (!pass(1))
+        {
+            return;
+        }
+        M3_WIDE_MARK(M3_PHASE_SOLVE)
+        for (int32_t m = gtid; m < moverCount; m += gstride)
+        {
+            m3IntegratePosition(w, s.movers[m], h, dP, dQ);
+        }
+        if (!m3GridSync(bar, blocks))
+        {
+            return;
+        }
+        M3_WIDE_MARK(M3_PHASE_INTEGRATE_P)
+        if (!pass(2))
+        {
+            return;
+        }
+        M3_WIDE_MARK(M3_PHASE_RELAX)
+    }
+    // Forces live one step (solver.c:4207-4211).
+    for (int32_t m = gtid; m < moverCount; m += gstride)
+    {
+        const int32_t i = s.movers[m];
+        w.force[i] = v3(0.0f, 0.0f, 0.0f);
+        w.torque[i] = v3(0.0f, 0.0f, 0.0f);
+    }
+    // Restitution is serial in constraint order (solver.c:2879-2906).
+    if (anyRestitution)
+    {
+        if (lead)
+        {
+            const m3real threshold = sc->restitutionThreshold;
+            for (int32_t i = 0; i < constraintCount; ++i)
+            {
+                m3RestituteContact(w, m3ConAt(s.rows, s.conSlot[i]), invI, threshold);
+            }
+        }
+        if (!m3GridSync(bar, blocks))
+        {
+            return;
+        }
+    }
+    for (int32_t i = gtid; i < constraintCount; i += gstride)
+    {
+        m3StoreContact(m3ConAt(s.rows, i), man);
+    }
+    for (int32_t r = gtid; r < jointCount; r += gstride)
+    {
+        m3StoreJoint(w, &jrows[r]);
+    }
+    if (!m3GridSync(bar, blocks)) // breakage reads the stored joint impulses
+    {
+        return;
+    }
+    // Breakage: each joint's test alone over the grid, the destruction of
+    // the broken ones in ascending order on one thread.
+    const int32_t jointMax = sc->jointMax;
+    for (int32_t j = gtid; j < jointMax; j += gstride)
+    {
+        s.jointFlag[j] = m3JointBreaksDev(w, j, invH) ? 1 : 0;
+    }
+    if (!m3GridSync(bar, blocks))
+    {
+        return;
+    }
+    if (lead)
+    {
+        sc->lastInvH = invH;
+        // Wind phase (solver.c:4220-4229).
+        if (sc->windGustHertz > 0.0f)
+        {
+            sc->windPhase += 2.0f * M3_PI * sc->windGustHertz * dt;
+            if (sc->windPhase > 2.0f * M3_PI)
+            {
+                sc->windPhase -=
+                    2.0f * M3_PI * (m3real)(int32_t)(sc->windPhase / (2.0f * M3_PI));
+            }
+        }
+        for (int32_t j = 0; j < jointMax; ++j)
+        {
+            if (s.jointFlag[j] != 0)
+            {
+                m3DestroyBrokenJointDev(w, j);
+            }
+        }
+    }
+    M3_WIDE_MARK(M3_PHASE_STORE)
+#undef M3_WIDE_MARK
+}
+
+// A barrier that gave up marks the world failed (after the wide kernel,
+// one thread).
+__global__ void m3WideStatusKernel(const m3WorldView* views, const int32_t* order)
+{
+    const m3WorldView& w = views[order[0]];
+    m3Scratch s;
+    ScratchCarve(&s, w.scratch, w.sc->bodyCap, w.sc->shapeCap, w.sc->jointCap, w.sc->pairCap);
+    if (s.gridBar[2] != 0 && w.sc->status == 0)
+    {
+        w.sc->status = M3GPU_ERR_CUDA;
+        w.sc->statusDetail = 7001;
+    }
+}
+
+// ---------------------------------------------------------------------
 // The tree arm of the continuous phase for one shape of a fast body
 // (solver.c:3081-3274): every static target whose tree leaf touches the
 // swept box [lo, hi], swept by the time of impact bounded by `*fraction`.
@@ -2289,7 +2605,8 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3SubstepKernel(const m3WorldV
 // voxel target.
 __device__ __noinline__ int32_t SweepStaticTargets(const m3WorldView& w, const m3Pos3* com0,
                                                    const m3Quat* rot0, int32_t i, int32_t sh,
-                                                   int32_t shapeMax, const double* lo,
+                                                   const int32_t* targets, int32_t targetCount,
+                                                   const double* lo,
                                                    const double* hi, const m3Pos3& base,
                                                    const m3ProxyDev& proxyB,
                                                    const m3SweepDev& fastSweep, m3real* fraction,
@@ -2298,8 +2615,11 @@ __device__ __noinline__ int32_t SweepStaticTargets(const m3WorldView& w, const m
     const m3real limit = *fraction;
     int32_t hits = 0;
     m3real hitFraction = limit;
-    for (int32_t o = 0; o < shapeMax; ++o)
+    // `targets` lists, ascending, the alive non-plane shapes of static
+    // bodies: the only shapes the checks below can let through.
+    for (int32_t n = 0; n < targetCount; ++n)
     {
+        const int32_t o = targets[n];
         if (w.shapeAlive[o] == 0 || w.shapeType[o] == M3_SHAPE_PLANE || o == sh ||
             w.proxyId[o] == M3_TREE_NULL)
         {
@@ -2410,24 +2730,69 @@ __global__ void __launch_bounds__(M3_BLOCK, 2) m3FinishKernel(const m3WorldView*
     // a mesh or voxel target, or two tree hits for one shape are refused.
     if (sc->continuousEnabled != 0)
     {
-        // Whether the world holds any static non-plane shape: without one
-        // the tree arm finds nothing, and fast bodies meet only planes.
-        __shared__ int32_t s_targets;
+        // The targets, once per step and ascending: the static non-plane
+        // shapes (the tree arm's only candidates) and the planes (at most
+        // M3_MAX_PLANES: the broadphase refuses more).  Without a static
+        // target the tree arm finds nothing, and fast bodies meet only
+        // planes.
+        __shared__ int32_t s_planeList[M3_MAX_PLANES];
+        __shared__ int32_t s_planeCount;
         if (tid == 0)
         {
-            s_targets = 0;
+            s_planeCount = 0;
         }
         __syncthreads();
         for (int32_t o = tid; o < shapeMax; o += M3_BLOCK)
         {
-            if (w.shapeAlive[o] != 0 && w.shapeType[o] != M3_SHAPE_PLANE &&
-                w.btype[w.shapeBody[o]] == M3_BODY_STATIC)
+            int32_t flag = 0;
+            if (w.shapeAlive[o] != 0)
             {
-                s_targets = 1;
+                if (w.shapeType[o] == M3_SHAPE_PLANE)
+                {
+                    const int32_t k = atomicAdd(&s_planeCount, 1);
+                    if (k < M3_MAX_PLANES)
+                    {
+                        s_planeList[k] = o;
+                    }
+                }
+                else if (w.btype[w.shapeBody[o]] == M3_BODY_STATIC)
+                {
+                    flag = 1;
+                }
+            }
+            s.staticList[o] = flag;
+        }
+        __syncthreads();
+        if (tid == 0)
+        {
+            // Planes in ascending shape order (the reference's scan).
+            const int32_t n = s_planeCount < M3_MAX_PLANES ? s_planeCount : M3_MAX_PLANES;
+            for (int32_t a = 1; a < n; ++a)
+            {
+                const int32_t v = s_planeList[a];
+                int32_t b = a - 1;
+                while (b >= 0 && s_planeList[b] > v)
+                {
+                    s_planeList[b + 1] = s_planeList[b];
+                    b -= 1;
+                }
+                s_planeList[b + 1] = v;
+            }
+            s_planeCount = n;
+        }
+        const int32_t targetCount = BlockExclusiveScan<M3_BLOCK>(s.staticList, shapeMax);
+        int32_t* targets = s.targetList;
+        for (int32_t o = tid; o < shapeMax; o += M3_BLOCK)
+        {
+            const int32_t next = o + 1 < shapeMax ? s.staticList[o + 1] : targetCount;
+            if (next != s.staticList[o])
+            {
+                targets[s.staticList[o]] = o;
             }
         }
         __syncthreads();
-        const bool staticTargets = s_targets != 0;
+        const bool staticTargets = targetCount > 0;
+        const int32_t planeCount = s_planeCount;
         for (int32_t i = tid; i < bodyMax; i += M3_BLOCK)
         {
             if (w.bodyAlive[i] == 0 || w.btype[i] != M3_BODY_DYNAMIC)
@@ -2494,8 +2859,9 @@ __global__ void __launch_bounds__(M3_BLOCK, 2) m3FinishKernel(const m3WorldView*
                 proxyB.count = ProxyPoints(w, sh, &proxyB.points, scratchB, &proxyB.radius);
                 int32_t refusal = 0;
                 const int32_t hits =
-                    staticTargets ? SweepStaticTargets(w, s.com0, s.rot0, i, sh, shapeMax, lo, hi,
-                                                       base, proxyB, fastSweep, &fraction, &refusal)
+                    staticTargets ? SweepStaticTargets(w, s.com0, s.rot0, i, sh, targets,
+                                                       targetCount, lo, hi, base, proxyB,
+                                                       fastSweep, &fraction, &refusal)
                                   : 0;
                 if (refusal != 0)
                 {
@@ -2507,13 +2873,10 @@ __global__ void __launch_bounds__(M3_BLOCK, 2) m3FinishKernel(const m3WorldView*
                     s_status = M3GPU_ERR_UNSUPPORTED;
                     sc->statusDetail = 3002;
                 }
-                for (int32_t p = 0; p < shapeMax; ++p)
+                for (int32_t k = 0; k < planeCount; ++k)
                 {
-                    if (w.shapeAlive[p] != 0 && w.shapeType[p] == M3_SHAPE_PLANE)
-                    {
-                        ContinuousVersusPlane(w, i, sh, p, base, lc, sc1, sc2, q0, xfEnd.q,
-                                              &fraction);
-                    }
+                    ContinuousVersusPlane(w, i, sh, s_planeList[k], base, lc, sc1, sc2, q0,
+                                          xfEnd.q, &fraction);
                 }
             }
             if (fraction < 1.0f)
@@ -3112,9 +3475,73 @@ static void ClassStage(int32_t stage, const m3WorldView* views, const int32_t* o
     }
 }
 
+// Wide worlds: a single world with at least this many shape slots steps
+// its substep loop over a cooperative grid (m3WideSubstepKernel).
+static int32_t s_wideMinShapes = 4096;
+static int32_t s_smCount = 148;
+
+extern "C" int32_t m3gpu_set_wide_min_shapes(int32_t shapes)
+{
+    M3_DEVICE_GUARD;
+    const int32_t previous = s_wideMinShapes;
+    if (shapes > 0)
+    {
+        s_wideMinShapes = shapes;
+    }
+    return previous;
+}
+
+// Blocks of the wide grid for a world: enough to give each level's rows
+// a thread or so (about one block per 512 shape slots), at least 8, and
+// never more than can be resident at once (a cooperative launch).
+static int32_t WideBlocks(const m3HostWorld* w)
+{
+    static int32_t maxResident = 0;
+    const int32_t shapes = w->hv.sc->shapeMax;
+    if (shapes < s_wideMinShapes)
+    {
+        return 0;
+    }
+    if (maxResident == 0)
+    {
+        int device = 0;
+        int sms = 0;
+        int perSm = 0;
+        cudaGetDevice(&device);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        s_smCount = sms;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, m3WideSubstepKernel<256>, 256, 0);
+        maxResident = sms * perSm;
+        if (maxResident <= 0)
+        {
+            maxResident = -1; // cooperative launch impossible: never wide
+        }
+    }
+    if (maxResident < 0)
+    {
+        return 0;
+    }
+    // At most one block per SM: the other half of each SM stays free for
+    // the tree walks running beside the step on their own stream.
+    int32_t blocks = shapes / 512;
+    blocks = blocks < 8 ? 8 : blocks;
+    blocks = blocks < s_smCount ? blocks : s_smCount;
+    return blocks < maxResident ? blocks : maxResident;
+}
+
+static void LaunchWideSubstep(const m3WorldView* views, const int32_t* order, float dt,
+                              int32_t substeps, int32_t blocks)
+{
+    void* args[] = {(void*)&views, (void*)&order, (void*)&dt, (void*)&substeps};
+    cudaLaunchCooperativeKernel((const void*)m3WideSubstepKernel<256>, dim3(blocks), dim3(256),
+                                args, 0, 0);
+    m3WideStatusKernel<<<1, 1>>>(views, order);
+}
+
 static void LaunchSolve(const m3WorldView* views, const int32_t* order, int32_t count, float dt,
                         int32_t substeps, int32_t cacheBytes, const cudaEvent_t* marks,
-                        const int32_t* classFirst = nullptr, const int32_t* classCache = nullptr)
+                        const int32_t* classFirst = nullptr, const int32_t* classCache = nullptr,
+                        int32_t wideBlocks = 0)
 {
     if (classFirst == nullptr)
     {
@@ -3129,7 +3556,11 @@ static void LaunchSolve(const m3WorldView* views, const int32_t* order, int32_t 
     {
         cudaEventRecord(marks[0]);
     }
-    if (classFirst == nullptr)
+    if (wideBlocks > 0)
+    {
+        LaunchWideSubstep(views, order, dt, substeps, wideBlocks);
+    }
+    else if (classFirst == nullptr)
     {
         m3SubstepKernel<256, 2><<<count, 256, cacheBytes>>>(views, order, count, dt, substeps,
                                                             cacheBytes);
@@ -3492,6 +3923,8 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
         }
     }
     const cudaStream_t treeStream = s_classStreams.tree;
+    // One large world alone: its substep loop over the whole grid.
+    const int32_t wideBlocks = count == 1 ? WideBlocks(worlds[0]) : 0;
     m3TreeTable* treeTable = nullptr;
     if (anyTracked && steps > 0)
     {
@@ -3549,7 +3982,7 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
         LaunchNarrow(s_batch.dviews, s_batch.doffsets, count, anyTerrain);
         cudaEventRecord(ev[2]);
         LaunchSolve(s_batch.dviews, s_batch.dorder, count, dt, substeps, s_batch.cacheBytes,
-                    ev + 3, s_batch.classFirst, s_batch.classCache);
+                    ev + 3, s_batch.classFirst, s_batch.classCache, wideBlocks);
         cudaEventRecord(ev[5]);
         s_launches += 5 + (count <= M3_NARROW_SMALL_BATCH ? 1 : M3_NARROW_LAUNCHES + (anyTerrain ? M3_TERRAIN_LAUNCHES : 0));
     }

@@ -67,15 +67,20 @@ def build(force: bool = False) -> bool:
     return LIB_PATH.exists()
 
 
-_lib: C.CDLL | None = None
+# The patched build for the largest world: the reference with only its
+# step scratch cap raised from 1 << 28 to 1 << 30 bytes (oracle/Makefile).
+BIG_LIB_PATH = REF_DIR / "libmaul3d_ref_big.so"
+_libs: dict[str, C.CDLL] = {}
 
 
-def lib() -> C.CDLL:
-    global _lib
-    if _lib is None:
-        if not LIB_PATH.exists():
+def lib(variant: str = "stock") -> C.CDLL:
+    """The reference engine: "stock" (unmodified) or "big" (the patched
+    scratch cap, for worlds the stock build stalls on)."""
+    if variant not in _libs:
+        path = LIB_PATH if variant == "stock" else BIG_LIB_PATH
+        if not path.exists():
             build()
-        h = C.CDLL(str(LIB_PATH))
+        h = C.CDLL(str(path))
         abi.bind_common(h)
         for name, n in (("m3o_copy_bodies", 5), ("m3o_copy_pairs", 2), ("m3o_copy_joints", 4)):
             fn = getattr(h, name)
@@ -93,45 +98,51 @@ def lib() -> C.CDLL:
         h.m3o_step_trace.restype = None
         h.m3o_copy_hull.argtypes = [m3WorldId, C.c_int32, C.c_void_p]
         h.m3o_copy_hull.restype = C.c_int32
-        _lib = h
-    return _lib
+        _libs[variant] = h
+    return _libs[variant]
 
 
 class RefWorld:
-    """One world inside the reference engine."""
+    """One world inside the reference engine (the stock build unless
+    `variant` says "big")."""
 
-    def __init__(self, wid: m3WorldId):
+    def __init__(self, wid: m3WorldId, variant: str = "stock"):
         if wid.index1 == 0:
             raise RuntimeError("reference refused to create the world")
         self.id = wid
+        self.lib = lib(variant)
 
     @classmethod
-    def scene(cls, scene: int, seed: int = 0, param: int = 0) -> "RefWorld":
-        return cls(lib().m3s_build(scene, seed, param))
+    def scene(cls, scene: int, seed: int = 0, param: int = 0,
+              variant: str = "stock") -> "RefWorld":
+        return cls(lib(variant).m3s_build(scene, seed, param), variant)
 
     def step(self, dt: float = 1.0 / 60.0, substeps: int = 4, steps: int = 1) -> None:
-        lib().m3o_step_trace(self.id, dt, substeps, steps, None)
+        self.lib.m3o_step_trace(self.id, dt, substeps, steps, None)
 
     def trace(self, dt: float, substeps: int, steps: int) -> np.ndarray:
         """Step and return the world hash after every step."""
         out = np.zeros(steps, np.uint64)
-        lib().m3o_step_trace(self.id, dt, substeps, steps, out.ctypes.data)
+        self.lib.m3o_step_trace(self.id, dt, substeps, steps, out.ctypes.data)
         return out
 
     def hash(self) -> int:
-        return int(lib().m3World_Hash(self.id))
+        return int(self.lib.m3World_Hash(self.id))
 
     def destroy(self) -> None:
-        lib().m3DestroyWorld(self.id)
+        self.lib.m3DestroyWorld(self.id)
 
     def body_count(self) -> int:
-        return int(lib().m3o_body_max(self.id))
+        return int(self.lib.m3o_body_max(self.id))
 
     def pair_count(self) -> int:
-        return int(lib().m3o_pair_count(self.id))
+        return int(self.lib.m3o_pair_count(self.id))
 
     def scratch_overflow(self) -> int:
-        return int(lib().m3o_scratch_overflow(self.id))
+        return int(self.lib.m3o_scratch_overflow(self.id))
+
+    def step_count(self) -> int:
+        return int(self.lib.m3o_step_count(self.id))
 
     def state(self) -> WorldState:
         n = self.body_count()
@@ -140,13 +151,13 @@ class RefWorld:
         ang = np.zeros(n, VEC3)
         awake = np.zeros(n, np.uint8)
         sleep = np.zeros(n, np.float32)
-        lib().m3o_copy_bodies(self.id, xf.ctypes.data, lin.ctypes.data, ang.ctypes.data,
+        self.lib.m3o_copy_bodies(self.id, xf.ctypes.data, lin.ctypes.data, ang.ctypes.data,
                               awake.ctypes.data, sleep.ctypes.data, n)
         p = self.pair_count()
         keys = np.zeros(p, np.uint64)
         man = np.zeros(p, MANIFOLD)
         if p > 0:
-            lib().m3o_copy_pairs(self.id, keys.ctypes.data, man.ctypes.data, p)
+            self.lib.m3o_copy_pairs(self.id, keys.ctypes.data, man.ctypes.data, p)
         return WorldState(xf, lin, ang, awake, sleep, keys, man)
 
     def mass(self) -> dict:
@@ -154,7 +165,7 @@ class RefWorld:
         out = {"invMass": np.zeros(n, np.float32), "invInertia": np.zeros(n, MAT3),
                "inertia": np.zeros(n, MAT3), "localCenter": np.zeros(n, VEC3),
                "minExtent": np.zeros(n, np.float32), "maxExtent": np.zeros(n, np.float32)}
-        lib().m3o_copy_mass(self.id, *[out[k].ctypes.data for k in
+        self.lib.m3o_copy_mass(self.id, *[out[k].ctypes.data for k in
                                        ("invMass", "invInertia", "inertia", "localCenter",
                                         "minExtent", "maxExtent")], n)
         return out
