@@ -47,6 +47,9 @@
 #include <vector>
 
 #define M3_BLOCK 256
+// Planes a world may hold (the broadphase enumerates their pairs
+// directly; more are refused).
+#define M3_MAX_PLANES 16
 // Colouring: the marker of a constraint not coloured yet, and the
 // parallel rounds before the serial finish.
 #define M3_COLOR_PENDING 0xFF
@@ -144,6 +147,8 @@ struct m3Scratch
     uint32_t* gridBar;     // 4 words: the wide kernels' grid barrier (count, generation, error)
     int32_t* staticList;   // per shape: static-target flags, then their scan
     int32_t* targetList;   // the continuous phase's static targets, ascending
+    int2* jointBodies;     // per joint row: its two bodies (the level walk's compact input)
+    int32_t* broadState;   // 20 words: a wide world's broadphase between its kernels
 };
 
 static __host__ __device__ inline int64_t NextPow2(int64_t n)
@@ -220,6 +225,8 @@ static __host__ __device__ inline int64_t ScratchCarve(m3Scratch* s, uint8_t* ba
     M3_CARVE(gridBar, uint32_t, 4)
     M3_CARVE(staticList, int32_t, shapeCap + 1)
     M3_CARVE(targetList, int32_t, shapeCap)
+    M3_CARVE(jointBodies, int2, jointCap)
+    M3_CARVE(broadState, int32_t, 4 + M3_MAX_PLANES)
     M3_CARVE(treeMoveBox, m3Aabb, (int64_t)treeLag * shapeCap)
     M3_CARVE(treeMoveShape, int32_t, (int64_t)treeLag * shapeCap)
 #undef M3_CARVE
@@ -380,7 +387,6 @@ __device__ __forceinline__ uint64_t OrderKey(double x)
     return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
 }
 
-#define M3_MAX_PLANES 16
 
 // The broadphase tree's leaves as the broadphase reads them: each
 // shape's leaf bounds, copied out of the tree once per batch; the
@@ -537,7 +543,16 @@ __device__ __forceinline__ void SweepFrom(const m3WorldView& w, const m3Scratch&
 #define M3_LONG_ROW 64
 #define M3_LONG_ROWS 16
 
-template <int NT, int MIN_BLOCKS>
+// PART 0 is the whole broadphase of one world per block.  A wide world
+// splits it around the sweep: PART 1 (bounds, tree moves, sort; one
+// block) leaves the plane list and the sweep count in s.broadState,
+// m3WideSweepKernel counts and records the pairs over the whole grid,
+// PART 2 (scan, fill, row order; one block) finishes.
+#define M3_BS_PLANES 0
+#define M3_BS_SWEEP 1
+#define M3_BS_PAIRS 2
+#define M3_BS_PLANE0 4
+template <int NT, int MIN_BLOCKS, int PART = 0>
 __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3BroadKernel(const m3WorldView* views,
                                                           const int32_t* order, int32_t count,
                                                           int32_t treeLag)
@@ -566,13 +581,22 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3BroadKernel(const m3WorldVie
         // must never replay a slot (or scratch shared with another world)
         // left by an older step.
         int32_t slot = 0;
-        if (sc->treeTracked != 0)
+        if (PART != 2 && sc->treeTracked != 0)
         {
             slot = (int32_t)((uint32_t)sc->treeHead % (uint32_t)treeLag);
             sc->treeHead += 1;
             s.treeMoveCount[slot] = 0;
         }
         s_treeSlot = slot;
+        if (PART == 2 && s_status == 0)
+        {
+            s_planeCount = s.broadState[M3_BS_PLANES];
+            s_sweepPairs = s.broadState[M3_BS_PAIRS];
+            for (int32_t k = 0; k < s_planeCount && k < M3_MAX_PLANES; ++k)
+            {
+                s_planes[k] = s.broadState[M3_BS_PLANE0 + k];
+            }
+        }
     }
     __syncthreads();
     const int32_t treeSlot = s_treeSlot;
@@ -582,6 +606,8 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3BroadKernel(const m3WorldVie
     }
     long long t_phase = clock64();
     const int32_t shapeMax = sc->shapeMax;
+    if (PART != 2)
+    {
 
     // Fresh bounds once per shape; the sweep set and the plane list.
     for (int32_t i = tid; i < shapeMax; i += NT)
@@ -710,6 +736,20 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3BroadKernel(const m3WorldVie
     }
 
     M3_PHASE_MARK(M3_PHASE_SORT)
+    if (PART == 1)
+    {
+        if (tid == 0)
+        {
+            s.broadState[M3_BS_PLANES] = s_planeCount;
+            s.broadState[M3_BS_SWEEP] = n;
+            s.broadState[M3_BS_PAIRS] = 0;
+            for (int32_t k = 0; k < s_planeCount; ++k)
+            {
+                s.broadState[M3_BS_PLANE0 + k] = s_planes[k];
+            }
+        }
+        return;
+    }
     // Count every row's pairs; the sweep's pairs are recorded on the way
     // so the fill below need not sweep again.
     const int32_t planeCount = s_planeCount;
@@ -743,6 +783,8 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3BroadKernel(const m3WorldVie
         }
     }
     __syncthreads();
+    }
+    const int32_t planeCount = s_planeCount;
     const int32_t total = BlockExclusiveScan<NT>(s.rowCount, shapeMax);
     if (total > sc->pairCap)
     {
@@ -899,6 +941,58 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3BroadKernel(const m3WorldVie
     if (tid == 0)
     {
         sc->newPairCount = total;
+    }
+}
+
+// A wide world's sweep (between m3BroadKernel PART 1 and PART 2): every
+// sorted position sweeps its own candidates, as the per-world kernel's
+// threads do, over the whole grid; row counts and the recorded pairs go
+// through global atomics (the fill orders each row afterwards).
+__global__ void __launch_bounds__(256) m3WideSweepKernel(const m3WorldView* views,
+                                                        const int32_t* order)
+{
+    const m3WorldView& w = views[order[0]];
+    m3WorldScalars* sc = w.sc;
+    if (sc->status != 0)
+    {
+        return;
+    }
+    m3Scratch s;
+    ScratchCarve(&s, w.scratch, sc->bodyCap, sc->shapeCap, sc->jointCap, sc->pairCap);
+    const int32_t n = s.broadState[M3_BS_SWEEP];
+    const int32_t planeCount = s.broadState[M3_BS_PLANES];
+    const int32_t pairCap = sc->pairCap;
+    const int32_t shapeMax = sc->shapeMax;
+    const int32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int32_t gstride = gridDim.x * blockDim.x;
+    int32_t* recorded = &s.broadState[M3_BS_PAIRS];
+    for (int32_t p = gtid; p < n; p += gstride)
+    {
+        SweepFrom(w, s, p, n, [&](int32_t lo, int32_t hi) {
+            atomicAdd(&s.rowCount[lo], 1);
+            const int32_t r = atomicAdd(recorded, 1);
+            if (r < pairCap)
+            {
+                s.sweepPairs[r] = ((uint64_t)(uint32_t)lo << 32) | (uint64_t)(uint32_t)hi;
+            }
+        });
+    }
+    for (int32_t i = gtid; i < shapeMax; i += gstride)
+    {
+        if (w.shapeAlive[i] == 0 || w.shapeType[i] == M3_SHAPE_PLANE)
+        {
+            continue;
+        }
+        for (int32_t k = 0; k < planeCount; ++k)
+        {
+            const int32_t pl = s.broadState[M3_BS_PLANE0 + k];
+            const int32_t lo = pl < i ? pl : i;
+            const int32_t hi = pl < i ? i : pl;
+            if (PairAllowed(w, lo, hi))
+            {
+                atomicAdd(&s.rowCount[lo], 1);
+            }
+        }
     }
 }
 
@@ -1398,7 +1492,7 @@ template <int NT, int MIN_BLOCKS>
 __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3PrepareKernel(const m3WorldView* views,
                                                             const int32_t* order, int32_t count,
                                                             float dt, int32_t substeps,
-                                                            int32_t cacheBytes)
+                                                            int32_t cacheBytes, int32_t wide = 0)
 {
     const int32_t wi = order[blockIdx.x];
     const m3WorldView& w = views[wi];
@@ -1586,57 +1680,65 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3PrepareKernel(const m3WorldV
         int32_t next = j + 1 < jointMax ? s.jointFlag[j + 1] : jointCount;
         if (next != s.jointFlag[j])
         {
-            m3PrepareJoint(w, &s.joints[s.jointFlag[j]], j, h);
+            const int32_t r = s.jointFlag[j];
+            m3PrepareJoint(w, &s.joints[r], j, h);
+            s.jointBodies[r] = make_int2(s.joints[r].bodyA, s.joints[r].bodyB);
         }
+    }
+    for (int32_t i = tid; i < bodyMax; i += NT)
+    {
+        s.ready[i] = -1;
+    }
+    __syncthreads();
+    // The levels follow the slot order: one thread walks the rows' body
+    // pairs (a compact array, read ahead of the walk's own dependences).
+    if (tid == 0)
+    {
+        int32_t levels = 0;
+        for (int32_t r = 0; r < jointCount; ++r)
+        {
+            const int2 ab = s.jointBodies[r];
+            const int32_t la = s.ready[ab.x];
+            const int32_t lb = s.ready[ab.y];
+            const int32_t level = 1 + (la > lb ? la : lb);
+            s.ready[ab.x] = level;
+            s.ready[ab.y] = level;
+            s.jointLevel[r] = level;
+            levels = level + 1 > levels ? level + 1 : levels;
+        }
+        s_jointLevels = levels;
+        sc->jointConstraintCount = jointCount;
+    }
+    __syncthreads();
+    // Rows grouped by level (any order inside a level: its rows touch
+    // disjoint bodies).
+    const int32_t jointLevelCount = s_jointLevels;
+    for (int32_t k = tid; k <= jointLevelCount; k += NT)
+    {
+        s.jointLevelStart[k] = 0;
+    }
+    __syncthreads();
+    for (int32_t r = tid; r < jointCount; r += NT)
+    {
+        atomicAdd(&s.jointLevelStart[s.jointLevel[r] + 1], 1);
     }
     __syncthreads();
     if (tid == 0)
     {
-        int32_t levels = 0;
-        if (jointCount > 0)
+        for (int32_t k = 0; k < jointLevelCount; ++k)
         {
-            for (int32_t i = 0; i < bodyMax; ++i)
-            {
-                s.ready[i] = -1;
-            }
-            for (int32_t r = 0; r < jointCount; ++r)
-            {
-                int32_t a = s.joints[r].bodyA;
-                int32_t b = s.joints[r].bodyB;
-                int32_t la = s.ready[a];
-                int32_t lb = s.ready[b];
-                int32_t level = 1 + (la > lb ? la : lb);
-                s.ready[a] = level;
-                s.ready[b] = level;
-                s.jointLevel[r] = level;
-                levels = level + 1 > levels ? level + 1 : levels;
-            }
-            for (int32_t k = 0; k <= levels; ++k)
-            {
-                s.jointLevelStart[k] = 0;
-            }
-            for (int32_t r = 0; r < jointCount; ++r)
-            {
-                s.jointLevelStart[s.jointLevel[r] + 1] += 1;
-            }
-            for (int32_t k = 0; k < levels; ++k)
-            {
-                s.jointLevelStart[k + 1] += s.jointLevelStart[k];
-            }
-            for (int32_t r = 0; r < jointCount; ++r)
-            {
-                int32_t level = s.jointLevel[r];
-                s.jointOrder[s.jointLevelStart[level]] = r;
-                s.jointLevelStart[level] += 1;
-            }
-            for (int32_t k = levels; k > 0; --k)
-            {
-                s.jointLevelStart[k] = s.jointLevelStart[k - 1];
-            }
-            s.jointLevelStart[0] = 0;
+            s.jointLevelStart[k + 1] += s.jointLevelStart[k];
         }
-        s_jointLevels = levels;
-        sc->jointConstraintCount = jointCount;
+    }
+    __syncthreads();
+    for (int32_t k = tid; k <= jointLevelCount; k += NT)
+    {
+        s.levelFill[k] = s.jointLevelStart[k];
+    }
+    __syncthreads();
+    for (int32_t r = tid; r < jointCount; r += NT)
+    {
+        s.jointOrder[atomicAdd(&s.levelFill[s.jointLevel[r]], 1)] = r;
     }
     __syncthreads();
     if (s_status != 0)
@@ -1961,8 +2063,10 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3PrepareKernel(const m3WorldV
     __syncthreads();
     M3_PHASE_MARK(M3_PHASE_COLOR)
     // Contact rows (solver.c:261-405), prepared straight into their
-    // solve slots; consecutive threads write consecutive slots.
-    for (int32_t slot = tid; slot < constraintCount; slot += NT)
+    // solve slots; consecutive threads write consecutive slots.  A wide
+    // world's rows are prepared over the whole grid instead
+    // (m3WideRowsKernel, right after this kernel).
+    for (int32_t slot = tid; slot < constraintCount && wide == 0; slot += NT)
     {
         m3ContactDev c;
         m3PrepareContact(w, &c, s.conPairIndex[s.lists[slot]], keys, man, soft, staticSoft,
@@ -2580,6 +2684,46 @@ __global__ void __launch_bounds__(NT, 2) m3WideSubstepKernel(const m3WorldView* 
     }
     M3_WIDE_MARK(M3_PHASE_STORE)
 #undef M3_WIDE_MARK
+}
+
+// A wide world's contact rows (solver.c:261-405), one per thread over
+// the whole grid, straight into the solve slots the prepare kernel
+// assigned: the same arithmetic as the per-world kernel's row loop.
+__global__ void __launch_bounds__(256) m3WideRowsKernel(const m3WorldView* views,
+                                                       const int32_t* order, float dt,
+                                                       int32_t substeps)
+{
+    const m3WorldView& w = views[order[0]];
+    m3WorldScalars* sc = w.sc;
+    if (sc->status != 0)
+    {
+        return;
+    }
+    m3Scratch s;
+    ScratchCarve(&s, w.scratch, sc->bodyCap, sc->shapeCap, sc->jointCap, sc->pairCap);
+    const uint64_t* keys = sc->pairBuf == 0 ? w.keys0 : w.keys1;
+    m3Manifold* man = sc->pairBuf == 0 ? w.man0 : w.man1;
+    const m3real h = dt / (m3real)substeps;
+    const m3SoftDev soft = m3MakeSoft(sc->contactHertz, sc->contactDampingRatio, h);
+    const m3SoftDev staticSoft = m3MakeSoft(2.0f * sc->contactHertz, sc->contactDampingRatio, h);
+    const int32_t constraintCount = s.plan->constraintCount;
+    for (int32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < constraintCount;
+         slot += gridDim.x * blockDim.x)
+    {
+        m3ContactDev c;
+        m3PrepareContact(w, &c, s.conPairIndex[s.lists[slot]], keys, man, soft, staticSoft,
+                         s.bodyInvI);
+        m3WriteContactRow(s.rows, slot, c);
+        if (c.restitution != 0.0f)
+        {
+            atomicOr(&s.plan->anyRestitution, 1);
+        }
+        if (c.rollingResistance > 0.0f && (!c.dynA || !c.dynB))
+        {
+            atomicExch(&sc->status, M3GPU_ERR_UNSUPPORTED);
+            sc->statusDetail = 2001;
+        }
+    }
 }
 
 // A barrier that gave up marks the world failed (after the wide kernel,
@@ -3532,6 +3676,7 @@ static int32_t WideBlocks(const m3HostWorld* w)
 static void LaunchWideSubstep(const m3WorldView* views, const int32_t* order, float dt,
                               int32_t substeps, int32_t blocks)
 {
+    m3WideRowsKernel<<<4 * s_smCount, 256>>>(views, order, dt, substeps);
     void* args[] = {(void*)&views, (void*)&order, (void*)&dt, (void*)&substeps};
     cudaLaunchCooperativeKernel((const void*)m3WideSubstepKernel<256>, dim3(blocks), dim3(256),
                                 args, 0, 0);
@@ -3543,7 +3688,14 @@ static void LaunchSolve(const m3WorldView* views, const int32_t* order, int32_t 
                         const int32_t* classFirst = nullptr, const int32_t* classCache = nullptr,
                         int32_t wideBlocks = 0)
 {
-    if (classFirst == nullptr)
+    if (wideBlocks > 0)
+    {
+        // One world: the largest class's prepare kernel, rows left to the
+        // wide grid.
+        const int32_t bytes = classCache != nullptr ? classCache[0] : cacheBytes;
+        m3PrepareKernel<512, 1><<<1, 512, bytes>>>(views, order, count, dt, substeps, bytes, 1);
+    }
+    else if (classFirst == nullptr)
     {
         m3PrepareKernel<256, 2><<<count, 256, cacheBytes>>>(views, order, count, dt, substeps,
                                                             cacheBytes);
@@ -3955,8 +4107,22 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
                 cudaStreamWaitEvent(0, TreeEventFor(need), 0);
             }
         }
-        m3BroadKernel<M3_BLOCK, 2><<<count, M3_BLOCK>>>(s_batch.dviews, s_batch.dorder, count,
-                                                        M3_TREE_LAG);
+        if (wideBlocks > 0)
+        {
+            // One large world: its sweep over the whole grid between the
+            // head and the tail of its broadphase.
+            m3BroadKernel<512, 1, 1><<<1, 512>>>(s_batch.dviews, s_batch.dorder, count,
+                                                  M3_TREE_LAG);
+            m3WideSweepKernel<<<4 * s_smCount, 256>>>(s_batch.dviews, s_batch.dorder);
+            m3BroadKernel<512, 1, 2><<<1, 512>>>(s_batch.dviews, s_batch.dorder, count,
+                                                  M3_TREE_LAG);
+            s_launches += 2;
+        }
+        else
+        {
+            m3BroadKernel<M3_BLOCK, 2><<<count, M3_BLOCK>>>(s_batch.dviews, s_batch.dorder, count,
+                                                            M3_TREE_LAG);
+        }
         cudaEventRecord(ev[1]);
         if (anyTracked)
         {
