@@ -479,7 +479,8 @@ M3GPU_API int32_t m3gpu_world_stats(m3WorldId world, uint64_t* out);
  * reference's per-phase step profile, world.h:578-593).  `out` holds 16
  * values: islands, prepare, colour+movers, integrate velocities, warm
  * start, bias solve, integrate positions, relax, store, continuous,
- * sleep, bounds, sweep sort, pair count, pair fill, unused. */
+ * sleep, bounds, sweep sort, pair count, pair fill, and last the number
+ * of broadphase tree leaf moves replayed (a count, not cycles). */
 M3GPU_API int32_t m3gpu_world_phase_cycles(m3WorldId world, uint64_t* out);
 
 /* White-box readback for parity tests.  Each copies [0, maxIndex) (or

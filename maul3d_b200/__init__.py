@@ -277,11 +277,12 @@ def profile(world) -> dict[str, float]:
 
 PHASES = ("islands", "prepare", "colour+movers", "integrate_v", "warm_start", "bias_solve",
           "integrate_p", "relax", "store", "continuous", "sleep", "bounds", "sweep_sort",
-          "pair_count", "pair_fill")
+          "pair_count", "pair_fill", "tree_moves")
 
 
 def world_phase_cycles(world) -> np.ndarray:
-    """Device clock cycles the world's block spent per step phase (PHASES)."""
+    """Device clock cycles the world's block spent per step phase (PHASES;
+    the last entry counts the broadphase tree's leaf moves replayed)."""
     out = (C.c_uint64 * 16)()
     _check(lib.m3gpu_world_phase_cycles(world.id, out))
     return np.array(list(out), dtype=np.uint64)

@@ -50,6 +50,16 @@
 // Planes a world may hold (the broadphase enumerates their pairs
 // directly; more are refused).
 #define M3_MAX_PLANES 16
+// The wide kernels' grid: at most this many blocks, and the layout of the
+// wide prepare kernel's grid-shared words.
+#define M3_WIDE_MAX_BLOCKS 512
+#define M3_WW_FLAG 0        // 3 words: the colouring rounds' pending flags (round % 3)
+#define M3_WW_LEVELS 3      // joint levels
+#define M3_WW_CLEVELS 4     // contact levels
+#define M3_WW_FILL 8        // 17 words: colour sizes, then cursors
+#define M3_WW_PART 32       // M3_WIDE_MAX_BLOCKS + 1 words: the grid scan's block totals
+#define M3_WW_BLOCKCOLOR (M3_WW_PART + M3_WIDE_MAX_BLOCKS + 1)
+#define M3_WW_WORDS (M3_WW_BLOCKCOLOR + M3_WIDE_MAX_BLOCKS * (M3_GRAPH_COLORS + 1))
 // Colouring: the marker of a constraint not coloured yet, and the
 // parallel rounds before the serial finish.
 #define M3_COLOR_PENDING 0xFF
@@ -149,6 +159,7 @@ struct m3Scratch
     int32_t* targetList;   // the continuous phase's static targets, ascending
     int2* jointBodies;     // per joint row: its two bodies (the level walk's compact input)
     int32_t* broadState;   // 20 words: a wide world's broadphase between its kernels
+    int32_t* wideWork;     // the wide prepare kernel's grid-shared words (M3_WW_*)
 };
 
 static __host__ __device__ inline int64_t NextPow2(int64_t n)
@@ -227,6 +238,7 @@ static __host__ __device__ inline int64_t ScratchCarve(m3Scratch* s, uint8_t* ba
     M3_CARVE(targetList, int32_t, shapeCap)
     M3_CARVE(jointBodies, int2, jointCap)
     M3_CARVE(broadState, int32_t, 4 + M3_MAX_PLANES)
+    M3_CARVE(wideWork, int32_t, M3_WW_WORDS)
     M3_CARVE(treeMoveBox, m3Aabb, (int64_t)treeLag * shapeCap)
     M3_CARVE(treeMoveShape, int32_t, (int64_t)treeLag * shapeCap)
 #undef M3_CARVE
@@ -480,6 +492,9 @@ __global__ void __launch_bounds__(32)
     {
         return;
     }
+    // Observer only: leaf moves replayed, in the phase counters' spare
+    // slot (a count, not cycles).
+    sc->phase[15] += (uint64_t)moves;
     const m3TreeArrayStore store{w.treeNodes};
     const int32_t* shapes = s.treeMoveShape + (int64_t)slot * sc->shapeCap;
     const m3Aabb* boxes = s.treeMoveBox + (int64_t)slot * sc->shapeCap;
@@ -588,6 +603,13 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3BroadKernel(const m3WorldVie
             s.treeMoveCount[slot] = 0;
         }
         s_treeSlot = slot;
+        if (PART == 1)
+        {
+            // The wide kernels of this step start their grid barrier
+            // with no arrivals and no error.
+            s.gridBar[0] = 0;
+            s.gridBar[2] = 0;
+        }
         if (PART == 2 && s_status == 0)
         {
             s_planeCount = s.broadState[M3_BS_PLANES];
@@ -2459,6 +2481,711 @@ __device__ bool m3GridSync(uint32_t* bar, uint32_t blocks)
     return s_ok != 0;
 }
 
+// Exclusive prefix sum of a[0, n) over a cooperative grid: each block
+// scans its contiguous chunk, the chunks' totals (ww[M3_WW_PART..])
+// give each block its offset.  Every thread of the grid calls it;
+// returns the total, or -1 when a barrier gave up.
+template <int NT>
+__device__ int32_t GridExclusiveScan(int32_t* a, int32_t n, int32_t* ww, uint32_t* bar)
+{
+    __shared__ int32_t s_offset;
+    __shared__ int32_t s_total;
+    const int32_t blocks = (int32_t)gridDim.x;
+    const int32_t chunk = (n + blocks - 1) / blocks;
+    const int32_t lo = (int32_t)blockIdx.x * chunk < n ? (int32_t)blockIdx.x * chunk : n;
+    const int32_t hi = lo + chunk < n ? lo + chunk : n;
+    const int32_t t = BlockExclusiveScan<NT>(a + lo, hi - lo);
+    if (threadIdx.x == 0)
+    {
+        ww[M3_WW_PART + blockIdx.x] = t;
+    }
+    if (!m3GridSync(bar, (uint32_t)blocks))
+    {
+        return -1;
+    }
+    if (threadIdx.x == 0)
+    {
+        int32_t off = 0;
+        int32_t total = 0;
+        for (int32_t b = 0; b < blocks; ++b)
+        {
+            const int32_t v = ((volatile int32_t*)ww)[M3_WW_PART + b];
+            off += b < (int32_t)blockIdx.x ? v : 0;
+            total += v;
+        }
+        s_offset = off;
+        s_total = total;
+    }
+    __syncthreads();
+    for (int32_t i = lo + (int32_t)threadIdx.x; i < hi; i += NT)
+    {
+        a[i] += s_offset;
+    }
+    const int32_t total = s_total;
+    if (!m3GridSync(bar, (uint32_t)blocks))
+    {
+        return -1;
+    }
+    return total;
+}
+
+// The preparation of one wide world over a cooperative grid: the same
+// stages, in the same order and with the same arithmetic, as
+// m3PrepareKernel's (islands and wake, contact and joint selection, joint
+// rows and their levels, the greedy colouring in rounds, solve slots,
+// the joint/contact level schedule, movers), with grid barriers where the
+// per-world kernel has block barriers.  The walks that are serial there
+// (the joint levels, the colouring's finish after its rounds, the
+// overflow bucket's fill) are serial here too, on one thread.  The
+// contact rows are left to m3WideRowsKernel.
+template <int NT>
+__global__ void __launch_bounds__(NT, 2) m3WidePrepareKernel(const m3WorldView* views,
+                                                           const int32_t* order, float dt,
+                                                           int32_t substeps)
+{
+    const m3WorldView& w = views[order[0]];
+    m3WorldScalars* sc = w.sc;
+    if (sc->status != 0)
+    {
+        return;
+    }
+    m3Scratch s;
+    ScratchCarve(&s, w.scratch, sc->bodyCap, sc->shapeCap, sc->jointCap, sc->pairCap);
+    uint32_t* bar = s.gridBar;
+    int32_t* ww = s.wideWork;
+    volatile int32_t* vww = ww;
+    volatile int32_t* vstatus = &sc->status;
+    const uint32_t blocks = gridDim.x;
+    const int32_t tid = threadIdx.x;
+    const int32_t gtid = (int32_t)blockIdx.x * NT + tid;
+    const int32_t gstride = (int32_t)blocks * NT;
+    const bool lead = blockIdx.x == 0 && tid == 0;
+    long long t_phase = clock64();
+#define M3_WIDE_MARK(k)                                                                            \
+    if (lead)                                                                                      \
+    {                                                                                              \
+        long long now_ = clock64();                                                                \
+        sc->phase[k] += (uint64_t)(now_ - t_phase);                                                \
+        t_phase = now_;                                                                            \
+    }
+#define M3_GSYNC()                                                                                 \
+    if (!m3GridSync(bar, blocks))                                                                  \
+    {                                                                                              \
+        return;                                                                                    \
+    }
+    // The pair list and manifolds built by the collide kernels become
+    // the current ones.
+    if (lead)
+    {
+        sc->pairBuf = 1 - sc->pairBuf;
+        sc->pairCount = sc->newPairCount;
+    }
+    M3_GSYNC()
+    const int32_t bodyMax = sc->bodyMax;
+    const int32_t jointMax = sc->jointMax;
+    const int32_t pairCount = ((volatile int32_t*)&sc->pairCount)[0];
+    const int32_t pairBuf = ((volatile int32_t*)&sc->pairBuf)[0];
+    const uint64_t* keys = pairBuf == 0 ? w.keys0 : w.keys1;
+    m3Manifold* man = pairBuf == 0 ? w.man0 : w.man1;
+
+    // Begin-of-step centres and rotations (solver.c:3866-3877); island
+    // arrays reset; the rows' world inverse inertia.
+    for (int32_t i = gtid; i < bodyMax; i += gstride)
+    {
+        s.parent[i] = i;
+        s.forced[i] = 0;
+        s.forcedRoot[i] = 0;
+        if (w.bodyAlive[i] == 0)
+        {
+            s.bodyInvI[i] = m3ZeroMat3();
+            continue;
+        }
+        const m3Transform xf = w.xf[i];
+        m3Vec3 rlc = m3RotateVec3(xf.q, w.lc[i]);
+        m3Pos3 c;
+        c.x = xf.p.x + (double)rlc.x;
+        c.y = xf.p.y + (double)rlc.y;
+        c.z = xf.p.z + (double)rlc.z;
+        s.com0[i] = c;
+        s.rot0[i] = xf.q;
+        s.bodyInvI[i] = m3WorldInvInertiaDev(w, i);
+    }
+    M3_GSYNC()
+    // Island wake pass (solver.c:3468-3578).
+    for (int32_t k = gtid; k < pairCount; k += gstride)
+    {
+        if (man[k].pointCount == 0)
+        {
+            continue;
+        }
+        const uint64_t key = keys[k];
+        const int32_t shapeA = (int32_t)(key >> 32);
+        const int32_t shapeB = (int32_t)(key & 0xFFFFFFFFu);
+        if (w.sensor[shapeA] != 0 || w.sensor[shapeB] != 0)
+        {
+            continue;
+        }
+        MarkKinematicContact(w, s, w.shapeBody[shapeA], w.shapeBody[shapeB]);
+    }
+    for (int32_t j = gtid; j < jointMax; j += gstride)
+    {
+        if (w.jointAlive[j] != 0)
+        {
+            MarkKinematicContact(w, s, w.jbodyA[j], w.jbodyB[j]);
+        }
+    }
+    M3_GSYNC()
+    for (int32_t i = gtid; i < bodyMax; i += gstride)
+    {
+        if (w.bodyAlive[i] == 0 || w.btype[i] != M3_BODY_DYNAMIC)
+        {
+            continue;
+        }
+        if (w.awake[i] != 0 || s.forced[i] != 0)
+        {
+            s.forcedRoot[IslandFind(s.parent, i)] = 1;
+        }
+    }
+    M3_GSYNC()
+    for (int32_t i = gtid; i < bodyMax; i += gstride)
+    {
+        s.deltaPos[i] = v3(0.0f, 0.0f, 0.0f);
+        s.deltaRot[i] = m3IdentityQuat();
+        if (w.bodyAlive[i] == 0 || w.btype[i] != M3_BODY_DYNAMIC)
+        {
+            continue;
+        }
+        if (w.awake[i] == 0 && s.forcedRoot[IslandFind(s.parent, i)] != 0)
+        {
+            w.awake[i] = 1;
+            w.sleepTime[i] = 0.0f;
+        }
+    }
+    M3_GSYNC()
+    M3_WIDE_MARK(M3_PHASE_ISLANDS)
+
+    // Contact selection (solver.c:156-405).
+    const m3real h = dt / (m3real)substeps;
+    for (int32_t k = gtid; k < pairCount; k += gstride)
+    {
+        int32_t flag = 0;
+        if (man[k].pointCount != 0)
+        {
+            const uint64_t key = keys[k];
+            const int32_t shapeA = (int32_t)(key >> 32);
+            const int32_t shapeB = (int32_t)(key & 0xFFFFFFFFu);
+            const int32_t bodyA = w.shapeBody[shapeA];
+            const int32_t bodyB = w.shapeBody[shapeB];
+            const int awakeDynA = w.btype[bodyA] == M3_BODY_DYNAMIC && w.awake[bodyA] != 0;
+            const int awakeDynB = w.btype[bodyB] == M3_BODY_DYNAMIC && w.awake[bodyB] != 0;
+            if ((awakeDynA || awakeDynB) && w.sensor[shapeA] == 0 && w.sensor[shapeB] == 0)
+            {
+                flag = 1;
+            }
+        }
+        s.pairFlag[k] = flag;
+    }
+    // Joint selection in slot order.
+    for (int32_t j = gtid; j < jointMax; j += gstride)
+    {
+        int32_t flag = 0;
+        if (w.jointAlive[j] != 0)
+        {
+            const int32_t refusal = m3JointRefusal(w, j);
+            if (refusal != 0)
+            {
+                atomicExch(&sc->status, M3GPU_ERR_UNSUPPORTED);
+                sc->statusDetail = refusal;
+            }
+            else if (m3JointActive(w, j))
+            {
+                flag = 1;
+            }
+        }
+        s.jointFlag[j] = flag;
+    }
+    M3_GSYNC()
+    const int32_t constraintCount = GridExclusiveScan<NT>(s.pairFlag, pairCount, ww, bar);
+    if (constraintCount < 0)
+    {
+        return;
+    }
+    const int32_t jointCount = GridExclusiveScan<NT>(s.jointFlag, jointMax, ww, bar);
+    if (jointCount < 0 || *vstatus != 0)
+    {
+        return;
+    }
+    for (int32_t k = gtid; k < pairCount; k += gstride)
+    {
+        const int32_t next = k + 1 < pairCount ? s.pairFlag[k + 1] : constraintCount;
+        if (next != s.pairFlag[k])
+        {
+            s.conPairIndex[s.pairFlag[k]] = k;
+        }
+    }
+    // Joint rows (solver.c:699-1042), then their dependency levels.
+    for (int32_t j = gtid; j < jointMax; j += gstride)
+    {
+        const int32_t next = j + 1 < jointMax ? s.jointFlag[j + 1] : jointCount;
+        if (next != s.jointFlag[j])
+        {
+            const int32_t r = s.jointFlag[j];
+            m3PrepareJoint(w, &s.joints[r], j, h);
+            s.jointBodies[r] = make_int2(s.joints[r].bodyA, s.joints[r].bodyB);
+        }
+    }
+    for (int32_t i = gtid; i < bodyMax; i += gstride)
+    {
+        s.ready[i] = -1;
+    }
+    M3_GSYNC()
+    if (lead)
+    {
+        int32_t levels = 0;
+        for (int32_t r = 0; r < jointCount; ++r)
+        {
+            const int2 ab = s.jointBodies[r];
+            const int32_t la = s.ready[ab.x];
+            const int32_t lb = s.ready[ab.y];
+            const int32_t level = 1 + (la > lb ? la : lb);
+            s.ready[ab.x] = level;
+            s.ready[ab.y] = level;
+            s.jointLevel[r] = level;
+            levels = level + 1 > levels ? level + 1 : levels;
+        }
+        ww[M3_WW_LEVELS] = levels;
+        sc->jointConstraintCount = jointCount;
+    }
+    M3_GSYNC()
+    const int32_t jointLevels = vww[M3_WW_LEVELS];
+    for (int32_t k = gtid; k <= jointLevels; k += gstride)
+    {
+        s.jointLevelStart[k] = 0;
+    }
+    M3_GSYNC()
+    for (int32_t r = gtid; r < jointCount; r += gstride)
+    {
+        atomicAdd(&s.jointLevelStart[s.jointLevel[r] + 1], 1);
+    }
+    M3_GSYNC()
+    if (lead)
+    {
+        for (int32_t k = 0; k < jointLevels; ++k)
+        {
+            s.jointLevelStart[k + 1] += s.jointLevelStart[k];
+        }
+    }
+    M3_GSYNC()
+    for (int32_t k = gtid; k <= jointLevels; k += gstride)
+    {
+        s.levelFill[k] = s.jointLevelStart[k];
+    }
+    M3_GSYNC()
+    for (int32_t r = gtid; r < jointCount; r += gstride)
+    {
+        s.jointOrder[atomicAdd(&s.levelFill[s.jointLevel[r]], 1)] = r;
+    }
+    M3_GSYNC()
+    M3_WIDE_MARK(M3_PHASE_PREPARE)
+
+    // Greedy 16-colour first-free-bit colouring in constraint order, the
+    // overflow bucket last (solver.c:2750-2810), in rounds: each round
+    // colours every uncoloured constraint that is the earliest
+    // uncoloured one on each of its awake dynamic bodies (exactly the
+    // masks the serial walk sees); after M3_COLOR_ROUNDS rounds one
+    // thread finishes the rest in order.
+    uint32_t* cMask = s.bodyMask;
+    int32_t* cMin0 = s.colorMin;
+    int32_t* cMin1 = s.colorMin + sc->bodyCap;
+    int2* cPair = s.conPair;
+    uint8_t* cColor = s.colors;
+    for (int32_t i = gtid; i < bodyMax; i += gstride)
+    {
+        cMask[i] = 0u;
+        cMin0[i] = INT32_MAX;
+        cMin1[i] = INT32_MAX;
+    }
+    for (int32_t i = gtid; i < constraintCount; i += gstride)
+    {
+        const uint64_t key = keys[s.conPairIndex[i]];
+        const int32_t bodyA = w.shapeBody[(int32_t)(key >> 32)];
+        const int32_t bodyB = w.shapeBody[(int32_t)(key & 0xFFFFFFFFu)];
+        const int32_t a = w.btype[bodyA] == M3_BODY_DYNAMIC && w.awake[bodyA] ? bodyA : -1;
+        const int32_t b = w.btype[bodyB] == M3_BODY_DYNAMIC && w.awake[bodyB] ? bodyB : -1;
+        cPair[i] = make_int2(a, b);
+        cColor[i] = M3_COLOR_PENDING;
+    }
+    if (lead)
+    {
+        ww[M3_WW_FLAG] = 0;
+        ww[M3_WW_FLAG + 1] = 0;
+        ww[M3_WW_FLAG + 2] = 0;
+    }
+    M3_GSYNC()
+    // Round r raises flag r % 3 and every block reads it after the round's
+    // last barrier; it is cleared again at the start of round r + 2, after
+    // two more barriers, when no block can still be reading it.
+    bool pendingLeft = constraintCount > 0;
+    for (int32_t round = 0; pendingLeft && round < M3_COLOR_ROUNDS; ++round)
+    {
+        int32_t* cur = (round & 1) ? cMin1 : cMin0;
+        int32_t* nxt = (round & 1) ? cMin0 : cMin1;
+        if (lead)
+        {
+            ww[M3_WW_FLAG + (round + 1) % 3] = 0; // the next round's flag
+        }
+        for (int32_t i = gtid; i < constraintCount; i += gstride)
+        {
+            if (cColor[i] == M3_COLOR_PENDING)
+            {
+                const int2 p = cPair[i];
+                if (p.x >= 0)
+                {
+                    atomicMin(&cur[p.x], i);
+                }
+                if (p.y >= 0)
+                {
+                    atomicMin(&cur[p.y], i);
+                }
+            }
+        }
+        M3_GSYNC()
+        bool waiting = false;
+        for (int32_t i = gtid; i < constraintCount; i += gstride)
+        {
+            if (cColor[i] != M3_COLOR_PENDING)
+            {
+                continue;
+            }
+            const int2 p = cPair[i];
+            const bool ready = (p.x < 0 || cur[p.x] == i) && (p.y < 0 || cur[p.y] == i);
+            if (p.x >= 0)
+            {
+                nxt[p.x] = INT32_MAX;
+            }
+            if (p.y >= 0)
+            {
+                nxt[p.y] = INT32_MAX;
+            }
+            if (!ready)
+            {
+                waiting = true;
+                continue;
+            }
+            const uint32_t mask = (p.x >= 0 ? cMask[p.x] : 0u) | (p.y >= 0 ? cMask[p.y] : 0u);
+            int32_t color = __ffs((int)~mask) - 1;
+            color = color < M3_GRAPH_COLORS ? color : M3_GRAPH_COLORS;
+            cColor[i] = (uint8_t)color;
+            if (color < M3_GRAPH_COLORS)
+            {
+                const uint32_t bit = 1u << color;
+                if (p.x >= 0)
+                {
+                    cMask[p.x] |= bit;
+                }
+                if (p.y >= 0)
+                {
+                    cMask[p.y] |= bit;
+                }
+            }
+        }
+        if (waiting)
+        {
+            ww[M3_WW_FLAG + round % 3] = 1;
+        }
+        M3_GSYNC()
+        pendingLeft = vww[M3_WW_FLAG + round % 3] != 0;
+    }
+    if (pendingLeft)
+    {
+        if (lead)
+        {
+            for (int32_t i = 0; i < constraintCount; ++i)
+            {
+                if (cColor[i] != M3_COLOR_PENDING)
+                {
+                    continue;
+                }
+                const int2 p = cPair[i];
+                const uint32_t mask =
+                    (p.x >= 0 ? cMask[p.x] : 0u) | (p.y >= 0 ? cMask[p.y] : 0u);
+                int32_t color = __ffs((int)~mask) - 1;
+                color = color < M3_GRAPH_COLORS ? color : M3_GRAPH_COLORS;
+                cColor[i] = (uint8_t)color;
+                if (color < M3_GRAPH_COLORS)
+                {
+                    const uint32_t bit = 1u << color;
+                    if (p.x >= 0)
+                    {
+                        cMask[p.x] |= bit;
+                    }
+                    if (p.y >= 0)
+                    {
+                        cMask[p.y] |= bit;
+                    }
+                }
+            }
+        }
+        M3_GSYNC()
+    }
+    // Slots: colour by colour, constraint order inside a colour (a stable
+    // counting sort).  Each block owns a contiguous range of constraints:
+    // its count per colour, then its first slot per colour, then its
+    // slots in order, chunk by chunk.
+    __shared__ int32_t s_colorFill[M3_GRAPH_COLORS + 1];
+    __shared__ int32_t s_warpColor[NT / 32][M3_GRAPH_COLORS + 1];
+    const int32_t chunk = (constraintCount + (int32_t)blocks - 1) / (int32_t)blocks;
+    const int32_t cLo = (int32_t)blockIdx.x * chunk < constraintCount ? (int32_t)blockIdx.x * chunk
+                                                                      : constraintCount;
+    const int32_t cHi = cLo + chunk < constraintCount ? cLo + chunk : constraintCount;
+    if (tid <= M3_GRAPH_COLORS)
+    {
+        s_colorFill[tid] = 0;
+    }
+    __syncthreads();
+    for (int32_t i = cLo + tid; i < cHi; i += NT)
+    {
+        atomicAdd(&s_colorFill[cColor[i]], 1);
+    }
+    __syncthreads();
+    if (tid <= M3_GRAPH_COLORS)
+    {
+        ww[M3_WW_BLOCKCOLOR + blockIdx.x * (M3_GRAPH_COLORS + 1) + tid] = s_colorFill[tid];
+    }
+    M3_GSYNC()
+    if (lead)
+    {
+        // Colour offsets, then each block's first slot per colour.
+        int32_t cursor = 0;
+        int32_t used = 0;
+        for (int32_t c = 0; c <= M3_GRAPH_COLORS; ++c)
+        {
+            int32_t n = 0;
+            for (uint32_t b = 0; b < blocks; ++b)
+            {
+                int32_t* cell = &ww[M3_WW_BLOCKCOLOR + b * (M3_GRAPH_COLORS + 1) + c];
+                const int32_t v = *cell;
+                *cell = cursor + n;
+                n += v;
+            }
+            s.plan->starts[c] = cursor;
+            cursor += n;
+            used += n > 0 ? 1 : 0;
+        }
+        s.plan->starts[M3_GRAPH_COLORS + 1] = cursor;
+        sc->lastColorCount = used;
+        sc->constraintCount = constraintCount;
+    }
+    M3_GSYNC()
+    if (tid <= M3_GRAPH_COLORS)
+    {
+        s_colorFill[tid] = vww[M3_WW_BLOCKCOLOR + blockIdx.x * (M3_GRAPH_COLORS + 1) + tid];
+    }
+    __syncthreads();
+    {
+        const int32_t lane = tid & 31;
+        const int32_t warp = tid >> 5;
+        const uint32_t ltMask = (1u << lane) - 1u;
+        for (int32_t c0 = cLo; c0 < cHi; c0 += NT)
+        {
+            const int32_t i = c0 + tid;
+            const int32_t color = i < cHi ? (int32_t)cColor[i] : M3_GRAPH_COLORS + 1;
+            for (int32_t k = tid; k < (NT / 32) * (M3_GRAPH_COLORS + 1); k += NT)
+            {
+                (&s_warpColor[0][0])[k] = 0;
+            }
+            __syncthreads();
+            const uint32_t peers = __match_any_sync(0xFFFFFFFFu, color);
+            const int32_t rank = __popc(peers & ltMask);
+            if (rank == 0 && color <= M3_GRAPH_COLORS)
+            {
+                s_warpColor[warp][color] = __popc(peers);
+            }
+            __syncthreads();
+            if (color <= M3_GRAPH_COLORS)
+            {
+                int32_t slot = s_colorFill[color] + rank;
+                for (int32_t k = 0; k < warp; ++k)
+                {
+                    slot += s_warpColor[k][color];
+                }
+                s.lists[slot] = i;
+                s.conSlot[i] = slot;
+            }
+            __syncthreads();
+            if (tid <= M3_GRAPH_COLORS)
+            {
+                int32_t add = 0;
+                for (int32_t k = 0; k < NT / 32; ++k)
+                {
+                    add += s_warpColor[k][tid];
+                }
+                s_colorFill[tid] += add;
+            }
+            __syncthreads();
+        }
+    }
+    // The joint/contact schedule: a contact's level is at least one past
+    // the last joint level on either of its awake dynamic bodies and one
+    // past the level of the previous contact (colour order) on either of
+    // them; the overflow colour stays last and serial.
+    int32_t* cLast = cMin0;
+    for (int32_t i = gtid; i < bodyMax; i += gstride)
+    {
+        cLast[i] = jointCount > 0 ? s.ready[i] + 1 : 0;
+    }
+    if (lead)
+    {
+        ww[M3_WW_CLEVELS] = 0;
+    }
+    M3_GSYNC()
+    for (int32_t color = 0; color < M3_GRAPH_COLORS; ++color)
+    {
+        const int32_t k0 = s.plan->starts[color];
+        const int32_t k1 = s.plan->starts[color + 1];
+        for (int32_t k = k0 + gtid; k < k1; k += gstride)
+        {
+            const int32_t i = s.lists[k];
+            const int2 p = cPair[i];
+            int32_t level = 0;
+            if (p.x >= 0)
+            {
+                level = cLast[p.x] > level ? cLast[p.x] : level;
+            }
+            if (p.y >= 0)
+            {
+                level = cLast[p.y] > level ? cLast[p.y] : level;
+            }
+            s.conLevel[i] = level;
+            if (p.x >= 0)
+            {
+                cLast[p.x] = level + 1;
+            }
+            if (p.y >= 0)
+            {
+                cLast[p.y] = level + 1;
+            }
+            atomicMax(&ww[M3_WW_CLEVELS], level + 1);
+        }
+        if (k1 > k0)
+        {
+            M3_GSYNC()
+        }
+    }
+    const int32_t contactLevels = vww[M3_WW_CLEVELS];
+    const int32_t levels = contactLevels > jointLevels ? contactLevels : jointLevels;
+    for (int32_t k = gtid; k <= levels + 1; k += gstride)
+    {
+        s.levelStart[k] = 0;
+    }
+    M3_GSYNC()
+    for (int32_t i = gtid; i < constraintCount; i += gstride)
+    {
+        const int32_t level = cColor[i] == M3_GRAPH_COLORS ? levels : s.conLevel[i];
+        s.conLevel[i] = level;
+        atomicAdd(&s.levelStart[level + 1], 1);
+    }
+    M3_GSYNC()
+    if (lead)
+    {
+        for (int32_t k = 0; k <= levels; ++k)
+        {
+            s.levelStart[k + 1] += s.levelStart[k];
+        }
+    }
+    M3_GSYNC()
+    for (int32_t k = gtid; k <= levels; k += gstride)
+    {
+        s.levelFill[k] = s.levelStart[k];
+    }
+    M3_GSYNC()
+    for (int32_t i = gtid; i < constraintCount; i += gstride)
+    {
+        const int32_t level = s.conLevel[i];
+        if (level < levels)
+        {
+            const int32_t slot = atomicAdd(&s.levelFill[level], 1);
+            s.lists[slot] = i;
+            s.conSlot[i] = slot;
+        }
+    }
+    if (lead && s.levelStart[levels + 1] > s.levelStart[levels])
+    {
+        // The overflow bucket keeps constraint order (it runs serially).
+        int32_t slot = s.levelStart[levels];
+        for (int32_t i = 0; i < constraintCount; ++i)
+        {
+            if (s.conLevel[i] == levels)
+            {
+                s.lists[slot] = i;
+                s.conSlot[i] = slot;
+                slot += 1;
+            }
+        }
+    }
+    M3_GSYNC()
+    M3_WIDE_MARK(M3_PHASE_COLOR)
+
+    // Movers: alive, enabled, kinematic or awake dynamic, ascending
+    // (solver.c:3945-3983), with the kinematic servo.
+    for (int32_t i = gtid; i < bodyMax; i += gstride)
+    {
+        int32_t flag = 0;
+        if (w.bodyAlive[i] != 0 && w.enabled[i] != 0)
+        {
+            const uint8_t type = w.btype[i];
+            if (type == M3_BODY_KINEMATIC || (type == M3_BODY_DYNAMIC && w.awake[i] != 0))
+            {
+                flag = 1;
+            }
+            if (type == M3_BODY_KINEMATIC && w.hasTarget[i] != 0)
+            {
+                m3real servoInvDt = 1.0f / dt;
+                const m3Transform now = w.xf[i];
+                const m3Transform want = w.target[i];
+                w.v[i] = v3((m3real)(want.p.x - now.p.x) * servoInvDt,
+                            (m3real)(want.p.y - now.p.y) * servoInvDt,
+                            (m3real)(want.p.z - now.p.z) * servoInvDt);
+                m3Quat dq = m3MulQuat(want.q, q4(-now.q.x, -now.q.y, -now.q.z, now.q.w));
+                if (dq.w < 0.0f)
+                {
+                    dq = q4(-dq.x, -dq.y, -dq.z, -dq.w);
+                }
+                w.w[i] = m3MulSV3(2.0f * servoInvDt, v3(dq.x, dq.y, dq.z));
+                w.hasTarget[i] = 0;
+            }
+        }
+        s.moverFlag[i] = flag;
+    }
+    M3_GSYNC()
+    const int32_t moverCount = GridExclusiveScan<NT>(s.moverFlag, bodyMax, ww, bar);
+    if (moverCount < 0)
+    {
+        return;
+    }
+    for (int32_t i = gtid; i < bodyMax; i += gstride)
+    {
+        const int32_t next = i + 1 < bodyMax ? s.moverFlag[i + 1] : moverCount;
+        if (next != s.moverFlag[i])
+        {
+            s.movers[s.moverFlag[i]] = i;
+        }
+    }
+    if (lead)
+    {
+        m3StepPlan* plan = s.plan;
+        plan->constraintCount = constraintCount;
+        plan->jointCount = jointCount;
+        plan->jointLevels = jointLevels;
+        plan->moverCount = moverCount;
+        plan->anyRestitution = 0; // the rows kernel raises it
+        plan->levels = levels;
+    }
+    M3_WIDE_MARK(M3_PHASE_COLOR)
+#undef M3_GSYNC
+#undef M3_WIDE_MARK
+}
+
 template <int NT>
 __global__ void __launch_bounds__(NT, 2) m3WideSubstepKernel(const m3WorldView* views,
                                                            const int32_t* order, float dt,
@@ -3654,7 +4381,11 @@ static int32_t WideBlocks(const m3HostWorld* w)
         cudaGetDevice(&device);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
         s_smCount = sms;
+        int perSmPrepare = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, m3WideSubstepKernel<256>, 256, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSmPrepare, m3WidePrepareKernel<256>, 256,
+                                                      0);
+        perSm = perSm < perSmPrepare ? perSm : perSmPrepare;
         maxResident = sms * perSm;
         if (maxResident <= 0)
         {
@@ -3670,6 +4401,7 @@ static int32_t WideBlocks(const m3HostWorld* w)
     int32_t blocks = shapes / 512;
     blocks = blocks < 8 ? 8 : blocks;
     blocks = blocks < s_smCount ? blocks : s_smCount;
+    blocks = blocks < M3_WIDE_MAX_BLOCKS ? blocks : M3_WIDE_MAX_BLOCKS;
     return blocks < maxResident ? blocks : maxResident;
 }
 
@@ -3690,10 +4422,11 @@ static void LaunchSolve(const m3WorldView* views, const int32_t* order, int32_t 
 {
     if (wideBlocks > 0)
     {
-        // One world: the largest class's prepare kernel, rows left to the
-        // wide grid.
-        const int32_t bytes = classCache != nullptr ? classCache[0] : cacheBytes;
-        m3PrepareKernel<512, 1><<<1, 512, bytes>>>(views, order, count, dt, substeps, bytes, 1);
+        // One world: its preparation over the whole grid, then its rows.
+        void* args[] = {(void*)&views, (void*)&order, (void*)&dt, (void*)&substeps};
+        cudaLaunchCooperativeKernel((const void*)m3WidePrepareKernel<256>, dim3(wideBlocks),
+                                    dim3(256), args, 0, 0);
+        m3WideStatusKernel<<<1, 1>>>(views, order);
     }
     else if (classFirst == nullptr)
     {
