@@ -56,14 +56,19 @@
 #define M3_WW_FLAG 0        // 3 words: the colouring rounds' pending flags (round % 3)
 #define M3_WW_LEVELS 3      // joint levels
 #define M3_WW_CLEVELS 4     // contact levels
-#define M3_WW_FILL 8        // 17 words: colour sizes, then cursors
+#define M3_WW_JFLAG 5       // 3 words: the joint-level rounds' change flags (round % 3)
+#define M3_WW_BROKEN 8      // broken joints this step
 #define M3_WW_PART 32       // M3_WIDE_MAX_BLOCKS + 1 words: the grid scan's block totals
 #define M3_WW_BLOCKCOLOR (M3_WW_PART + M3_WIDE_MAX_BLOCKS + 1)
 #define M3_WW_WORDS (M3_WW_BLOCKCOLOR + M3_WIDE_MAX_BLOCKS * (M3_GRAPH_COLORS + 1))
 // Colouring: the marker of a constraint not coloured yet, and the
-// parallel rounds before the serial finish.
+// parallel rounds before the serial finish (one block per world; a wide
+// world's grid affords many more rounds).
 #define M3_COLOR_PENDING 0xFF
 #define M3_COLOR_ROUNDS 64
+#define M3_WIDE_COLOR_ROUNDS 4096
+// Rounds of the wide joint-level relaxation before the serial walk.
+#define M3_WIDE_JOINT_ROUNDS 4096
 
 // Step phases timed with the SM clock by thread 0 of each world's block
 // right after the barrier that closes the phase.
@@ -160,6 +165,8 @@ struct m3Scratch
     int2* jointBodies;     // per joint row: its two bodies (the level walk's compact input)
     int32_t* broadState;   // 20 words: a wide world's broadphase between its kernels
     int32_t* wideWork;     // the wide prepare kernel's grid-shared words (M3_WW_*)
+    int32_t* jointAdj;     // 2 per joint row: rows by body (the wide joint levels)
+    int2* jointPrev;       // per joint row: the previous row on each of its bodies
 };
 
 static __host__ __device__ inline int64_t NextPow2(int64_t n)
@@ -239,6 +246,8 @@ static __host__ __device__ inline int64_t ScratchCarve(m3Scratch* s, uint8_t* ba
     M3_CARVE(jointBodies, int2, jointCap)
     M3_CARVE(broadState, int32_t, 4 + M3_MAX_PLANES)
     M3_CARVE(wideWork, int32_t, M3_WW_WORDS)
+    M3_CARVE(jointAdj, int32_t, 2 * (int64_t)jointCap)
+    M3_CARVE(jointPrev, int2, jointCap)
     M3_CARVE(treeMoveBox, m3Aabb, (int64_t)treeLag * shapeCap)
     M3_CARVE(treeMoveShape, int32_t, (int64_t)treeLag * shapeCap)
 #undef M3_CARVE
@@ -2734,27 +2743,134 @@ __global__ void __launch_bounds__(NT, 2) m3WidePrepareKernel(const m3WorldView* 
             s.jointBodies[r] = make_int2(s.joints[r].bodyA, s.joints[r].bodyB);
         }
     }
+    // Joint levels: a row's level is one past the latest earlier row on
+    // either of its bodies (the serial walk's rule).  Each row finds that
+    // previous row on each body from the body's rows, then every row
+    // relaxes level = 1 + max(previous levels) until nothing changes;
+    // a row's value is exact once its whole chain of previous rows is,
+    // so the rounds needed are the longest chain.  Past the round cap the
+    // serial walk decides (same result).
+    int32_t* adjCount = s.colorMin;                 // per body, then offsets
+    int32_t* adjFill = s.colorMin + sc->bodyCap;    // per body: fill cursors
     for (int32_t i = gtid; i < bodyMax; i += gstride)
     {
+        adjCount[i] = 0;
         s.ready[i] = -1;
     }
+    if (lead)
+    {
+        ww[M3_WW_JFLAG] = 0;
+        ww[M3_WW_JFLAG + 1] = 0;
+        ww[M3_WW_JFLAG + 2] = 0;
+    }
     M3_GSYNC()
+    for (int32_t r = gtid; r < jointCount; r += gstride)
+    {
+        const int2 ab = s.jointBodies[r];
+        atomicAdd(&adjCount[ab.x], 1);
+        if (ab.y != ab.x)
+        {
+            atomicAdd(&adjCount[ab.y], 1);
+        }
+    }
+    M3_GSYNC()
+    if (GridExclusiveScan<NT>(adjCount, bodyMax, ww, bar) < 0)
+    {
+        return;
+    }
+    for (int32_t i = gtid; i < bodyMax; i += gstride)
+    {
+        adjFill[i] = adjCount[i];
+    }
+    M3_GSYNC()
+    for (int32_t r = gtid; r < jointCount; r += gstride)
+    {
+        const int2 ab = s.jointBodies[r];
+        s.jointAdj[atomicAdd(&adjFill[ab.x], 1)] = r;
+        if (ab.y != ab.x)
+        {
+            s.jointAdj[atomicAdd(&adjFill[ab.y], 1)] = r;
+        }
+    }
+    M3_GSYNC()
+    for (int32_t r = gtid; r < jointCount; r += gstride)
+    {
+        const int2 ab = s.jointBodies[r];
+        int32_t pa = -1;
+        for (int32_t k = adjCount[ab.x]; k < adjFill[ab.x]; ++k)
+        {
+            const int32_t o = s.jointAdj[k];
+            pa = o < r && o > pa ? o : pa;
+        }
+        int32_t pb = -1;
+        for (int32_t k = adjCount[ab.y]; k < adjFill[ab.y]; ++k)
+        {
+            const int32_t o = s.jointAdj[k];
+            pb = o < r && o > pb ? o : pb;
+        }
+        s.jointPrev[r] = make_int2(pa, pb);
+        s.jointLevel[r] = 0;
+    }
+    M3_GSYNC()
+    bool changed = jointCount > 0;
+    int32_t jround = 0;
+    for (; changed && jround < M3_WIDE_JOINT_ROUNDS; ++jround)
+    {
+        if (lead)
+        {
+            ww[M3_WW_JFLAG + (jround + 1) % 3] = 0;
+        }
+        bool mine = false;
+        for (int32_t r = gtid; r < jointCount; r += gstride)
+        {
+            const int2 pr = s.jointPrev[r];
+            const int32_t la = pr.x >= 0 ? ((volatile int32_t*)s.jointLevel)[pr.x] : -1;
+            const int32_t lb = pr.y >= 0 ? ((volatile int32_t*)s.jointLevel)[pr.y] : -1;
+            const int32_t level = 1 + (la > lb ? la : lb);
+            if (level != s.jointLevel[r])
+            {
+                s.jointLevel[r] = level;
+                mine = true;
+            }
+        }
+        if (mine)
+        {
+            ww[M3_WW_JFLAG + jround % 3] = 1;
+        }
+        M3_GSYNC()
+        changed = vww[M3_WW_JFLAG + jround % 3] != 0;
+    }
     if (lead)
     {
         int32_t levels = 0;
-        for (int32_t r = 0; r < jointCount; ++r)
+        if (changed)
         {
-            const int2 ab = s.jointBodies[r];
-            const int32_t la = s.ready[ab.x];
-            const int32_t lb = s.ready[ab.y];
-            const int32_t level = 1 + (la > lb ? la : lb);
-            s.ready[ab.x] = level;
-            s.ready[ab.y] = level;
-            s.jointLevel[r] = level;
-            levels = level + 1 > levels ? level + 1 : levels;
+            // Chains longer than the round cap: the serial walk.
+            for (int32_t r = 0; r < jointCount; ++r)
+            {
+                const int2 ab = s.jointBodies[r];
+                const int32_t la = s.ready[ab.x];
+                const int32_t lb = s.ready[ab.y];
+                const int32_t level = 1 + (la > lb ? la : lb);
+                s.ready[ab.x] = level;
+                s.ready[ab.y] = level;
+                s.jointLevel[r] = level;
+            }
         }
-        ww[M3_WW_LEVELS] = levels;
+        ww[M3_WW_LEVELS] = 0;
         sc->jointConstraintCount = jointCount;
+        (void)levels;
+    }
+    M3_GSYNC()
+    // The levels' count, and each body's last joint level (its latest
+    // row's: levels grow along a body's rows).
+    for (int32_t r = gtid; r < jointCount; r += gstride)
+    {
+        const int32_t level = s.jointLevel[r];
+        atomicMax(&ww[M3_WW_LEVELS], level + 1);
+        const int2 ab = s.jointBodies[r];
+        atomicMax(&s.ready[ab.x], level);
+        atomicMax(&s.ready[ab.y], level);
     }
     M3_GSYNC()
     const int32_t jointLevels = vww[M3_WW_LEVELS];
@@ -2826,7 +2942,7 @@ __global__ void __launch_bounds__(NT, 2) m3WidePrepareKernel(const m3WorldView* 
     // last barrier; it is cleared again at the start of round r + 2, after
     // two more barriers, when no block can still be reading it.
     bool pendingLeft = constraintCount > 0;
-    for (int32_t round = 0; pendingLeft && round < M3_COLOR_ROUNDS; ++round)
+    for (int32_t round = 0; pendingLeft && round < M3_WIDE_COLOR_ROUNDS; ++round)
     {
         int32_t* cur = (round & 1) ? cMin1 : cMin0;
         int32_t* nxt = (round & 1) ? cMin0 : cMin1;
@@ -3377,12 +3493,31 @@ __global__ void __launch_bounds__(NT, 2) m3WideSubstepKernel(const m3WorldView* 
     {
         return;
     }
-    // Breakage: each joint's test alone over the grid, the destruction of
-    // the broken ones in ascending order on one thread.
+    // Breakage: each joint's test alone over the grid, the broken ones
+    // listed in ascending order (a grid scan of the flags), then destroyed
+    // in that order on one thread.
     const int32_t jointMax = sc->jointMax;
     for (int32_t j = gtid; j < jointMax; j += gstride)
     {
         s.jointFlag[j] = m3JointBreaksDev(w, j, invH) ? 1 : 0;
+    }
+    if (!m3GridSync(bar, blocks))
+    {
+        return;
+    }
+    int32_t* ww = s.wideWork;
+    const int32_t brokenCount = GridExclusiveScan<NT>(s.jointFlag, jointMax, ww, bar);
+    if (brokenCount < 0)
+    {
+        return;
+    }
+    for (int32_t j = gtid; j < jointMax; j += gstride)
+    {
+        const int32_t next = j + 1 < jointMax ? s.jointFlag[j + 1] : brokenCount;
+        if (next != s.jointFlag[j])
+        {
+            s.jointOrder[s.jointFlag[j]] = j;
+        }
     }
     if (!m3GridSync(bar, blocks))
     {
@@ -3401,12 +3536,9 @@ __global__ void __launch_bounds__(NT, 2) m3WideSubstepKernel(const m3WorldView* 
                     2.0f * M3_PI * (m3real)(int32_t)(sc->windPhase / (2.0f * M3_PI));
             }
         }
-        for (int32_t j = 0; j < jointMax; ++j)
+        for (int32_t k = 0; k < brokenCount; ++k)
         {
-            if (s.jointFlag[j] != 0)
-            {
-                m3DestroyBrokenJointDev(w, j);
-            }
+            m3DestroyBrokenJointDev(w, s.jointOrder[k]);
         }
     }
     M3_WIDE_MARK(M3_PHASE_STORE)
