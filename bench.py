@@ -42,6 +42,7 @@ calls are the timing barrier and the max/sum reductions of the result.
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import json
 import os
 import statistics
@@ -417,6 +418,111 @@ def serving_run(m3, requests: int, seed: int, rates: list[float]) -> dict:
     return out
 
 
+# ---------------------------------------------------------------------------
+# Single large worlds (the wide path: one world over the whole grid)
+# ---------------------------------------------------------------------------
+# (key, workload, scene, seed, param, substeps, device steps, window start,
+#  reference window steps, reference build)
+SINGLE_WORLDS = [
+    ("c1", "box pyramid: a 20-row wall of 210 unit boxes on a plane (1000 steps)",
+     1, 0, 20, 4, 1000, 0, 1000, "stock"),
+    ("c2", "rain field: 10,000 spheres, capsules and QuickHull hulls falling 5-100 m onto a "
+           "255 x 255 heightfield (600 steps)", 10, 3, 10000, 4, 600, 300, 10, "stock"),
+    ("c5", "city: 1000 towers of 10 x 10 x 2 boxes welded by 460,000 breakable fixed joints, "
+           "4000 projectiles, 8 substeps", 9, 5, 1000, 8, 13, 3, 1, "big"),
+]
+
+
+def _golden_hash(scene: int, seed: int, param: int, step: int):
+    """The reference's hash after `step` steps from the committed traces
+    (tests/golden), or None."""
+    for name in ("large_traces.json", "traces.json"):
+        path = ROOT / "tests" / "golden" / name
+        if not path.exists():
+            continue
+        for c in json.loads(path.read_text())["cases"]:
+            if (c["scene"], c["seed"], c["param"]) != (scene, seed, param):
+                continue
+            if "trace" in c and step <= len(c["trace"]):
+                return c["trace"][step - 1]
+            if "hashes" in c and str(step) in c["hashes"]:
+                return c["hashes"][str(step)]
+    return None
+
+
+def single_world_run(m3, args, spec) -> dict:
+    """One large world stepped alone: the device's body-substeps/s over
+    the whole run (CUDA events, every stream idle at the end), the world
+    hash checked against the reference's recorded trace; beside it the
+    reference on the host cores, serially and on all host threads through
+    its own task hooks, over a window of the same run (the device world's
+    snapshot at the window's start, restored into the reference: same
+    state, same steps), its hashes checked too."""
+    import torch
+    from oracle import ref
+    key, workload, scene, seed, param, substeps, steps, start, window, variant = spec
+    g = m3.World.scene(scene, seed, param)
+    bodies = g.body_count() - 1  # the static ground body is not simulated
+    m3.reserve_worlds([g])
+    m3.upload_worlds([g])
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    ms = 0.0
+    snap = None
+    done = 0
+    for chunk in ([start, steps - start] if start > 0 else [steps]):
+        torch.cuda.synchronize()
+        e0.record()
+        m3.step_worlds([g], DT, substeps, chunk)
+        m3.synchronize()
+        e1.record()
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
+        done += chunk
+        if done == start:
+            snap = m3.snapshot(g)
+    got = f"{int(m3.hash_worlds([g])[0]):016x}"
+    want = _golden_hash(scene, seed, param, steps)
+    value = bodies * substeps * steps / (ms / 1000.0)
+    line = {"workload": workload, "bodies": bodies, "substeps": substeps, "steps": steps,
+            "value": value, "unit": UNIT, "ms_per_step": ms / steps,
+            "hash_check": {"step": steps, "device": got, "reference": want,
+                           "equal": want is not None and got == want}}
+    g.destroy()
+    # The reference over the window [start, start + window).
+    if args.no_cpu_baseline or not ref.build():
+        return line
+    lib = ref.lib(variant)
+    threads = os.cpu_count() or 1
+    out = {}
+    for label, nthreads in (("serial", 1), ("threads", threads)):
+        r = ref.RefWorld.scene(scene, seed, param, variant=variant)
+        if snap is not None:
+            ref.abi.bind_snapshot(lib)
+            buf = (C.c_uint8 * len(snap)).from_buffer_copy(snap)
+            if not lib.m3World_Restore(r.id, buf, len(snap)):
+                r.destroy()
+                line["cpu_reference"] = {"unavailable": "the reference refused the snapshot"}
+                return line
+        used = r.use_threads(nthreads)
+        t0 = time.perf_counter()
+        r.step(DT, substeps, window)
+        sec = time.perf_counter() - t0
+        h = r.hash()
+        r.destroy()
+        out[label] = {"value": bodies * substeps * window / sec, "unit": UNIT, "cores": used,
+                      "ms_per_step": 1000.0 * sec / window}
+        wantw = _golden_hash(scene, seed, param, start + window)
+        out[label]["hash_equal"] = wantw is not None and f"{h:016x}" == wantw
+    out["window"] = f"steps {start + 1}-{start + window} (the device world's snapshot after " \
+                    f"step {start}, restored into the reference)" if start > 0 else \
+                    f"steps 1-{window} from creation"
+    out["kind"] = "reference" + (" (scratch cap raised: the stock build stalls)"
+                                 if variant == "big" else "")
+    line["cpu_reference"] = out
+    return line
+
+
 def config_block(args, **extra) -> dict:
     cfg = {"workload": f"batched uneven worlds: {args.worlds} worlds per GPU, dynamic bodies "
                        f"log-uniform [{args.lo}, {args.hi}], box stacks + spheres + 3 revolute "
@@ -451,6 +557,8 @@ def main() -> None:
     ap.add_argument("--serving-requests", type=int, default=256)
     ap.add_argument("--terrain-worlds", type=int, default=1024)
     ap.add_argument("--terrain-steps", type=int, default=20)
+    ap.add_argument("--single", default="c1,c2,c5",
+                    help="single large worlds to run after the batch (comma list, or none)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -645,6 +753,11 @@ def main() -> None:
         serving = serving_run(m3, args.serving_requests, rank_seed + 77, [400.0, 0.0])
     # The terrain batch runs after the serving loop, so that its host
     # threads and device memory leave the latency figures alone.
+    singles = None
+    if rank == 0 and args.single not in ("", "none"):
+        want = set(args.single.split(","))
+        singles = {spec[0]: single_world_run(m3, args, spec) for spec in SINGLE_WORLDS
+                   if spec[0] in want}
     terrain = None
     if rank == 0 and args.terrain_worlds > 0 and not args.no_cpu_baseline:
         terrain = terrain_run(m3, args, rank_seed + 91)
@@ -659,6 +772,7 @@ def main() -> None:
             "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
             "cpu_baseline": cpu, "plain_gpu": plain, "bit_exact_check": verified,
             "hash_ms": hash_ms, "clocks": clocks, "terrain": terrain, "serving": serving,
+            "single_worlds": singles,
         }
         print(json.dumps(line))
     if world_size > 1:

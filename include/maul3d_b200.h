@@ -333,6 +333,11 @@ M3GPU_API m3ShapeId m3CreatePlaneShape(m3BodyId bodyId, const m3ShapeDef* def,
                                        const m3Plane* plane);
 M3GPU_API m3ShapeId m3CreateCapsuleShape(m3BodyId bodyId, const m3ShapeDef* def,
                                          const m3Capsule* capsule);
+/* shape.c:988-1030 (shape.h:143-149): convex hull of 4-256 points
+ * (QuickHull, bit-identical slab to the reference's); null for a stale
+ * body or def, no points, a non-finite point or a degenerate cloud. */
+M3GPU_API m3ShapeId m3CreateHullShape(m3BodyId bodyId, const m3ShapeDef* def,
+                                      const m3Vec3* points, int32_t count);
 M3GPU_API m3ShapeId m3CreateBoxShape(m3BodyId bodyId, const m3ShapeDef* def,
                                      m3Vec3 halfExtents);
 /* Replaces m3CreateHeightFieldGridShape (include/maul3d/shape.h:194-202,

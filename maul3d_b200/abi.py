@@ -53,6 +53,7 @@ SCENE_SHOTS = 6
 SCENE_PLANK = 7
 SCENE_BOUNCE = 8
 SCENE_CITY = 9
+SCENE_RAIN = 10
 
 
 def _ptr(a: np.ndarray) -> C.c_void_p:
@@ -302,6 +303,9 @@ def bind_create(lib: C.CDLL) -> C.CDLL:
     lib.m3CreateCapsuleShape.restype = m3ShapeId
     lib.m3CreateBoxShape.argtypes = [m3BodyId, C.POINTER(m3ShapeDef), m3Vec3]
     lib.m3CreateBoxShape.restype = m3ShapeId
+    lib.m3CreateHullShape.argtypes = [m3BodyId, C.POINTER(m3ShapeDef), C.POINTER(m3Vec3),
+                                      C.c_int32]
+    lib.m3CreateHullShape.restype = m3ShapeId
     lib.m3CreateHeightFieldGridShape.argtypes = [m3BodyId, C.POINTER(m3ShapeDef),
                                                  C.POINTER(C.c_float), C.c_int32, C.c_int32,
                                                  C.c_float]

@@ -33,7 +33,8 @@ DET_DEVICE = ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"]
 DET_HOST = ["-ffp-contract=off", "-fno-fast-math", "-fno-unsafe-math-optimizations"]
 
 CU_SOURCES = ["step.cu", "hash.cu", "upload.cu"]
-CPP_SOURCES = ["world.cpp", "device.cpp", "capi.cpp", "hostmem.cpp", "snapshot.cpp", "serve.cpp"]
+CPP_SOURCES = ["world.cpp", "device.cpp", "capi.cpp", "hostmem.cpp", "snapshot.cpp", "serve.cpp",
+               "quickhull.cpp"]
 C_SOURCES = ["scenes.c"]
 
 

@@ -230,6 +230,11 @@ inline void m3AttachDevicePools(m3HostWorld* w, m3WorldView* view)
     view->hfSamples = w->dhf != nullptr ? (const float*)(w->dhf + headers) : nullptr;
 }
 
+// Convex hull of a point cloud into a hull slab (quickhull.cpp): the
+// reference's QuickHull with unit-density mass properties; the half-edge
+// table is the caller's to build.
+bool m3QuickHull(const m3Vec3* points, int32_t count, m3HullData* out);
+
 // Registry (world.cpp).
 m3HostWorld* m3gpuWorldFromId(m3WorldId id);
 m3HostWorld* m3gpuWorldFromIndex0(uint16_t index0);

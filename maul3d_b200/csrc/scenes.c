@@ -50,6 +50,12 @@
 //                       per tower launched at 20-40 m/s toward seeded
 //                       towers: 1000 towers are 204,000 bodies and
 //                       460,000 joints.
+//   M3S_RAIN            the mixed rain field: `param` bodies (10,000 in
+//                       the configuration), 40 % spheres, 30 % capsules,
+//                       30 % QuickHull hulls of 16-32 points, on a jittered
+//                       grid 2.4 m apart at heights 5-100 m above a
+//                       255 x 255 heightfield of 1 m cells (four seeded
+//                       sine octaves, 4 m amplitude).
 
 #include <m3_scene_api.h> // resolved by -I: product or oracle shim
 
@@ -68,6 +74,7 @@ enum
     M3S_PLANK = 7,
     M3S_BOUNCE = 8,
     M3S_CITY = 9,
+    M3S_RAIN = 10,
 };
 
 static uint64_t SceneSplitMix(uint64_t* state)
@@ -781,6 +788,116 @@ static m3WorldId City(uint64_t seed, int32_t towers)
     return world;
 }
 
+// Height of the rain field's terrain at sample (x, z): four octaves of
+// sin x cos, frequency doubling and weight halving per octave, scaled to
+// a 4 m amplitude.
+static double RainHeight(const double* ph, double x, double z)
+{
+    double h = 0.0;
+    double weight = 1.0;
+    double total = 0.0;
+    double f = 0.045;
+    for (int32_t o = 0; o < 4; ++o)
+    {
+        h += weight * sin(f * x + ph[2 * o]) * cos(f * z + ph[2 * o + 1]);
+        total += weight;
+        weight *= 0.5;
+        f *= 2.0;
+    }
+    return 4.0 * h / total;
+}
+
+static m3WorldId Rain(uint64_t seed, int32_t bodies)
+{
+    if (bodies < 1)
+    {
+        bodies = 1;
+    }
+    const int32_t n = 255;
+    const float cell = 1.0f;
+    const double half = 0.5 * (double)(n - 1) * (double)cell;
+    m3WorldDef def = m3DefaultWorldDef();
+    def.bodyCapacity = bodies + 4;
+    def.shapeCapacity = bodies + 4;
+    def.jointCapacity = 4;
+    m3WorldId world = m3CreateWorld(&def);
+    uint64_t rng = seed ^ 0x4A1Full;
+    double ph[8];
+    for (int32_t k = 0; k < 8; ++k)
+    {
+        ph[k] = SceneRand(&rng, 0.0, 6.283185307179586);
+    }
+    static float heights[255 * 255];
+    for (int32_t iz = 0; iz < n; ++iz)
+    {
+        for (int32_t ix = 0; ix < n; ++ix)
+        {
+            heights[iz * n + ix] = (float)RainHeight(ph, (double)ix, (double)iz);
+        }
+    }
+    m3BodyDef gd = m3DefaultBodyDef();
+    gd.position = (m3Pos3){-half, 0.0, -half};
+    m3BodyId ground = m3CreateBody(world, &gd);
+    m3ShapeDef hd = m3DefaultShapeDef();
+    hd.friction = 0.6f;
+    m3CreateHeightFieldGridShape(ground, &hd, heights, n, n, cell);
+    int32_t side = 1;
+    while (side * side < bodies)
+    {
+        side += 1;
+    }
+    const double spacing = 2.4;
+    const double span = spacing * (double)(side - 1);
+    m3BodyDef bd = m3DefaultBodyDef();
+    bd.type = m3_dynamicBody;
+    for (int32_t b = 0; b < bodies; ++b)
+    {
+        const double x = -0.5 * span + spacing * (double)(b % side) + SceneRand(&rng, -0.3, 0.3);
+        const double z = -0.5 * span + spacing * (double)(b / side) + SceneRand(&rng, -0.3, 0.3);
+        bd.position = (m3Pos3){x, SceneRand(&rng, 5.0, 100.0), z};
+        m3BodyId body = m3CreateBody(world, &bd);
+        m3ShapeDef sd = m3DefaultShapeDef();
+        sd.density = (float)SceneRand(&rng, 0.5, 2.0);
+        sd.friction = (float)SceneRand(&rng, 0.3, 0.9);
+        const int32_t kind = b % 10;
+        if (kind < 4)
+        {
+            m3Sphere ball = {{0.0f, 0.0f, 0.0f}, (float)SceneRand(&rng, 0.25, 0.75)};
+            m3CreateSphereShape(body, &sd, &ball);
+        }
+        else if (kind < 7)
+        {
+            const float r = (float)SceneRand(&rng, 0.2, 0.5);
+            const float hh = (float)SceneRand(&rng, 0.3, 1.0);
+            m3Capsule cap = {{0.0f, -hh, 0.0f}, {0.0f, hh, 0.0f}, r};
+            m3CreateCapsuleShape(body, &sd, &cap);
+        }
+        else
+        {
+            // 16-32 points uniform in the unit ball (rejection from the
+            // cube), scaled by U[0.5, 1.5].
+            m3Vec3 pts[32];
+            const int32_t count = 16 + (int32_t)(SceneSplitMix(&rng) % 17u);
+            const double scale = SceneRand(&rng, 0.5, 1.5);
+            for (int32_t k = 0; k < count; ++k)
+            {
+                double px;
+                double py;
+                double pz;
+                do
+                {
+                    px = SceneRand(&rng, -1.0, 1.0);
+                    py = SceneRand(&rng, -1.0, 1.0);
+                    pz = SceneRand(&rng, -1.0, 1.0);
+                } while (px * px + py * py + pz * pz > 1.0);
+                pts[k] = (m3Vec3){(float)(scale * px), (float)(scale * py), (float)(scale * pz)};
+            }
+            m3CreateHullShape(body, &sd, pts, count);
+        }
+    }
+    return world;
+}
+
 // Build one seeded scene; returns the null world id for an unknown
 // scene number.
 M3S_API m3WorldId m3s_build(int32_t scene, uint64_t seed, int32_t param)
@@ -807,6 +924,8 @@ M3S_API m3WorldId m3s_build(int32_t scene, uint64_t seed, int32_t param)
         return Bounce(seed, param > 0 ? param : 40);
     case M3S_CITY:
         return City(seed, param > 0 ? param : 1000);
+    case M3S_RAIN:
+        return Rain(seed, param > 0 ? param : 10000);
     default:
     {
         m3WorldId none = {0, 0};

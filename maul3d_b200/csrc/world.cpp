@@ -859,7 +859,8 @@ extern "C" m3ShapeDef m3DefaultShapeDef(void)
 
 static m3ShapeId CreateShapeCommon(m3BodyId bodyId, const m3ShapeDef* def, uint8_t type,
                                    const m3ShapeGeom* geom, const m3HeightFieldDev* grid = nullptr,
-                                   const float* heights = nullptr)
+                                   const float* heights = nullptr,
+                                   const m3HullData* prebuilt = nullptr)
 {
     m3ShapeId nullId = {0, 0, 0};
     int32_t b;
@@ -895,8 +896,16 @@ static m3ShapeId CreateShapeCommon(m3BodyId bodyId, const m3ShapeDef* def, uint8
     int32_t hullIndex = -1;
     if (type == M3_SHAPE_HULL)
     {
+        // A box from its half extents, or a hull built from points.
         m3HullData data;
-        BuildBoxHull(&data, geom->v);
+        if (prebuilt != nullptr)
+        {
+            data = *prebuilt;
+        }
+        else
+        {
+            BuildBoxHull(&data, geom->v);
+        }
         hullIndex = InternHull(w, &data);
         if (hullIndex < 0)
         {
@@ -1036,6 +1045,49 @@ extern "C" m3ShapeId m3CreateCapsuleShape(m3BodyId bodyId, const m3ShapeDef* def
     geom.v2 = capsule->point2;
     geom.s2 = 0.0f;
     return CreateShapeCommon(bodyId, def, M3_SHAPE_CAPSULE, &geom);
+}
+
+// shape.c:988-1030 (shape.h:143-149): the convex hull of a point cloud
+// (QuickHull, quickhull.cpp), interned like every hull slab.  Null for a
+// stale body or def, no points, a non-finite point, or a cloud the hull
+// builder refuses (fewer than 4 or more than 256 points, degenerate, over
+// the slab's caps).
+extern "C" m3ShapeId m3CreateHullShape(m3BodyId bodyId, const m3ShapeDef* def,
+                                       const m3Vec3* points, int32_t count)
+{
+    m3ShapeId nullId = {0, 0, 0};
+    m3gpuClearError();
+    int32_t b;
+    if (ResolveBody(bodyId, &b) == nullptr || def == nullptr ||
+        def->internalValue != M3_SHAPE_COOKIE)
+    {
+        m3gpuSetError(M3GPU_ERR_INVALID, "m3CreateHullShape: stale body or invalid def");
+        return nullId;
+    }
+    if (points == nullptr || count <= 0)
+    {
+        m3gpuSetError(M3GPU_ERR_INVALID, "m3CreateHullShape: no points");
+        return nullId;
+    }
+    for (int32_t i = 0; i < count; ++i)
+    {
+        if (!FiniteV3(points[i]))
+        {
+            m3gpuSetError(M3GPU_ERR_INVALID, "m3CreateHullShape: non-finite point %d", i);
+            return nullId;
+        }
+    }
+    m3HullData data;
+    if (!m3QuickHull(points, count, &data))
+    {
+        m3gpuSetError(M3GPU_ERR_INVALID,
+                      "m3CreateHullShape: degenerate cloud, or over the hull caps");
+        return nullId;
+    }
+    BuildHalfEdges(&data);
+    m3ShapeGeom geom;
+    memset(&geom, 0, sizeof(geom));
+    return CreateShapeCommon(bodyId, def, M3_SHAPE_HULL, &geom, nullptr, nullptr, &data);
 }
 
 extern "C" m3ShapeId m3CreateBoxShape(m3BodyId bodyId, const m3ShapeDef* def, m3Vec3 halfExtents)

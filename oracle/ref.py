@@ -98,6 +98,8 @@ def lib(variant: str = "stock") -> C.CDLL:
         h.m3o_step_trace.restype = None
         h.m3o_copy_hull.argtypes = [m3WorldId, C.c_int32, C.c_void_p]
         h.m3o_copy_hull.restype = C.c_int32
+        h.m3o_use_task_pool.argtypes = [m3WorldId, C.c_int32]
+        h.m3o_use_task_pool.restype = C.c_int32
         _libs[variant] = h
     return _libs[variant]
 
@@ -140,6 +142,11 @@ class RefWorld:
 
     def scratch_overflow(self) -> int:
         return int(self.lib.m3o_scratch_overflow(self.id))
+
+    def use_threads(self, threads: int) -> int:
+        """Step on `threads` host threads through the reference's own task
+        hooks (1: serial); returns the threads in use."""
+        return int(self.lib.m3o_use_task_pool(self.id, threads))
 
     def step_count(self) -> int:
         return int(self.lib.m3o_step_count(self.id))
