@@ -483,6 +483,18 @@ def single_world_run(m3, args, spec) -> dict:
             snap = m3.snapshot(g)
     got = f"{int(m3.hash_worlds([g])[0]):016x}"
     want = _golden_hash(scene, seed, param, steps)
+    # The window's device continuation from the restored snapshot: the
+    # reference's restore of the same bytes must continue identically
+    # (its own restore does not always reproduce its uninterrupted run,
+    # so the restored runs are compared with each other).
+    window_hash = None
+    if snap is not None:
+        gr = m3.World.scene(scene, seed, param)
+        buf = (C.c_uint8 * len(snap)).from_buffer_copy(snap)
+        if m3.lib.m3World_Restore(gr.id, buf, len(snap)):
+            gr.step(DT, substeps, window)
+            window_hash = gr.hash()
+        gr.destroy()
     value = bodies * substeps * steps / (ms / 1000.0)
     line = {"workload": workload, "bodies": bodies, "substeps": substeps, "steps": steps,
             "value": value, "unit": UNIT, "ms_per_step": ms / steps,
@@ -512,8 +524,11 @@ def single_world_run(m3, args, spec) -> dict:
         r.destroy()
         out[label] = {"value": bodies * substeps * window / sec, "unit": UNIT, "cores": used,
                       "ms_per_step": 1000.0 * sec / window}
-        wantw = _golden_hash(scene, seed, param, start + window)
-        out[label]["hash_equal"] = wantw is not None and f"{h:016x}" == wantw
+        if snap is None:
+            wantw = _golden_hash(scene, seed, param, start + window)
+            out[label]["hash_equal"] = wantw is not None and f"{h:016x}" == wantw
+        else:
+            out[label]["hash_equal"] = window_hash is not None and h == window_hash
     out["window"] = f"steps {start + 1}-{start + window} (the device world's snapshot after " \
                     f"step {start}, restored into the reference)" if start > 0 else \
                     f"steps 1-{window} from creation"
