@@ -533,104 +533,6 @@ __global__ void __launch_bounds__(32)
     }
 }
 
-// One large world's tree walk (a launch of one world): the same walk
-// with the world's nodes behind a direct-mapped, write-through cache in
-// the SM's shared memory (slot = node id modulo a power of two).  Every
-// move starts at the root and ends there, so the upper levels are read
-// again and again; a single thread walks, so the cache needs no
-// coherence beyond its own writes.
-struct m3TreeCachedStore
-{
-    m3TreeNode* nodes;
-    m3TreeNode* cache;
-    int32_t* tags;
-    int32_t mask;
-    __device__ m3TreeNode Get(int32_t i) const
-    {
-        const int32_t k = i & mask;
-        if (tags[k] == i)
-        {
-            return cache[k];
-        }
-        const m3TreeNode n = nodes[i];
-        cache[k] = n;
-        tags[k] = i;
-        return n;
-    }
-    __device__ void Put(int32_t i, const m3TreeNode& n) const
-    {
-        nodes[i] = n;
-        const int32_t k = i & mask;
-        cache[k] = n;
-        tags[k] = i;
-    }
-};
-
-__global__ void __launch_bounds__(32) m3TreeCachedKernel(const m3WorldView* views,
-                                                        const int32_t* order, int32_t treeLag,
-                                                        int32_t slots)
-{
-    extern __shared__ __align__(16) uint8_t s_treeCache[];
-    const int32_t lane = (int32_t)threadIdx.x;
-    const m3WorldView& w = views[order[0]];
-    m3WorldScalars* sc = w.sc;
-    if (sc->treeTracked == 0)
-    {
-        return;
-    }
-    m3Scratch s;
-    ScratchCarve(&s, w.scratch, sc->bodyCap, sc->shapeCap, sc->jointCap, sc->pairCap, treeLag);
-    const int32_t slot = (int32_t)((uint32_t)sc->treeTail % (uint32_t)treeLag);
-    const int32_t moves = s.treeMoveCount[slot];
-    __syncwarp();
-    if (lane == 0)
-    {
-        sc->treeTail += 1;
-    }
-    if (moves <= 0 || sc->status != 0 || moves > sc->shapeMax)
-    {
-        return;
-    }
-    m3TreeNode* cache = (m3TreeNode*)s_treeCache;
-    int32_t* tags = (int32_t*)(cache + slots);
-    for (int32_t k = lane; k < slots; k += 32)
-    {
-        tags[k] = -1;
-    }
-    __syncwarp();
-    if (lane != 0)
-    {
-        return;
-    }
-    sc->phase[15] += (uint64_t)moves;
-    const m3TreeCachedStore store{w.treeNodes, cache, tags, slots - 1};
-    const m3TreeRef tree = m3WorldTree(w);
-    const int32_t* shapes = s.treeMoveShape + (int64_t)slot * sc->shapeCap;
-    const m3Aabb* boxes = s.treeMoveBox + (int64_t)slot * sc->shapeCap;
-    const int32_t shapeMax = sc->shapeMax;
-    const int32_t nodeCap = 2 * sc->shapeCap;
-    for (int32_t m = 0; m < moves; ++m)
-    {
-        const int32_t shape = shapes[m];
-        const m3Aabb box = boxes[m];
-        const int32_t old = shape >= 0 && shape < shapeMax ? w.proxyId[shape] : M3_TREE_NULL;
-        if (old == M3_TREE_NULL || old < 0 || old >= nodeCap)
-        {
-            atomicExch(&sc->status, M3GPU_ERR_INVALID);
-            sc->statusDetail = 6001;
-            return;
-        }
-        m3TreeRemove(tree, store, old);
-        const int32_t leaf = m3TreeInsert(tree, store, box.lo, box.hi, shape);
-        w.proxyId[shape] = leaf;
-        if (leaf == M3_TREE_NULL)
-        {
-            atomicExch(&sc->status, M3GPU_ERR_CAPACITY);
-            return;
-        }
-    }
-}
-
 // Visit every non-plane pair (a < b) whose fresh bounds overlap and that
 // the filter allows, from the sweep position `p` of the sorted order.
 template <typename F>
@@ -4635,36 +4537,6 @@ static int32_t WideBlocks(const m3HostWorld* w)
     return blocks < maxResident ? blocks : maxResident;
 }
 
-// Cache slots (a power of two) for one world's tree walk: the world's
-// node count rounded down, at most what 200 KiB of shared memory holds;
-// 0 (no cache) for small trees, which stay in L1.
-static int32_t TreeCacheSlots(const m3HostWorld* w)
-{
-    static bool attributeSet = false;
-    const int32_t nodes = 2 * w->shapeCap;
-    if (w->hv.sc->shapeMax < 1024)
-    {
-        return 0;
-    }
-    const int32_t perSlot = (int32_t)sizeof(m3TreeNode) + 4;
-    int32_t slots = 1;
-    while (2 * slots <= nodes && 2 * slots * perSlot <= 200 * 1024)
-    {
-        slots *= 2;
-    }
-    if (!attributeSet)
-    {
-        if (cudaFuncSetAttribute(m3TreeCachedKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 200 * 1024) != cudaSuccess)
-        {
-            cudaGetLastError();
-            return 0;
-        }
-        attributeSet = true;
-    }
-    return slots;
-}
-
 static void LaunchWideSubstep(const m3WorldView* views, const int32_t* order, float dt,
                               int32_t substeps, int32_t blocks)
 {
@@ -5068,10 +4940,8 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
         }
     }
     const cudaStream_t treeStream = s_classStreams.tree;
-    // One large world alone: its substep loop over the whole grid, its
-    // tree walk behind a shared-memory node cache.
+    // One large world alone: its substep loop over the whole grid.
     const int32_t wideBlocks = count == 1 ? WideBlocks(worlds[0]) : 0;
-    const int32_t treeCacheSlots = count == 1 ? TreeCacheSlots(worlds[0]) : 0;
     m3TreeTable* treeTable = nullptr;
     if (anyTracked && steps > 0)
     {
@@ -5123,17 +4993,8 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
         {
             cudaEventRecord(s_classStreams.broadDone[(size_t)step], 0);
             cudaStreamWaitEvent(treeStream, s_classStreams.broadDone[(size_t)step], 0);
-            if (treeCacheSlots > 0)
-            {
-                m3TreeCachedKernel<<<1, 32, (size_t)treeCacheSlots * (sizeof(m3TreeNode) + 4),
-                                     treeStream>>>(treeTable->views, treeTable->order,
-                                                   M3_TREE_LAG, treeCacheSlots);
-            }
-            else
-            {
-                m3TreeKernel<<<count, 32, 0, treeStream>>>(treeTable->views, treeTable->order,
-                                                           count, M3_TREE_LAG);
-            }
+            m3TreeKernel<<<count, 32, 0, treeStream>>>(treeTable->views, treeTable->order,
+                                                       count, M3_TREE_LAG);
             const uint64_t q = RecordTreeLaunch(treeStream);
             treeTable->lastSeq = q;
             for (m3HostWorld* w : tracked)
