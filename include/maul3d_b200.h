@@ -448,6 +448,15 @@ M3GPU_API int64_t m3gpu_uploaded_bytes(void);
  * result, bit for bit, as m3gpu_step_worlds on the same world. */
 M3GPU_API int32_t m3gpu_step_world_noalloc(m3WorldId world, float dt, int32_t substeps);
 
+/* The broadphase tree (no reference counterpart): the tree is state only a
+ * snapshot reads, so a step records its leaf moves and replays them into
+ * the tree later -- once 16 steps have gathered, beside the following
+ * steps, or at once when the tree is read (m3World_Snapshot, any readback
+ * of the world) or overwritten.  This call replays every recorded move of
+ * `count` worlds and waits until the trees are current; m3World_Snapshot
+ * does the same for its world by itself. */
+M3GPU_API int32_t m3gpu_flush_trees(const m3WorldId* worlds, int32_t count);
+
 /* Wait for all device work of the library to finish. */
 M3GPU_API int32_t m3gpu_synchronize(void);
 

@@ -87,6 +87,8 @@ def _load() -> C.CDLL:
     lib.m3gpu_world_stats.restype = C.c_int32
     lib.m3gpu_world_phase_cycles.argtypes = [m3WorldId, C.POINTER(C.c_uint64)]
     lib.m3gpu_world_phase_cycles.restype = C.c_int32
+    lib.m3gpu_flush_trees.argtypes = [C.POINTER(m3WorldId), C.c_int32]
+    lib.m3gpu_flush_trees.restype = C.c_int32
     lib.m3gpu_set_wide_min_shapes.argtypes = [C.c_int32]
     lib.m3gpu_set_wide_min_shapes.restype = C.c_int32
     return lib
@@ -206,6 +208,12 @@ def hash_worlds(worlds) -> np.ndarray:
     _check(lib.m3gpu_hash_worlds(_ids(worlds), len(worlds),
                                  out.ctypes.data_as(C.POINTER(C.c_uint64))))
     return out
+
+
+def flush_trees(worlds) -> None:
+    """Replay every recorded tree move of the worlds and wait (the trees
+    are then current, as a snapshot needs them)."""
+    _check(lib.m3gpu_flush_trees(_ids(worlds), len(worlds)))
 
 
 def synchronize() -> None:

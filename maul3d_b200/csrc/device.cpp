@@ -741,7 +741,9 @@ void m3gpuRelease(m3HostWorld* w)
         m3gpuEnsureDevice();
         cudaDeviceSynchronize();
     }
-    w->treePendingCount = 0;
+    w->treeCount = 0;
+    w->treeFirst = 0;
+    w->treeUnlaunched = 0;
     w->leafBoxValid = false;
     if (w->dslab != nullptr)
     {

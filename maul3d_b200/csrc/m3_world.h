@@ -131,9 +131,14 @@ struct m3StepProfile
     bool valid = false;
 };
 
-// Steps the broadphase tree kernel may trail the step: the depth of the
-// ring of per-step move lists in each world's scratch.
-#define M3_TREE_LAG 8
+// The broadphase tree is state only snapshots read: each step records
+// its leaf moves in a ring of this many per-step lists in the world's
+// scratch, and the moves are replayed into the tree later -- once
+// M3_TREE_REPLAY_AT steps have gathered (on the tree's own stream, beside
+// the following steps), when the ring would overflow, or at once when
+// something reads or overwrites the tree.
+#define M3_TREE_LAG 32
+#define M3_TREE_REPLAY_AT 16
 
 struct m3HostWorld
 {
@@ -211,13 +216,15 @@ struct m3HostWorld
     bool pairTailsToDevice = false;
     bool pairTailsOnDevice = false;
     m3StepProfile profile;
-    // Tree launches (their sequence numbers, oldest first) that have yet
-    // to replay this world's recorded moves, one per ring slot in use;
-    // and whether the scratch's copy of the tree leaves' bounds is
-    // current (it is kept by the broadphase once made).
-    uint64_t treePending[M3_TREE_LAG] = {};
-    int32_t treePendingFirst = 0;
-    int32_t treePendingCount = 0;
+    // The steps whose moves sit in the ring, oldest first: for each, the
+    // sequence number of the tree launch replaying it (0 while no launch
+    // covers it yet; those are the newest `treeUnlaunched` entries); and
+    // whether the scratch's copy of the tree leaves' bounds is current
+    // (it is kept by the broadphase once made).
+    uint64_t treeSlotSeq[M3_TREE_LAG] = {};
+    int32_t treeFirst = 0;
+    int32_t treeCount = 0;
+    int32_t treeUnlaunched = 0;
     bool leafBoxValid = false;
 };
 

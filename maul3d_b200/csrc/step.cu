@@ -448,59 +448,13 @@ __global__ void __launch_bounds__(M3_BLOCK) m3LeafBoxKernel(const m3WorldView* v
 // snapshot reads, so this runs on its own stream beside the following
 // steps, each world up to M3_TREE_LAG steps behind (the move lists sit in
 // a ring of that depth).
-__global__ void __launch_bounds__(32)
-    m3TreeKernel(const m3WorldView* views, const int32_t* order, int32_t count, int32_t treeLag)
+// One step's leaf moves of one world, replayed by lane 0 (the lanes
+// have prefetched the world's nodes).
+__device__ void m3ReplayTreeStep(const m3WorldView& w, const m3Scratch& s, int32_t slot,
+                                 int32_t moves)
 {
-    const int32_t k = blockIdx.x;
-    const int32_t lane = (int32_t)threadIdx.x;
-    if (k >= count)
-    {
-        return;
-    }
-    const m3WorldView& w = views[order[k]];
     m3WorldScalars* sc = w.sc;
-    if (sc->treeTracked == 0)
-    {
-        return;
-    }
-    m3Scratch s;
-    ScratchCarve(&s, w.scratch, sc->bodyCap, sc->shapeCap, sc->jointCap, sc->pairCap, treeLag);
     const m3TreeRef tree = m3WorldTree(w);
-    // The oldest recorded step: one launch replays one step of each of
-    // its worlds, in the order the broadphase recorded them.
-    const int32_t slot = (int32_t)((uint32_t)sc->treeTail % (uint32_t)treeLag);
-    const int32_t moves = s.treeMoveCount[slot];
-    __syncwarp();
-    if (lane == 0)
-    {
-        sc->treeTail += 1;
-    }
-    // A refused world's tree is not kept (its state is unspecified after
-    // a refusal), and a move count above the shape slots cannot come
-    // from this world's broadphase.
-    if (moves <= 0 || sc->status != 0 || moves > sc->shapeMax)
-    {
-        return;
-    }
-    // The walk below is a chain of dependent loads: bring the world's
-    // nodes into L2 first, one bulk prefetch per 64 KiB piece (the array
-    // is 256-byte aligned and 144 bytes a shape, so every piece is a
-    // multiple of 16 bytes).
-    {
-        const int64_t bytes = (int64_t)sizeof(m3TreeNode) * 2 * sc->shapeCap;
-        const uint8_t* base = (const uint8_t*)w.treeNodes;
-        for (int64_t off = (int64_t)lane << 16; off < bytes; off += (int64_t)32 << 16)
-        {
-            const int64_t left = bytes - off;
-            const uint32_t piece = (uint32_t)(left < 65536 ? left : 65536);
-            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(base + off), "r"(piece)
-                         : "memory");
-        }
-    }
-    if (lane != 0)
-    {
-        return;
-    }
     // Observer only: leaf moves replayed, in the phase counters' spare
     // slot (a count, not cycles).
     sc->phase[15] += (uint64_t)moves;
@@ -528,6 +482,76 @@ __global__ void __launch_bounds__(32)
         {
             // The reference's pair update refuses with m3_errorCapacity.
             atomicExch(&sc->status, M3GPU_ERR_CAPACITY);
+            return;
+        }
+    }
+}
+
+// The replay of each world's oldest `steps[world]` recorded steps (the
+// world's index in `views`), in the order the broadphase recorded them.
+__global__ void __launch_bounds__(32)
+    m3TreeKernel(const m3WorldView* views, const int32_t* order, int32_t count, int32_t treeLag,
+                 const int32_t* steps)
+{
+    const int32_t k = blockIdx.x;
+    const int32_t lane = (int32_t)threadIdx.x;
+    if (k >= count)
+    {
+        return;
+    }
+    const int32_t wi = order[k];
+    const int32_t n = steps[wi];
+    const m3WorldView& w = views[wi];
+    m3WorldScalars* sc = w.sc;
+    if (sc->treeTracked == 0 || n <= 0)
+    {
+        return;
+    }
+    m3Scratch s;
+    ScratchCarve(&s, w.scratch, sc->bodyCap, sc->shapeCap, sc->jointCap, sc->pairCap, treeLag);
+    const int32_t tail = sc->treeTail;
+    __syncwarp();
+    if (lane == 0)
+    {
+        sc->treeTail = tail + n;
+    }
+    // A refused world's tree is not kept (its state is unspecified after
+    // a refusal).
+    if (sc->status != 0)
+    {
+        return;
+    }
+    // The walk below is a chain of dependent loads: bring the world's
+    // nodes into L2 first, one bulk prefetch per 64 KiB piece (the array
+    // is 256-byte aligned and 144 bytes a shape, so every piece is a
+    // multiple of 16 bytes).
+    {
+        const int64_t bytes = (int64_t)sizeof(m3TreeNode) * 2 * sc->shapeCap;
+        const uint8_t* base = (const uint8_t*)w.treeNodes;
+        for (int64_t off = (int64_t)lane << 16; off < bytes; off += (int64_t)32 << 16)
+        {
+            const int64_t left = bytes - off;
+            const uint32_t piece = (uint32_t)(left < 65536 ? left : 65536);
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(base + off), "r"(piece)
+                         : "memory");
+        }
+    }
+    if (lane != 0)
+    {
+        return;
+    }
+    for (int32_t i = 0; i < n; ++i)
+    {
+        const int32_t slot = (int32_t)((uint32_t)(tail + i) % (uint32_t)treeLag);
+        const int32_t moves = s.treeMoveCount[slot];
+        // A move count above the shape slots cannot come from this
+        // world's broadphase.
+        if (moves > 0 && moves <= sc->shapeMax)
+        {
+            m3ReplayTreeStep(w, s, slot, moves);
+        }
+        if (sc->status != 0)
+        {
             return;
         }
     }
@@ -4154,11 +4178,9 @@ struct m3ClassStreams
     cudaStream_t stream[M3_CLASSES] = {};
     cudaEvent_t fork = nullptr;
     cudaEvent_t join[M3_CLASSES] = {};
-    // The broadphase tree's stream and its per-step events: the
-    // broadphase of step k done (the tree launches' own events are a
-    // ring by launch, below).
+    // The broadphase tree's stream (its launches' events are a ring by
+    // launch, below).
     cudaStream_t tree = nullptr;
-    std::vector<cudaEvent_t> broadDone;
 };
 static m3ClassStreams s_classStreams;
 
@@ -4191,22 +4213,6 @@ static int32_t EnsureClassStreams()
         return m3gpuSetError(M3GPU_ERR_CUDA, "class streams: %s", cudaGetErrorString(e));
     }
     s_classStreams.device = device;
-    return M3GPU_OK;
-}
-
-// Events for `steps` steps of the tree pipeline.
-static int32_t EnsureTreeEvents(int32_t steps)
-{
-    while ((int32_t)s_classStreams.broadDone.size() < steps)
-    {
-        cudaEvent_t a = nullptr;
-        cudaError_t e = cudaEventCreateWithFlags(&a, cudaEventDisableTiming);
-        if (e != cudaSuccess)
-        {
-            return m3gpuSetError(M3GPU_ERR_CUDA, "tree events: %s", cudaGetErrorString(e));
-        }
-        s_classStreams.broadDone.push_back(a);
-    }
     return M3GPU_OK;
 }
 
@@ -4786,6 +4792,8 @@ struct m3TreeTable
 {
     m3WorldView* views = nullptr;
     int32_t* order = nullptr;
+    int32_t* steps = nullptr;     // per world: recorded steps to replay
+    int32_t* hostSteps = nullptr; // page-locked staging of `steps`
     int32_t cap = 0;
     uint64_t lastSeq = 0;
 };
@@ -4809,13 +4817,25 @@ static int32_t TakeTreeTable(int32_t count, m3TreeTable** out)
     {
         cudaFree(t.views);
         cudaFree(t.order);
+        cudaFree(t.steps);
+        cudaFreeHost(t.hostSteps);
         t.views = nullptr;
         t.order = nullptr;
+        t.steps = nullptr;
+        t.hostSteps = nullptr;
         t.cap = 0;
         cudaError_t e = cudaMalloc((void**)&t.views, sizeof(m3WorldView) * (size_t)count);
         if (e == cudaSuccess)
         {
             e = cudaMalloc((void**)&t.order, sizeof(int32_t) * (size_t)count);
+        }
+        if (e == cudaSuccess)
+        {
+            e = cudaMalloc((void**)&t.steps, sizeof(int32_t) * (size_t)count);
+        }
+        if (e == cudaSuccess)
+        {
+            e = cudaMallocHost((void**)&t.hostSteps, sizeof(int32_t) * (size_t)count);
         }
         if (e != cudaSuccess)
         {
@@ -4840,17 +4860,126 @@ static int32_t TakeTreeTable(int32_t count, m3TreeTable** out)
     return M3GPU_OK;
 }
 
+// Launches the replay of every recorded step no launch covers yet, for
+// the worlds of `table` (views index i = worlds[i]), on `stream` after the
+// events it already waits for; the covered steps take the launch's
+// sequence number.
+static void LaunchTreeReplay(m3TreeTable* table, m3HostWorld** worlds, int32_t count,
+                             cudaStream_t stream)
+{
+    for (int32_t i = 0; i < count; ++i)
+    {
+        table->hostSteps[i] = worlds[i]->hv.sc->treeTracked != 0 ? worlds[i]->treeUnlaunched : 0;
+    }
+    cudaMemcpyAsync(table->steps, table->hostSteps, sizeof(int32_t) * (size_t)count,
+                    cudaMemcpyHostToDevice, stream);
+    m3TreeKernel<<<count, 32, 0, stream>>>(table->views, table->order, count, M3_TREE_LAG,
+                                           table->steps);
+    const uint64_t q = RecordTreeLaunch(stream);
+    table->lastSeq = q;
+    s_launches += 1;
+    for (int32_t i = 0; i < count; ++i)
+    {
+        m3HostWorld* w = worlds[i];
+        for (int32_t k = w->treeCount - w->treeUnlaunched; k < w->treeCount; ++k)
+        {
+            w->treeSlotSeq[(w->treeFirst + k) % M3_TREE_LAG] = q;
+        }
+        w->treeUnlaunched = 0;
+    }
+}
+
+// A replay of the batch's unlaunched steps with its own copy of the
+// batch table, on the tree's stream after everything the default stream
+// holds so far (the steps' broadphases included).
+static int32_t ReplayBatch(m3HostWorld** worlds, int32_t count, cudaStream_t treeStream)
+{
+    static cudaEvent_t fork = nullptr;
+    if (fork == nullptr && cudaEventCreateWithFlags(&fork, cudaEventDisableTiming) != cudaSuccess)
+    {
+        fork = nullptr;
+        return m3gpuSetError(M3GPU_ERR_CUDA, "tree replay event");
+    }
+    m3TreeTable* table = nullptr;
+    const int32_t rc = TakeTreeTable(count, &table);
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
+    cudaEventRecord(fork, 0);
+    cudaStreamWaitEvent(treeStream, fork, 0);
+    LaunchTreeReplay(table, worlds, count, treeStream);
+    return M3GPU_OK;
+}
+
+// One world's replay table (views and order of one entry), for readers
+// of a single world's tree.
+static m3WorldView* s_oneView = nullptr;
+static int32_t* s_oneOrder = nullptr;
+static int32_t* s_oneSteps = nullptr;
+
 void m3gpuWaitTree(m3HostWorld* w)
 {
     M3_DEVICE_GUARD;
-    if (w->treePendingCount > 0)
+    if (w->treeCount == 0)
     {
-        const uint64_t last =
-            w->treePending[(w->treePendingFirst + w->treePendingCount - 1) % M3_TREE_LAG];
-        cudaStreamWaitEvent(0, TreeEventFor(last), 0);
-        w->treePendingCount = 0;
-        w->treePendingFirst = 0;
+        return;
     }
+    // Launches already covering some of its steps come first.
+    uint64_t last = 0;
+    for (int32_t k = 0; k < w->treeCount; ++k)
+    {
+        const uint64_t q = w->treeSlotSeq[(w->treeFirst + k) % M3_TREE_LAG];
+        last = q > last ? q : last;
+    }
+    if (last != 0)
+    {
+        cudaStreamWaitEvent(0, TreeEventFor(last), 0);
+    }
+    if (w->treeUnlaunched > 0 && w->dslab != nullptr)
+    {
+        // The rest replayed here, on the default stream, before the
+        // reader's own work.
+        if (s_oneView == nullptr)
+        {
+            cudaMalloc((void**)&s_oneView, sizeof(m3WorldView));
+            cudaMalloc((void**)&s_oneOrder, 2 * sizeof(int32_t));
+            s_oneSteps = s_oneOrder + 1;
+        }
+        m3WorldView view = w->dv;
+        m3AttachDevicePools(w, &view);
+        const int32_t table[2] = {0, w->treeUnlaunched};
+        cudaMemcpy(s_oneView, &view, sizeof(view), cudaMemcpyHostToDevice);
+        cudaMemcpy(s_oneOrder, table, sizeof(table), cudaMemcpyHostToDevice);
+        m3TreeKernel<<<1, 32>>>(s_oneView, s_oneOrder, 1, M3_TREE_LAG, s_oneSteps);
+        s_launches += 1;
+    }
+    w->treeCount = 0;
+    w->treeFirst = 0;
+    w->treeUnlaunched = 0;
+}
+
+// Every recorded move of the worlds replayed into their trees, and the
+// trees finished (the tree stream's work done).
+extern "C" int32_t m3gpu_flush_trees(const m3WorldId* worldIds, int32_t count)
+{
+    M3_DEVICE_GUARD;
+    m3gpuClearError();
+    int32_t rc = m3gpuEnsureDevice();
+    for (int32_t i = 0; rc == M3GPU_OK && i < count; ++i)
+    {
+        m3HostWorld* w = m3gpuWorldFromId(worldIds[i]);
+        if (w == nullptr)
+        {
+            return m3gpuSetError(M3GPU_ERR_INVALID, "stale world id at position %d", i);
+        }
+        m3gpuWaitTree(w);
+    }
+    if (rc == M3GPU_OK)
+    {
+        rc = Check(cudaDeviceSynchronize(), "flush trees");
+    }
+    return rc;
 }
 
 int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t substeps,
@@ -4899,11 +5028,6 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
             return rc;
         }
     }
-    rc = EnsureTreeEvents(steps);
-    if (rc != M3GPU_OK)
-    {
-        return rc;
-    }
     cudaEventRecord(s_events[0]);
     // The broadphase tree: the leaves' bounds once per fresh slab, then
     // per step the tree kernel on its own stream, each world at most
@@ -4942,29 +5066,37 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
     const cudaStream_t treeStream = s_classStreams.tree;
     // One large world alone: its substep loop over the whole grid.
     const int32_t wideBlocks = count == 1 ? WideBlocks(worlds[0]) : 0;
-    m3TreeTable* treeTable = nullptr;
-    if (anyTracked && steps > 0)
-    {
-        rc = TakeTreeTable(count, &treeTable);
-        if (rc != M3GPU_OK)
-        {
-            return rc;
-        }
-    }
     for (int32_t step = 0; step < steps; ++step)
     {
         const cudaEvent_t* ev = &s_events[(size_t)(M3_STAGES * step)];
         if (anyTracked)
         {
-            // The step reuses each world's oldest ring slot once the ring
-            // is full: the launch replaying that slot must be done.
+            // The step records into each world's oldest ring slot once the
+            // ring is full: the launch replaying that slot must be done
+            // (and launched first, if none covers it yet).
+            bool unlaunchedFull = false;
+            for (m3HostWorld* w : tracked)
+            {
+                unlaunchedFull = unlaunchedFull ||
+                                 (w->treeCount == M3_TREE_LAG && w->treeUnlaunched == M3_TREE_LAG);
+            }
+            if (unlaunchedFull)
+            {
+                rc = ReplayBatch(worlds, count, treeStream);
+                if (rc != M3GPU_OK)
+                {
+                    return rc;
+                }
+            }
             uint64_t need = 0;
             for (m3HostWorld* w : tracked)
             {
-                if (w->treePendingCount == M3_TREE_LAG)
+                if (w->treeCount == M3_TREE_LAG)
                 {
-                    const uint64_t q = w->treePending[w->treePendingFirst];
+                    const uint64_t q = w->treeSlotSeq[w->treeFirst];
                     need = q > need ? q : need;
+                    w->treeFirst = (w->treeFirst + 1) % M3_TREE_LAG;
+                    w->treeCount -= 1;
                 }
             }
             if (need != 0)
@@ -4991,23 +5123,25 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
         cudaEventRecord(ev[1]);
         if (anyTracked)
         {
-            cudaEventRecord(s_classStreams.broadDone[(size_t)step], 0);
-            cudaStreamWaitEvent(treeStream, s_classStreams.broadDone[(size_t)step], 0);
-            m3TreeKernel<<<count, 32, 0, treeStream>>>(treeTable->views, treeTable->order,
-                                                       count, M3_TREE_LAG);
-            const uint64_t q = RecordTreeLaunch(treeStream);
-            treeTable->lastSeq = q;
+            // The step's moves are recorded; once M3_TREE_REPLAY_AT steps
+            // wait in a world's ring, the batch's recorded steps are
+            // replayed on the tree's stream beside the following steps.
+            bool replay = false;
             for (m3HostWorld* w : tracked)
             {
-                if (w->treePendingCount == M3_TREE_LAG)
-                {
-                    w->treePendingFirst = (w->treePendingFirst + 1) % M3_TREE_LAG;
-                    w->treePendingCount -= 1;
-                }
-                w->treePending[(w->treePendingFirst + w->treePendingCount) % M3_TREE_LAG] = q;
-                w->treePendingCount += 1;
+                w->treeSlotSeq[(w->treeFirst + w->treeCount) % M3_TREE_LAG] = 0;
+                w->treeCount += 1;
+                w->treeUnlaunched += 1;
+                replay = replay || w->treeUnlaunched >= M3_TREE_REPLAY_AT;
             }
-            s_launches += 1;
+            if (replay)
+            {
+                rc = ReplayBatch(worlds, count, treeStream);
+                if (rc != M3GPU_OK)
+                {
+                    return rc;
+                }
+            }
         }
         m3PairOffsetsKernel<<<1, M3_BLOCK>>>(s_batch.dviews, count, s_batch.doffsets);
         LaunchNarrow(s_batch.dviews, s_batch.doffsets, count, anyTerrain);
@@ -5017,10 +5151,11 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
         cudaEventRecord(ev[5]);
         s_launches += 5 + (count <= M3_NARROW_SMALL_BATCH ? 1 : M3_NARROW_LAUNCHES + (anyTerrain ? M3_TERRAIN_LAUNCHES : 0));
     }
-    // The trees finish behind this call, on their own stream: a later
-    // step waits only for a ring slot it reuses, and anything reading or
-    // overwriting a world's tree waits for that world's launches
-    // (m3gpuWaitTree); m3gpu_synchronize waits for everything.
+    // The trees catch up later: replays already launched finish on their
+    // own stream, recorded steps not yet launched wait in the ring; a
+    // later step waits only for a ring slot it reuses, and anything that
+    // reads or overwrites a world's tree first replays the world's
+    // recorded steps (m3gpuWaitTree, m3gpu_flush_trees).
     cudaMemsetAsync(s_dstatus, 0, sizeof(int32_t));
     m3StatusKernel<<<(count + 255) / 256, 256>>>(s_batch.dviews, count, s_dstatus);
     s_launches += 1;
@@ -5168,7 +5303,7 @@ int32_t m3gpuHashBatch(m3HostWorld** worlds, int32_t count, uint64_t* out)
 
 static __device__ __align__(256) uint8_t g_noallocScratch[M3_NOALLOC_SCRATCH_BYTES];
 static __device__ __align__(256) m3WorldView g_noallocView;
-static __device__ __align__(256) int32_t g_noallocTable[4]; // order[1], offsets[2], spare
+static __device__ __align__(256) int32_t g_noallocTable[4]; // order[1], offsets[2], tree steps[1]
 
 struct m3NoallocSymbols
 {
@@ -5259,11 +5394,13 @@ extern "C" int32_t m3gpu_step_world_noalloc(m3WorldId worldId, float dt, int32_t
     m3AttachDevicePools(w, &view);
     view.scratch = sym.scratch;
     view.scratchBytes = M3_NOALLOC_SCRATCH_BYTES;
-    const int32_t zero = 0;
+    // Launch table: order {0}, then two words for the pair offsets, then
+    // the one step the tree replays.
+    const int32_t table[4] = {0, 0, 0, 1};
     rc = Check(cudaMemcpy(sym.view, &view, sizeof(view), cudaMemcpyHostToDevice), "noalloc view");
     if (rc == M3GPU_OK)
     {
-        rc = Check(cudaMemcpy(sym.table, &zero, sizeof(zero), cudaMemcpyHostToDevice),
+        rc = Check(cudaMemcpy(sym.table, table, sizeof(table), cudaMemcpyHostToDevice),
                    "noalloc order");
     }
     if (rc != M3GPU_OK)
@@ -5280,7 +5417,7 @@ extern "C" int32_t m3gpu_step_world_noalloc(m3WorldId worldId, float dt, int32_t
     w->leafBoxValid = false;
     m3LeafBoxKernel<<<1, M3_BLOCK>>>(sym.view, 1);
     m3BroadKernel<M3_BLOCK, 1><<<1, M3_BLOCK>>>(sym.view, order, 1, 1);
-    m3TreeKernel<<<1, 32>>>(sym.view, order, 1, 1);
+    m3TreeKernel<<<1, 32>>>(sym.view, order, 1, 1, sym.table + 3);
     m3PairOffsetsKernel<<<1, M3_BLOCK>>>(sym.view, 1, offsets);
     m3NarrowKernel<<<148, 128>>>(sym.view, offsets, 1);
     LaunchSolve(sym.view, order, 1, dt, substeps, cacheBytes, nullptr);
