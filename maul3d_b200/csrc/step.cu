@@ -4965,19 +4965,49 @@ extern "C" int32_t m3gpu_flush_trees(const m3WorldId* worldIds, int32_t count)
 {
     M3_DEVICE_GUARD;
     m3gpuClearError();
-    int32_t rc = m3gpuEnsureDevice();
-    for (int32_t i = 0; rc == M3GPU_OK && i < count; ++i)
+    if (worldIds == nullptr || count <= 0)
     {
-        m3HostWorld* w = m3gpuWorldFromId(worldIds[i]);
-        if (w == nullptr)
+        return m3gpuSetError(M3GPU_ERR_INVALID, "empty world list");
+    }
+    std::vector<m3HostWorld*> ws((size_t)count);
+    for (int32_t i = 0; i < count; ++i)
+    {
+        ws[(size_t)i] = m3gpuWorldFromId(worldIds[i]);
+        if (ws[(size_t)i] == nullptr)
         {
             return m3gpuSetError(M3GPU_ERR_INVALID, "stale world id at position %d", i);
         }
-        m3gpuWaitTree(w);
+    }
+    int32_t rc = m3gpuEnsureDevice();
+    if (rc == M3GPU_OK)
+    {
+        rc = EnsureClassStreams();
+    }
+    bool unlaunched = false;
+    for (m3HostWorld* w : ws)
+    {
+        unlaunched = unlaunched || (w->treeUnlaunched > 0 && w->dslab != nullptr &&
+                                    !w->hostDirty && w->hv.sc->treeTracked != 0);
+    }
+    if (rc == M3GPU_OK && unlaunched)
+    {
+        // Every world's unlaunched steps in one launch, one warp a world.
+        rc = PrepareBatch(ws.data(), count);
+        if (rc == M3GPU_OK)
+        {
+            rc = ReplayBatch(ws.data(), count, s_classStreams.tree);
+        }
     }
     if (rc == M3GPU_OK)
     {
         rc = Check(cudaDeviceSynchronize(), "flush trees");
+    }
+    if (rc == M3GPU_OK)
+    {
+        for (m3HostWorld* w : ws)
+        {
+            m3gpuWaitTree(w); // nothing left to replay: clears the ring's record
+        }
     }
     return rc;
 }
