@@ -582,6 +582,10 @@ def main() -> None:
     ap.add_argument("--terrain-steps", type=int, default=20)
     ap.add_argument("--single", default="c1,c2,c5",
                     help="single large worlds to run after the batch (comma list, or none)")
+    ap.add_argument("--single-only", action="store_true",
+                    help="run only the single large worlds (profiling), print them and exit")
+    ap.add_argument("--city-towers", type=int, default=1000,
+                    help="towers of the c5 city world (1000 in the configuration)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -598,6 +602,13 @@ def main() -> None:
     local_rank = env_int("LOCAL_RANK", 0)
     torch.cuda.set_device(local_rank)
     m3.set_device(local_rank)
+    if args.single_only:
+        want = set(args.single.split(","))
+        specs = [spec for spec in SINGLE_WORLDS if spec[0] in want]
+        specs = [spec[:4] + (args.city_towers,) + spec[5:] if spec[0] == "c5" else spec
+                 for spec in specs]
+        print(json.dumps({spec[0]: single_world_run(m3, args, spec) for spec in specs}))
+        return
     if world_size > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300),
