@@ -693,6 +693,9 @@ def main() -> None:
     achieved = (sub_bytes / args.steps) / (kms / args.steps / 1000.0) / 1e9
     roofline = {"kernel": "m3SubstepKernel", "bound": "hbm", "achieved": achieved,
                 "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                "limiter": "latency: dependent row solves between block barriers; rows and "
+                           "bodies are re-read from L1, L2 and shared memory, so DRAM traffic "
+                           "stays below the algorithmic bytes",
                 "traffic": SUBSTEP_TRAFFIC_DEFAULT if default_workload(args) else None,
                 "traffic_source": "ncu dram bytes of one step's three size-class launches on "
                                   "this workload",
