@@ -28,9 +28,12 @@ Lines printed by rank 0 (one JSON object):
             same worlds for the same W+K steps, every sampled world's
             hash checked against the device's;
   serving   the serving path: replay containers (snapshot + journal of
-            impulse frames) of worlds of 200-5000 bodies arriving as a
-            Poisson process, p50/p99 latency from arrival to final hash
-            and throughput, plus a run with every request at once.
+            impulse frames) of worlds of 200-5000 bodies (boxes, spheres,
+            16-point hulls) arriving as a Poisson process at 100-20,000
+            requests/s, p50/p99 latency from arrival to final hash and
+            throughput, a run with every request at once, and the
+            reference's restore + replay of the same containers on the
+            host cores, every answer compared.
 
 Multi-GPU: one process per GPU (torchrun), each rank its own 4096
 worlds (weak scaling), no collective on the data path; the only NCCL
@@ -353,20 +356,76 @@ def terrain_run(m3, args, seed: int) -> dict:
             "bit_exact_check": {"worlds_checked": len(sample), "mismatches": mismatches}}
 
 
-def serving_run(m3, requests: int, seed: int, rates: list[float]) -> dict:
-    """Serving: replay containers (a snapshot of a world of 200-5000
-    bodies plus a journal of 4-16 frames, each frame 1-8 linear impulses
-    of 1-50 N s and one step of 1/60 s in 4 substeps) arrive as a Poisson
-    process; one server on this GPU batches every active request's frame
-    per tick.  Latency is arrival to final hash; the saturated run
-    submits everything at once."""
+SERVING_RATES = [100.0, 1000.0, 4000.0, 20000.0, 0.0]
+
+
+def reference_serving(containers, caps, threads: int) -> tuple[float, list[int]]:
+    """The reference serving the same containers on the host cores: per
+    request a fresh world of the snapshot's capacities, m3World_Restore,
+    m3World_JournalReplay, m3World_Hash; requests in waves of 64 (its
+    world table), worlds created serially, restore + replay one request
+    per task on `threads` threads.  Returns (seconds, hashes)."""
+    from oracle import ref
+    lib = ref.abi.bind_replay(ref.abi.bind_snapshot(ref.abi.bind_create(ref.lib())))
+    hashes = [0] * len(containers)
+    t0 = time.perf_counter()
+    for first in range(0, len(containers), 64):
+        wave = list(range(first, min(first + 64, len(containers))))
+        ids = {}
+        for i in wave:
+            d = lib.m3DefaultWorldDef()
+            (d.bodyCapacity, d.shapeCapacity, d.meshCapacity, d.jointCapacity, d.voxelCapacity,
+             d.characterCapacity) = caps[i]
+            ids[i] = lib.m3CreateWorld(C.byref(d))
+        queue = list(wave)
+        lock = threading.Lock()
+        failed = []
+
+        def worker():
+            while True:
+                with lock:
+                    if not queue:
+                        return
+                    i = queue.pop(0)
+                snap, journal = containers[i]
+                sb = (C.c_uint8 * len(snap)).from_buffer_copy(snap)
+                jb = (C.c_uint8 * len(journal)).from_buffer_copy(journal)
+                if not (lib.m3World_Restore(ids[i], sb, len(snap)) and
+                        lib.m3World_JournalReplay(ids[i], jb, len(journal))):
+                    failed.append(i)
+
+        pool = [threading.Thread(target=worker) for _ in range(min(threads, len(wave)))]
+        for t in pool:
+            t.start()
+        for t in pool:
+            t.join()
+        for i in wave:
+            hashes[i] = 0 if i in failed else int(lib.m3World_Hash(ids[i]))
+            lib.m3DestroyWorld(ids[i])
+    return time.perf_counter() - t0, hashes
+
+
+def serving_run(m3, distinct: int, seed: int, rates: list[float], budget: int,
+                cpu_baseline: bool) -> dict:
+    """Serving: replay containers of the served configuration's worlds
+    (200-5000 bodies, log-uniform: boxes, spheres and 16-point QuickHull
+    hulls on a plane, stepped 5 steps in) plus a journal of 4-16 frames,
+    each 1-8 linear impulses of 1-50 N s on random bodies and one step of
+    1/60 s in 4 substeps.  Requests arrive as a Poisson process at each
+    rate (`distinct` different containers, submitted in turn; per rate
+    about one second of arrivals, 256-2048 requests; rate 0 submits
+    `distinct` at once); one server on this GPU under a device budget
+    batches every active request's frame per tick.  Latency is arrival to
+    final hash.  Every answer is compared with the reference's restore +
+    replay of the same container, which is also timed on the host cores
+    (all at once) as the serving baseline."""
     from maul3d_b200 import abi
     rng = np.random.default_rng(seed)
-    sizes = np.exp(rng.uniform(np.log(200), np.log(5000), requests)).astype(int)
-    worlds = [m3.World.scene(abi.SCENE_UNEVEN, seed + i, int(n)) for i, n in enumerate(sizes)]
-    m3.step_worlds(worlds, DT, 4, 5)  # in motion, with contacts and warm starts
-    containers, work = [], []
-    for w, n in zip(worlds, sizes):
+    sizes = np.exp(rng.uniform(np.log(200), np.log(5000), distinct)).astype(int)
+    containers, raw, caps, work = [], [], [], []
+    for i, n in enumerate(sizes):
+        w = m3.World.scene(abi.SCENE_MIXED, seed + i, int(n))
+        m3.step_worlds([w], DT, 4, 5)  # in motion, with contacts and warm starts
         bodies = w.body_count()
         frames = int(rng.integers(4, 17))
         journal = b""
@@ -378,43 +437,74 @@ def serving_run(m3, requests: int, seed: int, rates: list[float]) -> dict:
                                                     int(rng.integers(2, bodies + 1)), 0,
                                                     [float(x) for x in d.astype(np.float32)])
             journal += abi.journal_step(DT, 4)
-        containers.append(abi.encode_container(m3.lib, m3.snapshot(w), journal))
+        snap = m3.snapshot(w)
+        containers.append(abi.encode_container(m3.lib, snap, journal))
+        raw.append((snap, journal))
+        caps.append(tuple(int.from_bytes(snap[o:o + 4], "little")
+                          for o in (24, 44, 92, 112, 132, 152)))
         work.append(int(n) * frames * 4)
         w.destroy()
-    out = {"requests": requests, "bodies": "log-uniform [200, 5000]", "frames": "U{4..16}",
-           "impulses_per_frame": "U{1..8}, 1-50 N s", "runs": []}
+    out = {"workload": f"{distinct} distinct containers: worlds of 200-5000 bodies "
+                       "(log-uniform; boxes, spheres, 16-point hulls), 4-16 frames of 1-8 "
+                       "impulses of 1-50 N s, 4 substeps",
+           "device_budget_bytes": budget, "runs": []}
+    served = {}
+    mismatched_runs = 0
     for rate in rates:
-        server = m3.Server()
-        arrivals = (np.cumsum(rng.exponential(1.0 / rate, requests)) if rate > 0
-                    else np.zeros(requests))
-        latency = np.zeros(requests)
-        ticket_of = {}
-        submitted = 0
-        finished = 0
-        ticks = 0
+        count = distinct if rate <= 0 else int(min(2048, max(256, rate)))
+        arrivals = (np.cumsum(rng.exponential(1.0 / rate, count)) if rate > 0
+                    else np.zeros(count))
+        server = m3.Server(device_budget=budget)
+        latency = np.zeros(count)
+        which = {}
+        submitted = finished = ticks = 0
         t0 = time.perf_counter()
-        while finished < requests:
+        while finished < count:
             now = time.perf_counter() - t0
-            while submitted < requests and arrivals[submitted] <= now:
-                ticket_of[server.submit(containers[submitted])] = submitted
+            while submitted < count and arrivals[submitted] <= now:
+                which[server.submit(containers[submitted % distinct])] = submitted
                 submitted += 1
-            if server.tick() == 0 and submitted < requests:
+            if server.tick() == 0 and submitted < count:
                 time.sleep(max(0.0, arrivals[submitted] - (time.perf_counter() - t0)))
             ticks += 1
             t, h, st = server.poll()
             done_at = time.perf_counter() - t0
             for k in range(len(t)):
-                i = ticket_of[int(t[k])]
+                i = which[int(t[k])]
                 latency[i] = done_at - arrivals[i]
                 finished += 1
+                key = i % distinct
+                answer = int(h[k]) if int(st[k]) == 0 else -int(st[k])
+                if served.setdefault(key, answer) != answer:
+                    mismatched_runs += 1
         wall = time.perf_counter() - t0
+        stats = server.stats()
         server.close()
         out["runs"].append({
             "arrival_rate_per_s": rate if rate > 0 else "all at once",
+            "requests": count,
             "p50_latency_ms": float(np.percentile(latency, 50) * 1e3),
             "p99_latency_ms": float(np.percentile(latency, 99) * 1e3),
-            "requests_per_s": requests / wall,
-            "body_substeps_per_s": float(sum(work)) / wall, "ticks": ticks})
+            "requests_per_s": count / wall,
+            "body_substeps_per_s": float(sum(work[i % distinct] for i in range(count))) / wall,
+            "ticks": ticks, "peak_active": stats["peakActive"],
+            "peak_device_bytes": stats["peakHeldBytes"],
+            "host_ms": {k: round(stats[k], 1) for k in
+                        ("prepareMs", "admitMs", "stepMs", "retireMs", "waitMs")},
+            "workers": stats["workers"]})
+    out["same_answer_every_time"] = mismatched_runs == 0
+    if cpu_baseline:
+        threads = os.cpu_count() or 1
+        secs, ref_hashes = reference_serving(raw, caps, threads)
+        mism = sum(1 for i in range(distinct) if served.get(i) != ref_hashes[i])
+        out["cpu_reference"] = {
+            "requests_per_s": distinct / secs,
+            "body_substeps_per_s": float(sum(work)) / secs, "cores": threads,
+            "kind": "reference",
+            "sample": f"the {distinct} distinct containers at once: restore + journal replay "
+                      f"+ hash per request, one request per task"}
+        out["bit_exact_check"] = {"requests_checked": distinct, "mismatches": mism,
+                                  "against": "the reference's restore + replay"}
     return out
 
 
@@ -577,7 +667,10 @@ def main() -> None:
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--serving-requests", type=int, default=256)
+    ap.add_argument("--serving-requests", type=int, default=256,
+                    help="distinct serving containers (0: no serving run)")
+    ap.add_argument("--serving-budget-gb", type=int, default=16,
+                    help="the server's device memory budget")
     ap.add_argument("--terrain-worlds", type=int, default=1024)
     ap.add_argument("--terrain-steps", type=int, default=20)
     ap.add_argument("--single", default="c1,c2,c5",
@@ -792,8 +885,9 @@ def main() -> None:
                              f"every sampled world's final hash compared with the device's"}
 
     serving = None
-    if args.serving_requests > 0:
-        serving = serving_run(m3, args.serving_requests, rank_seed + 77, [400.0, 0.0])
+    if args.serving_requests > 0 and rank == 0:
+        serving = serving_run(m3, args.serving_requests, rank_seed + 77, SERVING_RATES,
+                              args.serving_budget_gb << 30, not args.no_cpu_baseline)
     # The terrain batch runs after the serving loop, so that its host
     # threads and device memory leave the latency figures alone.
     singles = None

@@ -514,13 +514,16 @@ M3GPU_API int32_t m3gpu_copy_joints(m3WorldId world, void* impulse, void* perp, 
 
 /* Serving: replay containers in, final world hashes out.  A server
  * admits queued requests while their device memory fits `deviceBudget`
- * bytes (and at most `maxActive` at once): each is restored into a fresh
- * world and its journal validated whole.  Every m3gpu_serve_tick then
- * advances every active request by one frame (its body commands and the
- * step that closes them) in one batched launch sequence, and retires the
- * requests whose journal is done with the world hash the reference's
- * m3World_Restore + m3World_JournalReplay would give.  A request's result
- * does not depend on the others in the batch. */
+ * bytes (and at most `maxActive` at once, preparing and active): worker
+ * threads restore each into a fresh world and validate its journal whole
+ * while the GPU steps the others.  Every m3gpu_serve_tick starts
+ * preparing what fits, admits the prepared requests in submission order
+ * (waiting for one only when nothing is active), advances every active
+ * request by one frame (its body commands and the step that closes them)
+ * in one batched launch sequence, and retires the requests whose journal
+ * is done with the world hash the reference's m3World_Restore +
+ * m3World_JournalReplay would give.  A request's result does not depend
+ * on the others in the batch. */
 typedef struct m3gpuServer m3gpuServer;
 M3GPU_API m3gpuServer* m3gpu_serve_create(int64_t deviceBudget, int32_t maxActive);
 M3GPU_API void m3gpu_serve_destroy(m3gpuServer* server);
@@ -536,6 +539,23 @@ M3GPU_API int32_t m3gpu_serve_tick(m3gpuServer* server);
 M3GPU_API int32_t m3gpu_serve_poll(m3gpuServer* server, int64_t* tickets, uint64_t* hashes,
                                    int32_t* status, int32_t capacity);
 M3GPU_API int32_t m3gpu_serve_active(const m3gpuServer* server);
+/* Counters and host times of a server since its creation.  Device bytes
+ * are the allocator's (size-class) bytes of the slab and hull pool of
+ * each preparing or active request. */
+typedef struct m3gpuServeStats
+{
+    int64_t submitted, completed, refused, ticks;
+    int64_t heldBytes;     /* device bytes of preparing + active requests now */
+    int64_t peakHeldBytes; /* the most ever held at once */
+    int64_t budget;
+    int32_t queued, preparing, active, peakActive, workers, reserved;
+    double prepareMs; /* worker time building, restoring and parsing (summed over workers) */
+    double admitMs;   /* ticking thread: world table entry and device reservation */
+    double stepMs;    /* ticking thread: the batched frames */
+    double retireMs;  /* ticking thread: device hashes and world release */
+    double waitMs;    /* ticking thread: waiting for a preparation with nothing active */
+} m3gpuServeStats;
+M3GPU_API int32_t m3gpu_serve_stats(m3gpuServer* server, m3gpuServeStats* out);
 
 /* White-box test hook: one broadphase tree move on the host image (remove
  * the shape's leaf, insert [lo, hi]), as the step's tree refresh makes

@@ -72,6 +72,8 @@ def _load() -> C.CDLL:
     lib.m3gpu_serve_poll.restype = C.c_int32
     lib.m3gpu_serve_active.argtypes = [C.c_void_p]
     lib.m3gpu_serve_active.restype = C.c_int32
+    lib.m3gpu_serve_stats.argtypes = [C.c_void_p, C.POINTER(abi.m3gpuServeStats)]
+    lib.m3gpu_serve_stats.restype = C.c_int32
     lib.m3gpu_set_device.argtypes = [C.c_int32]
     lib.m3gpu_set_device.restype = C.c_int32
     for name in ("m3gpu_reserve_worlds", "m3gpu_upload_worlds"):
@@ -329,6 +331,12 @@ class Server:
 
     def active(self) -> int:
         return int(lib.m3gpu_serve_active(self.handle))
+
+    def stats(self) -> dict:
+        """Counters and host times since creation (m3gpu_serve_stats)."""
+        out = abi.m3gpuServeStats()
+        _check(lib.m3gpu_serve_stats(self.handle, C.byref(out)))
+        return {name: getattr(out, name) for name, _ in out._fields_ if name != "reserved"}
 
     def poll(self, capacity: int = 4096):
         """Finished requests: arrays of tickets, hashes and statuses."""

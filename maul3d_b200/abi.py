@@ -54,6 +54,7 @@ SCENE_PLANK = 7
 SCENE_BOUNCE = 8
 SCENE_CITY = 9
 SCENE_RAIN = 10
+SCENE_MIXED = 11
 
 
 def _ptr(a: np.ndarray) -> C.c_void_p:
@@ -76,7 +77,18 @@ class m3Profile(C.Structure):
         "continuous", "sleep", "characters", "softBodies")]
 
 
+class m3gpuServeStats(C.Structure):
+    """A server's counters and host times (m3gpu_serve_stats)."""
+    _fields_ = ([(name, C.c_int64) for name in (
+        "submitted", "completed", "refused", "ticks", "heldBytes", "peakHeldBytes", "budget")] +
+        [(name, C.c_int32) for name in (
+            "queued", "preparing", "active", "peakActive", "workers", "reserved")] +
+        [(name, C.c_double) for name in (
+            "prepareMs", "admitMs", "stepMs", "retireMs", "waitMs")])
+
+
 assert C.sizeof(m3Counters) == 88 and C.sizeof(m3Profile) == 44
+assert C.sizeof(m3gpuServeStats) == 120
 
 
 def bind_common(lib: C.CDLL) -> C.CDLL:

@@ -84,9 +84,10 @@ int32_t m3gpuEnsureDevice(void)
 }
 
 // Device memory for slabs and hull pools: blocks carved from large
-// cudaMalloc chunks of the current device and reused through exact-size
-// free lists (cudaMalloc is a slow driver call: one per 512 MiB instead
-// of two per world).  Chunks stay allocated until the process exits.
+// cudaMalloc chunks of the current device and reused through free lists
+// per size class (m3SizeClass; cudaMalloc is a slow driver call: one per
+// 512 MiB instead of two per world).  Chunks stay allocated until the
+// process exits.
 namespace
 {
 constexpr size_t kDevChunkBytes = (size_t)512 << 20;
@@ -113,7 +114,7 @@ DevArena& TheDevArena()
 
 size_t RoundDev(size_t bytes)
 {
-    return bytes == 0 ? M3_SLAB_ALIGN : (bytes + M3_SLAB_ALIGN - 1) / M3_SLAB_ALIGN * M3_SLAB_ALIGN;
+    return m3SizeClass(bytes, M3_SLAB_ALIGN);
 }
 } // namespace
 
@@ -342,6 +343,9 @@ static int32_t UploadPrepare(m3HostWorld* w)
     {
         if (w->dhulls != nullptr)
         {
+            // Steps in flight may still read the old pool; its block goes
+            // back to the free lists only once they are done.
+            cudaDeviceSynchronize();
             DevFree(w->dhulls, (size_t)w->dhullCap * sizeof(m3HullData));
             w->dhulls = nullptr;
         }

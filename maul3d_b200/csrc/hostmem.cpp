@@ -5,8 +5,8 @@
 // per 64 MiB instead of two per world).  Uploads from a locked chunk are
 // plain asynchronous DMA copies.
 //
-// Blocks are reused through exact-size free lists; chunks stay mapped
-// (and, once locked, locked) until the process exits.
+// Blocks are reused through free lists per size class (m3SizeClass);
+// chunks stay mapped (and, once locked, locked) until the process exits.
 #include "m3_world.h"
 
 #include <cuda_runtime.h>
@@ -34,7 +34,7 @@ struct Arena
 {
     std::mutex mu;
     std::vector<Chunk> chunks;
-    std::map<size_t, std::vector<void*>> freeBlocks; // by page-rounded size
+    std::map<size_t, std::vector<void*>> freeBlocks; // by size class
 };
 
 Arena& TheArena()
@@ -45,8 +45,7 @@ Arena& TheArena()
 
 size_t RoundPages(size_t bytes)
 {
-    const size_t page = M3_HOST_PAGE;
-    return bytes == 0 ? page : (bytes + page - 1) / page * page;
+    return m3SizeClass(bytes, M3_HOST_PAGE);
 }
 } // namespace
 

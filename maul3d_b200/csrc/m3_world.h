@@ -17,6 +17,22 @@
 // granular blocks from large mappings, page-locked chunk by chunk when a
 // world becomes device-resident, so uploads are asynchronous DMA copies.
 #define M3_HOST_PAGE 4096
+
+// Size classes of the host and device block allocators: `bytes` in
+// granules, rounded up to m * 2^k granules with 8 <= m < 16 (at most an
+// eighth over), so that freed blocks of worlds of similar size serve the
+// next ones instead of fresh memory.
+inline size_t m3SizeClass(size_t bytes, size_t granule)
+{
+    const size_t n = bytes == 0 ? 1 : (bytes + granule - 1) / granule;
+    if (n <= 16)
+    {
+        return n * granule;
+    }
+    const int k = 63 - __builtin_clzll((unsigned long long)n) - 3;
+    const size_t m = (n + ((size_t)1 << k) - 1) >> k;
+    return (m << k) * granule;
+}
 void* m3HostAlloc(size_t bytes);
 void m3HostFree(void* p, size_t bytes);
 // Page-lock every chunk not locked yet (one driver call per chunk).
@@ -290,6 +306,15 @@ struct m3JournalRecordView
 };
 // Parses and validates a whole journal against a world's bodies; false
 // (with the error set) on the first bad or unsupported record.
+// Worlds outside the world table (world.cpp): built on any thread,
+// entered into the table later (the null id and the world deleted when
+// the table is full), or deleted without ever entering it.
+m3HostWorld* m3gpuNewWorld(const m3WorldDef* def);
+m3WorldId m3gpuAttachWorld(m3HostWorld* w);
+void m3gpuDeleteWorld(m3HostWorld* w);
+// m3World_Restore on a world object (snapshot.cpp).
+bool m3gpuRestoreWorld(m3HostWorld* w, const void* data, int32_t size);
+
 bool m3ParseJournal(const m3HostWorld* w, const uint8_t* stream, int32_t size,
                     std::vector<m3JournalRecordView>* out);
 

@@ -56,6 +56,12 @@
 //                       grid 2.4 m apart at heights 5-100 m above a
 //                       255 x 255 heightfield of 1 m cells (four seeded
 //                       sine octaves, 4 m amplitude).
+//   M3S_MIXED           one served world: `param` dynamic bodies, a third
+//                       each boxes (half extent U[0.25, 0.5]), spheres
+//                       (radius U[0.25, 0.5]) and QuickHull hulls of 16
+//                       points on a sphere of radius U[0.3, 0.6], in
+//                       columns of four on a jittered 1.6 m grid above a
+//                       ground plane, dropped from 0.1-0.4 m gaps.
 
 #include <m3_scene_api.h> // resolved by -I: product or oracle shim
 
@@ -75,6 +81,7 @@ enum
     M3S_BOUNCE = 8,
     M3S_CITY = 9,
     M3S_RAIN = 10,
+    M3S_MIXED = 11,
 };
 
 static uint64_t SceneSplitMix(uint64_t* state)
@@ -898,6 +905,76 @@ static m3WorldId Rain(uint64_t seed, int32_t bodies)
     return world;
 }
 
+static m3WorldId Mixed(uint64_t seed, int32_t bodies)
+{
+    if (bodies < 4)
+    {
+        bodies = 4;
+    }
+    m3WorldDef def = m3DefaultWorldDef();
+    def.bodyCapacity = bodies + 4;
+    def.shapeCapacity = bodies + 4;
+    def.jointCapacity = 4;
+    m3WorldId world = m3CreateWorld(&def);
+    SceneGround(world, 0.6f);
+    uint64_t rng = seed ^ 0x5E4Dull;
+    const int32_t columns = (bodies + 3) / 4;
+    int32_t side = 1;
+    while (side * side < columns)
+    {
+        side += 1;
+    }
+    const double spacing = 1.6;
+    const double span = spacing * (double)(side - 1);
+    m3BodyDef bd = m3DefaultBodyDef();
+    bd.type = m3_dynamicBody;
+    for (int32_t b = 0; b < bodies; ++b)
+    {
+        const int32_t c = b / 4;
+        const double x = -0.5 * span + spacing * (double)(c % side) + SceneRand(&rng, -0.1, 0.1);
+        const double z = -0.5 * span + spacing * (double)(c / side) + SceneRand(&rng, -0.1, 0.1);
+        const double y = 0.6 + 1.2 * (double)(b % 4) + SceneRand(&rng, 0.1, 0.4);
+        bd.position = (m3Pos3){x, y, z};
+        m3BodyId body = m3CreateBody(world, &bd);
+        m3ShapeDef sd = m3DefaultShapeDef();
+        sd.friction = (float)SceneRand(&rng, 0.4, 0.8);
+        const int32_t kind = (int32_t)(SceneSplitMix(&rng) % 3u);
+        if (kind == 0)
+        {
+            const float h = (float)SceneRand(&rng, 0.25, 0.5);
+            m3CreateBoxShape(body, &sd, (m3Vec3){h, h, h});
+        }
+        else if (kind == 1)
+        {
+            m3Sphere ball = {{0.0f, 0.0f, 0.0f}, (float)SceneRand(&rng, 0.25, 0.5)};
+            m3CreateSphereShape(body, &sd, &ball);
+        }
+        else
+        {
+            m3Vec3 pts[16];
+            const double scale = SceneRand(&rng, 0.3, 0.6);
+            for (int32_t k = 0; k < 16; ++k)
+            {
+                double px;
+                double py;
+                double pz;
+                double rr;
+                do
+                {
+                    px = SceneRand(&rng, -1.0, 1.0);
+                    py = SceneRand(&rng, -1.0, 1.0);
+                    pz = SceneRand(&rng, -1.0, 1.0);
+                    rr = px * px + py * py + pz * pz;
+                } while (rr > 1.0 || rr < 0.04);
+                const double inv = scale / sqrt(rr);
+                pts[k] = (m3Vec3){(float)(inv * px), (float)(inv * py), (float)(inv * pz)};
+            }
+            m3CreateHullShape(body, &sd, pts, 16);
+        }
+    }
+    return world;
+}
+
 // Build one seeded scene; returns the null world id for an unknown
 // scene number.
 M3S_API m3WorldId m3s_build(int32_t scene, uint64_t seed, int32_t param)
@@ -926,6 +1003,8 @@ M3S_API m3WorldId m3s_build(int32_t scene, uint64_t seed, int32_t param)
         return City(seed, param > 0 ? param : 1000);
     case M3S_RAIN:
         return Rain(seed, param > 0 ? param : 10000);
+    case M3S_MIXED:
+        return Mixed(seed, param > 0 ? param : 1000);
     default:
     {
         m3WorldId none = {0, 0};

@@ -4,15 +4,20 @@
 // the end of the journal, what a verifier compares against the
 // container's recorded final hash.
 //
-// The server keeps a queue and a set of active requests.  Each tick it
-// admits queued requests while their device memory fits the budget
-// (restore into a fresh world, journal parsed and validated whole), then
+// A request moves through three sets.  Queued: submitted, waiting for
+// room.  Preparing: its device memory counted against the budget, a
+// worker thread builds its world off the world table, restores the
+// snapshot into it and parses and validates the journal whole.
+// Active: entered into the world table and reserved on the device.  Each
+// tick starts preparing queued requests while they fit the budget and
+// the active limit, admits the prepared ones in submission order, and
 // advances every active request by one frame: the frame's body commands
 // and its step run for all active worlds in one batched launch sequence
 // (worlds grouped by step arguments), the commands applied by a device
-// kernel.  Requests whose journal is done are hashed on the device and
-// retired.  A request's result does not depend on what else is in the
-// batch: worlds never interact.
+// kernel.  The workers keep preparing while the frame runs on the GPU.
+// Requests whose journal is done are hashed on the device and retired.
+// A request's result does not depend on what else is in the batch:
+// worlds never interact.
 #include "m3_world.h"
 #include "m3_ops.h"
 
@@ -20,9 +25,12 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
+#include <condition_variable>
 #include <deque>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <thread>
 #include <utility>
 #include <vector>
@@ -164,10 +172,13 @@ struct Request
     std::vector<uint8_t> snapshot;
     std::vector<uint8_t> journal;
     m3WorldId world{0, 0};
-    m3HostWorld* host = nullptr;
+    m3HostWorld* host = nullptr;  // in the world table: active
+    m3HostWorld* built = nullptr; // prepared off the table, not yet admitted
     std::vector<m3JournalRecordView> records;
     size_t next = 0;
     int64_t deviceBytes = 0;
+    int32_t code = M3GPU_OK; // the preparation's refusal
+    bool ready = false;      // prepared (under the server's mutex)
 };
 
 struct Completion
@@ -207,9 +218,17 @@ bool ReadShape(const std::vector<uint8_t>& snap, SnapshotShape* out)
 int64_t DeviceBytes(const SnapshotShape& s)
 {
     const int32_t pairCap = 8 * s.shape;
-    return m3LayoutPersistent(nullptr, nullptr, s.body, s.shape, s.joint, pairCap) +
-           m3gpuScratchBytes(s.body, s.shape, s.joint, pairCap) +
-           (int64_t)(s.hulls < 4 ? 4 : s.hulls) * (int64_t)sizeof(m3HullData);
+    const int64_t slab = m3LayoutPersistent(nullptr, nullptr, s.body, s.shape, s.joint, pairCap) +
+                         m3gpuScratchBytes(s.body, s.shape, s.joint, pairCap);
+    const int64_t hulls = (int64_t)(s.hulls < 4 ? 4 : s.hulls) * (int64_t)sizeof(m3HullData);
+    // What the device allocator hands out: its size classes.
+    return (int64_t)m3SizeClass((size_t)slab, M3_SLAB_ALIGN) +
+           (int64_t)m3SizeClass((size_t)hulls, M3_SLAB_ALIGN);
+}
+
+double MsSince(std::chrono::steady_clock::time_point t0)
+{
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 } // namespace
 
@@ -218,10 +237,22 @@ struct m3gpuServer
     int64_t budget = 0;
     int32_t maxActive = 0;
     int64_t nextTicket = 1;
-    int64_t activeBytes = 0;
+    int64_t heldBytes = 0; // device bytes of preparing and active requests
     std::deque<std::unique_ptr<Request>> queue;
+    std::deque<std::unique_ptr<Request>> preparing; // submission order
     std::vector<std::unique_ptr<Request>> active;
     std::deque<Completion> done;
+    m3gpuServeStats stats{};
+
+    // Preparation workers: `jobs` holds requests of `preparing` not yet
+    // taken; a worker marks its request ready under `mu`.
+    std::mutex mu;
+    std::condition_variable jobReady;
+    std::condition_variable prepared;
+    std::deque<Request*> jobs;
+    std::vector<std::thread> workers;
+    bool stopping = false;
+    std::atomic<int64_t> prepareUs{0};
 };
 
 namespace
@@ -229,22 +260,102 @@ namespace
 void Retire(m3gpuServer* s, std::unique_ptr<Request>& r, uint64_t hash, int32_t status)
 {
     s->done.push_back(Completion{r->ticket, hash, status});
+    if (status == M3GPU_OK)
+    {
+        s->stats.completed += 1;
+    }
+    else
+    {
+        s->stats.refused += 1;
+    }
     if (r->host != nullptr)
     {
         m3DestroyWorld(r->world);
         r->host = nullptr;
     }
+    if (r->built != nullptr)
+    {
+        m3gpuDeleteWorld(r->built);
+        r->built = nullptr;
+    }
 }
 
-// Admits queued requests while they fit; refused ones retire at once
-// with their error code.  Worlds are created in order (the world table
-// is shared), restored and their journals parsed on host threads (each
-// touches only its own world), then reserved on the device in order.
-void Admit(m3gpuServer* s)
+// A worker's preparation of one request: its world built off the world
+// table with the snapshot's capacities, the snapshot restored into it and
+// the journal parsed and validated whole.  Touches only the request.
+void Prepare(Request& r)
 {
-    std::vector<std::unique_ptr<Request>> batch;
-    int64_t bytes = s->activeBytes;
-    while (!s->queue.empty() && (int32_t)(s->active.size() + batch.size()) < s->maxActive)
+    SnapshotShape shape;
+    ReadShape(r.snapshot, &shape); // checked when the request started
+    m3WorldDef def = m3DefaultWorldDef();
+    def.bodyCapacity = shape.body;
+    def.shapeCapacity = shape.shape;
+    def.meshCapacity = shape.mesh;
+    def.jointCapacity = shape.joint;
+    def.voxelCapacity = shape.voxel;
+    def.characterCapacity = shape.character;
+    m3HostWorld* w = m3gpuNewWorld(&def);
+    int32_t code = M3GPU_OK;
+    if (w == nullptr ||
+        !m3gpuRestoreWorld(w, r.snapshot.data(), (int32_t)r.snapshot.size()) ||
+        !m3ParseJournal(w, r.journal.data(), (int32_t)r.journal.size(), &r.records))
+    {
+        code = m3gpu_last_error();
+        code = code != M3GPU_OK ? code : M3GPU_ERR_INVALID;
+        if (w != nullptr)
+        {
+            m3gpuDeleteWorld(w);
+            w = nullptr;
+        }
+    }
+    if (w != nullptr)
+    {
+        // Nobody can snapshot a served world: it keeps no broadphase tree.
+        w->hv.sc->treeTracked = 0;
+    }
+    // The inputs live on in the world; the request keeps only its parsed
+    // records.
+    std::vector<uint8_t>().swap(r.snapshot);
+    std::vector<uint8_t>().swap(r.journal);
+    r.built = w;
+    r.code = code;
+}
+
+void WorkerLoop(m3gpuServer* s)
+{
+    for (;;)
+    {
+        Request* r = nullptr;
+        {
+            std::unique_lock<std::mutex> lock(s->mu);
+            s->jobReady.wait(lock, [s] { return s->stopping || !s->jobs.empty(); });
+            if (s->stopping && s->jobs.empty())
+            {
+                return;
+            }
+            r = s->jobs.front();
+            s->jobs.pop_front();
+        }
+        const auto t0 = std::chrono::steady_clock::now();
+        Prepare(*r);
+        s->prepareUs += (int64_t)(MsSince(t0) * 1000.0);
+        {
+            std::lock_guard<std::mutex> lock(s->mu);
+            r->ready = true;
+        }
+        s->prepared.notify_all();
+    }
+}
+
+// Starts preparing queued requests while they fit: at most `maxActive`
+// preparing and active, their device bytes within the budget (a request
+// alone is always let in, so that one larger than the budget still
+// runs).  A container whose snapshot header is unreadable retires at once.
+void Start(m3gpuServer* s)
+{
+    int32_t started = 0;
+    while (!s->queue.empty() &&
+           (int32_t)(s->active.size() + s->preparing.size()) < s->maxActive)
     {
         std::unique_ptr<Request>& front = s->queue.front();
         SnapshotShape shape;
@@ -258,80 +369,79 @@ void Admit(m3gpuServer* s)
         {
             front->deviceBytes = DeviceBytes(shape);
         }
-        if (!(s->active.empty() && batch.empty()) && bytes + front->deviceBytes > s->budget)
+        const bool alone = s->active.empty() && s->preparing.empty();
+        if (!alone && s->heldBytes + front->deviceBytes > s->budget)
         {
             break; // the memory budget is full: wait for retirements
         }
-        std::unique_ptr<Request> r = std::move(front);
+        s->heldBytes += front->deviceBytes;
+        s->stats.peakHeldBytes = std::max(s->stats.peakHeldBytes, s->heldBytes);
+        Request* job = front.get();
+        s->preparing.push_back(std::move(front));
         s->queue.pop_front();
-        m3WorldDef def = m3DefaultWorldDef();
-        def.bodyCapacity = shape.body;
-        def.shapeCapacity = shape.shape;
-        def.meshCapacity = shape.mesh;
-        def.jointCapacity = shape.joint;
-        def.voxelCapacity = shape.voxel;
-        def.characterCapacity = shape.character;
-        r->world = m3CreateWorld(&def);
-        r->host = m3gpuWorldFromId(r->world);
-        if (r->host == nullptr)
         {
-            const int32_t code = m3gpu_last_error();
-            Retire(s, r, 0, code != M3GPU_OK ? code : M3GPU_ERR_INVALID);
-            continue;
+            std::lock_guard<std::mutex> lock(s->mu);
+            s->jobs.push_back(job);
         }
-        bytes += r->deviceBytes;
-        batch.push_back(std::move(r));
+        started += 1;
     }
-    if (batch.empty())
+    if (started > 0)
     {
-        return;
+        s->jobReady.notify_all();
     }
-    std::vector<int32_t> codes(batch.size(), M3GPU_OK);
-    std::atomic<size_t> nextJob{0};
-    auto work = [&]() {
-        for (size_t i = nextJob.fetch_add(1); i < batch.size(); i = nextJob.fetch_add(1))
+}
+
+// Admits prepared requests in submission order (the first one still
+// being prepared stops it; with nothing active it is waited for): each
+// enters the world table and is reserved on the device.
+void Admit(m3gpuServer* s)
+{
+    while (!s->preparing.empty())
+    {
+        Request* front = s->preparing.front().get();
         {
-            Request& r = *batch[i];
-            if (!m3World_Restore(r.world, r.snapshot.data(), (int32_t)r.snapshot.size()) ||
-                !m3ParseJournal(r.host, r.journal.data(), (int32_t)r.journal.size(), &r.records))
+            std::unique_lock<std::mutex> lock(s->mu);
+            if (!front->ready)
             {
-                const int32_t code = m3gpu_last_error();
-                codes[i] = code != M3GPU_OK ? code : M3GPU_ERR_INVALID;
+                if (!s->active.empty())
+                {
+                    return;
+                }
+                const auto t0 = std::chrono::steady_clock::now();
+                s->prepared.wait(lock, [front] { return front->ready; });
+                s->stats.waitMs += MsSince(t0);
             }
         }
-    };
-    const size_t threads =
-        std::min<size_t>(batch.size(), std::max(1u, std::thread::hardware_concurrency()));
-    std::vector<std::thread> pool;
-    for (size_t t = 1; t < threads; ++t)
-    {
-        pool.emplace_back(work);
-    }
-    work();
-    for (std::thread& t : pool)
-    {
-        t.join();
-    }
-    for (size_t i = 0; i < batch.size(); ++i)
-    {
-        std::unique_ptr<Request>& r = batch[i];
-        if (codes[i] == M3GPU_OK && m3gpuReserve(r->host) != M3GPU_OK)
+        const auto t0 = std::chrono::steady_clock::now();
+        std::unique_ptr<Request> r = std::move(s->preparing.front());
+        s->preparing.pop_front();
+        int32_t code = r->code;
+        if (code == M3GPU_OK)
         {
-            codes[i] = m3gpu_last_error();
+            m3HostWorld* w = r->built;
+            r->built = nullptr;
+            r->world = m3gpuAttachWorld(w); // deletes the world when the table is full
+            r->host = m3gpuWorldFromId(r->world);
+            if (r->host == nullptr)
+            {
+                code = m3gpu_last_error();
+                code = code != M3GPU_OK ? code : M3GPU_ERR_CAPACITY;
+            }
+            else if (m3gpuReserve(r->host) != M3GPU_OK)
+            {
+                code = m3gpu_last_error();
+            }
         }
-        if (codes[i] != M3GPU_OK)
+        if (code != M3GPU_OK)
         {
-            Retire(s, r, 0, codes[i]);
-            continue;
+            s->heldBytes -= r->deviceBytes;
+            Retire(s, r, 0, code);
         }
-        // Nobody can snapshot a served world: it keeps no broadphase tree.
-        r->host->hv.sc->treeTracked = 0;
-        // The inputs live on in the world; the request keeps only its
-        // parsed records.
-        std::vector<uint8_t>().swap(r->snapshot);
-        std::vector<uint8_t>().swap(r->journal);
-        s->activeBytes += r->deviceBytes;
-        s->active.push_back(std::move(r));
+        else
+        {
+            s->active.push_back(std::move(r));
+        }
+        s->stats.admitMs += MsSince(t0);
     }
 }
 } // namespace
@@ -347,6 +457,13 @@ extern "C" m3gpuServer* m3gpu_serve_create(int64_t deviceBudgetBytes, int32_t ma
     m3gpuServer* s = new m3gpuServer();
     s->budget = deviceBudgetBytes;
     s->maxActive = maxActive;
+    // Preparation workers: the host's threads but the ticking one.
+    const unsigned hw = std::max(2u, std::thread::hardware_concurrency());
+    const unsigned workers = std::min(32u, hw - 1);
+    for (unsigned t = 0; t < workers; ++t)
+    {
+        s->workers.emplace_back(WorkerLoop, s);
+    }
     return s;
 }
 
@@ -355,6 +472,23 @@ extern "C" void m3gpu_serve_destroy(m3gpuServer* s)
     if (s == nullptr)
     {
         return;
+    }
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->stopping = true;
+        s->jobs.clear(); // requests not yet taken are dropped
+    }
+    s->jobReady.notify_all();
+    for (std::thread& t : s->workers)
+    {
+        t.join();
+    }
+    for (std::unique_ptr<Request>& r : s->preparing)
+    {
+        if (r->built != nullptr)
+        {
+            m3gpuDeleteWorld(r->built);
+        }
     }
     for (std::unique_ptr<Request>& r : s->active)
     {
@@ -383,6 +517,7 @@ extern "C" int64_t m3gpu_serve_submit(m3gpuServer* s, const void* container, int
     r->journal.assign(jour, jour + view.journalBytes);
     const int64_t ticket = r->ticket;
     s->queue.push_back(std::move(r));
+    s->stats.submitted += 1;
     return ticket;
 }
 
@@ -393,7 +528,12 @@ extern "C" int32_t m3gpu_serve_tick(m3gpuServer* s)
     {
         return m3gpuSetError(M3GPU_ERR_INVALID, "m3gpu_serve_tick: null server");
     }
+    s->stats.ticks += 1;
+    Start(s);
     Admit(s);
+    Start(s); // room freed by refusals
+    s->stats.peakActive = std::max(s->stats.peakActive, (int32_t)s->active.size());
+    const auto tStep = std::chrono::steady_clock::now();
 
     // One frame of every active request: its commands up to and including
     // the next step, batched by step arguments.
@@ -451,6 +591,9 @@ extern "C" int32_t m3gpu_serve_tick(m3gpuServer* s)
         }
     }
 
+    s->stats.stepMs += MsSince(tStep);
+    const auto tRetire = std::chrono::steady_clock::now();
+
     // Retire finished requests: device hash of the finished worlds (a
     // world the device refused reports its refusal instead).
     std::vector<m3HostWorld*> finished;
@@ -475,7 +618,7 @@ extern "C" int32_t m3gpu_serve_tick(m3gpuServer* s)
         {
             std::unique_ptr<Request>& r = s->active[finishedAt[f]];
             const int32_t status = m3gpuWorldStatus(finished[f]);
-            s->activeBytes -= r->deviceBytes;
+            s->heldBytes -= r->deviceBytes;
             Retire(s, r, status == M3GPU_OK ? hashes[f] : 0, status);
         }
         std::vector<std::unique_ptr<Request>> keep;
@@ -489,7 +632,8 @@ extern "C" int32_t m3gpu_serve_tick(m3gpuServer* s)
         }
         s->active.swap(keep);
     }
-    return (int32_t)(s->active.size() + s->queue.size());
+    s->stats.retireMs += MsSince(tRetire);
+    return (int32_t)(s->active.size() + s->preparing.size() + s->queue.size());
 }
 
 extern "C" int32_t m3gpu_serve_poll(m3gpuServer* s, int64_t* tickets, uint64_t* hashes,
@@ -516,4 +660,21 @@ extern "C" int32_t m3gpu_serve_poll(m3gpuServer* s, int64_t* tickets, uint64_t* 
 extern "C" int32_t m3gpu_serve_active(const m3gpuServer* s)
 {
     return s == nullptr ? -1 : (int32_t)s->active.size();
+}
+
+extern "C" int32_t m3gpu_serve_stats(m3gpuServer* s, m3gpuServeStats* out)
+{
+    if (s == nullptr || out == nullptr)
+    {
+        return m3gpuSetError(M3GPU_ERR_INVALID, "m3gpu_serve_stats: null argument");
+    }
+    *out = s->stats;
+    out->heldBytes = s->heldBytes;
+    out->budget = s->budget;
+    out->queued = (int32_t)s->queue.size();
+    out->preparing = (int32_t)s->preparing.size();
+    out->active = (int32_t)s->active.size();
+    out->workers = (int32_t)s->workers.size();
+    out->prepareMs = (double)s->prepareUs.load() / 1000.0;
+    return M3GPU_OK;
 }

@@ -699,7 +699,19 @@ extern "C" bool m3World_Restore(m3WorldId worldId, const void* data, int32_t siz
 {
     m3gpuClearError();
     m3HostWorld* w = m3gpuWorldFromId(worldId);
-    if (w == nullptr || data == nullptr || size < (int32_t)sizeof(SnapshotHeader))
+    if (w == nullptr)
+    {
+        m3gpuSetError(M3GPU_ERR_INVALID, "m3World_Restore: stale world or short buffer");
+        return false;
+    }
+    return m3gpuRestoreWorld(w, data, size);
+}
+
+// The restore itself, on a world object (one of the table's, or one
+// built by m3gpuNewWorld on a serving thread).
+bool m3gpuRestoreWorld(m3HostWorld* w, const void* data, int32_t size)
+{
+    if (data == nullptr || size < (int32_t)sizeof(SnapshotHeader))
     {
         m3gpuSetError(M3GPU_ERR_INVALID, "m3World_Restore: stale world or short buffer");
         return false;

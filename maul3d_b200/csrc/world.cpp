@@ -108,10 +108,11 @@ extern "C" m3WorldDef m3DefaultWorldDef(void)
     return def;
 }
 
-extern "C" m3WorldId m3CreateWorld(const m3WorldDef* def)
+// Creation without the world table (world.c:64-460): validation, the
+// image and its initial arrays.  It touches only the new world and the
+// host memory arena, so it may run on any thread.
+m3HostWorld* m3gpuNewWorld(const m3WorldDef* def)
 {
-    m3WorldId nullId = {0, 0};
-    m3gpuClearError();
     if (def == nullptr || def->internalValue != M3_WORLD_COOKIE || def->bodyCapacity <= 0 ||
         def->shapeCapacity <= 0 || def->meshCapacity <= 0 || def->jointCapacity <= 0 ||
         def->voxelCapacity <= 0 || def->characterCapacity <= 0 || def->vehicleCapacity <= 0 ||
@@ -125,32 +126,10 @@ extern "C" m3WorldId m3CreateWorld(const m3WorldDef* def)
         !FiniteF(def->hitEventThreshold) || def->hitEventThreshold < 0.0f)
     {
         m3gpuSetError(M3GPU_ERR_INVALID, "m3CreateWorld: invalid world def");
-        return nullId;
+        return nullptr;
     }
-    int32_t slot = -1;
-    for (int32_t i = 0; i < (int32_t)s_worlds.size(); ++i)
-    {
-        if (s_worlds[i] == nullptr)
-        {
-            slot = i;
-            break;
-        }
-    }
-    if (slot < 0)
-    {
-        if ((int32_t)s_worlds.size() >= M3GPU_MAX_WORLDS)
-        {
-            m3gpuSetError(M3GPU_ERR_CAPACITY, "m3CreateWorld: world table full");
-            return nullId;
-        }
-        slot = (int32_t)s_worlds.size();
-        s_worlds.push_back(nullptr);
-        s_worldGenerations.push_back(0);
-    }
-
     m3HostWorld* w = new m3HostWorld();
-    w->slot = slot;
-    w->generation = s_worldGenerations[slot];
+    w->slot = -1;
     w->bodyCap = def->bodyCapacity;
     w->shapeCap = def->shapeCapacity;
     w->jointCap = def->jointCapacity;
@@ -214,9 +193,58 @@ extern "C" m3WorldId m3CreateWorld(const m3WorldDef* def)
         w->hv.jnextA[i] = -1;
         w->hv.jnextB[i] = -1;
     }
+    return w;
+}
+
+// Enters a world built by m3gpuNewWorld into the world table; when the
+// table is full the world is deleted and the null id returned.
+m3WorldId m3gpuAttachWorld(m3HostWorld* w)
+{
+    m3WorldId nullId = {0, 0};
+    int32_t slot = -1;
+    for (int32_t i = 0; i < (int32_t)s_worlds.size(); ++i)
+    {
+        if (s_worlds[i] == nullptr)
+        {
+            slot = i;
+            break;
+        }
+    }
+    if (slot < 0)
+    {
+        if ((int32_t)s_worlds.size() >= M3GPU_MAX_WORLDS)
+        {
+            delete w;
+            m3gpuSetError(M3GPU_ERR_CAPACITY, "m3CreateWorld: world table full");
+            return nullId;
+        }
+        slot = (int32_t)s_worlds.size();
+        s_worlds.push_back(nullptr);
+        s_worldGenerations.push_back(0);
+    }
+    w->slot = slot;
+    w->generation = s_worldGenerations[slot];
     s_worlds[slot] = w;
     m3WorldId id = {slot + 1, w->generation};
     return id;
+}
+
+// A world of m3gpuNewWorld that never entered the table (never resident).
+void m3gpuDeleteWorld(m3HostWorld* w)
+{
+    delete w;
+}
+
+extern "C" m3WorldId m3CreateWorld(const m3WorldDef* def)
+{
+    m3WorldId nullId = {0, 0};
+    m3gpuClearError();
+    m3HostWorld* w = m3gpuNewWorld(def);
+    if (w == nullptr)
+    {
+        return nullId;
+    }
+    return m3gpuAttachWorld(w);
 }
 
 extern "C" void m3DestroyWorld(m3WorldId worldId)

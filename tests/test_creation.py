@@ -9,7 +9,8 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from maul3d_b200.abi import SCENE_BOX_PYRAMID, SCENE_FREEFALL, SCENE_SPHERE_PYRAMID, SCENE_UNEVEN
+from maul3d_b200.abi import (SCENE_BOX_PYRAMID, SCENE_FREEFALL, SCENE_MIXED,
+                             SCENE_SPHERE_PYRAMID, SCENE_UNEVEN)
 
 SCENES = [
     (SCENE_SPHERE_PYRAMID, 0, 0),
@@ -18,6 +19,8 @@ SCENES = [
     (SCENE_UNEVEN, 1, 32),
     (SCENE_UNEVEN, 7, 600),
     (SCENE_UNEVEN, 5, 2048),
+    (SCENE_MIXED, 3, 200),
+    (SCENE_MIXED, 8, 1500),
 ]
 
 

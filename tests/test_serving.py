@@ -13,7 +13,7 @@ import pytest
 
 from conftest import cuda_available
 from maul3d_b200 import abi
-from maul3d_b200.abi import SCENE_TERRAIN, SCENE_TOWERS, SCENE_UNEVEN
+from maul3d_b200.abi import SCENE_MIXED, SCENE_TERRAIN, SCENE_TOWERS, SCENE_UNEVEN
 
 
 def _snapshot(lib, wid) -> bytes:
@@ -146,3 +146,114 @@ def test_unmodelled_content_completes_with_its_refusal(m3, oracle, ref):
     server.close()
     assert done[bad_t][1] == m3.M3GPU_ERR_UNSUPPORTED
     assert done[good_t] == (good[1], m3.M3GPU_OK)
+
+
+def _mixed_requests(oracle, ref, count, seed, bodies=(200, 600)):
+    """Containers of the served configuration's worlds (boxes, spheres and
+    16-point hulls on a plane), each stepped a little on the reference,
+    with the reference's hash after replaying the journal."""
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for i in range(count):
+        r = oracle.RefWorld.scene(SCENE_MIXED, 500 + i, int(rng.integers(*bodies)))
+        r.step(1.0 / 60.0, 4, int(rng.integers(1, 10)))
+        snap = _snapshot(ref, r.id)
+        journal = _journal(rng, r.body_count() - 1, int(rng.integers(4, 17)))
+        jb = (C.c_uint8 * len(journal)).from_buffer_copy(journal)
+        assert ref.m3World_JournalReplay(r.id, jb, len(journal))
+        reqs.append((abi.encode_container(ref, snap, journal, r.hash()), r.hash()))
+        r.destroy()
+    return reqs
+
+
+def test_a_stale_journal_is_refused_before_the_device(m3, oracle, ref):
+    # Preparation (world, restore, journal) runs on the worker threads; a
+    # journal naming a body the snapshot does not hold retires with
+    # M3GPU_ERR_INVALID without the device being touched, on a machine
+    # without one too.  Nothing stays held.
+    r = oracle.RefWorld.scene(SCENE_MIXED, 3, 120)
+    snap = _snapshot(ref, r.id)
+    r.destroy()
+    journal = (abi.journal_body_command(abi.OP_APPLY_LINEAR_IMPULSE, 100000, 0, [1.0, 0.0, 0.0]) +
+               abi.journal_step(1 / 60, 4))
+    container = abi.encode_container(ref, snap, journal)
+    server = m3.Server()
+    tickets = [server.submit(container) for _ in range(3)]
+    done = server.run()
+    stats = server.stats()
+    server.close()
+    assert all(done[t][1] == m3.M3GPU_ERR_INVALID for t in tickets)
+    assert stats["refused"] == 3 and stats["completed"] == 0
+    assert stats["heldBytes"] == 0 and stats["active"] == 0 and stats["preparing"] == 0
+
+
+def test_preparation_starts_only_what_the_budget_holds(m3, oracle, ref):
+    # Requests are counted against the device budget when their
+    # preparation starts: with room for two and a half of them, at most
+    # two are ever held (these are refused in preparation, so this runs
+    # without a device).
+    r = oracle.RefWorld.scene(SCENE_MIXED, 4, 300)
+    snap = _snapshot(ref, r.id)
+    r.destroy()
+    journal = (abi.journal_body_command(abi.OP_APPLY_LINEAR_IMPULSE, 100000, 0, [1.0, 0.0, 0.0]) +
+               abi.journal_step(1 / 60, 4))
+    container = abi.encode_container(ref, snap, journal)
+    one = m3.Server()
+    one.submit(container)
+    one.run()
+    size = one.stats()["peakHeldBytes"]
+    one.close()
+    assert size > 0
+    server = m3.Server(device_budget=int(2.5 * size))
+    for _ in range(6):
+        server.submit(container)
+    server.run()
+    stats = server.stats()
+    server.close()
+    assert stats["peakHeldBytes"] == 2 * size
+    assert stats["refused"] == 6 and stats["heldBytes"] == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not cuda_available(), reason="needs a CUDA device")
+def test_admission_keeps_within_the_device_budget(m3, oracle, ref):
+    # Six requests of about the same size under a budget of two and a half
+    # of them: never more than two held at once, every answer the
+    # reference's, whatever the admission order did.
+    reqs = _mixed_requests(oracle, ref, 6, 21, bodies=(300, 320))
+    one = m3.Server()
+    t = one.submit(reqs[0][0])
+    assert one.run()[t] == (reqs[0][1], m3.M3GPU_OK)
+    size = one.stats()["peakHeldBytes"]
+    one.close()
+    assert size > 0
+    server = m3.Server(device_budget=int(2.5 * size))
+    tickets = [server.submit(c) for c, _ in reqs]
+    done = server.run()
+    stats = server.stats()
+    server.close()
+    assert stats["peakHeldBytes"] <= int(2.5 * size)
+    assert stats["peakActive"] <= 2
+    assert stats["completed"] == len(reqs) and stats["heldBytes"] == 0
+    for t, (_, expected) in zip(tickets, reqs):
+        assert done[t] == (expected, m3.M3GPU_OK), f"ticket {t}"
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not cuda_available(), reason="needs a CUDA device")
+def test_served_hull_worlds_equal_the_reference(m3, oracle, ref):
+    # The served configuration's worlds (16-point QuickHull hulls, boxes,
+    # spheres) arriving while others run: submitted between ticks.
+    reqs = _mixed_requests(oracle, ref, 12, 5)
+    server = m3.Server(max_active=6)
+    tickets, done = [], {}
+    for k, (c, _) in enumerate(reqs):
+        tickets.append(server.submit(c))
+        if k % 3 == 2:
+            server.tick()
+            t, h, st = server.poll()
+            done.update({int(t[i]): (int(h[i]), int(st[i])) for i in range(len(t))})
+    done.update(server.run())
+    server.close()
+    for t, (_, expected) in zip(tickets, reqs):
+        assert done[t] == (expected, m3.M3GPU_OK), f"ticket {t}"
