@@ -412,10 +412,11 @@ def serving_run(m3, distinct: int, seed: int, rates: list[float], budget: int,
     hulls on a plane, stepped 5 steps in) plus a journal of 4-16 frames,
     each 1-8 linear impulses of 1-50 N s on random bodies and one step of
     1/60 s in 4 substeps.  Requests arrive as a Poisson process at each
-    rate (`distinct` different containers, submitted in turn; per rate
-    about one second of arrivals, 256-2048 requests; rate 0 submits
-    `distinct` at once); one server on this GPU under a device budget
-    batches every active request's frame per tick.  Latency is arrival to
+    rate (`distinct` different containers, submitted in turn from a
+    client thread; per rate about one second of arrivals, 256-2048
+    requests; rate 0 submits `distinct` at once); one server on this GPU
+    under a device budget batches every active request's frame per tick
+    on the main thread.  Latency is arrival to
     final hash.  Every answer is compared with the reference's restore +
     replay of the same container, which is also timed on the host cores
     (all at once) as the serving baseline."""
@@ -456,21 +457,28 @@ def serving_run(m3, distinct: int, seed: int, rates: list[float], budget: int,
                     else np.zeros(count))
         server = m3.Server(device_budget=budget)
         latency = np.zeros(count)
-        which = {}
-        submitted = finished = ticks = 0
+        finished = ticks = 0
         t0 = time.perf_counter()
+
+        def client():
+            # The arrivals, submitted from their own thread; request i gets
+            # ticket i + 1 (one submitter, tickets in order).
+            for i in range(count):
+                delay = arrivals[i] - (time.perf_counter() - t0)
+                if delay > 0:
+                    time.sleep(delay)
+                server.submit(containers[i % distinct])
+
+        submitter = threading.Thread(target=client)
+        submitter.start()
         while finished < count:
-            now = time.perf_counter() - t0
-            while submitted < count and arrivals[submitted] <= now:
-                which[server.submit(containers[submitted % distinct])] = submitted
-                submitted += 1
-            if server.tick() == 0 and submitted < count:
-                time.sleep(max(0.0, arrivals[submitted] - (time.perf_counter() - t0)))
+            if server.tick() == 0:
+                time.sleep(0.0002)  # nothing queued or running
             ticks += 1
             t, h, st = server.poll()
             done_at = time.perf_counter() - t0
             for k in range(len(t)):
-                i = which[int(t[k])]
+                i = int(t[k]) - 1
                 latency[i] = done_at - arrivals[i]
                 finished += 1
                 key = i % distinct
@@ -478,6 +486,7 @@ def serving_run(m3, distinct: int, seed: int, rates: list[float], budget: int,
                 if served.setdefault(key, answer) != answer:
                     mismatched_runs += 1
         wall = time.perf_counter() - t0
+        submitter.join()
         stats = server.stats()
         server.close()
         out["runs"].append({
@@ -671,6 +680,8 @@ def main() -> None:
                     help="distinct serving containers (0: no serving run)")
     ap.add_argument("--serving-budget-gb", type=int, default=16,
                     help="the server's device memory budget")
+    ap.add_argument("--serving-only", action="store_true",
+                    help="run only the serving sweep, print it and exit")
     ap.add_argument("--terrain-worlds", type=int, default=1024)
     ap.add_argument("--terrain-steps", type=int, default=20)
     ap.add_argument("--single", default="c1,c2,c5",
@@ -695,6 +706,11 @@ def main() -> None:
     local_rank = env_int("LOCAL_RANK", 0)
     torch.cuda.set_device(local_rank)
     m3.set_device(local_rank)
+    if args.serving_only:
+        print(json.dumps({"serving": serving_run(m3, args.serving_requests, args.seed + 77,
+                                                 SERVING_RATES, args.serving_budget_gb << 30,
+                                                 not args.no_cpu_baseline)}))
+        return
     if args.single_only:
         want = set(args.single.split(","))
         specs = [spec for spec in SINGLE_WORLDS if spec[0] in want]

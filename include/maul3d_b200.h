@@ -527,8 +527,10 @@ M3GPU_API int32_t m3gpu_copy_joints(m3WorldId world, void* impulse, void* perp, 
 typedef struct m3gpuServer m3gpuServer;
 M3GPU_API m3gpuServer* m3gpu_serve_create(int64_t deviceBudget, int32_t maxActive);
 M3GPU_API void m3gpu_serve_destroy(m3gpuServer* server);
-/* Queues a container; returns its ticket (> 0), or -1 for bytes that are
- * not a valid container. */
+/* Queues a container (copied); returns its ticket (> 0), or -1 for bytes
+ * that are not a valid container.  Any thread may submit, also while
+ * another thread ticks; tick, poll, active and stats belong to one
+ * thread at a time. */
 M3GPU_API int64_t m3gpu_serve_submit(m3gpuServer* server, const void* container, int32_t bytes);
 /* Admits, runs one frame, retires; returns the requests still queued or
  * active, or a negative error code. */

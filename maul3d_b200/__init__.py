@@ -316,8 +316,8 @@ class Server:
             raise M3GpuError(*last_error())
 
     def submit(self, container: bytes) -> int:
-        buf = (C.c_uint8 * len(container)).from_buffer_copy(container)
-        ticket = int(lib.m3gpu_serve_submit(self.handle, buf, len(container)))
+        # The server copies what it keeps: the bytes are passed in place.
+        ticket = int(lib.m3gpu_serve_submit(self.handle, bytes(container), len(container)))
         if ticket < 0:
             raise M3GpuError(*last_error())
         return ticket

@@ -12,12 +12,21 @@
 
 #include <string.h>
 
+#include <atomic>
 #include <map>
 #include <utility>
 #include <vector>
 
 static int s_deviceState = 0; // 0 unknown, 1 ready, -1 absent
 static int s_device = 0;
+// The device for page-locking host memory, readable from any thread
+// without the device lock: -1 until the device is ready.
+static std::atomic<int> s_lockDevice{-1};
+
+int m3gpuLockDevice(void)
+{
+    return s_lockDevice.load(std::memory_order_acquire);
+}
 
 // Bumped whenever any world's device allocations change (slab or hull
 // pool allocated, released): cached device views of a batch are valid
@@ -47,6 +56,7 @@ extern "C" int32_t m3gpu_set_device(int32_t device)
     }
     s_device = device;
     s_deviceState = 1;
+    s_lockDevice.store(device, std::memory_order_release);
     return M3GPU_OK;
 }
 
@@ -80,6 +90,7 @@ int32_t m3gpuEnsureDevice(void)
     }
     s_deviceState = 1;
     cudaSetDevice(s_device);
+    s_lockDevice.store(s_device, std::memory_order_release);
     return M3GPU_OK;
 }
 

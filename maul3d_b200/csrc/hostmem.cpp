@@ -32,7 +32,8 @@ struct Chunk
 
 struct Arena
 {
-    std::mutex mu;
+    std::mutex mu;     // chunks and free lists
+    std::mutex growMu; // held while a new chunk is made
     std::vector<Chunk> chunks;
     std::map<size_t, std::vector<void*>> freeBlocks; // by size class
 };
@@ -49,11 +50,35 @@ size_t RoundPages(size_t bytes)
 }
 } // namespace
 
-void* m3HostAlloc(size_t bytes)
+// Page-locks a chunk for the library's device (mapped too: the upload
+// kernel reads the images straight from there); false when no device is
+// up yet or the driver refuses (uploads from it then stay synchronous).
+static bool LockChunk(Chunk& c, int device)
 {
-    Arena& a = TheArena();
-    const size_t size = RoundPages(bytes);
-    std::lock_guard<std::mutex> lock(a.mu);
+    if (device < 0 || cudaSetDevice(device) != cudaSuccess ||
+        cudaHostRegister(c.base, c.bytes, cudaHostRegisterMapped | cudaHostRegisterPortable) !=
+            cudaSuccess)
+    {
+        cudaGetLastError();
+        return false;
+    }
+    c.locked = true;
+    void* dev = nullptr;
+    if (cudaHostGetDevicePointer(&dev, c.base, 0) == cudaSuccess)
+    {
+        c.deviceBase = (uint8_t*)dev;
+    }
+    else
+    {
+        cudaGetLastError();
+    }
+    return true;
+}
+
+// The free list of the block's size class, else a bump in the newest
+// chunk; null when neither has room.  Under the arena's mutex.
+static void* TakeBlock(Arena& a, size_t size)
+{
     auto it = a.freeBlocks.find(size);
     if (it != a.freeBlocks.end() && !it->second.empty())
     {
@@ -61,9 +86,7 @@ void* m3HostAlloc(size_t bytes)
         it->second.pop_back();
         return p;
     }
-    // Bump allocation in the newest chunk (older chunks' space comes back
-    // through the free lists); a block larger than a chunk gets a chunk
-    // of its own.
+    // Older chunks' space comes back through the free lists.
     if (!a.chunks.empty())
     {
         Chunk& c = a.chunks.back();
@@ -74,13 +97,46 @@ void* m3HostAlloc(size_t bytes)
             return p;
         }
     }
+    return nullptr;
+}
+
+void* m3HostAlloc(size_t bytes)
+{
+    Arena& a = TheArena();
+    const size_t size = RoundPages(bytes);
+    {
+        std::lock_guard<std::mutex> lock(a.mu);
+        if (void* p = TakeBlock(a, size))
+        {
+            return p;
+        }
+    }
+    // A new chunk, one thread at a time (the others that need one wait
+    // for it and then bump from it), made outside the arena's mutex so
+    // that allocations with room keep going meanwhile; a block larger
+    // than a chunk gets a chunk of its own.  Once the library's device
+    // is up the chunk is page-locked here, on the allocating thread,
+    // rather than by the next device reservation.
+    std::lock_guard<std::mutex> grow(a.growMu);
+    {
+        std::lock_guard<std::mutex> lock(a.mu);
+        if (void* p = TakeBlock(a, size))
+        {
+            return p;
+        }
+    }
     const size_t chunkBytes = size > kChunkBytes ? size : kChunkBytes;
     void* m = mmap(nullptr, chunkBytes, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS, -1, 0);
     if (m == MAP_FAILED)
     {
         throw std::bad_alloc();
     }
+    // Huge pages where the kernel offers them: a 2 MiB page is faulted
+    // in once instead of 512 times.
+    madvise(m, chunkBytes, MADV_HUGEPAGE);
     Chunk c{(uint8_t*)m, chunkBytes, size, false, nullptr};
+    LockChunk(c, m3gpuLockDevice());
+    std::lock_guard<std::mutex> lock(a.mu);
     a.chunks.push_back(c);
     return m;
 }
@@ -99,31 +155,13 @@ void m3HostFree(void* p, size_t bytes)
 int32_t m3HostLockAll(void)
 {
     Arena& a = TheArena();
+    const int device = m3gpuLockDevice();
     std::lock_guard<std::mutex> lock(a.mu);
     for (Chunk& c : a.chunks)
     {
-        if (c.locked)
+        if (!c.locked)
         {
-            continue;
-        }
-        // Mapped too: the upload kernel reads the images straight from here.
-        if (cudaHostRegister(c.base, c.bytes, cudaHostRegisterMapped | cudaHostRegisterPortable) ==
-            cudaSuccess)
-        {
-            c.locked = true;
-            void* dev = nullptr;
-            if (cudaHostGetDevicePointer(&dev, c.base, 0) == cudaSuccess)
-            {
-                c.deviceBase = (uint8_t*)dev;
-            }
-            else
-            {
-                cudaGetLastError();
-            }
-        }
-        else
-        {
-            cudaGetLastError(); // not fatal: uploads from it stay synchronous
+            LockChunk(c, device);
         }
     }
     return M3GPU_OK;

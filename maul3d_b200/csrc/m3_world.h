@@ -37,6 +37,9 @@ void* m3HostAlloc(size_t bytes);
 void m3HostFree(void* p, size_t bytes);
 // Page-lock every chunk not locked yet (one driver call per chunk).
 int32_t m3HostLockAll(void);
+// The library's device once it is up (page-locking host memory on any
+// thread), else -1 (device.cpp).
+int m3gpuLockDevice(void);
 // Whether [p, p + bytes) lies in a locked chunk.
 bool m3HostIsLocked(const void* p, size_t bytes);
 // The device's address of [p, p + bytes) when it lies in a locked (and

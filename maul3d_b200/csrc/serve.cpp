@@ -4,8 +4,9 @@
 // the end of the journal, what a verifier compares against the
 // container's recorded final hash.
 //
-// A request moves through three sets.  Queued: submitted, waiting for
-// room.  Preparing: its device memory counted against the budget, a
+// Clients submit from any thread (the container is copied on theirs);
+// one thread ticks.  A request moves through three sets.  Queued:
+// submitted, waiting for room.  Preparing: its device memory counted against the budget, a
 // worker thread builds its world off the world table, restores the
 // snapshot into it and parses and validates the journal whole.
 // Active: entered into the world table and reserved on the device.  Each
@@ -236,7 +237,11 @@ struct m3gpuServer
 {
     int64_t budget = 0;
     int32_t maxActive = 0;
+    // Submissions, from any thread: tickets and the inbox under inboxMu;
+    // each tick moves the inbox to the queue.
+    std::mutex inboxMu;
     int64_t nextTicket = 1;
+    std::deque<std::unique_ptr<Request>> inbox;
     int64_t heldBytes = 0; // device bytes of preparing and active requests
     std::deque<std::unique_ptr<Request>> queue;
     std::deque<std::unique_ptr<Request>> preparing; // submission order
@@ -509,15 +514,16 @@ extern "C" int64_t m3gpu_serve_submit(m3gpuServer* s, const void* container, int
         m3gpuSetError(M3GPU_ERR_INVALID, "m3gpu_serve_submit: not a replay container");
         return -1;
     }
+    // The copy happens on the caller's thread, outside the server's locks.
     std::unique_ptr<Request> r(new Request());
-    r->ticket = s->nextTicket++;
     const uint8_t* snap = (const uint8_t*)view.snapshot;
     const uint8_t* jour = (const uint8_t*)view.journal;
     r->snapshot.assign(snap, snap + view.snapshotBytes);
     r->journal.assign(jour, jour + view.journalBytes);
+    std::lock_guard<std::mutex> lock(s->inboxMu);
+    r->ticket = s->nextTicket++;
     const int64_t ticket = r->ticket;
-    s->queue.push_back(std::move(r));
-    s->stats.submitted += 1;
+    s->inbox.push_back(std::move(r));
     return ticket;
 }
 
@@ -529,6 +535,16 @@ extern "C" int32_t m3gpu_serve_tick(m3gpuServer* s)
         return m3gpuSetError(M3GPU_ERR_INVALID, "m3gpu_serve_tick: null server");
     }
     s->stats.ticks += 1;
+    {
+        // Requests submitted since the last tick, from any thread.
+        std::lock_guard<std::mutex> lock(s->inboxMu);
+        s->stats.submitted += (int64_t)s->inbox.size();
+        for (std::unique_ptr<Request>& r : s->inbox)
+        {
+            s->queue.push_back(std::move(r));
+        }
+        s->inbox.clear();
+    }
     Start(s);
     Admit(s);
     Start(s); // room freed by refusals
@@ -633,7 +649,8 @@ extern "C" int32_t m3gpu_serve_tick(m3gpuServer* s)
         s->active.swap(keep);
     }
     s->stats.retireMs += MsSince(tRetire);
-    return (int32_t)(s->active.size() + s->preparing.size() + s->queue.size());
+    std::lock_guard<std::mutex> lock(s->inboxMu);
+    return (int32_t)(s->active.size() + s->preparing.size() + s->queue.size() + s->inbox.size());
 }
 
 extern "C" int32_t m3gpu_serve_poll(m3gpuServer* s, int64_t* tickets, uint64_t* hashes,
@@ -671,7 +688,10 @@ extern "C" int32_t m3gpu_serve_stats(m3gpuServer* s, m3gpuServeStats* out)
     *out = s->stats;
     out->heldBytes = s->heldBytes;
     out->budget = s->budget;
-    out->queued = (int32_t)s->queue.size();
+    {
+        std::lock_guard<std::mutex> lock(s->inboxMu);
+        out->queued = (int32_t)(s->queue.size() + s->inbox.size());
+    }
     out->preparing = (int32_t)s->preparing.size();
     out->active = (int32_t)s->active.size();
     out->workers = (int32_t)s->workers.size();

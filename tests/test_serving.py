@@ -257,3 +257,34 @@ def test_served_hull_worlds_equal_the_reference(m3, oracle, ref):
     server.close()
     for t, (_, expected) in zip(tickets, reqs):
         assert done[t] == (expected, m3.M3GPU_OK), f"ticket {t}"
+
+
+def test_submissions_from_another_thread_are_all_answered(m3, oracle, ref):
+    # A client thread submits while this thread ticks; every ticket comes
+    # back once (refused in preparation here, so no device is needed).
+    import threading
+    r = oracle.RefWorld.scene(SCENE_MIXED, 6, 60)
+    snap = _snapshot(ref, r.id)
+    r.destroy()
+    journal = (abi.journal_body_command(abi.OP_APPLY_LINEAR_IMPULSE, 100000, 0, [1.0, 0.0, 0.0]) +
+               abi.journal_step(1 / 60, 4))
+    container = abi.encode_container(ref, snap, journal)
+    server = m3.Server()
+    tickets = []
+    client = threading.Thread(target=lambda: tickets.extend(server.submit(container)
+                                                            for _ in range(40)))
+    client.start()
+    seen = {}
+    while client.is_alive() or server.tick() > 0:
+        server.tick()
+        t, h, st = server.poll()
+        for k in range(len(t)):
+            assert int(t[k]) not in seen
+            seen[int(t[k])] = int(st[k])
+    client.join()
+    server.tick()
+    t, h, st = server.poll()
+    seen.update({int(t[k]): int(st[k]) for k in range(len(t))})
+    server.close()
+    assert sorted(seen) == sorted(tickets) == list(range(1, 41))
+    assert set(seen.values()) == {m3.M3GPU_ERR_INVALID}
