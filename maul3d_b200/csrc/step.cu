@@ -4133,6 +4133,10 @@ static void LaunchClass(int32_t stage, int32_t c, cudaStream_t stream, const m3W
 #undef M3_LAUNCH_CLASS
 }
 
+// The dynamic shared memory each class's kernels were last allowed
+// (0: never set, the default of 48 KB for static and dynamic together).
+static int32_t s_classSmemSet[M3_CLASSES] = {0, 0, 0};
+
 static int32_t SetClassSmem(int32_t c, int32_t bytes)
 {
     cudaError_t e = cudaSuccess;
@@ -4166,7 +4170,18 @@ static int32_t SetClassSmem(int32_t c, int32_t bytes)
         return m3gpuSetError(M3GPU_ERR_CUDA, "cudaFuncSetAttribute(class smem): %s",
                              cudaGetErrorString(e));
     }
+    s_classSmemSet[c] = bytes;
     return M3GPU_OK;
+}
+
+// Allows a class's kernels `bytes` of dynamic shared memory, raising the
+// limit when a launch needs more than it was last set to.  Always set,
+// never left to the default: the default's 48 KB covers the kernels'
+// static shared memory too, so a launch just under 48 KB of dynamic
+// shared memory would not fit it.
+static int32_t EnsureClassSmem(int32_t c, int32_t bytes)
+{
+    return bytes > s_classSmemSet[c] ? SetClassSmem(c, bytes) : M3GPU_OK;
 }
 
 // Streams for the classes (they run side by side), and the events that
@@ -4395,10 +4410,7 @@ static int32_t PrepareBatch(m3HostWorld** worlds, int32_t count)
         cWant = cWant < cap ? cWant : cap;
         cWant = cWant < limit ? cWant : limit;
         s_batch.classCache[k] = (int32_t)cWant;
-        if (cWant > 48 * 1024)
-        {
-            rc = SetClassSmem(k, (int32_t)cWant);
-        }
+        rc = EnsureClassSmem(k, (int32_t)cWant);
     }
     return rc;
 }
@@ -5440,6 +5452,12 @@ extern "C" int32_t m3gpu_step_world_noalloc(m3WorldId worldId, float dt, int32_t
     int32_t* order = sym.table;
     int32_t* offsets = sym.table + 1;
     const int32_t cacheBytes = (int32_t)cache;
+    // The 256-thread kernels (size class 1) run this world.
+    rc = EnsureClassSmem(1, cacheBytes);
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
     // Tree replays of earlier regular steps first; this call replays its
     // own moves in order on the default stream, and moves leaves the
     // slab scratch's copy of their bounds does not see.
