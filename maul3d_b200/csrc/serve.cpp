@@ -180,6 +180,7 @@ struct Request
     int64_t deviceBytes = 0;
     int32_t code = M3GPU_OK; // the preparation's refusal
     bool ready = false;      // prepared (under the server's mutex)
+    bool suspect = false;    // a step of its batch reported a refusal
 };
 
 struct Completion
@@ -396,30 +397,39 @@ void Start(m3gpuServer* s)
     }
 }
 
-// Admits prepared requests in submission order (the first one still
-// being prepared stops it; with nothing active it is waited for): each
-// enters the world table and is reserved on the device.
+// Admits every prepared request (in submission order among them; one
+// still being prepared holds up nobody behind it, and with nothing active
+// the oldest is waited for): each enters the world table and is reserved
+// on the device.  Results do not depend on the order of admission.
 void Admit(m3gpuServer* s)
 {
-    while (!s->preparing.empty())
+    std::vector<std::unique_ptr<Request>> ready;
     {
-        Request* front = s->preparing.front().get();
+        std::unique_lock<std::mutex> lock(s->mu);
+        if (s->active.empty() && !s->preparing.empty() && !s->preparing.front()->ready)
         {
-            std::unique_lock<std::mutex> lock(s->mu);
-            if (!front->ready)
+            const auto t0 = std::chrono::steady_clock::now();
+            Request* front = s->preparing.front().get();
+            s->prepared.wait(lock, [front] { return front->ready; });
+            s->stats.waitMs += MsSince(t0);
+        }
+        std::deque<std::unique_ptr<Request>> waiting;
+        for (std::unique_ptr<Request>& r : s->preparing)
+        {
+            if (r->ready)
             {
-                if (!s->active.empty())
-                {
-                    return;
-                }
-                const auto t0 = std::chrono::steady_clock::now();
-                s->prepared.wait(lock, [front] { return front->ready; });
-                s->stats.waitMs += MsSince(t0);
+                ready.push_back(std::move(r));
+            }
+            else
+            {
+                waiting.push_back(std::move(r));
             }
         }
-        const auto t0 = std::chrono::steady_clock::now();
-        std::unique_ptr<Request> r = std::move(s->preparing.front());
-        s->preparing.pop_front();
+        s->preparing.swap(waiting);
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    for (std::unique_ptr<Request>& r : ready)
+    {
         int32_t code = r->code;
         if (code == M3GPU_OK)
         {
@@ -446,8 +456,8 @@ void Admit(m3gpuServer* s)
         {
             s->active.push_back(std::move(r));
         }
-        s->stats.admitMs += MsSince(t0);
     }
+    s->stats.admitMs += MsSince(t0);
 }
 } // namespace
 
@@ -605,6 +615,15 @@ extern "C" int32_t m3gpu_serve_tick(m3gpuServer* s)
         {
             return rc;
         }
+        if (rc != M3GPU_OK)
+        {
+            // Some world of the batch refused: its requests read their
+            // own status when they retire (the others are known good).
+            for (size_t i : g.second)
+            {
+                s->active[i]->suspect = true;
+            }
+        }
     }
 
     s->stats.stepMs += MsSince(tStep);
@@ -633,7 +652,7 @@ extern "C" int32_t m3gpu_serve_tick(m3gpuServer* s)
         for (size_t f = 0; f < finished.size(); ++f)
         {
             std::unique_ptr<Request>& r = s->active[finishedAt[f]];
-            const int32_t status = m3gpuWorldStatus(finished[f]);
+            const int32_t status = r->suspect ? m3gpuWorldStatus(finished[f]) : M3GPU_OK;
             s->heldBytes -= r->deviceBytes;
             Retire(s, r, status == M3GPU_OK ? hashes[f] : 0, status);
         }
