@@ -357,6 +357,7 @@ def terrain_run(m3, args, seed: int) -> dict:
 
 
 SERVING_RATES = [100.0, 1000.0, 4000.0, 20000.0, 0.0]
+SERVING_CLIENTS = 4
 
 
 def reference_serving(containers, caps, threads: int) -> tuple[float, list[int]]:
@@ -412,8 +413,8 @@ def serving_run(m3, distinct: int, seed: int, rates: list[float], budget: int,
     hulls on a plane, stepped 5 steps in) plus a journal of 4-16 frames,
     each 1-8 linear impulses of 1-50 N s on random bodies and one step of
     1/60 s in 4 substeps.  Requests arrive as a Poisson process at each
-    rate (`distinct` different containers, submitted in turn from a
-    client thread; per rate about one second of arrivals, 256-2048
+    rate (`distinct` different containers, submitted in turn from four
+    client threads; per rate about one second of arrivals, 256-2048
     requests; rate 0 submits `distinct` at once); one server on this GPU
     under a device budget batches every active request's frame per tick
     on the main thread.  Latency is arrival to
@@ -467,35 +468,45 @@ def serving_run(m3, distinct: int, seed: int, rates: list[float], budget: int,
         server = m3.Server(device_budget=budget)
         latency = np.zeros(count)
         finished = ticks = 0
+        index_of = {}
+        lock = threading.Lock()
         t0 = time.perf_counter()
 
-        def client():
-            # The arrivals, submitted from their own thread; request i gets
-            # ticket i + 1 (one submitter, tickets in order).
-            for i in range(count):
+        def client(part):
+            # Arrivals part, part + CLIENTS, ...: submitted from their own
+            # thread at their arrival times (the container copy happens in
+            # the submitting thread, as a network thread's would).
+            for i in range(part, count, SERVING_CLIENTS):
                 delay = arrivals[i] - (time.perf_counter() - t0)
                 if delay > 0:
                     time.sleep(delay)
-                server.submit(containers[i % distinct])
+                ticket = server.submit(containers[i % distinct])
+                with lock:
+                    index_of[ticket] = i
 
-        submitter = threading.Thread(target=client)
-        submitter.start()
+        clients = [threading.Thread(target=client, args=(k,)) for k in range(SERVING_CLIENTS)]
+        for c in clients:
+            c.start()
+        pending = []  # (ticket, done_at, answer) polled before the ticket was recorded
         while finished < count:
             if server.tick() == 0:
                 time.sleep(0.0002)  # nothing queued or running
             ticks += 1
             t, h, st = server.poll()
             done_at = time.perf_counter() - t0
-            for k in range(len(t)):
-                i = int(t[k]) - 1
-                latency[i] = done_at - arrivals[i]
+            pending.extend((int(t[k]), done_at, int(h[k]) if int(st[k]) == 0 else -int(st[k]))
+                           for k in range(len(t)))
+            with lock:
+                resolved = [(index_of[tk], at, ans) for tk, at, ans in pending if tk in index_of]
+                pending = [p for p in pending if p[0] not in index_of]
+            for i, at, answer in resolved:
+                latency[i] = at - arrivals[i]
                 finished += 1
-                key = i % distinct
-                answer = int(h[k]) if int(st[k]) == 0 else -int(st[k])
-                if served.setdefault(key, answer) != answer:
+                if served.setdefault(i % distinct, answer) != answer:
                     mismatched_runs += 1
         wall = time.perf_counter() - t0
-        submitter.join()
+        for c in clients:
+            c.join()
         stats = server.stats()
         server.close()
         out["runs"].append({
