@@ -358,6 +358,10 @@ def terrain_run(m3, args, seed: int) -> dict:
 
 SERVING_RATES = [100.0, 1000.0, 4000.0, 20000.0, 0.0]
 SERVING_CLIENTS = 4
+# At most this many requests preparing or active: a tick steps every
+# active request's frame, so the cap bounds a tick's time (and with it the
+# latency of everything in flight); bursts wait in the queue.
+SERVING_MAX_ACTIVE = 256
 
 
 def reference_serving(containers, caps, threads: int) -> tuple[float, list[int]]:
@@ -450,12 +454,13 @@ def serving_run(m3, distinct: int, seed: int, rates: list[float], budget: int,
     out = {"workload": f"{distinct} distinct containers: worlds of 200-5000 bodies "
                        "(log-uniform; boxes, spheres, 16-point hulls), 4-16 frames of 1-8 "
                        "impulses of 1-50 N s, 4 substeps",
-           "device_budget_bytes": budget, "runs": []}
+           "device_budget_bytes": budget, "max_active": SERVING_MAX_ACTIVE,
+           "clients": SERVING_CLIENTS, "runs": []}
     served = {}
     mismatched_runs = 0
     # Untimed warm-up: every distinct container once, all at once (a
     # long-running server's host and device memory pools are warm).
-    warm = m3.Server(device_budget=budget)
+    warm = m3.Server(device_budget=budget, max_active=SERVING_MAX_ACTIVE)
     for c in containers:
         warm.submit(c)
     for ticket, (h, st) in warm.run().items():
@@ -465,7 +470,7 @@ def serving_run(m3, distinct: int, seed: int, rates: list[float], budget: int,
         count = distinct if rate <= 0 else int(min(2048, max(256, rate)))
         arrivals = (np.cumsum(rng.exponential(1.0 / rate, count)) if rate > 0
                     else np.zeros(count))
-        server = m3.Server(device_budget=budget)
+        server = m3.Server(device_budget=budget, max_active=SERVING_MAX_ACTIVE)
         latency = np.zeros(count)
         finished = ticks = 0
         index_of = {}

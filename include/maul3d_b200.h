@@ -512,6 +512,21 @@ M3GPU_API int32_t m3gpu_copy_pairs(m3WorldId world, uint64_t* keys, void* manifo
 M3GPU_API int32_t m3gpu_copy_joints(m3WorldId world, void* impulse, void* perp, void* limit,
                                     void* angular, int32_t cap);
 
+/* Device snapshot slots: copies of a world's device state kept in HBM for
+ * rollback (save a frame, step on, restore it, step again) without a host
+ * snapshot, a restore or an upload.  m3gpu_slots_reserve allocates
+ * `slots` slots (0 frees them; either frees the slots held before);
+ * m3gpu_slot_save copies the world's state into a slot, after uploading
+ * pending host changes; m3gpu_slot_restore copies it back.  A restored
+ * world steps, hashes and snapshots exactly as the world did after the
+ * save (and as m3World_Restore of a snapshot taken then would).  A slot
+ * is void once a body, shape or joint is created in the world or a
+ * snapshot is restored into it (M3GPU_ERR_INVALID).  Saves and restores
+ * are ordered with the steps on the device and return without waiting. */
+M3GPU_API int32_t m3gpu_slots_reserve(m3WorldId world, int32_t slots);
+M3GPU_API int32_t m3gpu_slot_save(m3WorldId world, int32_t slot);
+M3GPU_API int32_t m3gpu_slot_restore(m3WorldId world, int32_t slot);
+
 /* Serving: replay containers in, final world hashes out.  A server
  * admits queued requests while their device memory fits `deviceBudget`
  * bytes (and at most `maxActive` at once, preparing and active): worker

@@ -74,6 +74,9 @@ def _load() -> C.CDLL:
     lib.m3gpu_serve_active.restype = C.c_int32
     lib.m3gpu_serve_stats.argtypes = [C.c_void_p, C.POINTER(abi.m3gpuServeStats)]
     lib.m3gpu_serve_stats.restype = C.c_int32
+    for name in ("m3gpu_slots_reserve", "m3gpu_slot_save", "m3gpu_slot_restore"):
+        getattr(lib, name).argtypes = [abi.m3WorldId, C.c_int32]
+        getattr(lib, name).restype = C.c_int32
     lib.m3gpu_set_device.argtypes = [C.c_int32]
     lib.m3gpu_set_device.restype = C.c_int32
     for name in ("m3gpu_reserve_worlds", "m3gpu_upload_worlds"):
@@ -162,6 +165,16 @@ class World:
 
     def destroy(self) -> None:
         lib.m3DestroyWorld(self.id)
+
+    def reserve_slots(self, slots: int) -> None:
+        """Device snapshot slots in HBM (m3gpu_slots_reserve)."""
+        _check(lib.m3gpu_slots_reserve(self.id, slots))
+
+    def save_slot(self, slot: int) -> None:
+        _check(lib.m3gpu_slot_save(self.id, slot))
+
+    def restore_slot(self, slot: int) -> None:
+        _check(lib.m3gpu_slot_restore(self.id, slot))
 
     def body_count(self) -> int:
         return int(lib.m3gpu_body_max(self.id))

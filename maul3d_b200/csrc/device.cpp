@@ -746,6 +746,17 @@ int32_t m3gpuSyncHost(m3HostWorld* w)
     return m3gpuDownload(w);
 }
 
+static void FreeSlots(m3HostWorld* w)
+{
+    if (w->dslots != nullptr)
+    {
+        DevFree(w->dslots, (size_t)w->persistentBytes * (size_t)w->slotCount);
+        w->dslots = nullptr;
+    }
+    w->slotCount = 0;
+    w->slots.clear();
+}
+
 void m3gpuRelease(m3HostWorld* w)
 {
     M3_DEVICE_GUARD;
@@ -778,6 +789,143 @@ void m3gpuRelease(m3HostWorld* w)
     }
     w->dhfBytes = 0;
     w->dhfVersion = 0;
+    FreeSlots(w);
     w->hostDirty = true;
     w->deviceAhead = false;
+}
+
+// ---------------------------------------------------------------------
+// Device snapshot slots: the slab's persistent part (everything a step
+// reads and writes that outlives the step) copied within HBM, with the
+// host state a step can change beside it.  The step's scratch needs no
+// copy: a step rebuilds it, but for the tree's pending moves (replayed
+// before a save and before a restore) and the leaves' bounds (rebuilt
+// after a restore).
+// ---------------------------------------------------------------------
+static m3HostWorld* SlotWorld(m3WorldId world, int32_t slot, const char* what)
+{
+    m3HostWorld* w = m3gpuWorldFromId(world);
+    if (w == nullptr || slot < 0 || slot >= w->slotCount)
+    {
+        m3gpuSetError(M3GPU_ERR_INVALID, "%s: stale world or slot out of range", what);
+        return nullptr;
+    }
+    return w;
+}
+
+extern "C" int32_t m3gpu_slots_reserve(m3WorldId world, int32_t slots)
+{
+    M3_DEVICE_GUARD;
+    m3gpuClearError();
+    m3HostWorld* w = m3gpuWorldFromId(world);
+    if (w == nullptr || slots < 0)
+    {
+        return m3gpuSetError(M3GPU_ERR_INVALID, "m3gpu_slots_reserve: stale world or bad count");
+    }
+    int32_t rc = m3gpuEnsureDevice();
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
+    if (w->dslots != nullptr)
+    {
+        cudaDeviceSynchronize(); // no save or restore may still use them
+        FreeSlots(w);
+    }
+    if (slots == 0)
+    {
+        return M3GPU_OK;
+    }
+    rc = CudaCheck(DevAlloc((void**)&w->dslots, (size_t)w->persistentBytes * (size_t)slots),
+                   "allocate device snapshot slots");
+    if (rc != M3GPU_OK)
+    {
+        w->dslots = nullptr;
+        return rc;
+    }
+    w->slotCount = slots;
+    w->slots.assign((size_t)slots, m3HostWorld::DeviceSlot());
+    return M3GPU_OK;
+}
+
+extern "C" int32_t m3gpu_slot_save(m3WorldId world, int32_t slot)
+{
+    M3_DEVICE_GUARD;
+    m3gpuClearError();
+    m3HostWorld* w = SlotWorld(world, slot, "m3gpu_slot_save");
+    if (w == nullptr)
+    {
+        return M3GPU_ERR_INVALID;
+    }
+    int32_t rc = m3gpuEnsureDevice();
+    // The device copy must be the world: host changes uploaded, the
+    // tree's recorded moves replayed.
+    if (rc == M3GPU_OK && (w->dslab == nullptr || w->hostDirty))
+    {
+        rc = m3gpuUpload(w);
+    }
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
+    m3gpuWaitTree(w);
+    const size_t bytes = (size_t)w->persistentBytes;
+    rc = CudaCheck(cudaMemcpyAsync(w->dslots + bytes * (size_t)slot, w->dslab, bytes,
+                                   cudaMemcpyDeviceToDevice, 0),
+                   "save device snapshot slot");
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
+    m3HostWorld::DeviceSlot& d = w->slots[(size_t)slot];
+    d.valid = true;
+    d.structure = w->structure;
+    d.jointFree = w->jointFree;
+    d.brokenDrained = w->brokenDrained;
+    return M3GPU_OK;
+}
+
+extern "C" int32_t m3gpu_slot_restore(m3WorldId world, int32_t slot)
+{
+    M3_DEVICE_GUARD;
+    m3gpuClearError();
+    m3HostWorld* w = SlotWorld(world, slot, "m3gpu_slot_restore");
+    if (w == nullptr)
+    {
+        return M3GPU_ERR_INVALID;
+    }
+    const m3HostWorld::DeviceSlot& d = w->slots[(size_t)slot];
+    if (!d.valid || d.structure != w->structure || w->dslab == nullptr)
+    {
+        return m3gpuSetError(M3GPU_ERR_INVALID,
+                             "m3gpu_slot_restore: slot %d is empty, or the world was built on "
+                             "or restored since it was saved",
+                             slot);
+    }
+    int32_t rc = m3gpuEnsureDevice();
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
+    // Replays of the current timeline write the slab: they finish first.
+    m3gpuWaitTree(w);
+    const size_t bytes = (size_t)w->persistentBytes;
+    rc = CudaCheck(cudaMemcpyAsync(w->dslab, w->dslots + bytes * (size_t)slot, bytes,
+                                   cudaMemcpyDeviceToDevice, 0),
+                   "restore device snapshot slot");
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
+    w->jointFree = d.jointFree;
+    w->brokenDrained = d.brokenDrained;
+    // The device holds the world now; the host image is read back when
+    // needed, the pair arrays whole.
+    w->deviceAhead = true;
+    w->hostDirty = false;
+    w->pairTailsToDevice = false;
+    w->pairTailsOnDevice = true;
+    w->leafBoxValid = false;
+    m3JournalUnrecordable(w); // a rewind is not a command of the journal
+    return M3GPU_OK;
 }

@@ -235,6 +235,24 @@ struct m3HostWorld
     bool pairTailsToDevice = false;
     bool pairTailsOnDevice = false;
     m3StepProfile profile;
+
+    // Device snapshot slots (m3gpu_slots_reserve): `slotCount` copies of
+    // the slab's persistent part, one after another from `dslots`, and
+    // per slot the host state a step can change (joint slots freed by
+    // breakage and drained into the free queue) and the structure it
+    // belongs to.  `structure` counts the host's structural changes:
+    // bodies, shapes and joints created, snapshots restored.
+    struct DeviceSlot
+    {
+        bool valid = false;
+        uint64_t structure = 0;
+        m3FreeRing jointFree;
+        int32_t brokenDrained = 0;
+    };
+    uint8_t* dslots = nullptr;
+    int32_t slotCount = 0;
+    std::vector<DeviceSlot> slots;
+    uint64_t structure = 0;
     // The steps whose moves sit in the ring, oldest first: for each, the
     // sequence number of the tree launch replaying it (0 while no launch
     // covers it yet; those are the newest `treeUnlaunched` entries); and

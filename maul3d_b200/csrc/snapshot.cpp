@@ -998,7 +998,9 @@ bool m3gpuRestoreWorld(m3HostWorld* w, const void* data, int32_t size)
     w->hfVersion += 1;
     w->hfAtRestore = w->hfHeaders.size();
     // The image on the host is now the world; the next step uploads it,
-    // the pair arrays in full.
+    // the pair arrays in full.  Device snapshot slots saved before are
+    // void.
+    w->structure += 1;
     w->deviceAhead = false;
     w->hostDirty = true;
     w->pairTailsToDevice = true;

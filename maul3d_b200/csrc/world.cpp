@@ -370,6 +370,7 @@ extern "C" m3BodyId m3CreateBody(m3WorldId worldId, const m3BodyDef* def)
     v.jointHead[i] = -1;
     w->hostDirty = true;
     m3JournalUnrecordable(w); // creation is not recorded by this path
+    w->structure += 1;        // device snapshot slots saved before are void
     m3BodyId id = {i + 1, (uint16_t)w->slot, v.bodyGen[i]};
     return id;
 }
@@ -1001,6 +1002,7 @@ static m3ShapeId CreateShapeCommon(m3BodyId bodyId, const m3ShapeDef* def, uint8
     RecomputeMass(w, b);
     w->hostDirty = true;
     m3JournalUnrecordable(w); // creation is not recorded by this path
+    w->structure += 1;        // device snapshot slots saved before are void
     m3ShapeId id = {s + 1, (uint16_t)w->slot, v.shapeGen[s]};
     return id;
 }
@@ -1384,6 +1386,7 @@ extern "C" m3JointId m3CreateJoint(const m3JointDef* def)
     }
     w->hostDirty = true;
     m3JournalUnrecordable(w); // creation is not recorded by this path
+    w->structure += 1;        // device snapshot slots saved before are void
     m3JointId id = {j + 1, (uint16_t)w->slot, v.jointGen[j]};
     return id;
 }
