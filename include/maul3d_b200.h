@@ -512,6 +512,25 @@ M3GPU_API int32_t m3gpu_copy_pairs(m3WorldId world, uint64_t* keys, void* manifo
 M3GPU_API int32_t m3gpu_copy_joints(m3WorldId world, void* impulse, void* perp, void* limit,
                                     void* angular, int32_t cap);
 
+/* Body commands applied on the device before one step of the worlds:
+ * each as the reference's m3Body_SetLinearVelocity / SetAngularVelocity /
+ * ApplyForce / ApplyTorque / ApplyLinearImpulse / ApplyAngularImpulse
+ * call would (a stale body or a non-finite vector is a no-op; forces,
+ * torques and impulses reach dynamic bodies with mass only), in list
+ * order, without reading the worlds back to the host.  `world` indexes
+ * the call's world list; `op` is the command's journal record op (4, 5,
+ * 26, 27, 28, 29). */
+typedef struct m3gpuBodyCommand
+{
+    int32_t world;
+    int32_t op;
+    m3BodyId body;
+    m3Vec3 v;
+} m3gpuBodyCommand;
+M3GPU_API int32_t m3gpu_step_worlds_commands(const m3WorldId* worlds, int32_t count, float dt,
+                                             int32_t substeps, const m3gpuBodyCommand* commands,
+                                             int32_t commandCount);
+
 /* Device snapshot slots: copies of a world's device state kept in HBM for
  * rollback (save a frame, step on, restore it, step again) without a host
  * snapshot, a restore or an upload.  m3gpu_slots_reserve allocates

@@ -74,6 +74,10 @@ def _load() -> C.CDLL:
     lib.m3gpu_serve_active.restype = C.c_int32
     lib.m3gpu_serve_stats.argtypes = [C.c_void_p, C.POINTER(abi.m3gpuServeStats)]
     lib.m3gpu_serve_stats.restype = C.c_int32
+    lib.m3gpu_step_worlds_commands.argtypes = [C.POINTER(abi.m3WorldId), C.c_int32, C.c_float,
+                                               C.c_int32, C.POINTER(abi.m3gpuBodyCommand),
+                                               C.c_int32]
+    lib.m3gpu_step_worlds_commands.restype = C.c_int32
     for name in ("m3gpu_slots_reserve", "m3gpu_slot_save", "m3gpu_slot_restore"):
         getattr(lib, name).argtypes = [abi.m3WorldId, C.c_int32]
         getattr(lib, name).restype = C.c_int32
@@ -213,6 +217,16 @@ class World:
 def step_worlds(worlds, dt: float = 1.0 / 60.0, substeps: int = 4, steps: int = 1) -> None:
     """Step many worlds in one batched launch sequence (one block per world)."""
     _check(lib.m3gpu_step_worlds(_ids(worlds), len(worlds), dt, substeps, steps))
+
+
+def step_worlds_commands(worlds, commands, dt: float = 1.0 / 60.0, substeps: int = 4) -> None:
+    """Body commands on the device, then one step (m3gpu_step_worlds_commands).
+    `commands`: (world index, op, m3BodyId, (x, y, z)) tuples."""
+    arr = (abi.m3gpuBodyCommand * max(len(commands), 1))()
+    for k, (wi, op, body, v) in enumerate(commands):
+        arr[k] = abi.m3gpuBodyCommand(wi, op, body, abi.m3Vec3(*v))
+    _check(lib.m3gpu_step_worlds_commands(_ids(worlds), len(worlds), dt, substeps, arr,
+                                          len(commands)))
 
 
 def hash_worlds(worlds) -> np.ndarray:

@@ -87,6 +87,11 @@ class m3gpuServeStats(C.Structure):
             "prepareMs", "admitMs", "stepMs", "retireMs", "waitMs")])
 
 
+class m3gpuBodyCommand(C.Structure):
+    """A body command applied on the device (m3gpu_step_worlds_commands)."""
+    _fields_ = [("world", C.c_int32), ("op", C.c_int32), ("body", m3BodyId), ("v", m3Vec3)]
+
+
 assert C.sizeof(m3Counters) == 88 and C.sizeof(m3Profile) == 44
 assert C.sizeof(m3gpuServeStats) == 120
 

@@ -9,6 +9,7 @@
 
 #include <cuda_runtime.h>
 
+#include <math.h>
 #include <stdarg.h>
 #include <stdio.h>
 #include <string.h>
@@ -218,6 +219,70 @@ extern "C" int32_t m3gpu_step_worlds(const m3WorldId* worlds, int32_t count, flo
         for (m3HostWorld* w : ws)
         {
             RecordSteps(w, dt, substeps, steps);
+        }
+    }
+    return rc;
+}
+
+// Body commands on the device, then one step (body.c:818-1014 for the
+// commands' rules, as m3Body_Apply* / m3Body_Set*Velocity give them): a
+// stale body or a non-finite vector is a no-op; forces, torques and
+// impulses reach dynamic bodies with mass only.  Recorded in an active
+// journal like the calls they replace.
+extern "C" int32_t m3gpu_step_worlds_commands(const m3WorldId* worlds, int32_t count, float dt,
+                                              int32_t substeps, const m3gpuBodyCommand* commands,
+                                              int32_t commandCount)
+{
+    m3gpuClearError();
+    if (!(dt > 0.0f) || substeps < 1 || substeps > M3_MAX_SUBSTEPS || commandCount < 0 ||
+        (commandCount > 0 && commands == nullptr))
+    {
+        return m3gpuSetError(M3GPU_ERR_INVALID, "invalid dt, substeps or commands");
+    }
+    std::vector<m3HostWorld*> ws;
+    int32_t rc = Resolve(worlds, count, ws);
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
+    std::vector<m3BodyOp> ops;
+    ops.reserve((size_t)commandCount);
+    for (int32_t k = 0; k < commandCount; ++k)
+    {
+        const m3gpuBodyCommand& c = commands[k];
+        if (c.world < 0 || c.world >= count || !m3IsBodyOp(c.op))
+        {
+            return m3gpuSetError(M3GPU_ERR_INVALID, "command %d: bad world index or op", k);
+        }
+        m3HostWorld* w = ws[(size_t)c.world];
+        // Liveness, type and mass are creation-time data: the host image
+        // has them current even while the device is ahead.
+        const int32_t index = c.body.index1 - 1;
+        if (c.body.world0 != (uint16_t)w->slot || index < 0 || index >= w->hv.sc->bodyMax ||
+            w->hv.bodyAlive[index] == 0 || w->hv.bodyGen[index] != c.body.generation ||
+            !isfinite(c.v.x) || !isfinite(c.v.y) || !isfinite(c.v.z))
+        {
+            continue;
+        }
+        const bool needsMass = c.op != M3_OP_SET_LINEAR_VELOCITY && c.op != M3_OP_SET_ANGULAR_VELOCITY;
+        if (needsMass && !(w->hv.btype[index] == M3_BODY_DYNAMIC && w->hv.invMass[index] > 0.0f))
+        {
+            continue;
+        }
+        struct
+        {
+            m3BodyId id;
+            m3Vec3 v;
+        } record = {c.body, c.v};
+        m3JournalAppend(w, c.op, &record, (int32_t)sizeof(record));
+        ops.push_back(m3BodyOp{c.world, c.op, index, c.v});
+    }
+    rc = m3gpuStepBatch(ws.data(), count, dt, substeps, 1, ops.data(), (int32_t)ops.size());
+    if (rc == M3GPU_OK)
+    {
+        for (m3HostWorld* w : ws)
+        {
+            RecordSteps(w, dt, substeps, 1);
         }
     }
     return rc;

@@ -316,8 +316,13 @@ void Prepare(Request& r)
     }
     if (w != nullptr)
     {
-        // Nobody can snapshot a served world: it keeps no broadphase tree.
+        // Nobody can snapshot a served world: it keeps no broadphase tree,
+        // and its pair arrays past the live pairs (which only a snapshot
+        // reads; the step and the hash read the live pairs) stay on the
+        // host: the upload carries the live pairs alone, in the batched
+        // upload with the other admitted worlds.
         w->hv.sc->treeTracked = 0;
+        w->pairTailsToDevice = false;
     }
     // The inputs live on in the world; the request keeps only its parsed
     // records.

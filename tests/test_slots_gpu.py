@@ -113,3 +113,38 @@ def test_a_slot_is_void_once_the_world_is_built_on(m3):
     with pytest.raises(m3.M3GpuError):
         w.restore_slot(1)              # never saved
     w.destroy()
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not cuda_available(), reason="needs a CUDA device")
+def test_device_body_commands_equal_the_reference_body_calls(m3, oracle):
+    # Every command kind on random bodies, plus the no-ops: the static
+    # ground (impulses need mass), a stale id, a non-finite vector.
+    rlib = abi.bind_create(oracle.lib())
+    r = oracle.RefWorld.scene(SCENE_MIXED, 9, 300)
+    w = m3.World.scene(SCENE_MIXED, 9, 300)
+    bodies = w.body_count()
+    names = {abi.OP_APPLY_LINEAR_IMPULSE: "m3Body_ApplyLinearImpulse",
+             29: "m3Body_ApplyAngularImpulse", 26: "m3Body_ApplyForce", 27: "m3Body_ApplyTorque",
+             4: "m3Body_SetLinearVelocity", 5: "m3Body_SetAngularVelocity"}
+    ops = sorted(names)
+    rng = np.random.default_rng(4)
+    for step in range(30):
+        cmds = []
+        for _ in range(int(rng.integers(0, 9))):
+            op = ops[int(rng.integers(0, len(ops)))]
+            index1 = int(rng.integers(1, bodies + 1))
+            v = tuple(float(x) for x in rng.normal(size=3).astype(np.float32) * 5.0)
+            cmds.append((op, index1, 0, v))
+        if step == 7:
+            cmds.append((abi.OP_APPLY_LINEAR_IMPULSE, 1, 0, (0.0, 9.0, 0.0)))      # static ground
+            cmds.append((abi.OP_APPLY_LINEAR_IMPULSE, 100000, 0, (0.0, 9.0, 0.0)))  # stale
+            cmds.append((4, 3, 0, (float("nan"), 0.0, 0.0)))                       # non-finite
+        for op, index1, gen, v in cmds:
+            getattr(rlib, names[op])(abi.m3BodyId(index1, r.id.index1 - 1, gen), abi.m3Vec3(*v))
+        r.step(DT, SUB, 1)
+        m3.step_worlds_commands([w], [(0, op, abi.m3BodyId(index1, w.id.index1 - 1, gen), v)
+                                      for op, index1, gen, v in cmds], DT, SUB)
+        assert w.hash() == r.hash(), f"step {step}"
+    r.destroy()
+    w.destroy()
