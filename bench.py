@@ -12,7 +12,10 @@ One "step" = one m3World_Step of every world in the batch, everything
 the reference's step does included (the broadphase tree it keeps as
 snapshot state too).  The metric counts alive dynamic bodies x substeps
 x steps over all worlds and all ranks, divided by the max-over-ranks
-device time of exactly K steps.
+device time of exactly K steps.  First the packing autotuner steps a
+copy of the batch (the same worlds, built apart) --tune-steps times, real
+untimed steps that try packings of the worlds onto the SMs; the timed
+batch, built fresh, runs under the packing it leaves (`packing`).
 
 Lines printed by rank 0 (one JSON object):
   value     device-resident throughput (CUDA events around K steps);
@@ -690,6 +693,8 @@ def main() -> None:
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--tune-steps", type=int, default=24,
+                    help="untimed steps of the packing autotuner, on a copy of the batch (0: none)")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--worlds", type=int, default=4096)
     ap.add_argument("--lo", type=int, default=32)
@@ -757,6 +762,19 @@ def main() -> None:
     sizes = [all_sizes[i] for i in mine]
     seeds = [args.seed + i for i in mine]
     rank_seed = args.seed + 1_000_003 * rank
+    # The packing autotuner, on a batch of the same worlds built apart (its
+    # steps are real steps; the timed batch then starts from creation).
+    packing = m3.get_packing()
+    packing_ms = None
+    trials = []
+    if args.tune_steps > 0:
+        tune = m3.WorldBatch(build_worlds(m3, sizes, seeds))
+        m3.reserve_worlds(tune)
+        m3.upload_worlds(tune)
+        packing, packing_ms = m3.autotune_packing(tune, DT, args.substeps, args.tune_steps)
+        trials = m3.autotune_trials()
+        for w in tune:
+            w.destroy()
     worlds = m3.WorldBatch(build_worlds(m3, sizes, seeds))
     m3.reserve_worlds(worlds)
     m3.upload_worlds(worlds)
@@ -957,6 +975,16 @@ def main() -> None:
             "cpu_baseline": cpu, "plain_gpu": plain, "bit_exact_check": verified,
             "hash_ms": hash_ms, "clocks": clocks, "terrain": terrain, "serving": serving,
             "single_worlds": singles,
+            "packing": {"note": "the batch's packing onto the SMs (size-class bounds in shape "
+                                "slots, threads per world, shared-memory budget per class) "
+                                "chosen by the autotuner on a copy of the batch (same worlds, "
+                                "its own untimed steps from creation); trials: each candidate's "
+                                "prepare + substep ms against the mean of the steps beside it",
+                        "tune_steps": args.tune_steps, "chosen": packing,
+                        "prepare_substep_ms_per_step": packing_ms,
+                        "trials": [{"packing": t["packing"], "ms": round(t["ms"], 3),
+                                    "baseline_ms": round(t["baseline_ms"], 3),
+                                    "adopted": t["adopted"]} for t in trials]},
             "tree": {"note": "the broadphase tree (snapshot state) replays recorded leaf moves "
                              "every 16 steps beside the steps, or when read; catchup_ms = "
                              "replaying what the timed steps left, after them",

@@ -482,6 +482,56 @@ M3GPU_API int32_t m3gpu_kernel_ms(float* out);
  * the previous value (a value <= 0 only queries). */
 M3GPU_API int32_t m3gpu_set_wide_min_shapes(int32_t shapes);
 
+/* Packing of a batch's worlds onto the SMs (no reference counterpart:
+ * the reference steps one world per host thread).  The batched step
+ * splits its worlds, largest first, into three size classes by shape
+ * slots: class 0 holds worlds with at least minShapes[0] slots, class 1
+ * those with at least minShapes[1], class 2 the rest.  Each class's
+ * per-world kernels run `threads[c]` threads per world (512, 256 or 128:
+ * one, two or four worlds resident per SM) with up to `smemBytes[c]`
+ * bytes of shared memory per world for its tables (the body cache always
+ * fits; 0 keeps every table, body cache included, in global memory).
+ * Every packing gives the same bits; only the time differs. */
+typedef struct m3gpuPacking
+{
+    int32_t minShapes[2];
+    int32_t threads[3];
+    int32_t smemBytes[3];
+} m3gpuPacking;
+
+/* The packing in use, and a new one (checked: minShapes[0] >
+ * minShapes[1] >= 1, threads 128/256/512, smemBytes 0..204800).  It
+ * applies from the next batched step on. */
+M3GPU_API int32_t m3gpu_get_packing(m3gpuPacking* out);
+M3GPU_API int32_t m3gpu_set_packing(const m3gpuPacking* packing);
+
+/* Autotuner: steps the worlds exactly `steps` times (each a real step,
+ * bit for bit m3gpu_step_worlds(worlds, count, dt, substeps, 1), and
+ * recorded in an active journal the same way), timing the prepare and
+ * substep stages of each step under a candidate packing: candidates
+ * alternate with the packing in use, each judged against the mean of the
+ * steps beside it, and one that is at least 3 % faster becomes the packing
+ * in use, whose neighbours are tried next.  Leaves the fastest packing
+ * selected and returns it in `best` (optional) with its stage time per
+ * step in `bestMs` (optional).  Fewer than 3 steps only step. */
+M3GPU_API int32_t m3gpu_autotune_packing(const m3WorldId* worlds, int32_t count, float dt,
+                                         int32_t substeps, int32_t steps, m3gpuPacking* best,
+                                         float* bestMs);
+
+/* The last autotuning's trials, in order: each candidate packing, its
+ * step's prepare + substep device time, the mean of the two steps beside
+ * it under the packing then in use, and whether it was adopted.  Copies
+ * at most `cap` trials into `out` (may be null) and returns how many the
+ * tuning made. */
+typedef struct m3gpuPackingTrial
+{
+    m3gpuPacking packing;
+    float ms;
+    float baselineMs;
+    int32_t adopted;
+} m3gpuPackingTrial;
+M3GPU_API int32_t m3gpu_autotune_trials(m3gpuPackingTrial* out, int32_t cap);
+
 /* Work counters of one world accumulated over its device steps:
  * out[0] mover-substeps, out[1] contact-row-substeps, out[2]
  * joint-row-substeps, out[3] candidate pairs, out[4] steps, out[5] the

@@ -78,6 +78,16 @@ def _load() -> C.CDLL:
                                                C.c_int32, C.POINTER(abi.m3gpuBodyCommand),
                                                C.c_int32]
     lib.m3gpu_step_worlds_commands.restype = C.c_int32
+    lib.m3gpu_get_packing.argtypes = [C.POINTER(abi.m3gpuPacking)]
+    lib.m3gpu_get_packing.restype = C.c_int32
+    lib.m3gpu_set_packing.argtypes = [C.POINTER(abi.m3gpuPacking)]
+    lib.m3gpu_set_packing.restype = C.c_int32
+    lib.m3gpu_autotune_packing.argtypes = [C.POINTER(abi.m3WorldId), C.c_int32, C.c_float,
+                                           C.c_int32, C.c_int32, C.POINTER(abi.m3gpuPacking),
+                                           C.POINTER(C.c_float)]
+    lib.m3gpu_autotune_packing.restype = C.c_int32
+    lib.m3gpu_autotune_trials.argtypes = [C.POINTER(abi.m3gpuPackingTrial), C.c_int32]
+    lib.m3gpu_autotune_trials.restype = C.c_int32
     for name in ("m3gpu_slots_reserve", "m3gpu_slot_save", "m3gpu_slot_restore"):
         getattr(lib, name).argtypes = [abi.m3WorldId, C.c_int32]
         getattr(lib, name).restype = C.c_int32
@@ -227,6 +237,42 @@ def step_worlds_commands(worlds, commands, dt: float = 1.0 / 60.0, substeps: int
         arr[k] = abi.m3gpuBodyCommand(wi, op, body, abi.m3Vec3(*v))
     _check(lib.m3gpu_step_worlds_commands(_ids(worlds), len(worlds), dt, substeps, arr,
                                           len(commands)))
+
+
+def get_packing() -> dict:
+    """The batched step's packing in use (m3gpu_get_packing)."""
+    p = abi.m3gpuPacking()
+    _check(lib.m3gpu_get_packing(C.byref(p)))
+    return p.as_dict()
+
+
+def set_packing(packing: dict) -> None:
+    """Selects a packing (m3gpu_set_packing): {"min_shapes": [a, b],
+    "threads": [t0, t1, t2], "smem_bytes": [s0, s1, s2]}."""
+    _check(lib.m3gpu_set_packing(C.byref(abi.m3gpuPacking.from_dict(packing))))
+
+
+def autotune_packing(worlds, dt: float = 1.0 / 60.0, substeps: int = 4,
+                     steps: int = 24) -> tuple[dict, float]:
+    """Steps the worlds `steps` times while timing candidate packings
+    (m3gpu_autotune_packing); returns the packing left in use and its
+    prepare + substep device time per step in milliseconds."""
+    p = abi.m3gpuPacking()
+    ms = C.c_float(0.0)
+    _check(lib.m3gpu_autotune_packing(_ids(worlds), len(worlds), dt, substeps, steps,
+                                      C.byref(p), C.byref(ms)))
+    return p.as_dict(), float(ms.value)
+
+
+def autotune_trials() -> list[dict]:
+    """The last autotuning's candidates in order (m3gpu_autotune_trials):
+    packing, its step's prepare + substep ms, the mean of the steps beside
+    it under the packing then in use, and whether it was adopted."""
+    n = int(lib.m3gpu_autotune_trials(None, 0))
+    arr = (abi.m3gpuPackingTrial * max(n, 1))()
+    n = int(lib.m3gpu_autotune_trials(arr, n))
+    return [{"packing": t.packing.as_dict(), "ms": float(t.ms),
+             "baseline_ms": float(t.baselineMs), "adopted": bool(t.adopted)} for t in arr[:n]]
 
 
 def hash_worlds(worlds) -> np.ndarray:

@@ -92,7 +92,32 @@ class m3gpuBodyCommand(C.Structure):
     _fields_ = [("world", C.c_int32), ("op", C.c_int32), ("body", m3BodyId), ("v", m3Vec3)]
 
 
+class m3gpuPacking(C.Structure):
+    """The batched step's packing of worlds onto SMs (m3gpu_set_packing)."""
+    _fields_ = [("minShapes", C.c_int32 * 2), ("threads", C.c_int32 * 3),
+                ("smemBytes", C.c_int32 * 3)]
+
+    def as_dict(self) -> dict:
+        return {"min_shapes": list(self.minShapes), "threads": list(self.threads),
+                "smem_bytes": list(self.smemBytes)}
+
+    @classmethod
+    def from_dict(cls, d: dict) -> "m3gpuPacking":
+        p = cls()
+        p.minShapes[:] = list(d["min_shapes"])
+        p.threads[:] = list(d["threads"])
+        p.smemBytes[:] = list(d["smem_bytes"])
+        return p
+
+
+class m3gpuPackingTrial(C.Structure):
+    """One candidate of the last autotuning (m3gpu_autotune_trials)."""
+    _fields_ = [("packing", m3gpuPacking), ("ms", C.c_float), ("baselineMs", C.c_float),
+                ("adopted", C.c_int32)]
+
+
 assert C.sizeof(m3Counters) == 88 and C.sizeof(m3Profile) == 44
+assert C.sizeof(m3gpuPacking) == 32 and C.sizeof(m3gpuPackingTrial) == 44
 assert C.sizeof(m3gpuServeStats) == 120
 
 

@@ -288,6 +288,206 @@ extern "C" int32_t m3gpu_step_worlds_commands(const m3WorldId* worlds, int32_t c
     return rc;
 }
 
+// ---------------------------------------------------------------------
+// Packing autotuner.  Every packing steps the worlds to the same bits, so
+// the tuner times candidates on live steps instead of on copies: each of
+// its steps is a real step of the batch.  Candidates are the neighbours of
+// the packing in use (each class bound scaled down and up, each class's
+// threads per world switched, the two larger classes' shared-memory
+// budgets switched); a candidate's step sits between two steps of the
+// packing in use and is judged against their mean, so the slow drift of
+// a settling batch cancels.  A candidate at least 3 % faster is adopted
+// and its own neighbours are tried next.
+// ---------------------------------------------------------------------
+namespace
+{
+
+bool SamePacking(const m3gpuPacking& a, const m3gpuPacking& b)
+{
+    return memcmp(&a, &b, sizeof(a)) == 0;
+}
+
+std::vector<m3gpuPacking> PackingNeighbours(const m3gpuPacking& p)
+{
+    std::vector<m3gpuPacking> out;
+    auto push = [&](const m3gpuPacking& q) {
+        if (!(q.minShapes[1] >= 1 && q.minShapes[0] > q.minShapes[1]) || SamePacking(q, p))
+        {
+            return;
+        }
+        for (const m3gpuPacking& o : out)
+        {
+            if (SamePacking(o, q))
+            {
+                return;
+            }
+        }
+        out.push_back(q);
+    };
+    m3gpuPacking q = p;
+    q.minShapes[0] = p.minShapes[0] * 2 / 3;
+    push(q);
+    q = p;
+    q.minShapes[0] = p.minShapes[0] * 3 / 2;
+    push(q);
+    q = p;
+    q.minShapes[1] = p.minShapes[1] / 2;
+    push(q);
+    q = p;
+    q.minShapes[1] = p.minShapes[1] * 2;
+    push(q);
+    q = p;
+    q.threads[0] = p.threads[0] == 512 ? 256 : 512;
+    push(q);
+    q = p;
+    q.threads[1] = p.threads[1] == 256 ? 128 : 256;
+    push(q);
+    q = p;
+    q.threads[2] = p.threads[2] == 128 ? 256 : 128;
+    push(q);
+    q = p;
+    q.smemBytes[0] = p.smemBytes[0] > 110 * 1024 ? 110 * 1024 : 200 * 1024;
+    push(q);
+    q = p;
+    q.smemBytes[1] = p.smemBytes[1] > 54 * 1024 ? 54 * 1024 : 110 * 1024;
+    push(q);
+    return out;
+}
+
+// The last tuning's trials (m3gpu_autotune_trials); guarded by the
+// device lock like the tuning itself.
+std::vector<m3gpuPackingTrial> g_trials;
+
+} // namespace
+
+extern "C" int32_t m3gpu_autotune_trials(m3gpuPackingTrial* out, int32_t cap)
+{
+    M3_DEVICE_GUARD;
+    m3gpuClearError();
+    const int32_t n = (int32_t)g_trials.size();
+    for (int32_t i = 0; out != nullptr && i < n && i < cap; ++i)
+    {
+        out[i] = g_trials[(size_t)i];
+    }
+    return n;
+}
+
+extern "C" int32_t m3gpu_autotune_packing(const m3WorldId* worlds, int32_t count, float dt,
+                                          int32_t substeps, int32_t steps, m3gpuPacking* best,
+                                          float* bestMs)
+{
+    M3_DEVICE_GUARD;
+    m3gpuClearError();
+    if (!(dt > 0.0f) || substeps < 1 || substeps > M3_MAX_SUBSTEPS || steps < 0)
+    {
+        return m3gpuSetError(M3GPU_ERR_INVALID, "invalid dt, substeps or steps");
+    }
+    std::vector<m3HostWorld*> ws;
+    int32_t rc = Resolve(worlds, count, ws);
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
+    m3gpuPacking cur;
+    rc = m3gpu_get_packing(&cur);
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
+    int32_t done = 0;
+    // One real step under packing `p`; its prepare and substep stages'
+    // device time in *ms.
+    auto measure = [&](const m3gpuPacking& p, float* ms) -> int32_t {
+        int32_t r = m3gpu_set_packing(&p);
+        if (r == M3GPU_OK)
+        {
+            r = m3gpuStepBatch(ws.data(), count, dt, substeps, 1);
+        }
+        if (r != M3GPU_OK)
+        {
+            return r;
+        }
+        for (m3HostWorld* w : ws)
+        {
+            RecordSteps(w, dt, substeps, 1);
+        }
+        float stage[5];
+        r = m3gpu_kernel_ms(stage);
+        *ms = stage[2] + stage[3];
+        done += 1;
+        return r;
+    };
+    float base = 0.0f;
+    g_trials.clear();
+    if (steps >= 3)
+    {
+        rc = measure(cur, &base);
+        std::vector<m3gpuPacking> tried(1, cur);
+        std::vector<m3gpuPacking> queue = PackingNeighbours(cur);
+        size_t next = 0;
+        while (rc == M3GPU_OK && done + 2 <= steps && next < queue.size())
+        {
+            const m3gpuPacking cand = queue[next++];
+            bool seen = false;
+            for (const m3gpuPacking& t : tried)
+            {
+                seen = seen || SamePacking(t, cand);
+            }
+            if (seen)
+            {
+                continue;
+            }
+            tried.push_back(cand);
+            float candMs = 0.0f;
+            float after = 0.0f;
+            rc = measure(cand, &candMs);
+            if (rc == M3GPU_OK)
+            {
+                rc = measure(cur, &after);
+            }
+            if (rc != M3GPU_OK)
+            {
+                break;
+            }
+            const float mean = 0.5f * (base + after);
+            base = after;
+            const bool adopt = mean > 0.0f && candMs < 0.97f * mean;
+            g_trials.push_back(m3gpuPackingTrial{cand, candMs, mean, adopt ? 1 : 0});
+            if (adopt)
+            {
+                // Adopted: the next steps use it, and its neighbours
+                // come next.
+                cur = cand;
+                base = candMs;
+                queue = PackingNeighbours(cur);
+                next = 0;
+            }
+        }
+    }
+    // The remaining steps under the packing chosen.
+    while (rc == M3GPU_OK && done < steps)
+    {
+        rc = measure(cur, &base);
+    }
+    if (rc == M3GPU_OK)
+    {
+        rc = m3gpu_set_packing(&cur);
+    }
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
+    if (best != nullptr)
+    {
+        *best = cur;
+    }
+    if (bestMs != nullptr)
+    {
+        *bestMs = base;
+    }
+    return M3GPU_OK;
+}
+
 extern "C" int32_t m3gpu_hash_worlds(const m3WorldId* worlds, int32_t count, uint64_t* out)
 {
     m3gpuClearError();

@@ -4075,6 +4075,11 @@ struct m3BatchCache
     // each class's dynamic shared memory.
     int32_t classFirst[4] = {0, 0, 0, 0};
     int32_t classCache[3] = {0, 0, 0};
+    // Each class's kernel variant (0: 512 threads, 1: 256, 2: 128), the
+    // largest-first order on the host, and the packing they came from.
+    int32_t classVariant[3] = {0, 1, 2};
+    std::vector<int32_t> horder;
+    uint64_t packingSeq = 0;
 };
 static m3BatchCache s_batch;
 
@@ -4089,16 +4094,29 @@ static int32_t Check(cudaError_t e, const char* what)
 
 // Substep size classes: a world's threads follow its size (shape slots;
 // the batch order is by shape slots, largest first, so each class is a
-// contiguous run of the order).  Large worlds get 512 threads: twice the
-// rows per colour in flight and half as many worlds resident at once,
-// whose rows then stay in L2 across the passes.  Small worlds get 128:
-// four worlds share an SM instead of two, hiding each other's joint
-// chains, with one warp for a level's joint rows and three for its
-// contact rows.  Every class keeps 128 registers per thread.
+// contiguous run of the order).  By default large worlds get 512
+// threads: twice the rows per colour in flight and half as many worlds
+// resident at once, whose rows then stay in L2 across the passes.  Small
+// worlds get 128: four worlds share an SM instead of two, hiding each
+// other's joint chains, with one warp for a level's joint rows and three
+// for its contact rows.  Every variant keeps 128 registers per thread.
+// The split, each class's variant and its shared-memory budget form the
+// packing (m3gpu_set_packing, m3gpu_autotune_packing).
 #define M3_CLASSES 3
-static const int32_t s_classMinShapes[M3_CLASSES] = {769, 161, 0};
+static m3gpuPacking s_packing = {{769, 161},
+                                 {512, 256, 128},
+                                 {200 * 1024, M3_TWO_BLOCK_SMEM, 54 * 1024}};
+// Bumped by every change of the packing: a prepared batch then splits
+// its classes again before its next step.
+static uint64_t s_packingSeq = 1;
 
-// One class's prepare (stage 0) or substep (stage 1) kernel.
+static int32_t VariantOfThreads(int32_t threads)
+{
+    return threads >= 512 ? 0 : threads >= 256 ? 1 : 2;
+}
+
+// One variant's prepare (stage 0) or substep (stage 1) kernel: variant 0
+// runs 512 threads per world, 1 runs 256, 2 runs 128.
 static void LaunchClass(int32_t stage, int32_t c, cudaStream_t stream, const m3WorldView* views,
                         const int32_t* order, int32_t count, float dt, int32_t substeps,
                         int32_t cacheBytes)
@@ -4133,7 +4151,7 @@ static void LaunchClass(int32_t stage, int32_t c, cudaStream_t stream, const m3W
 #undef M3_LAUNCH_CLASS
 }
 
-// The dynamic shared memory each class's kernels were last allowed
+// The dynamic shared memory each variant's kernels were last allowed
 // (0: never set, the default of 48 KB for static and dynamic together).
 static int32_t s_classSmemSet[M3_CLASSES] = {0, 0, 0};
 
@@ -4231,6 +4249,66 @@ static int32_t EnsureClassStreams()
     return M3GPU_OK;
 }
 
+// Size classes over the batch's largest-first order under the packing in
+// use, and each class's shared memory: its largest body cache, plus the
+// inverse inertia table and the joint rows within the class's budget
+// (the default budgets keep one 512-thread block, two 256-thread blocks
+// or four 128-thread blocks per SM); a budget of 0 keeps every table in
+// global memory.
+static int32_t ClassifyBatch()
+{
+    const int64_t limit = 200 * 1024;
+    const int32_t count = (int32_t)s_batch.worlds.size();
+    const std::vector<int32_t>& order = s_batch.horder;
+    m3HostWorld* const* worlds = s_batch.worlds.data();
+    const int32_t minShapes[M3_CLASSES] = {s_packing.minShapes[0], s_packing.minShapes[1], 0};
+    int32_t c = 0;
+    s_batch.classFirst[0] = 0;
+    for (int32_t k = 0; k < count; ++k)
+    {
+        const int32_t shapes = worlds[order[(size_t)k]]->hv.sc->shapeMax;
+        while (c < M3_CLASSES - 1 && shapes < minShapes[c])
+        {
+            s_batch.classFirst[++c] = k;
+        }
+    }
+    while (c < M3_CLASSES)
+    {
+        s_batch.classFirst[++c] = count;
+    }
+    int32_t rc = M3GPU_OK;
+    for (int32_t k = 0; rc == M3GPU_OK && k < M3_CLASSES; ++k)
+    {
+        int64_t cBodies = 0;
+        int64_t cWant = 0;
+        for (int32_t j = s_batch.classFirst[k]; j < s_batch.classFirst[k + 1]; ++j)
+        {
+            const m3WorldScalars* sc = worlds[order[(size_t)j]]->hv.sc;
+            const int64_t bodies = (int64_t)sc->bodyMax * M3_BODY_CACHE_BYTES;
+            const int64_t withTables =
+                m3AlignUp(m3AlignUp(bodies, 16) + (int64_t)sc->bodyMax * (int64_t)sizeof(m3Mat3),
+                          16) +
+                (int64_t)sc->jointMax * (int64_t)sizeof(m3JointDev);
+            cBodies = bodies > cBodies ? bodies : cBodies;
+            cWant = withTables > cWant ? withTables : cWant;
+        }
+        const int64_t budget = s_packing.smemBytes[k];
+        const int64_t cap = cBodies > budget ? cBodies : budget;
+        cWant = cWant < cap ? cWant : cap;
+        cWant = cWant < limit ? cWant : limit;
+        cWant = budget == 0 ? 0 : cWant;
+        const int32_t variant = VariantOfThreads(s_packing.threads[k]);
+        s_batch.classCache[k] = (int32_t)cWant;
+        s_batch.classVariant[k] = variant;
+        rc = EnsureClassSmem(variant, (int32_t)cWant);
+    }
+    if (rc == M3GPU_OK)
+    {
+        s_batch.packingSeq = s_packingSeq;
+    }
+    return rc;
+}
+
 static int32_t PrepareBatch(m3HostWorld** worlds, int32_t count)
 {
     std::vector<m3HostWorld*> dirty;
@@ -4259,7 +4337,8 @@ static int32_t PrepareBatch(m3HostWorld** worlds, int32_t count)
     }
     if (same)
     {
-        return M3GPU_OK;
+        // The same batch: split again only under a new packing.
+        return s_batch.packingSeq == s_packingSeq ? M3GPU_OK : ClassifyBatch();
     }
     if (count > s_batch.cap)
     {
@@ -4371,48 +4450,8 @@ static int32_t PrepareBatch(m3HostWorld** worlds, int32_t count)
     want = want < jointCap ? want : jointCap;
     const int64_t limit = 200 * 1024;
     s_batch.cacheBytes = (int32_t)(want < limit ? want : limit);
-    // Size classes over the largest-first order, and each class's shared
-    // memory: its largest body cache, plus the inverse inertia table and
-    // the joint rows within the budget that keeps the class's blocks per
-    // SM (one 512-thread block, two 256-thread blocks, four 128-thread
-    // blocks).
-    static const int64_t classSmem[M3_CLASSES] = {200 * 1024, M3_TWO_BLOCK_SMEM, 54 * 1024};
-    int32_t c = 0;
-    s_batch.classFirst[0] = 0;
-    for (int32_t k = 0; k < count; ++k)
-    {
-        const int32_t shapes = worlds[order[(size_t)k]]->hv.sc->shapeMax;
-        while (c < M3_CLASSES - 1 && shapes < s_classMinShapes[c])
-        {
-            s_batch.classFirst[++c] = k;
-        }
-    }
-    while (c < M3_CLASSES)
-    {
-        s_batch.classFirst[++c] = count;
-    }
-    for (int32_t k = 0; rc == M3GPU_OK && k < M3_CLASSES; ++k)
-    {
-        int64_t cBodies = 0;
-        int64_t cWant = 0;
-        for (int32_t j = s_batch.classFirst[k]; j < s_batch.classFirst[k + 1]; ++j)
-        {
-            const m3WorldScalars* sc = worlds[order[(size_t)j]]->hv.sc;
-            const int64_t bodies = (int64_t)sc->bodyMax * M3_BODY_CACHE_BYTES;
-            const int64_t withTables =
-                m3AlignUp(m3AlignUp(bodies, 16) + (int64_t)sc->bodyMax * (int64_t)sizeof(m3Mat3),
-                          16) +
-                (int64_t)sc->jointMax * (int64_t)sizeof(m3JointDev);
-            cBodies = bodies > cBodies ? bodies : cBodies;
-            cWant = withTables > cWant ? withTables : cWant;
-        }
-        const int64_t cap = cBodies > classSmem[k] ? cBodies : classSmem[k];
-        cWant = cWant < cap ? cWant : cap;
-        cWant = cWant < limit ? cWant : limit;
-        s_batch.classCache[k] = (int32_t)cWant;
-        rc = EnsureClassSmem(k, (int32_t)cWant);
-    }
-    return rc;
+    s_batch.horder = order;
+    return ClassifyBatch();
 }
 
 // Narrowphase grid: enough 128-thread blocks to fill every SM several
@@ -4489,8 +4528,8 @@ static void ClassStage(int32_t stage, const m3WorldView* views, const int32_t* o
             continue;
         }
         cudaStreamWaitEvent(s_classStreams.stream[c], s_classStreams.fork, 0);
-        LaunchClass(stage, c, s_classStreams.stream[c], views, order + classFirst[c], n, dt,
-                    substeps, classCache[c]);
+        LaunchClass(stage, s_batch.classVariant[c], s_classStreams.stream[c], views,
+                    order + classFirst[c], n, dt, substeps, classCache[c]);
         cudaEventRecord(s_classStreams.join[c], s_classStreams.stream[c]);
         cudaStreamWaitEvent(0, s_classStreams.join[c], 0);
     }
@@ -4510,6 +4549,52 @@ extern "C" int32_t m3gpu_set_wide_min_shapes(int32_t shapes)
         s_wideMinShapes = shapes;
     }
     return previous;
+}
+
+extern "C" int32_t m3gpu_get_packing(m3gpuPacking* out)
+{
+    M3_DEVICE_GUARD;
+    m3gpuClearError();
+    if (out == nullptr)
+    {
+        return m3gpuSetError(M3GPU_ERR_INVALID, "null packing");
+    }
+    *out = s_packing;
+    return M3GPU_OK;
+}
+
+extern "C" int32_t m3gpu_set_packing(const m3gpuPacking* p)
+{
+    M3_DEVICE_GUARD;
+    m3gpuClearError();
+    if (p == nullptr)
+    {
+        return m3gpuSetError(M3GPU_ERR_INVALID, "null packing");
+    }
+    if (!(p->minShapes[1] >= 1 && p->minShapes[0] > p->minShapes[1]))
+    {
+        return m3gpuSetError(M3GPU_ERR_INVALID, "class bounds %d, %d: need %d > %d >= 1",
+                             p->minShapes[0], p->minShapes[1], p->minShapes[0], p->minShapes[1]);
+    }
+    for (int32_t c = 0; c < M3_CLASSES; ++c)
+    {
+        const int32_t t = p->threads[c];
+        if (t != 128 && t != 256 && t != 512)
+        {
+            return m3gpuSetError(M3GPU_ERR_INVALID, "class %d: %d threads (128, 256 or 512)", c, t);
+        }
+        if (p->smemBytes[c] < 0 || p->smemBytes[c] > 200 * 1024)
+        {
+            return m3gpuSetError(M3GPU_ERR_INVALID, "class %d: %d bytes of shared memory "
+                                 "(0 to 204800)", c, p->smemBytes[c]);
+        }
+    }
+    if (memcmp(p, &s_packing, sizeof(s_packing)) != 0)
+    {
+        s_packing = *p;
+        s_packingSeq += 1;
+    }
+    return M3GPU_OK;
 }
 
 // Blocks of the wide grid for a world: enough to give each level's rows

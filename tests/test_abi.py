@@ -33,3 +33,27 @@ def test_library_links_no_reference_code():
                          capture_output=True, text=True, check=True).stdout
     assert "m3StepInternal" not in out
     assert "m3o_" not in out
+
+
+def test_packing_is_checked_and_kept(m3):
+    """m3gpu_set_packing refuses impossible packings and keeps the last
+    valid one (host state only: no device call)."""
+    import pytest
+    before = m3.get_packing()
+    try:
+        good = {"min_shapes": [500, 100], "threads": [256, 128, 512],
+                "smem_bytes": [100000, 0, 204800]}
+        m3.set_packing(good)
+        assert m3.get_packing() == good
+        for bad in ({"min_shapes": [100, 100], "threads": [512, 256, 128], "smem_bytes": [0, 0, 0]},
+                    {"min_shapes": [100, 0], "threads": [512, 256, 128], "smem_bytes": [0, 0, 0]},
+                    {"min_shapes": [500, 100], "threads": [512, 64, 128], "smem_bytes": [0, 0, 0]},
+                    {"min_shapes": [500, 100], "threads": [512, 256, 128],
+                     "smem_bytes": [0, -1, 0]},
+                    {"min_shapes": [500, 100], "threads": [512, 256, 128],
+                     "smem_bytes": [0, 0, 204801]}):
+            with pytest.raises(m3.M3GpuError):
+                m3.set_packing(bad)
+            assert m3.get_packing() == good
+    finally:
+        m3.set_packing(before)
