@@ -591,10 +591,20 @@ __device__ int32_t m3CollideFamily(const m3WorldView& w, uint64_t key, m3Manifol
         m3real offset = w.geom[planeShape].s;
         // Selection keeps the four smallest (sep, index) candidates as
         // it scans; equivalent to the reference's repeated argmin over
-        // the full candidate list.
+        // the full candidate list.  The four slots are registers: every
+        // index below is a compile-time constant.
         int32_t keepIdx[M3_MANIFOLD_MAX_POINTS];
         m3real keepSep[M3_MANIFOLD_MAX_POINTS];
         double keepW[M3_MANIFOLD_MAX_POINTS][3];
+#pragma unroll
+        for (int32_t s = 0; s < M3_MANIFOLD_MAX_POINTS; ++s)
+        {
+            keepIdx[s] = 0;
+            keepSep[s] = 0.0f;
+            keepW[s][0] = 0.0;
+            keepW[s][1] = 0.0;
+            keepW[s][2] = 0.0;
+        }
         int32_t keepCount = 0;
         const int32_t nv = hull->vertexCount;
         for (int32_t k = 0; k < nv; ++k)
@@ -609,76 +619,111 @@ __device__ int32_t m3CollideFamily(const m3WorldView& w, uint64_t key, m3Manifol
             {
                 continue;
             }
-            // Insert (sepF, k) into the sorted keep list; indices arrive
-            // ascending, so equal separations keep the earlier vertex.
-            int32_t pos = keepCount;
-            while (pos > 0 && sepF < keepSep[pos - 1])
+            // (sepF, k) goes after every kept entry it does not undercut
+            // (indices arrive ascending, so equal separations keep the
+            // earlier vertex); entries from there on move down one slot,
+            // the last falling off a full list.
+            int32_t pos = 0;
+#pragma unroll
+            for (int32_t s = 0; s < M3_MANIFOLD_MAX_POINTS; ++s)
             {
-                pos -= 1;
+                pos += (s < keepCount && !(sepF < keepSep[s])) ? 1 : 0;
             }
             if (pos >= M3_MANIFOLD_MAX_POINTS)
             {
                 continue;
             }
-            int32_t last = keepCount < M3_MANIFOLD_MAX_POINTS ? keepCount : M3_MANIFOLD_MAX_POINTS - 1;
-            for (int32_t s = last; s > pos; --s)
+#pragma unroll
+            for (int32_t s = M3_MANIFOLD_MAX_POINTS - 1; s > 0; --s)
             {
-                keepIdx[s] = keepIdx[s - 1];
-                keepSep[s] = keepSep[s - 1];
-                keepW[s][0] = keepW[s - 1][0];
-                keepW[s][1] = keepW[s - 1][1];
-                keepW[s][2] = keepW[s - 1][2];
+                if (s > pos && s <= keepCount)
+                {
+                    keepIdx[s] = keepIdx[s - 1];
+                    keepSep[s] = keepSep[s - 1];
+                    keepW[s][0] = keepW[s - 1][0];
+                    keepW[s][1] = keepW[s - 1][1];
+                    keepW[s][2] = keepW[s - 1][2];
+                }
             }
-            keepIdx[pos] = k;
-            keepSep[pos] = sepF;
-            keepW[pos][0] = wx;
-            keepW[pos][1] = wy;
-            keepW[pos][2] = wz;
+#pragma unroll
+            for (int32_t s = 0; s < M3_MANIFOLD_MAX_POINTS; ++s)
+            {
+                if (s == pos)
+                {
+                    keepIdx[s] = k;
+                    keepSep[s] = sepF;
+                    keepW[s][0] = wx;
+                    keepW[s][1] = wy;
+                    keepW[s][2] = wz;
+                }
+            }
             if (keepCount < M3_MANIFOLD_MAX_POINTS)
             {
                 keepCount += 1;
             }
         }
-        // Emit in ascending vertex index.
-        int32_t order[M3_MANIFOLD_MAX_POINTS];
-        for (int32_t a = 0; a < keepCount; ++a)
+        // Emit in ascending vertex index: a sorting network over the four
+        // slots by index (empty slots carry the largest index and stay
+        // last).
+#pragma unroll
+        for (int32_t s = 0; s < M3_MANIFOLD_MAX_POINTS; ++s)
         {
-            order[a] = a;
+            keepIdx[s] = s < keepCount ? keepIdx[s] : 0x7FFFFFFF;
         }
-        for (int32_t a = 0; a < keepCount; ++a)
-        {
-            for (int32_t b = a + 1; b < keepCount; ++b)
+        auto order2 = [&](int32_t a, int32_t b) {
+            if (keepIdx[b] < keepIdx[a])
             {
-                if (keepIdx[order[b]] < keepIdx[order[a]])
+                const int32_t ti = keepIdx[a];
+                keepIdx[a] = keepIdx[b];
+                keepIdx[b] = ti;
+                const m3real ts = keepSep[a];
+                keepSep[a] = keepSep[b];
+                keepSep[b] = ts;
+#pragma unroll
+                for (int32_t c = 0; c < 3; ++c)
                 {
-                    int32_t tmp = order[a];
-                    order[a] = order[b];
-                    order[b] = tmp;
+                    const double tw = keepW[a][c];
+                    keepW[a][c] = keepW[b][c];
+                    keepW[b][c] = tw;
                 }
             }
-        }
+        };
+        static_assert(M3_MANIFOLD_MAX_POINTS == 4, "the network sorts four slots");
+        order2(0, 1);
+        order2(2, 3);
+        order2(0, 2);
+        order2(1, 3);
+        order2(1, 2);
         fresh.normal = n;
         fresh.pointCount = keepCount;
-        for (int32_t k = 0; k < keepCount; ++k)
+#pragma unroll
+        for (int32_t k = 0; k < M3_MANIFOLD_MAX_POINTS; ++k)
         {
-            int32_t c = order[k];
-            double sepD = (double)keepSep[c];
-            double px = keepW[c][0] - (double)n.x * sepD;
-            double py = keepW[c][1] - (double)n.y * sepD;
-            double pz = keepW[c][2] - (double)n.z * sepD;
-            fresh.points[k].anchorA = m3FromCom(w, planeBody, px, py, pz);
-            fresh.points[k].anchorB = m3FromCom(w, hullBody, keepW[c][0], keepW[c][1], keepW[c][2]);
-            fresh.points[k].separation = keepSep[c];
-            fresh.points[k].id = (uint16_t)keepIdx[c];
+            if (k < keepCount)
+            {
+                double sepD = (double)keepSep[k];
+                double px = keepW[k][0] - (double)n.x * sepD;
+                double py = keepW[k][1] - (double)n.y * sepD;
+                double pz = keepW[k][2] - (double)n.z * sepD;
+                fresh.points[k].anchorA = m3FromCom(w, planeBody, px, py, pz);
+                fresh.points[k].anchorB =
+                    m3FromCom(w, hullBody, keepW[k][0], keepW[k][1], keepW[k][2]);
+                fresh.points[k].separation = keepSep[k];
+                fresh.points[k].id = (uint16_t)keepIdx[k];
+            }
         }
         if (planeShape != shapeA)
         {
             fresh.normal = m3Neg3(fresh.normal);
-            for (int32_t k = 0; k < keepCount; ++k)
+#pragma unroll
+            for (int32_t k = 0; k < M3_MANIFOLD_MAX_POINTS; ++k)
             {
-                m3Vec3 tmp = fresh.points[k].anchorA;
-                fresh.points[k].anchorA = fresh.points[k].anchorB;
-                fresh.points[k].anchorB = tmp;
+                if (k < keepCount)
+                {
+                    m3Vec3 tmp = fresh.points[k].anchorA;
+                    fresh.points[k].anchorA = fresh.points[k].anchorB;
+                    fresh.points[k].anchorB = tmp;
+                }
             }
         }
     }
@@ -997,43 +1042,72 @@ __device__ int32_t m3CollidePair(const m3WorldView& w, uint64_t key, m3Manifold*
     }
 }
 
-// Warm-start carry (manifold.c:2868-2908): binary search of the previous
-// step's sorted keys, pair-level friction payload, per-point impulse by
-// feature id.
-__device__ __forceinline__ void m3WarmCarry(m3Manifold* fresh, uint64_t key,
-                                            const uint64_t* oldKeys, const m3Manifold* oldMan,
-                                            int32_t oldCount)
+// Index of `key` in keys[0, n) (sorted ascending, unique), or -1.  The
+// search starts at `hint` (the pair's index in this step's list; pair
+// lists change little between steps, so the key is usually there or a
+// few slots away) and gallops outwards before bisecting what is left:
+// a handful of dependent loads instead of a full bisection's log2(n).
+// Keys are unique, so the answer is the same as any exact search's.
+__device__ __forceinline__ int32_t m3FindPairKey(const uint64_t* keys, int32_t n, uint64_t key,
+                                                 int32_t hint)
 {
-    if (fresh->pointCount <= 0 || oldCount <= 0)
+    if (n <= 0)
     {
-        return;
+        return -1;
     }
-    int32_t lo = 0;
-    int32_t hi = oldCount - 1;
+    const int32_t i = hint < 0 ? 0 : (hint < n ? hint : n - 1);
+    const uint64_t ki = keys[i];
+    if (ki == key)
+    {
+        return i;
+    }
+    int32_t lo;
+    int32_t hi;
+    if (ki < key)
+    {
+        lo = i + 1;
+        hi = n - 1;
+        for (int32_t step = 1; i + step < n; step <<= 1)
+        {
+            const uint64_t kj = keys[i + step];
+            if (kj == key)
+            {
+                return i + step;
+            }
+            if (kj > key)
+            {
+                hi = i + step - 1;
+                break;
+            }
+            lo = i + step + 1;
+        }
+    }
+    else
+    {
+        lo = 0;
+        hi = i - 1;
+        for (int32_t step = 1; i - step >= 0; step <<= 1)
+        {
+            const uint64_t kj = keys[i - step];
+            if (kj == key)
+            {
+                return i - step;
+            }
+            if (kj < key)
+            {
+                lo = i - step + 1;
+                break;
+            }
+            hi = i - step - 1;
+        }
+    }
     while (lo <= hi)
     {
-        int32_t mid = (lo + hi) / 2;
-        uint64_t k = oldKeys[mid];
+        const int32_t mid = (lo + hi) / 2;
+        const uint64_t k = keys[mid];
         if (k == key)
         {
-            const m3Manifold* previous = &oldMan[mid];
-            fresh->frictionImpulse = previous->frictionImpulse;
-            fresh->twistImpulse = previous->twistImpulse;
-            fresh->rollingImpulse = previous->rollingImpulse;
-            int32_t pc = previous->pointCount;
-            for (int32_t a = 0; a < fresh->pointCount; ++a)
-            {
-                for (int32_t o = 0; o < pc; ++o)
-                {
-                    if (previous->points[o].id == fresh->points[a].id)
-                    {
-                        fresh->points[a].normalImpulse = previous->points[o].normalImpulse;
-                        fresh->points[a].flags |= 1;
-                        break;
-                    }
-                }
-            }
-            return;
+            return mid;
         }
         if (k < key)
         {
@@ -1042,6 +1116,49 @@ __device__ __forceinline__ void m3WarmCarry(m3Manifold* fresh, uint64_t key,
         else
         {
             hi = mid - 1;
+        }
+    }
+    return -1;
+}
+
+// Warm-start carry (manifold.c:2868-2908): the previous step's manifold
+// of the same key, pair-level friction payload, per-point impulse by
+// feature id.  `hint` is the pair's index in this step's sorted list.
+// The point loop runs over fixed slots so the manifold stays in
+// registers.
+__device__ __forceinline__ void m3WarmCarry(m3Manifold* fresh, uint64_t key,
+                                            const uint64_t* oldKeys, const m3Manifold* oldMan,
+                                            int32_t oldCount, int32_t hint)
+{
+    if (fresh->pointCount <= 0 || oldCount <= 0)
+    {
+        return;
+    }
+    const int32_t at = m3FindPairKey(oldKeys, oldCount, key, hint);
+    if (at < 0)
+    {
+        return;
+    }
+    const m3Manifold* previous = &oldMan[at];
+    fresh->frictionImpulse = previous->frictionImpulse;
+    fresh->twistImpulse = previous->twistImpulse;
+    fresh->rollingImpulse = previous->rollingImpulse;
+    const int32_t pc = previous->pointCount;
+    const int32_t fc = fresh->pointCount;
+#pragma unroll
+    for (int32_t a = 0; a < M3_MANIFOLD_MAX_POINTS; ++a)
+    {
+        if (a < fc)
+        {
+            for (int32_t o = 0; o < pc; ++o)
+            {
+                if (previous->points[o].id == fresh->points[a].id)
+                {
+                    fresh->points[a].normalImpulse = previous->points[o].normalImpulse;
+                    fresh->points[a].flags |= 1;
+                    break;
+                }
+            }
         }
     }
 }

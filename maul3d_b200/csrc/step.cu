@@ -43,6 +43,8 @@
 
 #include <cuda_runtime.h>
 
+#include <string.h>
+
 #include <algorithm>
 #include <vector>
 
@@ -1132,7 +1134,7 @@ __global__ void __launch_bounds__(128) m3NarrowKernel(const m3WorldView* views,
             sc->statusDetail = 1000 + (int32_t)w.shapeType[(int32_t)(key >> 32)] * 10 +
                                (int32_t)w.shapeType[(int32_t)(key & 0xFFFFFFFFu)];
         }
-        m3WarmCarry(&fresh, key, oldKeys, oldMan, sc->pairCount);
+        m3WarmCarry(&fresh, key, oldKeys, oldMan, sc->pairCount, k);
         newMan[k] = fresh;
     }
 }
@@ -1350,7 +1352,7 @@ __global__ void __launch_bounds__(128)
             sc->statusDetail = 1000 + (int32_t)w.shapeType[(int32_t)(key >> 32)] * 10 +
                                (int32_t)w.shapeType[(int32_t)(key & 0xFFFFFFFFu)];
         }
-        m3WarmCarry(&fresh, key, oldKeys, oldMan, sc->pairCount);
+        m3WarmCarry(&fresh, key, oldKeys, oldMan, sc->pairCount, k);
         newMan[k] = fresh;
     }
 }
@@ -4725,13 +4727,23 @@ extern "C" int32_t m3gpu_world_stats(m3WorldId world, uint64_t* out)
     {
         return m3gpuSetError(M3GPU_ERR_INVALID, "stale world or null output");
     }
-    if (m3gpuSyncHost(w) != M3GPU_OK)
+    // The counters alone, read from the device's scalars when the device
+    // is ahead (no tree replay, no download of the world).
+    decltype(w->hv.sc->work) work;
+    memcpy(work, w->hv.sc->work, sizeof(work));
+    if (w->deviceAhead && w->dslab != nullptr)
     {
-        return m3gpu_last_error();
+        const int32_t rc = Check(cudaMemcpy(work, w->dv.sc->work, sizeof(work),
+                                            cudaMemcpyDeviceToHost),
+                                 "work counters");
+        if (rc != M3GPU_OK)
+        {
+            return rc;
+        }
     }
     for (int32_t k = 0; k < 5; ++k)
     {
-        out[k] = w->hv.sc->work[k];
+        out[k] = work[k];
     }
     out[5] = (uint64_t)w->hv.sc->bodyMax;
     return M3GPU_OK;
