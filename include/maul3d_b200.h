@@ -303,6 +303,31 @@ typedef struct m3Profile
 } m3Profile;
 M3GPU_API m3Profile m3World_GetProfile(m3WorldId worldId);
 
+/* world.h:213-224 / world.c:1472-1500: contact begin and end events of the
+ * world's LAST step, in the reference's canonical order (ascending pair
+ * key over the union of the previous and the current pair lists): begin
+ * when a pair's manifold gained points, end when it lost them or the pair
+ * vanished; pairs with a sensor go to the sensor streams (world.h:260-263).
+ * shapeA is the lower shape index.  Valid until the next step, restore or
+ * destruction of the world; a restore clears them.  `count` must be
+ * non-null (0 and NULL for a stale world). */
+typedef struct m3ContactEvent {
+    m3ShapeId shapeA;
+    m3ShapeId shapeB;
+} m3ContactEvent;
+M3GPU_API const m3ContactEvent* m3World_ContactBeginEvents(m3WorldId worldId, int32_t* count);
+M3GPU_API const m3ContactEvent* m3World_ContactEndEvents(m3WorldId worldId, int32_t* count);
+M3GPU_API const m3ContactEvent* m3World_SensorBeginEvents(m3WorldId worldId, int32_t* count);
+M3GPU_API const m3ContactEvent* m3World_SensorEndEvents(m3WorldId worldId, int32_t* count);
+
+/* world.h:302-311 / world.c:1063: the joints the last step broke, in the
+ * order it destroyed them (ascending joint index), each with the id it had
+ * (already stale when read). */
+typedef struct m3JointBreakEvent {
+    m3JointId joint;
+} m3JointBreakEvent;
+M3GPU_API const m3JointBreakEvent* m3World_JointBreakEvents(m3WorldId worldId, int32_t* count);
+
 /* body.c:35 (body.h:43) / body.h:49 / body.h:56-59 */
 M3GPU_API m3BodyDef m3DefaultBodyDef(void);
 M3GPU_API m3BodyId m3CreateBody(m3WorldId worldId, const m3BodyDef* def);

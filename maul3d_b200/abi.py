@@ -328,6 +328,48 @@ assert C.sizeof(m3JointDef) == 224 and m3JointDef.ratio.offset == 160
 assert m3JointDef.groundAnchorA.offset == 168 and m3JointDef.internalValue.offset == 216
 
 
+class m3ContactEvent(C.Structure):
+    """world.h:213-217: a pair of shapes, the lower index first."""
+    _fields_ = [("shapeA", m3ShapeId), ("shapeB", m3ShapeId)]
+
+
+class m3JointBreakEvent(C.Structure):
+    """world.h:302-305."""
+    _fields_ = [("joint", m3JointId)]
+
+
+EVENT_STREAMS = ("m3World_ContactBeginEvents", "m3World_ContactEndEvents",
+                 "m3World_SensorBeginEvents", "m3World_SensorEndEvents")
+
+
+def bind_events(lib: C.CDLL) -> C.CDLL:
+    """Declare the reference-named event streams on a handle."""
+    for name in EVENT_STREAMS:
+        fn = getattr(lib, name)
+        fn.argtypes = [m3WorldId, C.POINTER(C.c_int32)]
+        fn.restype = C.POINTER(m3ContactEvent)
+    lib.m3World_JointBreakEvents.argtypes = [m3WorldId, C.POINTER(C.c_int32)]
+    lib.m3World_JointBreakEvents.restype = C.POINTER(m3JointBreakEvent)
+    return lib
+
+
+def read_events(lib: C.CDLL, world: m3WorldId) -> dict:
+    """Every event stream of a world's last step as lists of (index1,
+    generation) tuples (the world index is left out: it is the engine's
+    own table slot)."""
+    out = {}
+    for name in EVENT_STREAMS:
+        n = C.c_int32(0)
+        ptr = getattr(lib, name)(world, C.byref(n))
+        out[name] = [((ptr[i].shapeA.index1, ptr[i].shapeA.generation),
+                      (ptr[i].shapeB.index1, ptr[i].shapeB.generation)) for i in range(n.value)]
+    n = C.c_int32(0)
+    ptr = lib.m3World_JointBreakEvents(world, C.byref(n))
+    out["m3World_JointBreakEvents"] = [(ptr[i].joint.index1, ptr[i].joint.generation)
+                                       for i in range(n.value)]
+    return out
+
+
 def bind_create(lib: C.CDLL) -> C.CDLL:
     """Declare the reference-named creation API on a handle."""
     lib.m3DefaultWorldDef.restype = m3WorldDef

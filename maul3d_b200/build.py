@@ -34,7 +34,7 @@ DET_HOST = ["-ffp-contract=off", "-fno-fast-math", "-fno-unsafe-math-optimizatio
 
 CU_SOURCES = ["step.cu", "hash.cu", "upload.cu"]
 CPP_SOURCES = ["world.cpp", "device.cpp", "capi.cpp", "hostmem.cpp", "snapshot.cpp", "serve.cpp",
-               "quickhull.cpp"]
+               "events.cpp", "quickhull.cpp"]
 C_SOURCES = ["scenes.c"]
 
 

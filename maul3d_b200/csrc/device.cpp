@@ -927,5 +927,6 @@ extern "C" int32_t m3gpu_slot_restore(m3WorldId world, int32_t slot)
     w->pairTailsOnDevice = true;
     w->leafBoxValid = false;
     m3JournalUnrecordable(w); // a rewind is not a command of the journal
+    m3MarkEventEpoch(w, false);  // like a restore: no events until a step
     return M3GPU_OK;
 }

@@ -55,6 +55,11 @@ typedef struct m3WorldScalars
     int32_t moverCount;
     int32_t jointConstraintCount;
     int32_t newPairCount; // pair list the running step is building
+    // The previous step's pair count (the other pair buffer) and where the
+    // ring of broken joints stood when the last step began: the last
+    // step's event streams are read from them.
+    int32_t prevPairCount;
+    int32_t stepBrokenStart;
     // Joints the device destroyed (breakage), as a ring over jbroken:
     // the host drains entries [drained, brokenCount) into its free queue.
     int32_t brokenCount;

@@ -193,6 +193,18 @@ struct m3HostWorld
     std::vector<uint8_t> snapshotCarry;
     std::vector<uint8_t> snapshotHeaderCarry;
     std::vector<float> heightFieldCellCarry;
+    // Event streams of the world's last step (world.h:207-313): computed
+    // on the first read after a step from the device's two pair lists and
+    // its ring of broken joints.  stepEpoch counts device step calls and
+    // restores; the streams are current when eventsEpoch equals it.
+    uint64_t stepEpoch = 0;
+    bool lastEpochIsStep = false;
+    uint64_t eventsEpoch = 0;
+    std::vector<m3ContactEvent> beginEvents;
+    std::vector<m3ContactEvent> endEvents;
+    std::vector<m3ContactEvent> sensorBeginEvents;
+    std::vector<m3ContactEvent> sensorEndEvents;
+    std::vector<m3JointBreakEvent> jointBreakEvents;
     // Journal recording (world.c:1348-1398): records appended to the
     // caller's buffer while active; overflow latches and ends it.
     uint8_t* journalBuffer = nullptr;
@@ -347,6 +359,15 @@ void m3JournalUnrecordable(m3HostWorld* w);
 
 // Queue the joint slots the device freed since the last call (world.cpp).
 void m3DrainBrokenJoints(m3HostWorld* w);
+
+// A world's event streams start over: a step just ran on the device
+// (`stepped`), or a restore replaced its state (no events until the next
+// step).
+inline void m3MarkEventEpoch(m3HostWorld* w, bool stepped)
+{
+    w->stepEpoch += 1;
+    w->lastEpochIsStep = stepped;
+}
 
 // Step and hash entry points (step.cu).
 // `ops` (optional) are body commands applied on the device before the

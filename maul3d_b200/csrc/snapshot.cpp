@@ -1005,6 +1005,8 @@ bool m3gpuRestoreWorld(m3HostWorld* w, const void* data, int32_t size)
     w->hostDirty = true;
     w->pairTailsToDevice = true;
     w->pairTailsOnDevice = false;
+    // Events are observations of a step, never state (snapshot.c:867-879).
+    m3MarkEventEpoch(w, false);
     return true;
 }
 

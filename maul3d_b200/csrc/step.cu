@@ -1576,7 +1576,9 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3PrepareKernel(const m3WorldV
             // The pair list and manifolds built by the collide kernels
             // become the current ones.
             sc->pairBuf = 1 - sc->pairBuf;
+            sc->prevPairCount = sc->pairCount;
             sc->pairCount = sc->newPairCount;
+            sc->stepBrokenStart = sc->brokenCount;
         }
     }
     __syncthreads();
@@ -2613,7 +2615,9 @@ __global__ void __launch_bounds__(NT, 2) m3WidePrepareKernel(const m3WorldView* 
     if (lead)
     {
         sc->pairBuf = 1 - sc->pairBuf;
+        sc->prevPairCount = sc->pairCount;
         sc->pairCount = sc->newPairCount;
+        sc->stepBrokenStart = sc->brokenCount;
     }
     M3_GSYNC()
     const int32_t bodyMax = sc->bodyMax;
@@ -5309,6 +5313,10 @@ int32_t m3gpuStepBatch(m3HostWorld** worlds, int32_t count, float dt, int32_t su
     {
         worlds[i]->deviceAhead = true;
         worlds[i]->pairTailsOnDevice = true;
+        if (rc == M3GPU_OK && steps > 0)
+        {
+            m3MarkEventEpoch(worlds[i], true);
+        }
     }
     if (rc != M3GPU_OK)
     {
@@ -5580,6 +5588,7 @@ extern "C" int32_t m3gpu_step_world_noalloc(m3WorldId worldId, float dt, int32_t
     {
         return rc;
     }
+    m3MarkEventEpoch(w, true);
     if (status != 0)
     {
         int32_t detail = 0;
