@@ -76,12 +76,12 @@ SCENE_TERRAIN = 5
 # substep 3 passes x (456 B record + 2 x 48 B v,w + 2 x 28 B dp,dq); per
 # joint row per substep 3 x (472 + 152).
 # DRAM bytes (read + write) of one step's m3SubstepKernel launches (the
-# three size classes) on the default workload, from ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum, one pass each;
-# profiles/m3SubstepKernel_uneven4096.txt gives the command):
-# 875.0 + 345.2 MB (512-thread class), 342.7 + 130.1 MB (256), 79.8 +
-# 95.9 MB (128).  Reported for that workload only.
-SUBSTEP_TRAFFIC_DEFAULT = (875.0 + 345.2 + 342.7 + 130.1 + 79.8 + 95.9) * 1e6
+# three size classes; the 4th step from creation) on the default
+# workload, from ncu (dram__bytes_read.sum + dram__bytes_write.sum, one
+# pass; profiles/m3SubstepKernel_uneven4096.txt gives the command):
+# 902.5 + 677.7 MB (512-thread class), 381.8 + 391.5 MB (256), 80.5 +
+# 102.4 MB (128).  Reported for that workload only.
+SUBSTEP_TRAFFIC_DEFAULT = (902.5 + 677.7 + 381.8 + 391.5 + 80.5 + 102.4) * 1e6
 BYTES_PER_MOVER_SUBSTEP = 314
 BYTES_PER_CONTACT_SUBSTEP = 3 * (456 + 2 * 48 + 2 * 28)
 BYTES_PER_JOINT_SUBSTEP = 3 * (472 + 152)
@@ -779,8 +779,10 @@ def main() -> None:
     m3.reserve_worlds(worlds)
     m3.upload_worlds(worlds)
 
-    # Warm-up steps (untimed).
+    # Warm-up steps (untimed), and their tree moves replayed: the timed
+    # steps' catch-up is reported apart, below.
     m3.step_worlds(worlds, DT, args.substeps, args.warmup)
+    m3.flush_trees(worlds)
     stats0 = np.stack([m3.world_stats(w) for w in worlds])
 
     sampler = ClockSampler(local_rank)

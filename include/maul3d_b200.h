@@ -328,6 +328,16 @@ typedef struct m3JointBreakEvent {
 } m3JointBreakEvent;
 M3GPU_API const m3JointBreakEvent* m3World_JointBreakEvents(m3WorldId worldId, int32_t* count);
 
+/* world.h:287-300 / solver.c:4295-4306: one event per body the last step
+ * moved (every mover, ascending body index) with its transform after the
+ * step; fellAsleep marks the step its island fell asleep. */
+typedef struct m3BodyMoveEvent {
+    m3BodyId body;
+    m3Transform transform;
+    bool fellAsleep;
+} m3BodyMoveEvent;
+M3GPU_API const m3BodyMoveEvent* m3World_BodyMoveEvents(m3WorldId worldId, int32_t* count);
+
 /* body.c:35 (body.h:43) / body.h:49 / body.h:56-59 */
 M3GPU_API m3BodyDef m3DefaultBodyDef(void);
 M3GPU_API m3BodyId m3CreateBody(m3WorldId worldId, const m3BodyDef* def);

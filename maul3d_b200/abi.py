@@ -338,6 +338,15 @@ class m3JointBreakEvent(C.Structure):
     _fields_ = [("joint", m3JointId)]
 
 
+class m3Transform(C.Structure):
+    _fields_ = [("p", m3Pos3), ("q", m3Quat)]
+
+
+class m3BodyMoveEvent(C.Structure):
+    """world.h:295-300."""
+    _fields_ = [("body", m3BodyId), ("transform", m3Transform), ("fellAsleep", C.c_bool)]
+
+
 EVENT_STREAMS = ("m3World_ContactBeginEvents", "m3World_ContactEndEvents",
                  "m3World_SensorBeginEvents", "m3World_SensorEndEvents")
 
@@ -350,13 +359,16 @@ def bind_events(lib: C.CDLL) -> C.CDLL:
         fn.restype = C.POINTER(m3ContactEvent)
     lib.m3World_JointBreakEvents.argtypes = [m3WorldId, C.POINTER(C.c_int32)]
     lib.m3World_JointBreakEvents.restype = C.POINTER(m3JointBreakEvent)
+    lib.m3World_BodyMoveEvents.argtypes = [m3WorldId, C.POINTER(C.c_int32)]
+    lib.m3World_BodyMoveEvents.restype = C.POINTER(m3BodyMoveEvent)
     return lib
 
 
-def read_events(lib: C.CDLL, world: m3WorldId) -> dict:
+def read_events(lib: C.CDLL, world: m3WorldId, moves: bool = True) -> dict:
     """Every event stream of a world's last step as lists of (index1,
     generation) tuples (the world index is left out: it is the engine's
-    own table slot)."""
+    own table slot); body move events add the transform's bytes and the
+    fell-asleep flag."""
     out = {}
     for name in EVENT_STREAMS:
         n = C.c_int32(0)
@@ -367,6 +379,12 @@ def read_events(lib: C.CDLL, world: m3WorldId) -> dict:
     ptr = lib.m3World_JointBreakEvents(world, C.byref(n))
     out["m3World_JointBreakEvents"] = [(ptr[i].joint.index1, ptr[i].joint.generation)
                                        for i in range(n.value)]
+    if moves:
+        n = C.c_int32(0)
+        ptr = lib.m3World_BodyMoveEvents(world, C.byref(n))
+        out["m3World_BodyMoveEvents"] = [
+            (ptr[i].body.index1, ptr[i].body.generation, bytes(ptr[i].transform),
+             bool(ptr[i].fellAsleep)) for i in range(n.value)]
     return out
 
 

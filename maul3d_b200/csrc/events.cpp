@@ -1,5 +1,5 @@
 // Event streams of a world's last step (world.h:207-313): contact and
-// sensor begin/end events and joint-break events.
+// sensor begin/end events, joint-break events and body move events.
 //
 // The device step keeps the previous step's pair list and manifolds in
 // the second pair buffer (the two buffers swap every step), records the
@@ -8,7 +8,9 @@
 // events need no work inside the step: the first read after a step
 // copies the two key lists, the manifolds' point counts and the step's
 // ring entries back and walks them as the reference's step does
-// (solver.c:3747-3815 for contacts, solver.c:4233-4257 for breaks).
+// (solver.c:3747-3815 for contacts, solver.c:4233-4257 for breaks); the
+// move events read the step's mover list (still in the world's scratch)
+// and the bodies' transforms.
 // Shape liveness and generations come from the host image, which this
 // path never changes behind the host's back (the device destroys joints
 // only, never shapes).
@@ -17,7 +19,9 @@
 #include <cuda_runtime.h>
 
 #include <stddef.h>
+#include <string.h>
 
+#include <type_traits>
 #include <vector>
 
 namespace
@@ -92,9 +96,9 @@ int32_t EnsureEvents(m3HostWorld* w)
         return M3GPU_OK;
     }
     const bool curIs0 = sc.pairBuf == 0;
-    const int32_t newCount = sc.pairCount < 0 ? 0 : (sc.pairCount < sc.pairCap ? sc.pairCount : sc.pairCap);
-    const int32_t oldCount =
-        sc.prevPairCount < 0 ? 0 : (sc.prevPairCount < sc.pairCap ? sc.prevPairCount : sc.pairCap);
+    auto clampCount = [&](int32_t n) { return n < 0 ? 0 : (n < sc.pairCap ? n : sc.pairCap); };
+    const int32_t newCount = clampCount(sc.pairCount);
+    const int32_t oldCount = clampCount(sc.prevPairCount);
     std::vector<uint64_t> newKeys;
     std::vector<uint64_t> oldKeys;
     std::vector<int32_t> newPoints;
@@ -204,6 +208,82 @@ int32_t EnsureEvents(m3HostWorld* w)
     return M3GPU_OK;
 }
 
+// Body move events of the last step (solver.c:4295-4306): the step's
+// movers in ascending order, each with its transform after the step and
+// whether its island fell asleep on this step.
+int32_t EnsureMoveEvents(m3HostWorld* w)
+{
+    if (w->moveEventsEpoch == w->stepEpoch)
+    {
+        return M3GPU_OK;
+    }
+    w->moveEvents.clear();
+    if (!w->lastEpochIsStep || w->dslab == nullptr)
+    {
+        w->moveEventsEpoch = w->stepEpoch;
+        return M3GPU_OK;
+    }
+    m3WorldScalars sc;
+    int32_t rc = Cuda(cudaMemcpy(&sc, w->dv.sc, sizeof(sc), cudaMemcpyDeviceToHost),
+                      "event scalars");
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
+    const int32_t bodies = sc.bodyMax;
+    const int32_t movers = sc.moverCount;
+    if (sc.status != 0 || movers <= 0 || movers > bodies)
+    {
+        w->moveEventsEpoch = w->stepEpoch;
+        return M3GPU_OK;
+    }
+    std::vector<int32_t> list((size_t)movers);
+    std::vector<m3Transform> xf((size_t)bodies);
+    std::vector<uint8_t> type((size_t)bodies);
+    std::vector<uint8_t> awake((size_t)bodies);
+    rc = Cuda(cudaMemcpy(list.data(), m3gpuDeviceMovers(w), sizeof(int32_t) * (size_t)movers,
+                         cudaMemcpyDeviceToHost),
+              "event movers");
+    if (rc == M3GPU_OK)
+    {
+        rc = Cuda(cudaMemcpy(xf.data(), w->dv.xf, sizeof(m3Transform) * (size_t)bodies,
+                             cudaMemcpyDeviceToHost),
+                  "event transforms");
+    }
+    if (rc == M3GPU_OK)
+    {
+        rc = Cuda(cudaMemcpy(type.data(), w->dv.btype, (size_t)bodies, cudaMemcpyDeviceToHost),
+                  "event body types");
+    }
+    if (rc == M3GPU_OK)
+    {
+        rc = Cuda(cudaMemcpy(awake.data(), w->dv.awake, (size_t)bodies, cudaMemcpyDeviceToHost),
+                  "event awake flags");
+    }
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
+    const uint16_t world0 = (uint16_t)w->slot;
+    w->moveEvents.reserve((size_t)movers);
+    for (int32_t m = 0; m < movers; ++m)
+    {
+        const int32_t i = list[(size_t)m];
+        if (i < 0 || i >= bodies)
+        {
+            continue;
+        }
+        m3BodyMoveEvent e;
+        memset(&e, 0, sizeof(e));
+        e.body = m3BodyId{i + 1, world0, w->hv.bodyGen[i]};
+        e.transform = xf[(size_t)i];
+        e.fellAsleep = type[(size_t)i] == M3_BODY_DYNAMIC && awake[(size_t)i] == 0;
+        w->moveEvents.push_back(e);
+    }
+    w->moveEventsEpoch = w->stepEpoch;
+    return M3GPU_OK;
+}
+
 template <class T>
 const T* Stream(m3WorldId worldId, int32_t* count, std::vector<T> m3HostWorld::*member)
 {
@@ -215,7 +295,8 @@ const T* Stream(m3WorldId worldId, int32_t* count, std::vector<T> m3HostWorld::*
     }
     *count = 0;
     m3HostWorld* w = m3gpuWorldFromId(worldId);
-    if (w == nullptr || EnsureEvents(w) != M3GPU_OK)
+    const bool moves = std::is_same<T, m3BodyMoveEvent>::value;
+    if (w == nullptr || (moves ? EnsureMoveEvents(w) : EnsureEvents(w)) != M3GPU_OK)
     {
         return nullptr;
     }
@@ -249,4 +330,9 @@ extern "C" const m3ContactEvent* m3World_SensorEndEvents(m3WorldId worldId, int3
 extern "C" const m3JointBreakEvent* m3World_JointBreakEvents(m3WorldId worldId, int32_t* count)
 {
     return Stream(worldId, count, &m3HostWorld::jointBreakEvents);
+}
+
+extern "C" const m3BodyMoveEvent* m3World_BodyMoveEvents(m3WorldId worldId, int32_t* count)
+{
+    return Stream(worldId, count, &m3HostWorld::moveEvents);
 }

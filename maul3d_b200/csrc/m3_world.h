@@ -205,6 +205,10 @@ struct m3HostWorld
     std::vector<m3ContactEvent> sensorBeginEvents;
     std::vector<m3ContactEvent> sensorEndEvents;
     std::vector<m3JointBreakEvent> jointBreakEvents;
+    // Body move events, built on their own first read (they copy every
+    // body's transform back).
+    uint64_t moveEventsEpoch = 0;
+    std::vector<m3BodyMoveEvent> moveEvents;
     // Journal recording (world.c:1348-1398): records appended to the
     // caller's buffer while active; overflow latches and ends it.
     uint8_t* journalBuffer = nullptr;
@@ -368,6 +372,11 @@ inline void m3MarkEventEpoch(m3HostWorld* w, bool stepped)
     w->stepEpoch += 1;
     w->lastEpochIsStep = stepped;
 }
+
+// The device address of the last step's mover list (ascending body
+// indices; its length is the scalars' moverCount) in a world's slab
+// scratch (step.cu).
+const int32_t* m3gpuDeviceMovers(const m3HostWorld* w);
 
 // Step and hash entry points (step.cu).
 // `ops` (optional) are body commands applied on the device before the

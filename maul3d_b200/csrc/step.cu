@@ -4557,6 +4557,13 @@ extern "C" int32_t m3gpu_set_wide_min_shapes(int32_t shapes)
     return previous;
 }
 
+const int32_t* m3gpuDeviceMovers(const m3HostWorld* w)
+{
+    m3Scratch s;
+    ScratchCarve(&s, w->dv.scratch, w->bodyCap, w->shapeCap, w->jointCap, w->pairCap);
+    return s.movers;
+}
+
 extern "C" int32_t m3gpu_get_packing(m3gpuPacking* out)
 {
     M3_DEVICE_GUARD;
@@ -5589,6 +5596,23 @@ extern "C" int32_t m3gpu_step_world_noalloc(m3WorldId worldId, float dt, int32_t
         return rc;
     }
     m3MarkEventEpoch(w, true);
+    if (status == 0)
+    {
+        // The step's mover list (its body move events) into the world's
+        // own scratch: the static array belongs to every call.
+        m3Scratch from;
+        m3Scratch to;
+        ScratchCarve(&from, sym.scratch, w->bodyCap, w->shapeCap, w->jointCap, w->pairCap);
+        ScratchCarve(&to, w->dv.scratch, w->bodyCap, w->shapeCap, w->jointCap, w->pairCap);
+        rc = Check(cudaMemcpy(to.movers, from.movers,
+                              sizeof(int32_t) * (size_t)w->hv.sc->bodyMax,
+                              cudaMemcpyDeviceToDevice),
+                   "noalloc movers");
+        if (rc != M3GPU_OK)
+        {
+            return rc;
+        }
+    }
     if (status != 0)
     {
         int32_t detail = 0;

@@ -1,11 +1,13 @@
 """Event streams of the last step (needs a B200).
 
-Contact begin/end, sensor begin/end and joint-break events
+Contact begin/end, sensor begin/end, joint-break and body move events
 (world.h:207-313) must be the reference's, stream for stream and in the
 same order, after every step: bodies settling and bouncing (contacts
-begin and end), towers whose welds break (joint-break events with the
-ids the joints had), and spheres falling through a sensor box (sensor
-streams).  A restore clears every stream in both engines.
+begin and end, bodies falling asleep), towers whose welds break
+(joint-break events with the ids the joints had), and spheres falling
+through a sensor box (sensor streams).  Body move events carry the
+post-step transform, compared byte for byte.  A restore clears every
+stream in both engines.
 """
 import ctypes as C
 
@@ -45,7 +47,8 @@ def test_event_streams_equal_the_reference_every_step(m3, oracle, libs, scene, s
     glib, rlib = libs
     g = m3.World.scene(scene, seed, param)
     r = oracle.RefWorld.scene(scene, seed, param)
-    seen = {name: 0 for name in abi.EVENT_STREAMS + ("m3World_JointBreakEvents",)}
+    seen = {name: 0 for name in abi.EVENT_STREAMS + ("m3World_JointBreakEvents",
+                                                     "m3World_BodyMoveEvents")}
     for s in range(steps):
         g.step(DT, substeps, 1)
         r.step(DT, substeps, 1)
@@ -55,6 +58,7 @@ def test_event_streams_equal_the_reference_every_step(m3, oracle, libs, scene, s
     assert g.hash() == r.hash()
     # The scenes do what they are here for.
     assert seen["m3World_ContactBeginEvents"] > 0
+    assert seen["m3World_BodyMoveEvents"] > 0
     if scene in (SCENE_UNEVEN, SCENE_BOUNCE):
         assert seen["m3World_ContactEndEvents"] > 0
     if scene == SCENE_CITY:
