@@ -328,6 +328,23 @@ typedef struct m3JointBreakEvent {
 } m3JointBreakEvent;
 M3GPU_API const m3JointBreakEvent* m3World_JointBreakEvents(m3WorldId worldId, int32_t* count);
 
+/* world.h:265-285 / solver.c:2987-3033: hit events of the last step, in
+ * contact constraint order: at most one per contact whose shapes include
+ * one that enabled hit events, for its fastest-approaching point whose
+ * approach beat the world's hit threshold and whose impulse fired.  point
+ * is the contact point on shape A's body in world space, normal runs from
+ * A to B.  At most the world's pair capacity; the rest are counted by
+ * m3World_HitEventsDropped. */
+typedef struct m3HitEvent {
+    m3ShapeId shapeA;
+    m3ShapeId shapeB;
+    m3Pos3 point;
+    m3Vec3 normal;
+    m3real approachSpeed;
+} m3HitEvent;
+M3GPU_API const m3HitEvent* m3World_HitEvents(m3WorldId worldId, int32_t* count);
+M3GPU_API int32_t m3World_HitEventsDropped(m3WorldId worldId);
+
 /* world.h:287-300 / solver.c:4295-4306: one event per body the last step
  * moved (every mover, ascending body index) with its transform after the
  * step; fellAsleep marks the step its island fell asleep. */

@@ -347,6 +347,12 @@ class m3BodyMoveEvent(C.Structure):
     _fields_ = [("body", m3BodyId), ("transform", m3Transform), ("fellAsleep", C.c_bool)]
 
 
+class m3HitEvent(C.Structure):
+    """world.h:270-277."""
+    _fields_ = [("shapeA", m3ShapeId), ("shapeB", m3ShapeId), ("point", m3Pos3),
+                ("normal", m3Vec3), ("approachSpeed", C.c_float)]
+
+
 EVENT_STREAMS = ("m3World_ContactBeginEvents", "m3World_ContactEndEvents",
                  "m3World_SensorBeginEvents", "m3World_SensorEndEvents")
 
@@ -361,6 +367,10 @@ def bind_events(lib: C.CDLL) -> C.CDLL:
     lib.m3World_JointBreakEvents.restype = C.POINTER(m3JointBreakEvent)
     lib.m3World_BodyMoveEvents.argtypes = [m3WorldId, C.POINTER(C.c_int32)]
     lib.m3World_BodyMoveEvents.restype = C.POINTER(m3BodyMoveEvent)
+    lib.m3World_HitEvents.argtypes = [m3WorldId, C.POINTER(C.c_int32)]
+    lib.m3World_HitEvents.restype = C.POINTER(m3HitEvent)
+    lib.m3World_HitEventsDropped.argtypes = [m3WorldId]
+    lib.m3World_HitEventsDropped.restype = C.c_int32
     return lib
 
 
@@ -368,7 +378,7 @@ def read_events(lib: C.CDLL, world: m3WorldId, moves: bool = True) -> dict:
     """Every event stream of a world's last step as lists of (index1,
     generation) tuples (the world index is left out: it is the engine's
     own table slot); body move events add the transform's bytes and the
-    fell-asleep flag."""
+    fell-asleep flag, hit events the bytes of point, normal and speed."""
     out = {}
     for name in EVENT_STREAMS:
         n = C.c_int32(0)
@@ -385,6 +395,14 @@ def read_events(lib: C.CDLL, world: m3WorldId, moves: bool = True) -> dict:
         out["m3World_BodyMoveEvents"] = [
             (ptr[i].body.index1, ptr[i].body.generation, bytes(ptr[i].transform),
              bool(ptr[i].fellAsleep)) for i in range(n.value)]
+    n = C.c_int32(0)
+    ptr = lib.m3World_HitEvents(world, C.byref(n))
+    out["m3World_HitEvents"] = [
+        ((ptr[i].shapeA.index1, ptr[i].shapeA.generation),
+         (ptr[i].shapeB.index1, ptr[i].shapeB.generation),
+         bytes(ptr[i].point) + bytes(ptr[i].normal) + bytes(C.c_float(ptr[i].approachSpeed)))
+        for i in range(n.value)]
+    out["m3World_HitEventsDropped"] = int(lib.m3World_HitEventsDropped(world))
     return out
 
 

@@ -1,5 +1,5 @@
 // Event streams of a world's last step (world.h:207-313): contact and
-// sensor begin/end events, joint-break events and body move events.
+// sensor begin/end events, joint-break, body move and hit events.
 //
 // The device step keeps the previous step's pair list and manifolds in
 // the second pair buffer (the two buffers swap every step), records the
@@ -10,7 +10,10 @@
 // ring entries back and walks them as the reference's step does
 // (solver.c:3747-3815 for contacts, solver.c:4233-4257 for breaks); the
 // move events read the step's mover list (still in the world's scratch)
-// and the bodies' transforms.
+// and the bodies' transforms; the hit events, which need each contact's
+// impulses and its body's transform before the continuous phase moves
+// it, are the one stream the step writes itself (a flag and a record per
+// contact constraint, in the world's scratch).
 // Shape liveness and generations come from the host image, which this
 // path never changes behind the host's back (the device destroys joints
 // only, never shapes).
@@ -284,6 +287,82 @@ int32_t EnsureMoveEvents(m3HostWorld* w)
     return M3GPU_OK;
 }
 
+// Hit events of the last step (solver.c:2987-3033): the step left one
+// flag and, where set, one event per contact constraint in constraint
+// order; the first pair-capacity events are kept, the rest counted.
+int32_t EnsureHitEvents(m3HostWorld* w)
+{
+    if (w->hitEventsEpoch == w->stepEpoch)
+    {
+        return M3GPU_OK;
+    }
+    w->hitEvents.clear();
+    w->hitEventsDropped = 0;
+    if (!w->lastEpochIsStep || w->dslab == nullptr)
+    {
+        w->hitEventsEpoch = w->stepEpoch;
+        return M3GPU_OK;
+    }
+    m3WorldScalars sc;
+    int32_t rc = Cuda(cudaMemcpy(&sc, w->dv.sc, sizeof(sc), cudaMemcpyDeviceToHost),
+                      "event scalars");
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
+    const int32_t n = sc.constraintCount;
+    if (sc.status != 0 || n <= 0 || n > sc.pairCap)
+    {
+        w->hitEventsEpoch = w->stepEpoch;
+        return M3GPU_OK;
+    }
+    const uint8_t* dflags = nullptr;
+    const m3HitEvent* dhits = nullptr;
+    m3gpuDeviceHits(w, &dflags, &dhits);
+    std::vector<uint8_t> flags((size_t)n);
+    rc = Cuda(cudaMemcpy(flags.data(), dflags, (size_t)n, cudaMemcpyDeviceToHost), "hit flags");
+    if (rc != M3GPU_OK)
+    {
+        return rc;
+    }
+    int32_t last = -1;
+    for (int32_t i = 0; i < n; ++i)
+    {
+        last = flags[(size_t)i] != 0 ? i : last;
+    }
+    std::vector<m3HitEvent> records((size_t)(last + 1));
+    if (last >= 0)
+    {
+        rc = Cuda(cudaMemcpy(records.data(), dhits, sizeof(m3HitEvent) * (size_t)(last + 1),
+                             cudaMemcpyDeviceToHost),
+                  "hit events");
+        if (rc != M3GPU_OK)
+        {
+            return rc;
+        }
+    }
+    const uint16_t world0 = (uint16_t)w->slot;
+    const size_t cap = (size_t)sc.pairCap;
+    for (int32_t i = 0; i <= last; ++i)
+    {
+        if (flags[(size_t)i] == 0)
+        {
+            continue;
+        }
+        if (w->hitEvents.size() >= cap)
+        {
+            w->hitEventsDropped += 1;
+            continue;
+        }
+        m3HitEvent e = records[(size_t)i];
+        e.shapeA.world0 = world0;
+        e.shapeB.world0 = world0;
+        w->hitEvents.push_back(e);
+    }
+    w->hitEventsEpoch = w->stepEpoch;
+    return M3GPU_OK;
+}
+
 template <class T>
 const T* Stream(m3WorldId worldId, int32_t* count, std::vector<T> m3HostWorld::*member)
 {
@@ -295,8 +374,14 @@ const T* Stream(m3WorldId worldId, int32_t* count, std::vector<T> m3HostWorld::*
     }
     *count = 0;
     m3HostWorld* w = m3gpuWorldFromId(worldId);
-    const bool moves = std::is_same<T, m3BodyMoveEvent>::value;
-    if (w == nullptr || (moves ? EnsureMoveEvents(w) : EnsureEvents(w)) != M3GPU_OK)
+    int32_t rc = M3GPU_OK;
+    if (w != nullptr)
+    {
+        rc = std::is_same<T, m3BodyMoveEvent>::value ? EnsureMoveEvents(w)
+             : std::is_same<T, m3HitEvent>::value    ? EnsureHitEvents(w)
+                                                     : EnsureEvents(w);
+    }
+    if (w == nullptr || rc != M3GPU_OK)
     {
         return nullptr;
     }
@@ -335,4 +420,21 @@ extern "C" const m3JointBreakEvent* m3World_JointBreakEvents(m3WorldId worldId, 
 extern "C" const m3BodyMoveEvent* m3World_BodyMoveEvents(m3WorldId worldId, int32_t* count)
 {
     return Stream(worldId, count, &m3HostWorld::moveEvents);
+}
+
+extern "C" const m3HitEvent* m3World_HitEvents(m3WorldId worldId, int32_t* count)
+{
+    return Stream(worldId, count, &m3HostWorld::hitEvents);
+}
+
+extern "C" int32_t m3World_HitEventsDropped(m3WorldId worldId)
+{
+    M3_DEVICE_GUARD;
+    m3gpuClearError();
+    m3HostWorld* w = m3gpuWorldFromId(worldId);
+    if (w == nullptr || EnsureHitEvents(w) != M3GPU_OK)
+    {
+        return 0;
+    }
+    return w->hitEventsDropped;
 }

@@ -687,6 +687,58 @@ __device__ void m3StoreContact(const m3ConRef& c, m3Manifold* manifolds)
     manifold->rollingImpulse = v3(c.a(M3A_ROLLING), c.a(M3A_ROLLING + 1), c.a(M3A_ROLLING + 2));
 }
 
+// The hit event of one contact constraint (solver.c:2987-3033), if any:
+// for a pair with a hit-enabled shape, the fastest-approaching point whose
+// approach beat `threshold` and whose impulse fired.  Written after the
+// impulses are final and before the continuous phase moves any body, as
+// the reference's store does; shape ids carry the world index 0 (the host
+// fills it in).  Returns whether there is one.
+__device__ bool m3HitCandidate(const m3WorldView& w, const m3ConRef& c, const uint64_t* keys,
+                               m3real threshold, m3HitEvent* out)
+{
+    const uint64_t key = keys[c.n(M3C_MANIFOLD)];
+    const int32_t shapeA = (int32_t)(key >> 32);
+    const int32_t shapeB = (int32_t)(key & 0xFFFFFFFFu);
+    if (w.hitEvents[shapeA] == 0 && w.hitEvents[shapeB] == 0)
+    {
+        return false;
+    }
+    const int32_t pc = c.n(M3C_POINTS);
+    int32_t best = -1;
+    m3real bestSpeed = 0.0f;
+    for (int32_t k = 0; k < pc; ++k)
+    {
+        const m3real rv = c.f(M3C_POINT0 + M3C_POINT_WORDS * k + 9);
+        if (rv < -threshold && c.a(M3A_TOTAL_NORMAL + k) > 0.0f && (best < 0 || rv < bestSpeed))
+        {
+            best = k;
+            bestSpeed = rv;
+        }
+    }
+    if (best < 0)
+    {
+        return false;
+    }
+    const int32_t bodyA = c.n(M3C_BODY_A);
+    const m3Transform xf = w.xf[bodyA];
+    const m3Vec3 lcA = m3RotateVec3(xf.q, w.lc[bodyA]);
+    const m3Vec3 rA = c.v(M3C_POINT0 + M3C_POINT_WORDS * best);
+    m3HitEvent e;
+    e.shapeA.index1 = shapeA + 1;
+    e.shapeA.world0 = 0;
+    e.shapeA.generation = w.shapeGen[shapeA];
+    e.shapeB.index1 = shapeB + 1;
+    e.shapeB.world0 = 0;
+    e.shapeB.generation = w.shapeGen[shapeB];
+    e.point.x = xf.p.x + (double)lcA.x + (double)rA.x;
+    e.point.y = xf.p.y + (double)lcA.y + (double)rA.y;
+    e.point.z = xf.p.z + (double)lcA.z + (double)rA.z;
+    e.normal = c.v(M3C_NORMAL);
+    e.approachSpeed = -bestSpeed;
+    *out = e;
+    return true;
+}
+
 // Implicit gyroscopic step, one Newton iteration in body coordinates,
 // isotropic tensors gated out (solver.c:2933-2977).
 __device__ m3Vec3 m3GyroscopicOmega(const m3WorldView& w, int32_t body, m3Vec3 om, m3real h)

@@ -209,6 +209,10 @@ struct m3HostWorld
     // body's transform back).
     uint64_t moveEventsEpoch = 0;
     std::vector<m3BodyMoveEvent> moveEvents;
+    // Hit events, likewise built on their own first read.
+    uint64_t hitEventsEpoch = 0;
+    std::vector<m3HitEvent> hitEvents;
+    int32_t hitEventsDropped = 0;
     // Journal recording (world.c:1348-1398): records appended to the
     // caller's buffer while active; overflow latches and ends it.
     uint8_t* journalBuffer = nullptr;
@@ -377,6 +381,9 @@ inline void m3MarkEventEpoch(m3HostWorld* w, bool stepped)
 // indices; its length is the scalars' moverCount) in a world's slab
 // scratch (step.cu).
 const int32_t* m3gpuDeviceMovers(const m3HostWorld* w);
+// The device addresses of the last step's per-constraint hit flags and
+// hit events (constraint order; the scalars' constraintCount entries).
+void m3gpuDeviceHits(const m3HostWorld* w, const uint8_t** flags, const m3HitEvent** hits);
 
 // Step and hash entry points (step.cu).
 // `ops` (optional) are body commands applied on the device before the

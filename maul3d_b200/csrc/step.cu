@@ -169,6 +169,8 @@ struct m3Scratch
     int32_t* wideWork;     // the wide prepare kernel's grid-shared words (M3_WW_*)
     int32_t* jointAdj;     // 2 per joint row: rows by body (the wide joint levels)
     int2* jointPrev;       // per joint row: the previous row on each of its bodies
+    uint8_t* hitFlag;      // per contact constraint: whether the step left a hit event
+    m3HitEvent* hits;      // per contact constraint: that event (world index 0)
 };
 
 static __host__ __device__ inline int64_t NextPow2(int64_t n)
@@ -250,6 +252,8 @@ static __host__ __device__ inline int64_t ScratchCarve(m3Scratch* s, uint8_t* ba
     M3_CARVE(wideWork, int32_t, M3_WW_WORDS)
     M3_CARVE(jointAdj, int32_t, 2 * (int64_t)jointCap)
     M3_CARVE(jointPrev, int2, jointCap)
+    M3_CARVE(hitFlag, uint8_t, pairCap)
+    M3_CARVE(hits, m3HitEvent, pairCap)
     M3_CARVE(treeMoveBox, m3Aabb, (int64_t)treeLag * shapeCap)
     M3_CARVE(treeMoveShape, int32_t, (int64_t)treeLag * shapeCap)
 #undef M3_CARVE
@@ -2427,6 +2431,18 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3SubstepKernel(const m3WorldV
     {
         m3StoreContact(m3ConAt(s.rows, i), man);
     }
+    // Hit events, per constraint in constraint order (solver.c:2987-3033).
+    {
+        const uint64_t* keys = sc->pairBuf == 0 ? w.keys0 : w.keys1;
+        const m3real hitThreshold = sc->hitEventThreshold;
+        for (int32_t i = tid; i < constraintCount; i += NT)
+        {
+            s.hitFlag[i] = m3HitCandidate(w, m3ConAt(s.rows, s.conSlot[i]), keys, hitThreshold,
+                                          &s.hits[i])
+                               ? 1
+                               : 0;
+        }
+    }
     for (int32_t r = tid; r < jointCount; r += NT)
     {
         m3StoreJoint(w, &jrows[r]);
@@ -3515,6 +3531,17 @@ __global__ void __launch_bounds__(NT, 2) m3WideSubstepKernel(const m3WorldView* 
     {
         m3StoreContact(m3ConAt(s.rows, i), man);
     }
+    {
+        const uint64_t* keys = ((volatile int32_t*)&sc->pairBuf)[0] == 0 ? w.keys0 : w.keys1;
+        const m3real hitThreshold = sc->hitEventThreshold;
+        for (int32_t i = gtid; i < constraintCount; i += gstride)
+        {
+            s.hitFlag[i] = m3HitCandidate(w, m3ConAt(s.rows, s.conSlot[i]), keys, hitThreshold,
+                                          &s.hits[i])
+                               ? 1
+                               : 0;
+        }
+    }
     for (int32_t r = gtid; r < jointCount; r += gstride)
     {
         m3StoreJoint(w, &jrows[r]);
@@ -4564,6 +4591,14 @@ const int32_t* m3gpuDeviceMovers(const m3HostWorld* w)
     return s.movers;
 }
 
+void m3gpuDeviceHits(const m3HostWorld* w, const uint8_t** flags, const m3HitEvent** hits)
+{
+    m3Scratch s;
+    ScratchCarve(&s, w->dv.scratch, w->bodyCap, w->shapeCap, w->jointCap, w->pairCap);
+    *flags = s.hitFlag;
+    *hits = s.hits;
+}
+
 extern "C" int32_t m3gpu_get_packing(m3gpuPacking* out)
 {
     M3_DEVICE_GUARD;
@@ -5608,6 +5643,19 @@ extern "C" int32_t m3gpu_step_world_noalloc(m3WorldId worldId, float dt, int32_t
                               sizeof(int32_t) * (size_t)w->hv.sc->bodyMax,
                               cudaMemcpyDeviceToDevice),
                    "noalloc movers");
+        // And its hit events.
+        if (rc == M3GPU_OK)
+        {
+            rc = Check(cudaMemcpy(to.hitFlag, from.hitFlag, (size_t)w->pairCap,
+                                  cudaMemcpyDeviceToDevice),
+                       "noalloc hit flags");
+        }
+        if (rc == M3GPU_OK)
+        {
+            rc = Check(cudaMemcpy(to.hits, from.hits, sizeof(m3HitEvent) * (size_t)w->pairCap,
+                                  cudaMemcpyDeviceToDevice),
+                       "noalloc hit events");
+        }
         if (rc != M3GPU_OK)
         {
             return rc;
