@@ -359,7 +359,7 @@ def terrain_run(m3, args, seed: int) -> dict:
             "bit_exact_check": {"worlds_checked": len(sample), "mismatches": mismatches}}
 
 
-SERVING_RATES = [100.0, 1000.0, 4000.0, 20000.0, 0.0]
+SERVING_RATES = [100.0, 400.0, 1000.0, 4000.0, 20000.0, 0.0]
 SERVING_CLIENTS = 4
 # At most this many requests preparing or active: a tick steps every
 # active request's frame, so the cap bounds a tick's time (and with it the
