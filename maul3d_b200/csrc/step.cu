@@ -171,6 +171,8 @@ struct m3Scratch
     int2* jointPrev;       // per joint row: the previous row on each of its bodies
     uint8_t* hitFlag;      // per contact constraint: whether the step left a hit event
     m3HitEvent* hits;      // per contact constraint: that event (world index 0)
+    m3Transform* xfPre;    // per body: its end pose before a continuous pull-back
+    uint8_t* pulled;       // per body: whether the continuous phase pulled it back
 };
 
 static __host__ __device__ inline int64_t NextPow2(int64_t n)
@@ -254,6 +256,8 @@ static __host__ __device__ inline int64_t ScratchCarve(m3Scratch* s, uint8_t* ba
     M3_CARVE(jointPrev, int2, jointCap)
     M3_CARVE(hitFlag, uint8_t, pairCap)
     M3_CARVE(hits, m3HitEvent, pairCap)
+    M3_CARVE(xfPre, m3Transform, bodyCap)
+    M3_CARVE(pulled, uint8_t, bodyCap)
     M3_CARVE(treeMoveBox, m3Aabb, (int64_t)treeLag * shapeCap)
     M3_CARVE(treeMoveShape, int32_t, (int64_t)treeLag * shapeCap)
 #undef M3_CARVE
@@ -3656,6 +3660,82 @@ __global__ void m3WideStatusKernel(const m3WorldView* views, const int32_t* orde
     }
 }
 
+// A bullet's sweep against the moving bodies (solver.c:3237-3270 with
+// the non-static branch): every alive, enabled, non-bullet, non-sensor
+// shape of another non-static body whose current tree leaf (the
+// broadphase's copy, refreshed this step) touches the swept box
+// [lo, hi] and that the filters let through, swept with the target's own
+// motion.  The reference visits bodies in ascending order, so a target
+// below the bullet shows its pose after its own pull-back and one above
+// it its pose before; bullets never sweep against bullets.  Counts the
+// hits below `limit` like SweepStaticTargets and leaves the last one's
+// fraction in *hitFraction.
+__device__ __noinline__ int32_t SweepMovingTargets(const m3WorldView& w, const m3Scratch& s,
+                                                   int32_t bullet, int32_t sh, const double* lo,
+                                                   const double* hi, const m3Pos3& base,
+                                                   const m3ProxyDev& proxyB,
+                                                   const m3SweepDev& fastSweep, m3real limit,
+                                                   m3real* hitFraction)
+{
+    int32_t hits = 0;
+    const int32_t shapeMax = w.sc->shapeMax;
+    for (int32_t o = 0; o < shapeMax; ++o)
+    {
+        if (w.shapeAlive[o] == 0 || w.shapeType[o] == M3_SHAPE_PLANE || o == sh ||
+            s.hasLeaf[o] == 0 || w.sensor[o] != 0)
+        {
+            continue;
+        }
+        const int32_t ob = w.shapeBody[o];
+        if (ob == bullet || w.btype[ob] == M3_BODY_STATIC || w.enabled[ob] == 0 ||
+            w.bullet[ob] != 0)
+        {
+            continue;
+        }
+        const m3Aabb& leaf = s.leafBox[o];
+        if (!(leaf.lo[0] <= hi[0] && lo[0] <= leaf.hi[0] && leaf.lo[1] <= hi[1] &&
+              lo[1] <= leaf.hi[1] && leaf.lo[2] <= hi[2] && lo[2] <= leaf.hi[2]))
+        {
+            continue;
+        }
+        const int32_t gi = w.group[o];
+        if (gi != 0 && gi == w.group[sh])
+        {
+            if (gi < 0)
+            {
+                continue;
+            }
+        }
+        else if (!((w.category[o] & w.mask[sh]) != 0 && (w.category[sh] & w.mask[o]) != 0))
+        {
+            continue;
+        }
+        m3Vec3 scratchA[2];
+        m3ProxyDev proxyA;
+        proxyA.count = ProxyPoints(w, o, &proxyA.points, scratchA, &proxyA.radius);
+        const m3Pos3 oc0 = s.com0[ob];
+        const m3Transform oxf = (ob > bullet && s.pulled[ob] != 0) ? s.xfPre[ob] : w.xf[ob];
+        const m3Vec3 orlc = m3RotateVec3(oxf.q, w.lc[ob]);
+        m3SweepDev sweepA;
+        sweepA.localCenter = w.lc[ob];
+        sweepA.c1 = v3((m3real)(oc0.x - base.x), (m3real)(oc0.y - base.y),
+                       (m3real)(oc0.z - base.z));
+        sweepA.c2 = v3((m3real)(oxf.p.x + (double)orlc.x - base.x),
+                       (m3real)(oxf.p.y + (double)orlc.y - base.y),
+                       (m3real)(oxf.p.z + (double)orlc.z - base.z));
+        sweepA.q1 = s.rot0[ob];
+        sweepA.q2 = oxf.q;
+        int32_t state;
+        const m3real t = m3TimeOfImpactDev(proxyA, sweepA, proxyB, fastSweep, limit, &state);
+        if (state == M3_TOI_HIT && 0.0f < t && t < limit)
+        {
+            hits += 1;
+            *hitFraction = t;
+        }
+    }
+    return hits;
+}
+
 // ---------------------------------------------------------------------
 // The tree arm of the continuous phase for one shape of a fast body
 // (solver.c:3081-3274): every static target whose tree leaf touches the
@@ -3785,9 +3865,12 @@ __global__ void __launch_bounds__(M3_BLOCK, 2) m3FinishKernel(const m3WorldView*
     const int32_t moverCount = s.plan->moverCount;
     // Continuous phase (solver.c:3349-3425).  A non-bullet fast body
     // sweeps only against static targets, and a pull-back moves only the
-    // fast body itself, so bodies are independent and run in parallel.
-    // Static tree targets and then planes are swept per shape; a bullet,
-    // a mesh or voxel target, or two tree hits for one shape are refused.
+    // fast body itself, so those bodies are independent and run in
+    // parallel.  Bullets follow, also in parallel (they never sweep
+    // against one another), each seeing every moving target as the
+    // reference's ascending walk would.  Tree targets and then planes are
+    // swept per shape; a mesh or voxel target, or two tree hits for one
+    // shape (whose order would matter), are refused.
     if (sc->continuousEnabled != 0)
     {
         // The targets, once per step and ascending: the static non-plane
@@ -3855,99 +3938,133 @@ __global__ void __launch_bounds__(M3_BLOCK, 2) m3FinishKernel(const m3WorldView*
         const int32_t planeCount = s_planeCount;
         for (int32_t i = tid; i < bodyMax; i += M3_BLOCK)
         {
-            if (w.bodyAlive[i] == 0 || w.btype[i] != M3_BODY_DYNAMIC)
+            s.pulled[i] = 0;
+        }
+        __syncthreads();
+        // Two passes: the non-bullets (independent of one another), then
+        // the bullets, which also sweep against moving bodies and must see
+        // each target as the reference's ascending walk leaves it.
+        for (int32_t pass = 0; pass < 2; ++pass)
+        {
+            if (pass == 1)
             {
-                continue;
+                __syncthreads();
             }
-            const m3Transform xfEnd = w.xf[i];
-            m3Vec3 rlc = m3RotateVec3(xfEnd.q, w.lc[i]);
-            double cx = xfEnd.p.x + (double)rlc.x;
-            double cy = xfEnd.p.y + (double)rlc.y;
-            double cz = xfEnd.p.z + (double)rlc.z;
-            const m3Pos3 c0 = s.com0[i];
-            m3Vec3 dc = v3((m3real)(cx - c0.x), (m3real)(cy - c0.y), (m3real)(cz - c0.z));
-            m3Quat q0 = s.rot0[i];
-            m3Quat dq = m3MulQuat(xfEnd.q, q4(-q0.x, -q0.y, -q0.z, q0.w));
-            m3real arc = 2.0f * sqrtf(dq.x * dq.x + dq.y * dq.y + dq.z * dq.z) * w.maxExt[i];
-            m3real maxMotion = sqrtf(m3Dot3(dc, dc)) + arc;
-            if (!(maxMotion > 0.5f * w.minExt[i]))
+            for (int32_t i = tid; i < bodyMax; i += M3_BLOCK)
             {
-                continue;
-            }
-            if (w.bullet[i] != 0)
-            {
-                s_status = M3GPU_ERR_UNSUPPORTED;
-                sc->statusDetail = 3001;
-                continue;
-            }
-            // Relative sweep about the begin centre (MakeRelativeSweep).
-            const m3Pos3 base = c0;
-            const m3Vec3 lc = w.lc[i];
-            const m3Vec3 sc1 = v3((m3real)(c0.x - base.x), (m3real)(c0.y - base.y),
-                                  (m3real)(c0.z - base.z));
-            const m3Vec3 sc2 = v3((m3real)(xfEnd.p.x + (double)rlc.x - base.x),
-                                  (m3real)(xfEnd.p.y + (double)rlc.y - base.y),
-                                  (m3real)(xfEnd.p.z + (double)rlc.z - base.z));
-            m3real fraction = 1.0f;
-            double pad = (double)(w.maxExt[i] + M3_AABB_MARGIN);
-            double lo[3] = {(c0.x < cx ? c0.x : cx) - pad, (c0.y < cy ? c0.y : cy) - pad,
-                            (c0.z < cz ? c0.z : cz) - pad};
-            double hi[3] = {(c0.x > cx ? c0.x : cx) + pad, (c0.y > cy ? c0.y : cy) + pad,
-                            (c0.z > cz ? c0.z : cz) + pad};
-            m3SweepDev fastSweep;
-            fastSweep.localCenter = lc;
-            fastSweep.c1 = sc1;
-            fastSweep.c2 = sc2;
-            fastSweep.q1 = q0;
-            fastSweep.q2 = xfEnd.q;
-            for (int32_t sh = w.shapeHead[i]; sh != -1; sh = w.shapeNext[sh])
-            {
-                if (w.sensor[sh] != 0)
+                if (w.bodyAlive[i] == 0 || w.btype[i] != M3_BODY_DYNAMIC ||
+                    (w.bullet[i] != 0) != (pass == 1))
                 {
                     continue;
                 }
-                // The tree query (solver.c:3081-3274): static targets whose
-                // tree leaf touches the swept box, each swept by the time
-                // of impact.  Static leaves never move, so their boxes are
-                // read straight from the tree.  The reference visits them
-                // in tree order, each call bounded by the fraction so far;
-                // with one hit the order does not matter (every target
-                // sees the fraction of the earlier shapes), with two or
-                // more it would, and the world is refused.
-                m3Vec3 scratchB[2];
-                m3ProxyDev proxyB;
-                proxyB.count = ProxyPoints(w, sh, &proxyB.points, scratchB, &proxyB.radius);
-                int32_t refusal = 0;
-                const int32_t hits =
-                    staticTargets ? SweepStaticTargets(w, s.com0, s.rot0, i, sh, targets,
-                                                       targetCount, lo, hi, base, proxyB,
-                                                       fastSweep, &fraction, &refusal)
-                                  : 0;
-                if (refusal != 0)
+                const m3Transform xfEnd = w.xf[i];
+                m3Vec3 rlc = m3RotateVec3(xfEnd.q, w.lc[i]);
+                double cx = xfEnd.p.x + (double)rlc.x;
+                double cy = xfEnd.p.y + (double)rlc.y;
+                double cz = xfEnd.p.z + (double)rlc.z;
+                const m3Pos3 c0 = s.com0[i];
+                m3Vec3 dc = v3((m3real)(cx - c0.x), (m3real)(cy - c0.y), (m3real)(cz - c0.z));
+                m3Quat q0 = s.rot0[i];
+                m3Quat dq = m3MulQuat(xfEnd.q, q4(-q0.x, -q0.y, -q0.z, q0.w));
+                m3real arc = 2.0f * sqrtf(dq.x * dq.x + dq.y * dq.y + dq.z * dq.z) * w.maxExt[i];
+                m3real maxMotion = sqrtf(m3Dot3(dc, dc)) + arc;
+                if (!(maxMotion > 0.5f * w.minExt[i]))
                 {
+                    continue;
+                }
+                if (pass == 1 && sc->treeTracked == 0)
+                {
+                    // A world that keeps no tree keeps no leaf boxes to query.
                     s_status = M3GPU_ERR_UNSUPPORTED;
-                    sc->statusDetail = refusal;
+                    sc->statusDetail = 3001;
+                    continue;
                 }
-                if (hits > 1)
+                // Relative sweep about the begin centre (MakeRelativeSweep).
+                const m3Pos3 base = c0;
+                const m3Vec3 lc = w.lc[i];
+                const m3Vec3 sc1 = v3((m3real)(c0.x - base.x), (m3real)(c0.y - base.y),
+                                      (m3real)(c0.z - base.z));
+                const m3Vec3 sc2 = v3((m3real)(xfEnd.p.x + (double)rlc.x - base.x),
+                                      (m3real)(xfEnd.p.y + (double)rlc.y - base.y),
+                                      (m3real)(xfEnd.p.z + (double)rlc.z - base.z));
+                m3real fraction = 1.0f;
+                double pad = (double)(w.maxExt[i] + M3_AABB_MARGIN);
+                double lo[3] = {(c0.x < cx ? c0.x : cx) - pad, (c0.y < cy ? c0.y : cy) - pad,
+                                (c0.z < cz ? c0.z : cz) - pad};
+                double hi[3] = {(c0.x > cx ? c0.x : cx) + pad, (c0.y > cy ? c0.y : cy) + pad,
+                                (c0.z > cz ? c0.z : cz) + pad};
+                m3SweepDev fastSweep;
+                fastSweep.localCenter = lc;
+                fastSweep.c1 = sc1;
+                fastSweep.c2 = sc2;
+                fastSweep.q1 = q0;
+                fastSweep.q2 = xfEnd.q;
+                for (int32_t sh = w.shapeHead[i]; sh != -1; sh = w.shapeNext[sh])
                 {
-                    s_status = M3GPU_ERR_UNSUPPORTED;
-                    sc->statusDetail = 3002;
+                    if (w.sensor[sh] != 0)
+                    {
+                        continue;
+                    }
+                    // The tree query (solver.c:3081-3274): static targets whose
+                    // tree leaf touches the swept box, each swept by the time
+                    // of impact.  Static leaves never move, so their boxes are
+                    // read straight from the tree.  The reference visits them
+                    // in tree order, each call bounded by the fraction so far;
+                    // with one hit the order does not matter (every target
+                    // sees the fraction of the earlier shapes), with two or
+                    // more it would, and the world is refused.
+                    m3Vec3 scratchB[2];
+                    m3ProxyDev proxyB;
+                    proxyB.count = ProxyPoints(w, sh, &proxyB.points, scratchB, &proxyB.radius);
+                    int32_t refusal = 0;
+                    const m3real entry = fraction;
+                    int32_t hits =
+                        staticTargets ? SweepStaticTargets(w, s.com0, s.rot0, i, sh, targets,
+                                                           targetCount, lo, hi, base, proxyB,
+                                                           fastSweep, &fraction, &refusal)
+                                      : 0;
+                    if (pass == 1)
+                    {
+                        // A bullet's moving targets, bounded by the same entry
+                        // fraction: with one hit in all, the order is moot.
+                        m3real moving = entry;
+                        const int32_t movingHits = SweepMovingTargets(w, s, i, sh, lo, hi, base,
+                                                                      proxyB, fastSweep, entry,
+                                                                      &moving);
+                        if (movingHits == 1 && hits == 0)
+                        {
+                            fraction = moving;
+                        }
+                        hits += movingHits;
+                    }
+                    if (refusal != 0)
+                    {
+                        s_status = M3GPU_ERR_UNSUPPORTED;
+                        sc->statusDetail = refusal;
+                    }
+                    if (hits > 1)
+                    {
+                        s_status = M3GPU_ERR_UNSUPPORTED;
+                        sc->statusDetail = 3002;
+                    }
+                    for (int32_t k = 0; k < planeCount; ++k)
+                    {
+                        ContinuousVersusPlane(w, i, sh, s_planeList[k], base, lc, sc1, sc2, q0,
+                                              xfEnd.q, &fraction);
+                    }
                 }
-                for (int32_t k = 0; k < planeCount; ++k)
+                if (fraction < 1.0f)
                 {
-                    ContinuousVersusPlane(w, i, sh, s_planeList[k], base, lc, sc1, sc2, q0,
-                                          xfEnd.q, &fraction);
+                    m3Transform xf = SweepTransform(lc, sc1, sc2, q0, xfEnd.q, fraction);
+                    m3Transform out;
+                    out.q = xf.q;
+                    out.p.x = base.x + xf.p.x;
+                    out.p.y = base.y + xf.p.y;
+                    out.p.z = base.z + xf.p.z;
+                    s.xfPre[i] = xfEnd;
+                    s.pulled[i] = 1;
+                    w.xf[i] = out;
                 }
-            }
-            if (fraction < 1.0f)
-            {
-                m3Transform xf = SweepTransform(lc, sc1, sc2, q0, xfEnd.q, fraction);
-                m3Transform out;
-                out.q = xf.q;
-                out.p.x = base.x + xf.p.x;
-                out.p.y = base.y + xf.p.y;
-                out.p.z = base.z + xf.p.z;
-                w.xf[i] = out;
             }
         }
         __syncthreads();
