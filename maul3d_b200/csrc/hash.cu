@@ -27,9 +27,10 @@
 //
 // The stream itself is the record sequence of m3_hash.h (header, bodies,
 // shapes, joints, pair count, pairs).  Each round of the outer loop
-// stages up to one record per thread into shared memory (lengths by a
-// counting pass and a block scan, then the bytes) and hashes the staged
-// bytes tile by tile, carrying (lo, hi) across tiles and rounds.  The
+// stages up to one record per thread of the block's first half into
+// shared memory (lengths by a counting pass and a block scan, then the
+// bytes) and hashes the staged bytes tile by tile, carrying (lo, hi)
+// across tiles and rounds.  The
 // result is bit-identical to m3WorldHashView.
 #include "m3_world.h"
 #include "m3_hash.h"
@@ -39,7 +40,11 @@
 #define M3H_BLOCK 256
 #define M3H_WARPS (M3H_BLOCK / 32)
 #define M3H_RECORD_MAX 256 // longest record of the stream (a body: 197 bytes)
-#define M3H_STAGE_BYTES (M3H_BLOCK * M3H_RECORD_MAX)
+// Records staged per round: half the block, so that the stage (32 KB)
+// lets four blocks share an SM (the registers allow four; a 64 KB stage
+// allowed three).
+#define M3H_ROUND_RECORDS (M3H_BLOCK / 2)
+#define M3H_STAGE_BYTES (M3H_ROUND_RECORDS * M3H_RECORD_MAX)
 #define M3H_CHUNK 32
 #define M3H_TILE (M3H_BLOCK * M3H_CHUNK)
 #define M3H_MUL 435u // P = 2^40 + 435
@@ -377,11 +382,11 @@ __global__ void __launch_bounds__(M3H_BLOCK) m3HashKernel(const m3WorldView* vie
     const int32_t records = m3HashRecordCount(w);
     uint32_t lo = (uint32_t)M3_HASH_INIT;
     uint32_t hi = (uint32_t)(M3_HASH_INIT >> 32);
-    for (int32_t r0 = 0; r0 < records; r0 += M3H_BLOCK)
+    for (int32_t r0 = 0; r0 < records; r0 += M3H_ROUND_RECORDS)
     {
         const int32_t r = r0 + tid;
         int32_t len = 0;
-        if (r < records)
+        if (tid < M3H_ROUND_RECORDS && r < records)
         {
             m3CountSink c{0};
             m3HashRecord(w, r, c);
