@@ -356,7 +356,7 @@ __device__ void FnvTile(const uint8_t* tile, int32_t n, uint32_t& lo, uint32_t& 
     hi = hA * hi + hC;
 }
 
-__global__ void __launch_bounds__(M3H_BLOCK) m3HashKernel(const m3WorldView* views,
+__global__ void __launch_bounds__(M3H_BLOCK, 5) m3HashKernel(const m3WorldView* views,
                                                           const int32_t* order, int32_t count,
                                                           uint64_t* out)
 {
