@@ -1549,6 +1549,8 @@ __device__ void ContinuousVersusPlane(const m3WorldView& w, int32_t body, int32_
 // Shared-memory bytes per body of the substep-loop cache: v, w, the
 // position delta (12 B each) and the rotation delta (16 B).
 #define M3_BODY_CACHE_BYTES 52
+// Velocities alone (linear and angular).
+#define M3_BODY_VELOCITY_BYTES 24
 // Dynamic shared memory per block that still lets two 256-thread blocks
 // share an SM (228 KB per SM, 1 KB reserved per block, static arrays).
 #define M3_TWO_BLOCK_SMEM (110 * 1024)
@@ -2267,6 +2269,23 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3SubstepKernel(const m3WorldV
     m3Vec3* dP = s.deltaPos;
     m3Quat* dQ = s.deltaRot;
     const bool cached = (int64_t)bodyMax * M3_BODY_CACHE_BYTES <= (int64_t)cacheBytes;
+    // A world too large for the whole cache keeps at least its velocities
+    // there (the rows' read-modify-write chain); the substep deltas, which
+    // rows only read, stay in global memory.
+    const bool cachedV =
+        !cached && (int64_t)bodyMax * M3_BODY_VELOCITY_BYTES <= (int64_t)cacheBytes;
+    if (cachedV)
+    {
+        m3Vec3* cv = (m3Vec3*)s_bodyCache;
+        m3Vec3* cw = cv + bodyMax;
+        for (int32_t i = tid; i < bodyMax; i += NT)
+        {
+            cv[i] = w.v[i];
+            cw[i] = w.w[i];
+        }
+        wl.v = cv;
+        wl.w = cw;
+    }
     if (cached)
     {
         m3Quat* cq = (m3Quat*)s_bodyCache;
@@ -2290,8 +2309,12 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3SubstepKernel(const m3WorldV
     // dependency chain is a sequence of single-thread row solves, each
     // bound by the latency of its row reads.
     const m3Mat3* invI = s.bodyInvI;
-    int64_t smemUsed = m3AlignUp(cached ? (int64_t)bodyMax * M3_BODY_CACHE_BYTES : 0, 16);
-    if (cached && smemUsed + (int64_t)bodyMax * (int64_t)sizeof(m3Mat3) <= (int64_t)cacheBytes)
+    int64_t smemUsed = m3AlignUp(cached    ? (int64_t)bodyMax * M3_BODY_CACHE_BYTES
+                                 : cachedV ? (int64_t)bodyMax * M3_BODY_VELOCITY_BYTES
+                                           : 0,
+                                 16);
+    if ((cached || cachedV) &&
+        smemUsed + (int64_t)bodyMax * (int64_t)sizeof(m3Mat3) <= (int64_t)cacheBytes)
     {
         m3Mat3* table = (m3Mat3*)(s_bodyCache + smemUsed);
         const int32_t words = bodyMax * (int32_t)(sizeof(m3Mat3) / 4);
@@ -2422,7 +2445,7 @@ __global__ void __launch_bounds__(NT, MIN_BLOCKS) m3SubstepKernel(const m3WorldV
         }
     }
     __syncthreads();
-    if (cached)
+    if (cached || cachedV)
     {
         for (int32_t i = tid; i < bodyMax; i += NT)
         {

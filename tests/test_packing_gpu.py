@@ -124,3 +124,30 @@ def test_packing_change_reclassifies_a_prepared_batch(m3, reference_traces, rest
     assert got == [t[STEPS - 1] for t in reference_traces]
     for w in worlds:
         w.destroy()
+
+
+def test_world_beyond_the_body_cache_in_a_batch(m3, oracle, restore_packing):
+    """A 4,600-body world stepped in a batch (not alone, so not on the
+    wide path): its 52-byte-a-body cache would pass the 200 KB shared-memory
+    limit, so only its velocities are cached; a world that needs more than
+    even those (the 0-byte budget) keeps everything in global memory.  Both
+    match the reference every step."""
+    specs = [(SCENE_UNEVEN, 331, 4600), (SCENE_UNEVEN, 332, 300)]
+    refs = [oracle.RefWorld.scene(*spec) for spec in specs]
+    traces = []
+    for r in refs:
+        trace = []
+        for _ in range(8):
+            r.step(DT, SUB, 1)
+            trace.append(r.hash())
+        traces.append(trace)
+        r.destroy()
+    for packing in (DEFAULT, PACKINGS["no_shared"]):
+        m3.set_packing(packing)
+        worlds = [m3.World.scene(*spec) for spec in specs]
+        for step in range(8):
+            m3.step_worlds(worlds, DT, SUB, 1)
+            got = [int(h) for h in m3.hash_worlds(worlds)]
+            assert got == [t[step] for t in traces], f"step {step + 1}"
+        for w in worlds:
+            w.destroy()
