@@ -561,7 +561,7 @@ M3GPU_API int32_t m3gpu_set_packing(const m3gpuPacking* packing);
  * bit for bit m3gpu_step_worlds(worlds, count, dt, substeps, 1), and
  * recorded in an active journal the same way), timing the prepare and
  * substep stages of each step under a candidate packing: candidates
- * alternate with the packing in use, each judged against the mean of the
+ * alternate with the packing in use, each compared with the mean of the
  * steps beside it, and one that is at least 3 % faster becomes the packing
  * in use, whose neighbours are tried next.  Leaves the fastest packing
  * selected and returns it in `best` (optional) with its stage time per

@@ -295,7 +295,7 @@ extern "C" int32_t m3gpu_step_worlds_commands(const m3WorldId* worlds, int32_t c
 // the packing in use (each class bound scaled down and up, each class's
 // threads per world switched, the two larger classes' shared-memory
 // budgets switched); a candidate's step sits between two steps of the
-// packing in use and is judged against their mean, so the slow drift of
+// packing in use and is compared with their mean, so the slow drift of
 // a settling batch cancels.  A candidate at least 3 % faster is adopted
 // and its own neighbours are tried next.
 // ---------------------------------------------------------------------
