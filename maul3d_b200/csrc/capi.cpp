@@ -294,10 +294,11 @@ extern "C" int32_t m3gpu_step_worlds_commands(const m3WorldId* worlds, int32_t c
 // its steps is a real step of the batch.  Candidates are the neighbours of
 // the packing in use (each class bound scaled down and up, each class's
 // threads per world switched, the two larger classes' shared-memory
-// budgets switched); a candidate's step sits between two steps of the
-// packing in use and is compared with their mean, so the slow drift of
-// a settling batch cancels.  A candidate at least 3 % faster is adopted
-// and its own neighbours are tried next.
+// budgets switched, the largest class at two worlds per SM); a
+// candidate's step sits between two steps of the packing in use and is
+// compared with their mean, so the slow drift of a settling batch
+// cancels.  A candidate at least 3 % faster is adopted and its own
+// neighbours are tried next.
 // ---------------------------------------------------------------------
 namespace
 {
@@ -345,8 +346,17 @@ std::vector<m3gpuPacking> PackingNeighbours(const m3gpuPacking& p)
     q = p;
     q.threads[2] = p.threads[2] == 128 ? 256 : 128;
     push(q);
+    // The largest class at two worlds per SM: the most shared memory two
+    // blocks can have (a 2048-body world's body cache and joint rows fit;
+    // its inverse-inertia table stays in global memory), alone and with
+    // 256 threads a world (the register file then holds two).
+    const int32_t twoPerSm = 113664;
     q = p;
-    q.smemBytes[0] = p.smemBytes[0] > 110 * 1024 ? 110 * 1024 : 200 * 1024;
+    q.smemBytes[0] = p.smemBytes[0] > twoPerSm ? twoPerSm : 200 * 1024;
+    push(q);
+    q = p;
+    q.threads[0] = 256;
+    q.smemBytes[0] = twoPerSm;
     push(q);
     q = p;
     q.smemBytes[1] = p.smemBytes[1] > 54 * 1024 ? 54 * 1024 : 110 * 1024;
@@ -396,9 +406,15 @@ extern "C" int32_t m3gpu_autotune_packing(const m3WorldId* worlds, int32_t count
     }
     int32_t done = 0;
     // One real step under packing `p`; its prepare and substep stages'
-    // device time in *ms.
+    // device time in *ms.  The broadphase trees' pending moves are
+    // replayed first, untimed: a replay launched beside the step (every
+    // 16 steps) would share the SMs with it and slow the stages timed.
     auto measure = [&](const m3gpuPacking& p, float* ms) -> int32_t {
-        int32_t r = m3gpu_set_packing(&p);
+        int32_t r = m3gpu_flush_trees(worlds, count);
+        if (r == M3GPU_OK)
+        {
+            r = m3gpu_set_packing(&p);
+        }
         if (r == M3GPU_OK)
         {
             r = m3gpuStepBatch(ws.data(), count, dt, substeps, 1);
