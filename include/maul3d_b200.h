@@ -201,6 +201,25 @@ M3GPU_API void m3DestroyWorld(m3WorldId worldId);
 /* world.h:94 */
 M3GPU_API bool m3World_IsValid(m3WorldId worldId);
 
+/* World settings (world.h:92, 134-176, 288; world.c:785-1117): the same
+ * argument checks (a refused value is a no-op), the same journal records,
+ * applied from the next step on.  Turning sleeping off wakes every
+ * sleeping body.  A wind that blows needs a near-unit direction. */
+M3GPU_API void m3World_SetGravity(m3WorldId worldId, m3Vec3 gravity);
+M3GPU_API m3Vec3 m3World_GetGravity(m3WorldId worldId);
+M3GPU_API void m3World_SetContactTuning(m3WorldId worldId, float hertz, float dampingRatio,
+                                        float pushMaxSpeed);
+M3GPU_API void m3World_SetRestitutionThreshold(m3WorldId worldId, float value);
+M3GPU_API void m3World_SetMaximumLinearSpeed(m3WorldId worldId, float value);
+M3GPU_API void m3World_SetMaximumAngularSpeed(m3WorldId worldId, float value);
+M3GPU_API void m3World_EnableSleeping(m3WorldId worldId, bool flag);
+M3GPU_API bool m3World_IsSleepingEnabled(m3WorldId worldId);
+M3GPU_API void m3World_EnableContinuous(m3WorldId worldId, bool flag);
+M3GPU_API bool m3World_IsContinuousEnabled(m3WorldId worldId);
+M3GPU_API void m3World_SetHitEventThreshold(m3WorldId worldId, float value);
+M3GPU_API void m3World_SetWind(m3WorldId worldId, m3Vec3 direction, float speed, float gustHertz,
+                               float gustScale);
+
 /* snapshot.c:603 (world.h:203): the exact byte count m3World_Snapshot
  * writes, -1 for a stale id. */
 M3GPU_API int32_t m3World_SnapshotSize(m3WorldId worldId);

@@ -170,6 +170,11 @@ def journal_body_command(op: int, index1: int, generation: int, v) -> bytes:
 OP_JOINT_SET_BREAK = 55
 
 
+def journal_record(op: int, payload: bytes) -> bytes:
+    """Any record: {int32 op; int32 bytes; payload} (world.c:1348-1366)."""
+    return struct.pack("<ii", op, len(payload)) + payload
+
+
 def journal_joint_break(index1: int, generation: int, max_force: float, max_torque: float) -> bytes:
     """One joint threshold record: {m3JointId id; float maxForce, maxTorque} (world.c:3111)."""
     payload = struct.pack("<iHHff", index1, 0, generation, max_force, max_torque)
@@ -404,6 +409,29 @@ def read_events(lib: C.CDLL, world: m3WorldId, moves: bool = True) -> dict:
         for i in range(n.value)]
     out["m3World_HitEventsDropped"] = int(lib.m3World_HitEventsDropped(world))
     return out
+
+
+def bind_settings(lib: C.CDLL) -> C.CDLL:
+    """Declare the reference-named world settings on a handle."""
+    lib.m3World_SetGravity.argtypes = [m3WorldId, m3Vec3]
+    lib.m3World_GetGravity.argtypes = [m3WorldId]
+    lib.m3World_GetGravity.restype = m3Vec3
+    lib.m3World_SetContactTuning.argtypes = [m3WorldId, C.c_float, C.c_float, C.c_float]
+    for name in ("m3World_SetRestitutionThreshold", "m3World_SetMaximumLinearSpeed",
+                 "m3World_SetMaximumAngularSpeed", "m3World_SetHitEventThreshold"):
+        getattr(lib, name).argtypes = [m3WorldId, C.c_float]
+    for name in ("m3World_EnableSleeping", "m3World_EnableContinuous"):
+        getattr(lib, name).argtypes = [m3WorldId, C.c_bool]
+    for name in ("m3World_IsSleepingEnabled", "m3World_IsContinuousEnabled"):
+        getattr(lib, name).argtypes = [m3WorldId]
+        getattr(lib, name).restype = C.c_bool
+    lib.m3World_SetWind.argtypes = [m3WorldId, m3Vec3, C.c_float, C.c_float, C.c_float]
+    for name in ("m3World_SetGravity", "m3World_SetContactTuning",
+                 "m3World_SetRestitutionThreshold", "m3World_SetMaximumLinearSpeed",
+                 "m3World_SetMaximumAngularSpeed", "m3World_SetHitEventThreshold",
+                 "m3World_EnableSleeping", "m3World_EnableContinuous", "m3World_SetWind"):
+        getattr(lib, name).restype = None
+    return lib
 
 
 def bind_create(lib: C.CDLL) -> C.CDLL:

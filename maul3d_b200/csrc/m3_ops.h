@@ -19,6 +19,16 @@ enum
     M3_OP_APPLY_LINEAR_IMPULSE = 28,
     M3_OP_APPLY_ANGULAR_IMPULSE = 29,
     M3_OP_JOINT_SET_BREAK = 55,
+    // World settings (world_internal.h:146-175).
+    M3_OP_SET_GRAVITY = 39,
+    M3_OP_SET_CONTACT_TUNING = 44,
+    M3_OP_SET_RESTITUTION_THRESHOLD = 45,
+    M3_OP_SET_MAXIMUM_LINEAR_SPEED = 46,
+    M3_OP_ENABLE_SLEEPING = 47,
+    M3_OP_ENABLE_CONTINUOUS = 48,
+    M3_OP_SET_HIT_EVENT_THRESHOLD = 49,
+    M3_OP_SET_WIND = 60,
+    M3_OP_SET_MAXIMUM_ANGULAR_SPEED = 66,
 };
 
 // One command for the device kernel: `world` indexes the batch, `body`
@@ -30,6 +40,16 @@ typedef struct m3BodyOp
     int32_t body;
     m3Vec3 v;
 } m3BodyOp;
+
+// World settings: host-side records of the journal (never device ops).
+M3_HD bool m3IsWorldSettingOp(int32_t op)
+{
+    return op == M3_OP_SET_GRAVITY || op == M3_OP_SET_CONTACT_TUNING ||
+           op == M3_OP_SET_RESTITUTION_THRESHOLD || op == M3_OP_SET_MAXIMUM_LINEAR_SPEED ||
+           op == M3_OP_ENABLE_SLEEPING || op == M3_OP_ENABLE_CONTINUOUS ||
+           op == M3_OP_SET_HIT_EVENT_THRESHOLD || op == M3_OP_SET_WIND ||
+           op == M3_OP_SET_MAXIMUM_ANGULAR_SPEED;
+}
 
 // Joint commands ride the same record: `body` is then the joint slot.
 M3_HD bool m3IsJointOp(int32_t op)

@@ -344,7 +344,12 @@ struct m3JournalRecordView
     float dt;
     int32_t substeps;
     uint16_t generation; // joint records
+    float setting[6];    // world-setting records: their payload's words
 };
+// Applies a validated world-setting record (world.c:734-783, 1013-1082)
+// to the host image: the setting's fields, and for sleeping turned off
+// every sleeping dynamic body woken.  world.cpp.
+void m3ApplyWorldSetting(m3HostWorld* w, int32_t op, const float* words);
 // Parses and validates a whole journal against a world's bodies; false
 // (with the error set) on the first bad or unsupported record.
 // Worlds outside the world table (world.cpp): built on any thread,

@@ -286,6 +286,21 @@ void Retire(m3gpuServer* s, std::unique_ptr<Request>& r, uint64_t hash, int32_t 
     }
 }
 
+// Served journals carry body and joint commands and steps: the frames run
+// as device ops in a batched step.  A world-setting record is refused.
+bool NoSettings(const std::vector<m3JournalRecordView>& records)
+{
+    for (const m3JournalRecordView& rec : records)
+    {
+        if (m3IsWorldSettingOp(rec.op))
+        {
+            m3gpuSetError(M3GPU_ERR_UNSUPPORTED, "served journal: world setting op %d", rec.op);
+            return false;
+        }
+    }
+    return true;
+}
+
 // A worker's preparation of one request: its world built off the world
 // table with the snapshot's capacities, the snapshot restored into it and
 // the journal parsed and validated whole.  Touches only the request.
@@ -304,7 +319,8 @@ void Prepare(Request& r)
     int32_t code = M3GPU_OK;
     if (w == nullptr ||
         !m3gpuRestoreWorld(w, r.snapshot.data(), (int32_t)r.snapshot.size()) ||
-        !m3ParseJournal(w, r.journal.data(), (int32_t)r.journal.size(), &r.records))
+        !m3ParseJournal(w, r.journal.data(), (int32_t)r.journal.size(), &r.records) ||
+        !NoSettings(r.records))
     {
         code = m3gpu_last_error();
         code = code != M3GPU_OK ? code : M3GPU_ERR_INVALID;

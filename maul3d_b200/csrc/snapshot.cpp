@@ -1012,7 +1012,8 @@ bool m3gpuRestoreWorld(m3HostWorld* w, const void* data, int32_t size)
 
 // world.c:3187-3218 (world.h:606): replays a recorded command stream:
 // records of (op, payload bytes, payload).  Covered ops: steps (run on
-// the GPU), velocity sets, forces, torques and impulses.  The stream is
+// the GPU), velocity sets, forces, torques and impulses, joint break
+// thresholds and the world settings.  The stream is
 // validated whole before anything is applied (framing, op, payload
 // size, body ids, finite vectors, step arguments), so a refusal leaves
 // the world untouched, as the reference's snapshot-backed rollback does.
@@ -1049,7 +1050,14 @@ extern "C" bool m3World_JournalReplay(m3WorldId worldId, const void* data, int32
         {
             return false;
         }
-        m3ApplyBodyOp(w->hv, r.op, r.body, r.v);
+        if (m3IsWorldSettingOp(r.op))
+        {
+            m3ApplyWorldSetting(w, r.op, r.setting);
+        }
+        else
+        {
+            m3ApplyBodyOp(w->hv, r.op, r.body, r.v);
+        }
         w->hostDirty = true;
     }
     return true;
@@ -1139,6 +1147,54 @@ bool m3ParseJournal(const m3HostWorld* w, const uint8_t* stream, int32_t size,
             }
             r.body = j;
             r.generation = id.generation;
+        }
+        else if (m3IsWorldSettingOp(op))
+        {
+            // world.c:2485-2620, 2943-2990, 3006-3020: the settings'
+            // records, their payloads checked as the reference's replay
+            // checks them (hostile bytes fail loudly).
+            const int32_t want = op == M3_OP_SET_WIND                                   ? 24
+                                 : op == M3_OP_SET_GRAVITY || op == M3_OP_SET_CONTACT_TUNING ? 12
+                                                                                       : 4;
+            if (bytes != want)
+            {
+                m3gpuSetError(M3GPU_ERR_INVALID, "journal: bad setting record (op %d)", op);
+                return false;
+            }
+            memset(r.setting, 0, sizeof(r.setting));
+            memcpy(r.setting, payload, (size_t)bytes);
+            const float* f = r.setting;
+            bool ok = true;
+            switch (op)
+            {
+            case M3_OP_SET_GRAVITY:
+                ok = isfinite(f[0]) && isfinite(f[1]) && isfinite(f[2]);
+                break;
+            case M3_OP_SET_CONTACT_TUNING:
+                ok = isfinite(f[0]) && f[0] > 0.0f && isfinite(f[1]) && f[1] > 0.0f &&
+                     isfinite(f[2]) && f[2] > 0.0f;
+                break;
+            case M3_OP_SET_RESTITUTION_THRESHOLD:
+            case M3_OP_SET_HIT_EVENT_THRESHOLD:
+                ok = isfinite(f[0]) && f[0] >= 0.0f;
+                break;
+            case M3_OP_SET_MAXIMUM_LINEAR_SPEED:
+            case M3_OP_SET_MAXIMUM_ANGULAR_SPEED:
+                ok = isfinite(f[0]) && f[0] > 0.0f;
+                break;
+            case M3_OP_SET_WIND:
+                ok = isfinite(f[0]) && isfinite(f[1]) && isfinite(f[2]) && isfinite(f[3]) &&
+                     f[3] >= 0.0f && isfinite(f[4]) && f[4] >= 0.0f && isfinite(f[5]) &&
+                     f[5] >= 0.0f;
+                break;
+            default: // the sleeping and continuous flags: any value
+                break;
+            }
+            if (!ok)
+            {
+                m3gpuSetError(M3GPU_ERR_INVALID, "journal: bad setting values (op %d)", op);
+                return false;
+            }
         }
         else if (op <= 0)
         {

@@ -1443,6 +1443,225 @@ extern "C" void m3Joint_SetBreakThresholds(m3JointId jointId, float maxForce, fl
     w->hostDirty = true;
 }
 
+// ---------------------------------------------------------------------
+// World settings (world.c:734-1117, world.h:92-176, 288): each public
+// setter validates its arguments as the reference's does, records its
+// journal record, and changes the world's scalars on the host image (the
+// next step uploads them).  The journal replay applies the same records
+// through m3ApplyWorldSetting.
+// ---------------------------------------------------------------------
+void m3ApplyWorldSetting(m3HostWorld* w, int32_t op, const float* f)
+{
+    m3WorldView& v = w->hv;
+    m3WorldScalars* sc = v.sc;
+    switch (op)
+    {
+    case M3_OP_SET_GRAVITY:
+        sc->gravity = v3(f[0], f[1], f[2]);
+        break;
+    case M3_OP_SET_CONTACT_TUNING:
+        sc->contactHertz = f[0];
+        sc->contactDampingRatio = f[1];
+        sc->contactPushMaxSpeed = f[2];
+        break;
+    case M3_OP_SET_RESTITUTION_THRESHOLD:
+        sc->restitutionThreshold = f[0];
+        break;
+    case M3_OP_SET_MAXIMUM_LINEAR_SPEED:
+        sc->maximumLinearSpeed = f[0];
+        break;
+    case M3_OP_SET_MAXIMUM_ANGULAR_SPEED:
+        sc->maximumAngularSpeed = f[0];
+        break;
+    case M3_OP_SET_HIT_EVENT_THRESHOLD:
+        sc->hitEventThreshold = f[0];
+        break;
+    case M3_OP_ENABLE_SLEEPING:
+    case M3_OP_ENABLE_CONTINUOUS:
+    {
+        int32_t on;
+        memcpy(&on, &f[0], sizeof(on));
+        if (op == M3_OP_ENABLE_CONTINUOUS)
+        {
+            sc->continuousEnabled = on != 0 ? 1 : 0;
+            break;
+        }
+        sc->sleepEnabled = on != 0 ? 1 : 0;
+        if (on == 0)
+        {
+            // Sleeping turned off wakes every sleeping dynamic body
+            // (world.c:761-778, body.c:316-322).
+            for (int32_t i = 0; i < sc->bodyMax; ++i)
+            {
+                if (v.bodyAlive[i] != 0 && v.awake[i] == 0 && v.btype[i] == M3_BODY_DYNAMIC)
+                {
+                    v.awake[i] = 1;
+                    v.sleepTime[i] = 0.0f;
+                }
+            }
+        }
+        break;
+    }
+    case M3_OP_SET_WIND:
+        // The phase survives a retune (world.c:1075-1082).
+        sc->windDir = v3(f[0], f[1], f[2]);
+        sc->windSpeed = f[3];
+        sc->windGustHertz = f[4];
+        sc->windGustScale = f[5];
+        break;
+    default:
+        break;
+    }
+}
+
+// A world whose host image may change: the device's state read back first.
+static m3HostWorld* SettingWorld(m3WorldId worldId)
+{
+    m3gpuClearError();
+    m3HostWorld* w = m3gpuWorldFromId(worldId);
+    if (w == nullptr || m3gpuSyncHost(w) != M3GPU_OK)
+    {
+        return nullptr;
+    }
+    return w;
+}
+
+static void ApplySetting(m3HostWorld* w, int32_t op, const float* words, int32_t count)
+{
+    m3JournalAppend(w, op, words, (int32_t)sizeof(float) * count);
+    m3ApplyWorldSetting(w, op, words);
+    w->hostDirty = true;
+}
+
+extern "C" void m3World_SetGravity(m3WorldId worldId, m3Vec3 gravity)
+{
+    if (!FiniteV3(gravity))
+    {
+        return;
+    }
+    m3HostWorld* w = SettingWorld(worldId);
+    if (w != nullptr)
+    {
+        const float words[3] = {gravity.x, gravity.y, gravity.z};
+        ApplySetting(w, M3_OP_SET_GRAVITY, words, 3);
+    }
+}
+
+extern "C" m3Vec3 m3World_GetGravity(m3WorldId worldId)
+{
+    m3HostWorld* w = m3gpuWorldFromId(worldId);
+    return w != nullptr ? w->hv.sc->gravity : v3(0.0f, 0.0f, 0.0f);
+}
+
+extern "C" void m3World_SetContactTuning(m3WorldId worldId, float hertz, float dampingRatio,
+                                         float pushMaxSpeed)
+{
+    if (!FiniteF(hertz) || hertz <= 0.0f || !FiniteF(dampingRatio) || dampingRatio <= 0.0f ||
+        !FiniteF(pushMaxSpeed) || pushMaxSpeed <= 0.0f)
+    {
+        return;
+    }
+    m3HostWorld* w = SettingWorld(worldId);
+    if (w != nullptr)
+    {
+        const float words[3] = {hertz, dampingRatio, pushMaxSpeed};
+        ApplySetting(w, M3_OP_SET_CONTACT_TUNING, words, 3);
+    }
+}
+
+// One float setting: `strict` refuses zero as well as negatives.
+static void FloatSetting(m3WorldId worldId, int32_t op, float value, bool strict)
+{
+    if (!FiniteF(value) || value < 0.0f || (strict && value == 0.0f))
+    {
+        return;
+    }
+    m3HostWorld* w = SettingWorld(worldId);
+    if (w != nullptr)
+    {
+        ApplySetting(w, op, &value, 1);
+    }
+}
+
+extern "C" void m3World_SetRestitutionThreshold(m3WorldId worldId, float value)
+{
+    FloatSetting(worldId, M3_OP_SET_RESTITUTION_THRESHOLD, value, false);
+}
+
+extern "C" void m3World_SetMaximumLinearSpeed(m3WorldId worldId, float value)
+{
+    FloatSetting(worldId, M3_OP_SET_MAXIMUM_LINEAR_SPEED, value, true);
+}
+
+extern "C" void m3World_SetMaximumAngularSpeed(m3WorldId worldId, float value)
+{
+    FloatSetting(worldId, M3_OP_SET_MAXIMUM_ANGULAR_SPEED, value, true);
+}
+
+extern "C" void m3World_SetHitEventThreshold(m3WorldId worldId, float value)
+{
+    FloatSetting(worldId, M3_OP_SET_HIT_EVENT_THRESHOLD, value, false);
+}
+
+static void FlagSetting(m3WorldId worldId, int32_t op, bool flag)
+{
+    m3HostWorld* w = SettingWorld(worldId);
+    if (w != nullptr)
+    {
+        const int32_t on = flag ? 1 : 0;
+        float word;
+        memcpy(&word, &on, sizeof(word));
+        ApplySetting(w, op, &word, 1);
+    }
+}
+
+extern "C" void m3World_EnableSleeping(m3WorldId worldId, bool flag)
+{
+    FlagSetting(worldId, M3_OP_ENABLE_SLEEPING, flag);
+}
+
+extern "C" bool m3World_IsSleepingEnabled(m3WorldId worldId)
+{
+    m3HostWorld* w = m3gpuWorldFromId(worldId);
+    return w != nullptr && w->hv.sc->sleepEnabled != 0;
+}
+
+extern "C" void m3World_EnableContinuous(m3WorldId worldId, bool flag)
+{
+    FlagSetting(worldId, M3_OP_ENABLE_CONTINUOUS, flag);
+}
+
+extern "C" bool m3World_IsContinuousEnabled(m3WorldId worldId)
+{
+    m3HostWorld* w = m3gpuWorldFromId(worldId);
+    return w != nullptr && w->hv.sc->continuousEnabled != 0;
+}
+
+extern "C" void m3World_SetWind(m3WorldId worldId, m3Vec3 direction, float speed, float gustHertz,
+                                float gustScale)
+{
+    if (!FiniteV3(direction) || !FiniteF(speed) || speed < 0.0f || !FiniteF(gustHertz) ||
+        gustHertz < 0.0f || !FiniteF(gustScale) || gustScale < 0.0f)
+    {
+        return;
+    }
+    if (speed > 0.0f)
+    {
+        // A blowing wind demands a near-unit direction.
+        const m3real len2 = m3Dot3(direction, direction);
+        if (len2 < 0.99f || len2 > 1.01f)
+        {
+            return;
+        }
+    }
+    m3HostWorld* w = SettingWorld(worldId);
+    if (w != nullptr)
+    {
+        const float words[6] = {direction.x, direction.y, direction.z, speed, gustHertz, gustScale};
+        ApplySetting(w, M3_OP_SET_WIND, words, 6);
+    }
+}
+
 // White-box hook for the tests: one broadphase tree move on the host
 // image, as the step's tree kernel makes it (remove the shape's leaf,
 // insert `lo`..`hi`).  Returns the new leaf, or -1.
