@@ -384,6 +384,20 @@ M3GPU_API m3Vec3 m3Body_GetLinearVelocity(m3BodyId bodyId);
 M3GPU_API m3Vec3 m3Body_GetAngularVelocity(m3BodyId bodyId);
 /* body.h: awake query (dynamic bodies sleep; others report true) */
 M3GPU_API bool m3Body_IsAwake(m3BodyId bodyId);
+/* body.c:910-958 (body.h:117-121): a force or impulse at a world point
+ * (dynamic bodies with mass only; a non-finite argument is a no-op);
+ * body.c:639-703 (body.h:86-94): the six motion-lock bits (others are
+ * refused) and the spin-cap escape, each journaled like the reference's;
+ * body.c:514-527, 632 (body.h:64-70): type, user data and enabled flag. */
+M3GPU_API void m3Body_ApplyForceAtPoint(m3BodyId bodyId, m3Vec3 force, m3Pos3 point);
+M3GPU_API void m3Body_ApplyLinearImpulseAtPoint(m3BodyId bodyId, m3Vec3 impulse, m3Pos3 point);
+M3GPU_API void m3Body_SetMotionLocks(m3BodyId bodyId, uint32_t locks);
+M3GPU_API uint32_t m3Body_GetMotionLocks(m3BodyId bodyId);
+M3GPU_API void m3Body_SetAllowFastRotation(m3BodyId bodyId, bool allow);
+M3GPU_API bool m3Body_GetAllowFastRotation(m3BodyId bodyId);
+M3GPU_API m3BodyType m3Body_GetType(m3BodyId bodyId);
+M3GPU_API uint64_t m3Body_GetUserData(m3BodyId bodyId);
+M3GPU_API bool m3Body_IsEnabled(m3BodyId bodyId);
 
 /* body.h:115-123 (body.c:818-1014): commands between steps.  Forces,
  * torques and impulses act on dynamic bodies with mass; velocity sets on

@@ -434,6 +434,25 @@ def bind_settings(lib: C.CDLL) -> C.CDLL:
     return lib
 
 
+def bind_body_commands(lib: C.CDLL) -> C.CDLL:
+    """Declare the reference-named body commands at a world point, the
+    motion locks, the fast-rotation switch and the body getters."""
+    for name in ("m3Body_ApplyForceAtPoint", "m3Body_ApplyLinearImpulseAtPoint"):
+        getattr(lib, name).argtypes = [m3BodyId, m3Vec3, m3Pos3]
+        getattr(lib, name).restype = None
+    lib.m3Body_SetMotionLocks.argtypes = [m3BodyId, C.c_uint32]
+    lib.m3Body_SetMotionLocks.restype = None
+    lib.m3Body_GetMotionLocks.argtypes = [m3BodyId]
+    lib.m3Body_GetMotionLocks.restype = C.c_uint32
+    lib.m3Body_SetAllowFastRotation.argtypes = [m3BodyId, C.c_bool]
+    lib.m3Body_SetAllowFastRotation.restype = None
+    for name, res in (("m3Body_GetAllowFastRotation", C.c_bool), ("m3Body_GetType", C.c_int32),
+                      ("m3Body_GetUserData", C.c_uint64), ("m3Body_IsEnabled", C.c_bool)):
+        getattr(lib, name).argtypes = [m3BodyId]
+        getattr(lib, name).restype = res
+    return lib
+
+
 def bind_create(lib: C.CDLL) -> C.CDLL:
     """Declare the reference-named creation API on a handle."""
     lib.m3DefaultWorldDef.restype = m3WorldDef

@@ -29,6 +29,11 @@ enum
     M3_OP_SET_HIT_EVENT_THRESHOLD = 49,
     M3_OP_SET_WIND = 60,
     M3_OP_SET_MAXIMUM_ANGULAR_SPEED = 66,
+    // Host-side body commands (world_internal.h:137-174).
+    M3_OP_APPLY_FORCE_AT_POINT = 30,
+    M3_OP_APPLY_IMPULSE_AT_POINT = 31,
+    M3_OP_SET_MOTION_LOCKS = 36,
+    M3_OP_SET_ALLOW_FAST_ROTATION = 65,
 };
 
 // One command for the device kernel: `world` indexes the batch, `body`
@@ -49,6 +54,14 @@ M3_HD bool m3IsWorldSettingOp(int32_t op)
            op == M3_OP_ENABLE_SLEEPING || op == M3_OP_ENABLE_CONTINUOUS ||
            op == M3_OP_SET_HIT_EVENT_THRESHOLD || op == M3_OP_SET_WIND ||
            op == M3_OP_SET_MAXIMUM_ANGULAR_SPEED;
+}
+
+// Body commands applied on the host image only (a world point or lock
+// bits ride their records): never device ops.
+M3_HD bool m3IsHostBodyOp(int32_t op)
+{
+    return op == M3_OP_APPLY_FORCE_AT_POINT || op == M3_OP_APPLY_IMPULSE_AT_POINT ||
+           op == M3_OP_SET_MOTION_LOCKS || op == M3_OP_SET_ALLOW_FAST_ROTATION;
 }
 
 // Joint commands ride the same record: `body` is then the joint slot.

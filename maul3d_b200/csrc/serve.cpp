@@ -287,14 +287,15 @@ void Retire(m3gpuServer* s, std::unique_ptr<Request>& r, uint64_t hash, int32_t 
 }
 
 // Served journals carry body and joint commands and steps: the frames run
-// as device ops in a batched step.  A world-setting record is refused.
+// as device ops in a batched step.  A record that only the host applies
+// (a world setting, a force at a point, motion locks) is refused.
 bool NoSettings(const std::vector<m3JournalRecordView>& records)
 {
     for (const m3JournalRecordView& rec : records)
     {
-        if (m3IsWorldSettingOp(rec.op))
+        if (m3IsWorldSettingOp(rec.op) || m3IsHostBodyOp(rec.op))
         {
-            m3gpuSetError(M3GPU_ERR_UNSUPPORTED, "served journal: world setting op %d", rec.op);
+            m3gpuSetError(M3GPU_ERR_UNSUPPORTED, "served journal: host-side op %d", rec.op);
             return false;
         }
     }

@@ -1012,8 +1012,9 @@ bool m3gpuRestoreWorld(m3HostWorld* w, const void* data, int32_t size)
 
 // world.c:3187-3218 (world.h:606): replays a recorded command stream:
 // records of (op, payload bytes, payload).  Covered ops: steps (run on
-// the GPU), velocity sets, forces, torques and impulses, joint break
-// thresholds and the world settings.  The stream is
+// the GPU), velocity sets, forces, torques and impulses (also at a world
+// point), motion locks, the fast-rotation flag, joint break thresholds and
+// the world settings.  The stream is
 // validated whole before anything is applied (framing, op, payload
 // size, body ids, finite vectors, step arguments), so a refusal leaves
 // the world untouched, as the reference's snapshot-backed rollback does.
@@ -1053,6 +1054,10 @@ extern "C" bool m3World_JournalReplay(m3WorldId worldId, const void* data, int32
         if (m3IsWorldSettingOp(r.op))
         {
             m3ApplyWorldSetting(w, r.op, r.setting);
+        }
+        else if (m3IsHostBodyOp(r.op))
+        {
+            m3ApplyHostBodyOp(w, r.op, r.body, r.v, r.point, r.bits);
         }
         else
         {
@@ -1147,6 +1152,43 @@ bool m3ParseJournal(const m3HostWorld* w, const uint8_t* stream, int32_t size,
             }
             r.body = j;
             r.generation = id.generation;
+        }
+        else if (m3IsHostBodyOp(op))
+        {
+            // world.c:2323-2352, 2419-2439, 2904-2928: forces and impulses
+            // at a world point {m3BodyId; m3Vec3; m3Pos3}, motion locks and
+            // the fast-rotation flag {m3BodyId; uint32}; the id is
+            // retargeted to this world.
+            const bool point =
+                op == M3_OP_APPLY_FORCE_AT_POINT || op == M3_OP_APPLY_IMPULSE_AT_POINT;
+            if (bytes != (point ? 48 : 12))
+            {
+                m3gpuSetError(M3GPU_ERR_INVALID, "journal: bad body record (op %d)", op);
+                return false;
+            }
+            m3BodyId id;
+            memcpy(&id, payload, 8);
+            const int32_t index = id.index1 - 1;
+            bool ok = index >= 0 && index < w->hv.sc->bodyMax && w->hv.bodyAlive[index] != 0 &&
+                      w->hv.bodyGen[index] == id.generation;
+            if (point)
+            {
+                memcpy(&r.v, payload + 8, 12);
+                memcpy(&r.point, payload + 24, 24);
+                ok = ok && isfinite(r.v.x) && isfinite(r.v.y) && isfinite(r.v.z) &&
+                     isfinite(r.point.x) && isfinite(r.point.y) && isfinite(r.point.z);
+            }
+            else
+            {
+                memcpy(&r.bits, payload + 8, 4);
+                ok = ok && (op != M3_OP_SET_ALLOW_FAST_ROTATION || r.bits <= 1u);
+            }
+            if (!ok)
+            {
+                m3gpuSetError(M3GPU_ERR_INVALID, "journal: stale body or bad values (op %d)", op);
+                return false;
+            }
+            r.body = index;
         }
         else if (m3IsWorldSettingOp(op))
         {

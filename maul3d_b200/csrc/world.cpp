@@ -479,6 +479,171 @@ extern "C" void m3Body_SetAngularVelocity(m3BodyId bodyId, m3Vec3 velocity)
 }
 
 // ---------------------------------------------------------------------
+// Host-side body commands and getters (body.c:283-303, 379-404, 514-527,
+// 632-703, 910-958): forces and impulses at a world point, motion locks,
+// the fast-rotation escape.  Each public call checks as the reference's,
+// records the reference's journal record and changes the host image (the
+// next step uploads it); the journal replay applies the same records.
+// ---------------------------------------------------------------------
+static m3Vec3 ForceArm(const m3WorldView& v, int32_t i, m3Pos3 point)
+{
+    const m3Transform xf = v.xf[i];
+    const m3Vec3 rlc = m3RotateVec3(xf.q, v.lc[i]);
+    return v3((m3real)(point.x - xf.p.x) - rlc.x, (m3real)(point.y - xf.p.y) - rlc.y,
+              (m3real)(point.z - xf.p.z) - rlc.z);
+}
+
+void m3ApplyHostBodyOp(m3HostWorld* w, int32_t op, int32_t i, m3Vec3 f, m3Pos3 point,
+                       uint32_t bits)
+{
+    m3WorldView& v = w->hv;
+    switch (op)
+    {
+    case M3_OP_APPLY_FORCE_AT_POINT:
+        v.force[i] = m3Add3(v.force[i], f);
+        v.torque[i] = m3Add3(v.torque[i], m3Cross3(ForceArm(v, i, point), f));
+        m3WakeOnCommand(v, i, f);
+        break;
+    case M3_OP_APPLY_IMPULSE_AT_POINT:
+        v.v[i] = m3Add3(v.v[i], m3MulSV3(v.invMass[i], f));
+        v.w[i] = m3Add3(v.w[i],
+                        m3MulMV3(m3WorldInvInertiaHD(v, i), m3Cross3(ForceArm(v, i, point), f)));
+        m3WakeOnCommand(v, i, f);
+        break;
+    case M3_OP_SET_MOTION_LOCKS:
+        // The fast-rotation bit is its own command's (body.c:283-303).
+        v.locks[i] = (uint8_t)((v.locks[i] & M3_LOCKS_ALLOW_FAST_ROTATION) | (bits & 0x3Fu));
+        if (bits & 1u)
+            v.v[i].x = 0.0f;
+        if (bits & 2u)
+            v.v[i].y = 0.0f;
+        if (bits & 4u)
+            v.v[i].z = 0.0f;
+        if (bits & 8u)
+            v.w[i].x = 0.0f;
+        if (bits & 16u)
+            v.w[i].y = 0.0f;
+        if (bits & 32u)
+            v.w[i].z = 0.0f;
+        break;
+    case M3_OP_SET_ALLOW_FAST_ROTATION:
+        v.locks[i] = bits != 0 ? (uint8_t)(v.locks[i] | M3_LOCKS_ALLOW_FAST_ROTATION)
+                               : (uint8_t)(v.locks[i] & ~M3_LOCKS_ALLOW_FAST_ROTATION);
+        break;
+    default:
+        break;
+    }
+}
+
+// A force or impulse at a world point: {m3BodyId id; m3Vec3 v; m3Pos3 p}.
+static void PointCommand(m3BodyId id, int32_t op, m3Vec3 f, m3Pos3 point)
+{
+    m3gpuClearError();
+    int32_t index;
+    m3HostWorld* w = ResolveBody(id, &index);
+    if (w == nullptr || !FiniteV3(f) || !FinitePos3(point) || m3gpuSyncHost(w) != M3GPU_OK)
+    {
+        return;
+    }
+    if (!(w->hv.btype[index] == M3_BODY_DYNAMIC && w->hv.invMass[index] > 0.0f))
+    {
+        return;
+    }
+    struct
+    {
+        m3BodyId id;
+        m3Vec3 v;
+        m3Pos3 p;
+    } record;
+    memset(&record, 0, sizeof(record));
+    record.id = id;
+    record.v = f;
+    record.p = point;
+    m3JournalAppend(w, op, &record, (int32_t)sizeof(record));
+    m3ApplyHostBodyOp(w, op, index, f, point, 0u);
+    w->hostDirty = true;
+}
+
+extern "C" void m3Body_ApplyForceAtPoint(m3BodyId bodyId, m3Vec3 force, m3Pos3 point)
+{
+    PointCommand(bodyId, M3_OP_APPLY_FORCE_AT_POINT, force, point);
+}
+
+extern "C" void m3Body_ApplyLinearImpulseAtPoint(m3BodyId bodyId, m3Vec3 impulse, m3Pos3 point)
+{
+    PointCommand(bodyId, M3_OP_APPLY_IMPULSE_AT_POINT, impulse, point);
+}
+
+// Lock bits or the fast-rotation flag: {m3BodyId id; uint32 bits}.
+static void BitsCommand(m3BodyId id, int32_t op, uint32_t bits)
+{
+    m3gpuClearError();
+    int32_t index;
+    m3HostWorld* w = ResolveBody(id, &index);
+    if (w == nullptr || m3gpuSyncHost(w) != M3GPU_OK)
+    {
+        return;
+    }
+    struct
+    {
+        m3BodyId id;
+        uint32_t bits;
+    } record;
+    memset(&record, 0, sizeof(record));
+    record.id = id;
+    record.bits = bits;
+    m3JournalAppend(w, op, &record, (int32_t)sizeof(record));
+    m3ApplyHostBodyOp(w, op, index, v3(0.0f, 0.0f, 0.0f), m3Pos3{0.0, 0.0, 0.0}, bits);
+    w->hostDirty = true;
+}
+
+extern "C" void m3Body_SetMotionLocks(m3BodyId bodyId, uint32_t locks)
+{
+    if ((locks & ~0x3Fu) != 0)
+    {
+        return; // only the six lock bits exist
+    }
+    BitsCommand(bodyId, M3_OP_SET_MOTION_LOCKS, locks);
+}
+
+extern "C" void m3Body_SetAllowFastRotation(m3BodyId bodyId, bool allow)
+{
+    BitsCommand(bodyId, M3_OP_SET_ALLOW_FAST_ROTATION, allow ? 1u : 0u);
+}
+
+extern "C" uint32_t m3Body_GetMotionLocks(m3BodyId bodyId)
+{
+    return ReadBody(bodyId, 0u, [](const m3WorldView& v, int32_t i) {
+        return (uint32_t)(v.locks[i] & 0x3Fu);
+    });
+}
+
+extern "C" bool m3Body_GetAllowFastRotation(m3BodyId bodyId)
+{
+    return ReadBody(bodyId, false, [](const m3WorldView& v, int32_t i) {
+        return (v.locks[i] & M3_LOCKS_ALLOW_FAST_ROTATION) != 0;
+    });
+}
+
+extern "C" m3BodyType m3Body_GetType(m3BodyId bodyId)
+{
+    return ReadBody(bodyId, m3_staticBody,
+                    [](const m3WorldView& v, int32_t i) { return (m3BodyType)v.btype[i]; });
+}
+
+extern "C" uint64_t m3Body_GetUserData(m3BodyId bodyId)
+{
+    return ReadBody(bodyId, (uint64_t)0,
+                    [](const m3WorldView& v, int32_t i) { return v.userData[i]; });
+}
+
+extern "C" bool m3Body_IsEnabled(m3BodyId bodyId)
+{
+    return ReadBody(bodyId, false,
+                    [](const m3WorldView& v, int32_t i) { return v.enabled[i] != 0; });
+}
+
+// ---------------------------------------------------------------------
 // Mass properties (shape.c:48-300)
 // ---------------------------------------------------------------------
 

@@ -1,0 +1,150 @@
+"""Body commands at a world point, motion locks and the fast-rotation switch
+(body.h:64-121; body.c:283-303, 387-404, 639-709, 910-958) on the host:
+with valid and refused arguments they leave the world with the reference's
+hash, getters and journal bytes, the reference's journal of them replays
+here to the same world, and hostile records are refused whole
+(world.c:2323-2352, 2419-2439, 2904-2928).  Stepping after these commands
+is covered on the device by test_body_commands_gpu.py."""
+import ctypes as C
+import struct
+
+from maul3d_b200 import abi
+from maul3d_b200.abi import SCENE_TOWERS, SCENE_UNEVEN
+
+V = abi.m3Vec3
+P = abi.m3Pos3
+
+
+def _commands(lib, wid):
+    w0 = wid.index1 - 1
+    for k in range(5):
+        b = abi.m3BodyId(3 + k, w0, 0)
+        lib.m3Body_ApplyForceAtPoint(b, V(2.0 * k, 0.5, -1.0), P(0.25 * k, 3.0, -0.5))
+        lib.m3Body_ApplyLinearImpulseAtPoint(b, V(0.5, -1.5, 0.25 * k), P(1.0, 0.5 * k, 2.0))
+        lib.m3Body_SetMotionLocks(b, [0x01, 0x12, 0x3F, 0x24, 0x00][k])
+        lib.m3Body_SetAllowFastRotation(b, k % 2 == 0)
+    b = abi.m3BodyId(4, w0, 0)
+    lib.m3Body_ApplyForceAtPoint(b, V(float("nan"), 0.0, 0.0), P(0.0, 0.0, 0.0))   # refused
+    lib.m3Body_ApplyLinearImpulseAtPoint(b, V(1.0, 0.0, 0.0), P(float("inf"), 0.0, 0.0))
+    lib.m3Body_SetMotionLocks(b, 0x40)                                             # refused
+    lib.m3Body_SetMotionLocks(b, 0x108)                                            # refused
+    static = abi.m3BodyId(1, w0, 0)
+    lib.m3Body_ApplyForceAtPoint(static, V(1.0, 1.0, 1.0), P(0.0, 1.0, 0.0))      # not dynamic
+    lib.m3Body_ApplyLinearImpulseAtPoint(static, V(1.0, 1.0, 1.0), P(0.0, 1.0, 0.0))
+    lib.m3Body_SetMotionLocks(static, 0x07)
+    lib.m3Body_SetAllowFastRotation(abi.m3BodyId(6, w0, 0), True)
+    lib.m3Body_SetAllowFastRotation(abi.m3BodyId(6, w0, 0), False)
+    stale = abi.m3BodyId(3, w0, 9)
+    lib.m3Body_SetMotionLocks(stale, 0x01)
+    lib.m3Body_ApplyForceAtPoint(stale, V(1.0, 0.0, 0.0), P(0.0, 0.0, 0.0))
+
+
+def _engines(m3, oracle):
+    g = abi.bind_snapshot(abi.bind_body_commands(m3.lib))
+    r = abi.bind_snapshot(abi.bind_body_commands(oracle.lib()))
+    return g, r
+
+
+def _journal(lib, wid, action):
+    buf = (C.c_uint8 * 8192)()
+    assert lib.m3World_JournalBegin(wid, buf, 8192)
+    action()
+    n = lib.m3World_JournalEnd(wid)
+    assert n >= 0
+    return bytes(buf[:n])
+
+
+def _without_world_index(journal: bytes) -> bytes:
+    """The records with the world0 half of every body id cleared (replay
+    retargets it to the replaying world)."""
+    out = bytearray(journal)
+    cursor = 0
+    while cursor < len(out):
+        op, n = struct.unpack_from("<ii", out, cursor)
+        out[cursor + 12:cursor + 14] = b"\0\0"
+        cursor += 8 + n
+    return bytes(out)
+
+
+def _getters(lib, wid, count):
+    w0 = wid.index1 - 1
+    rows = []
+    for i in range(1, count + 1):
+        b = abi.m3BodyId(i, w0, 0)
+        rows.append((lib.m3Body_GetMotionLocks(b), lib.m3Body_GetAllowFastRotation(b),
+                     lib.m3Body_GetType(b), lib.m3Body_GetUserData(b), lib.m3Body_IsEnabled(b)))
+    stale = abi.m3BodyId(2, w0, 7)
+    rows.append((lib.m3Body_GetMotionLocks(stale), lib.m3Body_GetAllowFastRotation(stale),
+                 lib.m3Body_GetType(stale), lib.m3Body_GetUserData(stale),
+                 lib.m3Body_IsEnabled(stale)))
+    return rows
+
+
+def test_body_commands_match_the_reference(m3, oracle):
+    glib, rlib = _engines(m3, oracle)
+    for scene, seed, param in ((SCENE_UNEVEN, 31, 40), (SCENE_TOWERS, 32, 2)):
+        g = m3.World.scene(scene, seed, param)
+        r = oracle.RefWorld.scene(scene, seed, param)
+        gj = _journal(glib, g.id, lambda: _commands(glib, g.id))
+        rj = _journal(rlib, r.id, lambda: _commands(rlib, r.id))
+        assert _without_world_index(gj) == _without_world_index(rj) and len(rj) > 0
+        assert g.hash() == r.hash()
+        assert _getters(glib, g.id, 12) == _getters(rlib, r.id, 12)
+        w0 = g.id.index1 - 1
+        assert glib.m3Body_GetMotionLocks(abi.m3BodyId(5, w0, 0)) == 0x3F
+        assert glib.m3Body_GetAllowFastRotation(abi.m3BodyId(5, w0, 0))
+        g.destroy()
+        r.destroy()
+
+
+def test_reference_journal_of_body_commands_replays_here(m3, oracle):
+    glib, rlib = _engines(m3, oracle)
+    r = oracle.RefWorld.scene(SCENE_UNEVEN, 33, 40)
+    journal = _journal(rlib, r.id, lambda: _commands(rlib, r.id))
+    g = m3.World.scene(SCENE_UNEVEN, 33, 40)
+    buf = (C.c_uint8 * len(journal)).from_buffer_copy(journal)
+    assert glib.m3World_JournalReplay(g.id, buf, len(journal))
+    assert g.hash() == r.hash()
+    r.destroy()
+    g.destroy()
+
+
+def test_hostile_body_records_are_refused_whole(m3, oracle):
+    glib, rlib = _engines(m3, oracle)
+    g = m3.World.scene(SCENE_UNEVEN, 34, 40)
+    r = oracle.RefWorld.scene(SCENE_UNEVEN, 34, 40)
+    before = g.hash()
+    w0 = g.id.index1 - 1
+    body = bytes(abi.m3BodyId(3, w0, 0))
+    stale = bytes(abi.m3BodyId(3, w0, 5))
+    v = C.string_at(C.byref(V(1.0, 0.0, 0.0)), 12)
+    p = C.string_at(C.byref(P(0.0, 1.0, 0.0)), 24)
+    good = abi.journal_record(36, body + struct.pack("<I", 0x01))
+    for bad in (abi.journal_record(30, body + C.string_at(C.byref(V(float("nan"), 0.0, 0.0)), 12)
+                                   + bytes(4) + p),
+                abi.journal_record(31, body + v + bytes(4) + C.string_at(
+                    C.byref(P(0.0, float("inf"), 0.0)), 24)),
+                abi.journal_record(31, body + v + bytes(4) + p[:20]),
+                abi.journal_record(30, stale + v + bytes(4) + p),
+                abi.journal_record(65, body + struct.pack("<I", 2)),
+                abi.journal_record(36, stale + struct.pack("<I", 1)),
+                abi.journal_record(36, body + struct.pack("<H", 1))):
+        stream = good + bad
+        gbuf = (C.c_uint8 * len(stream)).from_buffer_copy(stream)
+        assert not glib.m3World_JournalReplay(g.id, gbuf, len(stream))
+        assert g.hash() == before
+        # The reference refuses the same streams.
+        rbuf = (C.c_uint8 * len(stream)).from_buffer_copy(stream)
+        assert not rlib.m3World_JournalReplay(r.id, rbuf, len(stream))
+    # Lock records carry a uint32; the reference keeps the low six bits.
+    wide = abi.journal_record(36, body + struct.pack("<I", 0x1C2))
+    gbuf = (C.c_uint8 * len(wide)).from_buffer_copy(wide)
+    rbuf = (C.c_uint8 * len(wide)).from_buffer_copy(wide)
+    r2 = oracle.RefWorld.scene(SCENE_UNEVEN, 34, 40)
+    assert glib.m3World_JournalReplay(g.id, gbuf, len(wide))
+    assert rlib.m3World_JournalReplay(r2.id, rbuf, len(wide))
+    assert g.hash() == r2.hash()
+    assert glib.m3Body_GetMotionLocks(abi.m3BodyId(3, w0, 0)) == 0x02
+    g.destroy()
+    r.destroy()
+    r2.destroy()
