@@ -398,6 +398,19 @@ M3GPU_API bool m3Body_GetAllowFastRotation(m3BodyId bodyId);
 M3GPU_API m3BodyType m3Body_GetType(m3BodyId bodyId);
 M3GPU_API uint64_t m3Body_GetUserData(m3BodyId bodyId);
 M3GPU_API bool m3Body_IsEnabled(m3BodyId bodyId);
+/* body.c:170-330, 531-637, 763-823 (body.h:64-106): runtime control,
+ * each journaled like the reference's.  A teleport or a pose target needs
+ * a finite position and a near-unit rotation (targets: kinematic bodies
+ * only); a teleport, a type change or an enable switch wakes the sleeping
+ * dynamic bodies around the body; a type change to dynamic rebuilds the
+ * mass from the body's shapes; sleep controls refuse a negative or
+ * non-finite threshold; forced sleep or wake reaches dynamic bodies only. */
+M3GPU_API void m3Body_SetTransform(m3BodyId bodyId, m3Pos3 position, m3Quat rotation);
+M3GPU_API void m3Body_SetTargetTransform(m3BodyId bodyId, m3Pos3 position, m3Quat rotation);
+M3GPU_API void m3Body_SetType(m3BodyId bodyId, m3BodyType type);
+M3GPU_API void m3Body_SetEnabled(m3BodyId bodyId, bool enabled);
+M3GPU_API void m3Body_SetSleepControls(m3BodyId bodyId, float threshold, bool canSleep);
+M3GPU_API void m3Body_SetAwake(m3BodyId bodyId, bool awake);
 
 /* body.h:115-123 (body.c:818-1014): commands between steps.  Forces,
  * torques and impulses act on dynamic bodies with mass; velocity sets on

@@ -436,7 +436,9 @@ def bind_settings(lib: C.CDLL) -> C.CDLL:
 
 def bind_body_commands(lib: C.CDLL) -> C.CDLL:
     """Declare the reference-named body commands at a world point, the
-    motion locks, the fast-rotation switch and the body getters."""
+    runtime controls (teleport, kinematic target, type, enable, motion
+    locks, sleep controls, forced sleep or wake, fast rotation) and the
+    body getters."""
     for name in ("m3Body_ApplyForceAtPoint", "m3Body_ApplyLinearImpulseAtPoint"):
         getattr(lib, name).argtypes = [m3BodyId, m3Vec3, m3Pos3]
         getattr(lib, name).restype = None
@@ -446,6 +448,20 @@ def bind_body_commands(lib: C.CDLL) -> C.CDLL:
     lib.m3Body_GetMotionLocks.restype = C.c_uint32
     lib.m3Body_SetAllowFastRotation.argtypes = [m3BodyId, C.c_bool]
     lib.m3Body_SetAllowFastRotation.restype = None
+    for name in ("m3Body_SetTransform", "m3Body_SetTargetTransform"):
+        getattr(lib, name).argtypes = [m3BodyId, m3Pos3, m3Quat]
+        getattr(lib, name).restype = None
+    lib.m3Body_SetType.argtypes = [m3BodyId, C.c_int32]
+    lib.m3Body_SetType.restype = None
+    for name in ("m3Body_SetEnabled", "m3Body_SetAwake"):
+        getattr(lib, name).argtypes = [m3BodyId, C.c_bool]
+        getattr(lib, name).restype = None
+    lib.m3Body_SetSleepControls.argtypes = [m3BodyId, C.c_float, C.c_bool]
+    lib.m3Body_SetSleepControls.restype = None
+    lib.m3Body_IsAwake.argtypes = [m3BodyId]
+    lib.m3Body_IsAwake.restype = C.c_bool
+    lib.m3Body_GetPosition.argtypes = [m3BodyId]
+    lib.m3Body_GetPosition.restype = m3Pos3
     for name, res in (("m3Body_GetAllowFastRotation", C.c_bool), ("m3Body_GetType", C.c_int32),
                       ("m3Body_GetUserData", C.c_uint64), ("m3Body_IsEnabled", C.c_bool)):
         getattr(lib, name).argtypes = [m3BodyId]

@@ -255,8 +255,8 @@ extern "C" int32_t m3gpu_step_worlds_commands(const m3WorldId* worlds, int32_t c
             return m3gpuSetError(M3GPU_ERR_INVALID, "command %d: bad world index or op", k);
         }
         m3HostWorld* w = ws[(size_t)c.world];
-        // Liveness, type and mass are creation-time data: the host image
-        // has them current even while the device is ahead.
+        // Liveness, type and mass change only through host calls: the
+        // host image has them current even while the device is ahead.
         const int32_t index = c.body.index1 - 1;
         if (c.body.world0 != (uint16_t)w->slot || index < 0 || index >= w->hv.sc->bodyMax ||
             w->hv.bodyAlive[index] == 0 || w->hv.bodyGen[index] != c.body.generation ||

@@ -32,7 +32,13 @@ enum
     // Host-side body commands (world_internal.h:137-174).
     M3_OP_APPLY_FORCE_AT_POINT = 30,
     M3_OP_APPLY_IMPULSE_AT_POINT = 31,
+    M3_OP_SET_TRANSFORM = 32,
+    M3_OP_SET_TARGET_TRANSFORM = 33,
+    M3_OP_SET_TYPE = 34,
+    M3_OP_SET_ENABLED = 35,
     M3_OP_SET_MOTION_LOCKS = 36,
+    M3_OP_SET_SLEEP_CONTROLS = 37,
+    M3_OP_SET_AWAKE = 38,
     M3_OP_SET_ALLOW_FAST_ROTATION = 65,
 };
 
@@ -56,12 +62,12 @@ M3_HD bool m3IsWorldSettingOp(int32_t op)
            op == M3_OP_SET_MAXIMUM_ANGULAR_SPEED;
 }
 
-// Body commands applied on the host image only (a world point or lock
-// bits ride their records): never device ops.
+// Body commands applied on the host image only (a world point, a pose,
+// lock bits, a type or a flag ride their records): never device ops.
 M3_HD bool m3IsHostBodyOp(int32_t op)
 {
-    return op == M3_OP_APPLY_FORCE_AT_POINT || op == M3_OP_APPLY_IMPULSE_AT_POINT ||
-           op == M3_OP_SET_MOTION_LOCKS || op == M3_OP_SET_ALLOW_FAST_ROTATION;
+    return (op >= M3_OP_APPLY_FORCE_AT_POINT && op <= M3_OP_SET_AWAKE) ||
+           op == M3_OP_SET_ALLOW_FAST_ROTATION;
 }
 
 // Joint commands ride the same record: `body` is then the joint slot.

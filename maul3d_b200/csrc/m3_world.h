@@ -345,18 +345,19 @@ struct m3JournalRecordView
     int32_t substeps;
     uint16_t generation; // joint records
     float setting[6];    // world-setting records: their payload's words
-    m3Pos3 point;        // force and impulse at a point: the world point
-    uint32_t bits;       // motion locks, or the fast-rotation flag
+    m3Pos3 point;        // force and impulse at a point: the world point; a pose's position
+    m3Quat rotation;     // a pose's rotation
+    uint32_t bits;       // motion locks, a type, a flag (canSleep for sleep controls)
 };
 // Applies a validated world-setting record (world.c:734-783, 1013-1082)
 // to the host image: the setting's fields, and for sleeping turned off
 // every sleeping dynamic body woken.  world.cpp.
 void m3ApplyWorldSetting(m3HostWorld* w, int32_t op, const float* words);
-// Applies a validated host-side body command (body.c:283-303, 379-404,
-// 663-703) to the host image: `v` the force or impulse, `point` its world
-// point, `bits` the lock bits or the fast-rotation flag.  world.cpp.
-void m3ApplyHostBodyOp(m3HostWorld* w, int32_t op, int32_t body, m3Vec3 v, m3Pos3 point,
-                       uint32_t bits);
+// Applies a validated host-side body command (body.c:170-330, 379-404,
+// 663-703) to the host image, the body slot in `r.body`: `v` a force or
+// impulse with its world `point`; a pose (`point`, `rotation`); `bits`
+// the lock bits, type or flag; `setting[0]` a sleep threshold.  world.cpp.
+void m3ApplyHostBodyOp(m3HostWorld* w, const m3JournalRecordView& r);
 // Parses and validates a whole journal against a world's bodies; false
 // (with the error set) on the first bad or unsupported record.
 // Worlds outside the world table (world.cpp): built on any thread,

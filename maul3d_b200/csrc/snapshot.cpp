@@ -1057,7 +1057,7 @@ extern "C" bool m3World_JournalReplay(m3WorldId worldId, const void* data, int32
         }
         else if (m3IsHostBodyOp(r.op))
         {
-            m3ApplyHostBodyOp(w, r.op, r.body, r.v, r.point, r.bits);
+            m3ApplyHostBodyOp(w, r);
         }
         else
         {
@@ -1155,13 +1155,16 @@ bool m3ParseJournal(const m3HostWorld* w, const uint8_t* stream, int32_t size,
         }
         else if (m3IsHostBodyOp(op))
         {
-            // world.c:2323-2352, 2419-2439, 2904-2928: forces and impulses
-            // at a world point {m3BodyId; m3Vec3; m3Pos3}, motion locks and
-            // the fast-rotation flag {m3BodyId; uint32}; the id is
+            // world.c:2323-2465, 2904-2928: forces and impulses at a world
+            // point {m3BodyId; m3Vec3; m3Pos3}, poses {m3BodyId;
+            // m3Transform}, sleep controls {m3BodyId; float; int32}, and
+            // locks, types and flags {m3BodyId; uint32}; the id is
             // retargeted to this world.
             const bool point =
                 op == M3_OP_APPLY_FORCE_AT_POINT || op == M3_OP_APPLY_IMPULSE_AT_POINT;
-            if (bytes != (point ? 48 : 12))
+            const bool pose = op == M3_OP_SET_TRANSFORM || op == M3_OP_SET_TARGET_TRANSFORM;
+            const int32_t want = point || pose ? 48 : op == M3_OP_SET_SLEEP_CONTROLS ? 16 : 12;
+            if (bytes != want)
             {
                 m3gpuSetError(M3GPU_ERR_INVALID, "journal: bad body record (op %d)", op);
                 return false;
@@ -1178,10 +1181,35 @@ bool m3ParseJournal(const m3HostWorld* w, const uint8_t* stream, int32_t size,
                 ok = ok && isfinite(r.v.x) && isfinite(r.v.y) && isfinite(r.v.z) &&
                      isfinite(r.point.x) && isfinite(r.point.y) && isfinite(r.point.z);
             }
+            else if (pose)
+            {
+                memcpy(&r.point, payload + 8, 24);
+                memcpy(&r.rotation, payload + 32, 16);
+                const m3Quat q = r.rotation;
+                const float qq = q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w;
+                ok = ok && isfinite(r.point.x) && isfinite(r.point.y) && isfinite(r.point.z) &&
+                     isfinite(q.x) && isfinite(q.y) && isfinite(q.z) && isfinite(q.w) &&
+                     qq > 0.98f && qq < 1.02f;
+            }
+            else if (op == M3_OP_SET_SLEEP_CONTROLS)
+            {
+                // Any threshold: a non-positive or NaN one is the default.
+                memcpy(&r.setting[0], payload + 8, 4);
+                int32_t canSleep;
+                memcpy(&canSleep, payload + 12, 4);
+                r.bits = canSleep != 0 ? 1u : 0u;
+            }
             else
             {
                 memcpy(&r.bits, payload + 8, 4);
                 ok = ok && (op != M3_OP_SET_ALLOW_FAST_ROTATION || r.bits <= 1u);
+                if (op == M3_OP_SET_TYPE)
+                {
+                    // The reference keeps the low byte whatever it holds;
+                    // a byte that names no body type is refused here.
+                    r.bits &= 0xFFu;
+                    ok = ok && r.bits <= (uint32_t)M3_BODY_DYNAMIC;
+                }
             }
             if (!ok)
             {

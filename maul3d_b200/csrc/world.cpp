@@ -479,12 +479,16 @@ extern "C" void m3Body_SetAngularVelocity(m3BodyId bodyId, m3Vec3 velocity)
 }
 
 // ---------------------------------------------------------------------
-// Host-side body commands and getters (body.c:283-303, 379-404, 514-527,
-// 632-703, 910-958): forces and impulses at a world point, motion locks,
-// the fast-rotation escape.  Each public call checks as the reference's,
-// records the reference's journal record and changes the host image (the
-// next step uploads it); the journal replay applies the same records.
+// Host-side body commands and getters (body.c:170-330, 379-404, 514-823,
+// 910-958): forces and impulses at a world point, teleports and kinematic
+// targets, type changes, enabling, motion locks, sleep controls, forced
+// sleep or wake and the fast-rotation escape.  Each public call checks as
+// the reference's, records the reference's journal record and changes the
+// host image (the next step uploads it); the journal replay applies the
+// same records.
 // ---------------------------------------------------------------------
+static void RecomputeMass(m3HostWorld* w, int32_t b);
+
 static m3Vec3 ForceArm(const m3WorldView& v, int32_t i, m3Pos3 point)
 {
     const m3Transform xf = v.xf[i];
@@ -493,23 +497,112 @@ static m3Vec3 ForceArm(const m3WorldView& v, int32_t i, m3Pos3 point)
               (m3real)(point.z - xf.p.z) - rlc.z);
 }
 
-void m3ApplyHostBodyOp(m3HostWorld* w, int32_t op, int32_t i, m3Vec3 f, m3Pos3 point,
-                       uint32_t bits)
+// Wakes every sleeping dynamic body whose position, padded by its largest
+// extent and the box margin, overlaps the region around body `i` (its
+// position padded by its largest extent and four margins), in ascending
+// slots (body.c:170-205).
+static void WakeAround(m3WorldView& v, int32_t i)
+{
+    const double r = (double)v.maxExt[i] + 4.0 * (double)M3_AABB_MARGIN;
+    const m3Pos3 c = v.xf[i].p;
+    const double lo[3] = {c.x - r, c.y - r, c.z - r};
+    const double hi[3] = {c.x + r, c.y + r, c.z + r};
+    for (int32_t b = 0; b < v.sc->bodyMax; ++b)
+    {
+        if (v.bodyAlive[b] == 0 || v.btype[b] != M3_BODY_DYNAMIC || v.awake[b] != 0)
+        {
+            continue;
+        }
+        const double pad = (double)v.maxExt[b] + (double)M3_AABB_MARGIN;
+        const m3Pos3 p = v.xf[b].p;
+        if (p.x - pad <= hi[0] && p.x + pad >= lo[0] && p.y - pad <= hi[1] &&
+            p.y + pad >= lo[1] && p.z - pad <= hi[2] && p.z + pad >= lo[2])
+        {
+            v.awake[b] = 1;
+            v.sleepTime[b] = 0.0f;
+        }
+    }
+}
+
+static void Wake(m3WorldView& v, int32_t i)
+{
+    v.awake[i] = 1;
+    v.sleepTime[i] = 0.0f;
+}
+
+void m3ApplyHostBodyOp(m3HostWorld* w, const m3JournalRecordView& r)
 {
     m3WorldView& v = w->hv;
-    switch (op)
+    const int32_t i = r.body;
+    const uint32_t bits = r.bits;
+    switch (r.op)
     {
     case M3_OP_APPLY_FORCE_AT_POINT:
-        v.force[i] = m3Add3(v.force[i], f);
-        v.torque[i] = m3Add3(v.torque[i], m3Cross3(ForceArm(v, i, point), f));
-        m3WakeOnCommand(v, i, f);
+        v.force[i] = m3Add3(v.force[i], r.v);
+        v.torque[i] = m3Add3(v.torque[i], m3Cross3(ForceArm(v, i, r.point), r.v));
+        m3WakeOnCommand(v, i, r.v);
         break;
     case M3_OP_APPLY_IMPULSE_AT_POINT:
-        v.v[i] = m3Add3(v.v[i], m3MulSV3(v.invMass[i], f));
-        v.w[i] = m3Add3(v.w[i],
-                        m3MulMV3(m3WorldInvInertiaHD(v, i), m3Cross3(ForceArm(v, i, point), f)));
-        m3WakeOnCommand(v, i, f);
+        v.v[i] = m3Add3(v.v[i], m3MulSV3(v.invMass[i], r.v));
+        v.w[i] = m3Add3(v.w[i], m3MulMV3(m3WorldInvInertiaHD(v, i),
+                                         m3Cross3(ForceArm(v, i, r.point), r.v)));
+        m3WakeOnCommand(v, i, r.v);
         break;
+    case M3_OP_SET_TRANSFORM:
+        // The vacated and the arrival neighbourhoods wake (body.c:207-218).
+        WakeAround(v, i);
+        v.xf[i] = m3Transform{r.point, r.rotation};
+        WakeAround(v, i);
+        Wake(v, i);
+        break;
+    case M3_OP_SET_TARGET_TRANSFORM:
+        v.hasTarget[i] = 1;
+        v.target[i] = m3Transform{r.point, r.rotation};
+        Wake(v, i);
+        break;
+    case M3_OP_SET_TYPE:
+    {
+        // body.c:228-262: static drops its velocities; kinematic and static
+        // keep zero inverse mass; dynamic rebuilds its mass from its shapes.
+        const uint8_t type = (uint8_t)bits;
+        if (v.btype[i] == type)
+        {
+            break;
+        }
+        WakeAround(v, i);
+        v.btype[i] = type;
+        if (type == M3_BODY_STATIC)
+        {
+            v.v[i] = v3(0.0f, 0.0f, 0.0f);
+            v.w[i] = v3(0.0f, 0.0f, 0.0f);
+        }
+        if (type == M3_BODY_DYNAMIC)
+        {
+            RecomputeMass(w, i);
+        }
+        else
+        {
+            v.invMass[i] = 0.0f;
+            v.invI[i] = m3ZeroMat3();
+        }
+        Wake(v, i);
+        break;
+    }
+    case M3_OP_SET_ENABLED:
+    {
+        const uint8_t want = bits != 0 ? 1 : 0;
+        if (v.enabled[i] == want)
+        {
+            break;
+        }
+        v.enabled[i] = want;
+        WakeAround(v, i);
+        if (want)
+        {
+            Wake(v, i);
+        }
+        break;
+    }
     case M3_OP_SET_MOTION_LOCKS:
         // The fast-rotation bit is its own command's (body.c:283-303).
         v.locks[i] = (uint8_t)((v.locks[i] & M3_LOCKS_ALLOW_FAST_ROTATION) | (bits & 0x3Fu));
@@ -526,6 +619,30 @@ void m3ApplyHostBodyOp(m3HostWorld* w, int32_t op, int32_t i, m3Vec3 f, m3Pos3 p
         if (bits & 32u)
             v.w[i].z = 0.0f;
         break;
+    case M3_OP_SET_SLEEP_CONTROLS:
+        // body.c:305-314: a non-positive (or NaN) threshold is the default.
+        v.sleepThreshold[i] = r.setting[0] > 0.0f ? r.setting[0] : M3_SLEEP_VELOCITY_DEFAULT;
+        v.canSleep[i] = bits != 0 ? 1 : 0;
+        if (bits == 0)
+        {
+            Wake(v, i);
+        }
+        break;
+    case M3_OP_SET_AWAKE:
+        // body.c:316-330.  The reference also records the frozen body's
+        // pairs in its sleeping-pair buffer; that buffer is neither hashed
+        // nor saved, and the device finds every pair by its own rule.
+        if (bits != 0)
+        {
+            Wake(v, i);
+        }
+        else
+        {
+            v.awake[i] = 0;
+            v.v[i] = v3(0.0f, 0.0f, 0.0f);
+            v.w[i] = v3(0.0f, 0.0f, 0.0f);
+        }
+        break;
     case M3_OP_SET_ALLOW_FAST_ROTATION:
         v.locks[i] = bits != 0 ? (uint8_t)(v.locks[i] | M3_LOCKS_ALLOW_FAST_ROTATION)
                                : (uint8_t)(v.locks[i] & ~M3_LOCKS_ALLOW_FAST_ROTATION);
@@ -533,6 +650,25 @@ void m3ApplyHostBodyOp(m3HostWorld* w, int32_t op, int32_t i, m3Vec3 f, m3Pos3 p
     default:
         break;
     }
+}
+
+// Journals one host body command and applies it: `payload` is the
+// reference's record for `r.op`, `r` the command with the body slot.
+static void HostCommand(m3HostWorld* w, const m3JournalRecordView& r, const void* payload,
+                        int32_t bytes)
+{
+    m3JournalAppend(w, r.op, payload, bytes);
+    m3ApplyHostBodyOp(w, r);
+    w->hostDirty = true;
+}
+
+static m3JournalRecordView CommandView(int32_t op, int32_t index)
+{
+    m3JournalRecordView r;
+    memset(&r, 0, sizeof(r));
+    r.op = op;
+    r.body = index;
+    return r;
 }
 
 // A force or impulse at a world point: {m3BodyId id; m3Vec3 v; m3Pos3 p}.
@@ -559,9 +695,10 @@ static void PointCommand(m3BodyId id, int32_t op, m3Vec3 f, m3Pos3 point)
     record.id = id;
     record.v = f;
     record.p = point;
-    m3JournalAppend(w, op, &record, (int32_t)sizeof(record));
-    m3ApplyHostBodyOp(w, op, index, f, point, 0u);
-    w->hostDirty = true;
+    m3JournalRecordView r = CommandView(op, index);
+    r.v = f;
+    r.point = point;
+    HostCommand(w, r, &record, (int32_t)sizeof(record));
 }
 
 extern "C" void m3Body_ApplyForceAtPoint(m3BodyId bodyId, m3Vec3 force, m3Pos3 point)
@@ -574,7 +711,49 @@ extern "C" void m3Body_ApplyLinearImpulseAtPoint(m3BodyId bodyId, m3Vec3 impulse
     PointCommand(bodyId, M3_OP_APPLY_IMPULSE_AT_POINT, impulse, point);
 }
 
-// Lock bits or the fast-rotation flag: {m3BodyId id; uint32 bits}.
+// A pose: {m3BodyId id; m3Transform pose}; the rotation must be finite and
+// near unit length.  Targets reach kinematic bodies only (body.c:531-583).
+static void PoseCommand(m3BodyId id, int32_t op, m3Pos3 position, m3Quat rotation)
+{
+    m3gpuClearError();
+    int32_t index;
+    m3HostWorld* w = ResolveBody(id, &index);
+    const m3real qq = rotation.x * rotation.x + rotation.y * rotation.y +
+                      rotation.z * rotation.z + rotation.w * rotation.w;
+    if (w == nullptr || !FinitePos3(position) || !FiniteQuat(rotation) || !(qq > 0.98f) ||
+        !(qq < 1.02f) || m3gpuSyncHost(w) != M3GPU_OK)
+    {
+        return;
+    }
+    if (op == M3_OP_SET_TARGET_TRANSFORM && w->hv.btype[index] != M3_BODY_KINEMATIC)
+    {
+        return;
+    }
+    struct
+    {
+        m3BodyId id;
+        m3Transform pose;
+    } record;
+    memset(&record, 0, sizeof(record));
+    record.id = id;
+    record.pose = m3Transform{position, rotation};
+    m3JournalRecordView r = CommandView(op, index);
+    r.point = position;
+    r.rotation = rotation;
+    HostCommand(w, r, &record, (int32_t)sizeof(record));
+}
+
+extern "C" void m3Body_SetTransform(m3BodyId bodyId, m3Pos3 position, m3Quat rotation)
+{
+    PoseCommand(bodyId, M3_OP_SET_TRANSFORM, position, rotation);
+}
+
+extern "C" void m3Body_SetTargetTransform(m3BodyId bodyId, m3Pos3 position, m3Quat rotation)
+{
+    PoseCommand(bodyId, M3_OP_SET_TARGET_TRANSFORM, position, rotation);
+}
+
+// Lock bits, a type or a flag: {m3BodyId id; uint32 bits}.
 static void BitsCommand(m3BodyId id, int32_t op, uint32_t bits)
 {
     m3gpuClearError();
@@ -584,6 +763,10 @@ static void BitsCommand(m3BodyId id, int32_t op, uint32_t bits)
     {
         return;
     }
+    if (op == M3_OP_SET_AWAKE && w->hv.btype[index] != M3_BODY_DYNAMIC)
+    {
+        return; // body.c:795-800: dynamic bodies only
+    }
     struct
     {
         m3BodyId id;
@@ -592,9 +775,56 @@ static void BitsCommand(m3BodyId id, int32_t op, uint32_t bits)
     memset(&record, 0, sizeof(record));
     record.id = id;
     record.bits = bits;
-    m3JournalAppend(w, op, &record, (int32_t)sizeof(record));
-    m3ApplyHostBodyOp(w, op, index, v3(0.0f, 0.0f, 0.0f), m3Pos3{0.0, 0.0, 0.0}, bits);
-    w->hostDirty = true;
+    m3JournalRecordView r = CommandView(op, index);
+    r.bits = bits;
+    HostCommand(w, r, &record, (int32_t)sizeof(record));
+}
+
+extern "C" void m3Body_SetType(m3BodyId bodyId, m3BodyType type)
+{
+    if (type != m3_staticBody && type != m3_kinematicBody && type != m3_dynamicBody)
+    {
+        return;
+    }
+    BitsCommand(bodyId, M3_OP_SET_TYPE, (uint32_t)type);
+}
+
+extern "C" void m3Body_SetEnabled(m3BodyId bodyId, bool enabled)
+{
+    BitsCommand(bodyId, M3_OP_SET_ENABLED, enabled ? 1u : 0u);
+}
+
+extern "C" void m3Body_SetAwake(m3BodyId bodyId, bool awake)
+{
+    BitsCommand(bodyId, M3_OP_SET_AWAKE, awake ? 1u : 0u);
+}
+
+// {m3BodyId id; float threshold; int32 canSleep}; a negative or
+// non-finite threshold is refused (body.c:763-786).
+extern "C" void m3Body_SetSleepControls(m3BodyId bodyId, float threshold, bool canSleep)
+{
+    m3gpuClearError();
+    int32_t index;
+    m3HostWorld* w = ResolveBody(bodyId, &index);
+    if (w == nullptr || !isfinite(threshold) || threshold < 0.0f ||
+        m3gpuSyncHost(w) != M3GPU_OK)
+    {
+        return;
+    }
+    struct
+    {
+        m3BodyId id;
+        float threshold;
+        int32_t canSleep;
+    } record;
+    memset(&record, 0, sizeof(record));
+    record.id = bodyId;
+    record.threshold = threshold;
+    record.canSleep = canSleep ? 1 : 0;
+    m3JournalRecordView r = CommandView(M3_OP_SET_SLEEP_CONTROLS, index);
+    r.setting[0] = threshold;
+    r.bits = canSleep ? 1u : 0u;
+    HostCommand(w, r, &record, (int32_t)sizeof(record));
 }
 
 extern "C" void m3Body_SetMotionLocks(m3BodyId bodyId, uint32_t locks)

@@ -1,10 +1,12 @@
-"""Body commands at a world point, motion locks and the fast-rotation switch
-(body.h:64-121; body.c:283-303, 387-404, 639-709, 910-958) on the host:
-with valid and refused arguments they leave the world with the reference's
-hash, getters and journal bytes, the reference's journal of them replays
-here to the same world, and hostile records are refused whole
-(world.c:2323-2352, 2419-2439, 2904-2928).  Stepping after these commands
-is covered on the device by test_body_commands_gpu.py."""
+"""Body commands at a world point and the runtime controls: teleports,
+kinematic targets, type changes, enabling, motion locks, sleep controls,
+forced sleep or wake and the fast-rotation switch (body.h:64-121;
+body.c:170-330, 387-404, 531-823, 910-958) on the host.  With valid and
+refused arguments they leave the world with the reference's hash, getters
+and journal bytes, the reference's journal of them replays here to the
+same world, and hostile records are refused whole (world.c:2323-2465,
+2904-2928).  Stepping after these commands is covered on the device by
+test_body_commands_gpu.py."""
 import ctypes as C
 import struct
 
@@ -13,6 +15,7 @@ from maul3d_b200.abi import SCENE_TOWERS, SCENE_UNEVEN
 
 V = abi.m3Vec3
 P = abi.m3Pos3
+Q = abi.m3Quat
 
 
 def _commands(lib, wid):
@@ -37,6 +40,34 @@ def _commands(lib, wid):
     stale = abi.m3BodyId(3, w0, 9)
     lib.m3Body_SetMotionLocks(stale, 0x01)
     lib.m3Body_ApplyForceAtPoint(stale, V(1.0, 0.0, 0.0), P(0.0, 0.0, 0.0))
+    _controls(lib, wid)
+
+
+def _controls(lib, wid):
+    w0 = wid.index1 - 1
+    b = [abi.m3BodyId(k, w0, 0) for k in range(12)]
+    half = 0.5 ** 0.5
+    lib.m3Body_SetAwake(b[8], False)
+    lib.m3Body_SetAwake(b[9], False)
+    lib.m3Body_SetTransform(b[8], P(4.0, 6.0, -2.0), Q(0.0, half, 0.0, half))
+    lib.m3Body_SetTransform(b[9], P(1.0, 2.0, 3.0), Q(0.0, 0.0, 0.0, 2.0))      # refused
+    lib.m3Body_SetTransform(b[9], P(float("nan"), 2.0, 3.0), Q(0.0, 0.0, 0.0, 1.0))
+    lib.m3Body_SetTargetTransform(b[9], P(1.0, 2.0, 3.0), Q(0.0, 0.0, 0.0, 1.0))  # not kinematic
+    lib.m3Body_SetType(b[10], 1)
+    lib.m3Body_SetTargetTransform(b[10], P(0.5, 3.0, 0.5), Q(0.0, 0.0, half, half))
+    lib.m3Body_SetType(b[11], 0)
+    lib.m3Body_SetType(b[11], 2)
+    lib.m3Body_SetType(b[7], 2)                                                   # same type
+    lib.m3Body_SetType(b[6], 5)                                                   # refused
+    lib.m3Body_SetEnabled(b[5], False)
+    lib.m3Body_SetEnabled(b[4], False)
+    lib.m3Body_SetEnabled(b[4], True)
+    lib.m3Body_SetSleepControls(b[3], 0.2, False)
+    lib.m3Body_SetSleepControls(b[2], 0.0, True)
+    lib.m3Body_SetSleepControls(b[2], -1.0, True)                                 # refused
+    lib.m3Body_SetSleepControls(b[2], float("inf"), True)                         # refused
+    lib.m3Body_SetAwake(b[1], False)                                              # static
+    lib.m3Body_SetAwake(b[9], True)
 
 
 def _engines(m3, oracle):
@@ -72,11 +103,12 @@ def _getters(lib, wid, count):
     for i in range(1, count + 1):
         b = abi.m3BodyId(i, w0, 0)
         rows.append((lib.m3Body_GetMotionLocks(b), lib.m3Body_GetAllowFastRotation(b),
-                     lib.m3Body_GetType(b), lib.m3Body_GetUserData(b), lib.m3Body_IsEnabled(b)))
+                     lib.m3Body_GetType(b), lib.m3Body_GetUserData(b), lib.m3Body_IsEnabled(b),
+                     lib.m3Body_IsAwake(b)))
     stale = abi.m3BodyId(2, w0, 7)
     rows.append((lib.m3Body_GetMotionLocks(stale), lib.m3Body_GetAllowFastRotation(stale),
                  lib.m3Body_GetType(stale), lib.m3Body_GetUserData(stale),
-                 lib.m3Body_IsEnabled(stale)))
+                 lib.m3Body_IsEnabled(stale), lib.m3Body_IsAwake(stale)))
     return rows
 
 
@@ -128,7 +160,16 @@ def test_hostile_body_records_are_refused_whole(m3, oracle):
                 abi.journal_record(30, stale + v + bytes(4) + p),
                 abi.journal_record(65, body + struct.pack("<I", 2)),
                 abi.journal_record(36, stale + struct.pack("<I", 1)),
-                abi.journal_record(36, body + struct.pack("<H", 1))):
+                abi.journal_record(36, body + struct.pack("<H", 1)),
+                abi.journal_record(32, body + C.string_at(C.byref(P(0.0, 1.0, 0.0)), 24) +
+                                   struct.pack("<4f", 0.0, 0.0, 0.0, 1.5)),
+                abi.journal_record(33, stale + C.string_at(C.byref(P(0.0, 1.0, 0.0)), 24) +
+                                   struct.pack("<4f", 0.0, 0.0, 0.0, 1.0)),
+                abi.journal_record(32, body + struct.pack("<3d", 0.0, float("nan"), 0.0) +
+                                   struct.pack("<4f", 0.0, 0.0, 0.0, 1.0)),
+                abi.journal_record(35, stale + struct.pack("<i", 1)),
+                abi.journal_record(38, body + struct.pack("<i", 1)[:3]),
+                abi.journal_record(37, body + struct.pack("<fi", 0.5, 1)[:4])):
         stream = good + bad
         gbuf = (C.c_uint8 * len(stream)).from_buffer_copy(stream)
         assert not glib.m3World_JournalReplay(g.id, gbuf, len(stream))
@@ -145,6 +186,16 @@ def test_hostile_body_records_are_refused_whole(m3, oracle):
     assert rlib.m3World_JournalReplay(r2.id, rbuf, len(wide))
     assert g.hash() == r2.hash()
     assert glib.m3Body_GetMotionLocks(abi.m3BodyId(3, w0, 0)) == 0x02
+    # A type record keeps its low byte in both; one that names no body type
+    # is refused here (the reference would store a type no path knows).
+    for value, ok in ((0x102, True), (7, False)):
+        rec = abi.journal_record(34, body + struct.pack("<i", value))
+        gbuf = (C.c_uint8 * len(rec)).from_buffer_copy(rec)
+        rbuf = (C.c_uint8 * len(rec)).from_buffer_copy(rec)
+        assert bool(glib.m3World_JournalReplay(g.id, gbuf, len(rec))) == ok
+        if ok:
+            assert rlib.m3World_JournalReplay(r2.id, rbuf, len(rec))
+            assert g.hash() == r2.hash()
     g.destroy()
     r.destroy()
     r2.destroy()

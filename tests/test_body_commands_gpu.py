@@ -1,12 +1,15 @@
-"""Body commands at a world point, motion locks and the fast-rotation switch
-between device steps (needs a B200).
+"""Body commands at a world point and the runtime controls between device
+steps (needs a B200).
 
 Worlds step on the device; then forces and impulses at world points,
-motion locks and the fast-rotation switch are applied (later some locks
-are lifted) and the worlds step on: the locked components re-zero every
-substep (solver.c:4156-4177) and the switch bypasses the angular cap
-(solver.c:4131-4144).  Every step's hash must equal the reference
-engine's, which takes the same calls.
+motion locks, the fast-rotation switch, teleports, forced sleep, a body
+turned kinematic and servoed to a target, a body disabled and sleep
+controls are applied (later some locks are lifted, the kinematic body
+turns dynamic again and the disabled one comes back) and the worlds step
+on: the locked components re-zero every substep (solver.c:4156-4177), the
+switch bypasses the angular cap (solver.c:4131-4144), the target drives
+the kinematic body's velocity.  Every step's hash must equal the
+reference engine's, which takes the same calls.
 """
 import pytest
 
@@ -20,6 +23,7 @@ pytestmark = [pytest.mark.gpu,
 DT = 1.0 / 60.0
 V = abi.m3Vec3
 P = abi.m3Pos3
+Q = abi.m3Quat
 
 
 def _command(lib, wid, lift):
@@ -33,6 +37,24 @@ def _command(lib, wid, lift):
         lib.m3Body_ApplyForceAtPoint(b, V(-3.0, 8.0, 2.0 * k), P(1.0, 0.5, -0.5 * k))
         lib.m3Body_SetMotionLocks(b, [0x01, 0x2A, 0x07, 0x38, 0x12, 0x3F][k])
         lib.m3Body_SetAllowFastRotation(b, k % 3 == 0)
+    b = [abi.m3BodyId(k, w0, 0) for k in range(24)]
+    half = 0.5 ** 0.5
+    if lift:
+        lib.m3Body_SetType(b[16], 2)
+        lib.m3Body_SetEnabled(b[18], True)
+        lib.m3Body_SetAwake(b[20], True)
+        lib.m3Body_SetSleepControls(b[22], 0.0, True)
+        return
+    pos = lib.m3Body_GetPosition(b[14])
+    lib.m3Body_SetTransform(b[14], P(pos.x + 0.5, pos.y + 3.0, pos.z), Q(0.0, half, 0.0, half))
+    lib.m3Body_SetType(b[16], 1)
+    pos = lib.m3Body_GetPosition(b[16])
+    lib.m3Body_SetTargetTransform(b[16], P(pos.x, pos.y + 0.5, pos.z + 0.25),
+                                  Q(0.0, 0.0, 0.258819, 0.9659258))
+    lib.m3Body_SetEnabled(b[18], False)
+    lib.m3Body_SetAwake(b[20], False)
+    lib.m3Body_SetSleepControls(b[22], 0.3, False)
+    lib.m3Body_SetSleepControls(b[23], 0.5, True)
 
 
 @pytest.mark.parametrize("scene,seed,param", [(SCENE_UNEVEN, 91, 300), (SCENE_BOUNCE, 92, 50)])
