@@ -446,6 +446,26 @@ M3GPU_API m3ShapeId m3CreateHeightFieldGridShape(m3BodyId bodyId, const m3ShapeD
                                                  const float* heights, int32_t nx, int32_t nz,
                                                  float cellSize);
 M3GPU_API bool m3Shape_IsValid(m3ShapeId shapeId);
+/* shape.c:1351-1363 (shape.h:271): the body that carries the shape; a
+ * null id for a stale shape. */
+M3GPU_API m3BodyId m3Shape_GetBody(m3ShapeId shapeId);
+/* Materials and flags (shape.c:1387-1410, 1463-1600; shape.h:286-303),
+ * each journaled like the reference's.  Friction, restitution and rolling
+ * resistance must be finite and not negative, a density finite and
+ * positive (the body's mass is rebuilt from its shapes when asked); a
+ * refused value is a no-op.  Getters read 0 (false) for a stale shape. */
+M3GPU_API void m3Shape_SetFriction(m3ShapeId shapeId, float friction);
+M3GPU_API float m3Shape_GetFriction(m3ShapeId shapeId);
+M3GPU_API void m3Shape_SetRestitution(m3ShapeId shapeId, float restitution);
+M3GPU_API float m3Shape_GetRestitution(m3ShapeId shapeId);
+M3GPU_API void m3Shape_SetRollingResistance(m3ShapeId shapeId, float value);
+M3GPU_API float m3Shape_GetRollingResistance(m3ShapeId shapeId);
+M3GPU_API void m3Shape_SetDensity(m3ShapeId shapeId, float density, bool updateBodyMass);
+M3GPU_API float m3Shape_GetDensity(m3ShapeId shapeId);
+M3GPU_API void m3Shape_EnableHitEvents(m3ShapeId shapeId, bool flag);
+M3GPU_API bool m3Shape_AreHitEventsEnabled(m3ShapeId shapeId);
+M3GPU_API void m3Shape_EnablePreSolve(m3ShapeId shapeId, bool flag);
+M3GPU_API bool m3Shape_IsPreSolveEnabled(m3ShapeId shapeId);
 
 /* joint.c:15 (joint.h:134) and joint.h:136: spherical, revolute and
  * fixed joints are stepped on the device. */

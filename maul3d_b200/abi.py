@@ -469,6 +469,26 @@ def bind_body_commands(lib: C.CDLL) -> C.CDLL:
     return lib
 
 
+def bind_shape_commands(lib: C.CDLL) -> C.CDLL:
+    """Declare the reference-named shape materials, flags and getters."""
+    for name in ("m3Shape_SetFriction", "m3Shape_SetRestitution", "m3Shape_SetRollingResistance"):
+        getattr(lib, name).argtypes = [m3ShapeId, C.c_float]
+        getattr(lib, name).restype = None
+    lib.m3Shape_SetDensity.argtypes = [m3ShapeId, C.c_float, C.c_bool]
+    lib.m3Shape_SetDensity.restype = None
+    for name in ("m3Shape_EnableHitEvents", "m3Shape_EnablePreSolve"):
+        getattr(lib, name).argtypes = [m3ShapeId, C.c_bool]
+        getattr(lib, name).restype = None
+    for name, res in (("m3Shape_GetFriction", C.c_float), ("m3Shape_GetRestitution", C.c_float),
+                      ("m3Shape_GetRollingResistance", C.c_float),
+                      ("m3Shape_GetDensity", C.c_float),
+                      ("m3Shape_AreHitEventsEnabled", C.c_bool),
+                      ("m3Shape_IsPreSolveEnabled", C.c_bool), ("m3Shape_GetBody", m3BodyId)):
+        getattr(lib, name).argtypes = [m3ShapeId]
+        getattr(lib, name).restype = res
+    return lib
+
+
 def bind_create(lib: C.CDLL) -> C.CDLL:
     """Declare the reference-named creation API on a handle."""
     lib.m3DefaultWorldDef.restype = m3WorldDef

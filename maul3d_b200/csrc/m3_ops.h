@@ -40,6 +40,13 @@ enum
     M3_OP_SET_SLEEP_CONTROLS = 37,
     M3_OP_SET_AWAKE = 38,
     M3_OP_SET_ALLOW_FAST_ROTATION = 65,
+    // Shape materials and flags (world_internal.h:146-149, 156-157).
+    M3_OP_SET_SHAPE_FRICTION = 40,
+    M3_OP_SET_SHAPE_RESTITUTION = 41,
+    M3_OP_SET_SHAPE_ROLLING = 42,
+    M3_OP_SET_SHAPE_DENSITY = 43,
+    M3_OP_ENABLE_SHAPE_HIT_EVENTS = 50,
+    M3_OP_ENABLE_SHAPE_PRESOLVE = 51,
 };
 
 // One command for the device kernel: `world` indexes the batch, `body`
@@ -68,6 +75,13 @@ M3_HD bool m3IsHostBodyOp(int32_t op)
 {
     return (op >= M3_OP_APPLY_FORCE_AT_POINT && op <= M3_OP_SET_AWAKE) ||
            op == M3_OP_SET_ALLOW_FAST_ROTATION;
+}
+
+// Shape commands applied on the host image only: never device ops.
+M3_HD bool m3IsHostShapeOp(int32_t op)
+{
+    return (op >= M3_OP_SET_SHAPE_FRICTION && op <= M3_OP_SET_SHAPE_DENSITY) ||
+           op == M3_OP_ENABLE_SHAPE_HIT_EVENTS || op == M3_OP_ENABLE_SHAPE_PRESOLVE;
 }
 
 // Joint commands ride the same record: `body` is then the joint slot.

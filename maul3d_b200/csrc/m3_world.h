@@ -358,6 +358,11 @@ void m3ApplyWorldSetting(m3HostWorld* w, int32_t op, const float* words);
 // impulse with its world `point`; a pose (`point`, `rotation`); `bits`
 // the lock bits, type or flag; `setting[0]` a sleep threshold.  world.cpp.
 void m3ApplyHostBodyOp(m3HostWorld* w, const m3JournalRecordView& r);
+// Applies a validated shape command (shape.c:1387-1410, 1557-1565) to the
+// host image, the shape slot in `r.body`: `setting[0]` the friction,
+// restitution, rolling resistance or density; `bits` the flag, or for a
+// density whether the body's mass is rebuilt.  world.cpp.
+void m3ApplyHostShapeOp(m3HostWorld* w, const m3JournalRecordView& r);
 // Parses and validates a whole journal against a world's bodies; false
 // (with the error set) on the first bad or unsupported record.
 // Worlds outside the world table (world.cpp): built on any thread,

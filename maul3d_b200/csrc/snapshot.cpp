@@ -1059,6 +1059,10 @@ extern "C" bool m3World_JournalReplay(m3WorldId worldId, const void* data, int32
         {
             m3ApplyHostBodyOp(w, r);
         }
+        else if (m3IsHostShapeOp(r.op))
+        {
+            m3ApplyHostShapeOp(w, r);
+        }
         else
         {
             m3ApplyBodyOp(w->hv, r.op, r.body, r.v);
@@ -1214,6 +1218,50 @@ bool m3ParseJournal(const m3HostWorld* w, const uint8_t* stream, int32_t size,
             if (!ok)
             {
                 m3gpuSetError(M3GPU_ERR_INVALID, "journal: stale body or bad values (op %d)", op);
+                return false;
+            }
+            r.body = index;
+        }
+        else if (m3IsHostShapeOp(op))
+        {
+            // world.c:2500-2555, 3021-3049: materials {m3ShapeId; float}
+            // (finite, not negative), densities {m3ShapeId; float; int32}
+            // (finite, positive), flags {m3ShapeId; int32}; the id is
+            // retargeted to this world.
+            const bool flag =
+                op == M3_OP_ENABLE_SHAPE_HIT_EVENTS || op == M3_OP_ENABLE_SHAPE_PRESOLVE;
+            if (bytes != (op == M3_OP_SET_SHAPE_DENSITY ? 16 : 12))
+            {
+                m3gpuSetError(M3GPU_ERR_INVALID, "journal: bad shape record (op %d)", op);
+                return false;
+            }
+            m3ShapeId id;
+            memcpy(&id, payload, 8);
+            const int32_t index = id.index1 - 1;
+            bool ok = index >= 0 && index < w->hv.sc->shapeMax && w->hv.shapeAlive[index] != 0 &&
+                      w->hv.shapeGen[index] == id.generation;
+            if (flag)
+            {
+                int32_t on;
+                memcpy(&on, payload + 8, 4);
+                r.bits = on != 0 ? 1u : 0u;
+            }
+            else
+            {
+                memcpy(&r.setting[0], payload + 8, 4);
+                const float value = r.setting[0];
+                ok = ok && isfinite(value) &&
+                     (op == M3_OP_SET_SHAPE_DENSITY ? value > 0.0f : value >= 0.0f);
+                if (op == M3_OP_SET_SHAPE_DENSITY)
+                {
+                    int32_t update;
+                    memcpy(&update, payload + 12, 4);
+                    r.bits = update != 0 ? 1u : 0u;
+                }
+            }
+            if (!ok)
+            {
+                m3gpuSetError(M3GPU_ERR_INVALID, "journal: stale shape or bad value (op %d)", op);
                 return false;
             }
             r.body = index;

@@ -1589,6 +1589,195 @@ extern "C" bool m3Shape_IsValid(m3ShapeId shapeId)
            w->hv.shapeAlive[index] != 0 && w->hv.shapeGen[index] == shapeId.generation;
 }
 
+static m3HostWorld* ResolveShape(m3ShapeId id, int32_t* index)
+{
+    m3HostWorld* w = m3gpuWorldFromIndex0(id.world0);
+    const int32_t i = id.index1 - 1;
+    if (w == nullptr || i < 0 || i >= w->hv.sc->shapeMax || w->hv.shapeAlive[i] == 0 ||
+        w->hv.shapeGen[i] != id.generation)
+    {
+        *index = -1;
+        return nullptr;
+    }
+    *index = i;
+    return w;
+}
+
+extern "C" m3BodyId m3Shape_GetBody(m3ShapeId shapeId)
+{
+    int32_t index;
+    m3HostWorld* w = ResolveShape(shapeId, &index);
+    if (w == nullptr)
+    {
+        return m3BodyId{0, 0, 0};
+    }
+    const int32_t b = w->hv.shapeBody[index];
+    return m3BodyId{b + 1, (uint16_t)w->slot, w->hv.bodyGen[b]};
+}
+
+// Shape materials and flags (shape.c:1387-1410, 1463-1600): each public
+// call checks as the reference's, records its journal record and changes
+// the host image (the next step uploads it); replay applies the same
+// records.
+void m3ApplyHostShapeOp(m3HostWorld* w, const m3JournalRecordView& r)
+{
+    m3WorldView& v = w->hv;
+    const int32_t s = r.body;
+    switch (r.op)
+    {
+    case M3_OP_SET_SHAPE_FRICTION:
+        v.friction[s] = r.setting[0];
+        break;
+    case M3_OP_SET_SHAPE_RESTITUTION:
+        v.restitution[s] = r.setting[0];
+        break;
+    case M3_OP_SET_SHAPE_ROLLING:
+        v.rolling[s] = r.setting[0];
+        break;
+    case M3_OP_SET_SHAPE_DENSITY:
+        v.density[s] = r.setting[0];
+        if (r.bits != 0)
+        {
+            RecomputeMass(w, v.shapeBody[s]);
+        }
+        break;
+    case M3_OP_ENABLE_SHAPE_HIT_EVENTS:
+        v.hitEvents[s] = r.bits != 0 ? 1 : 0;
+        break;
+    case M3_OP_ENABLE_SHAPE_PRESOLVE:
+        v.preSolve[s] = r.bits != 0 ? 1 : 0;
+        break;
+    default:
+        break;
+    }
+}
+
+// {m3ShapeId id; float value} for a material, {m3ShapeId id; float
+// density; int32 updateMass} for a density, {m3ShapeId id; int32 on} for
+// a flag.
+static void ShapeCommand(m3ShapeId id, int32_t op, float value, uint32_t bits)
+{
+    m3gpuClearError();
+    int32_t index;
+    m3HostWorld* w = ResolveShape(id, &index);
+    if (w == nullptr || m3gpuSyncHost(w) != M3GPU_OK)
+    {
+        return;
+    }
+    uint8_t payload[16];
+    memset(payload, 0, sizeof(payload));
+    memcpy(payload, &id, 8);
+    int32_t bytes = 12;
+    if (op == M3_OP_ENABLE_SHAPE_HIT_EVENTS || op == M3_OP_ENABLE_SHAPE_PRESOLVE)
+    {
+        memcpy(payload + 8, &bits, 4);
+    }
+    else
+    {
+        memcpy(payload + 8, &value, 4);
+        if (op == M3_OP_SET_SHAPE_DENSITY)
+        {
+            memcpy(payload + 12, &bits, 4);
+            bytes = 16;
+        }
+    }
+    m3JournalRecordView r;
+    memset(&r, 0, sizeof(r));
+    r.op = op;
+    r.body = index;
+    r.setting[0] = value;
+    r.bits = bits;
+    m3JournalAppend(w, op, payload, bytes);
+    m3ApplyHostShapeOp(w, r);
+    w->hostDirty = true;
+}
+
+extern "C" void m3Shape_SetFriction(m3ShapeId shapeId, float friction)
+{
+    if (isfinite(friction) && friction >= 0.0f)
+    {
+        ShapeCommand(shapeId, M3_OP_SET_SHAPE_FRICTION, friction, 0u);
+    }
+}
+
+extern "C" void m3Shape_SetRestitution(m3ShapeId shapeId, float restitution)
+{
+    if (isfinite(restitution) && restitution >= 0.0f)
+    {
+        ShapeCommand(shapeId, M3_OP_SET_SHAPE_RESTITUTION, restitution, 0u);
+    }
+}
+
+extern "C" void m3Shape_SetRollingResistance(m3ShapeId shapeId, float value)
+{
+    if (isfinite(value) && value >= 0.0f)
+    {
+        ShapeCommand(shapeId, M3_OP_SET_SHAPE_ROLLING, value, 0u);
+    }
+}
+
+extern "C" void m3Shape_SetDensity(m3ShapeId shapeId, float density, bool updateBodyMass)
+{
+    if (isfinite(density) && density > 0.0f)
+    {
+        ShapeCommand(shapeId, M3_OP_SET_SHAPE_DENSITY, density, updateBodyMass ? 1u : 0u);
+    }
+}
+
+extern "C" void m3Shape_EnableHitEvents(m3ShapeId shapeId, bool flag)
+{
+    ShapeCommand(shapeId, M3_OP_ENABLE_SHAPE_HIT_EVENTS, 0.0f, flag ? 1u : 0u);
+}
+
+extern "C" void m3Shape_EnablePreSolve(m3ShapeId shapeId, bool flag)
+{
+    ShapeCommand(shapeId, M3_OP_ENABLE_SHAPE_PRESOLVE, 0.0f, flag ? 1u : 0u);
+}
+
+template <typename T, typename F> static T ReadShapeField(m3ShapeId id, T zero, F get)
+{
+    int32_t index;
+    m3HostWorld* w = ResolveShape(id, &index);
+    if (w == nullptr || m3gpuSyncHost(w) != M3GPU_OK)
+    {
+        return zero;
+    }
+    return get(w->hv, index);
+}
+
+extern "C" float m3Shape_GetFriction(m3ShapeId shapeId)
+{
+    return ReadShapeField(shapeId, 0.0f, [](const m3WorldView& v, int32_t s) { return v.friction[s]; });
+}
+
+extern "C" float m3Shape_GetRestitution(m3ShapeId shapeId)
+{
+    return ReadShapeField(shapeId, 0.0f,
+                     [](const m3WorldView& v, int32_t s) { return v.restitution[s]; });
+}
+
+extern "C" float m3Shape_GetRollingResistance(m3ShapeId shapeId)
+{
+    return ReadShapeField(shapeId, 0.0f, [](const m3WorldView& v, int32_t s) { return v.rolling[s]; });
+}
+
+extern "C" float m3Shape_GetDensity(m3ShapeId shapeId)
+{
+    return ReadShapeField(shapeId, 0.0f, [](const m3WorldView& v, int32_t s) { return v.density[s]; });
+}
+
+extern "C" bool m3Shape_AreHitEventsEnabled(m3ShapeId shapeId)
+{
+    return ReadShapeField(shapeId, false,
+                     [](const m3WorldView& v, int32_t s) { return v.hitEvents[s] != 0; });
+}
+
+extern "C" bool m3Shape_IsPreSolveEnabled(m3ShapeId shapeId)
+{
+    return ReadShapeField(shapeId, false,
+                     [](const m3WorldView& v, int32_t s) { return v.preSolve[s] != 0; });
+}
+
 // ---------------------------------------------------------------------
 // Joints (joint.c:15-330, :387-520)
 // ---------------------------------------------------------------------

@@ -174,7 +174,7 @@ def test_bad_or_unsupported_journals_are_refused_untouched(m3, libs):
     assert not _replay(ours, g.id, good + abi.journal_body_command(28, 3, 0, [float("nan"), 0, 0]))
     assert not _replay(ours, g.id, good + abi.journal_step(0.0, 4))
     assert not _replay(ours, g.id, good + abi.journal_step(1 / 60, 300))
-    unsupported = C.c_int32(40).value.to_bytes(4, "little") + (0).to_bytes(4, "little")
+    unsupported = C.c_int32(61).value.to_bytes(4, "little") + (0).to_bytes(4, "little")
     assert not _replay(ours, g.id, good + unsupported)
     assert m3.last_error()[0] == m3.M3GPU_ERR_UNSUPPORTED
     assert g.hash() == before
