@@ -477,6 +477,26 @@ M3GPU_API m3JointId m3CreateJoint(const m3JointDef* def);
  * dynamic bodies.  Negative or non-finite values are refused (no-op). */
 M3GPU_API void m3Joint_SetBreakThresholds(m3JointId jointId, float maxForce, float maxTorque);
 M3GPU_API bool m3Joint_IsValid(m3JointId jointId);
+/* Drives and switches (joint.c:548-624, 732-1129; joint.h:183-248), each
+ * journaled like the reference's and waking the joint's dynamic bodies:
+ * limits (finite and ordered; a toggled or moved limit drops its stored
+ * row impulses), motor (finite speed, finite non-negative effort),
+ * collide-connected, spring (revolute, prismatic, spherical, wheel and
+ * motor joints; finite positive hertz, finite non-negative damping ratio)
+ * and drive targets (an angle in [-pi, pi] for a revolute joint, a
+ * translation for a prismatic or wheel joint, a unit rotation for a
+ * spherical joint).  A refused value is a no-op.  The angle and
+ * translation getters read the current poses (0 for other types). */
+M3GPU_API void m3Joint_SetLimits(m3JointId jointId, bool enable, float lower, float upper);
+M3GPU_API void m3Joint_SetMotor(m3JointId jointId, bool enable, float speed, float maxEffort);
+M3GPU_API void m3Joint_SetCollideConnected(m3JointId jointId, bool collide);
+M3GPU_API bool m3Joint_GetCollideConnected(m3JointId jointId);
+M3GPU_API void m3Joint_SetSpring(m3JointId jointId, bool enable, float hertz, float dampingRatio);
+M3GPU_API void m3Joint_SetTargetAngle(m3JointId jointId, float radians);
+M3GPU_API void m3Joint_SetTargetTranslation(m3JointId jointId, float meters);
+M3GPU_API void m3Joint_SetTargetRotation(m3JointId jointId, m3Quat target);
+M3GPU_API m3real m3Joint_GetAngle(m3JointId jointId);
+M3GPU_API m3real m3Joint_GetTranslation(m3JointId jointId);
 
 /* ---------------------------------------------------------------------
  * 3. Device extensions (no reference counterpart)

@@ -489,6 +489,25 @@ def bind_shape_commands(lib: C.CDLL) -> C.CDLL:
     return lib
 
 
+def bind_joint_commands(lib: C.CDLL) -> C.CDLL:
+    """Declare the reference-named joint drives, switches and getters."""
+    for name in ("m3Joint_SetLimits", "m3Joint_SetMotor", "m3Joint_SetSpring"):
+        getattr(lib, name).argtypes = [m3JointId, C.c_bool, C.c_float, C.c_float]
+        getattr(lib, name).restype = None
+    lib.m3Joint_SetCollideConnected.argtypes = [m3JointId, C.c_bool]
+    lib.m3Joint_SetCollideConnected.restype = None
+    for name in ("m3Joint_SetTargetAngle", "m3Joint_SetTargetTranslation"):
+        getattr(lib, name).argtypes = [m3JointId, C.c_float]
+        getattr(lib, name).restype = None
+    lib.m3Joint_SetTargetRotation.argtypes = [m3JointId, m3Quat]
+    lib.m3Joint_SetTargetRotation.restype = None
+    for name, res in (("m3Joint_GetCollideConnected", C.c_bool), ("m3Joint_GetAngle", C.c_float),
+                      ("m3Joint_GetTranslation", C.c_float)):
+        getattr(lib, name).argtypes = [m3JointId]
+        getattr(lib, name).restype = res
+    return lib
+
+
 def bind_create(lib: C.CDLL) -> C.CDLL:
     """Declare the reference-named creation API on a handle."""
     lib.m3DefaultWorldDef.restype = m3WorldDef

@@ -47,6 +47,12 @@ enum
     M3_OP_SET_SHAPE_DENSITY = 43,
     M3_OP_ENABLE_SHAPE_HIT_EVENTS = 50,
     M3_OP_ENABLE_SHAPE_PRESOLVE = 51,
+    // Joint drives and switches (world_internal.h:158-163).
+    M3_OP_JOINT_SET_LIMITS = 52,
+    M3_OP_JOINT_SET_MOTOR = 53,
+    M3_OP_JOINT_SET_COLLIDE = 54,
+    M3_OP_JOINT_SET_SPRING = 56,
+    M3_OP_JOINT_SET_TARGET = 57,
 };
 
 // One command for the device kernel: `world` indexes the batch, `body`
@@ -82,6 +88,13 @@ M3_HD bool m3IsHostShapeOp(int32_t op)
 {
     return (op >= M3_OP_SET_SHAPE_FRICTION && op <= M3_OP_SET_SHAPE_DENSITY) ||
            op == M3_OP_ENABLE_SHAPE_HIT_EVENTS || op == M3_OP_ENABLE_SHAPE_PRESOLVE;
+}
+
+// Joint commands applied on the host image only: never device ops.
+M3_HD bool m3IsHostJointOp(int32_t op)
+{
+    return (op >= M3_OP_JOINT_SET_LIMITS && op <= M3_OP_JOINT_SET_COLLIDE) ||
+           op == M3_OP_JOINT_SET_SPRING || op == M3_OP_JOINT_SET_TARGET;
 }
 
 // Joint commands ride the same record: `body` is then the joint slot.

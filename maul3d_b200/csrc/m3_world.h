@@ -363,6 +363,12 @@ void m3ApplyHostBodyOp(m3HostWorld* w, const m3JournalRecordView& r);
 // restitution, rolling resistance or density; `bits` the flag, or for a
 // density whether the body's mass is rebuilt.  world.cpp.
 void m3ApplyHostShapeOp(m3HostWorld* w, const m3JournalRecordView& r);
+// Applies a validated joint command (joint.c:562-590, 620-624, 1014-1029)
+// to the host image, the joint slot in `r.body`: `bits` the enable or
+// collide switch; `setting[0..1]` the limits, the motor's speed and
+// effort or the spring's hertz and damping ratio; `setting[0]` with
+// `rotation` a drive target.  world.cpp.
+void m3ApplyHostJointOp(m3HostWorld* w, const m3JournalRecordView& r);
 // Parses and validates a whole journal against a world's bodies; false
 // (with the error set) on the first bad or unsupported record.
 // Worlds outside the world table (world.cpp): built on any thread,

@@ -293,7 +293,8 @@ bool NoSettings(const std::vector<m3JournalRecordView>& records)
 {
     for (const m3JournalRecordView& rec : records)
     {
-        if (m3IsWorldSettingOp(rec.op) || m3IsHostBodyOp(rec.op) || m3IsHostShapeOp(rec.op))
+        if (m3IsWorldSettingOp(rec.op) || m3IsHostBodyOp(rec.op) || m3IsHostShapeOp(rec.op) ||
+            m3IsHostJointOp(rec.op))
         {
             m3gpuSetError(M3GPU_ERR_UNSUPPORTED, "served journal: host-side op %d", rec.op);
             return false;

@@ -1063,6 +1063,10 @@ extern "C" bool m3World_JournalReplay(m3WorldId worldId, const void* data, int32
         {
             m3ApplyHostShapeOp(w, r);
         }
+        else if (m3IsHostJointOp(r.op))
+        {
+            m3ApplyHostJointOp(w, r);
+        }
         else
         {
             m3ApplyBodyOp(w->hv, r.op, r.body, r.v);
@@ -1221,6 +1225,63 @@ bool m3ParseJournal(const m3HostWorld* w, const uint8_t* stream, int32_t size,
                 return false;
             }
             r.body = index;
+        }
+        else if (m3IsHostJointOp(op))
+        {
+            // world.c:3050-3179: limits and motor {m3JointId; int32; float;
+            // float} (finite; limits ordered, a motor joint's budgets not
+            // negative), collide {m3JointId; int32}, spring {m3JointId;
+            // int32; float; float} (hertz finite and positive, damping
+            // finite and not negative), target {m3JointId; float; m3Quat}
+            // (finite); the id is retargeted to this world.
+            const int32_t want = op == M3_OP_JOINT_SET_COLLIDE  ? 12
+                                 : op == M3_OP_JOINT_SET_TARGET ? 28
+                                                                : 20;
+            if (bytes != want)
+            {
+                m3gpuSetError(M3GPU_ERR_INVALID, "journal: bad joint record (op %d)", op);
+                return false;
+            }
+            m3JointId id;
+            memcpy(&id, payload, 8);
+            const int32_t j = id.index1 - 1;
+            bool ok = j >= 0 && j < w->hv.sc->jointMax && w->hv.jointAlive[j] != 0 &&
+                      w->hv.jointGen[j] == id.generation;
+            int32_t enable = 0;
+            if (op == M3_OP_JOINT_SET_TARGET)
+            {
+                memcpy(&r.setting[0], payload + 8, 4);
+                memcpy(&r.rotation, payload + 12, 16);
+                const m3Quat q = r.rotation;
+                ok = ok && isfinite(r.setting[0]) && isfinite(q.x) && isfinite(q.y) &&
+                     isfinite(q.z) && isfinite(q.w);
+            }
+            else
+            {
+                memcpy(&enable, payload + 8, 4);
+                if (op != M3_OP_JOINT_SET_COLLIDE)
+                {
+                    memcpy(&r.setting[0], payload + 12, 8);
+                    const float a = r.setting[0];
+                    const float b = r.setting[1];
+                    ok = ok && isfinite(a) && isfinite(b);
+                    if (ok && op == M3_OP_JOINT_SET_LIMITS)
+                    {
+                        ok = w->hv.jtype[j] == m3_motorJoint ? a >= 0.0f && b >= 0.0f : a <= b;
+                    }
+                    if (op == M3_OP_JOINT_SET_SPRING)
+                    {
+                        ok = ok && a > 0.0f && b >= 0.0f;
+                    }
+                }
+            }
+            if (!ok)
+            {
+                m3gpuSetError(M3GPU_ERR_INVALID, "journal: stale joint or bad values (op %d)", op);
+                return false;
+            }
+            r.bits = enable != 0 ? 1u : 0u;
+            r.body = j;
         }
         else if (m3IsHostShapeOp(op))
         {

@@ -2028,6 +2028,288 @@ extern "C" void m3Joint_SetBreakThresholds(m3JointId jointId, float maxForce, fl
 }
 
 // ---------------------------------------------------------------------
+// Joint drives and switches (joint.c:548-624, 732-1129): limits, motor,
+// collide-connected, spring and drive targets.  Each public call checks
+// as the reference's, records its journal record and changes the host
+// image (the next step uploads it); replay applies the same records.
+// ---------------------------------------------------------------------
+static m3HostWorld* ResolveJoint(m3JointId id, int32_t* index)
+{
+    m3HostWorld* w = m3gpuWorldFromIndex0(id.world0);
+    const int32_t j = id.index1 - 1;
+    if (w == nullptr || j < 0 || j >= w->hv.sc->jointMax || w->hv.jointAlive[j] == 0 ||
+        w->hv.jointGen[j] != id.generation)
+    {
+        *index = -1;
+        return nullptr;
+    }
+    *index = j;
+    return w;
+}
+
+// The joint's dynamic bodies wake (joint.c:548-560).
+static void WakeJointBodies(m3WorldView& v, int32_t j)
+{
+    const int32_t ends[2] = {v.jbodyA[j], v.jbodyB[j]};
+    for (int32_t k = 0; k < 2; ++k)
+    {
+        if (ends[k] >= 0 && v.btype[ends[k]] == M3_BODY_DYNAMIC)
+        {
+            Wake(v, ends[k]);
+        }
+    }
+}
+
+void m3ApplyHostJointOp(m3HostWorld* w, const m3JournalRecordView& r)
+{
+    m3WorldView& v = w->hv;
+    const int32_t j = r.body;
+    const bool on = r.bits != 0;
+    switch (r.op)
+    {
+    case M3_OP_JOINT_SET_LIMITS:
+        // The cone angle rides limits.z and is kept; the lower and upper
+        // rows' stored impulses are dropped.
+        v.jflags[j] = (uint8_t)((v.jflags[j] & ~1u) | (on ? 1u : 0u));
+        v.jlimits[j].x = r.setting[0];
+        v.jlimits[j].y = r.setting[1];
+        v.jlimitImp[j].x = 0.0f;
+        v.jlimitImp[j].y = 0.0f;
+        break;
+    case M3_OP_JOINT_SET_MOTOR:
+        v.jflags[j] = (uint8_t)((v.jflags[j] & ~2u) | (on ? 2u : 0u));
+        v.jmotor[j].x = r.setting[0];
+        v.jmotor[j].y = r.setting[1];
+        if (v.jtype[j] == m3_genericJoint)
+        {
+            v.jlimitImp[j].y = 0.0f;
+        }
+        else
+        {
+            v.jperp[j].z = 0.0f;
+        }
+        break;
+    case M3_OP_JOINT_SET_COLLIDE:
+        v.jcollide[j] = on ? 1 : 0;
+        break;
+    case M3_OP_JOINT_SET_SPRING:
+        v.jflags[j] = (uint8_t)((v.jflags[j] & ~8u) | (on ? 8u : 0u));
+        v.jspring[j] = v3(r.setting[0], r.setting[1], 0.0f);
+        v.jspringImp[j] = v3(0.0f, 0.0f, 0.0f);
+        break;
+    case M3_OP_JOINT_SET_TARGET:
+        v.jtargetScalar[j] = r.setting[0];
+        v.jtargetQ[j] = r.rotation;
+        break;
+    default:
+        return;
+    }
+    WakeJointBodies(v, j);
+}
+
+// {m3JointId id; int32 enable; float a; float b} for limits, motor and
+// spring, {m3JointId id; int32 on} for collide, {m3JointId id; float
+// scalar; m3Quat q} for a target.
+static void JointCommand(m3HostWorld* w, m3JointId id, int32_t j, int32_t op, uint32_t bits,
+                         float a, float b, m3Quat q)
+{
+    uint8_t payload[28];
+    memset(payload, 0, sizeof(payload));
+    memcpy(payload, &id, 8);
+    int32_t bytes;
+    if (op == M3_OP_JOINT_SET_COLLIDE)
+    {
+        memcpy(payload + 8, &bits, 4);
+        bytes = 12;
+    }
+    else if (op == M3_OP_JOINT_SET_TARGET)
+    {
+        memcpy(payload + 8, &a, 4);
+        memcpy(payload + 12, &q, 16);
+        bytes = 28;
+    }
+    else
+    {
+        memcpy(payload + 8, &bits, 4);
+        memcpy(payload + 12, &a, 4);
+        memcpy(payload + 16, &b, 4);
+        bytes = 20;
+    }
+    m3JournalRecordView r;
+    memset(&r, 0, sizeof(r));
+    r.op = op;
+    r.body = j;
+    r.bits = bits;
+    r.setting[0] = a;
+    r.setting[1] = b;
+    r.rotation = q;
+    m3JournalAppend(w, op, payload, bytes);
+    m3ApplyHostJointOp(w, r);
+    w->hostDirty = true;
+}
+
+// Resolves a joint and makes its world's host image current.
+static m3HostWorld* JointForWrite(m3JointId id, int32_t* j)
+{
+    m3gpuClearError();
+    m3HostWorld* w = ResolveJoint(id, j);
+    return w != nullptr && m3gpuSyncHost(w) == M3GPU_OK ? w : nullptr;
+}
+
+extern "C" void m3Joint_SetLimits(m3JointId jointId, bool enable, float lower, float upper)
+{
+    int32_t j;
+    m3HostWorld* w = JointForWrite(jointId, &j);
+    if (w == nullptr || !isfinite(lower) || !isfinite(upper))
+    {
+        return;
+    }
+    // A motor joint's two budgets are independent non-negatives; every
+    // other type wants an ordered range.
+    if (w->hv.jtype[j] == m3_motorJoint ? (lower < 0.0f || upper < 0.0f) : lower > upper)
+    {
+        return;
+    }
+    JointCommand(w, jointId, j, M3_OP_JOINT_SET_LIMITS, enable ? 1u : 0u, lower, upper,
+                 m3IdentityQuat());
+}
+
+extern "C" void m3Joint_SetMotor(m3JointId jointId, bool enable, float speed, float maxEffort)
+{
+    int32_t j;
+    m3HostWorld* w = JointForWrite(jointId, &j);
+    if (w == nullptr || !isfinite(speed) || !isfinite(maxEffort) || maxEffort < 0.0f)
+    {
+        return;
+    }
+    JointCommand(w, jointId, j, M3_OP_JOINT_SET_MOTOR, enable ? 1u : 0u, speed, maxEffort,
+                 m3IdentityQuat());
+}
+
+extern "C" void m3Joint_SetCollideConnected(m3JointId jointId, bool collide)
+{
+    int32_t j;
+    m3HostWorld* w = JointForWrite(jointId, &j);
+    if (w != nullptr)
+    {
+        JointCommand(w, jointId, j, M3_OP_JOINT_SET_COLLIDE, collide ? 1u : 0u, 0.0f, 0.0f,
+                     m3IdentityQuat());
+    }
+}
+
+extern "C" bool m3Joint_GetCollideConnected(m3JointId jointId)
+{
+    int32_t j;
+    m3HostWorld* w = ResolveJoint(jointId, &j);
+    return w != nullptr && m3gpuSyncHost(w) == M3GPU_OK && w->hv.jcollide[j] != 0;
+}
+
+// The types whose spring drives a target (joint.c:1031-1036).
+static bool JointTypeDrives(uint8_t type)
+{
+    return type == m3_revoluteJoint || type == m3_prismaticJoint || type == m3_sphericalJoint ||
+           type == m3_wheelJoint || type == m3_motorJoint;
+}
+
+extern "C" void m3Joint_SetSpring(m3JointId jointId, bool enable, float hertz, float dampingRatio)
+{
+    int32_t j;
+    m3HostWorld* w = JointForWrite(jointId, &j);
+    if (w == nullptr || !JointTypeDrives(w->hv.jtype[j]) || !isfinite(hertz) || hertz <= 0.0f ||
+        !isfinite(dampingRatio) || dampingRatio < 0.0f)
+    {
+        return;
+    }
+    JointCommand(w, jointId, j, M3_OP_JOINT_SET_SPRING, enable ? 1u : 0u, hertz, dampingRatio,
+                 m3IdentityQuat());
+}
+
+extern "C" void m3Joint_SetTargetAngle(m3JointId jointId, float radians)
+{
+    int32_t j;
+    m3HostWorld* w = JointForWrite(jointId, &j);
+    if (w == nullptr || w->hv.jtype[j] != m3_revoluteJoint || !isfinite(radians) ||
+        radians < -M3_PI || radians > M3_PI)
+    {
+        return;
+    }
+    JointCommand(w, jointId, j, M3_OP_JOINT_SET_TARGET, 0u, radians, 0.0f, m3IdentityQuat());
+}
+
+extern "C" void m3Joint_SetTargetTranslation(m3JointId jointId, float meters)
+{
+    int32_t j;
+    m3HostWorld* w = JointForWrite(jointId, &j);
+    if (w == nullptr ||
+        (w->hv.jtype[j] != m3_prismaticJoint && w->hv.jtype[j] != m3_wheelJoint) ||
+        !isfinite(meters))
+    {
+        return;
+    }
+    JointCommand(w, jointId, j, M3_OP_JOINT_SET_TARGET, 0u, meters, 0.0f, m3IdentityQuat());
+}
+
+extern "C" void m3Joint_SetTargetRotation(m3JointId jointId, m3Quat target)
+{
+    int32_t j;
+    m3HostWorld* w = JointForWrite(jointId, &j);
+    if (w == nullptr || w->hv.jtype[j] != m3_sphericalJoint || !FiniteQuat(target))
+    {
+        return;
+    }
+    const m3real len2 =
+        target.x * target.x + target.y * target.y + target.z * target.z + target.w * target.w;
+    if (len2 < 0.99f || len2 > 1.01f)
+    {
+        return;
+    }
+    JointCommand(w, jointId, j, M3_OP_JOINT_SET_TARGET, 0u, 0.0f, 0.0f, target);
+}
+
+// The twist of B's frame about A's frame z, doubled: the revolute (and
+// wheel) angle (joint.c:968-983).
+extern "C" m3real m3Joint_GetAngle(m3JointId jointId)
+{
+    int32_t j;
+    m3HostWorld* w = ResolveJoint(jointId, &j);
+    if (w == nullptr || m3gpuSyncHost(w) != M3GPU_OK ||
+        (w->hv.jtype[j] != m3_revoluteJoint && w->hv.jtype[j] != m3_wheelJoint))
+    {
+        return 0.0f;
+    }
+    const m3WorldView& v = w->hv;
+    const m3Quat qA = m3MulQuat(v.xf[v.jbodyA[j]].q, v.jframeA[j]);
+    const m3Quat qB = m3MulQuat(v.xf[v.jbodyB[j]].q, v.jframeB[j]);
+    const m3Quat rel = m3MulQuat(m3Quat{-qA.x, -qA.y, -qA.z, qA.w}, qB);
+    const m3real twist = rel.w < 0.0f ? m3Atan2(-rel.z, -rel.w) : m3Atan2(rel.z, rel.w);
+    return 2.0f * twist;
+}
+
+// The anchor separation along the slide axis: frame z for the prismatic,
+// frame x for the wheel (joint.c:985-1011).
+extern "C" m3real m3Joint_GetTranslation(m3JointId jointId)
+{
+    int32_t j;
+    m3HostWorld* w = ResolveJoint(jointId, &j);
+    if (w == nullptr || m3gpuSyncHost(w) != M3GPU_OK ||
+        (w->hv.jtype[j] != m3_prismaticJoint && w->hv.jtype[j] != m3_wheelJoint))
+    {
+        return 0.0f;
+    }
+    const m3WorldView& v = w->hv;
+    const m3Transform xfA = v.xf[v.jbodyA[j]];
+    const m3Transform xfB = v.xf[v.jbodyB[j]];
+    const m3Vec3 pA = m3RotateVec3(xfA.q, v.jlocalA[j]);
+    const m3Vec3 pB = m3RotateVec3(xfB.q, v.jlocalB[j]);
+    const m3Vec3 d = v3((m3real)(xfB.p.x + (double)pB.x - xfA.p.x - (double)pA.x),
+                        (m3real)(xfB.p.y + (double)pB.y - xfA.p.y - (double)pA.y),
+                        (m3real)(xfB.p.z + (double)pB.z - xfA.p.z - (double)pA.z));
+    const m3Quat frame = m3MulQuat(xfA.q, v.jframeA[j]);
+    const m3Vec3 local = v.jtype[j] == m3_wheelJoint ? v3(1.0f, 0.0f, 0.0f) : v3(0.0f, 0.0f, 1.0f);
+    return m3Dot3(d, m3RotateVec3(frame, local));
+}
+
+// ---------------------------------------------------------------------
 // World settings (world.c:734-1117, world.h:92-176, 288): each public
 // setter validates its arguments as the reference's does, records its
 // journal record, and changes the world's scalars on the host image (the
