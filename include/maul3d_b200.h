@@ -411,6 +411,12 @@ M3GPU_API void m3Body_SetType(m3BodyId bodyId, m3BodyType type);
 M3GPU_API void m3Body_SetEnabled(m3BodyId bodyId, bool enabled);
 M3GPU_API void m3Body_SetSleepControls(m3BodyId bodyId, float threshold, bool canSleep);
 M3GPU_API void m3Body_SetAwake(m3BodyId bodyId, bool awake);
+/* body.c:711-760 (body.h:95-96): a debug name of at most 31 bytes (longer
+ * ones are truncated), journaled and saved in snapshots, never hashed.
+ * GetName returns "" for a stale id; the pointer stays valid until the
+ * name changes, the world is restored or the world is destroyed. */
+M3GPU_API void m3Body_SetName(m3BodyId bodyId, const char* name);
+M3GPU_API const char* m3Body_GetName(m3BodyId bodyId);
 
 /* body.h:115-123 (body.c:818-1014): commands between steps.  Forces,
  * torques and impulses act on dynamic bodies with mass; velocity sets on

@@ -462,6 +462,10 @@ def bind_body_commands(lib: C.CDLL) -> C.CDLL:
     lib.m3Body_IsAwake.restype = C.c_bool
     lib.m3Body_GetPosition.argtypes = [m3BodyId]
     lib.m3Body_GetPosition.restype = m3Pos3
+    lib.m3Body_SetName.argtypes = [m3BodyId, C.c_char_p]
+    lib.m3Body_SetName.restype = None
+    lib.m3Body_GetName.argtypes = [m3BodyId]
+    lib.m3Body_GetName.restype = C.c_char_p
     for name, res in (("m3Body_GetAllowFastRotation", C.c_bool), ("m3Body_GetType", C.c_int32),
                       ("m3Body_GetUserData", C.c_uint64), ("m3Body_IsEnabled", C.c_bool)):
         getattr(lib, name).argtypes = [m3BodyId]

@@ -40,6 +40,7 @@ enum
     M3_OP_SET_SLEEP_CONTROLS = 37,
     M3_OP_SET_AWAKE = 38,
     M3_OP_SET_ALLOW_FAST_ROTATION = 65,
+    M3_OP_SET_BODY_NAME = 68,
     // Shape materials and flags (world_internal.h:146-149, 156-157).
     M3_OP_SET_SHAPE_FRICTION = 40,
     M3_OP_SET_SHAPE_RESTITUTION = 41,
@@ -80,7 +81,7 @@ M3_HD bool m3IsWorldSettingOp(int32_t op)
 M3_HD bool m3IsHostBodyOp(int32_t op)
 {
     return (op >= M3_OP_APPLY_FORCE_AT_POINT && op <= M3_OP_SET_AWAKE) ||
-           op == M3_OP_SET_ALLOW_FAST_ROTATION;
+           op == M3_OP_SET_ALLOW_FAST_ROTATION || op == M3_OP_SET_BODY_NAME;
 }
 
 // Shape commands applied on the host image only: never device ops.

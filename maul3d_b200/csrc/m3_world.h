@@ -17,6 +17,8 @@
 // granular blocks from large mappings, page-locked chunk by chunk when a
 // world becomes device-resident, so uploads are asynchronous DMA copies.
 #define M3_HOST_PAGE 4096
+// Bytes of one body's debug name, terminator included (world_internal.h:197).
+#define M3_BODY_NAME_BYTES 32
 
 // Size classes of the host and device block allocators: `bytes` in
 // granules, rounded up to m * 2^k granules with 8 <= m < 16 (at most an
@@ -192,6 +194,9 @@ struct m3HostWorld
     // world built here: it writes a fresh world's values).
     std::vector<uint8_t> snapshotCarry;
     std::vector<uint8_t> snapshotHeaderCarry;
+    // Debug names, M3_BODY_NAME_BYTES a body slot (body.c:711-760): saved
+    // in snapshots, never hashed, never on the device.
+    std::vector<char> bodyNames;
     std::vector<float> heightFieldCellCarry;
     // Event streams of the world's last step (world.h:207-313): computed
     // on the first read after a step from the device's two pair lists and
@@ -348,6 +353,7 @@ struct m3JournalRecordView
     m3Pos3 point;        // force and impulse at a point: the world point; a pose's position
     m3Quat rotation;     // a pose's rotation
     uint32_t bits;       // motion locks, a type, a flag (canSleep for sleep controls)
+    char name[M3_BODY_NAME_BYTES]; // a body name, zero-filled past its terminator
 };
 // Applies a validated world-setting record (world.c:734-783, 1013-1082)
 // to the host image: the setting's fields, and for sleeping turned off

@@ -36,7 +36,7 @@ constexpr int32_t kSolverRevision = 21;
 // (world_internal.h): debug name bytes per body, voxel chunk, vehicle
 // wheels / engine curve points / gears, soft-body tets / particles /
 // edges / anchors, water volumes, mesh caps and material table.
-constexpr int32_t kBodyNameBytes = 32;
+constexpr int32_t kBodyNameBytes = M3_BODY_NAME_BYTES;
 constexpr int32_t kVoxelChunkBytes = 12808;
 constexpr int32_t kVehicleWheels = 8;
 constexpr int32_t kEngineCurve = 8;
@@ -229,6 +229,7 @@ struct PoolBlocks
     std::vector<uint16_t> hfGens;
     std::vector<uint8_t> hfAlive;
     std::vector<int32_t> hfQueue;
+    std::vector<char> names;
     const uint8_t* shapeType = nullptr;
     const uint8_t* shapeAlive = nullptr;
     const uint8_t* hfIndex = nullptr;
@@ -248,6 +249,7 @@ struct PoolBlocks
         hfGens.assign((size_t)w->shapeCap, 0);
         hfAlive.assign((size_t)w->shapeCap, 0);
         hfQueue.assign((size_t)w->shapeCap, 0);
+        names.assign((size_t)w->bodyCap * kBodyNameBytes, 0);
     }
     // The world's pools as the walk writes them.
     void From(const m3HostWorld* w)
@@ -260,6 +262,10 @@ struct PoolBlocks
         }
         hullGens = w->hullGen;
         bodyQueue = w->bodyFree.queue;
+        if (w->bodyNames.size() == names.size())
+        {
+            names = w->bodyNames;
+        }
         shapeQueue = w->shapeFree.queue;
         hullQueue = w->hullFree.queue;
         jointQueue = w->jointFree.queue;
@@ -303,7 +309,7 @@ void WalkFixed(BlockWalk& b, const m3HostWorld* w, const m3WorldView& v, PoolBlo
     b.Keep(v.minExt, 4 * nb);
     b.Keep(v.maxExt, 4 * nb);
     b.Keep(v.userData, 8 * nb);
-    b.Carry(kBodyNameBytes * nb, Fill::kZero); // debug names, never hashed
+    b.Keep(pb.names.data(), kBodyNameBytes * nb); // debug names, never hashed
     b.Keep(v.force, 12 * nb);
     b.Keep(v.torque, 12 * nb);
     b.Keep(v.enabled, nb);
@@ -973,6 +979,7 @@ bool m3gpuRestoreWorld(m3HostWorld* w, const void* data, int32_t size)
         }
     }
     w->snapshotCarry.swap(carry);
+    w->bodyNames.swap(pb.names);
     w->snapshotHeaderCarry.assign(raw, raw + sizeof(SnapshotHeader));
     w->heightFieldCellCarry = hfCells;
     // The heightfield slots and samples (the index per shape came with
@@ -1171,7 +1178,10 @@ bool m3ParseJournal(const m3HostWorld* w, const uint8_t* stream, int32_t size,
             const bool point =
                 op == M3_OP_APPLY_FORCE_AT_POINT || op == M3_OP_APPLY_IMPULSE_AT_POINT;
             const bool pose = op == M3_OP_SET_TRANSFORM || op == M3_OP_SET_TARGET_TRANSFORM;
-            const int32_t want = point || pose ? 48 : op == M3_OP_SET_SLEEP_CONTROLS ? 16 : 12;
+            const int32_t want = point || pose                     ? 48
+                                 : op == M3_OP_SET_BODY_NAME         ? 8 + M3_BODY_NAME_BYTES
+                                 : op == M3_OP_SET_SLEEP_CONTROLS    ? 16
+                                                                     : 12;
             if (bytes != want)
             {
                 m3gpuSetError(M3GPU_ERR_INVALID, "journal: bad body record (op %d)", op);
@@ -1198,6 +1208,13 @@ bool m3ParseJournal(const m3HostWorld* w, const uint8_t* stream, int32_t size,
                 ok = ok && isfinite(r.point.x) && isfinite(r.point.y) && isfinite(r.point.z) &&
                      isfinite(q.x) && isfinite(q.y) && isfinite(q.z) && isfinite(q.w) &&
                      qq > 0.98f && qq < 1.02f;
+            }
+            else if (op == M3_OP_SET_BODY_NAME)
+            {
+                // Any bytes; the last is forced to the terminator
+                // (world.c:2620-2641).
+                memcpy(r.name, payload + 8, M3_BODY_NAME_BYTES);
+                r.name[M3_BODY_NAME_BYTES - 1] = 0;
             }
             else if (op == M3_OP_SET_SLEEP_CONTROLS)
             {

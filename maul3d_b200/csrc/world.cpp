@@ -143,6 +143,7 @@ m3HostWorld* m3gpuNewWorld(const m3WorldDef* def)
     w->shapeFree.Init(w->shapeCap);
     w->hullFree.Init(w->shapeCap);
     w->hullGen.assign((size_t)w->shapeCap, 0);
+    w->bodyNames.assign((size_t)w->bodyCap * M3_BODY_NAME_BYTES, 0);
     w->jointFree.Init(w->jointCap);
     w->persistentBytes =
         m3LayoutPersistent(nullptr, nullptr, w->bodyCap, w->shapeCap, w->jointCap, w->pairCap);
@@ -368,6 +369,7 @@ extern "C" m3BodyId m3CreateBody(m3WorldId worldId, const m3BodyDef* def)
     v.target[i].q = m3IdentityQuat();
     v.shapeHead[i] = -1;
     v.jointHead[i] = -1;
+    memset(&w->bodyNames[(size_t)i * M3_BODY_NAME_BYTES], 0, M3_BODY_NAME_BYTES);
     w->hostDirty = true;
     m3JournalUnrecordable(w); // creation is not recorded by this path
     w->structure += 1;        // device snapshot slots saved before are void
@@ -647,6 +649,18 @@ void m3ApplyHostBodyOp(m3HostWorld* w, const m3JournalRecordView& r)
         v.locks[i] = bits != 0 ? (uint8_t)(v.locks[i] | M3_LOCKS_ALLOW_FAST_ROTATION)
                                : (uint8_t)(v.locks[i] & ~M3_LOCKS_ALLOW_FAST_ROTATION);
         break;
+    case M3_OP_SET_BODY_NAME:
+    {
+        // Up to the first zero, at most 31 bytes, the rest zeroed
+        // (body.c:711-724).
+        char* slot = &w->bodyNames[(size_t)i * M3_BODY_NAME_BYTES];
+        memset(slot, 0, M3_BODY_NAME_BYTES);
+        for (int32_t k = 0; k < M3_BODY_NAME_BYTES - 1 && r.name[k] != 0; ++k)
+        {
+            slot[k] = r.name[k];
+        }
+        break;
+    }
     default:
         break;
     }
@@ -797,6 +811,47 @@ extern "C" void m3Body_SetEnabled(m3BodyId bodyId, bool enabled)
 extern "C" void m3Body_SetAwake(m3BodyId bodyId, bool awake)
 {
     BitsCommand(bodyId, M3_OP_SET_AWAKE, awake ? 1u : 0u);
+}
+
+// {m3BodyId id; char name[32]}: the name truncated to 31 bytes and
+// zero-filled (body.c:711-756).  Names are saved in snapshots, never hashed.
+extern "C" void m3Body_SetName(m3BodyId bodyId, const char* name)
+{
+    m3gpuClearError();
+    int32_t index;
+    m3HostWorld* w = ResolveBody(bodyId, &index);
+    if (w == nullptr || m3gpuSyncHost(w) != M3GPU_OK)
+    {
+        return;
+    }
+    struct
+    {
+        m3BodyId id;
+        char name[M3_BODY_NAME_BYTES];
+    } record;
+    memset(&record, 0, sizeof(record));
+    record.id = bodyId;
+    for (int32_t k = 0; name != nullptr && k < M3_BODY_NAME_BYTES - 1 && name[k] != 0; ++k)
+    {
+        record.name[k] = name[k];
+    }
+    m3JournalRecordView r = CommandView(M3_OP_SET_BODY_NAME, index);
+    memcpy(r.name, record.name, M3_BODY_NAME_BYTES);
+    m3JournalAppend(w, M3_OP_SET_BODY_NAME, &record, (int32_t)sizeof(record));
+    m3ApplyHostBodyOp(w, r);
+}
+
+// The body's name, "" for a stale id; valid until the name changes or the
+// world goes.
+extern "C" const char* m3Body_GetName(m3BodyId bodyId)
+{
+    int32_t index;
+    m3HostWorld* w = ResolveBody(bodyId, &index);
+    if (w == nullptr)
+    {
+        return "";
+    }
+    return &w->bodyNames[(size_t)index * M3_BODY_NAME_BYTES];
 }
 
 // {m3BodyId id; float threshold; int32 canSleep}; a negative or

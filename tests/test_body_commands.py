@@ -68,6 +68,11 @@ def _controls(lib, wid):
     lib.m3Body_SetSleepControls(b[2], float("inf"), True)                         # refused
     lib.m3Body_SetAwake(b[1], False)                                              # static
     lib.m3Body_SetAwake(b[9], True)
+    lib.m3Body_SetName(b[3], b"crate")
+    lib.m3Body_SetName(b[4], b"a name longer than thirty-one bytes is cut")
+    lib.m3Body_SetName(b[5], None)
+    lib.m3Body_SetName(b[3], b"")
+    lib.m3Body_SetName(b[6], b"lantern")
 
 
 def _engines(m3, oracle):
@@ -97,6 +102,13 @@ def _without_world_index(journal: bytes) -> bytes:
     return bytes(out)
 
 
+def _snapshot(lib, wid):
+    n = lib.m3World_SnapshotSize(wid)
+    buf = (C.c_uint8 * n)()
+    assert lib.m3World_Snapshot(wid, buf, n) == n
+    return bytes(buf)
+
+
 def _getters(lib, wid, count):
     w0 = wid.index1 - 1
     rows = []
@@ -104,11 +116,12 @@ def _getters(lib, wid, count):
         b = abi.m3BodyId(i, w0, 0)
         rows.append((lib.m3Body_GetMotionLocks(b), lib.m3Body_GetAllowFastRotation(b),
                      lib.m3Body_GetType(b), lib.m3Body_GetUserData(b), lib.m3Body_IsEnabled(b),
-                     lib.m3Body_IsAwake(b)))
+                     lib.m3Body_IsAwake(b), lib.m3Body_GetName(b)))
     stale = abi.m3BodyId(2, w0, 7)
     rows.append((lib.m3Body_GetMotionLocks(stale), lib.m3Body_GetAllowFastRotation(stale),
                  lib.m3Body_GetType(stale), lib.m3Body_GetUserData(stale),
-                 lib.m3Body_IsEnabled(stale), lib.m3Body_IsAwake(stale)))
+                 lib.m3Body_IsEnabled(stale), lib.m3Body_IsAwake(stale),
+                 lib.m3Body_GetName(stale)))
     return rows
 
 
@@ -125,6 +138,10 @@ def test_body_commands_match_the_reference(m3, oracle):
         w0 = g.id.index1 - 1
         assert glib.m3Body_GetMotionLocks(abi.m3BodyId(5, w0, 0)) == 0x3F
         assert glib.m3Body_GetAllowFastRotation(abi.m3BodyId(5, w0, 0))
+        assert glib.m3Body_GetName(abi.m3BodyId(4, w0, 0)) == b"a name longer than thirty-one b"
+        assert glib.m3Body_GetName(abi.m3BodyId(6, w0, 0)) == b"lantern"
+        # Names, locks and the other controls are in the snapshot bytes.
+        assert _snapshot(glib, g.id) == _snapshot(rlib, r.id)
         g.destroy()
         r.destroy()
 
@@ -137,8 +154,37 @@ def test_reference_journal_of_body_commands_replays_here(m3, oracle):
     buf = (C.c_uint8 * len(journal)).from_buffer_copy(journal)
     assert glib.m3World_JournalReplay(g.id, buf, len(journal))
     assert g.hash() == r.hash()
+    assert _snapshot(glib, g.id) == _snapshot(rlib, r.id)
+    # A restore brings the names back.
+    g2 = m3.World.scene(SCENE_UNEVEN, 33, 40)
+    snap = _snapshot(rlib, r.id)
+    sbuf = (C.c_uint8 * len(snap)).from_buffer_copy(snap)
+    assert glib.m3World_Restore(g2.id, sbuf, len(snap))
+    assert glib.m3Body_GetName(abi.m3BodyId(6, g2.id.index1 - 1, 0)) == b"lantern"
+    assert _snapshot(glib, g2.id) == snap
+    g2.destroy()
     r.destroy()
     g.destroy()
+
+
+def test_name_records_keep_bytes_up_to_the_terminator(m3, oracle):
+    # The reference forces the last byte to zero and copies up to the
+    # first zero: bytes after it never reach the world.
+    glib, rlib = _engines(m3, oracle)
+    g = m3.World.scene(SCENE_UNEVEN, 35, 40)
+    r = oracle.RefWorld.scene(SCENE_UNEVEN, 35, 40)
+    for wid, lib in ((g.id, glib), (r.id, rlib)):
+        body = bytes(abi.m3BodyId(3, wid.index1 - 1, 0))
+        rec = abi.journal_record(68, body + b"ab\0junk" + b"z" * 25)
+        buf = (C.c_uint8 * len(rec)).from_buffer_copy(rec)
+        assert lib.m3World_JournalReplay(wid, buf, len(rec))
+        assert lib.m3Body_GetName(abi.m3BodyId(3, wid.index1 - 1, 0)) == b"ab"
+        short = abi.journal_record(68, body + b"ab")
+        buf = (C.c_uint8 * len(short)).from_buffer_copy(short)
+        assert not lib.m3World_JournalReplay(wid, buf, len(short))
+    assert _snapshot(glib, g.id) == _snapshot(rlib, r.id)
+    g.destroy()
+    r.destroy()
 
 
 def test_hostile_body_records_are_refused_whole(m3, oracle):
