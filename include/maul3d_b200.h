@@ -473,6 +473,23 @@ M3GPU_API bool m3Shape_AreHitEventsEnabled(m3ShapeId shapeId);
 M3GPU_API void m3Shape_EnablePreSolve(m3ShapeId shapeId, bool flag);
 M3GPU_API bool m3Shape_IsPreSolveEnabled(m3ShapeId shapeId);
 
+/* world.h:512-524 */
+typedef struct m3ContactData {
+    m3ShapeId shapeA;
+    m3ShapeId shapeB;
+    m3Vec3 normal; /* from shape A toward shape B */
+    int32_t pointCount;
+    m3Pos3 points[4];
+    float separations[4];
+    float normalImpulses[4];
+} m3ContactData;
+/* query.c:1330-1409 (body.h:99, shape.h:274): up to `capacity` entries,
+ * one per manifold with points touching the body or shape, in the
+ * current pair list's order; points are body A's centre of mass plus the
+ * anchor.  0 for a stale id, a null `out` or a non-positive capacity. */
+M3GPU_API int32_t m3Body_GetContactData(m3BodyId bodyId, m3ContactData* out, int32_t capacity);
+M3GPU_API int32_t m3Shape_GetContactData(m3ShapeId shapeId, m3ContactData* out, int32_t capacity);
+
 /* joint.c:15 (joint.h:134) and joint.h:136: spherical, revolute and
  * fixed joints are stepped on the device. */
 M3GPU_API m3JointDef m3DefaultJointDef(void);

@@ -512,6 +512,21 @@ def bind_joint_commands(lib: C.CDLL) -> C.CDLL:
     return lib
 
 
+class m3ContactData(C.Structure):
+    _fields_ = [("shapeA", m3ShapeId), ("shapeB", m3ShapeId), ("normal", m3Vec3),
+                ("pointCount", C.c_int32), ("points", m3Pos3 * 4),
+                ("separations", C.c_float * 4), ("normalImpulses", C.c_float * 4)]
+
+
+def bind_contact_data(lib: C.CDLL) -> C.CDLL:
+    """Declare the reference-named contact readback on a handle."""
+    lib.m3Body_GetContactData.argtypes = [m3BodyId, C.c_void_p, C.c_int32]
+    lib.m3Body_GetContactData.restype = C.c_int32
+    lib.m3Shape_GetContactData.argtypes = [m3ShapeId, C.c_void_p, C.c_int32]
+    lib.m3Shape_GetContactData.restype = C.c_int32
+    return lib
+
+
 def bind_create(lib: C.CDLL) -> C.CDLL:
     """Declare the reference-named creation API on a handle."""
     lib.m3DefaultWorldDef.restype = m3WorldDef

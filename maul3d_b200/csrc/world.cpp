@@ -1833,6 +1833,95 @@ extern "C" bool m3Shape_IsPreSolveEnabled(m3ShapeId shapeId)
                      [](const m3WorldView& v, int32_t s) { return v.preSolve[s] != 0; });
 }
 
+// Contact readback (query.c:1330-1409): one entry per manifold with
+// points touching the body or shape, in the current pair list's order.
+// Points are body A's centre of mass plus the anchor, in f64.
+static void FillContact(const m3HostWorld* w, uint64_t key, const m3Manifold& m,
+                        m3ContactData* out)
+{
+    const m3WorldView& v = w->hv;
+    const int32_t a = (int32_t)(key >> 32);
+    const int32_t b = (int32_t)(key & 0xFFFFFFFFu);
+    out->shapeA = m3ShapeId{a + 1, (uint16_t)w->slot, v.shapeGen[a]};
+    out->shapeB = m3ShapeId{b + 1, (uint16_t)w->slot, v.shapeGen[b]};
+    out->normal = m.normal;
+    out->pointCount = m.pointCount;
+    const int32_t body = v.shapeBody[a];
+    const m3Transform xf = v.xf[body];
+    const m3Vec3 rc = m3RotateVec3(xf.q, v.lc[body]);
+    for (int32_t k = 0; k < 4; ++k)
+    {
+        if (k < m.pointCount)
+        {
+            const m3ManifoldPoint& p = m.points[k];
+            out->points[k] = m3Pos3{xf.p.x + (double)(rc.x + p.anchorA.x),
+                                    xf.p.y + (double)(rc.y + p.anchorA.y),
+                                    xf.p.z + (double)(rc.z + p.anchorA.z)};
+            out->separations[k] = p.separation;
+            out->normalImpulses[k] = p.normalImpulse;
+        }
+        else
+        {
+            out->points[k] = m3Pos3{0.0, 0.0, 0.0};
+            out->separations[k] = 0.0f;
+            out->normalImpulses[k] = 0.0f;
+        }
+    }
+}
+
+// Walks the current pair list, filling an entry for each manifold with
+// points whose shapes pass `touches`.
+template <typename F>
+static int32_t ReadContacts(m3HostWorld* w, m3ContactData* out, int32_t capacity, F touches)
+{
+    if (m3gpuSyncHost(w) != M3GPU_OK)
+    {
+        return 0;
+    }
+    const m3WorldView& v = w->hv;
+    const bool second = v.sc->pairBuf != 0;
+    const uint64_t* keys = second ? v.keys1 : v.keys0;
+    const m3Manifold* man = second ? v.man1 : v.man0;
+    int32_t written = 0;
+    for (int32_t i = 0; i < v.sc->pairCount && written < capacity; ++i)
+    {
+        const int32_t a = (int32_t)(keys[i] >> 32);
+        const int32_t b = (int32_t)(keys[i] & 0xFFFFFFFFu);
+        if (touches(a, b) && man[i].pointCount > 0)
+        {
+            FillContact(w, keys[i], man[i], &out[written]);
+            written += 1;
+        }
+    }
+    return written;
+}
+
+extern "C" int32_t m3Shape_GetContactData(m3ShapeId shapeId, m3ContactData* out, int32_t capacity)
+{
+    int32_t shape;
+    m3HostWorld* w = ResolveShape(shapeId, &shape);
+    if (w == nullptr || out == nullptr || capacity <= 0)
+    {
+        return 0;
+    }
+    return ReadContacts(w, out, capacity,
+                        [shape](int32_t a, int32_t b) { return a == shape || b == shape; });
+}
+
+extern "C" int32_t m3Body_GetContactData(m3BodyId bodyId, m3ContactData* out, int32_t capacity)
+{
+    int32_t body;
+    m3HostWorld* w = ResolveBody(bodyId, &body);
+    if (w == nullptr || out == nullptr || capacity <= 0)
+    {
+        return 0;
+    }
+    const int32_t* shapeBody = w->hv.shapeBody;
+    return ReadContacts(w, out, capacity, [body, shapeBody](int32_t a, int32_t b) {
+        return shapeBody[a] == body || shapeBody[b] == body;
+    });
+}
+
 // ---------------------------------------------------------------------
 // Joints (joint.c:15-330, :387-520)
 // ---------------------------------------------------------------------
