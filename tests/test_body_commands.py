@@ -245,3 +245,42 @@ def test_hostile_body_records_are_refused_whole(m3, oracle):
     g.destroy()
     r.destroy()
     r2.destroy()
+
+
+def test_mixed_host_journals_replay_both_ways(m3, oracle):
+    # Body, shape and joint commands and world settings recorded here
+    # replay in the reference, and the reference's in this library: both
+    # worlds end with the same hash and snapshot bytes.
+    import test_joint_commands as joints
+    import test_shape_commands as shapes
+    import test_world_settings as settings
+
+    def bind(lib):
+        for f in (abi.bind_body_commands, abi.bind_shape_commands, abi.bind_joint_commands,
+                  abi.bind_settings, abi.bind_snapshot):
+            lib = f(lib)
+        return lib
+
+    glib, rlib = bind(m3.lib), bind(oracle.lib())
+
+    def session(lib, wid):
+        _commands(lib, wid)
+        shapes._commands(lib, wid)
+        joints._commands(lib, wid)
+        settings._apply_settings(lib, wid)
+
+    g = m3.World.scene(SCENE_UNEVEN, 36, 60)
+    r = oracle.RefWorld.scene(SCENE_UNEVEN, 36, 60)
+    gj = _journal(glib, g.id, lambda: session(glib, g.id))
+    rj = _journal(rlib, r.id, lambda: session(rlib, r.id))
+    assert _without_world_index(gj) == _without_world_index(rj)
+    g2 = m3.World.scene(SCENE_UNEVEN, 36, 60)
+    r2 = oracle.RefWorld.scene(SCENE_UNEVEN, 36, 60)
+    gbuf = (C.c_uint8 * len(rj)).from_buffer_copy(rj)
+    rbuf = (C.c_uint8 * len(gj)).from_buffer_copy(gj)
+    assert glib.m3World_JournalReplay(g2.id, gbuf, len(rj))
+    assert rlib.m3World_JournalReplay(r2.id, rbuf, len(gj))
+    assert g.hash() == r.hash() == g2.hash() == r2.hash()
+    assert _snapshot(glib, g2.id) == _snapshot(rlib, r2.id) == _snapshot(rlib, r.id)
+    for w in (g, r, g2, r2):
+        w.destroy()
