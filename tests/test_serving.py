@@ -288,3 +288,26 @@ def test_submissions_from_another_thread_are_all_answered(m3, oracle, ref):
     server.close()
     assert sorted(seen) == sorted(tickets) == list(range(1, 41))
     assert set(seen.values()) == {m3.M3GPU_ERR_INVALID}
+
+
+def test_host_side_records_in_served_journals_are_refused(m3, oracle, ref):
+    # World settings, shape materials and runtime controls change the
+    # host image between frames: a served journal holding one completes
+    # with the refusal.  The refusal comes while the request is prepared
+    # on the host, before any device work.
+    r = oracle.RefWorld.scene(SCENE_UNEVEN, 7, 64)
+    snap = _snapshot(ref, r.id)
+    w0 = r.id.index1 - 1
+    records = (abi.journal_record(39, C.string_at(C.byref(abi.m3Vec3(0.0, -5.0, 0.0)), 12)),
+               abi.journal_record(40, bytes(abi.m3ShapeId(3, w0, 0)) + bytes(C.c_float(0.5))),
+               abi.journal_record(38, bytes(abi.m3BodyId(3, w0, 0)) + bytes(C.c_int32(0))),
+               abi.journal_record(52, bytes(abi.m3JointId(2, w0, 0)) +
+                                  bytes(C.c_int32(1)) + bytes(C.c_float(-0.5)) +
+                                  bytes(C.c_float(0.5))))
+    server = m3.Server()
+    tickets = [server.submit(abi.encode_container(ref, snap, rec + abi.journal_step(1 / 60, 4)))
+               for rec in records]
+    done = server.run()
+    server.close()
+    for t in tickets:
+        assert done[t] == (0, m3.M3GPU_ERR_UNSUPPORTED)
